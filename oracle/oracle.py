@@ -1,0 +1,406 @@
+"""ORACLE -- test infrastructure only.
+
+CPU checker for the dgemm-b200 hot path.  Three parts:
+
+* ``orc``: ctypes view of ``liborc.so`` (orc.c), the C restatement of the reference's
+  layout routines and Cannon schedule (each C function cites the reference lines it
+  follows), plus a double-double GEMM checker for sampled entries.
+* ``ref``: ctypes view of ``_ref/libref.so`` -- the reference's OWN hot-path sources
+  (src/Decompositions/*, src/Transfers/*, src/25DCannon.cpp) compiled by oracle/Makefile
+  against in-process MPI / host-CUDA test doubles.  Present only where the reference
+  tree was available at build time; tests fall back to the committed golden fixtures.
+* numpy helpers: seeded input generators for every benchmark configuration and the
+  FP64 GEMM oracle, which is host OpenBLAS ``dgemm`` (the reference validates with
+  ``cblas_dgemm``: src/Wrappers/cuBLASMp/cuBLASMpValidator.cpp:48).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs may import this
+module.  The product never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_ORC = os.path.join(HERE, "liborc.so")
+_REF = os.path.join(HERE, "_ref", "libref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def build(ref_root: str | None = None) -> None:
+    """Compile liborc.so and, when the reference tree exists, _ref/libref.so."""
+    cmd = ["make", "-s", "-C", HERE, "all"]
+    if ref_root:
+        cmd.append(f"REF={ref_root}")
+    subprocess.run(cmd, check=True)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _ptr_array(arrs):
+    return (_dp * len(arrs))(*[_ptr(a) for a in arrs])
+
+
+class _Orc:
+    def __init__(self, path=_ORC):
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        self.L = L
+        L.orc_numroc.restype = ctypes.c_int
+        L.orc_numroc.argtypes = [ctypes.c_int] * 5
+        L.orc_pblas_local_shape.argtypes = [ctypes.c_int] * 7 + [_ip, _ip, _ip]
+        L.orc_pblas_scatter.argtypes = [ctypes.c_int] * 6 + [_dp, ctypes.c_int64, ctypes.c_void_p, _i64p]
+        L.orc_pblas_scatter.restype = ctypes.c_int
+        L.orc_pblas_gather.argtypes = [ctypes.c_int] * 6 + [_dp, ctypes.c_int64, ctypes.c_void_p, _i64p]
+        L.orc_pblas_gather.restype = ctypes.c_int
+        L.orc_block2d_grid.argtypes = [ctypes.c_int, _ip, _ip]
+        L.orc_block2d_deliver.argtypes = [ctypes.c_int64] * 3 + [ctypes.c_int] * 3 + [_dp] * 3 + [ctypes.c_void_p] * 3
+        L.orc_block2d_gather.argtypes = [ctypes.c_int64] * 2 + [ctypes.c_int] * 3 + [_dp, ctypes.c_void_p]
+        L.orc_cannon_decompose.argtypes = [ctypes.c_int64, ctypes.c_int] + [_dp] * 3 + [ctypes.c_void_p] * 3
+        L.orc_cannon_reorder.argtypes = [ctypes.c_int64, ctypes.c_int, _dp, ctypes.c_void_p]
+        L.orc_cannon_schedule.argtypes = [ctypes.c_int] * 5 + [_ip]
+        L.orc_cannon_schedule.restype = ctypes.c_int
+        L.orc_copy_block.argtypes = [ctypes.c_int64] * 2 + [_dp, _dp] + [ctypes.c_int64] * 2 + [ctypes.c_int]
+        L.orc_dgemm_dd_sample.argtypes = [ctypes.c_char, ctypes.c_char, ctypes.c_int64, ctypes.c_double, _dp,
+                                          ctypes.c_int64, _dp, ctypes.c_int64, ctypes.c_double, _dp, ctypes.c_int64,
+                                          ctypes.c_int64, _i64p, _i64p, _dp]
+
+    # -- block-cyclic --------------------------------------------------------------
+    def numroc(self, n, nb, iproc, isrproc, nprocs):
+        return self.L.orc_numroc(n, nb, iproc, isrproc, nprocs)
+
+    def pblas_shapes(self, M, N, Mb, Nb, p, q):
+        out = []
+        for r in range(p * q):
+            a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            self.L.orc_pblas_local_shape(M, N, Mb, Nb, p, q, r, a, b, c)
+            out.append((a.value, b.value, c.value))
+        return out
+
+    def pblas_scatter(self, G, Mb, Nb, p, q):
+        """Global column-major G -> list of local column-major arrays (ld = numroc rows)."""
+        G = np.asfortranarray(G, dtype=np.float64)
+        M, N = G.shape
+        shapes = self.pblas_shapes(M, N, Mb, Nb, p, q)
+        locs = [np.zeros((r, c), dtype=np.float64, order="F") for r, c, _ in shapes]
+        lld = (ctypes.c_int64 * len(locs))(*[max(r, 1) for r, _, _ in shapes])
+        rc = self.L.orc_pblas_scatter(M, N, Mb, Nb, p, q, _ptr(G), M, _ptr_array(locs), lld)
+        if rc != 0:
+            raise ValueError("block-cyclic grid leaves a rank without rows or columns")
+        return locs
+
+    def pblas_gather(self, locs, M, N, Mb, Nb, p, q):
+        G = np.zeros((M, N), dtype=np.float64, order="F")
+        locs = [np.asfortranarray(l) for l in locs]
+        lld = (ctypes.c_int64 * len(locs))(*[max(l.shape[0], 1) for l in locs])
+        rc = self.L.orc_pblas_gather(M, N, Mb, Nb, p, q, _ptr(G), M, _ptr_array(locs), lld)
+        if rc != 0:
+            raise ValueError("block-cyclic grid leaves a rank without rows or columns")
+        return G
+
+    # -- 2D block --------------------------------------------------------------------
+    def block2d_grid(self, P):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self.L.orc_block2d_grid(P, a, b)
+        return a.value, b.value
+
+    @staticmethod
+    def block2d_tiles(M, N, K, dRow, dCol):
+        """(tileM, tileN) per rank, remainder on the last grid row/column."""
+        out = []
+        for i in range(dRow):
+            for j in range(dCol):
+                tm = M // dRow + (M % dRow if i + 1 == dRow else 0)
+                tn = N // dCol + (N % dCol if j + 1 == dCol else 0)
+                out.append((tm, tn))
+        return out
+
+    def block2d_deliver(self, A, B, C, P, col_major=True):
+        M, K = A.shape
+        N = B.shape[1]
+        dRow, dCol = self.block2d_grid(P)
+        order = "F" if col_major else "C"
+        A = np.asarray(A, dtype=np.float64, order=order)
+        B = np.asarray(B, dtype=np.float64, order=order)
+        C = np.asarray(C, dtype=np.float64, order=order)
+        tiles = self.block2d_tiles(M, N, K, dRow, dCol)
+        lA = [np.zeros((tm, K), order=order) for tm, _ in tiles]
+        lB = [np.zeros((K, tn), order=order) for _, tn in tiles]
+        lC = [np.zeros((tm, tn), order=order) for tm, tn in tiles]
+        self.L.orc_block2d_deliver(M, N, K, dRow, dCol, int(col_major), _ptr(A), _ptr(B), _ptr(C), _ptr_array(lA),
+                                   _ptr_array(lB), _ptr_array(lC))
+        return lA, lB, lC
+
+    def block2d_gather(self, lC, M, N, P, col_major=True, C=None):
+        dRow, dCol = self.block2d_grid(P)
+        order = "F" if col_major else "C"
+        C = np.zeros((M, N), order=order) if C is None else np.array(C, dtype=np.float64, order=order)
+        lC = [np.asarray(l, dtype=np.float64, order=order) for l in lC]
+        self.L.orc_block2d_gather(M, N, dRow, dCol, int(col_major), _ptr(C), _ptr_array(lC))
+        return C
+
+    # -- Cannon ----------------------------------------------------------------------
+    def cannon_decompose(self, A, B, C, p):
+        M = A.shape[0]
+        A, B, C = (np.asfortranarray(x, dtype=np.float64) for x in (A, B, C))
+        lm = M // p
+        mk = lambda: [np.zeros((lm, lm), order="F") for _ in range(p * p)]
+        lA, lB, lC = mk(), mk(), mk()
+        self.L.orc_cannon_decompose(M, p, _ptr(A), _ptr(B), _ptr(C), _ptr_array(lA), _ptr_array(lB), _ptr_array(lC))
+        return lA, lB, lC
+
+    def cannon_reorder(self, lC, M, p, C=None):
+        C = np.zeros((M, M), order="F") if C is None else np.array(C, dtype=np.float64, order="F")
+        lC = [np.asfortranarray(l) for l in lC]
+        self.L.orc_cannon_reorder(M, p, _ptr(C), _ptr_array(lC))
+        return C
+
+    def cannon_schedule(self, p, c, i, j, k):
+        pc3 = int((p * p * c / c ** 3) ** 0.5 + 1e-9)
+        out = (ctypes.c_int * max(pc3, 1))()
+        ok = self.L.orc_cannon_schedule(p, c, i, j, k, out)
+        return list(out)[:pc3], bool(ok)
+
+    # -- extended-precision checker -----------------------------------------------------
+    def dgemm_dd_sample(self, A, B, alpha, beta, C0, rows, cols, ta="N", tb="N"):
+        A = np.asfortranarray(A, dtype=np.float64)
+        B = np.asfortranarray(B, dtype=np.float64)
+        K = A.shape[0] if ta.upper() != "N" else A.shape[1]
+        C0p = _ptr(np.asfortranarray(C0)) if C0 is not None else None
+        ldc = C0.shape[0] if C0 is not None else 1
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        cols = np.ascontiguousarray(cols, dtype=np.int64)
+        out = np.zeros(len(rows))
+        if C0 is not None:
+            C0 = np.asfortranarray(C0)
+            C0p = _ptr(C0)
+        self.L.orc_dgemm_dd_sample(ta.encode(), tb.encode(), K, alpha, _ptr(A), A.shape[0], _ptr(B), B.shape[0],
+                                   beta, C0p, ldc, len(rows), rows.ctypes.data_as(_i64p),
+                                   cols.ctypes.data_as(_i64p), _ptr(out))
+        return out
+
+
+class _Ref:
+    """The reference's own code (oracle/_ref/libref.so)."""
+
+    def __init__(self, path=_REF):
+        L = ctypes.CDLL(path)
+        self.L = L
+        L.ref_last_error.restype = ctypes.c_char_p
+        L.ref_numroc.argtypes = [ctypes.c_int] * 5
+        L.ref_pblas_shapes.argtypes = [ctypes.c_int] * 6 + [_ip] * 3
+        L.ref_pblas_scatter.argtypes = [ctypes.c_int] * 6 + [_dp, ctypes.c_void_p]
+        L.ref_pblas_gather.argtypes = [ctypes.c_int] * 6 + [_dp, ctypes.c_void_p]
+        L.ref_block2d_shapes.argtypes = [ctypes.c_int] * 4 + [_ip] * 4
+        L.ref_block2d_deliver.argtypes = [ctypes.c_int] * 5 + [_dp] * 3 + [ctypes.c_void_p] * 3
+        L.ref_block2d_gather.argtypes = [ctypes.c_int] * 6 + [_dp, ctypes.c_void_p]
+        L.ref_cannon_decompose.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_int] + [_dp] * 3 + [
+            ctypes.c_void_p] * 3
+        L.ref_cannon_reorder.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_void_p]
+        L.ref_cannon_fulloffload.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double, _dp, _dp, _dp]
+        L.ref_cannon_trace.argtypes = [ctypes.c_int, ctypes.c_int, _ip]
+        L.ref_set_dgemm.argtypes = [ctypes.c_void_p]
+        self._blas = None
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError("reference run failed: " + self.L.ref_last_error().decode())
+
+    def use_openblas(self, threads: int | None = None) -> bool:
+        """Route the reference's cublasDgemm to host OpenBLAS (scipy's LP64 build)."""
+        import scipy
+
+        libs = glob.glob(os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs",
+                                      "libscipy_openblas-*.so"))
+        if not libs:
+            return False
+        blas = ctypes.CDLL(libs[0])
+        if threads:
+            blas.scipy_openblas_set_num_threads(int(threads))
+        self._blas = blas
+        self.L.ref_set_dgemm(ctypes.cast(blas.scipy_cblas_dgemm, ctypes.c_void_p))
+        return True
+
+    def use_naive(self):
+        self.L.ref_set_dgemm(None)
+
+    def numroc(self, n, nb, iproc, isrproc, nprocs):
+        return self.L.ref_numroc(n, nb, iproc, isrproc, nprocs)
+
+    def pblas_shapes(self, M, N, Mb, Nb, p, q):
+        P = p * q
+        a, b, c = (ctypes.c_int * P)(), (ctypes.c_int * P)(), (ctypes.c_int * P)()
+        self._check(self.L.ref_pblas_shapes(M, N, Mb, Nb, p, q, a, b, c))
+        return [(a[r], b[r], c[r]) for r in range(P)]
+
+    def pblas_scatter(self, G, Mb, Nb, p, q):
+        G = np.asfortranarray(G, dtype=np.float64)
+        M, N = G.shape
+        shapes = self.pblas_shapes(M, N, Mb, Nb, p, q)
+        locs = [np.zeros((r, c), order="F") for r, c, _ in shapes]
+        self._check(self.L.ref_pblas_scatter(M, N, Mb, Nb, p, q, _ptr(G), _ptr_array(locs)))
+        return locs
+
+    def pblas_gather(self, locs, M, N, Mb, Nb, p, q):
+        G = np.zeros((M, N), order="F")
+        locs = [np.asfortranarray(l) for l in locs]
+        self._check(self.L.ref_pblas_gather(M, N, Mb, Nb, p, q, _ptr(G), _ptr_array(locs)))
+        return G
+
+    def block2d_shapes(self, M, N, K, P):
+        dr, dc = ctypes.c_int(), ctypes.c_int()
+        lm, ln = (ctypes.c_int * P)(), (ctypes.c_int * P)()
+        self._check(self.L.ref_block2d_shapes(M, N, K, P, dr, dc, lm, ln))
+        return dr.value, dc.value, list(lm), list(ln)
+
+    def block2d_deliver(self, A, B, C, P, col_major=True):
+        M, K = A.shape
+        N = B.shape[1]
+        order = "F" if col_major else "C"
+        A = np.asarray(A, dtype=np.float64, order=order)
+        B = np.asarray(B, dtype=np.float64, order=order)
+        C = np.asarray(C, dtype=np.float64, order=order)
+        dr, dc, lm, ln = self.block2d_shapes(M, N, K, P)
+        lA = [np.zeros((lm[r], K), order=order) for r in range(P)]
+        lB = [np.zeros((K, ln[r]), order=order) for r in range(P)]
+        lC = [np.zeros((lm[r], ln[r]), order=order) for r in range(P)]
+        self._check(self.L.ref_block2d_deliver(M, N, K, P, int(col_major), _ptr(A), _ptr(B), _ptr(C),
+                                               _ptr_array(lA), _ptr_array(lB), _ptr_array(lC)))
+        return lA, lB, lC
+
+    def block2d_gather(self, lC, M, N, K, P, col_major=True, C=None):
+        order = "F" if col_major else "C"
+        C = np.zeros((M, N), order=order) if C is None else np.array(C, dtype=np.float64, order=order)
+        lC = [np.asarray(l, dtype=np.float64, order=order) for l in lC]
+        self._check(self.L.ref_block2d_gather(M, N, K, P, int(col_major), 0, _ptr(C), _ptr_array(lC)))
+        return C
+
+    def cannon_decompose(self, A, B, C, p, c=1):
+        M = A.shape[0]
+        A, B, C = (np.array(x, dtype=np.float64, order="F") for x in (A, B, C))
+        lm = M // p
+        mk = lambda: [np.zeros((lm, lm), order="F") for _ in range(p * p * c)]
+        lA, lB, lC = mk(), mk(), mk()
+        self._check(self.L.ref_cannon_decompose(M, p, c, _ptr(A), _ptr(B), _ptr(C), _ptr_array(lA), _ptr_array(lB),
+                                                _ptr_array(lC)))
+        return lA[:p * p], lB[:p * p], lC[:p * p]
+
+    def cannon_reorder(self, lC, M, p, c=1, C=None):
+        C = np.zeros((M, M), order="F") if C is None else np.array(C, dtype=np.float64, order="F")
+        lm = M // p
+        tiles = [np.asfortranarray(l) for l in lC] + [np.zeros((lm, lm), order="F")] * (p * p * (c - 1))
+        self._check(self.L.ref_cannon_reorder(M, p, c, _ptr(C), _ptr_array(tiles)))
+        return C
+
+    def cannon_fulloffload(self, A, B, C, p, c, alpha, beta):
+        M = A.shape[0]
+        A, B = (np.array(x, dtype=np.float64, order="F") for x in (A, B))
+        C = np.array(C, dtype=np.float64, order="F")
+        self._check(self.L.ref_cannon_fulloffload(M, p, c, alpha, beta, _ptr(A), _ptr(B), _ptr(C)))
+        return C
+
+    def cannon_trace(self, p, c):
+        pc3 = int((p * p * c / c ** 3) ** 0.5 + 1e-9)
+        P = p * p * c
+        out = (ctypes.c_int * (P * pc3 * 2))()
+        self._check(self.L.ref_cannon_trace(p, c, out))
+        return np.array(out, dtype=np.int64).reshape(P, pc3, 2)
+
+
+_orc_singleton = None
+_ref_singleton = None
+
+
+def orc() -> _Orc:
+    global _orc_singleton
+    if _orc_singleton is None:
+        _orc_singleton = _Orc()
+    return _orc_singleton
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF)
+
+
+def ref() -> _Ref:
+    global _ref_singleton
+    if _ref_singleton is None:
+        _ref_singleton = _Ref()
+    return _ref_singleton
+
+
+# ---- seeded inputs (numpy PCG64) ---------------------------------------------------------
+def uniform(shape, seed, lo=-1.0, hi=1.0):
+    """i.i.d. U[lo, hi) doubles, column-major."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.asfortranarray(rng.uniform(lo, hi, size=shape))
+
+
+def ozaki_matrix(shape, seed, phi):
+    """(U[0,1) - 0.5) * exp(phi * N(0,1)), the dynamic-range stress input of the FP64
+    emulation configuration (Ozaki/Uchino/Imamura test matrices)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    u = rng.random(size=shape) - 0.5
+    n = rng.standard_normal(size=shape)
+    return np.asfortranarray(u * np.exp(phi * n))
+
+
+def normal32(shape, seed):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.asfortranarray(rng.standard_normal(size=shape, dtype=np.float32))
+
+
+# ---- FP64 GEMM oracle + error metrics ------------------------------------------------------
+def op(X, t):
+    return X.T if t.upper() in ("T", "C") else X
+
+
+def dgemm(A, B, alpha=1.0, beta=0.0, C=None, ta="N", tb="N"):
+    """Host FP64 GEMM (OpenBLAS dgemm through numpy): alpha*op(A)@op(B) + beta*C."""
+    R = alpha * (op(A, ta) @ op(B, tb))
+    if beta != 0.0 and C is not None:
+        R = R + beta * C
+    return np.asfortranarray(R)
+
+
+def rel_errors(X, R):
+    """(max elementwise relative error with |ref| in the denominator, Frobenius relative
+    error).  The reference's Derror (src/Utilities/Validation.cpp:96-99) divides by the
+    signed reference value, so negative entries pass trivially; this uses |ref|."""
+    X = np.asarray(X, dtype=np.float64)
+    R = np.asarray(R, dtype=np.float64)
+    d = np.abs(X - R)
+    den = np.abs(R)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rel = np.where(den > 0, d / den, d)
+    fro = float(np.linalg.norm(d) / max(np.linalg.norm(R), np.finfo(float).tiny))
+    return float(rel.max()) if rel.size else 0.0, fro
+
+
+def digits_of_accuracy(ref_vals, vals):
+    """The reference's Dtest_equality digit count (Validation.cpp:57-83), with |a| in the
+    denominator instead of the signed a of Derror (:96-99).  Same loop: start at 1e-8,
+    tighten by 10x while nothing fails (up to 30 digits); 0 means it failed at 1e-8."""
+    ref_vals = np.asarray(ref_vals, dtype=np.float64).ravel()
+    vals = np.asarray(vals, dtype=np.float64).ravel()
+    d = np.abs(ref_vals - vals)
+    den = np.abs(ref_vals)
+    err = np.where(ref_vals == 0, d, d / np.where(den == 0, 1, den))
+    eps, acc = 1e-8, 8
+    failed = bool((err > eps).any())
+    while eps > np.finfo(float).tiny and not failed and acc < 30:
+        eps *= 0.1
+        acc += 1
+        failed = bool((err > eps).any())
+    return 0 if acc == 8 else acc
