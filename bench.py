@@ -1,0 +1,409 @@
+"""Benchmark: FP64-accurate GEMM TFLOP/s on one B200 -- Ozaki-emulated (INT8 tensor cores)
+vs native FP64 DMMA, at equal error against the host FP64 oracle.
+
+Workload (the FP64-emulation configuration): C = alpha*A*B + beta*C with
+M = N = K = 16384, column-major, entries (U[0,1) - 0.5) * exp(phi * N(0,1)), phi = 0.5
+(phi = 4.0 is measured for error only: the kernels are data-independent), seeded
+synthetic data.  One step = one dgt_dgemm call through the C ABI.  The slice count is
+the smallest S whose max/Frobenius relative error vs the oracle is <= the native DMMA
+kernel's ("equal error").  Inputs (2 GiB each) are larger than L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's own CPU implementation of the path: its
+2.5D Cannon driver code compiled from its sources (oracle/_ref) with the local
+cublasDgemm served by host OpenBLAS, on a bounded square sample, all host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "distributed-gemm-thesis_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "FP64-accurate GEMM TFLOP/s on 1 B200: emulated vs native DMMA at equal error"
+SIZE = 16384
+PHI = 0.5
+ALPHA, BETA = 1.0, 0.0
+SEED = 20261203
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dgt", choices=["dgt", "reference"])
+    ap.add_argument("--size", type=int, default=SIZE)
+    return ap.parse_args()
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != n_gpus and n_gpus > 1:
+        raise SystemExit(f"--gpus {n_gpus} needs torchrun with WORLD_SIZE={n_gpus} (got {world})")
+    import torch
+
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- reference arm (CPU) ------------------------------------------------------------------------
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return  # the reference arm runs on rank 0 only
+    import numpy as np
+
+    import oracle as O
+
+    cores = host_cores()
+    line = {"impl": "reference", "metric": METRIC, "unit": "TFLOP/s", "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup}
+    if not O.ref_available():
+        line["unavailable"] = "reference sources were not compiled (oracle/_ref/libref.so missing)"
+        print(json.dumps(line))
+        return
+    r = O.ref()
+    r.use_openblas(cores)
+    # bounded square sample: the reference's Summa25Decomposer (p = c = 1) over one local
+    # cublasDgemm (host OpenBLAS); calibrate the size so one step takes ~2-4 s
+    M = 2048
+    A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), np.zeros((M, M), order="F")
+    t0 = time.perf_counter()
+    r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA)
+    dt = time.perf_counter() - t0
+    rate = 2 * M ** 3 / max(dt, 1e-6)
+    M = int(min(args.size, max(2048, (3.0 * rate / 2) ** (1 / 3))) // 256 * 256)
+    A, B = O.ozaki_matrix((M, M), SEED, PHI), O.ozaki_matrix((M, M), SEED + 1, PHI)
+    C = np.zeros((M, M), order="F")
+    for _ in range(args.warmup):
+        r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    v = 2 * M ** 3 / (ms * 1e-3) / 1e12
+    sample = (f"reference Summa25Decomposer::multiply (p=c=1; src/25DCannon.cpp:286-375) with cublasDgemm served "
+              f"by host OpenBLAS dgemm, M=N=K={M} of the {args.size}^3 workload")
+    line.update({"value": v, "ms_per_step": ms, "dtype": "f64", "data": "synthetic",
+                 "config": {"workload": f"FP64 GEMM {args.size}^3 (bounded sample {M}^3), phi={PHI}",
+                            "sample_size": M, "cores": cores},
+                 "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "reference",
+                                  "sample": sample},
+                 "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line))
+
+
+# ---- dgt arm ------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import numpy as np
+    import torch
+
+    import dgt
+    import oracle as O
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    n = args.size
+    flops = 2.0 * n ** 3
+    h = dgt.Handle(stream=torch.cuda.current_stream().cuda_stream)
+
+    # inputs: generated on the host (seeded), pinned, copied to the device once
+    A_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    B_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    C_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    A_np = O.ozaki_matrix((n, n), SEED + 7 * rank, PHI)
+    B_np = O.ozaki_matrix((n, n), SEED + 7 * rank + 1, PHI)
+    A_h.numpy()[:] = A_np.T  # tensor rows = matrix columns: same bytes as column-major A
+    B_h.numpy()[:] = B_np.T
+    A = A_h.cuda()
+    B = B_h.cuda()
+    C = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    C_nat = torch.zeros_like(C)
+    pa, pb, pc = A.data_ptr(), B.data_ptr(), C.data_ptr()
+
+    def run(mode, S, out=pc):
+        h.dgemm("N", "N", n, n, n, ALPHA, pa, n, pb, n, BETA, out, n, mode=mode, slices=S)
+
+    # ---- accuracy: sampled rows vs the host FP64 oracle (OpenBLAS) ----
+    rows = np.sort(np.random.default_rng(1).choice(n, 48, replace=False))
+    want = ALPHA * (A_np[rows, :] @ B_np)
+
+    def rows_err(t):
+        got = t.cpu().numpy().T[rows, :]
+        return O.rel_errors(got, want)
+
+    run(dgt.FP64_NATIVE, 0, C_nat.data_ptr())
+    torch.cuda.synchronize()
+    nat_err = rows_err(C_nat)
+    chosen, errs = None, {}
+    for S in (6, 7, 8):
+        run(dgt.FP64_OZAKI_INT8, S)
+        torch.cuda.synchronize()
+        h.check_device()
+        errs[S] = rows_err(C)
+        if chosen is None and errs[S][0] <= nat_err[0] and errs[S][1] <= nat_err[1]:
+            chosen = S
+    equal_error = chosen is not None
+    S = chosen if chosen is not None else 8
+    # phi = 4.0 error (same kernels; data-dependent accuracy only)
+    A4 = O.ozaki_matrix((n, 2048), SEED + 99, 4.0)
+    B4 = O.ozaki_matrix((2048, 1024), SEED + 98, 4.0)
+    dA4 = torch.from_numpy(np.ascontiguousarray(A4.T)).cuda()
+    dB4 = torch.from_numpy(np.ascontiguousarray(B4.T)).cuda()
+    dC4 = torch.zeros((1024, n), dtype=torch.float64, device="cuda")
+    want4 = A4 @ B4
+    phi4 = {}
+    for mode, SS in ((dgt.FP64_NATIVE, 0), (dgt.FP64_OZAKI_INT8, S), (dgt.FP64_OZAKI_INT8, 8)):
+        h.dgemm("N", "N", n, 1024, 2048, 1.0, dA4.data_ptr(), n, dB4.data_ptr(), 2048, 0.0, dC4.data_ptr(), n,
+                mode=mode, slices=max(SS, 2))
+        torch.cuda.synchronize()
+        phi4[("native" if mode == dgt.FP64_NATIVE else f"int8_s{SS}")] = O.rel_errors(
+            dC4.cpu().numpy().T, want4)
+    del dA4, dB4, dC4
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    # ---- native DMMA (reference point of the metric) ----
+    nat_ms = timed(lambda: run(dgt.FP64_NATIVE, 0, C_nat.data_ptr()), max(2, args.steps // 2), 1)
+    nat_ms = max_over_ranks(nat_ms, world)
+
+    # ---- the headline: emulated FP64 at equal error, device-resident inputs ----
+    launches0 = h.launch_count()
+    sampler = ClockSampler(local)
+    sampler.start()
+    emu_ms = timed(lambda: run(dgt.FP64_OZAKI_INT8, S), args.steps, args.warmup)
+    clocks = sampler.stop()
+    launches = (h.launch_count() - launches0) // (args.steps + args.warmup)
+    emu_ms = max_over_ranks(emu_ms, world)
+    value = world * flops / (emu_ms * 1e-3) / 1e12
+
+    # ---- roofline of the dominant kernel (ozaki_i8_gemm), timed live with events ----
+    h.set_tuning(dgt.TUNE_PROFILE, 1)
+    splits, gemms = [], []
+    for _ in range(3):
+        run(dgt.FP64_OZAKI_INT8, S)
+        sp, gm = h.last_timings()
+        splits.append(sp)
+        gemms.append(gm)
+    h.set_tuning(dgt.TUNE_PROFILE, 0)
+    gemm_ms = statistics.median(gemms)
+    split_ms = statistics.median(splits)
+    kpad = -(-n // 128) * 128
+    pairs = S * (S + 1) // 2
+    int8_ops = 2.0 * n * n * kpad * pairs  # algorithmic INT8 tensor ops per launch
+    # INT8 dense peak, measured live the way the bf16 figure in MEASURED_PEAKS.json was:
+    # a cuBLASLt INT8 GEMM (torch._int_mm) of the same size, best of 3
+    i8 = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device="cuda")
+    for _ in range(2):
+        torch._int_mm(i8, i8)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch._int_mm(i8, i8)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    int8_peak = 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+    del i8
+    achieved = int8_ops / (gemm_ms * 1e-3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "ozaki_i8_gemm_traffic.txt")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.startswith("dram_bytes_per_launch_at_16384:"):
+                traffic = float(ln.split(":")[1].split()[0])
+
+    # ---- end to end through the C ABI: pinned host in, host out, every step ----
+    def e2e_step():
+        A.copy_(A_h, non_blocking=True)
+        B.copy_(B_h, non_blocking=True)
+        run(dgt.FP64_OZAKI_INT8, S)
+        C_h.copy_(C, non_blocking=True)
+
+    e2e_ms = timed(e2e_step, max(2, args.steps // 2), 1)
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    e2e_v = world * flops / (e2e_ms * 1e-3) / 1e12
+
+    # ---- CPU baseline: the reference's validation GEMM (OpenBLAS dgemm), bounded sample ----
+    cpu = None
+    if rank == 0 and world == 1:
+        cores = host_cores()
+        ms_rows = 256
+        t0 = time.perf_counter()
+        _ = A_np[:ms_rows, :] @ B_np
+        dt = time.perf_counter() - t0
+        rate = 2.0 * ms_rows * n * n / dt
+        ms_rows = int(min(n, max(256, 12.0 * rate / (2.0 * n * n))) // 64 * 64)
+        t0 = time.perf_counter()
+        _ = A_np[:ms_rows, :] @ B_np
+        dt = time.perf_counter() - t0
+        cpu = {"value": 2.0 * ms_rows * n * n / dt / 1e12, "unit": "TFLOP/s", "cores": cores, "kind": "port",
+               "sample": f"host OpenBLAS dgemm (numpy, {cores} threads) on the first {ms_rows} rows of A "
+                         f"times B ({ms_rows}x{n}x{n}), the reference's validation GEMM "
+                         f"(src/Wrappers/cuBLASMp/cuBLASMpValidator.cpp:48)"}
+
+    peaks = measured_peaks()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": emu_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"FP64-accurate GEMM C=alpha*A*B+beta*C, M=N=K={n}, column-major, "
+                                   f"(U-0.5)*exp({PHI}*N(0,1)) inputs, Ozaki INT8 slices S={S}",
+                       "M": n, "N": n, "K": n, "alpha": ALPHA, "beta": BETA, "phi": PHI, "slices": S,
+                       "l2": "inputs larger than L2 (2 GiB each), no flush", "parallelism":
+                           f"replicas x{world}" if world > 1 else "1 GPU"},
+            "native_dmma": {"value": world * flops / (nat_ms * 1e-3) / 1e12, "ms_per_step": nat_ms,
+                            "max_rel": nat_err[0], "fro_rel": nat_err[1]},
+            "emulated": {"value": value, "slices": S, "max_rel": errs[S][0], "fro_rel": errs[S][1],
+                         "equal_error": equal_error, "speedup_vs_native": nat_ms / emu_ms,
+                         "errors_by_slices": {str(k): v for k, v in errs.items()},
+                         "split_ms": split_ms, "gemm_ms": gemm_ms},
+            "phi4_errors": {k: {"max_rel": v[0], "fro_rel": v[1]} for k, v in phi4.items()},
+            "roofline": {"bound": "tensor", "kernel": "ozaki_i8_gemm", "achieved": achieved, "peak": int8_peak,
+                         "unit": "TOP/s (INT8)", "frac": achieved / int8_peak, "traffic": traffic,
+                         "peak_source": "measured live: cuBLASLt INT8 GEMM 8192^3 (torch._int_mm), best of 3",
+                         "algorithmic": f"{pairs} digit products x 2*M*N*K_pad INT8 ops"},
+            "e2e": {"value": e2e_v, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * 8 * n * n,
+                    "d2h_bytes_per_step": 8 * n * n},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
+        }
+        print(json.dumps(line))
+    h.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,629 @@
+// C-ABI entry points of libdgt: handle, validation, and the host side of the step
+// schedules (SUMMA panels and 2.5D Cannon rotations become K-segment lists of one
+// persistent grouped launch).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dgt_internal.cuh"
+
+namespace dgt {
+
+dgt_status ensure_workspace(dgt_context* h, size_t bytes, void** out, int slot) {
+    void*& ptr = slot == 0 ? h->workspace : h->workspace2;
+    size_t& cap = slot == 0 ? h->workspace_bytes : h->workspace2_bytes;
+    if (bytes > cap) {
+        if (ptr) {
+            cudaStreamSynchronize(h->stream);
+            cudaFree(ptr);
+            ptr = nullptr;
+            cap = 0;
+        }
+        size_t want = std::max(bytes, (size_t)1 << 20);
+        cudaError_t e = cudaMalloc(&ptr, want);
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return fail(h, DGT_ERROR_ALLOC, std::string("workspace cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        cap = want;
+    }
+    *out = ptr;
+    return DGT_SUCCESS;
+}
+
+void mark(dgt_context* h, int which) {
+    if (!h->profile) return;
+    if (!h->ev[which]) cudaEventCreate(&h->ev[which]);
+    cudaEventRecord(h->ev[which], h->stream);
+    if (which == 0) h->ev_split = true;
+}
+
+static int nmod(int a, int b) { return ((a % b) + b) % b; }
+
+// Cannon k-block order for rank (i,j,k).  The reference's skew and rotations
+// (src/25DCannon.cpp:303-310, :333-334, :364-365) give t_0 = i + j - k*pc3 and
+// t_r = t_{r-1} - r (mod pc); that order is kept when the stacks together visit every
+// k-block once, else the shift-by-one order t_r = t_0 - r is used (the fix).
+static bool cannon_order(int p, int c, int i, int j, int k, int* out) {
+    int pc3 = p / c, pc = p;
+    std::vector<int> seen(pc, 0);
+    for (int kk = 0; kk < c; ++kk) {
+        int t = nmod(i + j - kk * pc3, pc);
+        for (int r = 0; r < pc3; ++r) {
+            if (r > 0) t = nmod(t - r, pc);
+            seen[t]++;
+        }
+    }
+    bool covers = std::all_of(seen.begin(), seen.end(), [](int v) { return v == 1; });
+    int t = nmod(i + j - k * pc3, pc);
+    for (int r = 0; r < pc3; ++r) {
+        if (r > 0) t = covers ? nmod(t - r, pc) : nmod(t - 1, pc);
+        out[r] = t;
+    }
+    return covers;
+}
+
+}  // namespace dgt
+
+using namespace dgt;
+
+extern "C" {
+
+const char* dgt_status_string(dgt_status s) {
+    switch (s) {
+        case DGT_SUCCESS: return "DGT_SUCCESS";
+        case DGT_ERROR_INVALID_VALUE: return "DGT_ERROR_INVALID_VALUE";
+        case DGT_ERROR_UNSUPPORTED: return "DGT_ERROR_UNSUPPORTED";
+        case DGT_ERROR_CUDA: return "DGT_ERROR_CUDA";
+        case DGT_ERROR_TIMEOUT: return "DGT_ERROR_TIMEOUT";
+        case DGT_ERROR_ALLOC: return "DGT_ERROR_ALLOC";
+        case DGT_ERROR_NOT_INITIALIZED: return "DGT_ERROR_NOT_INITIALIZED";
+    }
+    return "DGT_UNKNOWN_STATUS";
+}
+
+dgt_status dgt_create(dgt_handle_t* handle) {
+    if (!handle) return DGT_ERROR_INVALID_VALUE;
+    *handle = nullptr;
+    auto* h = new dgt_context;
+    cudaError_t e = cudaGetDevice(&h->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (e == cudaSuccess) e = cudaMalloc(&h->dev_error, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(h->dev_error, 0, sizeof(unsigned int));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (h->dev_error) cudaFree(h->dev_error);
+        delete h;
+        return DGT_ERROR_CUDA;
+    }
+    *handle = h;
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_destroy(dgt_handle_t h) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    cudaStreamSynchronize(h->stream);
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->workspace) cudaFree(h->workspace);
+    if (h->workspace2) cudaFree(h->workspace2);
+    if (h->dev_error) cudaFree(h->dev_error);
+    delete h;
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_set_stream(dgt_handle_t h, dgt_stream_t stream) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    h->stream = (cudaStream_t)stream;
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_get_stream(dgt_handle_t h, dgt_stream_t* stream) {
+    if (!h || !stream) return DGT_ERROR_NOT_INITIALIZED;
+    *stream = (dgt_stream_t)h->stream;
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_set_fp64_mode(dgt_handle_t h, dgt_fp64_mode mode, int slices) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (mode < DGT_FP64_NATIVE || mode > DGT_FP64_AUTO) return fail(h, DGT_ERROR_INVALID_VALUE, "unknown FP64 mode");
+    if (mode != DGT_FP64_NATIVE && (slices < 2 || slices > 16))
+        return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+    h->fp64_mode = mode;
+    h->slices = slices;
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_set_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t value) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    switch (knob) {
+        case DGT_TUNE_DMMA_VARIANT:
+            if (value < 0 || value >= dmma_variant_count())
+                return fail(h, DGT_ERROR_INVALID_VALUE, "unknown DMMA variant");
+            h->dmma_variant = value;
+            return DGT_SUCCESS;
+        case DGT_TUNE_OZAKI_SLICES:
+            if (value < 2 || value > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+            h->slices = value;
+            return DGT_SUCCESS;
+        case DGT_TUNE_PROFILE:
+            h->profile = value != 0;
+            return DGT_SUCCESS;
+    }
+    return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
+}
+
+int32_t dgt_last_timings(dgt_handle_t h, float* out, int32_t n) {
+    if (!h || !out || n <= 0 || !h->profile || !h->ev[1] || !h->ev[2]) return 0;
+    if (cudaEventSynchronize(h->ev[2]) != cudaSuccess) return 0;
+    float split = 0.f, gemm = 0.f;
+    if (h->ev_split && h->ev[0]) cudaEventElapsedTime(&split, h->ev[0], h->ev[1]);
+    cudaEventElapsedTime(&gemm, h->ev[1], h->ev[2]);
+    out[0] = split;
+    if (n > 1) out[1] = gemm;
+    return n > 1 ? 2 : 1;
+}
+
+dgt_status dgt_get_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t* value) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!value) return fail(h, DGT_ERROR_INVALID_VALUE, "null output");
+    switch (knob) {
+        case DGT_TUNE_DMMA_VARIANT: *value = h->dmma_variant; return DGT_SUCCESS;
+        case DGT_TUNE_OZAKI_SLICES: *value = h->slices; return DGT_SUCCESS;
+        case DGT_TUNE_PROFILE: *value = h->profile ? 1 : 0; return DGT_SUCCESS;
+    }
+    return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
+}
+
+const char* dgt_last_error(dgt_handle_t h) { return h ? h->last_error.c_str() : "null handle"; }
+
+dgt_status dgt_check_device(dgt_handle_t h) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    DGT_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    unsigned int word = 0;
+    DGT_CUDA_TRY(h, cudaMemcpy(&word, h->dev_error, sizeof(word), cudaMemcpyDeviceToHost));
+    DGT_CUDA_TRY(h, cudaMemset(h->dev_error, 0, sizeof(word)));
+    if (word & DGT_DEVERR_TIMEOUT) return fail(h, DGT_ERROR_TIMEOUT, "a device-side wait exceeded its budget");
+    if (word & DGT_DEVERR_BOUNDS) return fail(h, DGT_ERROR_INVALID_VALUE, "a device-side bounds check failed");
+    return DGT_SUCCESS;
+}
+
+int64_t dgt_launch_count(dgt_handle_t h) { return h ? h->launches.load() : 0; }
+
+int32_t dgt_numroc(int32_t n, int32_t nb, int32_t iproc, int32_t isrproc, int32_t nprocs) {
+    // pblasDecomposition.cpp:3-23
+    if (nb <= 0 || nprocs <= 0) return 0;
+    int myDistance = (nprocs + iproc - isrproc) % nprocs;
+    int numBlocks = n / nb;
+    int r = (numBlocks / nprocs) * nb;
+    int extra = numBlocks % nprocs;
+    if (myDistance < extra)
+        r += nb;
+    else if (myDistance == extra)
+        r += n % nb;
+    return r;
+}
+
+dgt_status dgt_block2d_grid(int32_t P, int32_t* dRow, int32_t* dCol) {
+    // calculateVirtualDeviceGrid, 2DBlockSequentialDecomposition.cpp:27-54
+    if (P <= 0 || !dRow || !dCol) return DGT_ERROR_INVALID_VALUE;
+    int Px = (int)std::sqrt((double)P), Py = Px;
+    if (Px == 0) {
+        Py = P;
+        Px = 1;
+    }
+    int counter;
+    for (counter = Px; counter > 0; --counter)
+        if (P % counter == 0) break;
+    if (counter == 0) {
+        Px = P;
+        Py = 1;
+    } else {
+        Px = counter;
+        Py = P / counter;
+    }
+    *dRow = Py;
+    *dCol = Px;
+    return DGT_SUCCESS;
+}
+
+int32_t dgt_cannon_schedule(int32_t p, int32_t c, int32_t i, int32_t j, int32_t k, int32_t* out) {
+    if (p <= 0 || c <= 0 || p % c != 0 || !out) return -1;
+    return cannon_order(p, c, i, j, k, out) ? 1 : 0;
+}
+
+// ---- local GEMM -----------------------------------------------------------------------
+
+static dgt_status validate_gemm(dgt_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k,
+                                const void* A, int64_t lda, const void* B, int64_t ldb, const void* C, int64_t ldc) {
+    if (!valid_op(ta) || !valid_op(tb)) return fail(h, DGT_ERROR_INVALID_VALUE, "transpose must be N, T or C");
+    if (m < 0 || n < 0 || k < 0) return fail(h, DGT_ERROR_INVALID_VALUE, "negative dimension");
+    int64_t rowsA = is_trans(ta) ? k : m, rowsB = is_trans(tb) ? n : k;
+    if (lda < std::max<int64_t>(1, rowsA)) return fail(h, DGT_ERROR_INVALID_VALUE, "lda < rows of A");
+    if (ldb < std::max<int64_t>(1, rowsB)) return fail(h, DGT_ERROR_INVALID_VALUE, "ldb < rows of B");
+    if (ldc < std::max<int64_t>(1, m)) return fail(h, DGT_ERROR_INVALID_VALUE, "ldc < m");
+    if (m > 0 && n > 0 && !C) return fail(h, DGT_ERROR_INVALID_VALUE, "C is null");
+    if (m > 0 && n > 0 && k > 0 && (!A || !B)) return fail(h, DGT_ERROR_INVALID_VALUE, "A or B is null");
+    return DGT_SUCCESS;
+}
+
+static dgt_status native_single(dgt_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
+                                const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                                int64_t ldc) {
+    std::vector<Problem> probs(1);
+    Problem& p = probs[0];
+    p.m = m;
+    p.n = n;
+    p.alpha = (k == 0) ? 0.0 : alpha;
+    p.beta = beta;
+    p.C = C;
+    p.ldc = ldc;
+    p.seg_begin = 0;
+    p.seg_count = 1;
+    p.transa = is_trans(ta);
+    p.transb = is_trans(tb);
+    std::vector<KSegment> segs{KSegment{A, B, lda, ldb, k}};
+    h->ev_split = false;
+    mark(h, 1);
+    dgt_status st = launch_dmma_grouped(h, probs, segs);
+    mark(h, 2);
+    return st;
+}
+
+dgt_status dgt_dgemm_ex(dgt_handle_t h, char ta, char tb, int64_t m, int64_t n, int64_t k, const double* alpha,
+                        const double* A, int64_t lda, const double* B, int64_t ldb, const double* beta, double* C,
+                        int64_t ldc, dgt_fp64_mode mode, int slices) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!alpha || !beta) return fail(h, DGT_ERROR_INVALID_VALUE, "alpha/beta pointer is null");
+    dgt_status st = validate_gemm(h, ta, tb, m, n, k, A, lda, B, ldb, C, ldc);
+    if (st != DGT_SUCCESS) return st;
+    if (m == 0 || n == 0) return DGT_SUCCESS;
+    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_OZAKI_INT8;
+    if (mode == DGT_FP64_NATIVE || k == 0)
+        return native_single(h, ta, tb, m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc);
+    if (slices < 2 || slices > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+    return ozaki_dgemm(h, is_trans(ta), is_trans(tb), m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc, mode, slices);
+}
+
+dgt_status dgt_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64_t n, int64_t k, const double* alpha,
+                     const double* A, int64_t lda, const double* B, int64_t ldb, const double* beta, double* C,
+                     int64_t ldc) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    return dgt_dgemm_ex(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, h->fp64_mode, h->slices);
+}
+
+dgt_status dgt_dgemm_grouped(dgt_handle_t h, int count, const dgt_gemm_desc* d, dgt_fp64_mode mode, int slices) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (count < 0 || (count > 0 && !d)) return fail(h, DGT_ERROR_INVALID_VALUE, "bad descriptor array");
+    for (int i = 0; i < count; ++i) {
+        dgt_status st = validate_gemm(h, d[i].transa, d[i].transb, d[i].m, d[i].n, d[i].k, d[i].A, d[i].lda, d[i].B,
+                                      d[i].ldb, d[i].C, d[i].ldc);
+        if (st != DGT_SUCCESS) return st;
+    }
+    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
+    if (mode != DGT_FP64_NATIVE) {
+        for (int i = 0; i < count; ++i) {
+            if (d[i].m == 0 || d[i].n == 0) continue;
+            dgt_status st = dgt_dgemm_ex(h, d[i].transa, d[i].transb, d[i].m, d[i].n, d[i].k, &d[i].alpha, d[i].A,
+                                         d[i].lda, d[i].B, d[i].ldb, &d[i].beta, d[i].C, d[i].ldc, mode, slices);
+            if (st != DGT_SUCCESS) return st;
+        }
+        return DGT_SUCCESS;
+    }
+    std::vector<Problem> probs;
+    std::vector<KSegment> segs;
+    probs.reserve(count);
+    segs.reserve(count);
+    for (int i = 0; i < count; ++i) {
+        Problem p{};
+        p.m = d[i].m;
+        p.n = d[i].n;
+        p.alpha = d[i].k == 0 ? 0.0 : d[i].alpha;
+        p.beta = d[i].beta;
+        p.C = d[i].C;
+        p.ldc = d[i].ldc;
+        p.seg_begin = (int32_t)segs.size();
+        p.seg_count = 1;
+        p.transa = is_trans(d[i].transa);
+        p.transb = is_trans(d[i].transb);
+        segs.push_back(KSegment{d[i].A, d[i].B, d[i].lda, d[i].ldb, d[i].k});
+        probs.push_back(p);
+    }
+    return launch_dmma_grouped(h, probs, segs);
+}
+
+// ---- SUMMA on block-cyclic local buffers -------------------------------------------------
+
+dgt_status dgt_summa(dgt_handle_t h, const dgt_grid_layout* L, int64_t M, int64_t N, int64_t K, double alpha,
+                     const double* const* A_loc, const int64_t* lldA, const double* const* B_loc,
+                     const int64_t* lldB, double beta, double* const* C_loc, const int64_t* lldC, dgt_fp64_mode mode,
+                     int slices) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!L || !A_loc || !B_loc || !C_loc || !lldA || !lldB || !lldC)
+        return fail(h, DGT_ERROR_INVALID_VALUE, "null argument");
+    const int p = L->p, q = L->q;
+    if (p <= 0 || q <= 0 || L->c != 1) return fail(h, DGT_ERROR_INVALID_VALUE, "SUMMA needs p, q >= 1 and c == 1");
+    if (L->mb <= 0 || L->nb <= 0 || L->kb <= 0) return fail(h, DGT_ERROR_INVALID_VALUE, "block sizes must be > 0");
+    if (M < 0 || N < 0 || K < 0 || M > INT32_MAX || N > INT32_MAX || K > INT32_MAX)
+        return fail(h, DGT_ERROR_INVALID_VALUE, "dimension out of range");
+    const int64_t mb = L->mb, nb = L->nb, kb = L->kb;
+    auto roc = [](int64_t n, int64_t b, int i, int np) { return (int64_t)dgt_numroc((int)n, (int)b, i, 0, np); };
+    for (int r = 0; r < p * q; ++r) {
+        int i = r / q;
+        if (lldC[r] < std::max<int64_t>(1, roc(M, mb, i, p))) return fail(h, DGT_ERROR_INVALID_VALUE, "lldC < rows");
+        if (lldA[r] < std::max<int64_t>(1, roc(M, mb, i, p))) return fail(h, DGT_ERROR_INVALID_VALUE, "lldA < rows");
+        if (lldB[r] < std::max<int64_t>(1, roc(K, kb, i, p))) return fail(h, DGT_ERROR_INVALID_VALUE, "lldB < rows");
+    }
+    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
+    const int64_t kblocks = ceil_div(K, kb);
+    std::vector<Problem> probs;
+    std::vector<KSegment> segs;
+    for (int i = 0; i < p; ++i) {
+        for (int j = 0; j < q; ++j) {
+            const int r = i * q + j;
+            Problem pr{};
+            pr.m = roc(M, mb, i, p);
+            pr.n = roc(N, nb, j, q);
+            pr.alpha = K == 0 ? 0.0 : alpha;
+            pr.beta = beta;
+            pr.C = C_loc[r];
+            pr.ldc = lldC[r];
+            pr.seg_begin = (int32_t)segs.size();
+            // Panel t: A's block column t lives on process column t mod q at local column
+            // (t div q)*kb; B's block row t on process row t mod p at local row (t div p)*kb.
+            // Panels are visited owner pair by owner pair (t mod q, t mod p) so that runs
+            // that are contiguous in both local buffers merge into one segment.
+            std::vector<std::vector<int64_t>> classes;
+            std::vector<std::pair<int, int>> keys;
+            for (int64_t t = 0; t < kblocks; ++t) {
+                std::pair<int, int> key((int)(t % q), (int)(t % p));
+                auto it = std::find(keys.begin(), keys.end(), key);
+                if (it == keys.end()) {
+                    keys.push_back(key);
+                    classes.push_back({t});
+                } else {
+                    classes[it - keys.begin()].push_back(t);
+                }
+            }
+            for (auto& cls : classes) {
+                for (int64_t t : cls) {
+                    int ra = i * q + (int)(t % q);
+                    int rb = (int)(t % p) * q + j;
+                    int64_t kt = std::min(kb, K - t * kb);
+                    const double* a = A_loc[ra] + (t / q) * kb * lldA[ra];
+                    const double* b = B_loc[rb] + (t / p) * kb;
+                    if (pr.seg_count > 0) {
+                        KSegment& last = segs.back();
+                        if (last.lda == lldA[ra] && last.ldb == lldB[rb] && last.A + last.k * last.lda == a &&
+                            last.B + last.k == b) {
+                            last.k += kt;
+                            continue;
+                        }
+                    }
+                    segs.push_back(KSegment{a, b, lldA[ra], lldB[rb], kt});
+                    pr.seg_count++;
+                }
+            }
+            if (pr.seg_count == 0) {  // K == 0: C = beta*C
+                segs.push_back(KSegment{nullptr, nullptr, 1, 1, 0});
+                pr.seg_count = 1;
+            }
+            probs.push_back(pr);
+        }
+    }
+    if (mode == DGT_FP64_NATIVE) return launch_dmma_grouped(h, probs, segs);
+    return fail(h, DGT_ERROR_UNSUPPORTED, "SUMMA with Ozaki emulation is not implemented in this build");
+}
+
+// ---- 2.5D Cannon -----------------------------------------------------------------------------
+
+dgt_status dgt_cannon25d(dgt_handle_t h, int64_t M, int32_t p, int32_t c, char ta, char tb, double alpha,
+                         const double* const* A_tiles, const double* const* B_tiles, double beta,
+                         double* const* C_tiles, dgt_fp64_mode mode, int slices) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!A_tiles || !B_tiles || !C_tiles) return fail(h, DGT_ERROR_INVALID_VALUE, "null tile array");
+    // Summa25Decomposer ctor checks (src/25DCannon.cpp:7-23), as status codes
+    if (p <= 0 || c <= 0 || p % c != 0) return fail(h, DGT_ERROR_INVALID_VALUE, "need p % c == 0");
+    if (M <= 0 || M % p != 0) return fail(h, DGT_ERROR_INVALID_VALUE, "need M % p == 0");
+    if (!valid_op(ta) || !valid_op(tb)) return fail(h, DGT_ERROR_INVALID_VALUE, "transpose must be N, T or C");
+    if (p * p > 256) return fail(h, DGT_ERROR_UNSUPPORTED, "more than 256 tiles per stack");
+    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
+    if (mode != DGT_FP64_NATIVE)
+        return fail(h, DGT_ERROR_UNSUPPORTED, "Cannon with Ozaki emulation is not implemented in this build");
+    const int64_t lm = M / p, tile = lm * lm;
+    const int pc3 = p / c;
+    double* W = nullptr;
+    if (c > 1) {
+        void* ws = nullptr;
+        dgt_status st = ensure_workspace(h, (size_t)(c - 1) * p * p * tile * sizeof(double), &ws, 0);
+        if (st != DGT_SUCCESS) return st;
+        W = (double*)ws;
+    }
+    std::vector<Problem> probs;
+    std::vector<KSegment> segs;
+    std::vector<int> order(pc3);
+    for (int k = 0; k < c; ++k) {
+        for (int i = 0; i < p; ++i) {
+            for (int j = 0; j < p; ++j) {
+                cannon_order(p, c, i, j, k, order.data());
+                Problem pr{};
+                pr.m = lm;
+                pr.n = lm;
+                pr.alpha = alpha;
+                // stack 0 carries beta*C (src/25DCannon.cpp:322); other stacks start at 0
+                pr.beta = (k == 0) ? beta : 0.0;
+                pr.C = (k == 0) ? C_tiles[i * p + j] : W + ((int64_t)(k - 1) * p * p + i * p + j) * tile;
+                pr.ldc = lm;
+                pr.transa = is_trans(ta);
+                pr.transb = is_trans(tb);
+                pr.seg_begin = (int32_t)segs.size();
+                pr.seg_count = pc3;
+                for (int s = 0; s < pc3; ++s) {
+                    int t = order[s];
+                    segs.push_back(KSegment{A_tiles[i * p + t], B_tiles[t * p + j], lm, lm, lm});
+                }
+                probs.push_back(pr);
+            }
+        }
+    }
+    dgt_status st = launch_dmma_grouped(h, probs, segs);
+    if (st != DGT_SUCCESS || c == 1) return st;
+    // stack reduction (reduceResult, src/25DCannon.cpp:203-228) into the stack-0 tiles
+    return launch_stack_reduce(h, tile, p * p, c - 1, C_tiles, W, (int64_t)p * p * tile);
+}
+
+// ---- layout ------------------------------------------------------------------------------------
+
+static dgt_status check_cyclic(dgt_context* h, int64_t M, int64_t N, int64_t mb, int64_t nb, int p, int q,
+                               const void* g, int64_t ldg, const void* locals, const int64_t* lld) {
+    if (M < 0 || N < 0 || mb <= 0 || nb <= 0 || p <= 0 || q <= 0)
+        return fail(h, DGT_ERROR_INVALID_VALUE, "bad sizes or grid");
+    if (M > INT32_MAX || N > INT32_MAX) return fail(h, DGT_ERROR_INVALID_VALUE, "dimension out of range");
+    if (ldg < std::max<int64_t>(1, M)) return fail(h, DGT_ERROR_INVALID_VALUE, "ldg < M");
+    if (!g || !locals || !lld) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    for (int r = 0; r < p * q; ++r) {
+        int64_t rows = dgt_numroc((int)M, (int)mb, r / q, 0, p);
+        if (lld[r] < std::max<int64_t>(1, rows)) return fail(h, DGT_ERROR_INVALID_VALUE, "lld < local rows");
+    }
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_pack_block_cyclic(dgt_handle_t h, int64_t M, int64_t N, int64_t mb, int64_t nb, int32_t p, int32_t q,
+                                 const double* global, int64_t ldg, double* const* locals, const int64_t* lld) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    dgt_status st = check_cyclic(h, M, N, mb, nb, p, q, global, ldg, locals, lld);
+    if (st != DGT_SUCCESS) return st;
+    return launch_block_cyclic(h, true, M, N, mb, nb, p, q, (double*)global, ldg, locals, lld);
+}
+
+dgt_status dgt_unpack_block_cyclic(dgt_handle_t h, int64_t M, int64_t N, int64_t mb, int64_t nb, int32_t p,
+                                   int32_t q, double* global, int64_t ldg, const double* const* locals,
+                                   const int64_t* lld) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    dgt_status st = check_cyclic(h, M, N, mb, nb, p, q, global, ldg, locals, lld);
+    if (st != DGT_SUCCESS) return st;
+    return launch_block_cyclic(h, false, M, N, mb, nb, p, q, global, ldg, (double* const*)locals, lld);
+}
+
+// One strided copy in the reference's convention: copyBlock swaps rows and columns
+// when not column-major (sharedTransfers.cpp:43-44), as does MPI_Type_vector's use.
+static HostCopy mk_copy(int64_t rows, int64_t cols, const double* src, int64_t ldS, double* dst, int64_t ldD,
+                        bool col_major) {
+    if (!col_major) std::swap(rows, cols);
+    return HostCopy{src, dst, ldS, ldD, rows, cols};
+}
+
+dgt_status dgt_pack_block2d(dgt_handle_t h, int64_t M, int64_t N, int64_t K, int32_t P, int32_t col_major,
+                            const double* A, const double* B, const double* C, double* const* lA, double* const* lB,
+                            double* const* lC) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (M < 0 || N < 0 || K < 0 || P <= 0) return fail(h, DGT_ERROR_INVALID_VALUE, "bad sizes");
+    if (!A || !B || !C || !lA || !lB || !lC) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    int dRow, dCol;
+    dgt_block2d_grid(P, &dRow, &dCol);
+    if (M < dRow || N < dCol) return fail(h, DGT_ERROR_INVALID_VALUE, "matrix smaller than the grid");
+    bool cm = col_major != 0;
+    std::vector<HostCopy> copies;
+    // deliverMatrix, 2DBlockSequentialDecomposition.cpp:78-144
+    for (int i = 0; i < dRow; ++i) {
+        int64_t tileM = M / dRow + ((i + 1 == dRow) ? M % dRow : 0);
+        for (int j = 0; j < dCol; ++j) {
+            int r = i * dCol + j;
+            int64_t tileN = N / dCol + ((j + 1 == dCol) ? N % dCol : 0);
+            int64_t aOff = (M / dRow) * K * i, bOff = (N / dCol) * j, cOff = (M / dRow) * N * i + (N / dCol) * j;
+            int64_t lda = K, ldb = N, ldc = N, llda = K, lldb = tileN, lldc = tileN;
+            if (cm) {
+                aOff = (M / dRow) * i;
+                bOff = (N / dCol) * K * j;
+                cOff = (N / dCol) * M * j + (M / dRow) * i;
+                lda = M;
+                ldb = K;
+                ldc = M;
+                llda = tileM;
+                lldb = K;
+                lldc = tileM;
+            }
+            copies.push_back(mk_copy(tileM, K, A + aOff, lda, lA[r], llda, cm));
+            copies.push_back(mk_copy(K, tileN, B + bOff, ldb, lB[r], lldb, cm));
+            copies.push_back(mk_copy(tileM, tileN, C + cOff, ldc, lC[r], lldc, cm));
+        }
+    }
+    return launch_strided_copies(h, copies);
+}
+
+dgt_status dgt_unpack_block2d(dgt_handle_t h, int64_t M, int64_t N, int32_t P, int32_t col_major, double* C,
+                              const double* const* lC) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (M < 0 || N < 0 || P <= 0) return fail(h, DGT_ERROR_INVALID_VALUE, "bad sizes");
+    if (!C || !lC) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    int dRow, dCol;
+    dgt_block2d_grid(P, &dRow, &dCol);
+    if (M < dRow || N < dCol) return fail(h, DGT_ERROR_INVALID_VALUE, "matrix smaller than the grid");
+    bool cm = col_major != 0;
+    std::vector<HostCopy> copies;
+    // gatherResult, 2DBlockSequentialDecomposition.cpp:185-236 (every tile strided; the
+    // reference's copyBlock shortcut for rank 0 is not reproduced, see dgt.h)
+    for (int i = 0; i < dRow; ++i) {
+        int64_t tileM = M / dRow + ((i + 1 == dRow) ? M % dRow : 0);
+        for (int j = 0; j < dCol; ++j) {
+            int r = i * dCol + j;
+            int64_t tileN = N / dCol + ((j + 1 == dCol) ? N % dCol : 0);
+            int64_t cOff = (M / dRow) * N * i + (N / dCol) * j, ldc = N, lldc = tileN;
+            if (cm) {
+                cOff = (N / dCol) * M * j + (M / dRow) * i;
+                ldc = M;
+                lldc = tileM;
+            }
+            copies.push_back(mk_copy(tileM, tileN, lC[r], lldc, C + cOff, ldc, cm));
+        }
+    }
+    return launch_strided_copies(h, copies);
+}
+
+dgt_status dgt_pack_cannon2d(dgt_handle_t h, int64_t M, int32_t p, const double* A, const double* B,
+                             const double* C, double* const* lA, double* const* lB, double* const* lC) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (p <= 0 || M <= 0 || M % p != 0) return fail(h, DGT_ERROR_INVALID_VALUE, "need M % p == 0");
+    if (!A || !B || !C || !lA || !lB || !lC) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    const int64_t lm = M / p;
+    std::vector<HostCopy> copies;
+    // decompose2D, src/25DCannon.cpp:113-136: tile (i,j) at &X[lm*(j*M + i)], ld M
+    for (int i = 0; i < p; ++i)
+        for (int j = 0; j < p; ++j) {
+            int r = i * p + j;
+            int64_t off = lm * (j * M + i);
+            copies.push_back(HostCopy{A + off, lA[r], M, lm, lm, lm});
+            copies.push_back(HostCopy{B + off, lB[r], M, lm, lm, lm});
+            copies.push_back(HostCopy{C + off, lC[r], M, lm, lm, lm});
+        }
+    return launch_strided_copies(h, copies);
+}
+
+dgt_status dgt_unpack_cannon2d(dgt_handle_t h, int64_t M, int32_t p, double* C, const double* const* lC) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (p <= 0 || M <= 0 || M % p != 0) return fail(h, DGT_ERROR_INVALID_VALUE, "need M % p == 0");
+    if (!C || !lC) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    const int64_t lm = M / p;
+    std::vector<HostCopy> copies;
+    // reorderMatrix, src/25DCannon.cpp:254-271
+    for (int i = 0; i < p; ++i)
+        for (int j = 0; j < p; ++j) copies.push_back(HostCopy{lC[i * p + j], C + lm * (j * M + i), lm, M, lm, lm});
+    return launch_strided_copies(h, copies);
+}
+
+dgt_status dgt_copy_block(dgt_handle_t h, int64_t rows, int64_t cols, const double* src, double* dst, int64_t ldS,
+                          int64_t ldD, int32_t col_major) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (rows < 0 || cols < 0) return fail(h, DGT_ERROR_INVALID_VALUE, "negative size");
+    if (rows * cols == 0) return DGT_SUCCESS;  // copyBlock returns early (sharedTransfers.cpp:38-39)
+    if (!src || !dst) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    HostCopy c = mk_copy(rows, cols, src, ldS, dst, ldD, col_major != 0);
+    if (ldS < c.rows || ldD < c.rows) return fail(h, DGT_ERROR_INVALID_VALUE, "leading dimension < run length");
+    return launch_strided_copies(h, {c});
+}
+
+}  // extern "C"

@@ -1,0 +1,349 @@
+// Native FP64 GEMM on the FP64 tensor cores of sm_100a (DMMA, mma.sync .f64).
+//
+// This is the drop-in for the reference's local cublasDgemm (src/25DCannon.cpp:324-325,
+// :356-357; src/25DCannonNCCL.cpp:165-166, :202-203, :260-261, :291-292).  tcgen05 has no
+// FP64 kind, so FP64 tensor work on Blackwell goes through warp-level DMMA.
+//
+// One persistent kernel serves every caller: a plain GEMM is one problem with one
+// K-segment; a SUMMA / Cannon virtual rank is one problem whose K-segments are its step
+// schedule (panel reads replace the reference's broadcasts and shifts); a grouped
+// workload is many problems.  CTAs walk a static round-robin tile list (no inter-CTA
+// waits), so the launch cannot deadlock.
+//
+// Tile: 128 x 128 x 16, 8 warps (2 x 4), warp tile 64 x 32 of m16n8k4 DMMAs, a 4-stage
+// cp.async ring in shared memory padded so fragment loads are bank-conflict free.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "dgt_internal.cuh"
+
+namespace dgt {
+namespace {
+
+constexpr int BM = 128, BN = 128, THREADS = 256;
+constexpr int PAD = 4;
+constexpr int LD_MN = BM + PAD;  // [k][mn] layout row stride (doubles): 1056 B = 32 mod 128 banks
+constexpr int GROUP_M = 8;       // tile rasterisation group for L2 reuse
+
+// Kernel variants (the autotuner's knob): DMMA shape m16n8k{4,8}, K depth of a stage, ring depth.
+template <int MMAK_, int BK_, int STAGES_>
+struct Cfg {
+    static constexpr int MMAK = MMAK_, BK = BK_, STAGES = STAGES_;
+    static constexpr int LD_K = BK + PAD;  // [mn][k] row stride: (BK+4)*8 B = 32 mod 128 for BK in {16, 32}
+    static constexpr int STAGE_ELEMS = (BM * LD_K > BK * LD_MN) ? BM * LD_K : BK * LD_MN;
+    static constexpr size_t SMEM = (size_t)2 * STAGES * STAGE_ELEMS * sizeof(double);
+};
+constexpr int MAX_INLINE_PROBS = 32, MAX_INLINE_SEGS = 160;
+
+struct GroupedParams {
+    int nprob;
+    int total_tiles;
+    const Problem* probs;  // global table, or null -> inline
+    const KSegment* segs;
+    Problem inl_probs[MAX_INLINE_PROBS];
+    KSegment inl_segs[MAX_INLINE_SEGS];
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// Loads one BK-slice of an operand tile into shared memory.
+//  mn_major: global element (mn, k) at base[mn + k*ld]  -> smem [k][mn], row stride LD_MN
+//  else    : global element (mn, k) at base[k + mn*ld]  -> smem [mn][k], row stride LD_K
+// mn_lim / k_lim: valid extents from (mn0, k0); outside is zero-filled.
+template <int BK, int LD_K>
+__device__ __forceinline__ void load_tile(double* s, const double* base, int64_t ld, bool mn_major, int64_t mn0,
+                                          int64_t k0, int64_t mn_lim, int64_t k_lim, bool vec16, int tid) {
+    const uint32_t s_base = smem_u32(s);
+    if (mn_major) {
+        // BK columns of BM contiguous doubles: BK*64 two-double chunks
+#pragma unroll
+        for (int i = 0; i < BK / 4; ++i) {
+            int c = tid + i * THREADS;
+            int k = c >> 6;
+            int mn = (c & 63) * 2;
+            int64_t rem = mn_lim - mn;
+            int valid = (k < k_lim) ? (int)(rem >= 2 ? 2 : (rem > 0 ? rem : 0)) : 0;
+            const double* src = valid ? base + (mn0 + mn) + (k0 + k) * ld : base;
+            uint32_t dst = s_base + (uint32_t)((k * LD_MN + mn) * 8);
+            if (vec16) {
+                cp_async16(dst, src, valid * 8);
+            } else {
+                cp_async8(dst, src, valid >= 1 ? 8 : 0);
+                const double* src1 = valid >= 2 ? src + 1 : base;
+                cp_async8(dst + 8, src1, valid >= 2 ? 8 : 0);
+            }
+        }
+    } else {
+        // BM rows of BK contiguous doubles: BM*BK/2 two-double chunks
+#pragma unroll
+        for (int i = 0; i < BK / 4; ++i) {
+            int c = tid + i * THREADS;
+            int mn = c / (BK / 2);
+            int k = (c % (BK / 2)) * 2;
+            int64_t rem = k_lim - k;
+            int valid = (mn < mn_lim) ? (int)(rem >= 2 ? 2 : (rem > 0 ? rem : 0)) : 0;
+            const double* src = valid ? base + (k0 + k) + (mn0 + mn) * ld : base;
+            uint32_t dst = s_base + (uint32_t)((mn * LD_K + k) * 8);
+            if (vec16) {
+                cp_async16(dst, src, valid * 8);
+            } else {
+                cp_async8(dst, src, valid >= 1 ? 8 : 0);
+                const double* src1 = valid >= 2 ? src + 1 : base;
+                cp_async8(dst + 8, src1, valid >= 2 ? 8 : 0);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ int find_problem(const Problem* P, int nprob, int tile) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (P[mid].tile_begin <= tile)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class CF>
+__global__ void __launch_bounds__(THREADS, 1) dmma_grouped_kernel(const __grid_constant__ GroupedParams prm) {
+    constexpr int BK = CF::BK, STAGES = CF::STAGES, LD_K = CF::LD_K, STAGE_ELEMS = CF::STAGE_ELEMS;
+    constexpr int MMAK = CF::MMAK;
+    extern __shared__ __align__(16) double smem[];
+    double* sA = smem;
+    double* sB = smem + STAGES * STAGE_ELEMS;
+
+    const Problem* probs = prm.probs ? prm.probs : prm.inl_probs;
+    const KSegment* segs = prm.segs ? prm.segs : prm.inl_segs;
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps
+    const int g = lane >> 2, t = lane & 3;
+
+    for (int tile = blockIdx.x; tile < prm.total_tiles; tile += gridDim.x) {
+        const int pi = find_problem(probs, prm.nprob, tile);
+        const Problem pb = probs[pi];
+        // grouped rasterisation inside the problem
+        int local = tile - pb.tile_begin;
+        int in_group = GROUP_M * pb.tiles_n;
+        int group = local / in_group;
+        int first_m = group * GROUP_M;
+        int gsize = min(pb.tiles_m - first_m, GROUP_M);
+        int tm = first_m + (local % in_group) % gsize;
+        int tn = (local % in_group) / gsize;
+        const int64_t m0 = (int64_t)tm * BM, n0 = (int64_t)tn * BN;
+        const bool a_mn = (pb.transa == 0);  // A 'N': element (m,k) at A[m + k*lda]
+        const bool b_mn = (pb.transb != 0);  // B 'T': element (n,k) at B[n + k*ldb]
+
+        int total_kt = 0;
+        for (int s = 0; s < pb.seg_count; ++s) total_kt += (int)ceil_div(segs[pb.seg_begin + s].k, BK);
+
+        double acc[4][4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+        // loader state: which segment / k offset the next k-tile comes from
+        int ld_seg = 0;
+        int64_t ld_k0 = 0;
+        int issued = 0;
+        auto issue = [&](int stage) {
+            if (issued < total_kt) {
+                while (segs[pb.seg_begin + ld_seg].k <= 0) ++ld_seg;  // skip empty segments
+                const KSegment sg = segs[pb.seg_begin + ld_seg];
+                int64_t klim = sg.k - ld_k0;
+                bool va = (((uintptr_t)sg.A & 15) == 0) && ((sg.lda & 1) == 0);
+                bool vb = (((uintptr_t)sg.B & 15) == 0) && ((sg.ldb & 1) == 0);
+                load_tile<BK, LD_K>(sA + stage * STAGE_ELEMS, sg.A, sg.lda, a_mn, m0, ld_k0, pb.m - m0, klim, va, tid);
+                load_tile<BK, LD_K>(sB + stage * STAGE_ELEMS, sg.B, sg.ldb, b_mn, n0, ld_k0, pb.n - n0, klim, vb, tid);
+                ld_k0 += BK;
+                if (ld_k0 >= sg.k) {
+                    ld_k0 = 0;
+                    ++ld_seg;
+                }
+                ++issued;
+            }
+            cp_async_commit();
+        };
+
+#pragma unroll
+        for (int s = 0; s < STAGES - 1; ++s) issue(s);
+
+        for (int kt = 0; kt < total_kt; ++kt) {
+            cp_async_wait<STAGES - 2>();
+            __syncthreads();
+            issue((kt + STAGES - 1) % STAGES);
+            const double* a = sA + (kt % STAGES) * STAGE_ELEMS;
+            const double* b = sB + (kt % STAGES) * STAGE_ELEMS;
+#pragma unroll
+            for (int kk = 0; kk < BK; kk += MMAK) {
+                // B fragments of the warp's four n8 tiles, then one m16 tile of A at a time
+                double bf[4][MMAK / 4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int n = wn * 32 + j * 8 + g;
+#pragma unroll
+                    for (int h = 0; h < MMAK / 4; ++h)
+                        bf[j][h] = b_mn ? b[(kk + t + 4 * h) * LD_MN + n] : b[n * LD_K + kk + t + 4 * h];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int m = wm * 64 + i * 16 + g;
+                    double af[MMAK / 2];
+#pragma unroll
+                    for (int h = 0; h < MMAK / 4; ++h) {
+                        if (a_mn) {
+                            af[2 * h] = a[(kk + t + 4 * h) * LD_MN + m];
+                            af[2 * h + 1] = a[(kk + t + 4 * h) * LD_MN + m + 8];
+                        } else {
+                            af[2 * h] = a[m * LD_K + kk + t + 4 * h];
+                            af[2 * h + 1] = a[(m + 8) * LD_K + kk + t + 4 * h];
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if constexpr (MMAK == 4) {
+                            dmma_16x8x4(acc[i][j], af[0], af[1], bf[j][0]);
+                        } else {
+                            dmma_16x8x8(acc[i][j], af, bf[j]);
+                        }
+                    }
+                }
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();  // the next tile's prologue reuses the ring
+
+        // epilogue: C = alpha*acc + beta*C (beta == 0: C not read)
+        const double alpha = pb.alpha, beta = pb.beta;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    int64_t row = m0 + wm * 64 + i * 16 + g + h * 8;
+                    if (row >= pb.m) continue;
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        int64_t col = n0 + wn * 32 + j * 8 + 2 * t + e;
+                        if (col >= pb.n) continue;
+                        double* cp = pb.C + row + col * pb.ldc;
+                        double v = alpha * acc[i][j][h * 2 + e];
+                        if (beta != 0.0) v = fma(beta, *cp, v);
+                        *cp = v;
+                    }
+                }
+            }
+        }
+    }
+}
+
+using V0 = Cfg<4, 16, 4>;
+using V1 = Cfg<8, 16, 4>;
+using V2 = Cfg<8, 32, 3>;
+using V3 = Cfg<4, 32, 3>;
+
+template <class CF>
+cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stream) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(dmma_grouped_kernel<CF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)CF::SMEM);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    dmma_grouped_kernel<CF><<<grid, THREADS, CF::SMEM, stream>>>(prm);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int dmma_variant_count() { return 4; }
+
+dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs) {
+    // drop empty problems, lay out the tile prefix
+    std::vector<Problem> live;
+    live.reserve(probs.size());
+    int64_t tiles = 0;
+    for (auto p : probs) {
+        if (p.m <= 0 || p.n <= 0) continue;
+        p.tiles_m = (int32_t)ceil_div(p.m, BM);
+        p.tiles_n = (int32_t)ceil_div(p.n, BN);
+        p.tile_begin = (int32_t)tiles;
+        tiles += (int64_t)p.tiles_m * p.tiles_n;
+        live.push_back(p);
+    }
+    if (live.empty()) return DGT_SUCCESS;
+    if (tiles > INT32_MAX) return fail(h, DGT_ERROR_INVALID_VALUE, "problem too large (tile count exceeds 2^31)");
+
+    static thread_local GroupedParams prm;  // large; filled per launch (launch copies the value)
+    prm.nprob = (int)live.size();
+    prm.total_tiles = (int)tiles;
+    if ((int)live.size() <= MAX_INLINE_PROBS && (int)segs.size() <= MAX_INLINE_SEGS) {
+        prm.probs = nullptr;
+        prm.segs = nullptr;
+        std::copy(live.begin(), live.end(), prm.inl_probs);
+        std::copy(segs.begin(), segs.end(), prm.inl_segs);
+    } else {
+        size_t pbytes = live.size() * sizeof(Problem), sbytes = segs.size() * sizeof(KSegment);
+        size_t off = (pbytes + 255) / 256 * 256;
+        void* ws = nullptr;
+        dgt_status st = ensure_workspace(h, off + sbytes, &ws, 1);
+        if (st != DGT_SUCCESS) return st;
+        DGT_CUDA_TRY(h, cudaMemcpyAsync(ws, live.data(), pbytes, cudaMemcpyHostToDevice, h->stream));
+        DGT_CUDA_TRY(h, cudaMemcpyAsync((char*)ws + off, segs.data(), sbytes, cudaMemcpyHostToDevice, h->stream));
+        prm.probs = (const Problem*)ws;
+        prm.segs = (const KSegment*)((char*)ws + off);
+    }
+    int grid = (int)std::min<int64_t>(tiles, h->num_sms);
+    cudaError_t e;
+    switch (h->dmma_variant) {
+        case 1: e = launch_variant<V1>(prm, grid, h->stream); break;
+        case 2: e = launch_variant<V2>(prm, grid, h->stream); break;
+        case 3: e = launch_variant<V3>(prm, grid, h->stream); break;
+        default: e = launch_variant<V0>(prm, grid, h->stream); break;
+    }
+    h->launches.fetch_add(1);
+    if (e != cudaSuccess) return cuda_fail(h, e, "dmma_grouped_kernel launch");
+    return DGT_SUCCESS;
+}
+
+}  // namespace dgt

@@ -1,0 +1,119 @@
+// Shared internals of libdgt: the handle, status plumbing, workspace and the device
+// error word that bounded waits report into.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dgt.h"
+
+// Device error word bits (set by kernels, read by dgt_check_device).
+#define DGT_DEVERR_TIMEOUT 0x1u
+#define DGT_DEVERR_BOUNDS 0x2u
+
+struct dgt_context {
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int num_sms = 148;
+    dgt_fp64_mode fp64_mode = DGT_FP64_NATIVE;
+    int slices = 7;
+    int dmma_variant = 0;  // native FP64 kernel variant (see dgemm_dmma.cu)
+    bool profile = false;  // record phase events (DGT_TUNE_PROFILE)
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // split start, gemm start, gemm end
+    bool ev_split = false;  // last call had a split phase
+    std::string last_error;
+    unsigned int* dev_error = nullptr;  // one word in device memory
+    void* workspace = nullptr;
+    size_t workspace_bytes = 0;
+    void* workspace2 = nullptr;
+    size_t workspace2_bytes = 0;
+    std::atomic<int64_t> launches{0};
+};
+
+namespace dgt {
+
+inline dgt_status fail(dgt_context* h, dgt_status s, const std::string& msg) {
+    if (h) h->last_error = msg;
+    return s;
+}
+
+inline dgt_status cuda_fail(dgt_context* h, cudaError_t e, const char* what) {
+    return fail(h, DGT_ERROR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define DGT_CUDA_TRY(h, call)                                     \
+    do {                                                          \
+        cudaError_t _e = (call);                                  \
+        if (_e != cudaSuccess) return dgt::cuda_fail(h, _e, #call); \
+    } while (0)
+
+#define DGT_LAUNCH_CHECK(h, name)                                          \
+    do {                                                                   \
+        (h)->launches.fetch_add(1);                                        \
+        cudaError_t _e = cudaGetLastError();                               \
+        if (_e != cudaSuccess) return dgt::cuda_fail(h, _e, name " launch"); \
+    } while (0)
+
+// Phase markers for DGT_TUNE_PROFILE (no-ops unless profiling is on).
+void mark(dgt_context* h, int which);
+
+// Grows a handle-owned scratch buffer; never shrinks.  slot 0 or 1.
+dgt_status ensure_workspace(dgt_context* h, size_t bytes, void** out, int slot = 0);
+
+inline bool is_trans(char t) { return t == 'T' || t == 't' || t == 'C' || t == 'c'; }
+inline bool valid_op(char t) { return t == 'N' || t == 'n' || is_trans(t); }
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// ---- native FP64 GEMM engine (dgemm_dmma.cu) --------------------------------------------
+// One K-segment: C += op(A_seg) * op(B_seg) over k rows/cols.  A problem is a list of
+// segments that accumulate into the same C tile (the SUMMA / Cannon step schedule).
+struct KSegment {
+    const double* A;
+    const double* B;
+    int64_t lda, ldb;
+    int64_t k;
+};
+
+struct Problem {
+    int64_t m, n;
+    double alpha, beta;
+    double* C;
+    int64_t ldc;
+    int32_t seg_begin, seg_count;  // into the segment table
+    int32_t transa, transb;        // 0 = 'N', 1 = 'T'
+    int32_t tile_begin;            // prefix sum of tiles (filled by the launcher)
+    int32_t tiles_m, tiles_n;
+};
+
+int dmma_variant_count();
+// Launches the persistent grouped FP64 DMMA kernel over problems/segments (host arrays,
+// copied to device workspace).  Validation is the caller's job.
+dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs);
+
+// ---- layout engine (layout.cu) ---------------------------------------------------------
+// One strided copy: rows x cols, column-major (rows contiguous on both sides).
+struct HostCopy {
+    const double* src;
+    double* dst;
+    int64_t ldS, ldD, rows, cols;
+};
+dgt_status launch_block_cyclic(dgt_context* h, bool to_local, int64_t M, int64_t N, int64_t mb, int64_t nb, int p,
+                               int q, double* global, int64_t ldg, double* const* locals, const int64_t* lld);
+dgt_status launch_strided_copies(dgt_context* h, const std::vector<HostCopy>& copies);
+// C[t] += sum_{s < stacks} W[s*stack_stride + t*elems_per_tile + e] for every tile t.
+dgt_status launch_stack_reduce(dgt_context* h, int64_t elems_per_tile, int tiles, int stacks, double* const* C,
+                               const double* W, int64_t stack_stride);
+
+// ---- Ozaki emulation (ozaki.cu) -----------------------------------------------------------
+dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                       const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                       dgt_fp64_mode mode, int slices);
+
+}  // namespace dgt
