@@ -236,10 +236,11 @@ def main():
 
     # ---- accuracy: sampled rows vs the host FP64 oracle (OpenBLAS) ----
     rows = np.sort(np.random.default_rng(1).choice(n, 48, replace=False))
+    rows_t = torch.from_numpy(rows).cuda()
     want = ALPHA * (A_np[rows, :] @ B_np)
 
-    def rows_err(t):
-        got = t.cpu().numpy().T[rows, :]
+    def rows_err(t):  # tensor column r holds matrix row r: gather the sampled rows on device
+        got = t[:, rows_t].cpu().numpy().T
         return O.rel_errors(got, want)
 
     run(dgt.FP64_NATIVE, 0, C_nat.data_ptr())

@@ -23,15 +23,18 @@
 namespace dgt {
 namespace {
 
-constexpr int BM = 128, BN = 128, THREADS = 256;
+constexpr int BM = 128, BN = 128;
 constexpr int PAD = 4;
 constexpr int LD_MN = BM + PAD;  // [k][mn] layout row stride (doubles): 1056 B = 32 mod 128 banks
 constexpr int GROUP_M = 8;       // tile rasterisation group for L2 reuse
 
 // Kernel variants (the autotuner's knob): DMMA shape m16n8k{4,8}, K depth of a stage, ring depth.
-template <int MMAK_, int BK_, int STAGES_>
+template <int MMAK_, int BK_, int STAGES_, int NWARPS_ = 8>
 struct Cfg {
     static constexpr int MMAK = MMAK_, BK = BK_, STAGES = STAGES_;
+    static constexpr int THREADS = NWARPS_ * 32;
+    static constexpr int WARPS_M = NWARPS_ / 4;      // warps along M (4 along N, 32 columns each)
+    static constexpr int MT = BM / WARPS_M / 16;     // m16 tiles per warp
     static constexpr int LD_K = BK + PAD;  // [mn][k] row stride: (BK+4)*8 B = 32 mod 128 for BK in {16, 32}
     static constexpr int STAGE_ELEMS = (BM * LD_K > BK * LD_MN) ? BM * LD_K : BK * LD_MN;
     static constexpr size_t SMEM = (size_t)2 * STAGES * STAGE_ELEMS * sizeof(double);
@@ -81,14 +84,14 @@ __device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double (&a)[4]
 //  mn_major: global element (mn, k) at base[mn + k*ld]  -> smem [k][mn], row stride LD_MN
 //  else    : global element (mn, k) at base[k + mn*ld]  -> smem [mn][k], row stride LD_K
 // mn_lim / k_lim: valid extents from (mn0, k0); outside is zero-filled.
-template <int BK, int LD_K>
+template <int BK, int LD_K, int THREADS>
 __device__ __forceinline__ void load_tile(double* s, const double* base, int64_t ld, bool mn_major, int64_t mn0,
                                           int64_t k0, int64_t mn_lim, int64_t k_lim, bool vec16, int tid) {
     const uint32_t s_base = smem_u32(s);
     if (mn_major) {
         // BK columns of BM contiguous doubles: BK*64 two-double chunks
 #pragma unroll
-        for (int i = 0; i < BK / 4; ++i) {
+        for (int i = 0; i < BK * 64 / THREADS; ++i) {
             int c = tid + i * THREADS;
             int k = c >> 6;
             int mn = (c & 63) * 2;
@@ -107,7 +110,7 @@ __device__ __forceinline__ void load_tile(double* s, const double* base, int64_t
     } else {
         // BM rows of BK contiguous doubles: BM*BK/2 two-double chunks
 #pragma unroll
-        for (int i = 0; i < BK / 4; ++i) {
+        for (int i = 0; i < BM * BK / 2 / THREADS; ++i) {
             int c = tid + i * THREADS;
             int mn = c / (BK / 2);
             int k = (c % (BK / 2)) * 2;
@@ -139,9 +142,9 @@ __device__ __forceinline__ int find_problem(const Problem* P, int nprob, int til
 }
 
 template <class CF>
-__global__ void __launch_bounds__(THREADS, 1) dmma_grouped_kernel(const __grid_constant__ GroupedParams prm) {
+__global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __grid_constant__ GroupedParams prm) {
     constexpr int BK = CF::BK, STAGES = CF::STAGES, LD_K = CF::LD_K, STAGE_ELEMS = CF::STAGE_ELEMS;
-    constexpr int MMAK = CF::MMAK;
+    constexpr int MMAK = CF::MMAK, THREADS = CF::THREADS, MT = CF::MT, WTM = MT * 16;
     extern __shared__ __align__(16) double smem[];
     double* sA = smem;
     double* sB = smem + STAGES * STAGE_ELEMS;
@@ -151,7 +154,7 @@ __global__ void __launch_bounds__(THREADS, 1) dmma_grouped_kernel(const __grid_c
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps
+    const int wm = warp >> 2, wn = warp & 3;  // WARPS_M x 4 warps
     const int g = lane >> 2, t = lane & 3;
 
     for (int tile = blockIdx.x; tile < prm.total_tiles; tile += gridDim.x) {
@@ -172,9 +175,9 @@ __global__ void __launch_bounds__(THREADS, 1) dmma_grouped_kernel(const __grid_c
         int total_kt = 0;
         for (int s = 0; s < pb.seg_count; ++s) total_kt += (int)ceil_div(segs[pb.seg_begin + s].k, BK);
 
-        double acc[4][4][4];
+        double acc[MT][4][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < MT; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j)
 #pragma unroll
@@ -191,8 +194,10 @@ __global__ void __launch_bounds__(THREADS, 1) dmma_grouped_kernel(const __grid_c
                 int64_t klim = sg.k - ld_k0;
                 bool va = (((uintptr_t)sg.A & 15) == 0) && ((sg.lda & 1) == 0);
                 bool vb = (((uintptr_t)sg.B & 15) == 0) && ((sg.ldb & 1) == 0);
-                load_tile<BK, LD_K>(sA + stage * STAGE_ELEMS, sg.A, sg.lda, a_mn, m0, ld_k0, pb.m - m0, klim, va, tid);
-                load_tile<BK, LD_K>(sB + stage * STAGE_ELEMS, sg.B, sg.ldb, b_mn, n0, ld_k0, pb.n - n0, klim, vb, tid);
+                load_tile<BK, LD_K, THREADS>(sA + stage * STAGE_ELEMS, sg.A, sg.lda, a_mn, m0, ld_k0, pb.m - m0, klim,
+                                             va, tid);
+                load_tile<BK, LD_K, THREADS>(sB + stage * STAGE_ELEMS, sg.B, sg.ldb, b_mn, n0, ld_k0, pb.n - n0, klim,
+                                             vb, tid);
                 ld_k0 += BK;
                 if (ld_k0 >= sg.k) {
                     ld_k0 = 0;
@@ -224,8 +229,8 @@ __global__ void __launch_bounds__(THREADS, 1) dmma_grouped_kernel(const __grid_c
                         bf[j][h] = b_mn ? b[(kk + t + 4 * h) * LD_MN + n] : b[n * LD_K + kk + t + 4 * h];
                 }
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int m = wm * 64 + i * 16 + g;
+                for (int i = 0; i < MT; ++i) {
+                    const int m = wm * WTM + i * 16 + g;
                     double af[MMAK / 2];
 #pragma unroll
                     for (int h = 0; h < MMAK / 4; ++h) {
@@ -254,12 +259,12 @@ __global__ void __launch_bounds__(THREADS, 1) dmma_grouped_kernel(const __grid_c
         // epilogue: C = alpha*acc + beta*C (beta == 0: C not read)
         const double alpha = pb.alpha, beta = pb.beta;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < MT; ++i) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    int64_t row = m0 + wm * 64 + i * 16 + g + h * 8;
+                    int64_t row = m0 + wm * WTM + i * 16 + g + h * 8;
                     if (row >= pb.m) continue;
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
@@ -280,6 +285,9 @@ using V0 = Cfg<4, 16, 4>;
 using V1 = Cfg<8, 16, 4>;
 using V2 = Cfg<8, 32, 3>;
 using V3 = Cfg<4, 32, 3>;
+using V4 = Cfg<8, 16, 4, 16>;
+using V5 = Cfg<8, 32, 3, 16>;
+using V6 = Cfg<4, 16, 4, 16>;
 
 template <class CF>
 cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stream) {
@@ -290,13 +298,13 @@ cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stre
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    dmma_grouped_kernel<CF><<<grid, THREADS, CF::SMEM, stream>>>(prm);
+    dmma_grouped_kernel<CF><<<grid, CF::THREADS, CF::SMEM, stream>>>(prm);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-int dmma_variant_count() { return 4; }
+int dmma_variant_count() { return 7; }
 
 dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs) {
     // drop empty problems, lay out the tile prefix
@@ -339,6 +347,9 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
         case 1: e = launch_variant<V1>(prm, grid, h->stream); break;
         case 2: e = launch_variant<V2>(prm, grid, h->stream); break;
         case 3: e = launch_variant<V3>(prm, grid, h->stream); break;
+        case 4: e = launch_variant<V4>(prm, grid, h->stream); break;
+        case 5: e = launch_variant<V5>(prm, grid, h->stream); break;
+        case 6: e = launch_variant<V6>(prm, grid, h->stream); break;
         default: e = launch_variant<V0>(prm, grid, h->stream); break;
     }
     h->launches.fetch_add(1);

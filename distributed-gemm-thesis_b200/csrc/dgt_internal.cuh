@@ -112,6 +112,12 @@ dgt_status launch_stack_reduce(dgt_context* h, int64_t elems_per_tile, int tiles
                                const double* W, int64_t stack_stride);
 
 // ---- Ozaki emulation (ozaki.cu) -----------------------------------------------------------
+// Scratch bytes one INT8 Ozaki call needs (0 if the shape is unsupported).
+size_t ozaki_scratch_bytes(int S, int64_t m, int64_t n, int64_t k);
+// The INT8 Ozaki path on caller-provided scratch; no allocation, no handle.
+dgt_status ozaki_dgemm_on(cudaStream_t s, int num_sms, unsigned int* err, void* ws, size_t ws_bytes, bool ta,
+                          bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
+                          const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int S);
 dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
                        const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
                        dgt_fp64_mode mode, int slices);

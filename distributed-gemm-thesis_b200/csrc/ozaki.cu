@@ -533,44 +533,68 @@ static bool ozaki_schedule(int S, int64_t k_pad, std::vector<oz::Seg>& segs, std
     return true;
 }
 
-dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
-                       const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
-                       int64_t ldc, dgt_fp64_mode mode, int S) {
-    if (mode != DGT_FP64_OZAKI_INT8)
-        return fail(h, DGT_ERROR_UNSUPPORTED, "this build implements the INT8 Ozaki path only");
-    const int64_t m_pad = ceil_div(m, oz::TM) * oz::TM;
-    const int64_t n_pad = ceil_div(n, oz::TN) * oz::TN;
-    const int64_t k_pad = ceil_div(k, oz::TKB) * oz::TKB;
+// Scratch layout of one Ozaki call: planes A | planes B | amax A | amax B | exp A | exp B |
+// schedule.  Returns false when the shape is outside what the kernels support.
+struct OzakiLayout {
+    int64_t m_pad, n_pad, k_pad;
+    size_t pa, pb, xa, xb, ea, eb, sb, gb, total;
     std::vector<oz::Seg> segs;
     std::vector<oz::Group> groups;
-    if (!ozaki_schedule(S, k_pad, segs, groups))
-        return fail(h, DGT_ERROR_UNSUPPORTED, "K too large for exact INT32 accumulation of one digit product");
-    if ((int64_t)S * std::max(m_pad, n_pad) > INT32_MAX)
-        return fail(h, DGT_ERROR_UNSUPPORTED, "matrix too large for 32-bit TMA coordinates");
+};
 
-    // workspace: planes A | planes B | amax A | amax B | exp A | exp B | schedule
+static dgt_status ozaki_layout(dgt_context* h, int S, int64_t m, int64_t n, int64_t k, OzakiLayout& L) {
+    L.m_pad = ceil_div(m, oz::TM) * oz::TM;
+    L.n_pad = ceil_div(n, oz::TN) * oz::TN;
+    L.k_pad = ceil_div(k, oz::TKB) * oz::TKB;
+    if (!ozaki_schedule(S, L.k_pad, L.segs, L.groups))
+        return fail(h, DGT_ERROR_UNSUPPORTED, "K too large for exact INT32 accumulation of one digit product");
+    if ((int64_t)S * std::max(L.m_pad, L.n_pad) > INT32_MAX)
+        return fail(h, DGT_ERROR_UNSUPPORTED, "matrix too large for 32-bit TMA coordinates");
     auto up = [](size_t x) { return (x + 1023) / 1024 * 1024; };
-    const size_t pa = up((size_t)S * m_pad * k_pad), pb = up((size_t)S * n_pad * k_pad);
-    const size_t xa = up(m * 8), xb = up(n * 8), ea = up(m * 4), eb = up(n * 4);
-    const size_t sb = up(segs.size() * sizeof(oz::Seg)), gb = up(groups.size() * sizeof(oz::Group));
-    void* ws = nullptr;
-    dgt_status st = ensure_workspace(h, pa + pb + xa + xb + ea + eb + sb + gb, &ws, 0);
-    if (st != DGT_SUCCESS) return st;
+    L.pa = up((size_t)S * L.m_pad * L.k_pad);
+    L.pb = up((size_t)S * L.n_pad * L.k_pad);
+    L.xa = up(m * 8);
+    L.xb = up(n * 8);
+    L.ea = up(m * 4);
+    L.eb = up(n * 4);
+    L.sb = up(L.segs.size() * sizeof(oz::Seg));
+    L.gb = up(L.groups.size() * sizeof(oz::Group));
+    L.total = L.pa + L.pb + L.xa + L.xb + L.ea + L.eb + L.sb + L.gb;
+    return DGT_SUCCESS;
+}
+
+size_t ozaki_scratch_bytes(int S, int64_t m, int64_t n, int64_t k) {
+    OzakiLayout L;
+    return ozaki_layout(nullptr, S, m, n, k, L) == DGT_SUCCESS ? L.total : 0;
+}
+
+// The Ozaki INT8 path on caller-provided scratch (L.total bytes at ws).  h may be null:
+// then no profiling marks, launch counts or error messages are recorded.
+static dgt_status ozaki_run(dgt_context* h, cudaStream_t s, int num_sms, unsigned int* err, void* ws,
+                            const OzakiLayout& L, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                            const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                            int64_t ldc, int S) {
+    const int64_t m_pad = L.m_pad, n_pad = L.n_pad, k_pad = L.k_pad;
     char* p = (char*)ws;
     int8_t* planesA = (int8_t*)p;
-    int8_t* planesB = (int8_t*)(p + pa);
-    unsigned long long* amaxA = (unsigned long long*)(p + pa + pb);
-    unsigned long long* amaxB = (unsigned long long*)(p + pa + pb + xa);
-    int32_t* expA = (int32_t*)(p + pa + pb + xa + xb);
-    int32_t* expB = (int32_t*)(p + pa + pb + xa + xb + ea);
-    oz::Seg* dsegs = (oz::Seg*)(p + pa + pb + xa + xb + ea + eb);
-    oz::Group* dgroups = (oz::Group*)(p + pa + pb + xa + xb + ea + eb + sb);
+    int8_t* planesB = (int8_t*)(p + L.pa);
+    unsigned long long* amaxA = (unsigned long long*)(p + L.pa + L.pb);
+    unsigned long long* amaxB = (unsigned long long*)(p + L.pa + L.pb + L.xa);
+    int32_t* expA = (int32_t*)(p + L.pa + L.pb + L.xa + L.xb);
+    int32_t* expB = (int32_t*)(p + L.pa + L.pb + L.xa + L.xb + L.ea);
+    oz::Seg* dsegs = (oz::Seg*)(p + L.pa + L.pb + L.xa + L.xb + L.ea + L.eb);
+    oz::Group* dgroups = (oz::Group*)(p + L.pa + L.pb + L.xa + L.xb + L.ea + L.eb + L.sb);
+    auto counted = [&](const char* what) -> dgt_status {
+        if (h) h->launches.fetch_add(1);
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? DGT_SUCCESS : cuda_fail(h, e, what);
+    };
 
-    cudaStream_t s = h->stream;
-    DGT_CUDA_TRY(h, cudaMemcpyAsync(dsegs, segs.data(), segs.size() * sizeof(oz::Seg), cudaMemcpyHostToDevice, s));
-    DGT_CUDA_TRY(h, cudaMemcpyAsync(dgroups, groups.data(), groups.size() * sizeof(oz::Group),
+    DGT_CUDA_TRY(h, cudaMemcpyAsync(dsegs, L.segs.data(), L.segs.size() * sizeof(oz::Seg), cudaMemcpyHostToDevice,
+                                    s));
+    DGT_CUDA_TRY(h, cudaMemcpyAsync(dgroups, L.groups.data(), L.groups.size() * sizeof(oz::Group),
                                     cudaMemcpyHostToDevice, s));
-    mark(h, 0);
+    if (h) mark(h, 0);
     DGT_CUDA_TRY(h, cudaMemsetAsync(amaxA, 0, m * 8, s));
     DGT_CUDA_TRY(h, cudaMemsetAsync(amaxB, 0, n * 8, s));
 
@@ -584,7 +608,7 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
             dim3 grid((unsigned)ceil_div(MN, 256), (unsigned)ceil_div(k, kchunk));
             oz::amax_mn_contig<<<grid, 256, 0, s>>>(X, ld, MN, k, kchunk, out);
         }
-        h->launches.fetch_add(1);
+        return counted("ozaki amax");
     };
     auto split = [&](const double* X, int64_t ld, int64_t MN, int64_t mn_pad, bool kcontig,
                      const unsigned long long* am, int32_t* ex, int8_t* planes) {
@@ -593,13 +617,13 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
             oz::split_digits<true><<<grid, 128, 0, s>>>(X, ld, MN, k, mn_pad, k_pad, S, am, ex, planes);
         else
             oz::split_digits<false><<<grid, 128, 0, s>>>(X, ld, MN, k, mn_pad, k_pad, S, am, ex, planes);
-        h->launches.fetch_add(1);
+        return counted("ozaki split");
     };
-    amax(A, lda, m, ta, amaxA);
-    amax(B, ldb, n, !tb, amaxB);
-    split(A, lda, m, m_pad, ta, amaxA, expA, planesA);
-    split(B, ldb, n, n_pad, !tb, amaxB, expB, planesB);
-    DGT_LAUNCH_CHECK(h, "ozaki split");
+    dgt_status st;
+    if ((st = amax(A, lda, m, ta, amaxA)) != DGT_SUCCESS) return st;
+    if ((st = amax(B, ldb, n, !tb, amaxB)) != DGT_SUCCESS) return st;
+    if ((st = split(A, lda, m, m_pad, ta, amaxA, expA, planesA)) != DGT_SUCCESS) return st;
+    if ((st = split(B, ldb, n, n_pad, !tb, amaxB, expB, planesB)) != DGT_SUCCESS) return st;
 
     CUtensorMap tmA, tmB;
     if (!oz::make_plane_map(&tmA, planesA, (int64_t)S * m_pad, k_pad, oz::TM) ||
@@ -620,7 +644,7 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
     prm.n_pad = (int32_t)n_pad;
     prm.tiles_m = (int32_t)(m_pad / oz::TM);
     prm.tiles_n = (int32_t)(n_pad / oz::TN);
-    prm.ngroups = (int32_t)groups.size();
+    prm.ngroups = (int32_t)L.groups.size();
     prm.alpha = alpha;
     prm.beta = beta;
     prm.C = C;
@@ -628,14 +652,39 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
     prm.col_exp = expB;
     prm.segs = dsegs;
     prm.groups = dgroups;
-    prm.err = h->dev_error;
+    prm.err = err;
     const int tiles = prm.tiles_m * prm.tiles_n;
-    const int grid = std::min(tiles, h->num_sms);
-    mark(h, 1);
+    const int grid = std::min(tiles, num_sms);
+    if (h) mark(h, 1);
     oz::ozaki_i8_gemm<<<grid, oz::THREADS, oz::SMEM_BYTES, s>>>(tmA, tmB, prm);
-    DGT_LAUNCH_CHECK(h, "ozaki_i8_gemm");
-    mark(h, 2);
+    if ((st = counted("ozaki_i8_gemm")) != DGT_SUCCESS) return st;
+    if (h) mark(h, 2);
     return DGT_SUCCESS;
+}
+
+dgt_status ozaki_dgemm_on(cudaStream_t s, int num_sms, unsigned int* err, void* ws, size_t ws_bytes, bool ta,
+                          bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,
+                          const double* B, int64_t ldb, double beta, double* C, int64_t ldc, int S) {
+    OzakiLayout L;
+    dgt_status st = ozaki_layout(nullptr, S, m, n, k, L);
+    if (st != DGT_SUCCESS) return st;
+    if (L.total > ws_bytes) return DGT_ERROR_INVALID_VALUE;
+    return ozaki_run(nullptr, s, num_sms, err, ws, L, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, S);
+}
+
+dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                       const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                       int64_t ldc, dgt_fp64_mode mode, int S) {
+    if (mode != DGT_FP64_OZAKI_INT8)
+        return fail(h, DGT_ERROR_UNSUPPORTED, "this build implements the INT8 Ozaki path only");
+    OzakiLayout L;
+    dgt_status st = ozaki_layout(h, S, m, n, k, L);
+    if (st != DGT_SUCCESS) return st;
+    void* ws = nullptr;
+    st = ensure_workspace(h, L.total, &ws, 0);
+    if (st != DGT_SUCCESS) return st;
+    return ozaki_run(h, h->stream, h->num_sms, h->dev_error, ws, L, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C,
+                     ldc, S);
 }
 
 }  // namespace dgt

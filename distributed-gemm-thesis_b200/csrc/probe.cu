@@ -49,6 +49,45 @@ __global__ void __launch_bounds__(PROBE_THREADS) dfma_probe_kernel(double* out, 
     if (s == 12345.678) out[0] = s;
 }
 
+// Half the warps of each block run the DMMA loop, half the DFMA loop: shows whether the
+// FP64 tensor pipe and the FP64 FMA pipe run concurrently.
+__global__ void __launch_bounds__(PROBE_THREADS) mixed_probe_kernel(double* out, double seed) {
+    if ((threadIdx.x >> 5) & 1) {
+        double acc[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i] = seed * i;
+        const double a = 1.0000001, b = 1e-9 * threadIdx.x;
+        for (int it = 0; it < PROBE_ITERS * 16; ++it) {  // same FLOPs as a DMMA warp
+#pragma unroll
+            for (int i = 0; i < 8; ++i) acc[i] = fma(acc[i], a, b);
+        }
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s += acc[i];
+        if (s == 12345.678) out[0] = s;
+    } else {
+        double acc[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][e] = 0.0;
+        double a0 = seed + threadIdx.x * 1e-9, a1 = seed * 0.5, b0 = seed * 0.25;
+        for (int it = 0; it < PROBE_ITERS; ++it) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                asm volatile(
+                    "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+                    : "+d"(acc[i][0]), "+d"(acc[i][1]), "+d"(acc[i][2]), "+d"(acc[i][3])
+                    : "d"(a0), "d"(a1), "d"(b0));
+            }
+        }
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s += acc[i][0] + acc[i][1] + acc[i][2] + acc[i][3];
+        if (s == 12345.678) out[0] = s;
+    }
+}
+
 }  // namespace
 }  // namespace dgt
 
@@ -56,7 +95,7 @@ using namespace dgt;
 
 extern "C" dgt_status dgt_probe_peak(dgt_handle_t h, int32_t kind, double* tflops) {
     if (!h) return DGT_ERROR_NOT_INITIALIZED;
-    if (!tflops || (kind != 0 && kind != 1)) return fail(h, DGT_ERROR_INVALID_VALUE, "bad probe kind");
+    if (!tflops || kind < 0 || kind > 2) return fail(h, DGT_ERROR_INVALID_VALUE, "bad probe kind");
     void* ws = nullptr;
     dgt_status st = ensure_workspace(h, 64, &ws, 1);
     if (st != DGT_SUCCESS) return st;
@@ -69,8 +108,10 @@ extern "C" dgt_status dgt_probe_peak(dgt_handle_t h, int32_t kind, double* tflop
         cudaEventRecord(e0, h->stream);
         if (kind == 0)
             dmma_probe_kernel<<<blocks, PROBE_THREADS, 0, h->stream>>>((double*)ws, 1.0);
-        else
+        else if (kind == 1)
             dfma_probe_kernel<<<blocks, PROBE_THREADS, 0, h->stream>>>((double*)ws, 1.0);
+        else
+            mixed_probe_kernel<<<blocks, PROBE_THREADS, 0, h->stream>>>((double*)ws, 1.0);
         h->launches.fetch_add(1);
         cudaEventRecord(e1, h->stream);
         cudaError_t e = cudaEventSynchronize(e1);
@@ -85,8 +126,10 @@ extern "C" dgt_status dgt_probe_peak(dgt_handle_t h, int32_t kind, double* tflop
     double flops;
     if (kind == 0)
         flops = warps * PROBE_ITERS * 8 * (2.0 * 16 * 8 * 4);  // per warp-level m16n8k4
-    else
+    else if (kind == 1)
         flops = (double)blocks * PROBE_THREADS * PROBE_ITERS * 8 * 2.0;
+    else  // half the warps each, equal FLOPs per warp
+        flops = warps / 2 * PROBE_ITERS * 8 * (2.0 * 16 * 8 * 4) + (warps / 2) * 32 * PROBE_ITERS * 16 * 8 * 2.0;
     *tflops = flops / (best_ms * 1e-3) / 1e12;
     return DGT_SUCCESS;
 }
