@@ -111,6 +111,7 @@ dgt_status dgt_destroy(dgt_handle_t h) {
         if (e) cudaEventDestroy(e);
     if (h->workspace) cudaFree(h->workspace);
     if (h->workspace2) cudaFree(h->workspace2);
+    if (h->table) cudaFree(h->table);
     if (h->dev_error) cudaFree(h->dev_error);
     delete h;
     return DGT_SUCCESS;
@@ -153,6 +154,10 @@ dgt_status dgt_set_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t value) {
         case DGT_TUNE_PROFILE:
             h->profile = value != 0;
             return DGT_SUCCESS;
+        case DGT_TUNE_OZAKI_VARIANT:
+            if (value < 0 || value > 3) return fail(h, DGT_ERROR_INVALID_VALUE, "unknown Ozaki kernel variant");
+            h->ozaki_variant = value;
+            return DGT_SUCCESS;
     }
     return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
 }
@@ -175,6 +180,7 @@ dgt_status dgt_get_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t* value) {
         case DGT_TUNE_DMMA_VARIANT: *value = h->dmma_variant; return DGT_SUCCESS;
         case DGT_TUNE_OZAKI_SLICES: *value = h->slices; return DGT_SUCCESS;
         case DGT_TUNE_PROFILE: *value = h->profile ? 1 : 0; return DGT_SUCCESS;
+        case DGT_TUNE_OZAKI_VARIANT: *value = h->ozaki_variant; return DGT_SUCCESS;
     }
     return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
 }
@@ -282,7 +288,29 @@ dgt_status dgt_dgemm_ex(dgt_handle_t h, char ta, char tb, int64_t m, int64_t n, 
     dgt_status st = validate_gemm(h, ta, tb, m, n, k, A, lda, B, ldb, C, ldc);
     if (st != DGT_SUCCESS) return st;
     if (m == 0 || n == 0) return DGT_SUCCESS;
-    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_OZAKI_INT8;
+    // tuned choices for this shape class, if the autotuner has seen one
+    int dv = h->dmma_variant, ov = h->ozaki_variant;
+    if (mode == DGT_FP64_AUTO) {
+        const TuneEntry* e = tune_lookup(h, DGT_FP64_AUTO, m, n, k);
+        if (e) {
+            mode = (dgt_fp64_mode)e->mode;
+            slices = e->slices;
+            (e->mode == DGT_FP64_NATIVE ? dv : ov) = e->variant;
+        } else {
+            mode = DGT_FP64_OZAKI_INT8;
+        }
+    }
+    if (const TuneEntry* e = tune_lookup(h, mode, m, n, k)) (mode == DGT_FP64_NATIVE ? dv : ov) = e->variant;
+    struct Restore {
+        dgt_context* h;
+        int dv, ov;
+        ~Restore() {
+            h->dmma_variant = dv;
+            h->ozaki_variant = ov;
+        }
+    } restore{h, h->dmma_variant, h->ozaki_variant};
+    h->dmma_variant = dv;
+    h->ozaki_variant = ov;
     if (mode == DGT_FP64_NATIVE || k == 0)
         return native_single(h, ta, tb, m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc);
     if (slices < 2 || slices > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");

@@ -1,0 +1,206 @@
+// Autotuner: picks, per shape class, the native DMMA kernel variant, the INT8 Ozaki kernel
+// variant and the Ozaki slice count, by timing the candidates with CUDA events on the
+// caller's own buffers.  The slice count is the smallest whose result lies within `tol`
+// (relative Frobenius distance) of the native FP64 result -- the native kernel is the
+// accuracy yardstick the library has on the device.  Results are kept per handle, keyed
+// by (mode, ceil(log2 m), ceil(log2 n), ceil(log2 k)), used by later calls, and can be
+// saved to / loaded from a small JSON file.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "dgt_internal.cuh"
+
+namespace dgt {
+namespace {
+
+// sum((x - y)^2) and sum(y^2) over an m x n column-major pair, accumulated with atomics.
+__global__ void diff_norms(const double* __restrict__ X, const double* __restrict__ Y, int64_t m, int64_t n,
+                           int64_t ldx, int64_t ldy, double* __restrict__ out) {
+    double d2 = 0.0, y2 = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m * n; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t j = e / m, i = e - j * m;
+        double y = Y[i + j * ldy], d = X[i + j * ldx] - y;
+        d2 = fma(d, d, d2);
+        y2 = fma(y, y, y2);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+        y2 += __shfl_xor_sync(0xffffffffu, y2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, d2);
+        atomicAdd(out + 1, y2);
+    }
+}
+
+int lg(int64_t x) {
+    int b = 0;
+    while (((int64_t)1 << b) < x) ++b;
+    return b;
+}
+
+}  // namespace
+
+TuneKey tune_key(int mode, int64_t m, int64_t n, int64_t k) { return TuneKey{mode, lg(m), lg(n), lg(k)}; }
+
+const TuneEntry* tune_lookup(dgt_context* h, int mode, int64_t m, int64_t n, int64_t k) {
+    auto it = h->tune.find(tune_key(mode, m, n, k));
+    return it == h->tune.end() ? nullptr : &it->second;
+}
+
+}  // namespace dgt
+
+using namespace dgt;
+
+extern "C" {
+
+dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64_t n, int64_t k, const double* A,
+                              int64_t lda, const double* B, int64_t ldb, double* C, int64_t ldc, dgt_fp64_mode mode,
+                              double tol, dgt_tune_result* result) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!result) return fail(h, DGT_ERROR_INVALID_VALUE, "null result");
+    if (m <= 0 || n <= 0 || k <= 0 || !A || !B || !C) return fail(h, DGT_ERROR_INVALID_VALUE, "bad shape or pointer");
+    if (mode != DGT_FP64_NATIVE && mode != DGT_FP64_OZAKI_INT8 && mode != DGT_FP64_AUTO)
+        return fail(h, DGT_ERROR_UNSUPPORTED, "the autotuner covers the native, INT8 Ozaki and AUTO modes");
+    const double one = 1.0, zero = 0.0;
+    cudaEvent_t e0, e1;
+    DGT_CUDA_TRY(h, cudaEventCreate(&e0));
+    DGT_CUDA_TRY(h, cudaEventCreate(&e1));
+    const int saved_dv = h->dmma_variant, saved_ov = h->ozaki_variant;
+    auto time_call = [&](dgt_fp64_mode md, int S, float* ms) -> dgt_status {
+        dgt_status st = DGT_SUCCESS;
+        float best = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {  // first call warms up
+            cudaEventRecord(e0, h->stream);
+            st = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc, md, S);
+            cudaEventRecord(e1, h->stream);
+            if (st != DGT_SUCCESS) return st;
+            if (cudaEventSynchronize(e1) != cudaSuccess) return cuda_fail(h, cudaGetLastError(), "autotune timing");
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (rep > 0) best = std::min(best, t);
+        }
+        *ms = best;
+        return DGT_SUCCESS;
+    };
+    // the tuner must measure raw variants, not earlier tuning decisions
+    std::map<TuneKey, TuneEntry> saved_table;
+    saved_table.swap(h->tune);
+    dgt_status st = DGT_SUCCESS;
+    TuneEntry nat{DGT_FP64_NATIVE, 0, 0, 1e30f, 0.0}, ozk{DGT_FP64_OZAKI_INT8, 0, h->slices, 1e30f, 0.0};
+    if (mode != DGT_FP64_OZAKI_INT8) {
+        for (int v = 0; v < dmma_variant_count() && st == DGT_SUCCESS; ++v) {
+            h->dmma_variant = v;
+            float t;
+            st = time_call(DGT_FP64_NATIVE, 0, &t);
+            if (st == DGT_SUCCESS && t < nat.ms) nat = TuneEntry{DGT_FP64_NATIVE, v, 0, t, 0.0};
+        }
+    }
+    if (st == DGT_SUCCESS && mode != DGT_FP64_NATIVE) {
+        int S = h->slices;
+        if (mode == DGT_FP64_AUTO) {
+            // reference: the native result, kept in workspace slot 1
+            void* ref = nullptr;
+            st = ensure_workspace(h, (size_t)m * n * sizeof(double) + 64, &ref, 1);
+            if (st == DGT_SUCCESS) {
+                h->dmma_variant = nat.variant;
+                st = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, (double*)ref, m, DGT_FP64_NATIVE, 0);
+            }
+            double* sums = (double*)ref + (size_t)m * n;
+            S = 0;
+            for (int s = 4; s <= 14 && st == DGT_SUCCESS; ++s) {
+                st = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc, DGT_FP64_OZAKI_INT8, s);
+                if (st != DGT_SUCCESS) break;
+                cudaMemsetAsync(sums, 0, 2 * sizeof(double), h->stream);
+                diff_norms<<<h->num_sms * 4, 256, 0, h->stream>>>(C, (double*)ref, m, n, ldc, m, sums);
+                double hs[2] = {0, 0};
+                cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, h->stream);
+                if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+                    st = cuda_fail(h, cudaGetLastError(), "autotune accuracy check");
+                    break;
+                }
+                double rel = hs[1] > 0 ? std::sqrt(hs[0] / hs[1]) : std::sqrt(hs[0]);
+                if (rel <= tol) {
+                    S = s;
+                    ozk.rel_diff = rel;
+                    break;
+                }
+            }
+            if (st == DGT_SUCCESS && S == 0) S = -1;  // no slice count reaches tol: emulation not eligible
+        }
+        for (int v = 0; v < 4 && st == DGT_SUCCESS && S > 0; ++v) {
+            h->ozaki_variant = v;
+            float t;
+            st = time_call(DGT_FP64_OZAKI_INT8, S, &t);
+            if (st == DGT_SUCCESS && t < ozk.ms) ozk = TuneEntry{DGT_FP64_OZAKI_INT8, v, S, t, ozk.rel_diff};
+        }
+    }
+    h->tune.swap(saved_table);
+    h->dmma_variant = saved_dv;
+    h->ozaki_variant = saved_ov;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != DGT_SUCCESS) return st;
+    if (mode != DGT_FP64_OZAKI_INT8) h->tune[tune_key(DGT_FP64_NATIVE, m, n, k)] = nat;
+    if (mode != DGT_FP64_NATIVE && ozk.ms < 1e29f) h->tune[tune_key(DGT_FP64_OZAKI_INT8, m, n, k)] = ozk;
+    TuneEntry best = nat;
+    if (mode == DGT_FP64_OZAKI_INT8 || (mode == DGT_FP64_AUTO && ozk.ms < nat.ms)) best = ozk;
+    if (mode == DGT_FP64_AUTO) h->tune[tune_key(DGT_FP64_AUTO, m, n, k)] = best;
+    result->mode = best.mode;
+    result->variant = best.variant;
+    result->slices = best.slices;
+    result->ms = best.ms;
+    result->rel_diff = best.rel_diff;
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_autotune_save(dgt_handle_t h, const char* path) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!path) return fail(h, DGT_ERROR_INVALID_VALUE, "null path");
+    FILE* f = std::fopen(path, "w");
+    if (!f) return fail(h, DGT_ERROR_INVALID_VALUE, std::string("cannot write ") + path);
+    std::fprintf(f, "{\"dgt_tuning\": [\n");
+    size_t i = 0;
+    for (auto& kv : h->tune) {
+        const TuneKey& key = kv.first;
+        const TuneEntry& e = kv.second;
+        std::fprintf(f,
+                     "  {\"key_mode\": %d, \"lg_m\": %d, \"lg_n\": %d, \"lg_k\": %d, \"mode\": %d, \"variant\": %d, "
+                     "\"slices\": %d, \"ms\": %.6f, \"rel_diff\": %.6e}%s\n",
+                     key.mode, key.lm, key.ln, key.lk, e.mode, e.variant, e.slices, e.ms, e.rel_diff,
+                     (++i < h->tune.size()) ? "," : "");
+    }
+    std::fprintf(f, "]}\n");
+    std::fclose(f);
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_autotune_load(dgt_handle_t h, const char* path) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!path) return fail(h, DGT_ERROR_INVALID_VALUE, "null path");
+    FILE* f = std::fopen(path, "r");
+    if (!f) return fail(h, DGT_ERROR_INVALID_VALUE, std::string("cannot read ") + path);
+    char line[512];
+    int loaded = 0;
+    while (std::fgets(line, sizeof(line), f)) {
+        TuneKey key{};
+        TuneEntry e{};
+        if (std::sscanf(line,
+                        " {\"key_mode\": %d, \"lg_m\": %d, \"lg_n\": %d, \"lg_k\": %d, \"mode\": %d, \"variant\": %d, "
+                        "\"slices\": %d, \"ms\": %f, \"rel_diff\": %lf}",
+                        &key.mode, &key.lm, &key.ln, &key.lk, &e.mode, &e.variant, &e.slices, &e.ms,
+                        &e.rel_diff) == 9) {
+            h->tune[key] = e;
+            ++loaded;
+        }
+    }
+    std::fclose(f);
+    return loaded > 0 ? DGT_SUCCESS : fail(h, DGT_ERROR_INVALID_VALUE, "no tuning entries in file");
+}
+
+}  // extern "C"

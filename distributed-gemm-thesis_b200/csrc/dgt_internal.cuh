@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <map>
+#include <tuple>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -17,6 +19,21 @@
 #define DGT_DEVERR_TIMEOUT 0x1u
 #define DGT_DEVERR_BOUNDS 0x2u
 
+namespace dgt {
+// Autotuner table: shape class -> chosen kernel (autotune.cu).
+struct TuneKey {
+    int mode, lm, ln, lk;  // mode and ceil(log2) of m, n, k
+    bool operator<(const TuneKey& o) const {
+        return std::tie(mode, lm, ln, lk) < std::tie(o.mode, o.lm, o.ln, o.lk);
+    }
+};
+struct TuneEntry {
+    int mode, variant, slices;
+    float ms;
+    double rel_diff;
+};
+}  // namespace dgt
+
 struct dgt_context {
     cudaStream_t stream = nullptr;
     int device = 0;
@@ -24,6 +41,7 @@ struct dgt_context {
     dgt_fp64_mode fp64_mode = DGT_FP64_NATIVE;
     int slices = 7;
     int dmma_variant = 0;  // native FP64 kernel variant (see dgemm_dmma.cu)
+    int ozaki_variant = 0; // INT8 Ozaki kernel variant (see ozaki.cu)
     bool profile = false;  // record phase events (DGT_TUNE_PROFILE)
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // split start, gemm start, gemm end
     bool ev_split = false;  // last call had a split phase
@@ -34,6 +52,10 @@ struct dgt_context {
     void* workspace2 = nullptr;
     size_t workspace2_bytes = 0;
     std::atomic<int64_t> launches{0};
+    std::map<dgt::TuneKey, dgt::TuneEntry> tune;
+    void* table = nullptr;  // grouped-GEMM problem table (dgemm_dmma.cu)
+    size_t table_bytes = 0;
+    uint64_t table_hash = 0;
 };
 
 namespace dgt {
@@ -93,6 +115,8 @@ struct Problem {
 };
 
 int dmma_variant_count();
+TuneKey tune_key(int mode, int64_t m, int64_t n, int64_t k);
+const TuneEntry* tune_lookup(dgt_context* h, int mode, int64_t m, int64_t n, int64_t k);
 // Launches the persistent grouped FP64 DMMA kernel over problems/segments (host arrays,
 // copied to device workspace).  Validation is the caller's job.
 dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs);

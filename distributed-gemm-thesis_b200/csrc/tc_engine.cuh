@@ -1,0 +1,488 @@
+// The tcgen05 "digit GEMM" engine shared by the FP64 emulation (ozaki.cu) and the FP32
+// split GEMMs (sgemm.cu): C (+)= sum over flush groups of sums of digit-plane products,
+// operands staged by TMA from K-major planes, products in TMEM, folded by an epilogue.
+//
+// Persistent, one 128 x 256 output tile per CTA at a time, warp-specialised: warp 0 issues
+// TMA loads of the planes (swizzled boxes, STAGES-deep mbarrier ring), warp 1 issues
+// tcgen05.mma (M=128, N=256, K=32 bytes per instruction) into one of two 256-column TMEM
+// accumulators, the epilogue warps drain the other accumulator (tcgen05.ld.32x32b.x32) into
+// C while the next group multiplies.  Every mbarrier wait has an iteration budget; on
+// expiry the kernel records DGT_DEVERR_TIMEOUT, stops all roles, waits for its own MMAs and
+// loads, frees TMEM and returns.
+#pragma once
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dgt_internal.cuh"
+
+namespace dgt {
+namespace oz {
+
+constexpr int TM = 128, TN = 256;  // output tile
+constexpr int KPAD = 128;          // K of the digit planes is padded to a multiple of this
+constexpr uint32_t TMEM_COLS = 512;
+
+// Kernel variants (the autotuner's knob): epilogue warps (4 or 8), K bytes per pipeline
+// stage (128 with 128-byte swizzle, or 64 with 64-byte swizzle), ring depth.
+template <int EPI_, int TKB_, int STAGES_>
+struct OzCfg {
+    static constexpr int EPI = EPI_, TKB = TKB_, STAGES = STAGES_;
+    static constexpr int THREADS = 64 + 32 * EPI;
+    static constexpr int A_STAGE = TM * TKB, B_STAGE = TN * TKB;
+    static constexpr size_t SMEM = 1024 + (size_t)STAGES * (A_STAGE + B_STAGE) + 256 + (size_t)EPI * TN * 4;
+};
+constexpr int EXP_NONFINITE = 0x7fff;
+constexpr long long WAIT_BUDGET = 4000000000LL;  // clock64 cycles (~2 s) per wait
+constexpr int GROUP_M = 8;
+
+struct Seg {
+    int32_t a, b;       // digit-plane indices (0-based) of A and B
+    int32_t kb0, kb1;   // k-block range [kb0, kb1) in units of the kernel's stage depth
+};
+struct Group {
+    int32_t seg0, seg1;  // segments [seg0, seg1)
+    int32_t d;           // diagonal (1-based digit indices s + t)
+    int32_t pad;
+};
+
+struct Params {
+    int64_t m, n, ldc;
+    int32_t m_pad, n_pad;
+    int32_t tiles_m, tiles_n;
+    int32_t ngroups;
+    double alpha, beta;
+    double* C;
+    const int32_t* row_exp;
+    const int32_t* col_exp;
+    const Seg* segs_ext;      // schedule in device memory when it exceeds the inline tables
+    const Group* groups_ext;
+    unsigned int* err;
+    float* Cf;  // FP32 output (EPI_MODE 1)
+    float alpha_f, beta_f;
+    // The schedule travels inside the launch's parameters (so a captured CUDA graph needs
+    // no host-to-device copy); MAX_SEGS / MAX_GROUPS keep the block under 32 KB.
+    Seg segs[640];
+    Group groups[640];
+};
+constexpr int MAX_SEGS = 640, MAX_GROUPS = 640;
+
+// ---- small PTX wrappers --------------------------------------------------------------------
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait.  Returns false (and raises the CTA abort flag + device error word) when the
+// budget runs out or another role already aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                          unsigned int* err) {
+    long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > WAIT_BUDGET) {
+            *abort_flag = 1;
+            atomicOr(err, DGT_DEVERR_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int32_t x, int32_t y,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
+            "r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// K-major operand tile in shared memory with the swizzle the TMA box used: rows of TKB
+// bytes (128 -> SWIZZLE_128B, 64 -> SWIZZLE_64B), 8-row groups 8*TKB bytes apart (stride
+// byte offset), SM100 descriptor version 1.
+template <int TKB>
+__device__ __forceinline__ uint64_t smem_desc_k(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                        // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)((8 * TKB) >> 4) << 32;         // stride byte offset
+    d |= (uint64_t)1 << 46;                        // descriptor version (sm100)
+    d |= (uint64_t)(TKB == 128 ? 2 : 4) << 61;     // SWIZZLE_128B or SWIZZLE_64B
+    return d;
+}
+
+// Instruction descriptor: kind::i8, D = S32, A = B = signed 8-bit, both K-major, M=128, N=256.
+constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                              ((uint32_t)(TM >> 4) << 24);
+
+// Instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major, M=128, N=256.
+constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                                ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// 2^e for e in [-1022, 1023], built from the exponent field.
+__device__ __forceinline__ double pow2i(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+// x * 2^e for any e (at most three exact power-of-two steps).
+__device__ __forceinline__ double scale2(double x, int e) {
+    while (e > 1000) {
+        x *= pow2i(1000);
+        e -= 1000;
+    }
+    while (e < -1000) {
+        x *= pow2i(-1000);
+        e += 1000;
+    }
+    return x * pow2i(e);
+}
+
+// e with max in [2^(e-1), 2^e) from the bit pattern of max = |x|max (0 -> 0, inf/nan -> marker)
+__device__ __forceinline__ int exponent_of_max(unsigned long long bits) {
+    if (bits == 0ull) return 0;
+    if (bits >= 0x7ff0000000000000ull) return EXP_NONFINITE;
+    int ef = (int)(bits >> 52);
+    if (ef == 0) return (64 - __clzll((long long)bits)) - 1074;  // subnormal
+    return ef - 1022;
+}
+
+// ---- split kernels ---------------------------------------------------------------------------
+
+// Per-mn max |x| as the bit pattern of |x| (monotone for non-negative doubles).
+
+// KIND: 0 = INT8 digits (kind::i8, INT32 accumulator), 1 = BF16 operands (kind::f16, FP32
+// accumulator).  EPI: 0 = FP64 fold C = beta*C + alpha*sum_g 2^(e_i+f_j-7d_g) P_g,
+// 1 = FP32 output C = alpha*acc + beta*C (a single flush group).
+template <class CF, int KIND, int EPI_MODE>
+__global__ void __launch_bounds__(CF::THREADS, 1)
+    digit_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+               const __grid_constant__ Params P) {
+    constexpr int STAGES = CF::STAGES, TKB = CF::TKB, A_STAGE = CF::A_STAGE, B_STAGE = CF::B_STAGE;
+    constexpr int EPI = CF::EPI;
+    const Seg* SEGS = P.segs_ext ? P.segs_ext : P.segs;
+    const Group* GROUPS = P.groups_ext ? P.groups_ext : P.groups;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + STAGES * A_STAGE;
+    uint64_t* bars = (uint64_t*)(sB + STAGES * B_STAGE);
+    // bars: full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], done
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 5);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    int32_t* col_exp_all = (int32_t*)(tmem_slot + 4);  // TN entries per epilogue warp
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto full = [&](int s) { return su32(bars + s); };
+    auto empty = [&](int s) { return su32(bars + STAGES + s); };
+    auto accf = [&](int b) { return su32(bars + 2 * STAGES + b); };
+    auto acce = [&](int b) { return su32(bars + 2 * STAGES + 2 + b); };
+    const uint32_t done_bar = su32(bars + 2 * STAGES + 4);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(accf(b), 1);
+            mbar_init(acce(b), EPI);
+        }
+        mbar_init(done_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(su32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    const int total_tiles = P.tiles_m * P.tiles_n;
+    auto tile_coords = [&](int tile, int& tm, int& tn) {
+        int in_group = GROUP_M * P.tiles_n;
+        int grp = tile / in_group;
+        int first_m = grp * GROUP_M;
+        int gsize = min(P.tiles_m - first_m, GROUP_M);
+        tm = first_m + (tile % in_group) % gsize;
+        tn = (tile % in_group) / gsize;
+    };
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+                int tm, tn;
+                tile_coords(tile, tm, tn);
+                for (int g = 0; g < P.ngroups && ok; ++g) {
+                    const Group G = GROUPS[g];
+                    for (int si = G.seg0; si < G.seg1 && ok; ++si) {
+                        const Seg sg = SEGS[si];
+                        for (int kb = sg.kb0; kb < sg.kb1; ++kb) {
+                            const int s = it % STAGES;
+                            const uint32_t ph = (it / STAGES) & 1;
+                            if (!mbar_wait(empty(s), ph ^ 1, abort_flag, P.err)) {
+                                ok = false;
+                                break;
+                            }
+                            mbar_expect_tx(full(s), A_STAGE + B_STAGE);
+                            tma_load_2d(su32(sA + s * A_STAGE), &tmA, kb * TKB, sg.a * P.m_pad + tm * TM, full(s));
+                            tma_load_2d(su32(sB + s * B_STAGE), &tmB, kb * TKB, sg.b * P.n_pad + tn * TN, full(s));
+                            ++it;
+                        }
+                    }
+                }
+            }
+            // drain: wait for this CTA's own loads still in flight (bounded)
+            if (!ok) {
+                for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
+                    long long t0 = clock64();
+                    while (!mbar_try(full(j % STAGES), (j / STAGES) & 1) && clock64() - t0 < WAIT_BUDGET) {
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            uint32_t it = 0, gcount = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+                for (int g = 0; g < P.ngroups && ok; ++g, ++gcount) {
+                    const Group G = GROUPS[g];
+                    const int b = gcount & 1;
+                    const uint32_t u = gcount >> 1;
+                    if (!mbar_wait(acce(b), (u & 1) ^ 1, abort_flag, P.err)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t d_tmem = tmem_base + (uint32_t)(b * TN);
+                    uint32_t acc = 0;
+                    for (int si = G.seg0; si < G.seg1 && ok; ++si) {
+                        const Seg sg = SEGS[si];
+                        for (int kb = sg.kb0; kb < sg.kb1; ++kb) {
+                            const int s = it % STAGES;
+                            const uint32_t ph = (it / STAGES) & 1;
+                            if (!mbar_wait(full(s), ph, abort_flag, P.err)) {
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                            const uint64_t ad = smem_desc_k<TKB>(su32(sA + s * A_STAGE));
+                            const uint64_t bd = smem_desc_k<TKB>(su32(sB + s * B_STAGE));
+#pragma unroll
+                            for (int kk = 0; kk < TKB / 32; ++kk) {
+                                // advance 32 bytes (one K=32 step) inside the 128-byte swizzle atom
+                                if constexpr (KIND == 0)
+                                    mma_i8(d_tmem, ad + (uint64_t)(kk * 2), bd + (uint64_t)(kk * 2), IDESC_I8, acc);
+                                else
+                                    mma_bf16(d_tmem, ad + (uint64_t)(kk * 2), bd + (uint64_t)(kk * 2), IDESC_BF16, acc);
+                                acc = 1;
+                            }
+                            tc_commit(empty(s));
+                            ++it;
+                        }
+                    }
+                    if (ok) tc_commit(accf(b));
+                }
+            }
+            // every MMA this CTA issued has completed once done_bar flips
+            tc_commit(done_bar);
+            long long t0 = clock64();
+            while (!mbar_try(done_bar, 0) && clock64() - t0 < WAIT_BUDGET) {
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue: TMEM -> FP64 -> C ----------------
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int r_in = q * 32 + lane;
+        int32_t* col_exp_s = col_exp_all + (warp - 2) * TN;
+        uint32_t gcount = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+            int tm, tn;
+            tile_coords(tile, tm, tn);
+            const int64_t row = (int64_t)tm * TM + r_in;
+            const int64_t n0 = (int64_t)tn * TN;
+            // each epilogue warp keeps its own copy of the tile's column exponents, so warps
+            // never wait on one another (a warp that aborts cannot strand the others)
+            __syncwarp();
+            if constexpr (EPI_MODE == 0)
+                for (int c = lane; c < TN; c += 32) col_exp_s[c] = (n0 + c < P.n) ? P.col_exp[n0 + c] : 0;
+            __syncwarp();
+            const bool row_ok = row < P.m;
+            const int e_row = (EPI_MODE == 0 && row_ok) ? P.row_exp[row] : 0;
+            for (int g = 0; g < P.ngroups; ++g, ++gcount) {
+                const int b = gcount & 1;
+                const uint32_t u = gcount >> 1;
+                if (!mbar_wait(accf(b), u & 1, abort_flag, P.err)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const int d = GROUPS[g].d;
+                // with 8 epilogue warps, two warps share a lane quarter and split the columns
+                constexpr int CHUNKS = TN / 32 / (EPI / 4);
+                const int ch0 = ((warp - 2) / 4) * CHUNKS;
+                for (int ch = ch0; ch < ch0 + CHUNKS; ++ch) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TN + ch * 32), v);
+                    if (!row_ok) continue;
+                    const int64_t rem_cols = P.n - (n0 + ch * 32);
+                    const int ncols = rem_cols < 32 ? (int)rem_cols : 32;
+                    if constexpr (EPI_MODE == 1) {
+                        float* fbase = P.Cf + row + (n0 + ch * 32) * P.ldc;
+                        float prevf[32];
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) {
+                            prevf[c] = 0.f;
+                            if (c < ncols) {
+                                if (g > 0)
+                                    prevf[c] = fbase[c * P.ldc];
+                                else if (P.beta_f != 0.f)
+                                    prevf[c] = P.beta_f * fbase[c * P.ldc];
+                            }
+                        }
+#pragma unroll
+                        for (int c = 0; c < 32; ++c)
+                            if (c < ncols) fbase[c * P.ldc] = fmaf(P.alpha_f, __uint_as_float(v[c]), prevf[c]);
+                        continue;
+                    }
+                    double prev[32];
+                    double* cbase = P.C + row + (n0 + ch * 32) * P.ldc;
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        prev[c] = 0.0;
+                        if (c < ncols) {
+                            if (g > 0)
+                                prev[c] = cbase[c * P.ldc];
+                            else if (P.beta != 0.0)
+                                prev[c] = P.beta * cbase[c * P.ldc];
+                        }
+                    }
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        if (c < ncols) {
+                            const int ec = col_exp_s[ch * 32 + c];
+                            double t;
+                            const double acc_v =
+                                (KIND == 0) ? (double)(int32_t)v[c] : (double)__uint_as_float(v[c]);
+                            if (e_row == EXP_NONFINITE || ec == EXP_NONFINITE)
+                                t = __longlong_as_double(0x7ff8000000000000ll);
+                            else
+                                t = scale2(acc_v, e_row + ec - 7 * d);
+                            cbase[c * P.ldc] = fma(P.alpha, t, prev[c]);
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acce(b));
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+}
+
+
+
+inline PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// 2D map over the stacked digit planes: [S * rows_pad][k_pad] bytes, box = box_rows x tkb B.
+// k_pad_bytes is the row length in bytes (elements * element size).
+inline bool make_plane_map(CUtensorMap* map, void* base, int64_t rows_total, int64_t k_pad_bytes, int box_rows,
+                           int tkb) {
+    auto enc = get_encode();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)k_pad_bytes, (cuuint64_t)rows_total};
+    cuuint64_t strides[1] = {(cuuint64_t)k_pad_bytes};
+    cuuint32_t box[2] = {(cuuint32_t)tkb, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, tkb == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+
+}  // namespace oz
+}  // namespace dgt

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libdgt.so")
 SUCCESS, INVALID_VALUE, UNSUPPORTED, CUDA_ERROR, TIMEOUT, ALLOC, NOT_INITIALIZED = range(7)
 FP64_NATIVE, FP64_OZAKI_INT8, FP64_OZAKI_BF16, FP64_AUTO = range(4)
 FP32_SIMT, FP32_BF16X1, FP32_BF16X3 = range(3)
-TUNE_DMMA_VARIANT, TUNE_OZAKI_SLICES, TUNE_PROFILE = range(3)
+TUNE_DMMA_VARIANT, TUNE_OZAKI_SLICES, TUNE_PROFILE, TUNE_OZAKI_VARIANT = range(4)
 
 _c_i64 = ctypes.c_int64
 _c_i32 = ctypes.c_int32
@@ -39,6 +39,11 @@ class GemmDesc(ctypes.Structure):
     _fields_ = [("m", _c_i64), ("n", _c_i64), ("k", _c_i64), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
                 ("A", _vp), ("lda", _c_i64), ("B", _vp), ("ldb", _c_i64), ("C", _vp), ("ldc", _c_i64),
                 ("transa", ctypes.c_char), ("transb", ctypes.c_char)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("mode", _c_i32), ("variant", _c_i32), ("slices", _c_i32), ("ms", ctypes.c_float),
+                ("rel_diff", ctypes.c_double)]
 
 
 class GridLayout(ctypes.Structure):
@@ -79,6 +84,10 @@ SIGNATURES = [
     ("dgt_copy_block", _c_i32, [_vp, _c_i64, _c_i64, _vp, _vp, _c_i64, _c_i64, _c_i32]),
     ("dgt_set_tuning", _c_i32, [_vp, _c_i32, _c_i32]),
     ("dgt_get_tuning", _c_i32, [_vp, _c_i32, ctypes.POINTER(_c_i32)]),
+    ("dgt_autotune_dgemm", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _vp, _c_i64, _vp,
+                                     _c_i64, _vp, _c_i64, _c_i32, ctypes.c_double, ctypes.POINTER(TuneResult)]),
+    ("dgt_autotune_save", _c_i32, [_vp, ctypes.c_char_p]),
+    ("dgt_autotune_load", _c_i32, [_vp, ctypes.c_char_p]),
     ("dgt_probe_peak", _c_i32, [_vp, _c_i32, _dp]),
     ("dgt_last_timings", _c_i32, [_vp, ctypes.POINTER(ctypes.c_float), _c_i32]),
     ("dgt_launch_count", _c_i64, [_vp]),
@@ -171,6 +180,18 @@ class Handle:
         out = (ctypes.c_float * 2)()
         n = self.lib.dgt_last_timings(self.h, out, 2)
         return (out[0], out[1]) if n == 2 else (None, None)
+
+    def autotune(self, ta, tb, m, n, k, A, lda, B, ldb, C, ldc, mode=FP64_AUTO, tol=1e-14):
+        r = TuneResult()
+        self._check(self.lib.dgt_autotune_dgemm(self.h, ta.encode(), tb.encode(), m, n, k, _vp(A), lda, _vp(B), ldb,
+                                                _vp(C), ldc, mode, tol, ctypes.byref(r)))
+        return {"mode": r.mode, "variant": r.variant, "slices": r.slices, "ms": r.ms, "rel_diff": r.rel_diff}
+
+    def autotune_save(self, path):
+        self._check(self.lib.dgt_autotune_save(self.h, path.encode()))
+
+    def autotune_load(self, path):
+        self._check(self.lib.dgt_autotune_load(self.h, path.encode()))
 
     def probe_peak(self, kind: int) -> float:
         v = ctypes.c_double()

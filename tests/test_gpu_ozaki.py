@@ -107,3 +107,36 @@ def test_ozaki_large_4096(h):
     got = host(dC, (n, n))
     rows = np.random.default_rng(0).choice(n, 64, replace=False)
     assert O.rel_errors(got[rows, :], A[rows, :] @ B)[1] <= 1e-13
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_ozaki_kernel_variants(variant):
+    """Every tuning variant of the INT8 kernel (epilogue warps x stage depth) gives the
+    same digits-exact products: identical to variant 0, and within 1e-13 of the oracle."""
+    import torch
+
+    m, n, k = 300, 520, 1000
+    A, B, C = O.uniform((m, k), 41), O.uniform((k, n), 42), O.uniform((m, n), 43)
+    outs = []
+    for v in (0, variant):
+        with dgt.Handle() as hh:
+            hh.set_tuning(dgt.TUNE_OZAKI_VARIANT, v)
+            dA, dB, dC = dev(A), dev(B), dev(C)
+            hh.dgemm("N", "N", m, n, k, 1.25, ptr(dA), m, ptr(dB), k, 0.5, ptr(dC), m, mode=dgt.FP64_OZAKI_INT8,
+                     slices=7)
+            torch.cuda.synchronize()
+            hh.check_device()
+            outs.append(host(dC, (m, n)))
+    assert np.array_equal(outs[0], outs[1])
+    assert O.rel_errors(outs[1], O.dgemm(A, B, 1.25, 0.5, C))[1] <= 1e-13
+
+
+@pytest.mark.parametrize("shape", [(256, 256, 128), (300, 200, 2500), (1, 1, 1)])
+def test_ozaki_bf16_slices(h, shape):
+    """BF16 digit planes with exact FP32 accumulation (flushed every 1024 of K) give the
+    same accuracy as the INT8 planes."""
+    m, n, k = shape
+    got16, want = run(h, "N", "N", m, n, k, 1.5, -0.5, 7, mode=dgt.FP64_OZAKI_BF16)
+    got8, _ = run(h, "N", "N", m, n, k, 1.5, -0.5, 7)
+    assert O.rel_errors(got16, want)[1] <= 1e-13
+    assert O.rel_errors(got16, got8)[1] <= 1e-14
