@@ -14,8 +14,9 @@
 namespace dgt {
 
 dgt_status ensure_workspace(dgt_context* h, size_t bytes, void** out, int slot) {
-    void*& ptr = slot == 0 ? h->workspace : h->workspace2;
-    size_t& cap = slot == 0 ? h->workspace_bytes : h->workspace2_bytes;
+    if (slot < 0 || slot > 2) return fail(h, DGT_ERROR_INVALID_VALUE, "bad workspace slot");
+    void*& ptr = h->ws[slot];
+    size_t& cap = h->ws_bytes[slot];
     if (bytes > cap) {
         if (ptr) {
             cudaStreamSynchronize(h->stream);
@@ -67,6 +68,38 @@ static bool cannon_order(int p, int c, int i, int j, int k, int* out) {
     return covers;
 }
 
+// Emulated-FP64 execution of a step schedule: every segment of a problem is one Ozaki GEMM
+// (the reference issues one cublasDgemm per step too); the first applies the problem's beta,
+// the rest accumulate.  Each call splits its own operands, so every step is scaled on its
+// own panel -- the same numerics as a per-step local GEMM.
+dgt_status run_problems_emulated(dgt_context* h, const std::vector<Problem>& probs,
+                                        const std::vector<KSegment>& segs, dgt_fp64_mode mode, int slices) {
+    if (slices < 2 || slices > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+    for (const Problem& pr : probs) {
+        if (pr.m <= 0 || pr.n <= 0) continue;
+        bool first = true;
+        for (int s = 0; s < pr.seg_count; ++s) {
+            const KSegment& sg = segs[pr.seg_begin + s];
+            if (sg.k <= 0) continue;
+            const double beta = first ? pr.beta : 1.0;
+            dgt_status st = ozaki_dgemm(h, pr.transa != 0, pr.transb != 0, pr.m, pr.n, sg.k, pr.alpha, sg.A, sg.lda,
+                                        sg.B, sg.ldb, beta, pr.C, pr.ldc, mode, slices);
+            if (st != DGT_SUCCESS) return st;
+            first = false;
+        }
+        if (first && pr.beta != 1.0) {  // no K at all: C = beta * C through the native kernel
+            std::vector<Problem> one{pr};
+            one[0].alpha = 0.0;
+            one[0].seg_begin = 0;
+            one[0].seg_count = 1;
+            std::vector<KSegment> none{KSegment{nullptr, nullptr, 1, 1, 0}};
+            dgt_status st = launch_dmma_grouped(h, one, none);
+            if (st != DGT_SUCCESS) return st;
+        }
+    }
+    return DGT_SUCCESS;
+}
+
 }  // namespace dgt
 
 using namespace dgt;
@@ -109,8 +142,8 @@ dgt_status dgt_destroy(dgt_handle_t h) {
     cudaStreamSynchronize(h->stream);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
-    if (h->workspace) cudaFree(h->workspace);
-    if (h->workspace2) cudaFree(h->workspace2);
+    for (void* w : h->ws)
+        if (w) cudaFree(w);
     if (h->table) cudaFree(h->table);
     if (h->dev_error) cudaFree(h->dev_error);
     delete h;
@@ -155,7 +188,7 @@ dgt_status dgt_set_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t value) {
             h->profile = value != 0;
             return DGT_SUCCESS;
         case DGT_TUNE_OZAKI_VARIANT:
-            if (value < 0 || value > 3) return fail(h, DGT_ERROR_INVALID_VALUE, "unknown Ozaki kernel variant");
+            if (value < 0 || value > 4) return fail(h, DGT_ERROR_INVALID_VALUE, "unknown Ozaki kernel variant");
             h->ozaki_variant = value;
             return DGT_SUCCESS;
     }
@@ -333,15 +366,6 @@ dgt_status dgt_dgemm_grouped(dgt_handle_t h, int count, const dgt_gemm_desc* d, 
         if (st != DGT_SUCCESS) return st;
     }
     if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
-    if (mode != DGT_FP64_NATIVE) {
-        for (int i = 0; i < count; ++i) {
-            if (d[i].m == 0 || d[i].n == 0) continue;
-            dgt_status st = dgt_dgemm_ex(h, d[i].transa, d[i].transb, d[i].m, d[i].n, d[i].k, &d[i].alpha, d[i].A,
-                                         d[i].lda, d[i].B, d[i].ldb, &d[i].beta, d[i].C, d[i].ldc, mode, slices);
-            if (st != DGT_SUCCESS) return st;
-        }
-        return DGT_SUCCESS;
-    }
     std::vector<Problem> probs;
     std::vector<KSegment> segs;
     probs.reserve(count);
@@ -361,6 +385,7 @@ dgt_status dgt_dgemm_grouped(dgt_handle_t h, int count, const dgt_gemm_desc* d, 
         segs.push_back(KSegment{d[i].A, d[i].B, d[i].lda, d[i].ldb, d[i].k});
         probs.push_back(p);
     }
+    if (mode != DGT_FP64_NATIVE) return run_problems_emulated(h, probs, segs, mode, slices);
     return launch_dmma_grouped(h, probs, segs);
 }
 
@@ -444,7 +469,7 @@ dgt_status dgt_summa(dgt_handle_t h, const dgt_grid_layout* L, int64_t M, int64_
         }
     }
     if (mode == DGT_FP64_NATIVE) return launch_dmma_grouped(h, probs, segs);
-    return fail(h, DGT_ERROR_UNSUPPORTED, "SUMMA with Ozaki emulation is not implemented in this build");
+    return run_problems_emulated(h, probs, segs, mode, slices);
 }
 
 // ---- 2.5D Cannon -----------------------------------------------------------------------------
@@ -460,14 +485,12 @@ dgt_status dgt_cannon25d(dgt_handle_t h, int64_t M, int32_t p, int32_t c, char t
     if (!valid_op(ta) || !valid_op(tb)) return fail(h, DGT_ERROR_INVALID_VALUE, "transpose must be N, T or C");
     if (p * p > 256) return fail(h, DGT_ERROR_UNSUPPORTED, "more than 256 tiles per stack");
     if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
-    if (mode != DGT_FP64_NATIVE)
-        return fail(h, DGT_ERROR_UNSUPPORTED, "Cannon with Ozaki emulation is not implemented in this build");
     const int64_t lm = M / p, tile = lm * lm;
     const int pc3 = p / c;
     double* W = nullptr;
     if (c > 1) {
         void* ws = nullptr;
-        dgt_status st = ensure_workspace(h, (size_t)(c - 1) * p * p * tile * sizeof(double), &ws, 0);
+        dgt_status st = ensure_workspace(h, (size_t)(c - 1) * p * p * tile * sizeof(double), &ws, 2);
         if (st != DGT_SUCCESS) return st;
         W = (double*)ws;
     }
@@ -498,7 +521,8 @@ dgt_status dgt_cannon25d(dgt_handle_t h, int64_t M, int32_t p, int32_t c, char t
             }
         }
     }
-    dgt_status st = launch_dmma_grouped(h, probs, segs);
+    dgt_status st = (mode == DGT_FP64_NATIVE) ? launch_dmma_grouped(h, probs, segs)
+                                              : run_problems_emulated(h, probs, segs, mode, slices);
     if (st != DGT_SUCCESS || c == 1) return st;
     // stack reduction (reduceResult, src/25DCannon.cpp:203-228) into the stack-0 tiles
     return launch_stack_reduce(h, tile, p * p, c - 1, C_tiles, W, (int64_t)p * p * tile);

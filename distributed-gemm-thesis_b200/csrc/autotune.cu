@@ -133,11 +133,36 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
             }
             if (st == DGT_SUCCESS && S == 0) S = -1;  // no slice count reaches tol: emulation not eligible
         }
-        for (int v = 0; v < 4 && st == DGT_SUCCESS && S > 0; ++v) {
+        // every kernel variant must reproduce variant 0's result exactly (same digit products,
+        // same fold order); a variant that does not is never chosen
+        double* vref = nullptr;
+        double* vsums = nullptr;
+        if (st == DGT_SUCCESS && S > 0) {
+            void* w = nullptr;
+            st = ensure_workspace(h, 2 * (size_t)m * n * sizeof(double) + 64, &w, 1);
+            vref = (double*)w + (size_t)m * n;  // the first m*n doubles may hold the native reference
+            vsums = vref + (size_t)m * n;
+        }
+        for (int v = 0; v < 5 && st == DGT_SUCCESS && S > 0; ++v) {
             h->ozaki_variant = v;
             float t;
             st = time_call(DGT_FP64_OZAKI_INT8, S, &t);
-            if (st == DGT_SUCCESS && t < ozk.ms) ozk = TuneEntry{DGT_FP64_OZAKI_INT8, v, S, t, ozk.rel_diff};
+            if (st != DGT_SUCCESS) break;
+            if (v == 0) {
+                DGT_CUDA_TRY(h, cudaMemcpy2DAsync(vref, m * sizeof(double), C, ldc * sizeof(double), m * sizeof(double),
+                                                  n, cudaMemcpyDeviceToDevice, h->stream));
+            } else {
+                cudaMemsetAsync(vsums, 0, 2 * sizeof(double), h->stream);
+                diff_norms<<<h->num_sms * 4, 256, 0, h->stream>>>(C, vref, m, n, ldc, m, vsums);
+                double hs[2] = {1, 1};
+                cudaMemcpyAsync(hs, vsums, sizeof(hs), cudaMemcpyDeviceToHost, h->stream);
+                if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+                    st = cuda_fail(h, cudaGetLastError(), "autotune variant check");
+                    break;
+                }
+                if (hs[0] != 0.0) continue;  // not identical to variant 0
+            }
+            if (t < ozk.ms) ozk = TuneEntry{DGT_FP64_OZAKI_INT8, v, S, t, ozk.rel_diff};
         }
     }
     h->tune.swap(saved_table);

@@ -40,17 +40,17 @@ struct dgt_context {
     int num_sms = 148;
     dgt_fp64_mode fp64_mode = DGT_FP64_NATIVE;
     int slices = 7;
-    int dmma_variant = 0;  // native FP64 kernel variant (see dgemm_dmma.cu)
-    int ozaki_variant = 0; // INT8 Ozaki kernel variant (see ozaki.cu)
+    int dmma_variant = 2;  // native FP64 kernel variant (see dgemm_dmma.cu); 2 measured fastest
+    int ozaki_variant = 1; // INT8 Ozaki kernel variant (see ozaki.cu); 1 measured fastest
     bool profile = false;  // record phase events (DGT_TUNE_PROFILE)
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // split start, gemm start, gemm end
     bool ev_split = false;  // last call had a split phase
     std::string last_error;
     unsigned int* dev_error = nullptr;  // one word in device memory
-    void* workspace = nullptr;
-    size_t workspace_bytes = 0;
-    void* workspace2 = nullptr;
-    size_t workspace2_bytes = 0;
+    // workspace slots: 0 = split planes of the Ozaki / FP32 split paths, 1 = autotuner and
+    // probes, 2 = the 2.5D stacks' partial C tiles (live across the Ozaki calls of a Cannon step)
+    void* ws[3] = {nullptr, nullptr, nullptr};
+    size_t ws_bytes[3] = {0, 0, 0};
     std::atomic<int64_t> launches{0};
     std::map<dgt::TuneKey, dgt::TuneEntry> tune;
     void* table = nullptr;  // grouped-GEMM problem table (dgemm_dmma.cu)
@@ -85,7 +85,7 @@ inline dgt_status cuda_fail(dgt_context* h, cudaError_t e, const char* what) {
 // Phase markers for DGT_TUNE_PROFILE (no-ops unless profiling is on).
 void mark(dgt_context* h, int which);
 
-// Grows a handle-owned scratch buffer; never shrinks.  slot 0 or 1.
+// Grows a handle-owned scratch buffer; never shrinks.  slot 0, 1 or 2.
 dgt_status ensure_workspace(dgt_context* h, size_t bytes, void** out, int slot = 0);
 
 inline bool is_trans(char t) { return t == 'T' || t == 't' || t == 'C' || t == 'c'; }

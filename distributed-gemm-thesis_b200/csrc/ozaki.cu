@@ -190,15 +190,18 @@ struct OzakiLayout {
 };
 
 // variant: 0 = 4 epilogue warps / 128-byte stages x4, 1 = 8 warps / 128 B x4,
-//          2 = 4 warps / 64 B x8, 3 = 8 warps / 64 B x8
-static int variant_tkb(int variant) { return (variant >= 2) ? 64 : 128; }
+//          2 = 4 warps / 64 B x8, 3 = 8 warps / 64 B x8,
+//          4 = CTA pair (cta_group::2, 256 x 256 tiles), 8 warps / 128 B x6
+static int variant_tkb(int variant) { return (variant == 2 || variant == 3) ? 64 : 128; }
+static bool variant_pair(int variant) { return variant == 4; }
 
 static dgt_status ozaki_layout(dgt_context* h, int S, int64_t m, int64_t n, int64_t k, int variant, bool bf16,
                                OzakiLayout& L) {
     L.variant = variant;
     L.bf16 = bf16;
     L.tkb = variant_tkb(variant);
-    L.m_pad = ceil_div(m, oz::TM) * oz::TM;
+    const int64_t m_unit = variant_pair(variant) ? 2 * oz::TM : oz::TM;
+    L.m_pad = ceil_div(m, m_unit) * m_unit;
     L.n_pad = ceil_div(n, oz::TN) * oz::TN;
     L.k_pad = ceil_div(k, oz::KPAD) * oz::KPAD;
     if (!ozaki_schedule(S, L.k_pad, L.tkb, bf16, L.segs, L.groups))
@@ -226,7 +229,7 @@ size_t ozaki_scratch_bytes(int S, int64_t m, int64_t n, int64_t k) {
 
 template <class CF, int KIND>
 static cudaError_t launch_ozaki_variant(const CUtensorMap& tmA, const CUtensorMap& tmB, const oz::Params& prm,
-                                        int grid, cudaStream_t s) {
+                                        int num_sms, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(oz::digit_gemm<CF, KIND, 0>,
@@ -234,8 +237,26 @@ static cudaError_t launch_ozaki_variant(const CUtensorMap& tmA, const CUtensorMa
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    oz::digit_gemm<CF, KIND, 0><<<grid, CF::THREADS, CF::SMEM, s>>>(tmA, tmB, prm);
-    return cudaGetLastError();
+    const int tiles = prm.tiles_m * prm.tiles_n;
+    if constexpr (CF::PAIR) {
+        // one 2-CTA cluster per 256 x 256 tile, persistent over half the SMs' worth of clusters
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(2 * std::min(tiles, num_sms / 2)));
+        cfg.blockDim = dim3(CF::THREADS);
+        cfg.dynamicSmemBytes = CF::SMEM;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, oz::digit_gemm<CF, KIND, 0>, tmA, tmB, prm);
+    } else {
+        oz::digit_gemm<CF, KIND, 0><<<std::min(tiles, num_sms), CF::THREADS, CF::SMEM, s>>>(tmA, tmB, prm);
+        return cudaGetLastError();
+    }
 }
 
 // The Ozaki INT8 path on caller-provided scratch (L.total bytes at ws).  h may be null:
@@ -304,8 +325,11 @@ static dgt_status ozaki_run(dgt_context* h, cudaStream_t s, int num_sms, unsigne
 
     CUtensorMap tmA, tmB;
     const int64_t row_bytes = k_pad * (L.bf16 ? 2 : 1);
+    // box heights must equal what one CTA stages per operand: in the CTA-pair kernel each CTA
+    // holds only half of B's 256 rows (TN / 2), so its box is 128 rows high
+    const int b_box = variant_pair(L.variant) ? oz::TN / 2 : oz::TN;
     if (!oz::make_plane_map(&tmA, planesA, (int64_t)S * m_pad, row_bytes, oz::TM, L.tkb) ||
-        !oz::make_plane_map(&tmB, planesB, (int64_t)S * n_pad, row_bytes, oz::TN, L.tkb))
+        !oz::make_plane_map(&tmB, planesB, (int64_t)S * n_pad, row_bytes, b_box, L.tkb))
         return fail(h, DGT_ERROR_CUDA, "cuTensorMapEncodeTiled failed");
     static thread_local oz::Params prm;  // ~21 KB: keep it off the stack
     prm = oz::Params{};
@@ -314,7 +338,7 @@ static dgt_status ozaki_run(dgt_context* h, cudaStream_t s, int num_sms, unsigne
     prm.ldc = ldc;
     prm.m_pad = (int32_t)m_pad;
     prm.n_pad = (int32_t)n_pad;
-    prm.tiles_m = (int32_t)(m_pad / oz::TM);
+    prm.tiles_m = (int32_t)(m_pad / (variant_pair(L.variant) ? 2 * oz::TM : oz::TM));
     prm.tiles_n = (int32_t)(n_pad / oz::TN);
     prm.ngroups = (int32_t)L.groups.size();
     prm.alpha = alpha;
@@ -337,13 +361,14 @@ static dgt_status ozaki_run(dgt_context* h, cudaStream_t s, int num_sms, unsigne
     if (h) mark(h, 1);
     cudaError_t le;
     if (L.bf16) {
-        le = launch_ozaki_variant<oz::OzCfg<8, 128, 4>, 1>(tmA, tmB, prm, grid, s);
+        le = launch_ozaki_variant<oz::OzCfg<8, 128, 4>, 1>(tmA, tmB, prm, num_sms, s);
     } else {
         switch (L.variant) {
-            case 1: le = launch_ozaki_variant<oz::OzCfg<8, 128, 4>, 0>(tmA, tmB, prm, grid, s); break;
-            case 2: le = launch_ozaki_variant<oz::OzCfg<4, 64, 8>, 0>(tmA, tmB, prm, grid, s); break;
-            case 3: le = launch_ozaki_variant<oz::OzCfg<8, 64, 8>, 0>(tmA, tmB, prm, grid, s); break;
-            default: le = launch_ozaki_variant<oz::OzCfg<4, 128, 4>, 0>(tmA, tmB, prm, grid, s); break;
+            case 1: le = launch_ozaki_variant<oz::OzCfg<8, 128, 4>, 0>(tmA, tmB, prm, num_sms, s); break;
+            case 2: le = launch_ozaki_variant<oz::OzCfg<4, 64, 8>, 0>(tmA, tmB, prm, num_sms, s); break;
+            case 3: le = launch_ozaki_variant<oz::OzCfg<8, 64, 8>, 0>(tmA, tmB, prm, num_sms, s); break;
+            case 4: le = launch_ozaki_variant<oz::OzCfg<8, 128, 6, true>, 0>(tmA, tmB, prm, num_sms, s); break;
+            default: le = launch_ozaki_variant<oz::OzCfg<4, 128, 4>, 0>(tmA, tmB, prm, num_sms, s); break;
         }
     }
     if (h) h->launches.fetch_add(1);

@@ -28,11 +28,15 @@ constexpr uint32_t TMEM_COLS = 512;
 
 // Kernel variants (the autotuner's knob): epilogue warps (4 or 8), K bytes per pipeline
 // stage (128 with 128-byte swizzle, or 64 with 64-byte swizzle), ring depth.
-template <int EPI_, int TKB_, int STAGES_>
+// PAIR: a cluster of two CTAs shares one M=256 x N=256 tcgen05.mma (cta_group::2); each CTA
+// stages its 128 rows of A and half (128 rows) of B, so per-SM B traffic halves.
+template <int EPI_, int TKB_, int STAGES_, bool PAIR_ = false>
 struct OzCfg {
     static constexpr int EPI = EPI_, TKB = TKB_, STAGES = STAGES_;
+    static constexpr bool PAIR = PAIR_;
     static constexpr int THREADS = 64 + 32 * EPI;
-    static constexpr int A_STAGE = TM * TKB, B_STAGE = TN * TKB;
+    static constexpr int A_STAGE = TM * TKB, B_STAGE = (PAIR ? TN / 2 : TN) * TKB;
+    static constexpr int TILE_M = PAIR ? 2 * TM : TM;  // rows of output per (cluster) tile
     static constexpr size_t SMEM = 1024 + (size_t)STAGES * (A_STAGE + B_STAGE) + 256 + (size_t)EPI * TN * 4;
 };
 constexpr int EXP_NONFINITE = 0x7fff;
@@ -67,8 +71,30 @@ struct Params {
     // no host-to-device copy); MAX_SEGS / MAX_GROUPS keep the block under 32 KB.
     Seg segs[640];
     Group groups[640];
+    // grouped mode: per-problem descriptors in device memory, tiles numbered problem by problem
+    const struct GProb* gprobs;
+    int32_t nprob, total_tiles;
 };
 constexpr int MAX_SEGS = 640, MAX_GROUPS = 640;
+
+// One problem of a grouped launch: its planes' tensor maps, pads, output and scales.  A
+// segment whose kb1 is negative runs to the problem's own end of K (nkb stages).
+struct alignas(64) GProb {
+    CUtensorMap tmA, tmB;
+    int64_t m, n, ldc;
+    double* C;
+    const int32_t* row_exp;
+    const int32_t* col_exp;
+    double alpha, beta;
+    int32_t m_pad, n_pad, nkb, tiles_m, tiles_n, tile_begin;
+};
+
+// The tile a role works on: its coordinates and, in grouped mode, its problem descriptor
+// (fields are read through the kernel's accessors, so nothing is copied into registers).
+struct TileCtx {
+    const GProb* gp;
+    int32_t tm, tn;
+};
 
 // ---- small PTX wrappers --------------------------------------------------------------------
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -116,6 +142,64 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int32_t x, int32_t y,
+                                                 uint32_t leader_bar) {
+    // both CTAs of the pair load into their own shared memory; bytes complete on the
+    // leader's barrier (no multicast)
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3}], [%4];\n" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(leader_bar)
+        : "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+    return r;
+}
+
+// Address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t addr, uint32_t rank) {
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(out) : "r"(addr), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];\n" ::"r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// Commit of the pair's MMAs, arriving on the barrier at the same offset in every CTA of mask.
+__device__ __forceinline__ void tc_commit_pair(uint32_t bar, uint16_t mask) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n" ::"r"(
+                     bar),
+                 "h"(mask)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                              uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
 
@@ -159,6 +243,12 @@ __device__ __forceinline__ uint64_t smem_desc_k(uint32_t addr) {
 // Instruction descriptor: kind::i8, D = S32, A = B = signed 8-bit, both K-major, M=128, N=256.
 constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
                               ((uint32_t)(TM >> 4) << 24);
+
+// The pair's M=256 forms of both descriptors.
+constexpr uint32_t IDESC_I8_PAIR = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                                   ((uint32_t)((2 * TM) >> 4) << 24);
+constexpr uint32_t IDESC_BF16_PAIR = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                                     ((uint32_t)((2 * TM) >> 4) << 24);
 
 // Instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major, M=128, N=256.
 constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
@@ -208,12 +298,18 @@ __device__ __forceinline__ int exponent_of_max(unsigned long long bits) {
 // KIND: 0 = INT8 digits (kind::i8, INT32 accumulator), 1 = BF16 operands (kind::f16, FP32
 // accumulator).  EPI: 0 = FP64 fold C = beta*C + alpha*sum_g 2^(e_i+f_j-7d_g) P_g,
 // 1 = FP32 output C = alpha*acc + beta*C (a single flush group).
-template <class CF, int KIND, int EPI_MODE>
+template <class CF, int KIND, int EPI_MODE, bool GROUPED = false>
 __global__ void __launch_bounds__(CF::THREADS, 1)
     digit_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                const __grid_constant__ Params P) {
     constexpr int STAGES = CF::STAGES, TKB = CF::TKB, A_STAGE = CF::A_STAGE, B_STAGE = CF::B_STAGE;
     constexpr int EPI = CF::EPI;
+    constexpr bool PAIR = CF::PAIR;
+    constexpr int TILE_M = CF::TILE_M;
+    const uint32_t crank = PAIR ? cluster_rank() : 0;  // 0 = leader (issues the MMAs)
+    const bool leader = crank == 0;
+    const int unit = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;  // cluster (or CTA) index
+    const int units = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
     const Seg* SEGS = P.segs_ext ? P.segs_ext : P.segs;
     const Group* GROUPS = P.groups_ext ? P.groups_ext : P.groups;
     extern __shared__ uint8_t smem_raw[];
@@ -240,61 +336,105 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(accf(b), 1);
-            mbar_init(acce(b), EPI);
+            mbar_init(acce(b), PAIR ? 2 * EPI : EPI);  // the leader's counts both CTAs' epilogue warps
         }
         mbar_init(done_bar, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(su32(tmem_slot)),
-                     "r"(TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+        if constexpr (PAIR) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                             su32(tmem_slot)),
+                         "r"(TMEM_COLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                             su32(tmem_slot)),
+                         "r"(TMEM_COLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+        }
     }
     tc_fence_before();
     __syncthreads();
+    if constexpr (PAIR) cluster_sync();  // both CTAs' barriers and TMEM exist before any cross-CTA traffic
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
 
-    const int total_tiles = P.tiles_m * P.tiles_n;
-    auto tile_coords = [&](int tile, int& tm, int& tn) {
-        int in_group = GROUP_M * P.tiles_n;
+    const int total_tiles = GROUPED ? P.total_tiles : P.tiles_m * P.tiles_n;
+    auto raster = [](int tile, int tiles_m, int tiles_n) -> int2 {
+        int in_group = GROUP_M * tiles_n;
         int grp = tile / in_group;
         int first_m = grp * GROUP_M;
-        int gsize = min(P.tiles_m - first_m, GROUP_M);
-        tm = first_m + (tile % in_group) % gsize;
-        tn = (tile % in_group) / gsize;
+        int gsize = min(tiles_m - first_m, GROUP_M);
+        return make_int2(first_m + (tile % in_group) % gsize, (tile % in_group) / gsize);
     };
-
+    auto ctx_of = [&](int tile) -> TileCtx {
+        TileCtx c;
+        if constexpr (GROUPED) {
+            int lo = 0, hi = P.nprob - 1;  // last problem whose first tile is <= tile
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (P.gprobs[mid].tile_begin <= tile)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            c.gp = P.gprobs + lo;
+            const int2 t = raster(tile - c.gp->tile_begin, c.gp->tiles_m, c.gp->tiles_n);
+            c.tm = t.x;
+            c.tn = t.y;
+        } else {
+            c.gp = nullptr;
+            const int2 t = raster(tile, P.tiles_m, P.tiles_n);
+            c.tm = t.x;
+            c.tn = t.y;
+        }
+        return c;
+    };
+#define DGT_TILE_FIELD(cx, grouped_expr, single_expr) (GROUPED ? (cx).gp->grouped_expr : P.single_expr)
     if (warp == 0) {
         // ---------------- TMA producer ----------------
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
-                int tm, tn;
-                tile_coords(tile, tm, tn);
+            for (int tile = unit; tile < total_tiles && ok; tile += units) {
+                const TileCtx cx = ctx_of(tile);
+                const int tm = cx.tm, tn = cx.tn;
+                const CUtensorMap* tA = GROUPED ? &cx.gp->tmA : &tmA;
+                const CUtensorMap* tB = GROUPED ? &cx.gp->tmB : &tmB;
+                const int m_pad = DGT_TILE_FIELD(cx, m_pad, m_pad), n_pad = DGT_TILE_FIELD(cx, n_pad, n_pad);
                 for (int g = 0; g < P.ngroups && ok; ++g) {
                     const Group G = GROUPS[g];
                     for (int si = G.seg0; si < G.seg1 && ok; ++si) {
                         const Seg sg = SEGS[si];
-                        for (int kb = sg.kb0; kb < sg.kb1; ++kb) {
+                        const int kb1 = sg.kb1 < 0 ? DGT_TILE_FIELD(cx, nkb, ngroups) : sg.kb1;
+                        for (int kb = sg.kb0; kb < kb1; ++kb) {
                             const int s = it % STAGES;
                             const uint32_t ph = (it / STAGES) & 1;
                             if (!mbar_wait(empty(s), ph ^ 1, abort_flag, P.err)) {
                                 ok = false;
                                 break;
                             }
-                            mbar_expect_tx(full(s), A_STAGE + B_STAGE);
-                            tma_load_2d(su32(sA + s * A_STAGE), &tmA, kb * TKB, sg.a * P.m_pad + tm * TM, full(s));
-                            tma_load_2d(su32(sB + s * B_STAGE), &tmB, kb * TKB, sg.b * P.n_pad + tn * TN, full(s));
+                            if constexpr (PAIR) {
+                                const uint32_t lbar = map_to_rank(full(s), 0);
+                                if (leader) mbar_expect_tx(full(s), 2 * (A_STAGE + B_STAGE));
+                                tma_load_2d_pair(su32(sA + s * A_STAGE), tA, kb * TKB,
+                                                 sg.a * m_pad + tm * TILE_M + (int)crank * TM, lbar);
+                                tma_load_2d_pair(su32(sB + s * B_STAGE), tB, kb * TKB,
+                                                 sg.b * n_pad + tn * TN + (int)crank * (TN / 2), lbar);
+                            } else {
+                                mbar_expect_tx(full(s), A_STAGE + B_STAGE);
+                                tma_load_2d(su32(sA + s * A_STAGE), tA, kb * TKB, sg.a * m_pad + tm * TM, full(s));
+                                tma_load_2d(su32(sB + s * B_STAGE), tB, kb * TKB, sg.b * n_pad + tn * TN, full(s));
+                            }
                             ++it;
                         }
                     }
                 }
             }
             // drain: wait for this CTA's own loads still in flight (bounded)
-            if (!ok) {
+            if (!ok && leader) {
                 for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
                     long long t0 = clock64();
                     while (!mbar_try(full(j % STAGES), (j / STAGES) & 1) && clock64() - t0 < WAIT_BUDGET) {
@@ -303,11 +443,12 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
             }
         }
     } else if (warp == 1) {
-        // ---------------- MMA issuer ----------------
-        if (lane == 0) {
+        // ---------------- MMA issuer (the pair's leader only) ----------------
+        if (lane == 0 && leader) {
             uint32_t it = 0, gcount = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+            for (int tile = unit; tile < total_tiles && ok; tile += units) {
+                const TileCtx cx = ctx_of(tile);
                 for (int g = 0; g < P.ngroups && ok; ++g, ++gcount) {
                     const Group G = GROUPS[g];
                     const int b = gcount & 1;
@@ -321,7 +462,8 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                     uint32_t acc = 0;
                     for (int si = G.seg0; si < G.seg1 && ok; ++si) {
                         const Seg sg = SEGS[si];
-                        for (int kb = sg.kb0; kb < sg.kb1; ++kb) {
+                        const int kb1 = sg.kb1 < 0 ? DGT_TILE_FIELD(cx, nkb, ngroups) : sg.kb1;
+                        for (int kb = sg.kb0; kb < kb1; ++kb) {
                             const int s = it % STAGES;
                             const uint32_t ph = (it / STAGES) & 1;
                             if (!mbar_wait(full(s), ph, abort_flag, P.err)) {
@@ -333,22 +475,41 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                             const uint64_t bd = smem_desc_k<TKB>(su32(sB + s * B_STAGE));
 #pragma unroll
                             for (int kk = 0; kk < TKB / 32; ++kk) {
-                                // advance 32 bytes (one K=32 step) inside the 128-byte swizzle atom
-                                if constexpr (KIND == 0)
-                                    mma_i8(d_tmem, ad + (uint64_t)(kk * 2), bd + (uint64_t)(kk * 2), IDESC_I8, acc);
-                                else
-                                    mma_bf16(d_tmem, ad + (uint64_t)(kk * 2), bd + (uint64_t)(kk * 2), IDESC_BF16, acc);
+                                // advance 32 bytes (one K=32 step) inside the swizzle atom
+                                const uint64_t a_k = ad + (uint64_t)(kk * 2), b_k = bd + (uint64_t)(kk * 2);
+                                if constexpr (PAIR) {
+                                    if constexpr (KIND == 0)
+                                        mma_i8_pair(d_tmem, a_k, b_k, IDESC_I8_PAIR, acc);
+                                    else
+                                        mma_bf16_pair(d_tmem, a_k, b_k, IDESC_BF16_PAIR, acc);
+                                } else {
+                                    if constexpr (KIND == 0)
+                                        mma_i8(d_tmem, a_k, b_k, IDESC_I8, acc);
+                                    else
+                                        mma_bf16(d_tmem, a_k, b_k, IDESC_BF16, acc);
+                                }
                                 acc = 1;
                             }
-                            tc_commit(empty(s));
+                            if constexpr (PAIR)
+                                tc_commit_pair(empty(s), 0x3);  // frees the stage in both CTAs
+                            else
+                                tc_commit(empty(s));
                             ++it;
                         }
                     }
-                    if (ok) tc_commit(accf(b));
+                    if (ok) {
+                        if constexpr (PAIR)
+                            tc_commit_pair(accf(b), 0x3);  // both CTAs' epilogues may read their rows
+                        else
+                            tc_commit(accf(b));
+                    }
                 }
             }
             // every MMA this CTA issued has completed once done_bar flips
-            tc_commit(done_bar);
+            if constexpr (PAIR)
+                tc_commit_pair(done_bar, 0x1);
+            else
+                tc_commit(done_bar);
             long long t0 = clock64();
             while (!mbar_try(done_bar, 0) && clock64() - t0 < WAIT_BUDGET) {
             }
@@ -361,19 +522,20 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
         int32_t* col_exp_s = col_exp_all + (warp - 2) * TN;
         uint32_t gcount = 0;
         bool ok = true;
-        for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
-            int tm, tn;
-            tile_coords(tile, tm, tn);
-            const int64_t row = (int64_t)tm * TM + r_in;
+        for (int tile = unit; tile < total_tiles && ok; tile += units) {
+            const TileCtx cx = ctx_of(tile);
+            const int tm = cx.tm, tn = cx.tn;
+            const int64_t row = (int64_t)tm * TILE_M + (int64_t)crank * TM + r_in;
             const int64_t n0 = (int64_t)tn * TN;
             // each epilogue warp keeps its own copy of the tile's column exponents, so warps
             // never wait on one another (a warp that aborts cannot strand the others)
             __syncwarp();
             if constexpr (EPI_MODE == 0)
-                for (int c = lane; c < TN; c += 32) col_exp_s[c] = (n0 + c < P.n) ? P.col_exp[n0 + c] : 0;
+                for (int c = lane; c < TN; c += 32)
+                    col_exp_s[c] = (n0 + c < DGT_TILE_FIELD(cx, n, n)) ? DGT_TILE_FIELD(cx, col_exp, col_exp)[n0 + c] : 0;
             __syncwarp();
-            const bool row_ok = row < P.m;
-            const int e_row = (EPI_MODE == 0 && row_ok) ? P.row_exp[row] : 0;
+            const bool row_ok = row < DGT_TILE_FIELD(cx, m, m);
+            const int e_row = (EPI_MODE == 0 && row_ok) ? DGT_TILE_FIELD(cx, row_exp, row_exp)[row] : 0;
             for (int g = 0; g < P.ngroups; ++g, ++gcount) {
                 const int b = gcount & 1;
                 const uint32_t u = gcount >> 1;
@@ -390,7 +552,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                     uint32_t v[32];
                     tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TN + ch * 32), v);
                     if (!row_ok) continue;
-                    const int64_t rem_cols = P.n - (n0 + ch * 32);
+                    const int64_t rem_cols = DGT_TILE_FIELD(cx, n, n) - (n0 + ch * 32);
                     const int ncols = rem_cols < 32 ? (int)rem_cols : 32;
                     if constexpr (EPI_MODE == 1) {
                         float* fbase = P.Cf + row + (n0 + ch * 32) * P.ldc;
@@ -411,15 +573,21 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                         continue;
                     }
                     double prev[32];
-                    double* cbase = P.C + row + (n0 + ch * 32) * P.ldc;
+                    // ldc, alpha and beta are read at each use, not held in locals: as kernel
+                    // parameters they are free operands, while locals made the compiler keep 32
+                    // precomputed column addresses live (about 50 more registers, and spills)
+#define ldc DGT_TILE_FIELD(cx, ldc, ldc)
+#define alpha DGT_TILE_FIELD(cx, alpha, alpha)
+#define beta DGT_TILE_FIELD(cx, beta, beta)
+                    double* cbase = DGT_TILE_FIELD(cx, C, C) + row + (n0 + ch * 32) * ldc;
 #pragma unroll
                     for (int c = 0; c < 32; ++c) {
                         prev[c] = 0.0;
                         if (c < ncols) {
                             if (g > 0)
-                                prev[c] = cbase[c * P.ldc];
-                            else if (P.beta != 0.0)
-                                prev[c] = P.beta * cbase[c * P.ldc];
+                                prev[c] = cbase[c * ldc];
+                            else if (beta != 0.0)
+                                prev[c] = beta * cbase[c * ldc];
                         }
                     }
 #pragma unroll
@@ -433,23 +601,36 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                                 t = __longlong_as_double(0x7ff8000000000000ll);
                             else
                                 t = scale2(acc_v, e_row + ec - 7 * d);
-                            cbase[c * P.ldc] = fma(P.alpha, t, prev[c]);
+                            cbase[c * ldc] = fma(alpha, t, prev[c]);
                         }
                     }
+#undef ldc
+#undef alpha
+#undef beta
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(acce(b));
+                if (lane == 0) {
+                    if constexpr (PAIR)
+                        mbar_arrive_cluster(map_to_rank(acce(b), 0));
+                    else
+                        mbar_arrive(acce(b));
+                }
             }
         }
     }
 
     tc_fence_before();
     __syncthreads();
+    if constexpr (PAIR) cluster_sync();  // the leader's MMAs into this CTA's TMEM / smem are done
     tc_fence_after();
     if (warp == 1) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(TMEM_COLS));
+        if constexpr (PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(TMEM_COLS));
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem_base), "r"(TMEM_COLS));
     }
+#undef DGT_TILE_FIELD
 }
 
 

@@ -127,3 +127,67 @@ def test_grouped_ragged_products(h):
     h.check_device()
     for d, (_, _, dC, want) in zip(descs, keep):
         assert O.rel_errors(host(dC, (d["m"], d["n"])), want)[1] <= FRO_TOL
+
+
+def test_summa_emulated(h):
+    """SUMMA with every panel step as an INT8 Ozaki GEMM (8 slices)."""
+    import torch
+
+    M, N, K, b, p, q = 257, 131, 199, 32, 2, 3
+    A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
+    o = O.orc()
+
+    def pack(X, rows, cols):
+        shapes = o.pblas_shapes(rows, cols, b, b, p, q)
+        locs = [torch.zeros((max(c, 1), max(r, 1)), dtype=torch.float64, device="cuda") for r, c, _ in shapes]
+        lld = [max(r, 1) for r, _, _ in shapes]
+        dX = dev(X)
+        h.pack_block_cyclic(rows, cols, b, b, p, q, ptr(dX), rows, [ptr(l) for l in locs], lld)
+        return dX, locs, lld
+
+    _, lA, lldA = pack(A, M, K)
+    _, lB, lldB = pack(B, K, N)
+    dC, lC, lldC = pack(C, M, N)
+    h.summa(p, q, b, b, b, M, N, K, 1.5, [ptr(x) for x in lA], lldA, [ptr(x) for x in lB], lldB, -0.5,
+            [ptr(x) for x in lC], lldC, mode=dgt.FP64_OZAKI_INT8, slices=8)
+    h.unpack_block_cyclic(M, N, b, b, p, q, ptr(dC), M, [ptr(x) for x in lC], lldC)
+    torch.cuda.synchronize()
+    h.check_device()
+    assert O.rel_errors(host(dC, (M, N)), O.dgemm(A, B, 1.5, -0.5, C))[1] <= FRO_TOL
+
+
+@pytest.mark.parametrize("M,p,c", [(512, 4, 2), (384, 3, 1)])
+def test_cannon_emulated(h, M, p, c):
+    import torch
+
+    A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), O.uniform((M, M), 3)
+    dA, dB, dC = dev(A), dev(B), dev(C)
+    lm = M // p
+    tiles = lambda: [torch.zeros((lm, lm), dtype=torch.float64, device="cuda") for _ in range(p * p)]
+    tA, tB, tC = tiles(), tiles(), tiles()
+    h.pack_cannon2d(M, p, ptr(dA), ptr(dB), ptr(dC), [ptr(x) for x in tA], [ptr(x) for x in tB],
+                    [ptr(x) for x in tC])
+    h.cannon25d(M, p, c, 1.0, [ptr(x) for x in tA], [ptr(x) for x in tB], 0.5, [ptr(x) for x in tC],
+                mode=dgt.FP64_OZAKI_INT8, slices=8)
+    h.unpack_cannon2d(M, p, ptr(dC), [ptr(x) for x in tC])
+    torch.cuda.synchronize()
+    h.check_device()
+    assert O.rel_errors(host(dC, (M, M)), O.dgemm(A, B, 1.0, 0.5, C))[1] <= FRO_TOL
+
+
+def test_grouped_emulated(h):
+    import torch
+
+    rng = np.random.default_rng(9)
+    descs, keep = [], []
+    for i in range(12):
+        m, n, k = (int(x) for x in rng.integers(1, 400, 3))
+        A, B, C = O.uniform((m, k), 500 + i), O.uniform((k, n), 600 + i), O.uniform((m, n), 700 + i)
+        dA, dB, dC = dev(A), dev(B), dev(C)
+        descs.append(dict(m=m, n=n, k=k, alpha=1.0, beta=-1.0, A=ptr(dA), lda=m, B=ptr(dB), ldb=k, C=ptr(dC), ldc=m))
+        keep.append((dA, dB, dC, O.dgemm(A, B, 1.0, -1.0, C)))
+    h.dgemm_grouped(descs, mode=dgt.FP64_OZAKI_INT8, slices=8)
+    torch.cuda.synchronize()
+    h.check_device()
+    for d, (_, _, dC, want) in zip(descs, keep):
+        assert O.rel_errors(host(dC, (d["m"], d["n"])), want)[1] <= FRO_TOL
