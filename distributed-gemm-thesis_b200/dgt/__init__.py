@@ -91,6 +91,8 @@ SIGNATURES = [
     ("dgt_probe_peak", _c_i32, [_vp, _c_i32, _dp]),
     ("dgt_last_timings", _c_i32, [_vp, ctypes.POINTER(ctypes.c_float), _c_i32]),
     ("dgt_launch_count", _c_i64, [_vp]),
+    ("dgt_dgemm_ozaki_static", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _dp, _vp, _c_i64,
+                                         _vp, _c_i64, _dp, _vp, _c_i64, _c_i32]),
 ]
 
 _lib = None
