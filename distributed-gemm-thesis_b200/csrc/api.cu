@@ -68,32 +68,52 @@ static bool cannon_order(int p, int c, int i, int j, int k, int* out) {
     return covers;
 }
 
-// Emulated-FP64 execution of a step schedule: every segment of a problem is one Ozaki GEMM
-// (the reference issues one cublasDgemm per step too); the first applies the problem's beta,
-// the rest accumulate.  Each call splits its own operands, so every step is scaled on its
-// own panel -- the same numerics as a per-step local GEMM.
+// Emulated-FP64 execution of a step schedule.  Step t of every product is its t-th
+// segment with K > 0 (the reference issues one cublasDgemm per step too); the first step
+// applies the product's beta, later steps accumulate.  Each step splits its own operands,
+// so every step is scaled on its own panel -- the numerics of a per-step local GEMM.  With
+// INT8 slices all products' step t run as one grouped Ozaki pass (the products of one step
+// write distinct C); a step the grouped form does not support runs product by product.
 dgt_status run_problems_emulated(dgt_context* h, const std::vector<Problem>& probs,
-                                        const std::vector<KSegment>& segs, dgt_fp64_mode mode, int slices) {
+                                 const std::vector<KSegment>& segs, dgt_fp64_mode mode, int slices) {
     if (slices < 2 || slices > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
-    for (const Problem& pr : probs) {
+    std::vector<std::vector<const KSegment*>> steps(probs.size());
+    size_t max_steps = 0;
+    for (size_t i = 0; i < probs.size(); ++i) {
+        const Problem& pr = probs[i];
         if (pr.m <= 0 || pr.n <= 0) continue;
-        bool first = true;
-        for (int s = 0; s < pr.seg_count; ++s) {
-            const KSegment& sg = segs[pr.seg_begin + s];
-            if (sg.k <= 0) continue;
-            const double beta = first ? pr.beta : 1.0;
-            dgt_status st = ozaki_dgemm(h, pr.transa != 0, pr.transb != 0, pr.m, pr.n, sg.k, pr.alpha, sg.A, sg.lda,
-                                        sg.B, sg.ldb, beta, pr.C, pr.ldc, mode, slices);
-            if (st != DGT_SUCCESS) return st;
-            first = false;
-        }
-        if (first && pr.beta != 1.0) {  // no K at all: C = beta * C through the native kernel
+        for (int s = 0; s < pr.seg_count; ++s)
+            if (segs[pr.seg_begin + s].k > 0) steps[i].push_back(&segs[pr.seg_begin + s]);
+        max_steps = std::max(max_steps, steps[i].size());
+        if (steps[i].empty() && pr.beta != 1.0) {  // no K at all: C = beta * C through the native kernel
             std::vector<Problem> one{pr};
             one[0].alpha = 0.0;
             one[0].seg_begin = 0;
             one[0].seg_count = 1;
             std::vector<KSegment> none{KSegment{nullptr, nullptr, 1, 1, 0}};
             dgt_status st = launch_dmma_grouped(h, one, none);
+            if (st != DGT_SUCCESS) return st;
+        }
+    }
+    for (size_t t = 0; t < max_steps; ++t) {
+        std::vector<OzProblem> batch;
+        for (size_t i = 0; i < probs.size(); ++i) {
+            if (t >= steps[i].size()) continue;
+            const Problem& pr = probs[i];
+            const KSegment& sg = *steps[i][t];
+            batch.push_back(OzProblem{pr.transa != 0, pr.transb != 0, pr.m, pr.n, sg.k, pr.alpha,
+                                      t == 0 ? pr.beta : 1.0, sg.A, sg.lda, sg.B, sg.ldb, pr.C, pr.ldc});
+        }
+        if (mode == DGT_FP64_OZAKI_INT8) {
+            dgt_status st = ozaki_dgemm_grouped(h, batch, slices);
+            if (st != DGT_ERROR_UNSUPPORTED) {
+                if (st != DGT_SUCCESS) return st;
+                continue;
+            }
+        }
+        for (const OzProblem& b : batch) {
+            dgt_status st = ozaki_dgemm(h, b.ta, b.tb, b.m, b.n, b.k, b.alpha, b.A, b.lda, b.B, b.ldb, b.beta, b.C,
+                                        b.ldc, mode, slices);
             if (st != DGT_SUCCESS) return st;
         }
     }
@@ -145,6 +165,7 @@ dgt_status dgt_destroy(dgt_handle_t h) {
     for (void* w : h->ws)
         if (w) cudaFree(w);
     if (h->table) cudaFree(h->table);
+    if (h->oz_table) cudaFree(h->oz_table);
     if (h->dev_error) cudaFree(h->dev_error);
     delete h;
     return DGT_SUCCESS;

@@ -56,6 +56,9 @@ struct dgt_context {
     void* table = nullptr;  // grouped-GEMM problem table (dgemm_dmma.cu)
     size_t table_bytes = 0;
     uint64_t table_hash = 0;
+    void* oz_table = nullptr;  // grouped Ozaki tables: problems + pre-pass jobs (ozaki.cu)
+    size_t oz_table_bytes = 0;
+    uint64_t oz_table_hash = 0;
 };
 
 namespace dgt {
@@ -145,5 +148,23 @@ dgt_status ozaki_dgemm_on(cudaStream_t s, int num_sms, unsigned int* err, void* 
 dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
                        const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
                        dgt_fp64_mode mode, int slices);
+
+// One product of a grouped Ozaki launch (all sizes > 0; validation is the caller's job).
+struct OzProblem {
+    bool ta, tb;
+    int64_t m, n, k;
+    double alpha, beta;
+    const double* A;
+    int64_t lda;
+    const double* B;
+    int64_t ldb;
+    double* C;
+    int64_t ldc;
+};
+// All products in one INT8 Ozaki pass: one amax launch, one split launch, one persistent
+// digit-GEMM launch over every product's tiles.  Returns DGT_ERROR_UNSUPPORTED (with no
+// work issued) when a product's K is too long for whole-K exact INT32 digit products; the
+// caller then runs the products one by one.
+dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& probs, int slices);
 
 }  // namespace dgt

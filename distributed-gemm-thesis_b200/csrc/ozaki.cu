@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "dgt_internal.cuh"
@@ -37,12 +38,14 @@
 namespace dgt {
 namespace oz {
 
-// MN-contiguous operand: element (mn, kk) at X[mn + kk*ld]; one thread per mn, K split over y.
-__global__ void amax_mn_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K, int kchunk,
-                               unsigned long long* __restrict__ amax) {
-    int64_t mn = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// MN-contiguous operand: element (mn, kk) at X[mn + kk*ld]; one thread per mn, K split over
+// blocks (bx covers 256 mn, by a chunk of K).
+__device__ __forceinline__ void amax_mn_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                              int kchunk, unsigned long long* __restrict__ amax, int64_t bx,
+                                              int64_t by) {
+    int64_t mn = bx * blockDim.x + threadIdx.x;
     if (mn >= MN) return;
-    int64_t k0 = (int64_t)blockIdx.y * kchunk, k1 = min(K, k0 + kchunk);
+    int64_t k0 = by * kchunk, k1 = min(K, k0 + kchunk);
     unsigned long long mx = 0;
     for (int64_t kk = k0; kk < k1; ++kk) {
         unsigned long long b = (unsigned long long)__double_as_longlong(X[mn + kk * ld]) & 0x7fffffffffffffffull;
@@ -51,10 +54,15 @@ __global__ void amax_mn_contig(const double* __restrict__ X, int64_t ld, int64_t
     if (mx) atomicMax(amax + mn, mx);
 }
 
+__global__ void amax_mn_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K, int kchunk,
+                               unsigned long long* __restrict__ amax) {
+    amax_mn_block(X, ld, MN, K, kchunk, amax, blockIdx.x, blockIdx.y);
+}
+
 // K-contiguous operand: element (mn, kk) at X[kk + mn*ld]; one warp per mn.
-__global__ void amax_k_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                              unsigned long long* __restrict__ amax) {
-    int64_t mn = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+__device__ __forceinline__ void amax_k_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                             unsigned long long* __restrict__ amax, int64_t bx) {
+    int64_t mn = bx * (blockDim.x / 32) + threadIdx.x / 32;
     int lane = threadIdx.x & 31;
     if (mn >= MN) return;
     const double* row = X + mn * ld;
@@ -71,24 +79,29 @@ __global__ void amax_k_contig(const double* __restrict__ X, int64_t ld, int64_t 
     if (lane == 0) amax[mn] = mx;
 }
 
+__global__ void amax_k_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                              unsigned long long* __restrict__ amax) {
+    amax_k_block(X, ld, MN, K, amax, blockIdx.x);
+}
+
 // Digit planes: plane s holds digit s+1 of every element as int8 at [s][mn][kk] (K-major,
 // row length k_pad, mn_pad rows); padding rows/columns are written as 0.  Each thread
-// produces 32 consecutive kk of one mn.  Thread (mn) also writes exps[mn] once.
-// BF16OUT stores each digit as a BF16 value instead (exact: |digit| <= 127 < 2^8), two
-// bytes per element.
+// produces 32 consecutive kk of one mn (block bx covers 128 mn, by 32 of K).  The by == 0
+// blocks also write exps[mn].  BF16OUT stores each digit as a BF16 value instead (exact:
+// |digit| <= 127 < 2^8), two bytes per element.
 template <bool K_CONTIG, bool BF16OUT>
-__global__ void __launch_bounds__(128) split_digits(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                                                    int64_t mn_pad, int64_t k_pad, int S,
-                                                    const unsigned long long* __restrict__ amax,
-                                                    int32_t* __restrict__ exps, void* __restrict__ planes_v) {
-    const int64_t mn = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t k0 = (int64_t)blockIdx.y * 32;
+__device__ __forceinline__ void split_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                            int64_t mn_pad, int64_t k_pad, int S,
+                                            const unsigned long long* __restrict__ amax, int32_t* __restrict__ exps,
+                                            void* __restrict__ planes_v, int64_t bx, int64_t by) {
+    const int64_t mn = bx * blockDim.x + threadIdx.x;
+    const int64_t k0 = by * 32;
     if (mn >= mn_pad) return;
     double v[32];
     int e = 0;
     if (mn < MN) {
         e = exponent_of_max(amax[mn]);
-        if (blockIdx.y == 0) exps[mn] = e;
+        if (by == 0) exps[mn] = e;
     }
     const bool live = (mn < MN) && (e != EXP_NONFINITE);
 #pragma unroll
@@ -130,6 +143,66 @@ __global__ void __launch_bounds__(128) split_digits(const double* __restrict__ X
             for (int q = 0; q < 4; ++q) o4[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
         }
     }
+}
+
+template <bool K_CONTIG, bool BF16OUT>
+__global__ void __launch_bounds__(128) split_digits(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                                    int64_t mn_pad, int64_t k_pad, int S,
+                                                    const unsigned long long* __restrict__ amax,
+                                                    int32_t* __restrict__ exps, void* __restrict__ planes_v) {
+    split_block<K_CONTIG, BF16OUT>(X, ld, MN, K, mn_pad, k_pad, S, amax, exps, planes_v, blockIdx.x, blockIdx.y);
+}
+
+// ---- grouped pre-pass: one launch scales (or splits) every operand of a grouped call -------
+// Each operand is a job; a job owns a contiguous range of the launch's blocks, found by
+// binary search on the jobs' first block.
+struct SplitJob {
+    const double* X;
+    int64_t ld, MN, K, mn_pad, k_pad;
+    unsigned long long* amax;
+    int32_t* exps;
+    void* planes;
+    int32_t kcontig;
+    int32_t amax_bx;        // amax blocks along mn (MN-contiguous jobs: times amax_by along K)
+    int32_t amax_by;
+    int32_t split_bx;       // split blocks along mn (times k_pad / 32 along K)
+    int64_t amax_begin;     // first block of this job in the amax launch
+    int64_t split_begin;    // first block of this job in the split launch
+};
+constexpr int AMAX_KCHUNK = 512;
+
+__device__ __forceinline__ int find_job(const SplitJob* __restrict__ jobs, int njobs, int64_t blk, bool split) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int64_t b0 = split ? jobs[mid].split_begin : jobs[mid].amax_begin;
+        if (b0 <= blk)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) amax_grouped(const SplitJob* __restrict__ jobs, int njobs) {
+    const int64_t blk = blockIdx.x;
+    const SplitJob& J = jobs[find_job(jobs, njobs, blk, false)];
+    const int64_t local = blk - J.amax_begin;
+    if (J.kcontig)
+        amax_k_block(J.X, J.ld, J.MN, J.K, J.amax, local);
+    else
+        amax_mn_block(J.X, J.ld, J.MN, J.K, AMAX_KCHUNK, J.amax, local % J.amax_bx, local / J.amax_bx);
+}
+
+__global__ void __launch_bounds__(128) split_grouped(const SplitJob* __restrict__ jobs, int njobs, int S) {
+    const int64_t blk = blockIdx.x;
+    const SplitJob& J = jobs[find_job(jobs, njobs, blk, true)];
+    const int64_t local = blk - J.split_begin;
+    const int64_t bx = local % J.split_bx, by = local / J.split_bx;
+    if (J.kcontig)
+        split_block<true, false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, S, J.amax, J.exps, J.planes, bx, by);
+    else
+        split_block<false, false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, S, J.amax, J.exps, J.planes, bx, by);
 }
 
 // ---- the INT8 tcgen05 GEMM ---------------------------------------------------------------------
@@ -400,6 +473,219 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
     if (st != DGT_SUCCESS) return st;
     return ozaki_run(h, h->stream, h->num_sms, h->dev_error, ws, L, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C,
                      ldc, S);
+}
+
+
+// ---- grouped: every product of a batch in one pre-pass and one persistent GEMM launch ----------
+
+template <class CF>
+static cudaError_t launch_ozaki_grouped(const oz::Params& prm, int grid, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(oz::digit_gemm<CF, 0, 0, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    static const CUtensorMap unused = {};  // grouped mode reads each problem's maps from its table
+    oz::digit_gemm<CF, 0, 0, true><<<grid, CF::THREADS, CF::SMEM, s>>>(unused, unused, prm);
+    return cudaGetLastError();
+}
+
+dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& probs, int S) {
+    const int T = (int)probs.size();
+    if (T == 0) return DGT_SUCCESS;
+    if (S < 2 || S > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+    // variants 0 and 1 (4 or 8 epilogue warps, 128-byte stages); the others run as variant 1
+    const int variant = h->ozaki_variant == 0 ? 0 : 1;
+    const int tkb = 128;
+    auto up = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
+
+    // The flush schedule is built for the longest K: a group that is exact for it is exact for
+    // every shorter K.  Segments run over each product's own K (kb1 = -1).
+    int64_t k_pad_max = 0;
+    for (const OzProblem& p : probs) k_pad_max = std::max(k_pad_max, ceil_div(p.k, oz::KPAD) * oz::KPAD);
+    std::vector<oz::Seg> segs;
+    std::vector<oz::Group> groups;
+    if (!ozaki_schedule(S, k_pad_max, tkb, false, segs, groups) || segs.size() > (size_t)oz::MAX_SEGS ||
+        groups.size() > (size_t)oz::MAX_GROUPS)
+        return DGT_ERROR_UNSUPPORTED;
+    for (oz::Seg& sg : segs) {
+        if (sg.kb0 != 0) return DGT_ERROR_UNSUPPORTED;  // K-chunked diagonals: not in grouped form
+        sg.kb1 = -1;
+    }
+
+    // Tiles are numbered product by product, longest K first, so the persistent CTAs' static
+    // round-robin takes the heaviest tiles early.
+    std::vector<int> order(T);
+    for (int i = 0; i < T; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return probs[a].k > probs[b].k; });
+
+    // scratch: per product planes A | planes B (1 KB aligned), then all amax words, all exponents
+    struct Off {
+        int64_t m_pad, n_pad, k_pad;
+        size_t pa, pb, xa, xb, ea, eb;
+    };
+    std::vector<Off> off(T);
+    size_t planes = 0, amax_words = 0, exp_words = 0;
+    for (int i = 0; i < T; ++i) {
+        const OzProblem& p = probs[i];
+        Off& o = off[i];
+        o.m_pad = ceil_div(p.m, oz::TM) * oz::TM;
+        o.n_pad = ceil_div(p.n, oz::TN) * oz::TN;
+        o.k_pad = ceil_div(p.k, oz::KPAD) * oz::KPAD;
+        if ((int64_t)S * std::max(o.m_pad, o.n_pad) > INT32_MAX) return DGT_ERROR_UNSUPPORTED;
+        o.pa = planes;
+        planes += up((size_t)S * o.m_pad * o.k_pad, 1024);
+        o.pb = planes;
+        planes += up((size_t)S * o.n_pad * o.k_pad, 1024);
+        o.xa = amax_words;
+        amax_words += (size_t)p.m;
+        o.xb = amax_words;
+        amax_words += (size_t)p.n;
+        o.ea = exp_words;
+        exp_words += (size_t)p.m;
+        o.eb = exp_words;
+        exp_words += (size_t)p.n;
+    }
+    const size_t amax_at = planes, exp_at = up(amax_at + amax_words * 8, 256);
+    const size_t total = up(exp_at + exp_words * 4, 256);
+    void* ws = nullptr;
+    dgt_status st = ensure_workspace(h, total, &ws, 0);
+    if (st != DGT_SUCCESS) return st;
+    char* base = (char*)ws;
+    auto* amax = (unsigned long long*)(base + amax_at);
+    auto* exps = (int32_t*)(base + exp_at);
+
+    // host tables: GProb[T] (tensor maps inside, 64-byte aligned) and SplitJob[2T], zeroed
+    // byte for byte so that padding hashes the same on every call
+    const size_t gp_bytes = up((size_t)T * sizeof(oz::GProb), 256);
+    const size_t job_bytes = (size_t)2 * T * sizeof(oz::SplitJob);
+    static thread_local std::vector<oz::GProb> host_gp;
+    static thread_local std::vector<oz::SplitJob> host_jobs;
+    host_gp.resize(T);
+    host_jobs.resize(2 * (size_t)T);
+    std::memset((void*)host_gp.data(), 0, (size_t)T * sizeof(oz::GProb));
+    std::memset((void*)host_jobs.data(), 0, job_bytes);
+    oz::GProb* gp = host_gp.data();
+    oz::SplitJob* jobs = host_jobs.data();
+    int64_t amax_blocks = 0, split_blocks = 0;
+    int32_t tiles = 0;
+    for (int r = 0; r < T; ++r) {
+        const int i = order[r];
+        const OzProblem& p = probs[i];
+        const Off& o = off[i];
+        void* pA = base + o.pa;
+        void* pB = base + o.pb;
+        oz::GProb& g = gp[r];
+        if (!oz::make_plane_map(&g.tmA, pA, (int64_t)S * o.m_pad, o.k_pad, oz::TM, tkb) ||
+            !oz::make_plane_map(&g.tmB, pB, (int64_t)S * o.n_pad, o.k_pad, oz::TN, tkb))
+            return fail(h, DGT_ERROR_CUDA, "cuTensorMapEncodeTiled failed");
+        g.m = p.m;
+        g.n = p.n;
+        g.ldc = p.ldc;
+        g.C = p.C;
+        g.row_exp = exps + o.ea;
+        g.col_exp = exps + o.eb;
+        g.alpha = p.alpha;
+        g.beta = p.beta;
+        g.m_pad = (int32_t)o.m_pad;
+        g.n_pad = (int32_t)o.n_pad;
+        g.nkb = (int32_t)(o.k_pad / tkb);
+        g.tiles_m = (int32_t)(o.m_pad / oz::TM);
+        g.tiles_n = (int32_t)(o.n_pad / oz::TN);
+        g.tile_begin = tiles;
+        tiles += g.tiles_m * g.tiles_n;
+        // op(A) is m x k: 'N' -> MN-contiguous; op(B) as its transpose n x k: 'N' -> K-contiguous
+        const bool kc[2] = {p.ta, !p.tb};
+        const double* X[2] = {p.A, p.B};
+        const int64_t ld[2] = {p.lda, p.ldb}, MN[2] = {p.m, p.n}, pad[2] = {o.m_pad, o.n_pad};
+        const size_t xo[2] = {o.xa, o.xb}, eo[2] = {o.ea, o.eb};
+        void* pl[2] = {pA, pB};
+        for (int t = 0; t < 2; ++t) {
+            oz::SplitJob& J = jobs[2 * r + t];
+            J.X = X[t];
+            J.ld = ld[t];
+            J.MN = MN[t];
+            J.K = p.k;
+            J.mn_pad = pad[t];
+            J.k_pad = o.k_pad;
+            J.amax = amax + xo[t];
+            J.exps = exps + eo[t];
+            J.planes = pl[t];
+            J.kcontig = kc[t] ? 1 : 0;
+            J.amax_bx = (int32_t)(kc[t] ? ceil_div(MN[t], 8) : ceil_div(MN[t], 256));
+            J.amax_by = (int32_t)(kc[t] ? 1 : ceil_div(p.k, oz::AMAX_KCHUNK));
+            J.split_bx = (int32_t)ceil_div(pad[t], 128);
+            J.amax_begin = amax_blocks;
+            J.split_begin = split_blocks;
+            amax_blocks += (int64_t)J.amax_bx * J.amax_by;
+            split_blocks += (int64_t)J.split_bx * (o.k_pad / 32);
+        }
+    }
+    if (amax_blocks > INT32_MAX || split_blocks > INT32_MAX)
+        return fail(h, DGT_ERROR_UNSUPPORTED, "grouped Ozaki batch too large for one launch");
+
+    // device copy of the tables, uploaded only when their content changes (a repeated call,
+    // e.g. from a replayed CUDA graph, needs no copy)
+    uint64_t hash = 1469598103934665603ull;  // FNV-1a over both tables
+    auto mix = [&](const void* p, size_t n) {
+        const unsigned char* b = (const unsigned char*)p;
+        for (size_t i = 0; i < n; ++i) hash = (hash ^ b[i]) * 1099511628211ull;
+    };
+    mix(gp, (size_t)T * sizeof(oz::GProb));
+    mix(jobs, job_bytes);
+    const size_t table_bytes = gp_bytes + job_bytes;
+    if (table_bytes > h->oz_table_bytes) {
+        if (h->oz_table) {
+            DGT_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+            cudaFree(h->oz_table);
+            h->oz_table = nullptr;
+            h->oz_table_bytes = 0;
+        }
+        const size_t want = std::max<size_t>(table_bytes, 1 << 16);
+        cudaError_t e = cudaMalloc(&h->oz_table, want);
+        if (e != cudaSuccess) return cuda_fail(h, e, "grouped Ozaki table");
+        h->oz_table_bytes = want;
+        h->oz_table_hash = 0;
+    }
+    cudaStream_t s = h->stream;
+    if (hash != h->oz_table_hash) {
+        DGT_CUDA_TRY(h, cudaMemcpyAsync(h->oz_table, gp, (size_t)T * sizeof(oz::GProb), cudaMemcpyHostToDevice, s));
+        DGT_CUDA_TRY(h, cudaMemcpyAsync((char*)h->oz_table + gp_bytes, jobs, job_bytes, cudaMemcpyHostToDevice, s));
+        h->oz_table_hash = hash;
+    }
+    const auto* d_gp = (const oz::GProb*)h->oz_table;
+    const auto* d_jobs = (const oz::SplitJob*)((char*)h->oz_table + gp_bytes);
+
+    mark(h, 0);
+    DGT_CUDA_TRY(h, cudaMemsetAsync(amax, 0, amax_words * 8, s));
+    oz::amax_grouped<<<(unsigned)amax_blocks, 256, 0, s>>>(d_jobs, 2 * T);
+    h->launches.fetch_add(1);
+    DGT_CUDA_TRY(h, cudaGetLastError());
+    oz::split_grouped<<<(unsigned)split_blocks, 128, 0, s>>>(d_jobs, 2 * T, S);
+    h->launches.fetch_add(1);
+    DGT_CUDA_TRY(h, cudaGetLastError());
+
+    static thread_local oz::Params prm;
+    prm = oz::Params{};
+    prm.ngroups = (int32_t)groups.size();
+    std::copy(segs.begin(), segs.end(), prm.segs);
+    std::copy(groups.begin(), groups.end(), prm.groups);
+    prm.segs_ext = nullptr;
+    prm.groups_ext = nullptr;
+    prm.err = h->dev_error;
+    prm.gprobs = d_gp;
+    prm.nprob = T;
+    prm.total_tiles = tiles;
+    const int grid = std::min<int>(tiles, h->num_sms);
+    mark(h, 1);
+    cudaError_t le = variant == 0 ? launch_ozaki_grouped<oz::OzCfg<4, 128, 4>>(prm, grid, s)
+                                  : launch_ozaki_grouped<oz::OzCfg<8, 128, 4>>(prm, grid, s);
+    h->launches.fetch_add(1);
+    if (le != cudaSuccess) return cuda_fail(h, le, "grouped ozaki_i8_gemm launch");
+    mark(h, 2);
+    return DGT_SUCCESS;
 }
 
 }  // namespace dgt

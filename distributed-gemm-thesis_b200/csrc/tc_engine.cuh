@@ -153,6 +153,10 @@ __device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap
         : "memory");
 }
 
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;\n" ::"l"(map) : "memory");
+}
+
 __device__ __forceinline__ uint32_t cluster_rank() {
     uint32_t r;
     asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
@@ -403,6 +407,12 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                 const int tm = cx.tm, tn = cx.tn;
                 const CUtensorMap* tA = GROUPED ? &cx.gp->tmA : &tmA;
                 const CUtensorMap* tB = GROUPED ? &cx.gp->tmB : &tmB;
+                if constexpr (GROUPED) {
+                    // the problem's maps reached global memory by a host copy: order them for
+                    // the tensor-map proxy before the TMA unit reads them
+                    tensormap_acquire(tA);
+                    tensormap_acquire(tB);
+                }
                 const int m_pad = DGT_TILE_FIELD(cx, m_pad, m_pad), n_pad = DGT_TILE_FIELD(cx, n_pad, n_pad);
                 for (int g = 0; g < P.ngroups && ok; ++g) {
                     const Group G = GROUPS[g];

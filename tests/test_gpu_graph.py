@@ -1,6 +1,6 @@
 """CUDA-graph capture of the step schedules: after one warm-up call (which sizes the
 handle's workspace and uploads any grouped table), dgt_dgemm (native and Ozaki),
-dgt_cannon25d and dgt_dgemm_grouped issue only capturable work, so the whole batch can be
+dgt_cannon25d and dgt_dgemm_grouped (native and grouped Ozaki) issue only capturable work, so the whole batch can be
 captured once and replayed; replay results equal the eager results bit for bit."""
 import numpy as np
 import pytest
@@ -35,6 +35,10 @@ def test_capture_and_replay_all_paths():
         gkeep.append((ga, gb, gc))
         gdesc.append(dict(m=gm, n=gn, k=gk, alpha=1.0, beta=0.5, A=ptr(ga), lda=gm, B=ptr(gb), ldb=gk, C=ptr(gc), ldc=gm))
     gC0 = [x[2].clone() for x in gkeep]
+    # the same products again, emulated in one grouped Ozaki pass (own outputs)
+    ekeep = [dev(O.uniform((d["m"], d["n"]), 500 + i)) for i, d in enumerate(gdesc)]
+    edesc = [dict(d, C=ptr(c)) for d, c in zip(gdesc, ekeep)]
+    eC0 = [x.clone() for x in ekeep]
 
     def batch(h):
         h.dgemm("N", "N", m, n, k, 1.0, ptr(dA), m, ptr(dB), k, 0.5, ptr(outs["native"]), m, mode=dgt.FP64_NATIVE)
@@ -42,6 +46,7 @@ def test_capture_and_replay_all_paths():
                 slices=7)
         h.cannon25d(M, p, c, 1.0, [ptr(x) for x in tA], [ptr(x) for x in tB], 0.5, [ptr(x) for x in tC])
         h.dgemm_grouped(gdesc)
+        h.dgemm_grouped(edesc, mode=dgt.FP64_OZAKI_INT8, slices=7)
 
     def reset():
         for name in outs:
@@ -50,6 +55,8 @@ def test_capture_and_replay_all_paths():
             x.copy_(dev(x0))
         for x, x0 in zip(gkeep, gC0):
             x[2].copy_(x0)
+        for x, x0 in zip(ekeep, eC0):
+            x.copy_(x0)
 
     with dgt.Handle() as h:
         side = torch.cuda.Stream()
@@ -57,7 +64,8 @@ def test_capture_and_replay_all_paths():
         with torch.cuda.stream(side):
             batch(h)  # eager (also the warm-up)
         torch.cuda.synchronize()
-        eager = [t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep]
+        eager = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
+                 [x.clone() for x in ekeep])
         reset()
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
@@ -68,7 +76,8 @@ def test_capture_and_replay_all_paths():
         g.replay()
         torch.cuda.synchronize()
         h.check_device()
-        replay = [t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep]
+        replay = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
+                  [x.clone() for x in ekeep])
         for a, b in zip(eager, replay):
             assert torch.equal(a, b)
         # and a second replay after another reset gives the same again
