@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dgt", choices=["dgt", "reference"])
     ap.add_argument("--size", type=int, default=SIZE)
+    ap.add_argument("--workload", default="headline", choices=["headline"] + sorted(WORKLOADS),
+                    help="headline (default): the FP64-emulation line above; the others print one JSON "
+                         "line for another configuration: " + ", ".join(sorted(WORKLOADS)))
     return ap.parse_args()
 
 
@@ -199,11 +202,377 @@ def reference_arm(args):
     print(json.dumps(line))
 
 
+# ---- other configurations: python bench.py --workload NAME (one JSON line each, 1 GPU) -----------
+# Seeded synthetic inputs generated on the host with numpy, errors against the host FP64 GEMM
+# (numpy / OpenBLAS, the reference's validation GEMM) on sampled rows, times as the median of
+# CUDA-event-timed calls on the launching stream after warm-up.
+
+def _dev(torch, X):
+    """Device tensor holding the column-major bytes of the numpy matrix X (rows x cols)."""
+    import numpy as np
+
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(X).T)).cuda()
+
+
+def _rows_of(t, rows, shape):
+    """Rows `rows` of the column-major matrix held by device tensor t (shape = rows x cols)."""
+    import numpy as np
+    import torch
+
+    m, n = shape
+    flat = t.reshape(-1)[: m * n].view(n, m)
+    return flat[:, torch.as_tensor(rows, device=t.device)].cpu().numpy().T.astype(np.float64)
+
+
+def _rel(got, want):
+    import numpy as np
+
+    d = np.abs(got - want)
+    den = np.abs(want)
+    mx = float(np.max(d / np.where(den > 0, den, 1.0))) if d.size else 0.0
+    fro = float(np.linalg.norm(d) / max(np.linalg.norm(want), 1e-300)) if d.size else 0.0
+    return mx, fro
+
+
+def _time_ms(torch, fn, reps, warm=3, flush=None):
+    """Median CUDA-event time (ms) of `reps` calls; `flush` (a write larger than L2) runs
+    before each timed call, outside the events."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def _setup():
+    import torch
+
+    import dgt
+
+    torch.cuda.set_device(0)
+    return torch, dgt, dgt.Handle(stream=torch.cuda.current_stream().cuda_stream)
+
+
+def workload_summa(args):
+    """Plain FP64 SUMMA on virtual grids (4096^3 on 2x2 with 512 blocks; 15000x17000x9000 on
+    4x4 with 256 blocks, alpha 1.5, beta -0.5), with the block-cyclic pack/unpack kernels
+    timed against HBM bandwidth (L2 flushed before each layout call)."""
+    import numpy as np
+
+    torch, dgt, h = _setup()
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    dmma_peak = h.probe_peak(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    cfgs = [dict(name="4096^3 on 2x2, 512 blocks", M=4096, N=4096, K=4096, b=512, p=2, q=2, alpha=1.0, beta=0.0),
+            dict(name="15000x17000x9000 on 4x4, 256 blocks", M=15000, N=17000, K=9000, b=256, p=4, q=4, alpha=1.5,
+                 beta=-0.5)]
+    out = []
+    sampler = ClockSampler(0)
+    sampler.start()
+    for c in cfgs:
+        M, N, K, b, p, q, alpha, beta = (c[x] for x in ("M", "N", "K", "b", "p", "q", "alpha", "beta"))
+        rng = np.random.default_rng(SEED)
+        A = rng.uniform(-1, 1, (M, K))
+        B = rng.uniform(-1, 1, (K, N))
+        C = np.zeros((M, N)) if beta == 0.0 else rng.uniform(-1, 1, (M, N))
+        dA, dB, dC = _dev(torch, A), _dev(torch, B), _dev(torch, C)
+
+        def local_set(rows, cols):
+            shapes = [(dgt.numroc(rows, b, i, 0, p), dgt.numroc(cols, b, j, 0, q)) for i in range(p) for j in range(q)]
+            bufs = [torch.empty((cc, r), dtype=torch.float64, device="cuda") for r, cc in shapes]
+            return [x.data_ptr() for x in bufs], [r for r, _ in shapes], bufs
+
+        lA, lldA, kA = local_set(M, K)
+        lB, lldB, kB = local_set(K, N)
+        lC, lldC, kC = local_set(M, N)
+        packs = {"pack A": (lambda: h.pack_block_cyclic(M, K, b, b, p, q, dA.data_ptr(), M, lA, lldA), M * K),
+                 "pack B": (lambda: h.pack_block_cyclic(K, N, b, b, p, q, dB.data_ptr(), K, lB, lldB), K * N),
+                 "pack C": (lambda: h.pack_block_cyclic(M, N, b, b, p, q, dC.data_ptr(), M, lC, lldC), M * N)}
+        for f, _ in packs.values():
+            f()
+        summa = lambda: h.summa(p, q, b, b, b, M, N, K, alpha, lA, lldA, lB, lldB, beta, lC, lldC)
+        summa()
+        h.unpack_block_cyclic(M, N, b, b, p, q, dC.data_ptr(), M, lC, lldC)
+        torch.cuda.synchronize()
+        h.check_device()
+        rows = np.sort(np.random.default_rng(1).choice(M, 96, replace=False))
+        err = _rel(_rows_of(dC, rows, (M, N)), alpha * (A[rows, :] @ B) + beta * C[rows, :])
+        layout = {}
+        for name, (f, elems) in packs.items():
+            ms = _time_ms(torch, f, 10, flush=flush)
+            layout[name] = {"ms": ms, "GB/s": 16.0 * elems / (ms * 1e-3) / 1e9}
+        ms = _time_ms(torch, lambda: h.unpack_block_cyclic(M, N, b, b, p, q, dC.data_ptr(), M, lC, lldC), 10,
+                      flush=flush)
+        layout["unpack C"] = {"ms": ms, "GB/s": 16.0 * M * N / (ms * 1e-3) / 1e9}
+        tot_bytes = 16.0 * (M * K + K * N + 2 * M * N)
+        tot_ms = sum(v["ms"] for v in layout.values())
+        summa_ms = _time_ms(torch, summa, 10)
+        flops = 2.0 * M * N * K
+        dC2 = torch.zeros_like(dC)
+        glob_ms = _time_ms(torch, lambda: h.dgemm("N", "N", M, N, K, alpha, dA.data_ptr(), M, dB.data_ptr(), K, 0.0,
+                                                   dC2.data_ptr(), M), 5)
+        out.append({"config": c["name"], "summa_tflops": flops / (summa_ms * 1e-3) / 1e12, "summa_ms": summa_ms,
+                    "frac_of_dmma_peak": flops / (summa_ms * 1e-3) / 1e12 / dmma_peak,
+                    "one_global_dgemm_tflops": flops / (glob_ms * 1e-3) / 1e12,
+                    "max_rel": err[0], "fro_rel": err[1], "sampled_rows": len(rows),
+                    "layout": layout, "layout_total": {"bytes": tot_bytes, "ms": tot_ms,
+                                                       "GB/s": tot_bytes / (tot_ms * 1e-3) / 1e9,
+                                                       "frac_of_hbm": tot_bytes / (tot_ms * 1e-3) / 1e9 / hbm}})
+        del dA, dB, dC, dC2, kA, kB, kC
+        torch.cuda.empty_cache()
+    clocks = sampler.stop()
+    print(json.dumps({"workload": "summa", "unit": "TFLOP/s", "dtype": "f64", "data": "synthetic U[-1,1) seeded",
+                      "dmma_peak_tflops": dmma_peak, "dmma_peak_source": "dgt_probe_peak DMMA (measured)",
+                      "hbm_peak_gbs": hbm, "hbm_peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                      "results": out, "clocks": clocks}))
+    h.close()
+
+
+def _ozaki_inputs(n, seed, phi, k=None):
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    k = k or n
+    A = (rng.random((n, k)) - 0.5) * np.exp(phi * rng.standard_normal((n, k)))
+    B = (rng.random((k, n)) - 0.5) * np.exp(phi * rng.standard_normal((k, n)))
+    return A, B
+
+
+def workload_precision(args):
+    """FP64 emulation at M = N = K = 16384 for phi in {0.5, 4.0}: native DMMA, INT8 slices
+    4..8 (and 9, 10 for phi = 4), BF16 slices 7 and 8; error vs the host FP64 GEMM on 48
+    sampled rows; whole-call TFLOP/s (split + GEMM)."""
+    import numpy as np
+
+    torch, dgt, h = _setup()
+    n = args.size
+    flops = 2.0 * n ** 3
+    rows = np.sort(np.random.default_rng(1).choice(n, 48, replace=False))
+    out = []
+    sampler = ClockSampler(0)
+    sampler.start()
+    for phi in (0.5, 4.0):
+        A, B = _ozaki_inputs(n, SEED + int(phi * 10), phi)
+        dA, dB = _dev(torch, A), _dev(torch, B)
+        dC = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        want = A[rows, :] @ B
+        runs = [("native", dgt.FP64_NATIVE, 0)] + [(f"int8_s{S}", dgt.FP64_OZAKI_INT8, S) for S in (4, 5, 6, 7, 8)]
+        if phi > 1:
+            runs += [(f"int8_s{S}", dgt.FP64_OZAKI_INT8, S) for S in (9, 10)]
+        runs += [(f"bf16_s{S}", dgt.FP64_OZAKI_BF16, S) for S in (7, 8)]
+        for name, mode, S in runs:
+            f = lambda: h.dgemm("N", "N", n, n, n, 1.0, dA.data_ptr(), n, dB.data_ptr(), n, 0.0, dC.data_ptr(), n,
+                                mode=mode, slices=max(S, 2))
+            f()
+            torch.cuda.synchronize()
+            h.check_device()
+            err = _rel(_rows_of(dC, rows, (n, n)), want)
+            bf16 = mode == dgt.FP64_OZAKI_BF16
+            ms = _time_ms(torch, f, 1 if bf16 else 3, warm=0 if bf16 else 1)
+            out.append({"phi": phi, "method": name, "slices": S, "tflops": flops / (ms * 1e-3) / 1e12, "ms": ms,
+                        "max_rel": err[0], "fro_rel": err[1]})
+        del dA, dB, dC
+        torch.cuda.empty_cache()
+    clocks = sampler.stop()
+    print(json.dumps({"workload": "precision", "unit": "TFLOP/s (FP64-equivalent, 2*M*N*K)", "M": n, "N": n, "K": n,
+                      "dtype": "f64", "data": "synthetic (U[0,1)-0.5)*exp(phi*N(0,1)) seeded",
+                      "sampled_rows": len(rows), "ozaki_variant": h.get_tuning(dgt.TUNE_OZAKI_VARIANT),
+                      "results": out, "clocks": clocks}))
+    h.close()
+
+
+def workload_fp32(args):
+    """FP32 GEMM: 3xBF16 split, 1xBF16 and the FP32 SIMT kernel on 8192^3 and
+    32768 x 32768 x 512, N(0,1) inputs; error vs the host FP64 GEMM of the FP32 inputs on
+    32 sampled rows; BF16 tensor-pipe use = products x 2MNK / GEMM-kernel time vs the
+    measured BF16 peak."""
+    import numpy as np
+
+    torch, dgt, h = _setup()
+    peaks = measured_peaks()
+    bf16_peak = peaks.get("bf16_tflops") or 1590.0
+    out = []
+    sampler = ClockSampler(0)
+    sampler.start()
+    for (m, n, k) in ((8192, 8192, 8192), (32768, 32768, 512)):
+        rng = np.random.default_rng(SEED)
+        A = rng.standard_normal((m, k)).astype(np.float32)
+        B = rng.standard_normal((k, n)).astype(np.float32)
+        dA, dB = _dev(torch, A), _dev(torch, B)
+        dC = torch.zeros((n, m), dtype=torch.float32, device="cuda")
+        rows = np.sort(np.random.default_rng(2).choice(m, 32, replace=False))
+        want = A[rows, :].astype(np.float64) @ B.astype(np.float64)
+        for name, mode, prods in (("bf16x3", dgt.FP32_BF16X3, 3), ("bf16x1", dgt.FP32_BF16X1, 1),
+                                  ("simt", dgt.FP32_SIMT, 0)):
+            f = lambda: h.sgemm("N", "N", m, n, k, 1.0, dA.data_ptr(), m, dB.data_ptr(), k, 0.0, dC.data_ptr(), m,
+                                mode=mode)
+            f()
+            torch.cuda.synchronize()
+            h.check_device()
+            err = _rel(_rows_of(dC, rows, (m, n)), want)
+            ms = _time_ms(torch, f, 5)
+            h.set_tuning(dgt.TUNE_PROFILE, 1)
+            f()
+            split_ms, gemm_ms = h.last_timings()
+            h.set_tuning(dgt.TUNE_PROFILE, 0)
+            r = {"shape": [m, n, k], "method": name, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12, "ms": ms,
+                 "split_ms": split_ms, "gemm_ms": gemm_ms, "max_rel": err[0], "fro_rel": err[1]}
+            if prods and gemm_ms:
+                bf = prods * 2.0 * m * n * k / (gemm_ms * 1e-3) / 1e12
+                r.update({"bf16_tflops_executed": bf, "bf16_pipe_frac": bf / bf16_peak})
+            out.append(r)
+        del dA, dB, dC
+        torch.cuda.empty_cache()
+    clocks = sampler.stop()
+    print(json.dumps({"workload": "fp32", "unit": "TFLOP/s (FP32, 2*M*N*K)", "dtype": "f32",
+                      "data": "synthetic N(0,1) seeded", "bf16_peak_tflops": bf16_peak,
+                      "bf16_peak_source": "MEASURED_PEAKS.json bf16_tflops" if peaks else "fallback",
+                      "results": out, "clocks": clocks}))
+    h.close()
+
+
+def workload_batching(args):
+    """Batching: virtual 2.5D Cannon 4x4x2 on M = N = K = 8192 and 256 independent products
+    with M, N, K log-uniform in [128, 4096], U[-1,1) entries; native DMMA and INT8 Ozaki
+    (S = 7 and 8), each as one grouped call; eager vs CUDA-graph replay; per-product
+    emulation shown for contrast; errors vs the host FP64 GEMM on sampled rows."""
+    import numpy as np
+
+    torch, dgt, h = _setup()
+    res = {}
+    sampler = ClockSampler(0)
+    sampler.start()
+
+    def graph_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=torch.cuda.current_stream()):
+            fn()
+        ms = _time_ms(torch, g.replay, reps)
+        del g
+        return ms
+
+    side = torch.cuda.Stream()
+    h.set_stream(side.cuda_stream)
+    with torch.cuda.stream(side):
+        # ---- 2.5D Cannon 4x4x2, M = 8192 ----
+        M, p, c = 8192, 4, 2
+        rng = np.random.default_rng(SEED)
+        A, B = rng.uniform(-1, 1, (M, M)), rng.uniform(-1, 1, (M, M))
+        dA, dB = _dev(torch, A), _dev(torch, B)
+        dC = torch.zeros((M, M), dtype=torch.float64, device="cuda")
+        lm = M // p
+        tiles = lambda: [torch.zeros((lm, lm), dtype=torch.float64, device="cuda") for _ in range(p * p)]
+        tA, tB, tC = tiles(), tiles(), tiles()
+        h.pack_cannon2d(M, p, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), [x.data_ptr() for x in tA],
+                        [x.data_ptr() for x in tB], [x.data_ptr() for x in tC])
+        rows = np.sort(np.random.default_rng(1).choice(M, 32, replace=False))
+        want = A[rows, :] @ B
+        cannon = {}
+        for name, mode, S in (("native", dgt.FP64_NATIVE, 7), ("int8_s7", dgt.FP64_OZAKI_INT8, 7),
+                              ("int8_s8", dgt.FP64_OZAKI_INT8, 8)):
+            f = lambda: h.cannon25d(M, p, c, 1.0, [x.data_ptr() for x in tA], [x.data_ptr() for x in tB], 0.0,
+                                    [x.data_ptr() for x in tC], mode=mode, slices=S)
+            f()
+            h.unpack_cannon2d(M, p, dC.data_ptr(), [x.data_ptr() for x in tC])
+            torch.cuda.synchronize()
+            h.check_device()
+            err = _rel(_rows_of(dC, rows, (M, M)), want)
+            n0 = h.launch_count()
+            f()
+            launches = h.launch_count() - n0
+            ms = _time_ms(torch, f, 5)
+            gms = graph_ms(f)
+            cannon[name] = {"tflops": 2.0 * M ** 3 / (ms * 1e-3) / 1e12, "ms": ms, "graph_ms": gms,
+                            "graph_tflops": 2.0 * M ** 3 / (gms * 1e-3) / 1e12, "kernel_launches": launches,
+                            "max_rel": err[0], "fro_rel": err[1]}
+        res["cannon_4x4x2_8192"] = cannon
+        del dA, dB, dC, tA, tB, tC
+        torch.cuda.empty_cache()
+
+        # ---- 256 independent products ----
+        rng = np.random.default_rng(SEED + 5)
+        dims = np.exp(rng.uniform(np.log(128), np.log(4096), (256, 3))).round().astype(int)
+        descs, keep, outs, checks = [], [], [], []
+        flops = 0.0
+        for i, (m, n, k) in enumerate(dims):
+            m, n, k = int(m), int(n), int(k)
+            r = np.random.default_rng(SEED + 1000 + i)
+            Ai, Bi = r.uniform(-1, 1, (m, k)), r.uniform(-1, 1, (k, n))
+            dAi, dBi = _dev(torch, Ai), _dev(torch, Bi)
+            dCi = torch.zeros((n, m), dtype=torch.float64, device="cuda")
+            keep.append((dAi, dBi))
+            outs.append(dCi)
+            descs.append(dict(m=m, n=n, k=k, alpha=1.0, beta=0.0, A=dAi.data_ptr(), lda=m, B=dBi.data_ptr(), ldb=k,
+                              C=dCi.data_ptr(), ldc=m))
+            flops += 2.0 * m * n * k
+            if i % 8 == 0:  # 32 products checked on 8 sampled rows each
+                rr = np.sort(np.random.default_rng(i).choice(m, min(8, m), replace=False))
+                checks.append((i, rr, Ai[rr, :] @ Bi))
+        grouped = {}
+        for name, mode, S in (("native", dgt.FP64_NATIVE, 7), ("int8_s7", dgt.FP64_OZAKI_INT8, 7),
+                              ("int8_s8", dgt.FP64_OZAKI_INT8, 8)):
+            f = lambda: h.dgemm_grouped(descs, mode=mode, slices=S)
+            # kernel variant: the fastest of the library's variants for this batch
+            knob = dgt.TUNE_DMMA_VARIANT if mode == dgt.FP64_NATIVE else dgt.TUNE_OZAKI_VARIANT
+            cands = range(7) if mode == dgt.FP64_NATIVE else (0, 1)
+            best = None
+            for v in cands:
+                h.set_tuning(knob, v)
+                t = _time_ms(torch, f, 2, warm=1)
+                if best is None or t < best[1]:
+                    best = (v, t)
+            h.set_tuning(knob, best[0])
+            f()
+            torch.cuda.synchronize()
+            h.check_device()
+            errs = [_rel(_rows_of(outs[i], rr, (int(dims[i][0]), int(dims[i][1]))), w) for i, rr, w in checks]
+            n0 = h.launch_count()
+            f()
+            launches = h.launch_count() - n0
+            ms = _time_ms(torch, f, 5)
+            gms = graph_ms(f)
+            grouped[name] = {"tflops": flops / (ms * 1e-3) / 1e12, "ms": ms, "graph_ms": gms,
+                             "graph_tflops": flops / (gms * 1e-3) / 1e12, "kernel_launches": launches,
+                             "kernel_variant": best[0], "max_rel": max(e[0] for e in errs),
+                             "fro_rel": max(e[1] for e in errs)}
+        # contrast: one Ozaki call per product (S = 8)
+        per = lambda: [h.dgemm("N", "N", d["m"], d["n"], d["k"], 1.0, d["A"], d["lda"], d["B"], d["ldb"], 0.0,
+                               d["C"], d["ldc"], mode=dgt.FP64_OZAKI_INT8, slices=8) for d in descs]
+        ms = _time_ms(torch, per, 3, warm=1)
+        grouped["int8_s8_one_call_per_product"] = {"tflops": flops / (ms * 1e-3) / 1e12, "ms": ms}
+        res["grouped_256"] = {"flops": flops, "methods": grouped}
+    h.set_stream(0)
+    clocks = sampler.stop()
+    print(json.dumps({"workload": "batching", "unit": "TFLOP/s (FP64-equivalent)", "dtype": "f64",
+                      "data": "synthetic U[-1,1) seeded; dims log-uniform [128, 4096]", "results": res,
+                      "clocks": clocks}))
+    h.close()
+
+
+WORKLOADS = {"summa": workload_summa, "precision": workload_precision, "fp32": workload_fp32,
+             "batching": workload_batching}
+
+
 # ---- dgt arm ------------------------------------------------------------------------------------
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.workload != "headline":
+        WORKLOADS[args.workload](args)
         return
     import numpy as np
     import torch

@@ -13,6 +13,47 @@
 
 namespace dgt {
 
+dgt_status device_table(dgt_context* h, int n, const void* const* parts, const size_t* bytes, void** out,
+                        size_t* offsets) {
+    uint64_t hash = 1469598103934665603ull;  // FNV-1a over every part
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) {
+        offsets[i] = total;
+        total += (bytes[i] + 255) / 256 * 256;
+        const unsigned char* b = (const unsigned char*)parts[i];
+        for (size_t j = 0; j < bytes[i]; ++j) hash = (hash ^ b[j]) * 1099511628211ull;
+        hash = (hash ^ (uint64_t)bytes[i]) * 1099511628211ull;
+    }
+    ++h->table_clock;
+    for (auto& t : h->tables)
+        if (t.hash == hash && t.bytes == total) {
+            t.last_use = h->table_clock;
+            *out = t.ptr;
+            return DGT_SUCCESS;
+        }
+    if ((int)h->tables.size() >= kMaxDeviceTables) {
+        size_t lru = 0;
+        for (size_t i = 1; i < h->tables.size(); ++i)
+            if (h->tables[i].last_use < h->tables[lru].last_use) lru = i;
+        DGT_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->tables[lru].ptr);
+        h->tables.erase(h->tables.begin() + (std::ptrdiff_t)lru);
+    }
+    void* ptr = nullptr;
+    cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(total, 256));
+    if (e != cudaSuccess) return cuda_fail(h, e, "device table");
+    for (int i = 0; i < n; ++i) {
+        e = cudaMemcpyAsync((char*)ptr + offsets[i], parts[i], bytes[i], cudaMemcpyHostToDevice, h->stream);
+        if (e != cudaSuccess) {
+            cudaFree(ptr);
+            return cuda_fail(h, e, "device table upload");
+        }
+    }
+    h->tables.push_back(dgt_context::DevTable{hash, total, ptr, h->table_clock});
+    *out = ptr;
+    return DGT_SUCCESS;
+}
+
 dgt_status ensure_workspace(dgt_context* h, size_t bytes, void** out, int slot) {
     if (slot < 0 || slot > 2) return fail(h, DGT_ERROR_INVALID_VALUE, "bad workspace slot");
     void*& ptr = h->ws[slot];
@@ -164,8 +205,7 @@ dgt_status dgt_destroy(dgt_handle_t h) {
         if (e) cudaEventDestroy(e);
     for (void* w : h->ws)
         if (w) cudaFree(w);
-    if (h->table) cudaFree(h->table);
-    if (h->oz_table) cudaFree(h->oz_table);
+    for (auto& t : h->tables) cudaFree(t.ptr);
     if (h->dev_error) cudaFree(h->dev_error);
     delete h;
     return DGT_SUCCESS;

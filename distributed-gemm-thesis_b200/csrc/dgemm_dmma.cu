@@ -331,38 +331,16 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
         std::copy(live.begin(), live.end(), prm.inl_probs);
         std::copy(segs.begin(), segs.end(), prm.inl_segs);
     } else {
-        // Device table in a handle-owned buffer, uploaded only when its content changes, so
-        // a repeated grouped call (e.g. replayed from a CUDA graph) needs no copy.
-        size_t pbytes = live.size() * sizeof(Problem), sbytes = segs.size() * sizeof(KSegment);
-        size_t off = (pbytes + 255) / 256 * 256;
-        uint64_t hash = 1469598103934665603ull;  // FNV-1a over both tables
-        auto mix = [&](const void* p, size_t n) {
-            const unsigned char* b = (const unsigned char*)p;
-            for (size_t i = 0; i < n; ++i) hash = (hash ^ b[i]) * 1099511628211ull;
-        };
-        mix(live.data(), pbytes);
-        mix(segs.data(), sbytes);
-        if (off + sbytes > h->table_bytes) {
-            if (h->table) {
-                DGT_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-                cudaFree(h->table);
-                h->table = nullptr;
-                h->table_bytes = 0;
-            }
-            size_t want = std::max<size_t>(off + sbytes, 1 << 16);
-            cudaError_t e = cudaMalloc(&h->table, want);
-            if (e != cudaSuccess) return cuda_fail(h, e, "grouped table");
-            h->table_bytes = want;
-            h->table_hash = 0;
-        }
-        if (hash != h->table_hash) {
-            DGT_CUDA_TRY(h, cudaMemcpyAsync(h->table, live.data(), pbytes, cudaMemcpyHostToDevice, h->stream));
-            DGT_CUDA_TRY(h, cudaMemcpyAsync((char*)h->table + off, segs.data(), sbytes, cudaMemcpyHostToDevice,
-                                            h->stream));
-            h->table_hash = hash;
-        }
-        prm.probs = (const Problem*)h->table;
-        prm.segs = (const KSegment*)((char*)h->table + off);
+        // device table from the handle's cache: a repeated grouped call (e.g. replayed from a
+        // CUDA graph) needs no copy
+        const void* parts[2] = {live.data(), segs.data()};
+        const size_t bytes[2] = {live.size() * sizeof(Problem), segs.size() * sizeof(KSegment)};
+        size_t offs[2];
+        void* table = nullptr;
+        dgt_status st = device_table(h, 2, parts, bytes, &table, offs);
+        if (st != DGT_SUCCESS) return st;
+        prm.probs = (const Problem*)((char*)table + offs[0]);
+        prm.segs = (const KSegment*)((char*)table + offs[1]);
     }
     int grid = (int)std::min<int64_t>(tiles, h->num_sms);
     cudaError_t e;

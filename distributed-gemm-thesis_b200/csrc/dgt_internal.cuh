@@ -53,12 +53,16 @@ struct dgt_context {
     size_t ws_bytes[3] = {0, 0, 0};
     std::atomic<int64_t> launches{0};
     std::map<dgt::TuneKey, dgt::TuneEntry> tune;
-    void* table = nullptr;  // grouped-GEMM problem table (dgemm_dmma.cu)
-    size_t table_bytes = 0;
-    uint64_t table_hash = 0;
-    void* oz_table = nullptr;  // grouped Ozaki tables: problems + pre-pass jobs (ozaki.cu)
-    size_t oz_table_bytes = 0;
-    uint64_t oz_table_hash = 0;
+    // device copies of launch tables (grouped problems, Ozaki jobs and schedules), keyed by
+    // a hash of their content (see device_table)
+    struct DevTable {
+        uint64_t hash;
+        size_t bytes;
+        void* ptr;
+        uint64_t last_use;
+    };
+    std::vector<DevTable> tables;
+    uint64_t table_clock = 0;
 };
 
 namespace dgt {
@@ -87,6 +91,15 @@ inline dgt_status cuda_fail(dgt_context* h, cudaError_t e, const char* what) {
 
 // Phase markers for DGT_TUNE_PROFILE (no-ops unless profiling is on).
 void mark(dgt_context* h, int which);
+
+// Device copy of a host table made of n parts, part i placed at offsets[i] (256-byte
+// aligned), taken from a per-handle cache keyed by a hash of the content: a repeated call
+// (one replayed from a captured CUDA graph among them) finds its table resident and issues
+// no copy.  Up to kMaxDeviceTables tables stay resident; beyond that the least recently used
+// one is released (after the handle's stream drains).
+constexpr int kMaxDeviceTables = 64;
+dgt_status device_table(dgt_context* h, int n, const void* const* parts, const size_t* bytes, void** out,
+                        size_t* offsets);
 
 // Grows a handle-owned scratch buffer; never shrinks.  slot 0, 1 or 2.
 dgt_status ensure_workspace(dgt_context* h, size_t bytes, void** out, int slot = 0);

@@ -355,11 +355,16 @@ static dgt_status ozaki_run(dgt_context* h, cudaStream_t s, int num_sms, unsigne
     };
 
     const bool inline_sched = L.segs.size() <= (size_t)oz::MAX_SEGS && L.groups.size() <= (size_t)oz::MAX_GROUPS;
-    if (!inline_sched) {  // long BF16 schedules: device table (not capturable in a CUDA graph)
-        DGT_CUDA_TRY(h, cudaMemcpyAsync(dsegs, L.segs.data(), L.segs.size() * sizeof(oz::Seg),
-                                        cudaMemcpyHostToDevice, s));
-        DGT_CUDA_TRY(h, cudaMemcpyAsync(dgroups, L.groups.data(), L.groups.size() * sizeof(oz::Group),
-                                        cudaMemcpyHostToDevice, s));
+    if (!inline_sched) {  // long BF16 schedules: a device table from the handle's cache
+        if (!h) return DGT_ERROR_UNSUPPORTED;
+        const void* parts[2] = {L.segs.data(), L.groups.data()};
+        const size_t bytes[2] = {L.segs.size() * sizeof(oz::Seg), L.groups.size() * sizeof(oz::Group)};
+        size_t offs[2];
+        void* table = nullptr;
+        dgt_status st = device_table(h, 2, parts, bytes, &table, offs);
+        if (st != DGT_SUCCESS) return st;
+        dsegs = (oz::Seg*)((char*)table + offs[0]);
+        dgroups = (oz::Group*)((char*)table + offs[1]);
     }
     if (h) mark(h, 0);
     DGT_CUDA_TRY(h, cudaMemsetAsync(amaxA, 0, m * 8, s));
@@ -559,7 +564,6 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
 
     // host tables: GProb[T] (tensor maps inside, 64-byte aligned) and SplitJob[2T], zeroed
     // byte for byte so that padding hashes the same on every call
-    const size_t gp_bytes = up((size_t)T * sizeof(oz::GProb), 256);
     const size_t job_bytes = (size_t)2 * T * sizeof(oz::SplitJob);
     static thread_local std::vector<oz::GProb> host_gp;
     static thread_local std::vector<oz::SplitJob> host_jobs;
@@ -626,37 +630,17 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     if (amax_blocks > INT32_MAX || split_blocks > INT32_MAX)
         return fail(h, DGT_ERROR_UNSUPPORTED, "grouped Ozaki batch too large for one launch");
 
-    // device copy of the tables, uploaded only when their content changes (a repeated call,
-    // e.g. from a replayed CUDA graph, needs no copy)
-    uint64_t hash = 1469598103934665603ull;  // FNV-1a over both tables
-    auto mix = [&](const void* p, size_t n) {
-        const unsigned char* b = (const unsigned char*)p;
-        for (size_t i = 0; i < n; ++i) hash = (hash ^ b[i]) * 1099511628211ull;
-    };
-    mix(gp, (size_t)T * sizeof(oz::GProb));
-    mix(jobs, job_bytes);
-    const size_t table_bytes = gp_bytes + job_bytes;
-    if (table_bytes > h->oz_table_bytes) {
-        if (h->oz_table) {
-            DGT_CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-            cudaFree(h->oz_table);
-            h->oz_table = nullptr;
-            h->oz_table_bytes = 0;
-        }
-        const size_t want = std::max<size_t>(table_bytes, 1 << 16);
-        cudaError_t e = cudaMalloc(&h->oz_table, want);
-        if (e != cudaSuccess) return cuda_fail(h, e, "grouped Ozaki table");
-        h->oz_table_bytes = want;
-        h->oz_table_hash = 0;
-    }
+    // device copy of the tables from the handle's cache (a repeated call, e.g. from a
+    // replayed CUDA graph, needs no copy)
+    const void* parts[2] = {gp, jobs};
+    const size_t part_bytes[2] = {(size_t)T * sizeof(oz::GProb), job_bytes};
+    size_t offs[2];
+    void* table = nullptr;
+    st = device_table(h, 2, parts, part_bytes, &table, offs);
+    if (st != DGT_SUCCESS) return st;
     cudaStream_t s = h->stream;
-    if (hash != h->oz_table_hash) {
-        DGT_CUDA_TRY(h, cudaMemcpyAsync(h->oz_table, gp, (size_t)T * sizeof(oz::GProb), cudaMemcpyHostToDevice, s));
-        DGT_CUDA_TRY(h, cudaMemcpyAsync((char*)h->oz_table + gp_bytes, jobs, job_bytes, cudaMemcpyHostToDevice, s));
-        h->oz_table_hash = hash;
-    }
-    const auto* d_gp = (const oz::GProb*)h->oz_table;
-    const auto* d_jobs = (const oz::SplitJob*)((char*)h->oz_table + gp_bytes);
+    const auto* d_gp = (const oz::GProb*)((char*)table + offs[0]);
+    const auto* d_jobs = (const oz::SplitJob*)((char*)table + offs[1]);
 
     mark(h, 0);
     DGT_CUDA_TRY(h, cudaMemsetAsync(amax, 0, amax_words * 8, s));

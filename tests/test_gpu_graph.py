@@ -1,7 +1,8 @@
 """CUDA-graph capture of the step schedules: after one warm-up call (which sizes the
 handle's workspace and uploads any grouped table), dgt_dgemm (native and Ozaki),
-dgt_cannon25d and dgt_dgemm_grouped (native and grouped Ozaki) issue only capturable work, so the whole batch can be
-captured once and replayed; replay results equal the eager results bit for bit."""
+dgt_cannon25d (native, and emulated as one grouped Ozaki pass per step) and
+dgt_dgemm_grouped (native and grouped Ozaki) issue only capturable work, so the whole batch
+can be captured once and replayed; replay results equal the eager results bit for bit."""
 import numpy as np
 import pytest
 
@@ -26,6 +27,7 @@ def test_capture_and_replay_all_paths():
     tB = [dev(O.uniform((lm, lm), 40 + i)) for i in range(p * p)]
     tC0 = [O.uniform((lm, lm), 70 + i) for i in range(p * p)]
     tC = [dev(x) for x in tC0]
+    tE = [dev(x) for x in tC0]  # the same Cannon, emulated (one grouped Ozaki pass per step)
     # 40 grouped products (device-table path: more than 32 problems)
     rng = np.random.default_rng(0)
     gdesc, gkeep = [], []
@@ -45,6 +47,8 @@ def test_capture_and_replay_all_paths():
         h.dgemm("N", "N", m, n, k, 1.0, ptr(dA), m, ptr(dB), k, 0.5, ptr(outs["ozaki"]), m, mode=dgt.FP64_OZAKI_INT8,
                 slices=7)
         h.cannon25d(M, p, c, 1.0, [ptr(x) for x in tA], [ptr(x) for x in tB], 0.5, [ptr(x) for x in tC])
+        h.cannon25d(M, p, c, 1.0, [ptr(x) for x in tA], [ptr(x) for x in tB], 0.5, [ptr(x) for x in tE],
+                    mode=dgt.FP64_OZAKI_INT8, slices=7)
         h.dgemm_grouped(gdesc)
         h.dgemm_grouped(edesc, mode=dgt.FP64_OZAKI_INT8, slices=7)
 
@@ -52,6 +56,8 @@ def test_capture_and_replay_all_paths():
         for name in outs:
             outs[name].copy_(dev(C))
         for x, x0 in zip(tC, tC0):
+            x.copy_(dev(x0))
+        for x, x0 in zip(tE, tC0):
             x.copy_(dev(x0))
         for x, x0 in zip(gkeep, gC0):
             x[2].copy_(x0)
@@ -65,7 +71,7 @@ def test_capture_and_replay_all_paths():
             batch(h)  # eager (also the warm-up)
         torch.cuda.synchronize()
         eager = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
-                 [x.clone() for x in ekeep])
+                 [x.clone() for x in ekeep] + [x.clone() for x in tE])
         reset()
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
@@ -77,7 +83,7 @@ def test_capture_and_replay_all_paths():
         torch.cuda.synchronize()
         h.check_device()
         replay = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
-                  [x.clone() for x in ekeep])
+                  [x.clone() for x in ekeep] + [x.clone() for x in tE])
         for a, b in zip(eager, replay):
             assert torch.equal(a, b)
         # and a second replay after another reset gives the same again
