@@ -28,16 +28,27 @@ constexpr int PAD = 4;
 constexpr int LD_MN = BM + PAD;  // [k][mn] layout row stride (doubles): 1056 B = 32 mod 128 banks
 constexpr int GROUP_M = 8;       // tile rasterisation group for L2 reuse
 
-// Kernel variants (the autotuner's knob): DMMA shape m16n8k{4,8}, K depth of a stage, ring depth.
-template <int MMAK_, int BK_, int STAGES_, int NWARPS_ = 8>
+// Kernel variants (the autotuner's knob): DMMA shape m16n8k{4,8,16}, K depth of a stage, ring depth.
+//
+// PERM (k8 / k16 shapes only): fragments are read with 128-bit shared loads.  MMA rows g
+// and g+8 of an m16 tile are taken from adjacent physical rows 2g and 2g+1, and inside
+// every 8-deep K block logical k = t + 4h is read from physical k = 2t + h (h = 0, 1), the
+// same for A and B, so the product is unchanged.  Paddings keep every 8-lane phase of
+// those loads on distinct banks: [k][mn] rows of 130 doubles (1040 B = 16 mod 128),
+// A's [mn][k] rows of BK+4, B's [n][k] rows of BK+8 doubles (32 and 64 mod 128 B).
+template <int MMAK_, int BK_, int STAGES_, int NWARPS_ = 8, bool PERM_ = false>
 struct Cfg {
     static constexpr int MMAK = MMAK_, BK = BK_, STAGES = STAGES_;
+    static constexpr bool PERM = PERM_;
     static constexpr int THREADS = NWARPS_ * 32;
     static constexpr int WARPS_M = NWARPS_ / 4;      // warps along M (4 along N, 32 columns each)
     static constexpr int MT = BM / WARPS_M / 16;     // m16 tiles per warp
+    static constexpr int LDMN = PERM ? BM + 2 : LD_MN;  // [k][mn] row stride (doubles)
     static constexpr int LD_K = BK + PAD;  // [mn][k] row stride: (BK+4)*8 B = 32 mod 128 for BK in {16, 32}
-    static constexpr int STAGE_ELEMS = (BM * LD_K > BK * LD_MN) ? BM * LD_K : BK * LD_MN;
-    static constexpr size_t SMEM = (size_t)2 * STAGES * STAGE_ELEMS * sizeof(double);
+    static constexpr int LD_KB = PERM ? BK + 8 : LD_K;  // B's [n][k] row stride
+    static constexpr int STAGE_A = (BM * LD_K > BK * LDMN) ? BM * LD_K : BK * LDMN;
+    static constexpr int STAGE_B = (BN * LD_KB > BK * LDMN) ? BN * LD_KB : BK * LDMN;
+    static constexpr size_t SMEM = (size_t)STAGES * (STAGE_A + STAGE_B) * sizeof(double);
 };
 constexpr int MAX_INLINE_PROBS = 32, MAX_INLINE_SEGS = 160;
 
@@ -80,11 +91,22 @@ __device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double (&a)[4]
         : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
+// m16n8k16 (sm_90+ shape): A fragment a[2h] = A[g][t + 4h], a[2h+1] = A[g + 8][t + 4h],
+// B fragment b[h] = B[t + 4h][g], h = 0..3 (the k8 layout extended along K).
+__device__ __forceinline__ void dmma_16x8x16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+        "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+          "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 // Loads one BK-slice of an operand tile into shared memory.
 //  mn_major: global element (mn, k) at base[mn + k*ld]  -> smem [k][mn], row stride LD_MN
 //  else    : global element (mn, k) at base[k + mn*ld]  -> smem [mn][k], row stride LD_K
 // mn_lim / k_lim: valid extents from (mn0, k0); outside is zero-filled.
-template <int BK, int LD_K, int THREADS>
+template <int BK, int LD_K, int THREADS, int LD_MN = dgt::LD_MN>
 __device__ __forceinline__ void load_tile(double* s, const double* base, int64_t ld, bool mn_major, int64_t mn0,
                                           int64_t k0, int64_t mn_lim, int64_t k_lim, bool vec16, int tid) {
     const uint32_t s_base = smem_u32(s);
@@ -129,6 +151,31 @@ __device__ __forceinline__ void load_tile(double* s, const double* base, int64_t
     }
 }
 
+// Interior fast path of load_tile: every chunk in range and 16-byte aligned, so each thread
+// walks one base pointer with a constant stride and no per-chunk checks.
+template <int BK, int LD_K, int THREADS, int LD_MN>
+__device__ __forceinline__ void load_tile_full(double* s, const double* base, int64_t ld, bool mn_major, int64_t mn0,
+                                               int64_t k0, int tid) {
+    const uint32_t s_base = smem_u32(s);
+    if (mn_major) {
+        constexpr int KSTEP = THREADS / 64;  // k rows covered by one pass of the block
+        const int mn = (tid & 63) * 2, kb = tid / 64;
+        const double* src = base + (mn0 + mn) + (k0 + kb) * ld;
+        const int64_t step = (int64_t)KSTEP * ld;
+        const uint32_t dst = s_base + (uint32_t)((kb * LD_MN + mn) * 8);
+#pragma unroll
+        for (int i = 0; i < BK / KSTEP; ++i) cp_async16(dst + (uint32_t)(i * KSTEP * LD_MN * 8), src + i * step, 16);
+    } else {
+        constexpr int HB = BK / 2, MSTEP = THREADS / HB;  // rows covered by one pass of the block
+        const int mn = tid / HB, k = (tid % HB) * 2;
+        const double* src = base + (k0 + k) + (mn0 + mn) * ld;
+        const int64_t step = (int64_t)MSTEP * ld;
+        const uint32_t dst = s_base + (uint32_t)((mn * LD_K + k) * 8);
+#pragma unroll
+        for (int i = 0; i < BM / MSTEP; ++i) cp_async16(dst + (uint32_t)(i * MSTEP * LD_K * 8), src + i * step, 16);
+    }
+}
+
 __device__ __forceinline__ int find_problem(const Problem* P, int nprob, int tile) {
     int lo = 0, hi = nprob - 1;
     while (lo < hi) {
@@ -143,11 +190,14 @@ __device__ __forceinline__ int find_problem(const Problem* P, int nprob, int til
 
 template <class CF>
 __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __grid_constant__ GroupedParams prm) {
-    constexpr int BK = CF::BK, STAGES = CF::STAGES, LD_K = CF::LD_K, STAGE_ELEMS = CF::STAGE_ELEMS;
+    constexpr int BK = CF::BK, STAGES = CF::STAGES, LD_K = CF::LD_K, LD_KB = CF::LD_KB, LDMN = CF::LDMN;
+    constexpr int STAGE_A = CF::STAGE_A, STAGE_B = CF::STAGE_B;
     constexpr int MMAK = CF::MMAK, THREADS = CF::THREADS, MT = CF::MT, WTM = MT * 16;
+    constexpr bool PERM = CF::PERM;
+    static_assert(!PERM || MMAK >= 8, "128-bit fragment loads need the k8 or k16 shape");
     extern __shared__ __align__(16) double smem[];
     double* sA = smem;
-    double* sB = smem + STAGES * STAGE_ELEMS;
+    double* sB = smem + STAGES * STAGE_A;
 
     const Problem* probs = prm.probs ? prm.probs : prm.inl_probs;
     const KSegment* segs = prm.segs ? prm.segs : prm.inl_segs;
@@ -194,10 +244,16 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
                 int64_t klim = sg.k - ld_k0;
                 bool va = (((uintptr_t)sg.A & 15) == 0) && ((sg.lda & 1) == 0);
                 bool vb = (((uintptr_t)sg.B & 15) == 0) && ((sg.ldb & 1) == 0);
-                load_tile<BK, LD_K, THREADS>(sA + stage * STAGE_ELEMS, sg.A, sg.lda, a_mn, m0, ld_k0, pb.m - m0, klim,
-                                             va, tid);
-                load_tile<BK, LD_K, THREADS>(sB + stage * STAGE_ELEMS, sg.B, sg.ldb, b_mn, n0, ld_k0, pb.n - n0, klim,
-                                             vb, tid);
+                if (va && klim >= BK && pb.m - m0 >= BM)
+                    load_tile_full<BK, LD_K, THREADS, LDMN>(sA + stage * STAGE_A, sg.A, sg.lda, a_mn, m0, ld_k0, tid);
+                else
+                    load_tile<BK, LD_K, THREADS, LDMN>(sA + stage * STAGE_A, sg.A, sg.lda, a_mn, m0, ld_k0, pb.m - m0,
+                                                       klim, va, tid);
+                if (vb && klim >= BK && pb.n - n0 >= BN)
+                    load_tile_full<BK, LD_KB, THREADS, LDMN>(sB + stage * STAGE_B, sg.B, sg.ldb, b_mn, n0, ld_k0, tid);
+                else
+                    load_tile<BK, LD_KB, THREADS, LDMN>(sB + stage * STAGE_B, sg.B, sg.ldb, b_mn, n0, ld_k0, pb.n - n0,
+                                                        klim, vb, tid);
                 ld_k0 += BK;
                 if (ld_k0 >= sg.k) {
                     ld_k0 = 0;
@@ -215,8 +271,62 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
             cp_async_wait<STAGES - 2>();
             __syncthreads();
             issue((kt + STAGES - 1) % STAGES);
-            const double* a = sA + (kt % STAGES) * STAGE_ELEMS;
-            const double* b = sB + (kt % STAGES) * STAGE_ELEMS;
+            const double* a = sA + (kt % STAGES) * STAGE_A;
+            const double* b = sB + (kt % STAGES) * STAGE_B;
+            if constexpr (PERM) {
+                // physical k of fragment element h (logical k = t + 4h), see Cfg
+                auto kp = [&](int h) { return 8 * (h >> 1) + 2 * t + (h & 1); };
+#pragma unroll
+                for (int kk = 0; kk < BK; kk += MMAK) {
+                    double bf[4][MMAK / 4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int n = wn * 32 + j * 8 + g;
+                        if (b_mn) {
+#pragma unroll
+                            for (int h = 0; h < MMAK / 4; ++h) bf[j][h] = b[(kk + kp(h)) * LDMN + n];
+                        } else {
+#pragma unroll
+                            for (int q = 0; q < MMAK / 8; ++q) {
+                                const double2 v = *reinterpret_cast<const double2*>(b + n * LD_KB + kk + 8 * q + 2 * t);
+                                bf[j][2 * q] = v.x;
+                                bf[j][2 * q + 1] = v.y;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < MT; ++i) {
+                        const int mr = wm * WTM + i * 16 + 2 * g;  // physical rows of MMA rows g, g + 8
+                        double af[MMAK / 2];
+                        if (a_mn) {
+#pragma unroll
+                            for (int h = 0; h < MMAK / 4; ++h) {
+                                const double2 v = *reinterpret_cast<const double2*>(a + (kk + kp(h)) * LDMN + mr);
+                                af[2 * h] = v.x;
+                                af[2 * h + 1] = v.y;
+                            }
+                        } else {
+#pragma unroll
+                            for (int q = 0; q < MMAK / 8; ++q) {
+                                const double2 v0 = *reinterpret_cast<const double2*>(a + mr * LD_K + kk + 8 * q + 2 * t);
+                                const double2 v1 =
+                                    *reinterpret_cast<const double2*>(a + (mr + 1) * LD_K + kk + 8 * q + 2 * t);
+                                af[4 * q] = v0.x;
+                                af[4 * q + 1] = v1.x;
+                                af[4 * q + 2] = v0.y;
+                                af[4 * q + 3] = v1.y;
+                            }
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            if constexpr (MMAK == 8)
+                                dmma_16x8x8(acc[i][j], af, bf[j]);
+                            else
+                                dmma_16x8x16(acc[i][j], af, bf[j]);
+                        }
+                    }
+                }
+            } else {
 #pragma unroll
             for (int kk = 0; kk < BK; kk += MMAK) {
                 // B fragments of the warp's four n8 tiles, then one m16 tile of A at a time
@@ -226,7 +336,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
                     const int n = wn * 32 + j * 8 + g;
 #pragma unroll
                     for (int h = 0; h < MMAK / 4; ++h)
-                        bf[j][h] = b_mn ? b[(kk + t + 4 * h) * LD_MN + n] : b[n * LD_K + kk + t + 4 * h];
+                        bf[j][h] = b_mn ? b[(kk + t + 4 * h) * LDMN + n] : b[n * LD_KB + kk + t + 4 * h];
                 }
 #pragma unroll
                 for (int i = 0; i < MT; ++i) {
@@ -235,8 +345,8 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
 #pragma unroll
                     for (int h = 0; h < MMAK / 4; ++h) {
                         if (a_mn) {
-                            af[2 * h] = a[(kk + t + 4 * h) * LD_MN + m];
-                            af[2 * h + 1] = a[(kk + t + 4 * h) * LD_MN + m + 8];
+                            af[2 * h] = a[(kk + t + 4 * h) * LDMN + m];
+                            af[2 * h + 1] = a[(kk + t + 4 * h) * LDMN + m + 8];
                         } else {
                             af[2 * h] = a[m * LD_K + kk + t + 4 * h];
                             af[2 * h + 1] = a[(m + 8) * LD_K + kk + t + 4 * h];
@@ -246,12 +356,15 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
                     for (int j = 0; j < 4; ++j) {
                         if constexpr (MMAK == 4) {
                             dmma_16x8x4(acc[i][j], af[0], af[1], bf[j][0]);
-                        } else {
+                        } else if constexpr (MMAK == 8) {
                             dmma_16x8x8(acc[i][j], af, bf[j]);
+                        } else {
+                            dmma_16x8x16(acc[i][j], af, bf[j]);
                         }
                     }
                 }
             }
+            }  // PERM
         }
         cp_async_wait<0>();
         __syncthreads();  // the next tile's prologue reuses the ring
@@ -264,7 +377,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
             for (int j = 0; j < 4; ++j) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    int64_t row = m0 + wm * WTM + i * 16 + g + h * 8;
+                    int64_t row = m0 + wm * WTM + i * 16 + (PERM ? 2 * g + h : g + h * 8);
                     if (row >= pb.m) continue;
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
@@ -288,6 +401,13 @@ using V3 = Cfg<4, 32, 3>;
 using V4 = Cfg<8, 16, 4, 16>;
 using V5 = Cfg<8, 32, 3, 16>;
 using V6 = Cfg<4, 16, 4, 16>;
+using V7 = Cfg<16, 32, 3>;
+using V8 = Cfg<16, 32, 3, 16>;
+using V9 = Cfg<16, 16, 4>;
+using V10 = Cfg<8, 16, 4, 8, true>;
+using V11 = Cfg<16, 16, 4, 8, true>;
+using V12 = Cfg<8, 32, 2, 8, true>;
+using V13 = Cfg<16, 32, 2, 8, true>;
 
 template <class CF>
 cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stream) {
@@ -304,7 +424,7 @@ cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stre
 
 }  // namespace
 
-int dmma_variant_count() { return 7; }
+int dmma_variant_count() { return 14; }
 
 dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs) {
     // drop empty problems, lay out the tile prefix
@@ -351,6 +471,13 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
         case 4: e = launch_variant<V4>(prm, grid, h->stream); break;
         case 5: e = launch_variant<V5>(prm, grid, h->stream); break;
         case 6: e = launch_variant<V6>(prm, grid, h->stream); break;
+        case 7: e = launch_variant<V7>(prm, grid, h->stream); break;
+        case 8: e = launch_variant<V8>(prm, grid, h->stream); break;
+        case 9: e = launch_variant<V9>(prm, grid, h->stream); break;
+        case 10: e = launch_variant<V10>(prm, grid, h->stream); break;
+        case 11: e = launch_variant<V11>(prm, grid, h->stream); break;
+        case 12: e = launch_variant<V12>(prm, grid, h->stream); break;
+        case 13: e = launch_variant<V13>(prm, grid, h->stream); break;
         default: e = launch_variant<V0>(prm, grid, h->stream); break;
     }
     h->launches.fetch_add(1);

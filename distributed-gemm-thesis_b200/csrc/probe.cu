@@ -34,6 +34,30 @@ __global__ void __launch_bounds__(PROBE_THREADS) dmma_probe_kernel(double* out, 
     if (s == 12345.678) out[0] = s;  // keeps the loop live; never true for the probe inputs
 }
 
+// The same with the m16n8k16 shape (4x the FLOPs per instruction).
+__global__ void __launch_bounds__(PROBE_THREADS) dmma16_probe_kernel(double* out, double seed) {
+    double acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[i][e] = 0.0;
+    const double a = seed + threadIdx.x * 1e-9, b = seed * 0.25;
+    for (int it = 0; it < PROBE_ITERS / 4; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            asm volatile(
+                "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%4,%4,%4,%4,%4,%4,%4}, "
+                "{%5,%5,%5,%5}, {%0,%1,%2,%3};\n"
+                : "+d"(acc[i][0]), "+d"(acc[i][1]), "+d"(acc[i][2]), "+d"(acc[i][3])
+                : "d"(a), "d"(b));
+        }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += acc[i][0] + acc[i][1] + acc[i][2] + acc[i][3];
+    if (s == 12345.678) out[0] = s;
+}
+
 __global__ void __launch_bounds__(PROBE_THREADS) dfma_probe_kernel(double* out, double seed) {
     double acc[8];
 #pragma unroll
@@ -95,7 +119,7 @@ using namespace dgt;
 
 extern "C" dgt_status dgt_probe_peak(dgt_handle_t h, int32_t kind, double* tflops) {
     if (!h) return DGT_ERROR_NOT_INITIALIZED;
-    if (!tflops || kind < 0 || kind > 2) return fail(h, DGT_ERROR_INVALID_VALUE, "bad probe kind");
+    if (!tflops || kind < 0 || kind > 3) return fail(h, DGT_ERROR_INVALID_VALUE, "bad probe kind");
     void* ws = nullptr;
     dgt_status st = ensure_workspace(h, 64, &ws, 1);
     if (st != DGT_SUCCESS) return st;
@@ -110,6 +134,8 @@ extern "C" dgt_status dgt_probe_peak(dgt_handle_t h, int32_t kind, double* tflop
             dmma_probe_kernel<<<blocks, PROBE_THREADS, 0, h->stream>>>((double*)ws, 1.0);
         else if (kind == 1)
             dfma_probe_kernel<<<blocks, PROBE_THREADS, 0, h->stream>>>((double*)ws, 1.0);
+        else if (kind == 3)
+            dmma16_probe_kernel<<<blocks, PROBE_THREADS, 0, h->stream>>>((double*)ws, 1.0);
         else
             mixed_probe_kernel<<<blocks, PROBE_THREADS, 0, h->stream>>>((double*)ws, 1.0);
         h->launches.fetch_add(1);
@@ -124,8 +150,8 @@ extern "C" dgt_status dgt_probe_peak(dgt_handle_t h, int32_t kind, double* tflop
     cudaEventDestroy(e1);
     const double warps = (double)blocks * PROBE_THREADS / 32.0;
     double flops;
-    if (kind == 0)
-        flops = warps * PROBE_ITERS * 8 * (2.0 * 16 * 8 * 4);  // per warp-level m16n8k4
+    if (kind == 0 || kind == 3)
+        flops = warps * PROBE_ITERS * 8 * (2.0 * 16 * 8 * 4);  // per warp-level m16n8k4 (k16: a quarter as many)
     else if (kind == 1)
         flops = (double)blocks * PROBE_THREADS * PROBE_ITERS * 8 * 2.0;
     else  // half the warps each, equal FLOPs per warp

@@ -129,3 +129,19 @@ def test_double_double_sample_error(h):
     gpu_err = np.abs(got[rows, cols] - exact) / np.abs(exact)
     cpu_err = np.abs((A @ B)[rows, cols] - exact) / np.abs(exact)
     assert np.median(gpu_err) <= 4 * max(np.median(cpu_err), 1e-17)
+
+
+@pytest.mark.parametrize("variant", list(range(14)))
+def test_dmma_kernel_variants(variant):
+    """Every tuning variant of the native kernel (DMMA shape m16n8k4/k8/k16, K depth, ring
+    depth, 8 or 16 warps, 64- or 128-bit fragment loads) on ragged shapes, all four
+    transpose pairs, padded and 16-byte-misaligned operands."""
+    with dgt.Handle() as hh:
+        hh.set_tuning(dgt.TUNE_DMMA_VARIANT, variant)
+        for ta, tb in (("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")):
+            _, fro = run(hh, ta, tb, 257, 193, 131, 1.5, -0.5, seed=variant)
+            assert fro <= FRO_TOL, (variant, ta, tb)
+        _, fro = run(hh, "N", "N", 300, 64, 1000, 1.0, 0.0, seed=variant)
+        assert fro <= FRO_TOL
+        _, fro = run(hh, "N", "T", 129, 131, 77, 2.0, 1.0, pad=(1, 1, 1), offset=1)
+        assert fro <= FRO_TOL
