@@ -117,7 +117,8 @@ static bool cannon_order(int p, int c, int i, int j, int k, int* out) {
 // write distinct C); a step the grouped form does not support runs product by product.
 dgt_status run_problems_emulated(dgt_context* h, const std::vector<Problem>& probs,
                                  const std::vector<KSegment>& segs, dgt_fp64_mode mode, int slices) {
-    if (slices < 2 || slices > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+    if (!valid_slices(mode, slices))
+        return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16] (moduli: [8, 20])");
     std::vector<std::vector<const KSegment*>> steps(probs.size());
     size_t max_steps = 0;
     for (size_t i = 0; i < probs.size(); ++i) {
@@ -153,8 +154,12 @@ dgt_status run_problems_emulated(dgt_context* h, const std::vector<Problem>& pro
             }
         }
         for (const OzProblem& b : batch) {
-            dgt_status st = ozaki_dgemm(h, b.ta, b.tb, b.m, b.n, b.k, b.alpha, b.A, b.lda, b.B, b.ldb, b.beta, b.C,
-                                        b.ldc, mode, slices);
+            dgt_status st =
+                mode == DGT_FP64_OZAKI2_INT8
+                    ? ozaki2_dgemm(h, b.ta, b.tb, b.m, b.n, b.k, b.alpha, b.A, b.lda, b.B, b.ldb, b.beta, b.C, b.ldc,
+                                   slices)
+                    : ozaki_dgemm(h, b.ta, b.tb, b.m, b.n, b.k, b.alpha, b.A, b.lda, b.B, b.ldb, b.beta, b.C, b.ldc,
+                                  mode, slices);
             if (st != DGT_SUCCESS) return st;
         }
     }
@@ -225,9 +230,10 @@ dgt_status dgt_get_stream(dgt_handle_t h, dgt_stream_t* stream) {
 
 dgt_status dgt_set_fp64_mode(dgt_handle_t h, dgt_fp64_mode mode, int slices) {
     if (!h) return DGT_ERROR_NOT_INITIALIZED;
-    if (mode < DGT_FP64_NATIVE || mode > DGT_FP64_AUTO) return fail(h, DGT_ERROR_INVALID_VALUE, "unknown FP64 mode");
-    if (mode != DGT_FP64_NATIVE && (slices < 2 || slices > 16))
-        return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+    if (mode < DGT_FP64_NATIVE || mode > DGT_FP64_OZAKI2_INT8)
+        return fail(h, DGT_ERROR_INVALID_VALUE, "unknown FP64 mode");
+    if (mode != DGT_FP64_NATIVE && mode != DGT_FP64_AUTO && !valid_slices(mode, slices))
+        return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16] (moduli: [8, 20])");
     h->fp64_mode = mode;
     h->slices = slices;
     return DGT_SUCCESS;
@@ -407,7 +413,10 @@ dgt_status dgt_dgemm_ex(dgt_handle_t h, char ta, char tb, int64_t m, int64_t n, 
     h->ozaki_variant = ov;
     if (mode == DGT_FP64_NATIVE || k == 0)
         return native_single(h, ta, tb, m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc);
-    if (slices < 2 || slices > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+    if (!valid_slices(mode, slices))
+        return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16] (moduli: [8, 20])");
+    if (mode == DGT_FP64_OZAKI2_INT8)
+        return ozaki2_dgemm(h, is_trans(ta), is_trans(tb), m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc, slices);
     return ozaki_dgemm(h, is_trans(ta), is_trans(tb), m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc, mode, slices);
 }
 

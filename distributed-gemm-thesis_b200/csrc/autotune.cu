@@ -72,20 +72,31 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
     DGT_CUDA_TRY(h, cudaEventCreate(&e0));
     DGT_CUDA_TRY(h, cudaEventCreate(&e1));
     const int saved_dv = h->dmma_variant, saved_ov = h->ozaki_variant;
-    auto time_call = [&](dgt_fp64_mode md, int S, float* ms) -> dgt_status {
-        dgt_status st = DGT_SUCCESS;
-        float best = 1e30f;
-        for (int rep = 0; rep < 3; ++rep) {  // first call warms up
-            cudaEventRecord(e0, h->stream);
-            st = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc, md, S);
-            cudaEventRecord(e1, h->stream);
-            if (st != DGT_SUCCESS) return st;
-            if (cudaEventSynchronize(e1) != cudaSuccess) return cuda_fail(h, cudaGetLastError(), "autotune timing");
-            float t = 0.f;
-            cudaEventElapsedTime(&t, e0, e1);
-            if (rep > 0) best = std::min(best, t);
-        }
-        *ms = best;
+    // one timed call of the handle's current configuration
+    auto time_once = [&](dgt_fp64_mode md, int S, float* ms) -> dgt_status {
+        cudaEventRecord(e0, h->stream);
+        dgt_status st = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc, md, S);
+        cudaEventRecord(e1, h->stream);
+        if (st != DGT_SUCCESS) return st;
+        if (cudaEventSynchronize(e1) != cudaSuccess) return cuda_fail(h, cudaGetLastError(), "autotune timing");
+        cudaEventElapsedTime(ms, e0, e1);
+        return DGT_SUCCESS;
+    };
+    // Candidates run once untimed, then in ROUNDS interleaved rounds (each candidate once per
+    // round, best of the rounds), so a clock that drifts under the power cap while the tuner
+    // runs favours no candidate by its position in the list.
+    constexpr int ROUNDS = 3;
+    auto time_rounds = [&](const std::vector<int>& cands, int* knob, dgt_fp64_mode md, int S,
+                           std::vector<float>& best) -> dgt_status {
+        best.assign(cands.size(), 1e30f);
+        for (int r = 0; r < ROUNDS; ++r)
+            for (size_t c = 0; c < cands.size(); ++c) {
+                *knob = cands[c];
+                float t = 0.f;
+                dgt_status st = time_once(md, S, &t);
+                if (st != DGT_SUCCESS) return st;
+                best[c] = std::min(best[c], t);
+            }
         return DGT_SUCCESS;
     };
     // the tuner must measure raw variants, not earlier tuning decisions
@@ -94,12 +105,17 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
     dgt_status st = DGT_SUCCESS;
     TuneEntry nat{DGT_FP64_NATIVE, 0, 0, 1e30f, 0.0}, ozk{DGT_FP64_OZAKI_INT8, 0, h->slices, 1e30f, 0.0};
     if (mode != DGT_FP64_OZAKI_INT8) {
+        std::vector<int> cands;
         for (int v = 0; v < dmma_variant_count() && st == DGT_SUCCESS; ++v) {
             h->dmma_variant = v;
             float t;
-            st = time_call(DGT_FP64_NATIVE, 0, &t);
-            if (st == DGT_SUCCESS && t < nat.ms) nat = TuneEntry{DGT_FP64_NATIVE, v, 0, t, 0.0};
+            st = time_once(DGT_FP64_NATIVE, 0, &t);  // warm-up
+            cands.push_back(v);
         }
+        std::vector<float> best;
+        if (st == DGT_SUCCESS) st = time_rounds(cands, &h->dmma_variant, DGT_FP64_NATIVE, 0, best);
+        for (size_t c = 0; c < cands.size() && st == DGT_SUCCESS; ++c)
+            if (best[c] < nat.ms) nat = TuneEntry{DGT_FP64_NATIVE, cands[c], 0, best[c], 0.0};
     }
     if (st == DGT_SUCCESS && mode != DGT_FP64_NATIVE) {
         int S = h->slices;
@@ -143,10 +159,11 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
             vref = (double*)w + (size_t)m * n;  // the first m*n doubles may hold the native reference
             vsums = vref + (size_t)m * n;
         }
+        std::vector<int> cands;
         for (int v = 0; v < 5 && st == DGT_SUCCESS && S > 0; ++v) {
             h->ozaki_variant = v;
             float t;
-            st = time_call(DGT_FP64_OZAKI_INT8, S, &t);
+            st = time_once(DGT_FP64_OZAKI_INT8, S, &t);  // warm-up, and the result to check
             if (st != DGT_SUCCESS) break;
             if (v == 0) {
                 DGT_CUDA_TRY(h, cudaMemcpy2DAsync(vref, m * sizeof(double), C, ldc * sizeof(double), m * sizeof(double),
@@ -162,8 +179,12 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
                 }
                 if (hs[0] != 0.0) continue;  // not identical to variant 0
             }
-            if (t < ozk.ms) ozk = TuneEntry{DGT_FP64_OZAKI_INT8, v, S, t, ozk.rel_diff};
+            cands.push_back(v);
         }
+        std::vector<float> best;
+        if (st == DGT_SUCCESS && S > 0) st = time_rounds(cands, &h->ozaki_variant, DGT_FP64_OZAKI_INT8, S, best);
+        for (size_t c = 0; c < cands.size() && st == DGT_SUCCESS && S > 0; ++c)
+            if (best[c] < ozk.ms) ozk = TuneEntry{DGT_FP64_OZAKI_INT8, cands[c], S, best[c], ozk.rel_diff};
     }
     h->tune.swap(saved_table);
     h->dmma_variant = saved_dv;

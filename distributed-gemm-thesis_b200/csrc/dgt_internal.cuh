@@ -105,6 +105,10 @@ dgt_status device_table(dgt_context* h, int n, const void* const* parts, const s
 dgt_status ensure_workspace(dgt_context* h, size_t bytes, void** out, int slot = 0);
 
 inline bool is_trans(char t) { return t == 'T' || t == 't' || t == 'C' || t == 'c'; }
+// slices: digit slices of the Ozaki slice scheme, or moduli of the CRT scheme
+inline bool valid_slices(dgt_fp64_mode mode, int slices) {
+    return mode == DGT_FP64_OZAKI2_INT8 ? (slices >= 8 && slices <= 20) : (slices >= 2 && slices <= 16);
+}
 inline bool valid_op(char t) { return t == 'N' || t == 'n' || is_trans(t); }
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
@@ -161,6 +165,15 @@ dgt_status ozaki_dgemm_on(cudaStream_t s, int num_sms, unsigned int* err, void* 
 dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
                        const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
                        dgt_fp64_mode mode, int slices);
+
+// Per-row (or per-column) max |x| of op(A) / op(B)^T as the bit pattern of |x|, one word per
+// row; kcontig: element (mn, kk) at X[kk + mn*ld], else at X[mn + kk*ld].
+dgt_status ozaki_amax(dgt_context* h, cudaStream_t s, const double* X, int64_t ld, int64_t MN, int64_t K,
+                      bool kcontig, unsigned long long* out);
+// FP64-accurate GEMM by CRT over INT8 residues (ozaki2.cu); nmod = number of moduli.
+dgt_status ozaki2_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                        const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                        int64_t ldc, int nmod);
 
 // One product of a grouped Ozaki launch (all sizes > 0; validation is the caller's job).
 struct OzProblem {

@@ -672,4 +672,19 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     return DGT_SUCCESS;
 }
 
+
+dgt_status ozaki_amax(dgt_context* h, cudaStream_t s, const double* X, int64_t ld, int64_t MN, int64_t K,
+                      bool kcontig, unsigned long long* out) {
+    if (kcontig) {
+        oz::amax_k_contig<<<(unsigned)ceil_div(MN, 8), 256, 0, s>>>(X, ld, MN, K, out);
+    } else {
+        DGT_CUDA_TRY(h, cudaMemsetAsync(out, 0, (size_t)MN * 8, s));
+        dim3 grid((unsigned)ceil_div(MN, 256), (unsigned)ceil_div(K, oz::AMAX_KCHUNK));
+        oz::amax_mn_contig<<<grid, 256, 0, s>>>(X, ld, MN, K, oz::AMAX_KCHUNK, out);
+    }
+    if (h) h->launches.fetch_add(1);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DGT_SUCCESS : cuda_fail(h, e, "ozaki amax");
+}
+
 }  // namespace dgt

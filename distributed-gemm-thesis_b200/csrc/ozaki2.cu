@@ -1,0 +1,448 @@
+// FP64-accurate GEMM by the Chinese remainder theorem over INT8 residues (Ozaki scheme II:
+// Ozaki, Uchino, Imamura 2025, "Ozaki Scheme II: A GEMM-oriented emulation of
+// floating-point matrix multiplication using an integer modular technique").
+//
+//   1. Scale: row i of op(A) gets e_i with max_k |a_ik| in [2^(e_i-1), 2^e_i), column j of
+//      op(B) gets f_j likewise; A'_ik = trunc(a_ik 2^(beta-e_i)) and B'_kj = trunc(b_kj
+//      2^(beta-f_j)) are integers below 2^beta in magnitude (exact in FP64 for beta <= 58).
+//   2. Residues: for N pairwise coprime moduli p <= 256 with P = prod p > 2 k 2^(2 beta),
+//      A' mod p and B' mod p in the symmetric range [-(p/2), (p-1)/2] are INT8 planes.
+//   3. Multiply: (A' mod p)(B' mod p) is exact in INT32 (|sum| <= k 128^2 < 2^31) on the
+//      tcgen05 INT8 tensor cores -- one GEMM per modulus, N in all -- and its epilogue keeps
+//      only the residue of each element modulo p (one byte).
+//   4. Reconstruct: C'_ij = sum_p r_p W_p mod P (W_p = (P/p) ((P/p)^-1 mod p)), taken in
+//      the symmetric range, equals (A'B')_ij exactly; it is rounded once to FP64 (correctly)
+//      and scaled by 2^(e_i + f_j - 2 beta).  C = alpha C' + beta_C C.
+//
+// Against the slice scheme (ozaki.cu), N GEMMs replace S(S+1)/2 digit products for the
+// same number of operand bits (N = 17 moduli: beta = 58 bits at K <= 16384, versus 36
+// products for S = 8 slices of 7 bits), and the output is read and written once instead of
+// once per flush group.  The FLOP count reported for this path is 2*M*N*K.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "dgt_internal.cuh"
+#include "tc_engine.cuh"
+
+namespace dgt {
+namespace oz2 {
+
+constexpr int MAX_MODULI = 20, MIN_MODULI = 8;
+constexpr int NL = 6;          // 32-bit limbs of the CRT arithmetic (P < 2^160, sums < 2^192)
+constexpr int MAX_BETA = 58;   // |A'| < 2^58: residues by FP64 division stay exact
+// Pairwise coprime, largest first (greedy from 256 down).
+constexpr int kModuli[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                                     223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+
+struct ModTable {
+    int32_t p[MAX_MODULI];
+    double inv[MAX_MODULI];
+};
+
+struct CrtConst {
+    int32_t n;
+    uint32_t W[MAX_MODULI][NL];
+    uint32_t P[NL], Phalf[NL];  // Phalf = floor((P - 1) / 2)
+    double inv_P;               // 1 / P, rounded
+};
+
+// ---- host: CRT constants in 32-bit limbs ------------------------------------------------------
+using Big = std::vector<uint32_t>;  // little-endian limbs
+
+static void big_mul_small(Big& a, uint32_t m) {
+    uint64_t c = 0;
+    for (auto& x : a) {
+        const uint64_t t = (uint64_t)x * m + c;
+        x = (uint32_t)t;
+        c = t >> 32;
+    }
+    if (c) a.push_back((uint32_t)c);
+}
+
+static uint32_t big_div_small(Big& a, uint32_t d) {  // a /= d, returns a mod d
+    uint64_t r = 0;
+    for (size_t i = a.size(); i-- > 0;) {
+        const uint64_t cur = (r << 32) | a[i];
+        a[i] = (uint32_t)(cur / d);
+        r = cur % d;
+    }
+    while (a.size() > 1 && a.back() == 0) a.pop_back();
+    return (uint32_t)r;
+}
+
+static uint32_t inv_mod(uint32_t a, uint32_t p) {  // a^-1 mod p (gcd(a, p) = 1)
+    int64_t t = 0, nt = 1, r = p, nr = a % p;
+    while (nr) {
+        const int64_t q = r / nr;
+        std::swap(t, nt);
+        nt -= q * t;
+        std::swap(r, nr);
+        nr -= q * r;
+    }
+    return (uint32_t)(t < 0 ? t + p : t);
+}
+
+static double log2_product(int n) {
+    double s = 0;
+    for (int i = 0; i < n; ++i) s += std::log2((double)kModuli[i]);
+    return s;
+}
+
+// Largest beta with 2 k (2^beta - 1)^2 < P (with a 1e-9 margin on the logarithms).
+static int beta_for(int n, int64_t k) {
+    const double b = (log2_product(n) - 1.0 - std::log2((double)std::max<int64_t>(k, 1))) / 2.0 - 1e-9;
+    return std::min(MAX_BETA, (int)std::floor(b));
+}
+
+static void crt_constants(int n, CrtConst& cc, ModTable& mt) {
+    cc = CrtConst{};
+    mt = ModTable{};
+    cc.n = n;
+    Big P{1};
+    for (int i = 0; i < n; ++i) big_mul_small(P, (uint32_t)kModuli[i]);
+    for (int i = 0; i < n; ++i) {
+        const uint32_t p = (uint32_t)kModuli[i];
+        mt.p[i] = (int32_t)p;
+        mt.inv[i] = 1.0 / (double)p;
+        Big M = P;
+        big_div_small(M, p);  // M = P / p
+        Big Mm = M;
+        const uint32_t m_mod = big_div_small(Mm, p);
+        big_mul_small(M, inv_mod(m_mod, p));  // W = M * (M^-1 mod p) < P
+        for (int l = 0; l < NL; ++l) cc.W[i][l] = l < (int)M.size() ? M[l] : 0;
+    }
+    for (int l = 0; l < NL; ++l) cc.P[l] = l < (int)P.size() ? P[l] : 0;
+    Big H = P;  // floor((P - 1) / 2)
+    for (size_t l = 0; l < H.size(); ++l) {  // H -= 1 (P > 1)
+        if (H[l]--) break;
+    }
+    big_div_small(H, 2);
+    for (int l = 0; l < NL; ++l) cc.Phalf[l] = l < (int)H.size() ? H[l] : 0;
+    double pd = 0;
+    for (int l = NL - 1; l >= 0; --l) pd = pd * 4294967296.0 + (double)cc.P[l];
+    cc.inv_P = 1.0 / pd;
+}
+
+// ---- device: residue planes ----------------------------------------------------------------------
+// Plane j holds (A' mod p_j) in the symmetric range as int8 at [j][mn][kk] (K-major, row
+// length k_pad, mn_pad rows, zero padded).  Each thread produces 32 consecutive kk of one mn;
+// the by == 0 blocks also write exps[mn].
+template <bool K_CONTIG>
+__global__ void __launch_bounds__(128) split_residues(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                                      int64_t mn_pad, int64_t k_pad, int nmod, int beta,
+                                                      const unsigned long long* __restrict__ amax,
+                                                      int32_t* __restrict__ exps, int8_t* __restrict__ planes,
+                                                      const __grid_constant__ ModTable mt) {
+    const int64_t mn = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t k0 = (int64_t)blockIdx.y * 32;
+    if (mn >= mn_pad) return;
+    int e = 0;
+    if (mn < MN) {
+        e = oz::exponent_of_max(amax[mn]);
+        if (blockIdx.y == 0) exps[mn] = e;
+    }
+    const bool live = (mn < MN) && (e != oz::EXP_NONFINITE);
+    double v[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        const int64_t kk = k0 + i;
+        double x = 0.0;
+        if (live && kk < K) x = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
+        v[i] = live ? trunc(oz::scale2(x, beta - e)) : 0.0;  // an integer, |v| < 2^beta
+    }
+    const int64_t plane = mn_pad * k_pad;
+    for (int j = 0; j < nmod; ++j) {
+        const double p = (double)mt.p[j], inv = mt.inv[j];
+        const double lo = -(double)(mt.p[j] >> 1), hi = (double)((mt.p[j] - 1) >> 1);
+        uint32_t w[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) w[q] = 0;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            // |v / p| < 2^51, so rint(v * inv) is the nearest quotient or one off, and the
+            // remainder fma(-q, p, v) is an integer below 2^10: exact
+            double r = fma(-rint(v[i] * inv), p, v[i]);
+            if (r > hi) r -= p;
+            if (r > hi) r -= p;
+            if (r < lo) r += p;
+            if (r < lo) r += p;
+            w[i >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)r) << (8 * (i & 3));
+        }
+        uint4* o4 = reinterpret_cast<uint4*>(planes + j * plane + mn * k_pad + k0);
+        o4[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        o4[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    }
+}
+
+// ---- device: reconstruction -----------------------------------------------------------------------
+// X = sum_j r_j W_j reduced mod P into the symmetric range, rounded to FP64 once (round to
+// nearest even), times 2^shift.  r_j is byte `sel` of rr[j].  Every loop has a constant trip
+// count so the limbs stay in registers.
+__device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
+                                            int shift) {
+    uint64_t acc[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) acc[l] = 0;
+#pragma unroll
+    for (int j = 0; j < MAX_MODULI; ++j) {
+        if (j < cc.n) {
+            const uint64_t r = (rr[j] >> (8 * sel)) & 0xffu;
+#pragma unroll
+            for (int l = 0; l < NL; ++l) acc[l] += r * cc.W[j][l];  // < 20 * 2^40
+        }
+    }
+    uint32_t x[NL];
+    uint64_t c = 0;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        const uint64_t t = acc[l] + c;
+        x[l] = (uint32_t)t;
+        c = t >> 32;
+    }
+    // X < 20 * 256 * P < 2^13 P: q = floor(X / P) from the top limbs, exact or one off
+    const double xd = ldexp((double)x[5], 160) + ldexp((double)x[4], 128) + ldexp((double)x[3], 96) +
+                      ldexp((double)x[2], 64);
+    const uint32_t q = (uint32_t)floor(xd * cc.inv_P);
+    c = 0;
+    int64_t b = 0;  // X -= q P, borrow in b
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        const uint64_t t = (uint64_t)q * cc.P[l] + c;
+        c = t >> 32;
+        const int64_t d = (int64_t)x[l] - (int64_t)(uint32_t)t + b;
+        x[l] = (uint32_t)d;
+        b = d >> 32;
+    }
+    bool ge_P = true;  // X >= P (only meaningful when b == 0)
+    bool decided = false;
+#pragma unroll
+    for (int l = NL - 1; l >= 0; --l) {
+        if (!decided && x[l] != cc.P[l]) {
+            ge_P = x[l] > cc.P[l];
+            decided = true;
+        }
+    }
+    const int64_t sgn = b < 0 ? 1 : (ge_P ? -1 : 0);  // q one too large / one too small
+    int64_t cc2 = 0;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        const int64_t d = (int64_t)x[l] + sgn * (int64_t)cc.P[l] + cc2;
+        x[l] = (uint32_t)d;
+        cc2 = d >> 32;
+    }
+    // symmetric range: X > floor((P-1)/2) stands for X - P; work with the magnitude
+    bool above = false;
+    decided = false;
+#pragma unroll
+    for (int l = NL - 1; l >= 0; --l) {
+        if (!decided && x[l] != cc.Phalf[l]) {
+            above = x[l] > cc.Phalf[l];
+            decided = true;
+        }
+    }
+    if (above) {  // magnitude P - X
+        int64_t bb = 0;
+#pragma unroll
+        for (int l = 0; l < NL; ++l) {
+            const int64_t d = (int64_t)cc.P[l] - (int64_t)x[l] + bb;
+            x[l] = (uint32_t)d;
+            bb = d >> 32;
+        }
+    }
+    int L = 0;
+#pragma unroll
+    for (int l = 1; l < NL; ++l)
+        if (x[l] != 0u) L = l;
+    uint32_t a2 = 0, a1 = 0, a0 = 0;
+    bool sticky = false;
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        if (l == L) a2 = x[l];
+        if (l == L - 1) a1 = x[l];
+        if (l == L - 2) a0 = x[l];
+        if (l < L - 2 && x[l] != 0u) sticky = true;
+    }
+    if (a2 == 0u) return 0.0;
+    const int lz = __clz(a2);
+    const uint64_t top = ((uint64_t)a2 << 32) | a1;
+    const uint64_t top64 = lz ? (top << lz) | (uint64_t)(a0 >> (32 - lz)) : top;
+    sticky |= lz ? (uint32_t)(a0 << lz) != 0u : a0 != 0u;
+    // top64 carries the leading 64 bits; its bit 0 absorbs the rest as a sticky bit, so the
+    // one rounding to 53 bits is correct (round to nearest even)
+    const double d = __ull2double_rn(top64 | (uint64_t)sticky);
+    const double mag = oz::scale2(d, 32 * (L - 1) - lz + shift);
+    return above ? -mag : mag;
+}
+
+// Thread per 4 consecutive rows of one column of C; residue planes [j][col][row] with
+// leading dimension res_ld (a multiple of 4).
+__global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
+                                                       int64_t res_plane, int64_t m, int64_t n,
+                                                       const int32_t* __restrict__ row_exp,
+                                                       const int32_t* __restrict__ col_exp, int beta, double alpha,
+                                                       double beta_c, double* __restrict__ C, int64_t ldc,
+                                                       const __grid_constant__ CrtConst cc) {
+    const int64_t quads = (m + 3) / 4;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= quads * n) return;
+    const int64_t col = idx / quads, row0 = (idx % quads) * 4;
+    uint32_t rr[MAX_MODULI];  // four rows' residues per modulus, one byte each
+#pragma unroll
+    for (int j = 0; j < MAX_MODULI; ++j)
+        rr[j] = j < cc.n ? *reinterpret_cast<const uint32_t*>(res + j * res_plane + col * res_ld + row0) : 0u;
+    const int f = col_exp[col];
+#pragma unroll
+    for (int e4 = 0; e4 < 4; ++e4) {
+        const int64_t row = row0 + e4;
+        if (row >= m) break;
+        const int e = row_exp[row];
+        double val;
+        if (e == oz::EXP_NONFINITE || f == oz::EXP_NONFINITE)
+            val = __longlong_as_double(0x7ff8000000000000ll);
+        else
+            val = crt_value(rr, e4, cc, e + f - 2 * beta);
+        double* cp = C + row + col * ldc;
+        *cp = beta_c != 0.0 ? fma(alpha, val, beta_c * *cp) : alpha * val;
+    }
+}
+
+}  // namespace oz2
+
+// ---- host orchestration ------------------------------------------------------------------------
+
+template <class CF>
+static cudaError_t launch_residue_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const oz::Params& prm,
+                                       int num_sms, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(oz::digit_gemm<CF, 0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)CF::SMEM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int tiles = prm.tiles_m * prm.tiles_n;
+    if constexpr (CF::PAIR) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(2 * std::min(tiles, num_sms / 2)));
+        cfg.blockDim = dim3(CF::THREADS);
+        cfg.dynamicSmemBytes = CF::SMEM;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, oz::digit_gemm<CF, 0, 2>, tmA, tmB, prm);
+    } else {
+        oz::digit_gemm<CF, 0, 2><<<std::min(tiles, num_sms), CF::THREADS, CF::SMEM, s>>>(tmA, tmB, prm);
+        return cudaGetLastError();
+    }
+}
+
+dgt_status ozaki2_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                        const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
+                        int64_t ldc, int nmod) {
+    using namespace oz2;
+    if (nmod < MIN_MODULI || nmod > MAX_MODULI)
+        return fail(h, DGT_ERROR_INVALID_VALUE, "modulus count must be in [8, 20]");
+    const int bits = beta_for(nmod, k);
+    if (bits < 8) return fail(h, DGT_ERROR_UNSUPPORTED, "K too long for this modulus count");
+    // kernel variant: 0 (4 epilogue warps), 4 (CTA pair) or 1 (8 warps); all 128-byte stages
+    const int variant = (h->ozaki_variant == 0 || h->ozaki_variant == 4) ? h->ozaki_variant : 1;
+    const bool pair = variant == 4;
+    const int tkb = 128;
+    const int64_t m_unit = pair ? 2 * oz::TM : oz::TM;
+    const int64_t m_pad = ceil_div(m, m_unit) * m_unit, n_pad = ceil_div(n, oz::TN) * oz::TN;
+    const int64_t k_pad = ceil_div(k, oz::KPAD) * oz::KPAD;
+    if (k_pad >= (int64_t)1 << 17)  // k_pad * 128^2 must stay below 2^31
+        return fail(h, DGT_ERROR_UNSUPPORTED, "K too long for exact INT32 residue products");
+    if ((int64_t)nmod * std::max(m_pad, n_pad) > INT32_MAX)
+        return fail(h, DGT_ERROR_UNSUPPORTED, "matrix too large for 32-bit TMA coordinates");
+    auto up = [](size_t x) { return (x + 1023) / 1024 * 1024; };
+    const size_t pa = up((size_t)nmod * m_pad * k_pad), pb = up((size_t)nmod * n_pad * k_pad);
+    const size_t xa = up((size_t)m * 8), xb = up((size_t)n * 8), ea = up((size_t)m * 4), eb = up((size_t)n * 4);
+    const size_t rs = up((size_t)nmod * m_pad * n_pad);
+    void* ws = nullptr;
+    dgt_status st = ensure_workspace(h, pa + pb + xa + xb + ea + eb + rs, &ws, 0);
+    if (st != DGT_SUCCESS) return st;
+    char* p = (char*)ws;
+    int8_t* planesA = (int8_t*)p;
+    int8_t* planesB = (int8_t*)(p + pa);
+    auto* amaxA = (unsigned long long*)(p + pa + pb);
+    auto* amaxB = (unsigned long long*)(p + pa + pb + xa);
+    auto* expA = (int32_t*)(p + pa + pb + xa + xb);
+    auto* expB = (int32_t*)(p + pa + pb + xa + xb + ea);
+    auto* res = (uint8_t*)(p + pa + pb + xa + xb + ea + eb);
+
+    CrtConst cc;
+    ModTable mt;
+    crt_constants(nmod, cc, mt);
+    cudaStream_t s = h->stream;
+    mark(h, 0);
+    // op(A) is m x k: 'N' -> MN-contiguous; op(B) as its transpose n x k: 'N' -> K-contiguous
+    if ((st = ozaki_amax(h, s, A, lda, m, k, ta, amaxA)) != DGT_SUCCESS) return st;
+    if ((st = ozaki_amax(h, s, B, ldb, n, k, !tb, amaxB)) != DGT_SUCCESS) return st;
+    auto split = [&](const double* X, int64_t ld, int64_t MN, int64_t mn_pad, bool kcontig,
+                     const unsigned long long* am, int32_t* ex, int8_t* planes) -> dgt_status {
+        dim3 grid((unsigned)ceil_div(mn_pad, 128), (unsigned)(k_pad / 32));
+        if (kcontig)
+            split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, k, mn_pad, k_pad, nmod, bits, am, ex, planes, mt);
+        else
+            split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, k, mn_pad, k_pad, nmod, bits, am, ex, planes, mt);
+        h->launches.fetch_add(1);
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? DGT_SUCCESS : cuda_fail(h, e, "residue split");
+    };
+    if ((st = split(A, lda, m, m_pad, ta, amaxA, expA, planesA)) != DGT_SUCCESS) return st;
+    if ((st = split(B, ldb, n, n_pad, !tb, amaxB, expB, planesB)) != DGT_SUCCESS) return st;
+
+    CUtensorMap tmA, tmB;
+    if (!oz::make_plane_map(&tmA, planesA, (int64_t)nmod * m_pad, k_pad, oz::TM, tkb) ||
+        !oz::make_plane_map(&tmB, planesB, (int64_t)nmod * n_pad, k_pad, pair ? oz::TN / 2 : oz::TN, tkb))
+        return fail(h, DGT_ERROR_CUDA, "cuTensorMapEncodeTiled failed");
+    static thread_local oz::Params prm;
+    prm = oz::Params{};
+    prm.m = m;
+    prm.n = n;
+    prm.ldc = m_pad;
+    prm.m_pad = (int32_t)m_pad;
+    prm.n_pad = (int32_t)n_pad;
+    prm.tiles_m = (int32_t)(m_pad / m_unit);
+    prm.tiles_n = (int32_t)(n_pad / oz::TN);
+    prm.ngroups = nmod;
+    for (int j = 0; j < nmod; ++j) {  // one group per modulus: the residue product over all of K
+        prm.segs[j] = oz::Seg{j, j, 0, (int32_t)(k_pad / tkb)};
+        prm.groups[j] = oz::Group{j, j + 1, 0, mt.p[j]};
+    }
+    prm.res = res;
+    prm.res_ld = m_pad;
+    prm.res_plane = m_pad * n_pad;
+    prm.err = h->dev_error;
+    mark(h, 1);
+    cudaError_t le;
+    if (variant == 4)
+        le = launch_residue_gemm<oz::OzCfg<8, 128, 6, true>>(tmA, tmB, prm, h->num_sms, s);
+    else if (variant == 0)
+        le = launch_residue_gemm<oz::OzCfg<4, 128, 4>>(tmA, tmB, prm, h->num_sms, s);
+    else
+        le = launch_residue_gemm<oz::OzCfg<8, 128, 4>>(tmA, tmB, prm, h->num_sms, s);
+    h->launches.fetch_add(1);
+    if (le != cudaSuccess) return cuda_fail(h, le, "residue GEMM launch");
+    mark(h, 2);
+    const int64_t threads = ceil_div(m, 4) * n;
+    crt_reconstruct<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits,
+                                                                     alpha, beta, C, ldc, cc);
+    h->launches.fetch_add(1);
+    DGT_CUDA_TRY(h, cudaGetLastError());
+    return DGT_SUCCESS;
+}
+
+}  // namespace dgt

@@ -67,6 +67,10 @@ struct Params {
     unsigned int* err;
     float* Cf;  // FP32 output (EPI_MODE 1)
     float alpha_f, beta_f;
+    // EPI_MODE 2: group g's accumulator reduced modulo its modulus (Group::pad) is stored as
+    // one byte per element at res[g * res_plane + row + col * res_ld]
+    uint8_t* res;
+    int64_t res_ld, res_plane;
     // The schedule travels inside the launch's parameters (so a captured CUDA graph needs
     // no host-to-device copy); MAX_SEGS / MAX_GROUPS keep the block under 32 KB.
     Seg segs[640];
@@ -301,7 +305,8 @@ __device__ __forceinline__ int exponent_of_max(unsigned long long bits) {
 
 // KIND: 0 = INT8 digits (kind::i8, INT32 accumulator), 1 = BF16 operands (kind::f16, FP32
 // accumulator).  EPI: 0 = FP64 fold C = beta*C + alpha*sum_g 2^(e_i+f_j-7d_g) P_g,
-// 1 = FP32 output C = alpha*acc + beta*C (a single flush group).
+// 1 = FP32 output C = alpha*acc + beta*C (a single flush group), 2 = residues: each group's
+// INT32 accumulator modulo the group's modulus, one byte per element (CRT emulation).
 template <class CF, int KIND, int EPI_MODE, bool GROUPED = false>
 __global__ void __launch_bounds__(CF::THREADS, 1)
     digit_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -564,6 +569,23 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                     if (!row_ok) continue;
                     const int64_t rem_cols = DGT_TILE_FIELD(cx, n, n) - (n0 + ch * 32);
                     const int ncols = rem_cols < 32 ? (int)rem_cols : 32;
+                    if constexpr (EPI_MODE == 2) {
+                        // exact: |acc| < 2^31, so (double)acc / p floors to q or q - 1 at worst
+                        const int pm = GROUPS[g].pad;
+                        const double inv = 1.0 / (double)pm;
+                        uint8_t* rbase = P.res + (int64_t)g * P.res_plane + row + (n0 + ch * 32) * P.res_ld;
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) {
+                            if (c < ncols) {
+                                const int32_t x = (int32_t)v[c];
+                                int r = x - pm * (int)floor((double)x * inv);
+                                if (r < 0) r += pm;
+                                if (r >= pm) r -= pm;
+                                rbase[c * P.res_ld] = (uint8_t)r;
+                            }
+                        }
+                        continue;
+                    }
                     if constexpr (EPI_MODE == 1) {
                         float* fbase = P.Cf + row + (n0 + ch * 32) * P.ldc;
                         float prevf[32];

@@ -404,3 +404,94 @@ def digits_of_accuracy(ref_vals, vals):
         acc += 1
         failed = bool((err > eps).any())
     return 0 if acc == 8 else acc
+
+
+# ---- exact restatement of the CRT FP64 emulation (Ozaki scheme II) ------------------------------
+# Ozaki, Uchino, Imamura 2025 ("Ozaki Scheme II: A GEMM-oriented emulation of floating-point
+# matrix multiplication using an integer modular technique").  The product's path
+# (distributed-gemm-thesis_b200/csrc/ozaki2.cu) must agree with this bit for bit for
+# alpha = 1, beta = 0 away from subnormal results: the integer product A'B' is exact in both,
+# and both round it to FP64 once, to nearest even.
+OZAKI2_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                 223, 217, 211, 199, 197, 193, 191, 181, 179, 173)
+
+
+def ozaki2_beta(nmod: int, k: int) -> int:
+    """Operand bits for nmod moduli and inner dimension k: the largest beta (capped at 58)
+    with 2 k (2^beta - 1)^2 < P, chosen from logarithms with a 1e-9 margin."""
+    import math
+
+    lg = 0.0
+    for p in OZAKI2_MODULI[:nmod]:
+        lg += math.log2(float(p))
+    b = (lg - 1.0 - math.log2(float(max(k, 1)))) / 2.0 - 1e-9
+    return min(58, math.floor(b))
+
+
+def _exp_of_max(v: float) -> int:
+    """e with v in [2^(e-1), 2^e) (0 for v == 0)."""
+    import math
+
+    return 0 if v == 0.0 else math.frexp(v)[1]
+
+
+def ozaki2_exact(A, B, nmod: int, ta: str = "N", tb: str = "N"):
+    """C = op(A) op(B) as the CRT emulation computes it: operands scaled per row of op(A) /
+    column of op(B) to beta-bit integers (truncated), their integer product taken exactly,
+    rounded once to FP64 and scaled back.  Pure Python integers: small sizes only."""
+    import math
+
+    Aop, Bop = op(A, ta), op(B, tb)
+    m, k = Aop.shape
+    n = Bop.shape[1]
+    beta = ozaki2_beta(nmod, k)
+    P = 1
+    for p in OZAKI2_MODULI[:nmod]:
+        P *= p
+    assert 2 * k * (2 ** beta - 1) ** 2 < P  # the CRT range covers every product
+    ea = [_exp_of_max(float(np.max(np.abs(Aop[i, :])))) if k else 0 for i in range(m)]
+    fb = [_exp_of_max(float(np.max(np.abs(Bop[:, j])))) if k else 0 for j in range(n)]
+    Ai = [[int(math.trunc(math.ldexp(float(Aop[i, t]), beta - ea[i]))) for t in range(k)] for i in range(m)]
+    Bi = [[int(math.trunc(math.ldexp(float(Bop[t, j]), beta - fb[j]))) for t in range(k)] for j in range(n)]
+    C = np.empty((m, n))
+    for i in range(m):
+        for j in range(n):
+            exact = sum(a * b for a, b in zip(Ai[i], Bi[j]))
+            C[i, j] = math.ldexp(float(exact), ea[i] + fb[j] - 2 * beta)
+    return C
+
+
+def ozaki2_residue_check(A, B, nmod: int):
+    """The CRT identity the kernels rely on, checked in integers: residues of the scaled
+    operands in the symmetric ranges, their products reduced mod each p, recombined with
+    W_p = (P/p)((P/p)^-1 mod p) and centred, give the exact integer product."""
+    import math
+
+    m, k = A.shape
+    n = B.shape[1]
+    beta = ozaki2_beta(nmod, k)
+    mods = OZAKI2_MODULI[:nmod]
+    P = math.prod(mods)
+    ea = [_exp_of_max(float(np.max(np.abs(A[i, :])))) for i in range(m)]
+    fb = [_exp_of_max(float(np.max(np.abs(B[:, j])))) for j in range(n)]
+    Ai = np.array([[int(math.trunc(math.ldexp(float(A[i, t]), beta - ea[i]))) for t in range(k)]
+                   for i in range(m)], dtype=object)
+    Bi = np.array([[int(math.trunc(math.ldexp(float(B[t, j]), beta - fb[j]))) for j in range(n)]
+                   for t in range(k)], dtype=object)
+
+    def sym(x, p):
+        r = x % p
+        return r - p if r > (p - 1) // 2 else r
+
+    X = np.zeros((m, n), dtype=object)
+    for p in mods:
+        ra = np.vectorize(lambda x: sym(x, p), otypes=[np.int64])(Ai)
+        rb = np.vectorize(lambda x: sym(x, p), otypes=[np.int64])(Bi)
+        assert ra.min() >= -(p // 2) and ra.max() <= (p - 1) // 2
+        g = (ra @ rb) % p  # exact in int64 for these sizes
+        Mp = P // p
+        W = Mp * pow(Mp % p, -1, p)
+        X = X + g.astype(object) * W
+    X = np.vectorize(lambda x: x % P, otypes=[object])(X)
+    X = np.vectorize(lambda x: x - P if x > (P - 1) // 2 else x, otypes=[object])(X)
+    return X, Ai.dot(Bi)
