@@ -4,9 +4,11 @@ vs native FP64 DMMA, at equal error against the host FP64 oracle.
 Workload (the FP64-emulation configuration): C = alpha*A*B + beta*C with
 M = N = K = 16384, column-major, entries (U[0,1) - 0.5) * exp(phi * N(0,1)), phi = 0.5
 (phi = 4.0 is measured for error only: the kernels are data-independent), seeded
-synthetic data.  One step = one dgt_dgemm call through the C ABI.  The slice count is
-the smallest S whose max/Frobenius relative error vs the oracle is <= the native DMMA
-kernel's ("equal error").  Inputs (2 GiB each) are larger than L2, so no flush is needed.
+synthetic data.  One step = one dgt_dgemm call through the C ABI.  Two emulation schemes
+compete: CRT over INT8 residues (count = moduli) and INT8 digit slices (count = slices);
+each takes the smallest count whose max- and Frobenius-relative errors vs the oracle are
+<= the native DMMA kernel's ("equal error"), and the faster one is the headline (the
+other is reported beside it).  Inputs (2 GiB each) are larger than L2, so no flush.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -41,7 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dgt", choices=["dgt", "reference"])
     ap.add_argument("--size", type=int, default=SIZE)
-    ap.add_argument("--path", default="ozaki", choices=["native", "ozaki", "sgemm", "pack"],
+    ap.add_argument("--path", default="ozaki", choices=["native", "ozaki", "ozaki2", "sgemm", "pack"],
                     help="--workload once: which path to call")
     ap.add_argument("--variant", type=int, default=-1, help="--workload once: kernel variant (-1: default)")
     ap.add_argument("--slices", type=int, default=8, help="--workload once: Ozaki slice count")
@@ -354,8 +356,8 @@ def _ozaki_inputs(n, seed, phi, k=None):
 
 def workload_precision(args):
     """FP64 emulation at M = N = K = 16384 for phi in {0.5, 4.0}: native DMMA, INT8 slices
-    4..8 (and 9, 10 for phi = 4), BF16 slices 7 and 8; error vs the host FP64 GEMM on 48
-    sampled rows; whole-call TFLOP/s (split + GEMM)."""
+    4..8 (and 9, 10 for phi = 4), CRT with 12..17 moduli, BF16 slices 7 and 8; error vs the
+    host FP64 GEMM on 48 sampled rows; whole-call TFLOP/s (split + GEMM + reconstruction)."""
     import numpy as np
 
     torch, dgt, h = _setup()
@@ -373,6 +375,7 @@ def workload_precision(args):
         runs = [("native", dgt.FP64_NATIVE, 0)] + [(f"int8_s{S}", dgt.FP64_OZAKI_INT8, S) for S in (4, 5, 6, 7, 8)]
         if phi > 1:
             runs += [(f"int8_s{S}", dgt.FP64_OZAKI_INT8, S) for S in (9, 10)]
+        runs += [(f"crt_n{N}", dgt.FP64_OZAKI2_INT8, N) for N in (12, 13, 14, 15, 16, 17)]
         runs += [(f"bf16_s{S}", dgt.FP64_OZAKI_BF16, S) for S in (7, 8)]
         for name, mode, S in runs:
             f = lambda: h.dgemm("N", "N", n, n, n, 1.0, dA.data_ptr(), n, dB.data_ptr(), n, 0.0, dC.data_ptr(), n,
@@ -567,8 +570,8 @@ def workload_batching(args):
 
 def workload_once(args):
     """Two calls of one path at --size (the first warms up), for profiler captures: native
-    DGEMM, Ozaki INT8 DGEMM (--slices), 3xBF16 SGEMM, or a 4x4 block-cyclic pack with
-    256 blocks.  Prints the second call's CUDA-event time."""
+    DGEMM, Ozaki INT8 DGEMM (--slices = slices), CRT INT8 DGEMM (--slices = moduli), 3xBF16
+    SGEMM, or a 4x4 block-cyclic pack with 256 blocks.  Prints the second call's time."""
     import numpy as np
 
     torch, dgt, h = _setup()
@@ -596,7 +599,7 @@ def workload_once(args):
         A = torch.rand((n, n), dtype=torch.float64, device="cuda", generator=g) - 0.5
         B = torch.rand((n, n), dtype=torch.float64, device="cuda", generator=g) - 0.5
         C = torch.zeros((n, n), dtype=torch.float64, device="cuda")
-        mode = dgt.FP64_NATIVE if args.path == "native" else dgt.FP64_OZAKI_INT8
+        mode = {"native": dgt.FP64_NATIVE, "ozaki": dgt.FP64_OZAKI_INT8, "ozaki2": dgt.FP64_OZAKI2_INT8}[args.path]
         f = lambda: h.dgemm("N", "N", n, n, n, 1.0, A.data_ptr(), n, B.data_ptr(), n, 0.0, C.data_ptr(), n,
                             mode=mode, slices=args.slices)
         flops = 2.0 * n ** 3
@@ -670,20 +673,34 @@ def main():
     run(dgt.FP64_NATIVE, 0, C_nat.data_ptr())
     torch.cuda.synchronize()
     nat_err = rows_err(C_nat)
-    chosen, errs = None, {}
-    for S in (6, 7, 8):
-        run(dgt.FP64_OZAKI_INT8, S)
-        torch.cuda.synchronize()
-        h.check_device()
-        errs[S] = rows_err(C)
-        if chosen is None and errs[S][0] <= nat_err[0] and errs[S][1] <= nat_err[1]:
-            chosen = S
-    equal_error = chosen is not None
-    S = chosen if chosen is not None else 8
-    # kernel variants for this shape: the library's autotuner (CUDA events, caller's buffers)
-    h.set_tuning(dgt.TUNE_OZAKI_SLICES, S)
+    # Two emulation schemes are candidates: CRT over INT8 residues (count = moduli) and INT8
+    # digit slices (count = slices).  For each, the smallest count whose max- and Frobenius-
+    # relative errors are both <= the native kernel's ("equal error"); the faster of the two
+    # (after tuning kernel variants) is the headline.
+    schemes = {"crt": (dgt.FP64_OZAKI2_INT8, (14, 15, 16, 17)), "slices": (dgt.FP64_OZAKI_INT8, (6, 7, 8))}
+    errs, chosen = {}, {}
+    for name, (mode, counts) in schemes.items():
+        for cnt in counts:
+            run(mode, cnt)
+            torch.cuda.synchronize()
+            h.check_device()
+            errs[(name, cnt)] = rows_err(C)
+            e = errs[(name, cnt)]
+            if name not in chosen and e[0] <= nat_err[0] and e[1] <= nat_err[1]:
+                chosen[name] = cnt
+    equal_error = bool(chosen)
+    for name, (mode, counts) in schemes.items():
+        chosen.setdefault(name, counts[-1])
+    # kernel variants per scheme for this shape: the library's autotuner (CUDA events)
     tuned_native = h.autotune("N", "N", n, n, n, pa, n, pb, n, C_nat.data_ptr(), n, mode=dgt.FP64_NATIVE)
-    tuned_emu = h.autotune("N", "N", n, n, n, pa, n, pb, n, pc, n, mode=dgt.FP64_OZAKI_INT8)
+    tuned, scheme_ms = {}, {}
+    for name, (mode, _) in schemes.items():
+        h.set_tuning(dgt.TUNE_OZAKI_SLICES, chosen[name])
+        tuned[name] = h.autotune("N", "N", n, n, n, pa, n, pb, n, pc, n, mode=mode)
+        scheme_ms[name] = tuned[name]["ms"]
+    eligible = [nm for nm in schemes if (lambda e: e[0] <= nat_err[0] and e[1] <= nat_err[1])(errs[(nm, chosen[nm])])]
+    best = min(eligible or list(schemes), key=lambda nm: scheme_ms[nm])
+    MODE, S = schemes[best][0], chosen[best]
     # phi = 4.0 error (same kernels; data-dependent accuracy only)
     A4 = O.ozaki_matrix((n, 2048), SEED + 99, 4.0)
     B4 = O.ozaki_matrix((2048, 1024), SEED + 98, 4.0)
@@ -692,12 +709,13 @@ def main():
     dC4 = torch.zeros((1024, n), dtype=torch.float64, device="cuda")
     want4 = A4 @ B4
     phi4 = {}
-    for mode, SS in ((dgt.FP64_NATIVE, 0), (dgt.FP64_OZAKI_INT8, S), (dgt.FP64_OZAKI_INT8, 8)):
+    for label, mode, SS in (("native", dgt.FP64_NATIVE, 2), (f"crt_n{chosen['crt']}", dgt.FP64_OZAKI2_INT8,
+                                                              chosen["crt"]), ("crt_n17", dgt.FP64_OZAKI2_INT8, 17),
+                            (f"slices_s{chosen['slices']}", dgt.FP64_OZAKI_INT8, chosen["slices"])):
         h.dgemm("N", "N", n, 1024, 2048, 1.0, dA4.data_ptr(), n, dB4.data_ptr(), 2048, 0.0, dC4.data_ptr(), n,
-                mode=mode, slices=max(SS, 2))
+                mode=mode, slices=SS)
         torch.cuda.synchronize()
-        phi4[("native" if mode == dgt.FP64_NATIVE else f"int8_s{SS}")] = O.rel_errors(
-            dC4.cpu().numpy().T, want4)
+        phi4[label] = O.rel_errors(dC4.cpu().numpy().T, want4)
     del dA4, dB4, dC4
 
     def timed(fn, steps, warm):
@@ -720,21 +738,26 @@ def main():
     nat_ms = timed(lambda: run(dgt.FP64_NATIVE, 0, C_nat.data_ptr()), max(2, args.steps // 2), 1)
     nat_ms = max_over_ranks(nat_ms, world)
 
+    # ---- the other scheme, timed the same way (reported beside the headline) ----
+    other = [nm for nm in schemes if nm != best][0]
+    other_ms = timed(lambda: run(schemes[other][0], chosen[other]), max(2, args.steps // 2), 1)
+    other_ms = max_over_ranks(other_ms, world)
+
     # ---- the headline: emulated FP64 at equal error, device-resident inputs ----
     launches0 = h.launch_count()
     sampler = ClockSampler(local)
     sampler.start()
-    emu_ms = timed(lambda: run(dgt.FP64_OZAKI_INT8, S), args.steps, args.warmup)
+    emu_ms = timed(lambda: run(MODE, S), args.steps, args.warmup)
     clocks = sampler.stop()
     launches = (h.launch_count() - launches0) // (args.steps + args.warmup)
     emu_ms = max_over_ranks(emu_ms, world)
     value = world * flops / (emu_ms * 1e-3) / 1e12
 
-    # ---- roofline of the dominant kernel (ozaki_i8_gemm), timed live with events ----
+    # ---- roofline of the dominant kernel (the INT8 tcgen05 GEMM), timed live with events ----
     h.set_tuning(dgt.TUNE_PROFILE, 1)
     splits, gemms = [], []
     for _ in range(3):
-        run(dgt.FP64_OZAKI_INT8, S)
+        run(MODE, S)
         sp, gm = h.last_timings()
         splits.append(sp)
         gemms.append(gm)
@@ -742,26 +765,26 @@ def main():
     gemm_ms = statistics.median(gemms)
     split_ms = statistics.median(splits)
     kpad = -(-n // 128) * 128
-    pairs = S * (S + 1) // 2
-    int8_ops = 2.0 * n * n * kpad * pairs  # algorithmic INT8 tensor ops per launch
+    products = S if best == "crt" else S * (S + 1) // 2
+    int8_ops = 2.0 * n * n * kpad * products  # algorithmic INT8 tensor ops per launch
     # INT8 dense peak, measured live the way the bf16 figure in MEASURED_PEAKS.json was:
     # a cuBLASLt INT8 GEMM (torch._int_mm) of the same size, best of 3
     i8 = torch.randint(-127, 127, (8192, 8192), dtype=torch.int8, device="cuda")
     for _ in range(2):
         torch._int_mm(i8, i8)
     torch.cuda.synchronize()
-    best = 1e9
+    best_ms = 1e9
     for _ in range(3):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         torch._int_mm(i8, i8)
         e1.record()
         torch.cuda.synchronize()
-        best = min(best, e0.elapsed_time(e1))
-    int8_burst = 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+        best_ms = min(best_ms, e0.elapsed_time(e1))
+    int8_burst = 2.0 * 8192 ** 3 / (best_ms * 1e-3) / 1e12
     # sustained: the same GEMM looped for ~3 s under the power cap, rate of the last second
-    # (the digit GEMM runs inside a seconds-long timed region, so this is its ceiling)
-    reps = max(4, int(1000.0 / best))
+    # (the INT8 GEMM runs inside a seconds-long timed region, so this is its ceiling)
+    reps = max(4, int(1000.0 / best_ms))
     for _ in range(2 * reps):
         torch._int_mm(i8, i8)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -773,12 +796,12 @@ def main():
     int8_peak = 2.0 * 8192 ** 3 * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
     del i8
     achieved = int8_ops / (gemm_ms * 1e-3) / 1e12
-    # DRAM bytes of one digit-GEMM launch at this size, variant and slice count, from the
-    # committed ncu capture (lines "variant V slices S size N: BYTES")
+    # DRAM bytes of one GEMM launch at this size, scheme, variant and count, from the
+    # committed ncu capture (lines "SCHEME variant V count N size M: BYTES")
     traffic = None
     prof = os.path.join(ROOT, "profiles", "digit_gemm_dram_traffic.txt")
     if os.path.exists(prof):
-        key = f"variant {tuned_emu['variant']} slices {S} size {n}:"
+        key = f"{best} variant {tuned[best]['variant']} count {S} size {n}:"
         for ln in open(prof):
             if ln.startswith(key):
                 traffic = float(ln.split(":")[1].split()[0])
@@ -787,7 +810,7 @@ def main():
     def e2e_step():
         A.copy_(A_h, non_blocking=True)
         B.copy_(B_h, non_blocking=True)
-        run(dgt.FP64_OZAKI_INT8, S)
+        run(MODE, S)
         C_h.copy_(C, non_blocking=True)
 
     e2e_ms = timed(e2e_step, max(2, args.steps // 2), 1)
@@ -819,24 +842,30 @@ def main():
             "warmup": args.warmup, "ms_per_step": emu_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"FP64-accurate GEMM C=alpha*A*B+beta*C, M=N=K={n}, column-major, "
-                                   f"(U-0.5)*exp({PHI}*N(0,1)) inputs, Ozaki INT8 slices S={S}",
-                       "M": n, "N": n, "K": n, "alpha": ALPHA, "beta": BETA, "phi": PHI, "slices": S,
+                                   f"(U-0.5)*exp({PHI}*N(0,1)) inputs, emulated on INT8 tensor cores "
+                                   f"({'CRT, ' + str(S) + ' moduli' if best == 'crt' else str(S) + ' slices'})",
+                       "M": n, "N": n, "K": n, "alpha": ALPHA, "beta": BETA, "phi": PHI, "scheme": best, "count": S,
                        "l2": "inputs larger than L2 (2 GiB each), no flush", "parallelism":
                            f"replicas x{world}" if world > 1 else "1 GPU"},
             "native_dmma": {"value": world * flops / (nat_ms * 1e-3) / 1e12, "ms_per_step": nat_ms,
                             "max_rel": nat_err[0], "fro_rel": nat_err[1], "kernel_variant": tuned_native["variant"]},
-            "emulated": {"value": value, "slices": S, "max_rel": errs[S][0], "fro_rel": errs[S][1],
-                         "equal_error": equal_error, "speedup_vs_native": nat_ms / emu_ms,
-                         "errors_by_slices": {str(k): v for k, v in errs.items()},
-                         "split_ms": split_ms, "gemm_ms": gemm_ms, "kernel_variant": tuned_emu["variant"]},
+            "emulated": {"value": value, "scheme": best, "count": S, "max_rel": errs[(best, S)][0],
+                         "fro_rel": errs[(best, S)][1], "equal_error": equal_error,
+                         "speedup_vs_native": nat_ms / emu_ms, "split_ms": split_ms, "gemm_ms": gemm_ms,
+                         "kernel_variant": tuned[best]["variant"]},
+            "other_scheme": {"scheme": other, "count": chosen[other],
+                             "value": world * flops / (other_ms * 1e-3) / 1e12, "ms_per_step": other_ms,
+                             "max_rel": errs[(other, chosen[other])][0], "fro_rel": errs[(other, chosen[other])][1],
+                             "kernel_variant": tuned[other]["variant"]},
+            "errors_by_count": {f"{k[0]}_{k[1]}": v for k, v in errs.items()},
             "phi4_errors": {k: {"max_rel": v[0], "fro_rel": v[1]} for k, v in phi4.items()},
-            "roofline": {"bound": "tensor", "kernel": "oz::digit_gemm (INT8 Ozaki digit products)",
+            "roofline": {"bound": "tensor", "kernel": "oz::digit_gemm (INT8 tcgen05 GEMM of the emulation)",
                          "achieved": achieved, "peak": int8_peak,
                          "unit": "TOP/s (INT8)", "frac": achieved / int8_peak, "traffic": traffic,
                          "peak_source": "measured live, sustained: cuBLASLt INT8 GEMM 8192^3 (torch._int_mm) "
                                         "looped ~3 s under the power cap, last ~1 s",
                          "peak_burst": int8_burst, "frac_of_burst": achieved / int8_burst,
-                         "algorithmic": f"{pairs} digit products x 2*M*N*K_pad INT8 ops"},
+                         "algorithmic": f"{products} INT8 products x 2*M*N*K_pad ops"},
             "e2e": {"value": e2e_v, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * 8 * n * n,
                     "d2h_bytes_per_step": 8 * n * n},
             "gpu_launches": launches,

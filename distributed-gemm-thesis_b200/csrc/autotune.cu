@@ -65,8 +65,9 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
     if (!h) return DGT_ERROR_NOT_INITIALIZED;
     if (!result) return fail(h, DGT_ERROR_INVALID_VALUE, "null result");
     if (m <= 0 || n <= 0 || k <= 0 || !A || !B || !C) return fail(h, DGT_ERROR_INVALID_VALUE, "bad shape or pointer");
-    if (mode != DGT_FP64_NATIVE && mode != DGT_FP64_OZAKI_INT8 && mode != DGT_FP64_AUTO)
-        return fail(h, DGT_ERROR_UNSUPPORTED, "the autotuner covers the native, INT8 Ozaki and AUTO modes");
+    if (mode != DGT_FP64_NATIVE && mode != DGT_FP64_OZAKI_INT8 && mode != DGT_FP64_OZAKI2_INT8 &&
+        mode != DGT_FP64_AUTO)
+        return fail(h, DGT_ERROR_UNSUPPORTED, "the autotuner covers the native, INT8 Ozaki, CRT and AUTO modes");
     const double one = 1.0, zero = 0.0;
     cudaEvent_t e0, e1;
     DGT_CUDA_TRY(h, cudaEventCreate(&e0));
@@ -104,7 +105,7 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
     saved_table.swap(h->tune);
     dgt_status st = DGT_SUCCESS;
     TuneEntry nat{DGT_FP64_NATIVE, 0, 0, 1e30f, 0.0}, ozk{DGT_FP64_OZAKI_INT8, 0, h->slices, 1e30f, 0.0};
-    if (mode != DGT_FP64_OZAKI_INT8) {
+    if (mode == DGT_FP64_NATIVE || mode == DGT_FP64_AUTO) {
         std::vector<int> cands;
         for (int v = 0; v < dmma_variant_count() && st == DGT_SUCCESS; ++v) {
             h->dmma_variant = v;
@@ -117,85 +118,98 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
         for (size_t c = 0; c < cands.size() && st == DGT_SUCCESS; ++c)
             if (best[c] < nat.ms) nat = TuneEntry{DGT_FP64_NATIVE, cands[c], 0, best[c], 0.0};
     }
-    if (st == DGT_SUCCESS && mode != DGT_FP64_NATIVE) {
-        int S = h->slices;
+    // The emulated schemes: for AUTO, the smallest slice (modulus) count whose result is
+    // within tol of the native one; then every kernel variant that reproduces variant 0's
+    // result exactly (same products, same fold order), timed in rounds.
+    double* ref = nullptr;
+    if (st == DGT_SUCCESS && mode == DGT_FP64_AUTO) {
+        void* w = nullptr;  // native reference, a variant reference and two sums, in slot 1
+        st = ensure_workspace(h, 2 * (size_t)m * n * sizeof(double) + 64, &w, 1);
+        if (st == DGT_SUCCESS) {
+            ref = (double*)w;
+            h->dmma_variant = nat.variant;
+            st = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, ref, m, DGT_FP64_NATIVE, 0);
+        }
+    } else if (st == DGT_SUCCESS && mode != DGT_FP64_NATIVE) {
+        void* w = nullptr;
+        st = ensure_workspace(h, 2 * (size_t)m * n * sizeof(double) + 64, &w, 1);
+        ref = (double*)w;
+    }
+    double* vref = ref ? ref + (size_t)m * n : nullptr;
+    double* sums = vref ? vref + (size_t)m * n : nullptr;
+    auto rel_to = [&](const double* R, double* out) -> dgt_status {  // ||C - R|| / ||R||
+        cudaMemsetAsync(sums, 0, 2 * sizeof(double), h->stream);
+        diff_norms<<<h->num_sms * 4, 256, 0, h->stream>>>(C, R, m, n, ldc, m, sums);
+        double hs[2] = {0, 0};
+        cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, h->stream);
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) return cuda_fail(h, cudaGetLastError(), "autotune check");
+        *out = hs[1] > 0 ? std::sqrt(hs[0] / hs[1]) : std::sqrt(hs[0]);
+        return DGT_SUCCESS;
+    };
+    auto tune_emulated = [&](dgt_fp64_mode em, TuneEntry& out) -> dgt_status {
+        const bool crt = em == DGT_FP64_OZAKI2_INT8;
+        int S = crt ? (valid_slices(em, h->slices) ? h->slices : 16) : h->slices;
+        double rel_native = 0.0;
         if (mode == DGT_FP64_AUTO) {
-            // reference: the native result, kept in workspace slot 1
-            void* ref = nullptr;
-            st = ensure_workspace(h, (size_t)m * n * sizeof(double) + 64, &ref, 1);
-            if (st == DGT_SUCCESS) {
-                h->dmma_variant = nat.variant;
-                st = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, (double*)ref, m, DGT_FP64_NATIVE, 0);
-            }
-            double* sums = (double*)ref + (size_t)m * n;
             S = 0;
-            for (int s = 4; s <= 14 && st == DGT_SUCCESS; ++s) {
-                st = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc, DGT_FP64_OZAKI_INT8, s);
-                if (st != DGT_SUCCESS) break;
-                cudaMemsetAsync(sums, 0, 2 * sizeof(double), h->stream);
-                diff_norms<<<h->num_sms * 4, 256, 0, h->stream>>>(C, (double*)ref, m, n, ldc, m, sums);
-                double hs[2] = {0, 0};
-                cudaMemcpyAsync(hs, sums, sizeof(hs), cudaMemcpyDeviceToHost, h->stream);
-                if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
-                    st = cuda_fail(h, cudaGetLastError(), "autotune accuracy check");
-                    break;
-                }
-                double rel = hs[1] > 0 ? std::sqrt(hs[0] / hs[1]) : std::sqrt(hs[0]);
+            for (int s = crt ? 10 : 4; s <= (crt ? 20 : 14); ++s) {
+                dgt_status e = dgt_dgemm_ex(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc, em, s);
+                if (e != DGT_SUCCESS) return e;
+                double rel = 0;
+                if ((e = rel_to(ref, &rel)) != DGT_SUCCESS) return e;
                 if (rel <= tol) {
                     S = s;
-                    ozk.rel_diff = rel;
+                    rel_native = rel;
                     break;
                 }
             }
-            if (st == DGT_SUCCESS && S == 0) S = -1;  // no slice count reaches tol: emulation not eligible
-        }
-        // every kernel variant must reproduce variant 0's result exactly (same digit products,
-        // same fold order); a variant that does not is never chosen
-        double* vref = nullptr;
-        double* vsums = nullptr;
-        if (st == DGT_SUCCESS && S > 0) {
-            void* w = nullptr;
-            st = ensure_workspace(h, 2 * (size_t)m * n * sizeof(double) + 64, &w, 1);
-            vref = (double*)w + (size_t)m * n;  // the first m*n doubles may hold the native reference
-            vsums = vref + (size_t)m * n;
+            if (S == 0) return DGT_SUCCESS;  // no count reaches tol: not eligible
         }
         std::vector<int> cands;
-        for (int v = 0; v < 5 && st == DGT_SUCCESS && S > 0; ++v) {
+        const std::vector<int> all = crt ? std::vector<int>{0, 1, 4} : std::vector<int>{0, 1, 2, 3, 4};
+        for (int v : all) {
             h->ozaki_variant = v;
             float t;
-            st = time_once(DGT_FP64_OZAKI_INT8, S, &t);  // warm-up, and the result to check
-            if (st != DGT_SUCCESS) break;
-            if (v == 0) {
-                DGT_CUDA_TRY(h, cudaMemcpy2DAsync(vref, m * sizeof(double), C, ldc * sizeof(double), m * sizeof(double),
-                                                  n, cudaMemcpyDeviceToDevice, h->stream));
+            dgt_status e = time_once(em, S, &t);  // warm-up, and the result to check
+            if (e != DGT_SUCCESS) return e;
+            if (v == all[0]) {
+                DGT_CUDA_TRY(h, cudaMemcpy2DAsync(vref, m * sizeof(double), C, ldc * sizeof(double),
+                                                  m * sizeof(double), n, cudaMemcpyDeviceToDevice, h->stream));
             } else {
-                cudaMemsetAsync(vsums, 0, 2 * sizeof(double), h->stream);
-                diff_norms<<<h->num_sms * 4, 256, 0, h->stream>>>(C, vref, m, n, ldc, m, vsums);
-                double hs[2] = {1, 1};
-                cudaMemcpyAsync(hs, vsums, sizeof(hs), cudaMemcpyDeviceToHost, h->stream);
-                if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
-                    st = cuda_fail(h, cudaGetLastError(), "autotune variant check");
-                    break;
-                }
-                if (hs[0] != 0.0) continue;  // not identical to variant 0
+                double rel = 1;
+                if ((e = rel_to(vref, &rel)) != DGT_SUCCESS) return e;
+                if (rel != 0.0) continue;  // not identical to the first variant
             }
             cands.push_back(v);
         }
         std::vector<float> best;
-        if (st == DGT_SUCCESS && S > 0) st = time_rounds(cands, &h->ozaki_variant, DGT_FP64_OZAKI_INT8, S, best);
-        for (size_t c = 0; c < cands.size() && st == DGT_SUCCESS && S > 0; ++c)
-            if (best[c] < ozk.ms) ozk = TuneEntry{DGT_FP64_OZAKI_INT8, cands[c], S, best[c], ozk.rel_diff};
-    }
+        dgt_status e = time_rounds(cands, &h->ozaki_variant, em, S, best);
+        if (e != DGT_SUCCESS) return e;
+        for (size_t c = 0; c < cands.size(); ++c)
+            if (best[c] < out.ms) out = TuneEntry{em, cands[c], S, best[c], rel_native};
+        return DGT_SUCCESS;
+    };
+    TuneEntry crt{DGT_FP64_OZAKI2_INT8, 1, 16, 1e30f, 0.0};
+    if (st == DGT_SUCCESS && (mode == DGT_FP64_OZAKI_INT8 || mode == DGT_FP64_AUTO))
+        st = tune_emulated(DGT_FP64_OZAKI_INT8, ozk);
+    if (st == DGT_SUCCESS && (mode == DGT_FP64_OZAKI2_INT8 || mode == DGT_FP64_AUTO))
+        st = tune_emulated(DGT_FP64_OZAKI2_INT8, crt);
     h->tune.swap(saved_table);
     h->dmma_variant = saved_dv;
     h->ozaki_variant = saved_ov;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != DGT_SUCCESS) return st;
-    if (mode != DGT_FP64_OZAKI_INT8) h->tune[tune_key(DGT_FP64_NATIVE, m, n, k)] = nat;
-    if (mode != DGT_FP64_NATIVE && ozk.ms < 1e29f) h->tune[tune_key(DGT_FP64_OZAKI_INT8, m, n, k)] = ozk;
+    if (mode == DGT_FP64_NATIVE || mode == DGT_FP64_AUTO) h->tune[tune_key(DGT_FP64_NATIVE, m, n, k)] = nat;
+    if (ozk.ms < 1e29f) h->tune[tune_key(DGT_FP64_OZAKI_INT8, m, n, k)] = ozk;
+    if (crt.ms < 1e29f) h->tune[tune_key(DGT_FP64_OZAKI2_INT8, m, n, k)] = crt;
     TuneEntry best = nat;
-    if (mode == DGT_FP64_OZAKI_INT8 || (mode == DGT_FP64_AUTO && ozk.ms < nat.ms)) best = ozk;
+    if (mode == DGT_FP64_OZAKI_INT8) best = ozk;
+    if (mode == DGT_FP64_OZAKI2_INT8) best = crt;
+    if (mode == DGT_FP64_AUTO) {
+        if (ozk.ms < best.ms) best = ozk;
+        if (crt.ms < best.ms) best = crt;
+    }
     if (mode == DGT_FP64_AUTO) h->tune[tune_key(DGT_FP64_AUTO, m, n, k)] = best;
     result->mode = best.mode;
     result->variant = best.variant;

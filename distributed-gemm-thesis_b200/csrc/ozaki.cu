@@ -169,7 +169,7 @@ struct SplitJob {
     int64_t amax_begin;     // first block of this job in the amax launch
     int64_t split_begin;    // first block of this job in the split launch
 };
-constexpr int AMAX_KCHUNK = 512;
+constexpr int AMAX_KCHUNK = 64;  // K rows per block of the MN-contiguous amax (fills the GPU)
 
 __device__ __forceinline__ int find_job(const SplitJob* __restrict__ jobs, int njobs, int64_t blk, bool split) {
     int lo = 0, hi = njobs - 1;
@@ -367,20 +367,10 @@ static dgt_status ozaki_run(dgt_context* h, cudaStream_t s, int num_sms, unsigne
         dgroups = (oz::Group*)((char*)table + offs[1]);
     }
     if (h) mark(h, 0);
-    DGT_CUDA_TRY(h, cudaMemsetAsync(amaxA, 0, m * 8, s));
-    DGT_CUDA_TRY(h, cudaMemsetAsync(amaxB, 0, n * 8, s));
-
     // op(A) is m x k: 'N' -> element (i,kk) at A[i + kk*lda] (MN-contiguous); 'T' -> A[kk + i*lda]
     // op(B) as its transpose n x k: 'N' -> element (j,kk) at B[kk + j*ldb] (K-contiguous); 'T' -> B[j + kk*ldb]
     auto amax = [&](const double* X, int64_t ld, int64_t MN, bool kcontig, unsigned long long* out) {
-        if (kcontig) {
-            oz::amax_k_contig<<<(unsigned)ceil_div(MN, 8), 256, 0, s>>>(X, ld, MN, k, out);
-        } else {
-            int kchunk = 512;
-            dim3 grid((unsigned)ceil_div(MN, 256), (unsigned)ceil_div(k, kchunk));
-            oz::amax_mn_contig<<<grid, 256, 0, s>>>(X, ld, MN, k, kchunk, out);
-        }
-        return counted("ozaki amax");
+        return ozaki_amax(h, s, X, ld, MN, k, kcontig, out);
     };
     auto split = [&](const double* X, int64_t ld, int64_t MN, int64_t mn_pad, bool kcontig,
                      const unsigned long long* am, int32_t* ex, void* planes) {

@@ -34,22 +34,28 @@ namespace dgt {
 namespace oz2 {
 
 constexpr int MAX_MODULI = 20, MIN_MODULI = 8;
-constexpr int NL = 6;          // 32-bit limbs of the CRT arithmetic (P < 2^160, sums < 2^192)
 constexpr int MAX_BETA = 58;   // |A'| < 2^58: residues by FP64 division stay exact
 // Pairwise coprime, largest first (greedy from 256 down).
 constexpr int kModuli[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                                      223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
 
+// Residues of x = trunc(a 2^(beta-e)) (|x| < 2^58) modulo p, in integers: xu = x + 2^58 is
+// split into 20-bit chunks x0, x1, x2 and t = x2 c40 + x1 c20 + x0 + off (< 2^29) is congruent
+// to x; t / p = (t magic) >> 37 exactly for t < 2^29 (Granlund & Montgomery 1994, thm 4.2:
+// magic = floor(2^37 / p) + 1 for 2^7 < p <= 2^8).
 struct ModTable {
     int32_t p[MAX_MODULI];
-    double inv[MAX_MODULI];
+    uint32_t c20[MAX_MODULI], c40[MAX_MODULI];  // 2^20 mod p, 2^40 mod p
+    uint32_t off[MAX_MODULI];                    // p - (2^58 mod p)
+    uint32_t magic[MAX_MODULI];
 };
 
+constexpr int MAX_NW = 5;  // 32-bit limbs of W_p and P (P < 2^160)
 struct CrtConst {
     int32_t n;
-    uint32_t W[MAX_MODULI][NL];
-    uint32_t P[NL], Phalf[NL];  // Phalf = floor((P - 1) / 2)
-    double inv_P;               // 1 / P, rounded
+    uint32_t W[MAX_MODULI][MAX_NW];
+    uint32_t P[MAX_NW + 1], Phalf[MAX_NW + 1];  // Phalf = floor((P - 1) / 2)
+    double kq[MAX_NW + 1];                      // 2^(32 l) / P: X / P ~ sum_l x_l kq_l
 };
 
 // ---- host: CRT constants in 32-bit limbs ------------------------------------------------------
@@ -100,6 +106,9 @@ static int beta_for(int n, int64_t k) {
     return std::min(MAX_BETA, (int)std::floor(b));
 }
 
+// Limbs of W_p and P for n moduli (P < 2^(32 nw)).
+static int limbs_for(int n) { return (int)std::ceil(log2_product(n) / 32.0); }
+
 static void crt_constants(int n, CrtConst& cc, ModTable& mt) {
     cc = CrtConst{};
     mt = ModTable{};
@@ -109,24 +118,27 @@ static void crt_constants(int n, CrtConst& cc, ModTable& mt) {
     for (int i = 0; i < n; ++i) {
         const uint32_t p = (uint32_t)kModuli[i];
         mt.p[i] = (int32_t)p;
-        mt.inv[i] = 1.0 / (double)p;
+        mt.c20[i] = (uint32_t)((1ull << 20) % p);
+        mt.c40[i] = (uint32_t)((1ull << 40) % p);
+        mt.off[i] = p - (uint32_t)((1ull << 58) % p);
+        mt.magic[i] = (uint32_t)((1ull << 37) / p + 1);
         Big M = P;
         big_div_small(M, p);  // M = P / p
         Big Mm = M;
         const uint32_t m_mod = big_div_small(Mm, p);
         big_mul_small(M, inv_mod(m_mod, p));  // W = M * (M^-1 mod p) < P
-        for (int l = 0; l < NL; ++l) cc.W[i][l] = l < (int)M.size() ? M[l] : 0;
+        for (int l = 0; l < MAX_NW; ++l) cc.W[i][l] = l < (int)M.size() ? M[l] : 0;
     }
-    for (int l = 0; l < NL; ++l) cc.P[l] = l < (int)P.size() ? P[l] : 0;
+    for (int l = 0; l <= MAX_NW; ++l) cc.P[l] = l < (int)P.size() ? P[l] : 0;
     Big H = P;  // floor((P - 1) / 2)
     for (size_t l = 0; l < H.size(); ++l) {  // H -= 1 (P > 1)
         if (H[l]--) break;
     }
     big_div_small(H, 2);
-    for (int l = 0; l < NL; ++l) cc.Phalf[l] = l < (int)H.size() ? H[l] : 0;
+    for (int l = 0; l <= MAX_NW; ++l) cc.Phalf[l] = l < (int)H.size() ? H[l] : 0;
     double pd = 0;
-    for (int l = NL - 1; l >= 0; --l) pd = pd * 4294967296.0 + (double)cc.P[l];
-    cc.inv_P = 1.0 / pd;
+    for (int l = MAX_NW; l >= 0; --l) pd = pd * 4294967296.0 + (double)cc.P[l];
+    for (int l = 0; l <= MAX_NW; ++l) cc.kq[l] = std::ldexp(1.0, 32 * l) / pd;
 }
 
 // ---- device: residue planes ----------------------------------------------------------------------
@@ -148,31 +160,35 @@ __global__ void __launch_bounds__(128) split_residues(const double* __restrict__
         if (blockIdx.y == 0) exps[mn] = e;
     }
     const bool live = (mn < MN) && (e != oz::EXP_NONFINITE);
-    double v[32];
+    uint32_t x0[32], x1[32], x2[32];  // 20-bit chunks of x + 2^58
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
         const int64_t kk = k0 + i;
-        double x = 0.0;
-        if (live && kk < K) x = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
-        v[i] = live ? trunc(oz::scale2(x, beta - e)) : 0.0;  // an integer, |v| < 2^beta
+        double a = 0.0;
+        if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
+        // an integer below 2^beta <= 2^58 in magnitude (exact scaling, truncation toward 0)
+        const long long x = live ? __double2ll_rz(oz::scale2(a, beta - e)) : 0ll;
+        const unsigned long long xu = (unsigned long long)(x + (1ll << 58));
+        x0[i] = (uint32_t)(xu & 0xfffffu);
+        x1[i] = (uint32_t)((xu >> 20) & 0xfffffu);
+        x2[i] = (uint32_t)(xu >> 40);
     }
     const int64_t plane = mn_pad * k_pad;
     for (int j = 0; j < nmod; ++j) {
-        const double p = (double)mt.p[j], inv = mt.inv[j];
-        const double lo = -(double)(mt.p[j] >> 1), hi = (double)((mt.p[j] - 1) >> 1);
+        const uint32_t p = (uint32_t)mt.p[j], c20 = mt.c20[j], c40 = mt.c40[j], off = mt.off[j], mg = mt.magic[j];
+        const uint32_t half = (p - 1) >> 1;
         uint32_t w[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) w[q] = 0;
+        for (int q = 0; q < 8; ++q) {
+            uint32_t b[4];
 #pragma unroll
-        for (int i = 0; i < 32; ++i) {
-            // |v / p| < 2^51, so rint(v * inv) is the nearest quotient or one off, and the
-            // remainder fma(-q, p, v) is an integer below 2^10: exact
-            double r = fma(-rint(v[i] * inv), p, v[i]);
-            if (r > hi) r -= p;
-            if (r > hi) r -= p;
-            if (r < lo) r += p;
-            if (r < lo) r += p;
-            w[i >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)r) << (8 * (i & 3));
+            for (int u = 0; u < 4; ++u) {
+                const int i = 4 * q + u;
+                const uint32_t t = x2[i] * c40 + x1[i] * c20 + x0[i] + off;  // < 2^29, = x mod p
+                const uint32_t r = t - (__umulhi(t, mg) >> 5) * p;           // in [0, p)
+                b[u] = r > half ? r - p : r;                                  // symmetric, low byte
+            }
+            w[q] = __byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410);
         }
         uint4* o4 = reinterpret_cast<uint4*>(planes + j * plane + mn * k_pad + k0);
         o4[0] = make_uint4(w[0], w[1], w[2], w[3]);
@@ -181,88 +197,134 @@ __global__ void __launch_bounds__(128) split_residues(const double* __restrict__
 }
 
 // ---- device: reconstruction -----------------------------------------------------------------------
-// X = sum_j r_j W_j reduced mod P into the symmetric range, rounded to FP64 once (round to
-// nearest even), times 2^shift.  r_j is byte `sel` of rr[j].  Every loop has a constant trip
-// count so the limbs stay in registers.
+// x += y (ADD) or x -= y over N 32-bit limbs, one carry chain.
+template <int N, bool ADD>
+__device__ __forceinline__ void limbs_addsub(uint32_t (&x)[N], const uint32_t (&y)[N]) {
+    if constexpr (N == 3) {
+        if constexpr (ADD)
+        asm("add.cc.u32 %0, %0, %3;\n" "addc.cc.u32 %1, %1, %4;\n" "addc.u32 %2, %2, %5;\n"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2])
+            : "r"(y[0]), "r"(y[1]), "r"(y[2]));
+        else
+        asm("sub.cc.u32 %0, %0, %3;\n" "subc.cc.u32 %1, %1, %4;\n" "subc.u32 %2, %2, %5;\n"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2])
+            : "r"(y[0]), "r"(y[1]), "r"(y[2]));
+    }
+    if constexpr (N == 4) {
+        if constexpr (ADD)
+        asm("add.cc.u32 %0, %0, %4;\n" "addc.cc.u32 %1, %1, %5;\n" "addc.cc.u32 %2, %2, %6;\n" "addc.u32 %3, %3, %7;\n"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3])
+            : "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]));
+        else
+        asm("sub.cc.u32 %0, %0, %4;\n" "subc.cc.u32 %1, %1, %5;\n" "subc.cc.u32 %2, %2, %6;\n" "subc.u32 %3, %3, %7;\n"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3])
+            : "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]));
+    }
+    if constexpr (N == 5) {
+        if constexpr (ADD)
+        asm("add.cc.u32 %0, %0, %5;\n" "addc.cc.u32 %1, %1, %6;\n" "addc.cc.u32 %2, %2, %7;\n" "addc.cc.u32 %3, %3, %8;\n" "addc.u32 %4, %4, %9;\n"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4])
+            : "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]), "r"(y[4]));
+        else
+        asm("sub.cc.u32 %0, %0, %5;\n" "subc.cc.u32 %1, %1, %6;\n" "subc.cc.u32 %2, %2, %7;\n" "subc.cc.u32 %3, %3, %8;\n" "subc.u32 %4, %4, %9;\n"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4])
+            : "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]), "r"(y[4]));
+    }
+    if constexpr (N == 6) {
+        if constexpr (ADD)
+        asm("add.cc.u32 %0, %0, %6;\n" "addc.cc.u32 %1, %1, %7;\n" "addc.cc.u32 %2, %2, %8;\n" "addc.cc.u32 %3, %3, %9;\n" "addc.cc.u32 %4, %4, %10;\n" "addc.u32 %5, %5, %11;\n"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5])
+            : "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]), "r"(y[4]), "r"(y[5]));
+        else
+        asm("sub.cc.u32 %0, %0, %6;\n" "subc.cc.u32 %1, %1, %7;\n" "subc.cc.u32 %2, %2, %8;\n" "subc.cc.u32 %3, %3, %9;\n" "subc.cc.u32 %4, %4, %10;\n" "subc.u32 %5, %5, %11;\n"
+            : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5])
+            : "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]), "r"(y[4]), "r"(y[5]));
+    }
+}
+
+// a > b over N limbs (most significant last)
+template <int N>
+__device__ __forceinline__ bool limbs_gt(const uint32_t (&a)[N], const uint32_t (&b)[N]) {
+    bool gt = false, decided = false;
+#pragma unroll
+    for (int l = N - 1; l >= 0; --l) {
+        if (!decided && a[l] != b[l]) {
+            gt = a[l] > b[l];
+            decided = true;
+        }
+    }
+    return gt;
+}
+
+// X = sum_j r_j W_j (NW-limb W, NX = NW + 1 limbs for X < 2^13 P) reduced mod P into the
+// symmetric range, rounded to FP64 once (round to nearest even), times 2^shift.  r_j is byte
+// `sel` of rr[j].  Constant trip counts keep every limb in registers.
+template <int NW>
 __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
                                             int shift) {
-    uint64_t acc[NL];
+    constexpr int NX = NW + 1;
+    uint64_t acc[NW];
 #pragma unroll
-    for (int l = 0; l < NL; ++l) acc[l] = 0;
+    for (int l = 0; l < NW; ++l) acc[l] = 0;
 #pragma unroll
     for (int j = 0; j < MAX_MODULI; ++j) {
         if (j < cc.n) {
-            const uint64_t r = (rr[j] >> (8 * sel)) & 0xffu;
+            const uint32_t r = (rr[j] >> (8 * sel)) & 0xffu;
 #pragma unroll
-            for (int l = 0; l < NL; ++l) acc[l] += r * cc.W[j][l];  // < 20 * 2^40
+            for (int l = 0; l < NW; ++l) acc[l] += (uint64_t)r * cc.W[j][l];  // < 20 * 2^40
         }
     }
-    uint32_t x[NL];
+    uint32_t x[NX];
     uint64_t c = 0;
 #pragma unroll
-    for (int l = 0; l < NL; ++l) {
+    for (int l = 0; l < NW; ++l) {
         const uint64_t t = acc[l] + c;
         x[l] = (uint32_t)t;
         c = t >> 32;
     }
-    // X < 20 * 256 * P < 2^13 P: q = floor(X / P) from the top limbs, exact or one off
-    const double xd = ldexp((double)x[5], 160) + ldexp((double)x[4], 128) + ldexp((double)x[3], 96) +
-                      ldexp((double)x[2], 64);
-    const uint32_t q = (uint32_t)floor(xd * cc.inv_P);
+    x[NW] = (uint32_t)c;
+    // q = floor(X / P) to within one (X < 2^13 P); X -= q P
+    double xq = 0.0;
+#pragma unroll
+    for (int l = 0; l < NX; ++l) xq = fma((double)x[l], cc.kq[l], xq);
+    const uint32_t q = (uint32_t)xq;
+    uint32_t qp[NX];
     c = 0;
-    int64_t b = 0;  // X -= q P, borrow in b
 #pragma unroll
-    for (int l = 0; l < NL; ++l) {
+    for (int l = 0; l < NX; ++l) {
         const uint64_t t = (uint64_t)q * cc.P[l] + c;
+        qp[l] = (uint32_t)t;
         c = t >> 32;
-        const int64_t d = (int64_t)x[l] - (int64_t)(uint32_t)t + b;
-        x[l] = (uint32_t)d;
-        b = d >> 32;
     }
-    bool ge_P = true;  // X >= P (only meaningful when b == 0)
-    bool decided = false;
+    limbs_addsub<NX, false>(x, qp);  // X in [-P, 2P), two's complement
+    uint32_t Pl[NX], Ph[NX];
 #pragma unroll
-    for (int l = NL - 1; l >= 0; --l) {
-        if (!decided && x[l] != cc.P[l]) {
-            ge_P = x[l] > cc.P[l];
-            decided = true;
-        }
+    for (int l = 0; l < NX; ++l) {
+        Pl[l] = cc.P[l];
+        Ph[l] = cc.Phalf[l];
     }
-    const int64_t sgn = b < 0 ? 1 : (ge_P ? -1 : 0);  // q one too large / one too small
-    int64_t cc2 = 0;
+    if ((int32_t)x[NX - 1] < 0)
+        limbs_addsub<NX, true>(x, Pl);
+    else if (!limbs_gt<NX>(Pl, x))  // X >= P
+        limbs_addsub<NX, false>(x, Pl);
+    // symmetric range: X > floor((P-1)/2) stands for X - P; work with the magnitude P - X
+    const bool neg = limbs_gt<NX>(x, Ph);
+    if (neg) {
+        uint32_t m[NX];
 #pragma unroll
-    for (int l = 0; l < NL; ++l) {
-        const int64_t d = (int64_t)x[l] + sgn * (int64_t)cc.P[l] + cc2;
-        x[l] = (uint32_t)d;
-        cc2 = d >> 32;
-    }
-    // symmetric range: X > floor((P-1)/2) stands for X - P; work with the magnitude
-    bool above = false;
-    decided = false;
+        for (int l = 0; l < NX; ++l) m[l] = Pl[l];
+        limbs_addsub<NX, false>(m, x);
 #pragma unroll
-    for (int l = NL - 1; l >= 0; --l) {
-        if (!decided && x[l] != cc.Phalf[l]) {
-            above = x[l] > cc.Phalf[l];
-            decided = true;
-        }
-    }
-    if (above) {  // magnitude P - X
-        int64_t bb = 0;
-#pragma unroll
-        for (int l = 0; l < NL; ++l) {
-            const int64_t d = (int64_t)cc.P[l] - (int64_t)x[l] + bb;
-            x[l] = (uint32_t)d;
-            bb = d >> 32;
-        }
+        for (int l = 0; l < NX; ++l) x[l] = m[l];
     }
     int L = 0;
 #pragma unroll
-    for (int l = 1; l < NL; ++l)
+    for (int l = 1; l < NX; ++l)
         if (x[l] != 0u) L = l;
     uint32_t a2 = 0, a1 = 0, a0 = 0;
     bool sticky = false;
 #pragma unroll
-    for (int l = 0; l < NL; ++l) {
+    for (int l = 0; l < NX; ++l) {
         if (l == L) a2 = x[l];
         if (l == L - 1) a1 = x[l];
         if (l == L - 2) a0 = x[l];
@@ -277,11 +339,12 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
     // one rounding to 53 bits is correct (round to nearest even)
     const double d = __ull2double_rn(top64 | (uint64_t)sticky);
     const double mag = oz::scale2(d, 32 * (L - 1) - lz + shift);
-    return above ? -mag : mag;
+    return neg ? -mag : mag;
 }
 
 // Thread per 4 consecutive rows of one column of C; residue planes [j][col][row] with
 // leading dimension res_ld (a multiple of 4).
+template <int NW>
 __global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
                                                        int64_t res_plane, int64_t m, int64_t n,
                                                        const int32_t* __restrict__ row_exp,
@@ -306,7 +369,7 @@ __global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict
         if (e == oz::EXP_NONFINITE || f == oz::EXP_NONFINITE)
             val = __longlong_as_double(0x7ff8000000000000ll);
         else
-            val = crt_value(rr, e4, cc, e + f - 2 * beta);
+            val = crt_value<NW>(rr, e4, cc, e + f - 2 * beta);
         double* cp = C + row + col * ldc;
         *cp = beta_c != 0.0 ? fma(alpha, val, beta_c * *cp) : alpha * val;
     }
@@ -438,8 +501,25 @@ dgt_status ozaki2_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, 
     if (le != cudaSuccess) return cuda_fail(h, le, "residue GEMM launch");
     mark(h, 2);
     const int64_t threads = ceil_div(m, 4) * n;
-    crt_reconstruct<<<(unsigned)ceil_div(threads, 256), 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits,
-                                                                     alpha, beta, C, ldc, cc);
+    const unsigned blocks = (unsigned)ceil_div(threads, 256);
+    switch (limbs_for(nmod)) {
+        case 2:
+            crt_reconstruct<2><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta,
+                                                      C, ldc, cc);
+            break;
+        case 3:
+            crt_reconstruct<3><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta,
+                                                      C, ldc, cc);
+            break;
+        case 4:
+            crt_reconstruct<4><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta,
+                                                      C, ldc, cc);
+            break;
+        default:
+            crt_reconstruct<5><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta,
+                                                      C, ldc, cc);
+            break;
+    }
     h->launches.fetch_add(1);
     DGT_CUDA_TRY(h, cudaGetLastError());
     return DGT_SUCCESS;

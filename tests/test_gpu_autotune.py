@@ -20,10 +20,12 @@ def test_autotune_auto_mode_and_persistence(tmp_path):
     dA, dB, dC = dev(A), dev(B), dev(np.zeros((m, n)))
     with dgt.Handle() as h:
         r = h.autotune("N", "N", m, n, k, ptr(dA), m, ptr(dB), k, ptr(dC), m, mode=dgt.FP64_AUTO, tol=1e-14)
-        assert r["mode"] in (dgt.FP64_NATIVE, dgt.FP64_OZAKI_INT8)
+        assert r["mode"] in (dgt.FP64_NATIVE, dgt.FP64_OZAKI_INT8, dgt.FP64_OZAKI2_INT8)
         assert r["ms"] > 0
         if r["mode"] == dgt.FP64_OZAKI_INT8:
             assert 4 <= r["slices"] <= 14 and r["rel_diff"] <= 1e-14
+        if r["mode"] == dgt.FP64_OZAKI2_INT8:
+            assert 10 <= r["slices"] <= 20 and r["rel_diff"] <= 1e-14
         # a later AUTO call uses the recorded choice and stays FP64-accurate
         h.dgemm("N", "N", m, n, k, 1.0, ptr(dA), m, ptr(dB), k, 0.0, ptr(dC), m, mode=dgt.FP64_AUTO)
         torch.cuda.synchronize()
@@ -39,3 +41,19 @@ def test_autotune_auto_mode_and_persistence(tmp_path):
         assert O.rel_errors(host(dC, (m, n)), A @ B)[1] <= 1e-13
         with pytest.raises(dgt.DgtError):
             h2.autotune_load(os.path.join(str(tmp_path), "missing.json"))
+
+
+def test_autotune_crt_mode_variants():
+    """The CRT mode's kernel variants are tuned and the recorded choice is used."""
+    import torch
+
+    m, n, k = 512, 640, 768
+    A, B = O.uniform((m, k), 3), O.uniform((k, n), 4)
+    dA, dB, dC = dev(A), dev(B), dev(np.zeros((m, n)))
+    with dgt.Handle() as h:
+        h.set_fp64_mode(dgt.FP64_OZAKI2_INT8, 17)
+        r = h.autotune("N", "N", m, n, k, ptr(dA), m, ptr(dB), k, ptr(dC), m, mode=dgt.FP64_OZAKI2_INT8)
+        assert r["mode"] == dgt.FP64_OZAKI2_INT8 and r["variant"] in (0, 1, 4) and r["slices"] == 17
+        h.dgemm("N", "N", m, n, k, 1.0, ptr(dA), m, ptr(dB), k, 0.0, ptr(dC), m, mode=dgt.FP64_OZAKI2_INT8, slices=17)
+        torch.cuda.synchronize()
+        assert O.rel_errors(host(dC, (m, n)), A @ B)[1] <= 1e-15

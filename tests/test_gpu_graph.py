@@ -1,5 +1,6 @@
-"""CUDA-graph capture of the step schedules: after one warm-up call (which sizes the
-handle's workspace and uploads any grouped table), dgt_dgemm (native and Ozaki),
+"""CUDA-graph capture of the step schedules: after eager warm-up passes of the sequence
+(the first sizes the handle's workspace, the second runs with the final workspace and so
+leaves every launch table resident), dgt_dgemm (native and Ozaki),
 dgt_cannon25d (native, and emulated as one grouped Ozaki pass per step) and
 dgt_dgemm_grouped (native and grouped Ozaki) issue only capturable work, so the whole batch
 can be captured once and replayed; replay results equal the eager results bit for bit."""
@@ -68,7 +69,9 @@ def test_capture_and_replay_all_paths():
         side = torch.cuda.Stream()
         h.set_stream(side.cuda_stream)
         with torch.cuda.stream(side):
-            batch(h)  # eager (also the warm-up)
+            batch(h)  # eager: sizes the workspace (calls of different sizes may grow it)
+            reset()
+            batch(h)  # eager again, now with the final workspace: every table is resident
         torch.cuda.synchronize()
         eager = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
                  [x.clone() for x in ekeep] + [x.clone() for x in tE])
