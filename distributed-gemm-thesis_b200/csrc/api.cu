@@ -113,8 +113,9 @@ static bool cannon_order(int p, int c, int i, int j, int k, int* out) {
 // segment with K > 0 (the reference issues one cublasDgemm per step too); the first step
 // applies the product's beta, later steps accumulate.  Each step splits its own operands,
 // so every step is scaled on its own panel -- the numerics of a per-step local GEMM.  With
-// INT8 slices all products' step t run as one grouped Ozaki pass (the products of one step
-// write distinct C); a step the grouped form does not support runs product by product.
+// INT8 slices or CRT residues all products' step t run as one grouped pass (the products of
+// one step write distinct C); a step the grouped form does not support runs product by
+// product.
 dgt_status run_problems_emulated(dgt_context* h, const std::vector<Problem>& probs,
                                  const std::vector<KSegment>& segs, dgt_fp64_mode mode, int slices) {
     if (!valid_slices(mode, slices))
@@ -146,8 +147,8 @@ dgt_status run_problems_emulated(dgt_context* h, const std::vector<Problem>& pro
             batch.push_back(OzProblem{pr.transa != 0, pr.transb != 0, pr.m, pr.n, sg.k, pr.alpha,
                                       t == 0 ? pr.beta : 1.0, sg.A, sg.lda, sg.B, sg.ldb, pr.C, pr.ldc});
         }
-        if (mode == DGT_FP64_OZAKI_INT8) {
-            dgt_status st = ozaki_dgemm_grouped(h, batch, slices);
+        if (mode == DGT_FP64_OZAKI_INT8 || mode == DGT_FP64_OZAKI2_INT8) {
+            dgt_status st = ozaki_dgemm_grouped(h, batch, slices, mode == DGT_FP64_OZAKI2_INT8);
             if (st != DGT_ERROR_UNSUPPORTED) {
                 if (st != DGT_SUCCESS) return st;
                 continue;

@@ -1,0 +1,97 @@
+// Types shared by the two FP64 emulation schemes' grouped passes (ozaki.cu, ozaki2.cu):
+// the per-operand pre-pass job table, and the CRT scheme's modulus tables and reconstruction
+// jobs.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dgt_internal.cuh"
+
+namespace dgt {
+namespace oz {
+
+// One operand of a grouped pre-pass: a job owns a contiguous range of the launch's blocks,
+// found by binary search on the jobs' first block.
+struct SplitJob {
+    const double* X;
+    int64_t ld, MN, K, mn_pad, k_pad;
+    unsigned long long* amax;
+    int32_t* exps;
+    void* planes;
+    int32_t kcontig;
+    int32_t amax_bx;      // amax blocks along mn (MN-contiguous jobs: times amax_by along K)
+    int32_t amax_by;
+    int32_t split_bx;     // split blocks along mn (times k_pad / 32 along K)
+    int64_t amax_begin;   // first block of this job in the amax launch
+    int64_t split_begin;  // first block of this job in the split launch
+    int32_t bits;         // CRT scheme: operand bits of this product
+    int32_t unused;
+};
+constexpr int AMAX_KCHUNK = 64;  // K rows per block of the MN-contiguous amax (fills the GPU)
+
+__device__ __forceinline__ int find_job(const SplitJob* __restrict__ jobs, int njobs, int64_t blk, bool split) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int64_t b0 = split ? jobs[mid].split_begin : jobs[mid].amax_begin;
+        if (b0 <= blk)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+}  // namespace oz
+
+namespace oz2 {
+
+constexpr int MAX_MODULI = 20, MIN_MODULI = 8;
+constexpr int MAX_NW = 5;     // 32-bit limbs of W_p and P (P < 2^160)
+constexpr int MAX_BETA = 58;  // |A'| < 2^58
+
+// Residues of x = trunc(a 2^(beta-e)) (|x| < 2^58) modulo p, in integers: xu = x + 2^58 is
+// split into 20-bit chunks x0, x1, x2 and t = x2 c40 + x1 c20 + x0 + off (< 2^29) is congruent
+// to x; t / p = (t magic) >> 37 exactly for t < 2^29 (Granlund & Montgomery 1994, thm 4.2:
+// magic = floor(2^37 / p) + 1 for 2^7 < p <= 2^8).
+struct ModTable {
+    int32_t p[MAX_MODULI];
+    uint32_t c20[MAX_MODULI], c40[MAX_MODULI];  // 2^20 mod p, 2^40 mod p
+    uint32_t off[MAX_MODULI];                    // p - (2^58 mod p)
+    uint32_t magic[MAX_MODULI];
+};
+
+struct CrtConst {
+    int32_t n;
+    uint32_t W[MAX_MODULI][MAX_NW];
+    uint32_t P[MAX_NW + 1], Phalf[MAX_NW + 1];  // Phalf = floor((P - 1) / 2)
+    double kq[MAX_NW + 1];                      // 2^(32 l) / P: X / P ~ sum_l x_l kq_l
+};
+
+// One product of a grouped reconstruction: its residue planes, exponents, scaling and output;
+// it owns threads [thread_begin, thread_begin + ceil(m/4) n) of the launch.
+struct CrtJob {
+    const uint8_t* res;
+    int64_t res_ld, res_plane, m, n;
+    const int32_t* row_exp;
+    const int32_t* col_exp;
+    double alpha, beta;
+    double* C;
+    int64_t ldc;
+    int32_t bits, unused;
+    int64_t thread_begin;
+};
+
+// host helpers (ozaki2.cu)
+int beta_for(int nmod, int64_t k);   // operand bits: largest beta with 2 k (2^beta - 1)^2 < P
+int limbs_for(int nmod);             // 32-bit limbs of P
+void crt_constants(int nmod, CrtConst& cc, ModTable& mt);
+cudaError_t launch_split_residues_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks,
+                                          int nmod, const ModTable& mt);
+cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, int64_t threads, const CrtConst& cc,
+                               int nmod);
+
+}  // namespace oz2
+}  // namespace dgt

@@ -187,10 +187,11 @@ struct OzProblem {
     double* C;
     int64_t ldc;
 };
-// All products in one INT8 Ozaki pass: one amax launch, one split launch, one persistent
-// digit-GEMM launch over every product's tiles.  Returns DGT_ERROR_UNSUPPORTED (with no
-// work issued) when a product's K is too long for whole-K exact INT32 digit products; the
-// caller then runs the products one by one.
-dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& probs, int slices);
+// All products in one INT8 emulation pass: one amax launch, one split launch, one persistent
+// GEMM launch over every product's tiles (and, for the CRT scheme, one reconstruction
+// launch).  slices = digit slices, or moduli when crt.  Returns DGT_ERROR_UNSUPPORTED (with
+// no work issued) when a product's K is too long for the grouped form; the caller then runs
+// the products one by one.
+dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& probs, int slices, bool crt);
 
 }  // namespace dgt

@@ -32,6 +32,7 @@
 #include <cstring>
 #include <vector>
 
+#include "crt.cuh"
 #include "dgt_internal.cuh"
 #include "tc_engine.cuh"
 
@@ -154,36 +155,6 @@ __global__ void __launch_bounds__(128) split_digits(const double* __restrict__ X
 }
 
 // ---- grouped pre-pass: one launch scales (or splits) every operand of a grouped call -------
-// Each operand is a job; a job owns a contiguous range of the launch's blocks, found by
-// binary search on the jobs' first block.
-struct SplitJob {
-    const double* X;
-    int64_t ld, MN, K, mn_pad, k_pad;
-    unsigned long long* amax;
-    int32_t* exps;
-    void* planes;
-    int32_t kcontig;
-    int32_t amax_bx;        // amax blocks along mn (MN-contiguous jobs: times amax_by along K)
-    int32_t amax_by;
-    int32_t split_bx;       // split blocks along mn (times k_pad / 32 along K)
-    int64_t amax_begin;     // first block of this job in the amax launch
-    int64_t split_begin;    // first block of this job in the split launch
-};
-constexpr int AMAX_KCHUNK = 64;  // K rows per block of the MN-contiguous amax (fills the GPU)
-
-__device__ __forceinline__ int find_job(const SplitJob* __restrict__ jobs, int njobs, int64_t blk, bool split) {
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        const int64_t b0 = split ? jobs[mid].split_begin : jobs[mid].amax_begin;
-        if (b0 <= blk)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
 __global__ void __launch_bounds__(256) amax_grouped(const SplitJob* __restrict__ jobs, int njobs) {
     const int64_t blk = blockIdx.x;
     const SplitJob& J = jobs[find_job(jobs, njobs, blk, false)];
@@ -473,41 +444,54 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
 
 // ---- grouped: every product of a batch in one pre-pass and one persistent GEMM launch ----------
 
-template <class CF>
+template <class CF, int EPI>
 static cudaError_t launch_ozaki_grouped(const oz::Params& prm, int grid, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(oz::digit_gemm<CF, 0, 0, true>,
+        cudaError_t e = cudaFuncSetAttribute(oz::digit_gemm<CF, 0, EPI, true>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
         if (e != cudaSuccess) return e;
         attr = true;
     }
     static const CUtensorMap unused = {};  // grouped mode reads each problem's maps from its table
-    oz::digit_gemm<CF, 0, 0, true><<<grid, CF::THREADS, CF::SMEM, s>>>(unused, unused, prm);
+    oz::digit_gemm<CF, 0, EPI, true><<<grid, CF::THREADS, CF::SMEM, s>>>(unused, unused, prm);
     return cudaGetLastError();
 }
 
-dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& probs, int S) {
+dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& probs, int S, bool crt) {
     const int T = (int)probs.size();
     if (T == 0) return DGT_SUCCESS;
-    if (S < 2 || S > 16) return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16]");
+    if (!valid_slices(crt ? DGT_FP64_OZAKI2_INT8 : DGT_FP64_OZAKI_INT8, S))
+        return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16] (moduli: [8, 20])");
     // variants 0 and 1 (4 or 8 epilogue warps, 128-byte stages); the others run as variant 1
     const int variant = h->ozaki_variant == 0 ? 0 : 1;
     const int tkb = 128;
     auto up = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
 
-    // The flush schedule is built for the longest K: a group that is exact for it is exact for
-    // every shorter K.  Segments run over each product's own K (kb1 = -1).
     int64_t k_pad_max = 0;
     for (const OzProblem& p : probs) k_pad_max = std::max(k_pad_max, ceil_div(p.k, oz::KPAD) * oz::KPAD);
     std::vector<oz::Seg> segs;
     std::vector<oz::Group> groups;
-    if (!ozaki_schedule(S, k_pad_max, tkb, false, segs, groups) || segs.size() > (size_t)oz::MAX_SEGS ||
-        groups.size() > (size_t)oz::MAX_GROUPS)
-        return DGT_ERROR_UNSUPPORTED;
-    for (oz::Seg& sg : segs) {
-        if (sg.kb0 != 0) return DGT_ERROR_UNSUPPORTED;  // K-chunked diagonals: not in grouped form
-        sg.kb1 = -1;
+    oz2::CrtConst cc;
+    oz2::ModTable mt;
+    if (crt) {
+        // one group per modulus, each the residue product over the product's own K
+        if (k_pad_max >= (int64_t)1 << 17) return DGT_ERROR_UNSUPPORTED;
+        oz2::crt_constants(S, cc, mt);
+        for (int j = 0; j < S; ++j) {
+            segs.push_back(oz::Seg{j, j, 0, -1});
+            groups.push_back(oz::Group{j, j + 1, 0, mt.p[j]});
+        }
+    } else {
+        // The flush schedule is built for the longest K: a group that is exact for it is exact
+        // for every shorter K.  Segments run over each product's own K (kb1 = -1).
+        if (!ozaki_schedule(S, k_pad_max, tkb, false, segs, groups) || segs.size() > (size_t)oz::MAX_SEGS ||
+            groups.size() > (size_t)oz::MAX_GROUPS)
+            return DGT_ERROR_UNSUPPORTED;
+        for (oz::Seg& sg : segs) {
+            if (sg.kb0 != 0) return DGT_ERROR_UNSUPPORTED;  // K-chunked diagonals: not in grouped form
+            sg.kb1 = -1;
+        }
     }
 
     // Tiles are numbered product by product, longest K first, so the persistent CTAs' static
@@ -516,10 +500,12 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     for (int i = 0; i < T; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return probs[a].k > probs[b].k; });
 
-    // scratch: per product planes A | planes B (1 KB aligned), then all amax words, all exponents
+    // scratch: per product planes A | planes B | residues (CRT) (1 KB aligned), then all amax
+    // words, all exponents
     struct Off {
         int64_t m_pad, n_pad, k_pad;
-        size_t pa, pb, xa, xb, ea, eb;
+        size_t pa, pb, rs, xa, xb, ea, eb;
+        int bits;
     };
     std::vector<Off> off(T);
     size_t planes = 0, amax_words = 0, exp_words = 0;
@@ -529,11 +515,15 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
         o.m_pad = ceil_div(p.m, oz::TM) * oz::TM;
         o.n_pad = ceil_div(p.n, oz::TN) * oz::TN;
         o.k_pad = ceil_div(p.k, oz::KPAD) * oz::KPAD;
+        o.bits = crt ? oz2::beta_for(S, p.k) : 0;
+        if (crt && o.bits < 8) return DGT_ERROR_UNSUPPORTED;
         if ((int64_t)S * std::max(o.m_pad, o.n_pad) > INT32_MAX) return DGT_ERROR_UNSUPPORTED;
         o.pa = planes;
         planes += up((size_t)S * o.m_pad * o.k_pad, 1024);
         o.pb = planes;
         planes += up((size_t)S * o.n_pad * o.k_pad, 1024);
+        o.rs = planes;
+        if (crt) planes += up((size_t)S * o.m_pad * o.n_pad, 1024);
         o.xa = amax_words;
         amax_words += (size_t)p.m;
         o.xb = amax_words;
@@ -552,18 +542,23 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     auto* amax = (unsigned long long*)(base + amax_at);
     auto* exps = (int32_t*)(base + exp_at);
 
-    // host tables: GProb[T] (tensor maps inside, 64-byte aligned) and SplitJob[2T], zeroed
-    // byte for byte so that padding hashes the same on every call
+    // host tables: GProb[T] (tensor maps inside, 64-byte aligned), SplitJob[2T] and, for CRT,
+    // CrtJob[T], zeroed byte for byte so that padding hashes the same on every call
     const size_t job_bytes = (size_t)2 * T * sizeof(oz::SplitJob);
+    const size_t crt_bytes = crt ? (size_t)T * sizeof(oz2::CrtJob) : 0;
     static thread_local std::vector<oz::GProb> host_gp;
     static thread_local std::vector<oz::SplitJob> host_jobs;
+    static thread_local std::vector<oz2::CrtJob> host_crt;
     host_gp.resize(T);
     host_jobs.resize(2 * (size_t)T);
+    host_crt.resize(crt ? T : 1);
     std::memset((void*)host_gp.data(), 0, (size_t)T * sizeof(oz::GProb));
     std::memset((void*)host_jobs.data(), 0, job_bytes);
+    std::memset((void*)host_crt.data(), 0, host_crt.size() * sizeof(oz2::CrtJob));
     oz::GProb* gp = host_gp.data();
     oz::SplitJob* jobs = host_jobs.data();
-    int64_t amax_blocks = 0, split_blocks = 0;
+    oz2::CrtJob* cj = host_crt.data();
+    int64_t amax_blocks = 0, split_blocks = 0, crt_threads = 0;
     int32_t tiles = 0;
     for (int r = 0; r < T; ++r) {
         const int i = order[r];
@@ -589,6 +584,26 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
         g.tiles_m = (int32_t)(o.m_pad / oz::TM);
         g.tiles_n = (int32_t)(o.n_pad / oz::TN);
         g.tile_begin = tiles;
+        if (crt) {
+            g.res = (uint8_t*)(base + o.rs);
+            g.res_ld = o.m_pad;
+            g.res_plane = o.m_pad * o.n_pad;
+            oz2::CrtJob& c = cj[r];
+            c.res = g.res;
+            c.res_ld = g.res_ld;
+            c.res_plane = g.res_plane;
+            c.m = p.m;
+            c.n = p.n;
+            c.row_exp = g.row_exp;
+            c.col_exp = g.col_exp;
+            c.alpha = p.alpha;
+            c.beta = p.beta;
+            c.C = p.C;
+            c.ldc = p.ldc;
+            c.bits = o.bits;
+            c.thread_begin = crt_threads;
+            crt_threads += ceil_div(p.m, 4) * p.n;
+        }
         tiles += g.tiles_m * g.tiles_n;
         // op(A) is m x k: 'N' -> MN-contiguous; op(B) as its transpose n x k: 'N' -> K-contiguous
         const bool kc[2] = {p.ta, !p.tb};
@@ -613,33 +628,39 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
             J.split_bx = (int32_t)ceil_div(pad[t], 128);
             J.amax_begin = amax_blocks;
             J.split_begin = split_blocks;
+            J.bits = o.bits;
             amax_blocks += (int64_t)J.amax_bx * J.amax_by;
             split_blocks += (int64_t)J.split_bx * (o.k_pad / 32);
         }
     }
-    if (amax_blocks > INT32_MAX || split_blocks > INT32_MAX)
+    if (amax_blocks > INT32_MAX || split_blocks > INT32_MAX || crt_threads / 256 > INT32_MAX)
         return fail(h, DGT_ERROR_UNSUPPORTED, "grouped Ozaki batch too large for one launch");
 
     // device copy of the tables from the handle's cache (a repeated call, e.g. from a
     // replayed CUDA graph, needs no copy)
-    const void* parts[2] = {gp, jobs};
-    const size_t part_bytes[2] = {(size_t)T * sizeof(oz::GProb), job_bytes};
-    size_t offs[2];
+    const void* parts[3] = {gp, jobs, cj};
+    const size_t part_bytes[3] = {(size_t)T * sizeof(oz::GProb), job_bytes, crt_bytes};
+    size_t offs[3];
     void* table = nullptr;
-    st = device_table(h, 2, parts, part_bytes, &table, offs);
+    st = device_table(h, crt ? 3 : 2, parts, part_bytes, &table, offs);
     if (st != DGT_SUCCESS) return st;
     cudaStream_t s = h->stream;
     const auto* d_gp = (const oz::GProb*)((char*)table + offs[0]);
     const auto* d_jobs = (const oz::SplitJob*)((char*)table + offs[1]);
+    const auto* d_crt = crt ? (const oz2::CrtJob*)((char*)table + offs[2]) : nullptr;
 
     mark(h, 0);
     DGT_CUDA_TRY(h, cudaMemsetAsync(amax, 0, amax_words * 8, s));
     oz::amax_grouped<<<(unsigned)amax_blocks, 256, 0, s>>>(d_jobs, 2 * T);
     h->launches.fetch_add(1);
     DGT_CUDA_TRY(h, cudaGetLastError());
-    oz::split_grouped<<<(unsigned)split_blocks, 128, 0, s>>>(d_jobs, 2 * T, S);
+    if (crt) {
+        DGT_CUDA_TRY(h, oz2::launch_split_residues_grouped(s, d_jobs, 2 * T, split_blocks, S, mt));
+    } else {
+        oz::split_grouped<<<(unsigned)split_blocks, 128, 0, s>>>(d_jobs, 2 * T, S);
+        DGT_CUDA_TRY(h, cudaGetLastError());
+    }
     h->launches.fetch_add(1);
-    DGT_CUDA_TRY(h, cudaGetLastError());
 
     static thread_local oz::Params prm;
     prm = oz::Params{};
@@ -654,14 +675,22 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     prm.total_tiles = tiles;
     const int grid = std::min<int>(tiles, h->num_sms);
     mark(h, 1);
-    cudaError_t le = variant == 0 ? launch_ozaki_grouped<oz::OzCfg<4, 128, 4>>(prm, grid, s)
-                                  : launch_ozaki_grouped<oz::OzCfg<8, 128, 4>>(prm, grid, s);
+    cudaError_t le;
+    if (crt)
+        le = variant == 0 ? launch_ozaki_grouped<oz::OzCfg<4, 128, 4>, 2>(prm, grid, s)
+                          : launch_ozaki_grouped<oz::OzCfg<8, 128, 4>, 2>(prm, grid, s);
+    else
+        le = variant == 0 ? launch_ozaki_grouped<oz::OzCfg<4, 128, 4>, 0>(prm, grid, s)
+                          : launch_ozaki_grouped<oz::OzCfg<8, 128, 4>, 0>(prm, grid, s);
     h->launches.fetch_add(1);
-    if (le != cudaSuccess) return cuda_fail(h, le, "grouped ozaki_i8_gemm launch");
+    if (le != cudaSuccess) return cuda_fail(h, le, "grouped digit GEMM launch");
     mark(h, 2);
+    if (crt) {
+        DGT_CUDA_TRY(h, oz2::launch_crt_grouped(s, d_crt, T, crt_threads, cc, S));
+        h->launches.fetch_add(1);
+    }
     return DGT_SUCCESS;
 }
-
 
 dgt_status ozaki_amax(dgt_context* h, cudaStream_t s, const double* X, int64_t ld, int64_t MN, int64_t K,
                       bool kcontig, unsigned long long* out) {

@@ -27,36 +27,16 @@
 #include <cstdint>
 #include <vector>
 
+#include "crt.cuh"
 #include "dgt_internal.cuh"
 #include "tc_engine.cuh"
 
 namespace dgt {
 namespace oz2 {
 
-constexpr int MAX_MODULI = 20, MIN_MODULI = 8;
-constexpr int MAX_BETA = 58;   // |A'| < 2^58: residues by FP64 division stay exact
 // Pairwise coprime, largest first (greedy from 256 down).
 constexpr int kModuli[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                                      223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
-
-// Residues of x = trunc(a 2^(beta-e)) (|x| < 2^58) modulo p, in integers: xu = x + 2^58 is
-// split into 20-bit chunks x0, x1, x2 and t = x2 c40 + x1 c20 + x0 + off (< 2^29) is congruent
-// to x; t / p = (t magic) >> 37 exactly for t < 2^29 (Granlund & Montgomery 1994, thm 4.2:
-// magic = floor(2^37 / p) + 1 for 2^7 < p <= 2^8).
-struct ModTable {
-    int32_t p[MAX_MODULI];
-    uint32_t c20[MAX_MODULI], c40[MAX_MODULI];  // 2^20 mod p, 2^40 mod p
-    uint32_t off[MAX_MODULI];                    // p - (2^58 mod p)
-    uint32_t magic[MAX_MODULI];
-};
-
-constexpr int MAX_NW = 5;  // 32-bit limbs of W_p and P (P < 2^160)
-struct CrtConst {
-    int32_t n;
-    uint32_t W[MAX_MODULI][MAX_NW];
-    uint32_t P[MAX_NW + 1], Phalf[MAX_NW + 1];  // Phalf = floor((P - 1) / 2)
-    double kq[MAX_NW + 1];                      // 2^(32 l) / P: X / P ~ sum_l x_l kq_l
-};
 
 // ---- host: CRT constants in 32-bit limbs ------------------------------------------------------
 using Big = std::vector<uint32_t>;  // little-endian limbs
@@ -101,15 +81,15 @@ static double log2_product(int n) {
 }
 
 // Largest beta with 2 k (2^beta - 1)^2 < P (with a 1e-9 margin on the logarithms).
-static int beta_for(int n, int64_t k) {
+int beta_for(int n, int64_t k) {
     const double b = (log2_product(n) - 1.0 - std::log2((double)std::max<int64_t>(k, 1))) / 2.0 - 1e-9;
     return std::min(MAX_BETA, (int)std::floor(b));
 }
 
 // Limbs of W_p and P for n moduli (P < 2^(32 nw)).
-static int limbs_for(int n) { return (int)std::ceil(log2_product(n) / 32.0); }
+int limbs_for(int n) { return (int)std::ceil(log2_product(n) / 32.0); }
 
-static void crt_constants(int n, CrtConst& cc, ModTable& mt) {
+void crt_constants(int n, CrtConst& cc, ModTable& mt) {
     cc = CrtConst{};
     mt = ModTable{};
     cc.n = n;
@@ -146,18 +126,18 @@ static void crt_constants(int n, CrtConst& cc, ModTable& mt) {
 // length k_pad, mn_pad rows, zero padded).  Each thread produces 32 consecutive kk of one mn;
 // the by == 0 blocks also write exps[mn].
 template <bool K_CONTIG>
-__global__ void __launch_bounds__(128) split_residues(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                                                      int64_t mn_pad, int64_t k_pad, int nmod, int beta,
-                                                      const unsigned long long* __restrict__ amax,
-                                                      int32_t* __restrict__ exps, int8_t* __restrict__ planes,
-                                                      const __grid_constant__ ModTable mt) {
-    const int64_t mn = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t k0 = (int64_t)blockIdx.y * 32;
+__device__ __forceinline__ void residue_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                              int64_t mn_pad, int64_t k_pad, int nmod, int beta,
+                                              const unsigned long long* __restrict__ amax, int32_t* __restrict__ exps,
+                                              int8_t* __restrict__ planes, const ModTable& mt, int64_t bx,
+                                              int64_t by) {
+    const int64_t mn = bx * blockDim.x + threadIdx.x;
+    const int64_t k0 = by * 32;
     if (mn >= mn_pad) return;
     int e = 0;
     if (mn < MN) {
         e = oz::exponent_of_max(amax[mn]);
-        if (blockIdx.y == 0) exps[mn] = e;
+        if (by == 0) exps[mn] = e;
     }
     const bool live = (mn < MN) && (e != oz::EXP_NONFINITE);
     uint32_t x0[32], x1[32], x2[32];  // 20-bit chunks of x + 2^58
@@ -194,6 +174,30 @@ __global__ void __launch_bounds__(128) split_residues(const double* __restrict__
         o4[0] = make_uint4(w[0], w[1], w[2], w[3]);
         o4[1] = make_uint4(w[4], w[5], w[6], w[7]);
     }
+}
+
+template <bool K_CONTIG>
+__global__ void __launch_bounds__(128) split_residues(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                                      int64_t mn_pad, int64_t k_pad, int nmod, int beta,
+                                                      const unsigned long long* __restrict__ amax,
+                                                      int32_t* __restrict__ exps, int8_t* __restrict__ planes,
+                                                      const __grid_constant__ ModTable mt) {
+    residue_block<K_CONTIG>(X, ld, MN, K, mn_pad, k_pad, nmod, beta, amax, exps, planes, mt, blockIdx.x, blockIdx.y);
+}
+
+// Every operand of a grouped call in one launch (job table as for the digit split).
+__global__ void __launch_bounds__(128) split_residues_grouped(const oz::SplitJob* __restrict__ jobs, int njobs,
+                                                              int nmod, const __grid_constant__ ModTable mt) {
+    const int64_t blk = blockIdx.x;
+    const oz::SplitJob& J = jobs[oz::find_job(jobs, njobs, blk, true)];
+    const int64_t local = blk - J.split_begin;
+    const int64_t bx = local % J.split_bx, by = local / J.split_bx;
+    if (J.kcontig)
+        residue_block<true>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, nmod, J.bits, J.amax, J.exps,
+                            (int8_t*)J.planes, mt, bx, by);
+    else
+        residue_block<false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, nmod, J.bits, J.amax, J.exps,
+                             (int8_t*)J.planes, mt, bx, by);
 }
 
 // ---- device: reconstruction -----------------------------------------------------------------------
@@ -342,19 +346,13 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
     return neg ? -mag : mag;
 }
 
-// Thread per 4 consecutive rows of one column of C; residue planes [j][col][row] with
-// leading dimension res_ld (a multiple of 4).
+// Rows row0 .. row0+3 of column col of one product: residue planes [j][col][row] with leading
+// dimension res_ld (a multiple of 4).
 template <int NW>
-__global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
-                                                       int64_t res_plane, int64_t m, int64_t n,
-                                                       const int32_t* __restrict__ row_exp,
-                                                       const int32_t* __restrict__ col_exp, int beta, double alpha,
-                                                       double beta_c, double* __restrict__ C, int64_t ldc,
-                                                       const __grid_constant__ CrtConst cc) {
-    const int64_t quads = (m + 3) / 4;
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= quads * n) return;
-    const int64_t col = idx / quads, row0 = (idx % quads) * 4;
+__device__ __forceinline__ void crt_quad(const uint8_t* __restrict__ res, int64_t res_ld, int64_t res_plane,
+                                         int64_t m, int64_t row0, int64_t col, const int32_t* __restrict__ row_exp,
+                                         const int32_t* __restrict__ col_exp, int beta, double alpha, double beta_c,
+                                         double* __restrict__ C, int64_t ldc, const CrtConst& cc) {
     uint32_t rr[MAX_MODULI];  // four rows' residues per modulus, one byte each
 #pragma unroll
     for (int j = 0; j < MAX_MODULI; ++j)
@@ -373,6 +371,60 @@ __global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict
         double* cp = C + row + col * ldc;
         *cp = beta_c != 0.0 ? fma(alpha, val, beta_c * *cp) : alpha * val;
     }
+}
+
+// Thread per 4 consecutive rows of one column of C.
+template <int NW>
+__global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
+                                                       int64_t res_plane, int64_t m, int64_t n,
+                                                       const int32_t* __restrict__ row_exp,
+                                                       const int32_t* __restrict__ col_exp, int beta, double alpha,
+                                                       double beta_c, double* __restrict__ C, int64_t ldc,
+                                                       const __grid_constant__ CrtConst cc) {
+    const int64_t quads = (m + 3) / 4;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= quads * n) return;
+    crt_quad<NW>(res, res_ld, res_plane, m, (idx % quads) * 4, idx / quads, row_exp, col_exp, beta, alpha, beta_c, C,
+                 ldc, cc);
+}
+
+// Every product of a grouped call: thread -> product by binary search on thread_begin.
+template <int NW>
+__global__ void __launch_bounds__(256) crt_grouped(const CrtJob* __restrict__ jobs, int njobs, int64_t threads,
+                                                   const __grid_constant__ CrtConst cc) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= threads) return;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].thread_begin <= idx)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const CrtJob& J = jobs[lo];
+    const int64_t local = idx - J.thread_begin, quads = (J.m + 3) / 4;
+    if (local >= quads * J.n) return;
+    crt_quad<NW>(J.res, J.res_ld, J.res_plane, J.m, (local % quads) * 4, local / quads, J.row_exp, J.col_exp, J.bits,
+                 J.alpha, J.beta, J.C, J.ldc, cc);
+}
+
+cudaError_t launch_split_residues_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks,
+                                          int nmod, const ModTable& mt) {
+    split_residues_grouped<<<(unsigned)blocks, 128, 0, s>>>(jobs, njobs, nmod, mt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, int64_t threads, const CrtConst& cc,
+                               int nmod) {
+    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    switch (limbs_for(nmod)) {
+        case 2: crt_grouped<2><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
+        case 3: crt_grouped<3><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
+        case 4: crt_grouped<4><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
+        default: crt_grouped<5><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace oz2

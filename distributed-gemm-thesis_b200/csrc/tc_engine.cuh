@@ -91,6 +91,8 @@ struct alignas(64) GProb {
     const int32_t* col_exp;
     double alpha, beta;
     int32_t m_pad, n_pad, nkb, tiles_m, tiles_n, tile_begin;
+    uint8_t* res;  // EPI_MODE 2: residue planes of this product
+    int64_t res_ld, res_plane;
 };
 
 // The tile a role works on: its coordinates and, in grouped mode, its problem descriptor
@@ -573,7 +575,8 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                         // exact: |acc| < 2^31, so (double)acc / p floors to q or q - 1 at worst
                         const int pm = GROUPS[g].pad;
                         const double inv = 1.0 / (double)pm;
-                        uint8_t* rbase = P.res + (int64_t)g * P.res_plane + row + (n0 + ch * 32) * P.res_ld;
+                        uint8_t* rbase = DGT_TILE_FIELD(cx, res, res) + (int64_t)g * DGT_TILE_FIELD(cx, res_plane, res_plane) +
+                                         row + (n0 + ch * 32) * DGT_TILE_FIELD(cx, res_ld, res_ld);
 #pragma unroll
                         for (int c = 0; c < 32; ++c) {
                             if (c < ncols) {
@@ -581,7 +584,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                                 int r = x - pm * (int)floor((double)x * inv);
                                 if (r < 0) r += pm;
                                 if (r >= pm) r -= pm;
-                                rbase[c * P.res_ld] = (uint8_t)r;
+                                rbase[c * DGT_TILE_FIELD(cx, res_ld, res_ld)] = (uint8_t)r;
                             }
                         }
                         continue;

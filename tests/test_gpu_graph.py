@@ -42,6 +42,10 @@ def test_capture_and_replay_all_paths():
     ekeep = [dev(O.uniform((d["m"], d["n"]), 500 + i)) for i, d in enumerate(gdesc)]
     edesc = [dict(d, C=ptr(c)) for d, c in zip(gdesc, ekeep)]
     eC0 = [x.clone() for x in ekeep]
+    # and once more through the CRT scheme's grouped pass
+    rkeep = [dev(O.uniform((d["m"], d["n"]), 700 + i)) for i, d in enumerate(gdesc)]
+    rdesc = [dict(d, C=ptr(c)) for d, c in zip(gdesc, rkeep)]
+    rC0 = [x.clone() for x in rkeep]
 
     def batch(h):
         h.dgemm("N", "N", m, n, k, 1.0, ptr(dA), m, ptr(dB), k, 0.5, ptr(outs["native"]), m, mode=dgt.FP64_NATIVE)
@@ -52,6 +56,7 @@ def test_capture_and_replay_all_paths():
                     mode=dgt.FP64_OZAKI_INT8, slices=7)
         h.dgemm_grouped(gdesc)
         h.dgemm_grouped(edesc, mode=dgt.FP64_OZAKI_INT8, slices=7)
+        h.dgemm_grouped(rdesc, mode=dgt.FP64_OZAKI2_INT8, slices=16)
 
     def reset():
         for name in outs:
@@ -64,6 +69,8 @@ def test_capture_and_replay_all_paths():
             x[2].copy_(x0)
         for x, x0 in zip(ekeep, eC0):
             x.copy_(x0)
+        for x, x0 in zip(rkeep, rC0):
+            x.copy_(x0)
 
     with dgt.Handle() as h:
         side = torch.cuda.Stream()
@@ -74,7 +81,7 @@ def test_capture_and_replay_all_paths():
             batch(h)  # eager again, now with the final workspace: every table is resident
         torch.cuda.synchronize()
         eager = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
-                 [x.clone() for x in ekeep] + [x.clone() for x in tE])
+                 [x.clone() for x in ekeep] + [x.clone() for x in tE] + [x.clone() for x in rkeep])
         reset()
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
@@ -86,7 +93,7 @@ def test_capture_and_replay_all_paths():
         torch.cuda.synchronize()
         h.check_device()
         replay = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
-                  [x.clone() for x in ekeep] + [x.clone() for x in tE])
+                  [x.clone() for x in ekeep] + [x.clone() for x in tE] + [x.clone() for x in rkeep])
         for a, b in zip(eager, replay):
             assert torch.equal(a, b)
         # and a second replay after another reset gives the same again

@@ -128,3 +128,54 @@ def test_grouped_ragged_batch_against_oracle():
         h.check_device()
     for it, k in zip(items, keep):
         assert O.rel_errors(host(k[2], (it["m"], it["n"])), _want(it))[1] <= FRO_TOL
+
+
+def test_grouped_crt_matches_per_product_bitwise():
+    """The CRT scheme in one grouped pass (amax, residue split, residue GEMM, reconstruction)
+    equals one CRT call per product bit for bit: same operand bits per product, same residues,
+    same exact reconstruction."""
+    import torch
+
+    items = _batch(13, 20, 1, 700) + _batch(14, 4, 200, 5000)
+    with dgt.Handle() as h:
+        descs, keep = _descs(items)
+        n0 = h.launch_count()
+        h.dgemm_grouped(descs, mode=dgt.FP64_OZAKI2_INT8, slices=16)
+        torch.cuda.synchronize()
+        h.check_device()
+        assert h.launch_count() - n0 == 4
+        grouped = [host(k[2], (it["m"], it["n"])) for it, k in zip(items, keep)]
+        for idx, (it, d) in enumerate(zip(items, descs)):
+            dC = dev(it["C"])
+            h.dgemm(it["ta"], it["tb"], it["m"], it["n"], it["k"], it["alpha"], d["A"], d["lda"], d["B"], d["ldb"],
+                    it["beta"], ptr(dC), it["m"], mode=dgt.FP64_OZAKI2_INT8, slices=16)
+            torch.cuda.synchronize()
+            assert np.array_equal(host(dC, (it["m"], it["n"])), grouped[idx]), (it["m"], it["n"], it["k"])
+    for it, got in zip(items, grouped):
+        assert O.rel_errors(got, _want(it))[1] <= FRO_TOL
+
+
+def test_grouped_crt_edge_products():
+    import torch
+
+    items = _batch(15, 5, 32, 300)
+    items.append(dict(m=1, n=1, k=1, ta="N", tb="N", A=O.uniform((1, 1), 5), B=O.uniform((1, 1), 6),
+                      C=O.uniform((1, 1), 7), alpha=1.5, beta=-0.5))
+    items.append(dict(m=70, n=40, k=0, ta="N", tb="N", A=np.zeros((70, 1)), B=np.zeros((1, 40)),
+                      C=O.uniform((70, 40), 8), alpha=1.0, beta=0.5))
+    with dgt.Handle() as h:
+        descs, keep = _descs(items)
+        for d in descs:
+            if d["k"] == 0:
+                d["ldb"] = 1
+        x = dev(np.zeros((1, 1)))
+        descs.append(dict(m=0, n=5, k=5, alpha=1.0, beta=0.0, A=ptr(x), lda=1, B=ptr(x), ldb=5, C=ptr(x), ldc=1))
+        h.dgemm_grouped(descs, mode=dgt.FP64_OZAKI2_INT8, slices=17)
+        torch.cuda.synchronize()
+        h.check_device()
+    for it, k in zip(items, keep):
+        got = host(k[2], (it["m"], it["n"]))
+        if it["k"] == 0:
+            assert np.array_equal(got, 0.5 * it["C"])
+        else:
+            assert O.rel_errors(got, _want(it))[1] <= FRO_TOL
