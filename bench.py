@@ -149,14 +149,22 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The largest x over all ranks (every rank gets it); a device tensor under NCCL, a host
+    tensor under gloo."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_tflops(world, flops_per_rank, ms_max):
+    """Whole-job rate of `world` replicas that each did flops_per_rank, timed by the slowest."""
+    return world * flops_per_rank / (ms_max * 1e-3) / 1e12
 
 
 # ---- reference arm (CPU) ------------------------------------------------------------------------
@@ -751,7 +759,7 @@ def main():
     clocks = sampler.stop()
     launches = (h.launch_count() - launches0) // (args.steps + args.warmup)
     emu_ms = max_over_ranks(emu_ms, world)
-    value = world * flops / (emu_ms * 1e-3) / 1e12
+    value = job_tflops(world, flops, emu_ms)
 
     # ---- roofline of the dominant kernel (the INT8 tcgen05 GEMM), timed live with events ----
     h.set_tuning(dgt.TUNE_PROFILE, 1)
@@ -815,7 +823,7 @@ def main():
 
     e2e_ms = timed(e2e_step, max(2, args.steps // 2), 1)
     e2e_ms = max_over_ranks(e2e_ms, world)
-    e2e_v = world * flops / (e2e_ms * 1e-3) / 1e12
+    e2e_v = job_tflops(world, flops, e2e_ms)
 
     # ---- CPU baseline: the reference's validation GEMM (OpenBLAS dgemm), bounded sample ----
     cpu = None
@@ -847,14 +855,14 @@ def main():
                        "M": n, "N": n, "K": n, "alpha": ALPHA, "beta": BETA, "phi": PHI, "scheme": best, "count": S,
                        "l2": "inputs larger than L2 (2 GiB each), no flush", "parallelism":
                            f"replicas x{world}" if world > 1 else "1 GPU"},
-            "native_dmma": {"value": world * flops / (nat_ms * 1e-3) / 1e12, "ms_per_step": nat_ms,
+            "native_dmma": {"value": job_tflops(world, flops, nat_ms), "ms_per_step": nat_ms,
                             "max_rel": nat_err[0], "fro_rel": nat_err[1], "kernel_variant": tuned_native["variant"]},
             "emulated": {"value": value, "scheme": best, "count": S, "max_rel": errs[(best, S)][0],
                          "fro_rel": errs[(best, S)][1], "equal_error": equal_error,
                          "speedup_vs_native": nat_ms / emu_ms, "split_ms": split_ms, "gemm_ms": gemm_ms,
                          "kernel_variant": tuned[best]["variant"]},
             "other_scheme": {"scheme": other, "count": chosen[other],
-                             "value": world * flops / (other_ms * 1e-3) / 1e12, "ms_per_step": other_ms,
+                             "value": job_tflops(world, flops, other_ms), "ms_per_step": other_ms,
                              "max_rel": errs[(other, chosen[other])][0], "fro_rel": errs[(other, chosen[other])][1],
                              "kernel_variant": tuned[other]["variant"]},
             "errors_by_count": {f"{k[0]}_{k[1]}": v for k, v in errs.items()},
