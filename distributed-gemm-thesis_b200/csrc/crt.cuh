@@ -54,19 +54,23 @@ constexpr int MAX_BETA = 58;  // |A'| < 2^58
 
 // Residues of x = trunc(a 2^(beta-e)) (|x| < 2^58) modulo p, in integers: xu = x + 2^58 is
 // split into 20-bit chunks x0, x1, x2 and t = x2 c40 + x1 c20 + x0 + off (< 2^29) is congruent
-// to x; t / p = (t magic) >> 37 exactly for t < 2^29 (Granlund & Montgomery 1994, thm 4.2:
+// to x + floor(p/2); t / p = (t magic) >> 37 exactly for t < 2^29 (Granlund & Montgomery 1994, thm 4.2:
 // magic = floor(2^37 / p) + 1 for 2^7 < p <= 2^8).
+// The symmetric residue is (t + floor(p/2)) mod p - floor(p/2): off carries the + floor(p/2)
+// and h4 (floor(p/2) in every byte) takes it back off four packed residues at once.
 struct ModTable {
     int32_t p[MAX_MODULI];
     uint32_t c20[MAX_MODULI], c40[MAX_MODULI];  // 2^20 mod p, 2^40 mod p
-    uint32_t off[MAX_MODULI];                    // p - (2^58 mod p)
+    uint32_t off[MAX_MODULI];                    // p - (2^58 mod p) + floor(p/2)
     uint32_t magic[MAX_MODULI];
+    uint32_t h4[MAX_MODULI];                     // floor(p/2) * 0x01010101
 };
+constexpr int RES_ELEMS = 32;  // K elements one thread of the residue split turns into bytes (16: 2x slower)
 
 struct CrtConst {
     int32_t n;
     uint32_t W[MAX_MODULI][MAX_NW];
-    uint32_t P[MAX_NW + 1], Phalf[MAX_NW + 1];  // Phalf = floor((P - 1) / 2)
+    uint32_t P[MAX_NW + 1];
     double kq[MAX_NW + 1];                      // 2^(32 l) / P: X / P ~ sum_l x_l kq_l
 };
 

@@ -630,7 +630,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
             J.split_begin = split_blocks;
             J.bits = o.bits;
             amax_blocks += (int64_t)J.amax_bx * J.amax_by;
-            split_blocks += (int64_t)J.split_bx * (o.k_pad / 32);
+            split_blocks += (int64_t)J.split_bx * (o.k_pad / (crt ? oz2::RES_ELEMS : 32));
         }
     }
     if (amax_blocks > INT32_MAX || split_blocks > INT32_MAX || crt_threads / 256 > INT32_MAX)

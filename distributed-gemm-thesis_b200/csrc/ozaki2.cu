@@ -100,7 +100,8 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
         mt.p[i] = (int32_t)p;
         mt.c20[i] = (uint32_t)((1ull << 20) % p);
         mt.c40[i] = (uint32_t)((1ull << 40) % p);
-        mt.off[i] = p - (uint32_t)((1ull << 58) % p);
+        mt.off[i] = p - (uint32_t)((1ull << 58) % p) + (p >> 1);
+        mt.h4[i] = (p >> 1) * 0x01010101u;
         mt.magic[i] = (uint32_t)((1ull << 37) / p + 1);
         Big M = P;
         big_div_small(M, p);  // M = P / p
@@ -110,12 +111,6 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
         for (int l = 0; l < MAX_NW; ++l) cc.W[i][l] = l < (int)M.size() ? M[l] : 0;
     }
     for (int l = 0; l <= MAX_NW; ++l) cc.P[l] = l < (int)P.size() ? P[l] : 0;
-    Big H = P;  // floor((P - 1) / 2)
-    for (size_t l = 0; l < H.size(); ++l) {  // H -= 1 (P > 1)
-        if (H[l]--) break;
-    }
-    big_div_small(H, 2);
-    for (int l = 0; l <= MAX_NW; ++l) cc.Phalf[l] = l < (int)H.size() ? H[l] : 0;
     double pd = 0;
     for (int l = MAX_NW; l >= 0; --l) pd = pd * 4294967296.0 + (double)cc.P[l];
     for (int l = 0; l <= MAX_NW; ++l) cc.kq[l] = std::ldexp(1.0, 32 * l) / pd;
@@ -123,16 +118,17 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
 
 // ---- device: residue planes ----------------------------------------------------------------------
 // Plane j holds (A' mod p_j) in the symmetric range as int8 at [j][mn][kk] (K-major, row
-// length k_pad, mn_pad rows, zero padded).  Each thread produces 32 consecutive kk of one mn;
-// the by == 0 blocks also write exps[mn].
+// length k_pad, mn_pad rows, zero padded).  Each thread produces RES_ELEMS consecutive kk of
+// one mn; the by == 0 blocks also write exps[mn].
 template <bool K_CONTIG>
 __device__ __forceinline__ void residue_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
                                               int64_t mn_pad, int64_t k_pad, int nmod, int beta,
                                               const unsigned long long* __restrict__ amax, int32_t* __restrict__ exps,
                                               int8_t* __restrict__ planes, const ModTable& mt, int64_t bx,
                                               int64_t by) {
+    constexpr int E = RES_ELEMS;
     const int64_t mn = bx * blockDim.x + threadIdx.x;
-    const int64_t k0 = by * 32;
+    const int64_t k0 = by * E;
     if (mn >= mn_pad) return;
     int e = 0;
     if (mn < MN) {
@@ -140,9 +136,9 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         if (by == 0) exps[mn] = e;
     }
     const bool live = (mn < MN) && (e != oz::EXP_NONFINITE);
-    uint32_t x0[32], x1[32], x2[32];  // 20-bit chunks of x + 2^58
+    uint32_t x0[E], x1[E], x2[E];  // 20-bit chunks of x + 2^58
 #pragma unroll
-    for (int i = 0; i < 32; ++i) {
+    for (int i = 0; i < E; ++i) {
         const int64_t kk = k0 + i;
         double a = 0.0;
         if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
@@ -156,23 +152,23 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
     const int64_t plane = mn_pad * k_pad;
     for (int j = 0; j < nmod; ++j) {
         const uint32_t p = (uint32_t)mt.p[j], c20 = mt.c20[j], c40 = mt.c40[j], off = mt.off[j], mg = mt.magic[j];
-        const uint32_t half = (p - 1) >> 1;
-        uint32_t w[8];
+        const uint32_t h4 = mt.h4[j];
+        uint32_t w[E / 4];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < E / 4; ++q) {
             uint32_t b[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int i = 4 * q + u;
-                const uint32_t t = x2[i] * c40 + x1[i] * c20 + x0[i] + off;  // < 2^29, = x mod p
-                const uint32_t r = t - (__umulhi(t, mg) >> 5) * p;           // in [0, p)
-                b[u] = r > half ? r - p : r;                                  // symmetric, low byte
+                const uint32_t t = x2[i] * c40 + x1[i] * c20 + (x0[i] + off);  // < 2^29, = x + p/2 mod p
+                b[u] = t - (__umulhi(t, mg) >> 5) * p;                          // in [0, p)
             }
-            w[q] = __byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410);
+            // four residues, then minus floor(p/2) per byte: the symmetric residues as int8
+            w[q] = __vsub4(__byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410), h4);
         }
         uint4* o4 = reinterpret_cast<uint4*>(planes + j * plane + mn * k_pad + k0);
-        o4[0] = make_uint4(w[0], w[1], w[2], w[3]);
-        o4[1] = make_uint4(w[4], w[5], w[6], w[7]);
+#pragma unroll
+        for (int q = 0; q < E / 16; ++q) o4[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
     }
 }
 
@@ -246,24 +242,11 @@ __device__ __forceinline__ void limbs_addsub(uint32_t (&x)[N], const uint32_t (&
     }
 }
 
-// a > b over N limbs (most significant last)
-template <int N>
-__device__ __forceinline__ bool limbs_gt(const uint32_t (&a)[N], const uint32_t (&b)[N]) {
-    bool gt = false, decided = false;
-#pragma unroll
-    for (int l = N - 1; l >= 0; --l) {
-        if (!decided && a[l] != b[l]) {
-            gt = a[l] > b[l];
-            decided = true;
-        }
-    }
-    return gt;
-}
-
 // X = sum_j r_j W_j (NW-limb W, NX = NW + 1 limbs for X < 2^13 P) reduced mod P into the
 // symmetric range, rounded to FP64 once (round to nearest even), times 2^shift.  r_j is byte
-// `sel` of rr[j].  Constant trip counts keep every limb in registers.
-template <int NW>
+// `sel` of rr[j]; NM is the modulus count when known at compile time (0: cc.n).  Constant trip
+// counts keep every limb in registers.
+template <int NW, int NM>
 __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
                                             int shift) {
     constexpr int NX = NW + 1;
@@ -272,7 +255,7 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
     for (int l = 0; l < NW; ++l) acc[l] = 0;
 #pragma unroll
     for (int j = 0; j < MAX_MODULI; ++j) {
-        if (j < cc.n) {
+        if (NM ? j < NM : j < cc.n) {
             const uint32_t r = (rr[j] >> (8 * sel)) & 0xffu;
 #pragma unroll
             for (int l = 0; l < NW; ++l) acc[l] += (uint64_t)r * cc.W[j][l];  // < 20 * 2^40
@@ -287,11 +270,14 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
         c = t >> 32;
     }
     x[NW] = (uint32_t)c;
-    // q = floor(X / P) to within one (X < 2^13 P); X -= q P
+    // X = q P + C' with |C'| <= k (2^beta - 1)^2 < (P / 2)(1 - 1.3e-9) by the operand-bit rule
+    // (beta_for keeps a 1e-9 margin on its logarithms), so q is the integer nearest X / P, and
+    // the estimate from the top three limbs is within 2^-37 of X / P (X < 2^13 P; the dropped
+    // limbs are below 2^-37 P): rint gives q exactly, and X - q P is C' itself.
     double xq = 0.0;
 #pragma unroll
-    for (int l = 0; l < NX; ++l) xq = fma((double)x[l], cc.kq[l], xq);
-    const uint32_t q = (uint32_t)xq;
+    for (int l = (NX > 3 ? NX - 3 : 0); l < NX; ++l) xq = fma((double)x[l], cc.kq[l], xq);
+    const uint32_t q = (uint32_t)rint(xq);
     uint32_t qp[NX];
     c = 0;
 #pragma unroll
@@ -300,26 +286,15 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
         qp[l] = (uint32_t)t;
         c = t >> 32;
     }
-    limbs_addsub<NX, false>(x, qp);  // X in [-P, 2P), two's complement
-    uint32_t Pl[NX], Ph[NX];
+    limbs_addsub<NX, false>(x, qp);  // C', two's complement, |C'| < P / 2
+    const bool neg = (int32_t)x[NX - 1] < 0;
+    if (neg) {  // magnitude -C'
+        uint32_t z[NX];
 #pragma unroll
-    for (int l = 0; l < NX; ++l) {
-        Pl[l] = cc.P[l];
-        Ph[l] = cc.Phalf[l];
-    }
-    if ((int32_t)x[NX - 1] < 0)
-        limbs_addsub<NX, true>(x, Pl);
-    else if (!limbs_gt<NX>(Pl, x))  // X >= P
-        limbs_addsub<NX, false>(x, Pl);
-    // symmetric range: X > floor((P-1)/2) stands for X - P; work with the magnitude P - X
-    const bool neg = limbs_gt<NX>(x, Ph);
-    if (neg) {
-        uint32_t m[NX];
+        for (int l = 0; l < NX; ++l) z[l] = 0u;
+        limbs_addsub<NX, false>(z, x);
 #pragma unroll
-        for (int l = 0; l < NX; ++l) m[l] = Pl[l];
-        limbs_addsub<NX, false>(m, x);
-#pragma unroll
-        for (int l = 0; l < NX; ++l) x[l] = m[l];
+        for (int l = 0; l < NX; ++l) x[l] = z[l];
     }
     int L = 0;
 #pragma unroll
@@ -348,7 +323,7 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
 
 // Rows row0 .. row0+3 of column col of one product: residue planes [j][col][row] with leading
 // dimension res_ld (a multiple of 4).
-template <int NW>
+template <int NW, int NM>
 __device__ __forceinline__ void crt_quad(const uint8_t* __restrict__ res, int64_t res_ld, int64_t res_plane,
                                          int64_t m, int64_t row0, int64_t col, const int32_t* __restrict__ row_exp,
                                          const int32_t* __restrict__ col_exp, int beta, double alpha, double beta_c,
@@ -367,14 +342,14 @@ __device__ __forceinline__ void crt_quad(const uint8_t* __restrict__ res, int64_
         if (e == oz::EXP_NONFINITE || f == oz::EXP_NONFINITE)
             val = __longlong_as_double(0x7ff8000000000000ll);
         else
-            val = crt_value<NW>(rr, e4, cc, e + f - 2 * beta);
+            val = crt_value<NW, NM>(rr, e4, cc, e + f - 2 * beta);
         double* cp = C + row + col * ldc;
         *cp = beta_c != 0.0 ? fma(alpha, val, beta_c * *cp) : alpha * val;
     }
 }
 
 // Thread per 4 consecutive rows of one column of C.
-template <int NW>
+template <int NW, int NM>
 __global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
                                                        int64_t res_plane, int64_t m, int64_t n,
                                                        const int32_t* __restrict__ row_exp,
@@ -384,12 +359,12 @@ __global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict
     const int64_t quads = (m + 3) / 4;
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= quads * n) return;
-    crt_quad<NW>(res, res_ld, res_plane, m, (idx % quads) * 4, idx / quads, row_exp, col_exp, beta, alpha, beta_c, C,
+    crt_quad<NW, NM>(res, res_ld, res_plane, m, (idx % quads) * 4, idx / quads, row_exp, col_exp, beta, alpha, beta_c, C,
                  ldc, cc);
 }
 
 // Every product of a grouped call: thread -> product by binary search on thread_begin.
-template <int NW>
+template <int NW, int NM>
 __global__ void __launch_bounds__(256) crt_grouped(const CrtJob* __restrict__ jobs, int njobs, int64_t threads,
                                                    const __grid_constant__ CrtConst cc) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -405,7 +380,7 @@ __global__ void __launch_bounds__(256) crt_grouped(const CrtJob* __restrict__ jo
     const CrtJob& J = jobs[lo];
     const int64_t local = idx - J.thread_begin, quads = (J.m + 3) / 4;
     if (local >= quads * J.n) return;
-    crt_quad<NW>(J.res, J.res_ld, J.res_plane, J.m, (local % quads) * 4, local / quads, J.row_exp, J.col_exp, J.bits,
+    crt_quad<NW, NM>(J.res, J.res_ld, J.res_plane, J.m, (local % quads) * 4, local / quads, J.row_exp, J.col_exp, J.bits,
                  J.alpha, J.beta, J.C, J.ldc, cc);
 }
 
@@ -418,12 +393,17 @@ cudaError_t launch_split_residues_grouped(cudaStream_t s, const oz::SplitJob* jo
 cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, int64_t threads, const CrtConst& cc,
                                int nmod) {
     const unsigned blocks = (unsigned)((threads + 255) / 256);
-    switch (limbs_for(nmod)) {
-        case 2: crt_grouped<2><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
-        case 3: crt_grouped<3><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
-        case 4: crt_grouped<4><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
-        default: crt_grouped<5><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
-    }
+    if (nmod == 16)
+        crt_grouped<4, 16><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
+    else if (nmod == 17)
+        crt_grouped<5, 17><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
+    else
+        switch (limbs_for(nmod)) {
+            case 2: crt_grouped<2, 0><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
+            case 3: crt_grouped<3, 0><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
+            case 4: crt_grouped<4, 0><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
+            default: crt_grouped<5, 0><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
+        }
     return cudaGetLastError();
 }
 
@@ -507,7 +487,7 @@ dgt_status ozaki2_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, 
     if ((st = ozaki_amax(h, s, B, ldb, n, k, !tb, amaxB)) != DGT_SUCCESS) return st;
     auto split = [&](const double* X, int64_t ld, int64_t MN, int64_t mn_pad, bool kcontig,
                      const unsigned long long* am, int32_t* ex, int8_t* planes) -> dgt_status {
-        dim3 grid((unsigned)ceil_div(mn_pad, 128), (unsigned)(k_pad / 32));
+        dim3 grid((unsigned)ceil_div(mn_pad, 128), (unsigned)(k_pad / RES_ELEMS));
         if (kcontig)
             split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, k, mn_pad, k_pad, nmod, bits, am, ex, planes, mt);
         else
@@ -554,24 +534,21 @@ dgt_status ozaki2_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, 
     mark(h, 2);
     const int64_t threads = ceil_div(m, 4) * n;
     const unsigned blocks = (unsigned)ceil_div(threads, 256);
-    switch (limbs_for(nmod)) {
-        case 2:
-            crt_reconstruct<2><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta,
-                                                      C, ldc, cc);
-            break;
-        case 3:
-            crt_reconstruct<3><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta,
-                                                      C, ldc, cc);
-            break;
-        case 4:
-            crt_reconstruct<4><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta,
-                                                      C, ldc, cc);
-            break;
-        default:
-            crt_reconstruct<5><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta,
-                                                      C, ldc, cc);
-            break;
-    }
+#define DGT_CRT_LAUNCH(NW, NM)                                                                            \
+    crt_reconstruct<NW, NM><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta, \
+                                                   C, ldc, cc)
+    if (nmod == 16)
+        DGT_CRT_LAUNCH(4, 16);
+    else if (nmod == 17)
+        DGT_CRT_LAUNCH(5, 17);
+    else
+        switch (limbs_for(nmod)) {
+            case 2: DGT_CRT_LAUNCH(2, 0); break;
+            case 3: DGT_CRT_LAUNCH(3, 0); break;
+            case 4: DGT_CRT_LAUNCH(4, 0); break;
+            default: DGT_CRT_LAUNCH(5, 0); break;
+        }
+#undef DGT_CRT_LAUNCH
     h->launches.fetch_add(1);
     DGT_CUDA_TRY(h, cudaGetLastError());
     return DGT_SUCCESS;
