@@ -332,6 +332,18 @@ def workload_summa(args):
         tot_ms = sum(v["ms"] for v in layout.values())
         summa_ms = _time_ms(torch, summa, 10)
         flops = 2.0 * M * N * K
+        # the same SUMMA with every step emulated (CRT, 16 moduli; one grouped pass per panel
+        # step over the p x q virtual ranks), error on the same sampled rows
+        summa_crt = lambda: h.summa(p, q, b, b, b, M, N, K, alpha, lA, lldA, lB, lldB, beta, lC, lldC,
+                                    mode=dgt.FP64_OZAKI2_INT8, slices=16)
+        dC.copy_(_dev(torch, C))  # the original C (the native run's unpack overwrote dC)
+        packs["pack C"][0]()
+        summa_crt()
+        h.unpack_block_cyclic(M, N, b, b, p, q, dC.data_ptr(), M, lC, lldC)
+        torch.cuda.synchronize()
+        h.check_device()
+        err_crt = _rel(_rows_of(dC, rows, (M, N)), alpha * (A[rows, :] @ B) + beta * C[rows, :])
+        crt_ms = _time_ms(torch, summa_crt, 3, warm=1)
         dC2 = torch.zeros_like(dC)
         glob_ms = _time_ms(torch, lambda: h.dgemm("N", "N", M, N, K, alpha, dA.data_ptr(), M, dB.data_ptr(), K, 0.0,
                                                    dC2.data_ptr(), M), 5)
@@ -339,6 +351,8 @@ def workload_summa(args):
                     "frac_of_dmma_peak": flops / (summa_ms * 1e-3) / 1e12 / dmma_peak,
                     "one_global_dgemm_tflops": flops / (glob_ms * 1e-3) / 1e12,
                     "max_rel": err[0], "fro_rel": err[1], "sampled_rows": len(rows),
+                    "summa_crt16": {"tflops": flops / (crt_ms * 1e-3) / 1e12, "ms": crt_ms, "max_rel": err_crt[0],
+                                    "fro_rel": err_crt[1]},
                     "layout": layout, "layout_total": {"bytes": tot_bytes, "ms": tot_ms,
                                                        "GB/s": tot_bytes / (tot_ms * 1e-3) / 1e9,
                                                        "frac_of_hbm": tot_bytes / (tot_ms * 1e-3) / 1e9 / hbm}})
