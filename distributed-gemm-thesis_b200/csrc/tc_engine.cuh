@@ -592,15 +592,17 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                     if constexpr (EPI_MODE == 1) {
                         float* fbase = P.Cf + row + (n0 + ch * 32) * P.ldc;
                         float prevf[32];
+                        // read C only when it contributes (a later group, or beta != 0), behind one
+                        // warp-uniform branch: with per-element conditions the compiler may issue
+                        // the loads anyway (every address is stored to below), and a beta = 0 call
+                        // then waits on reads of C it never uses
+                        if (g > 0 || P.beta_f != 0.f) {
+                            const float ps = g > 0 ? 1.f : P.beta_f;
 #pragma unroll
-                        for (int c = 0; c < 32; ++c) {
-                            prevf[c] = 0.f;
-                            if (c < ncols) {
-                                if (g > 0)
-                                    prevf[c] = fbase[c * P.ldc];
-                                else if (P.beta_f != 0.f)
-                                    prevf[c] = P.beta_f * fbase[c * P.ldc];
-                            }
+                            for (int c = 0; c < 32; ++c) prevf[c] = c < ncols ? ps * fbase[c * P.ldc] : 0.f;
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 32; ++c) prevf[c] = 0.f;
                         }
 #pragma unroll
                         for (int c = 0; c < 32; ++c)
@@ -615,15 +617,15 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
 #define alpha DGT_TILE_FIELD(cx, alpha, alpha)
 #define beta DGT_TILE_FIELD(cx, beta, beta)
                     double* cbase = DGT_TILE_FIELD(cx, C, C) + row + (n0 + ch * 32) * ldc;
+                    // C is read only when it contributes (see the FP32 epilogue above); 1.0 * x is
+                    // exact, so a later group folds onto C unchanged
+                    if (g > 0 || beta != 0.0) {
+                        const double ps = g > 0 ? 1.0 : beta;
 #pragma unroll
-                    for (int c = 0; c < 32; ++c) {
-                        prev[c] = 0.0;
-                        if (c < ncols) {
-                            if (g > 0)
-                                prev[c] = cbase[c * ldc];
-                            else if (beta != 0.0)
-                                prev[c] = beta * cbase[c * ldc];
-                        }
+                        for (int c = 0; c < 32; ++c) prev[c] = c < ncols ? ps * cbase[c * ldc] : 0.0;
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) prev[c] = 0.0;
                     }
 #pragma unroll
                     for (int c = 0; c < 32; ++c) {
