@@ -572,19 +572,22 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                     const int64_t rem_cols = DGT_TILE_FIELD(cx, n, n) - (n0 + ch * 32);
                     const int ncols = rem_cols < 32 ? (int)rem_cols : 32;
                     if constexpr (EPI_MODE == 2) {
-                        // exact: |acc| < 2^31, so (double)acc / p floors to q or q - 1 at worst
-                        const int pm = GROUPS[g].pad;
-                        const double inv = 1.0 / (double)pm;
+                        // acc mod p in integers.  |acc| <= k_pad 2^14 <= 2^31 - 2^21 (k_pad < 2^17),
+                        // so x = acc + off (off = p floor(2^31 / p) >= 2^31 - 256, a multiple of p)
+                        // lies in (0, 2^32); t = (x >> 16)(2^16 mod p) + (x & 0xffff) < 2^24 is
+                        // congruent to acc, and t / p = umulhi(t, floor(2^32 / p) + 1) exactly for
+                        // t < 2^24 (Granlund & Montgomery 1994, thm 4.2)
+                        const uint32_t pm = (uint32_t)GROUPS[g].pad;
+                        const uint32_t off = pm * (0x80000000u / pm), c16 = (1u << 16) % pm;
+                        const uint32_t mg = (uint32_t)(0x100000000ull / pm) + 1u;
                         uint8_t* rbase = DGT_TILE_FIELD(cx, res, res) + (int64_t)g * DGT_TILE_FIELD(cx, res_plane, res_plane) +
                                          row + (n0 + ch * 32) * DGT_TILE_FIELD(cx, res_ld, res_ld);
 #pragma unroll
                         for (int c = 0; c < 32; ++c) {
                             if (c < ncols) {
-                                const int32_t x = (int32_t)v[c];
-                                int r = x - pm * (int)floor((double)x * inv);
-                                if (r < 0) r += pm;
-                                if (r >= pm) r -= pm;
-                                rbase[c * DGT_TILE_FIELD(cx, res_ld, res_ld)] = (uint8_t)r;
+                                const uint32_t x = v[c] + off;
+                                const uint32_t t = (x >> 16) * c16 + (x & 0xffffu);
+                                rbase[c * DGT_TILE_FIELD(cx, res_ld, res_ld)] = (uint8_t)(t - pm * __umulhi(t, mg));
                             }
                         }
                         continue;
