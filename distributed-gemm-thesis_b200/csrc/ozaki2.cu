@@ -442,9 +442,33 @@ static cudaError_t launch_residue_gemm(const CUtensorMap& tmA, const CUtensorMap
     }
 }
 
+static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+                                     double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                     double beta, double* C, int64_t ldc, int nmod);
+
+// K up to KMAX runs as one CRT product; longer K runs as consecutive K-chunks of KMAX, each a
+// full CRT product rounded once (beta on the first, accumulation after): one residue product
+// must stay exact in INT32, k_pad * 128^2 < 2^31.
 dgt_status ozaki2_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
                         const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,
                         int64_t ldc, int nmod) {
+    constexpr int64_t KMAX = 65536;
+    if (k <= KMAX) return ozaki2_dgemm_chunk(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nmod);
+    for (int64_t k0 = 0; k0 < k; k0 += KMAX) {
+        const int64_t kc = std::min(KMAX, k - k0);
+        // op(A) columns k0.. : 'N' -> A + k0 lda, 'T' -> A + k0; op(B) rows k0.. : 'N' -> B + k0, 'T' -> B + k0 ldb
+        const double* Ac = ta ? A + k0 : A + k0 * lda;
+        const double* Bc = tb ? B + k0 * ldb : B + k0;
+        dgt_status st = ozaki2_dgemm_chunk(h, ta, tb, m, n, kc, alpha, Ac, lda, Bc, ldb, k0 == 0 ? beta : 1.0, C,
+                                           ldc, nmod);
+        if (st != DGT_SUCCESS) return st;
+    }
+    return DGT_SUCCESS;
+}
+
+static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+                                     double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                     double beta, double* C, int64_t ldc, int nmod) {
     using namespace oz2;
     if (nmod < MIN_MODULI || nmod > MAX_MODULI)
         return fail(h, DGT_ERROR_INVALID_VALUE, "modulus count must be in [8, 20]");

@@ -112,10 +112,19 @@ def test_rejections(h):
     x = torch.zeros(4, dtype=torch.float64, device="cuda")
     with pytest.raises(dgt.DgtError):  # modulus count outside [8, 20]
         h.dgemm("N", "N", 2, 2, 2, 1.0, ptr(x), 2, ptr(x), 2, 0.0, ptr(x), 2, mode=dgt.FP64_OZAKI2_INT8, slices=7)
-    big = torch.zeros(131072, dtype=torch.float64, device="cuda")
-    with pytest.raises(dgt.DgtError):  # K beyond exact INT32 residue products
-        h.dgemm("N", "N", 1, 1, 131072, 1.0, ptr(big), 1, ptr(big), 131072, 0.0, ptr(x), 1,
-                mode=dgt.FP64_OZAKI2_INT8, slices=17)
+
+
+def test_long_k_runs_in_chunks(h):
+    """K = 150000 (beyond one exact INT32 residue product) runs as K-chunks of 65536."""
+    import torch
+
+    m, n, k = 3, 5, 150000
+    A, B, C = O.uniform((m, k), 61), O.uniform((k, n), 62), O.uniform((m, n), 63)
+    got = run(h, "N", "N", m, n, k, 1.5, -0.5, 17, A, B, C)
+    assert O.rel_errors(got, O.dgemm(A, B, 1.5, -0.5, C))[1] <= FRO_TOL
+    At, Bt = np.asfortranarray(A.T), np.asfortranarray(B.T)
+    got_t = run(h, "T", "T", m, n, k, 1.5, -0.5, 17, At, Bt, C)
+    assert O.rel_errors(got_t, O.dgemm(A, B, 1.5, -0.5, C))[1] <= FRO_TOL
 
 
 def test_grouped_and_cannon_through_crt(h):
