@@ -52,20 +52,28 @@ constexpr int MAX_MODULI = 20, MIN_MODULI = 8;
 constexpr int MAX_NW = 5;     // 32-bit limbs of W_p and P (P < 2^160)
 constexpr int MAX_BETA = 58;  // |A'| < 2^58
 
-// Residues of x = trunc(a 2^(beta-e)) (|x| < 2^58) modulo p, in integers: xu = x + 2^58 is
-// split into 20-bit chunks x0, x1, x2 and t = x2 c40 + x1 c20 + x0 + off (< 2^29) is congruent
-// to x + floor(p/2); t / p = (t magic) >> 37 exactly for t < 2^29 (Granlund & Montgomery 1994, thm 4.2:
-// magic = floor(2^37 / p) + 1 for 2^7 < p <= 2^8).
-// The symmetric residue is (t + floor(p/2)) mod p - floor(p/2): off carries the + floor(p/2)
-// and h4 (floor(p/2) in every byte) takes it back off four packed residues at once.
+// Residues of x = trunc(a 2^(beta-e)) (|x| <= 2^58) modulo p, in integers: x is cut into
+// 20-bit chunks x0, x1 (unsigned) and x2 = x >> 40 (arithmetic, |x2| <= 2^18), so
+// t = x2 c40 + x1 c20 + x0 (c20 = 2^20 mod p, c40 = 2^40 mod p) is congruent to x with
+// -2^26 < t < 2^29.  n = t + floor(p/2) + 2^18 p then lies in [0, 2^30), and with
+// magic = floor(2^38 / p) + 1 = 2^38 / p + e (0 < e <= 1), floor(n magic / 2^38) = floor(n / p)
+// because n e / 2^38 < 2^30 / 2^38 <= 1 / p (p <= 256).  One 32 x 32 -> 64-bit multiply-add
+// gives n magic = t magic + bias.  r = t - floor(n / p) p is the symmetric residue
+// ((x + floor(p/2)) mod p) - floor(p/2) minus 2^18 p, a multiple of 256, so the low byte of r
+// is the symmetric residue as int8.
 struct ModTable {
     int32_t p[MAX_MODULI];
-    uint32_t c20[MAX_MODULI], c40[MAX_MODULI];  // 2^20 mod p, 2^40 mod p
-    uint32_t off[MAX_MODULI];                    // p - (2^58 mod p) + floor(p/2)
-    uint32_t magic[MAX_MODULI];
-    uint32_t h4[MAX_MODULI];                     // floor(p/2) * 0x01010101
+    int32_t c20[MAX_MODULI], c40[MAX_MODULI];  // 2^20 mod p, 2^40 mod p
+    int32_t magic[MAX_MODULI];                 // floor(2^38 / p) + 1 (< 2^31 for p > 128)
+    long long bias[MAX_MODULI];                // (floor(p/2) + 2^18 p) magic
 };
-constexpr int RES_ELEMS = 32;  // K elements one thread of the residue split turns into bytes (16: 2x slower)
+// Residue split geometry: a block of 128 threads covers RES_ROWS rows (mn) and RES_KSPAN
+// consecutive kk, one 32-byte sector of every plane row; RES_TPR threads share a row, each
+// turning RES_ELEMS consecutive kk into bytes.
+constexpr int RES_KSPAN = 32;
+constexpr int RES_TPR = 2;
+constexpr int RES_ELEMS = RES_KSPAN / RES_TPR;
+constexpr int RES_ROWS = 128 / RES_TPR;
 
 struct CrtConst {
     int32_t n;

@@ -625,12 +625,12 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
             J.kcontig = kc[t] ? 1 : 0;
             J.amax_bx = (int32_t)(kc[t] ? ceil_div(MN[t], 8) : ceil_div(MN[t], 256));
             J.amax_by = (int32_t)(kc[t] ? 1 : ceil_div(p.k, oz::AMAX_KCHUNK));
-            J.split_bx = (int32_t)ceil_div(pad[t], 128);
+            J.split_bx = (int32_t)ceil_div(pad[t], crt ? oz2::RES_ROWS : 128);
             J.amax_begin = amax_blocks;
             J.split_begin = split_blocks;
             J.bits = o.bits;
             amax_blocks += (int64_t)J.amax_bx * J.amax_by;
-            split_blocks += (int64_t)J.split_bx * (o.k_pad / (crt ? oz2::RES_ELEMS : 32));
+            split_blocks += (int64_t)J.split_bx * (o.k_pad / (crt ? oz2::RES_KSPAN : 32));
         }
     }
     if (amax_blocks > INT32_MAX || split_blocks > INT32_MAX || crt_threads / 256 > INT32_MAX)

@@ -37,6 +37,12 @@ namespace oz2 {
 // Pairwise coprime, largest first (greedy from 256 down).
 constexpr int kModuli[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                                      223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+constexpr bool moduli_in_split_range() {  // the residue split's magic divide needs 128 < p <= 256
+    for (int p : kModuli)
+        if (p <= 128 || p > 256) return false;
+    return true;
+}
+static_assert(moduli_in_split_range(), "CRT moduli must lie in (128, 256]");
 
 // ---- host: CRT constants in 32-bit limbs ------------------------------------------------------
 using Big = std::vector<uint32_t>;  // little-endian limbs
@@ -98,11 +104,10 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
     for (int i = 0; i < n; ++i) {
         const uint32_t p = (uint32_t)kModuli[i];
         mt.p[i] = (int32_t)p;
-        mt.c20[i] = (uint32_t)((1ull << 20) % p);
-        mt.c40[i] = (uint32_t)((1ull << 40) % p);
-        mt.off[i] = p - (uint32_t)((1ull << 58) % p) + (p >> 1);
-        mt.h4[i] = (p >> 1) * 0x01010101u;
-        mt.magic[i] = (uint32_t)((1ull << 37) / p + 1);
+        mt.c20[i] = (int32_t)((1ull << 20) % p);
+        mt.c40[i] = (int32_t)((1ull << 40) % p);
+        mt.magic[i] = (int32_t)((1ull << 38) / p + 1);
+        mt.bias[i] = ((long long)(p >> 1) + ((long long)p << 18)) * mt.magic[i];
         Big M = P;
         big_div_small(M, p);  // M = P / p
         Big Mm = M;
@@ -118,8 +123,10 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
 
 // ---- device: residue planes ----------------------------------------------------------------------
 // Plane j holds (A' mod p_j) in the symmetric range as int8 at [j][mn][kk] (K-major, row
-// length k_pad, mn_pad rows, zero padded).  Each thread produces RES_ELEMS consecutive kk of
-// one mn; the by == 0 blocks also write exps[mn].
+// length k_pad, mn_pad rows, zero padded).  A thread produces RES_ELEMS consecutive kk of one
+// mn; the RES_TPR adjacent lanes of a row write one whole 32-byte sector per plane together
+// (lanes that wrote parts of a sector each made L2 fetch the sector from DRAM first).  The
+// seg == 0, by == 0 threads also write exps[mn].
 template <bool K_CONTIG>
 __device__ __forceinline__ void residue_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
                                               int64_t mn_pad, int64_t k_pad, int nmod, int beta,
@@ -127,48 +134,54 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
                                               int8_t* __restrict__ planes, const ModTable& mt, int64_t bx,
                                               int64_t by) {
     constexpr int E = RES_ELEMS;
-    const int64_t mn = bx * blockDim.x + threadIdx.x;
-    const int64_t k0 = by * E;
+    static_assert(E == 8 || E % 16 == 0, "residue split: RES_ELEMS must be 8 or a multiple of 16");
+    const int row = threadIdx.x / RES_TPR, seg = threadIdx.x % RES_TPR;
+    const int64_t mn = bx * RES_ROWS + row;
+    const int64_t k0 = by * RES_KSPAN + seg * E;
     if (mn >= mn_pad) return;
     int e = 0;
     if (mn < MN) {
         e = oz::exponent_of_max(amax[mn]);
-        if (by == 0) exps[mn] = e;
+        if (by == 0 && seg == 0) exps[mn] = e;
     }
     const bool live = (mn < MN) && (e != oz::EXP_NONFINITE);
-    uint32_t x0[E], x1[E], x2[E];  // 20-bit chunks of x + 2^58
+    int32_t x0[E], x1[E], x2[E];  // x = x2 2^40 + x1 2^20 + x0, x0 and x1 in [0, 2^20)
 #pragma unroll
     for (int i = 0; i < E; ++i) {
         const int64_t kk = k0 + i;
         double a = 0.0;
         if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
-        // an integer below 2^beta <= 2^58 in magnitude (exact scaling, truncation toward 0)
+        // an integer of magnitude <= 2^beta <= 2^58 (exact scaling, truncation toward 0)
         const long long x = live ? __double2ll_rz(oz::scale2(a, beta - e)) : 0ll;
-        const unsigned long long xu = (unsigned long long)(x + (1ll << 58));
-        x0[i] = (uint32_t)(xu & 0xfffffu);
-        x1[i] = (uint32_t)((xu >> 20) & 0xfffffu);
-        x2[i] = (uint32_t)(xu >> 40);
+        x0[i] = (int32_t)(x & 0xfffff);
+        x1[i] = (int32_t)((x >> 20) & 0xfffff);
+        x2[i] = (int32_t)(x >> 40);
     }
+    int8_t* out = planes + mn * k_pad + k0;
     const int64_t plane = mn_pad * k_pad;
-    for (int j = 0; j < nmod; ++j) {
-        const uint32_t p = (uint32_t)mt.p[j], c20 = mt.c20[j], c40 = mt.c40[j], off = mt.off[j], mg = mt.magic[j];
-        const uint32_t h4 = mt.h4[j];
+    for (int j = 0; j < nmod; ++j, out += plane) {
+        const int32_t p = mt.p[j], c20 = mt.c20[j], c40 = mt.c40[j], mg = mt.magic[j];
+        const long long bias = mt.bias[j];
         uint32_t w[E / 4];
 #pragma unroll
         for (int q = 0; q < E / 4; ++q) {
-            uint32_t b[4];
+            int32_t r[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int i = 4 * q + u;
-                const uint32_t t = x2[i] * c40 + x1[i] * c20 + (x0[i] + off);  // < 2^29, = x + p/2 mod p
-                b[u] = t - (__umulhi(t, mg) >> 5) * p;                          // in [0, p)
+                const int32_t t = x2[i] * c40 + x1[i] * c20 + x0[i];               // = x mod p, in (-2^26, 2^29)
+                const int32_t qt = (int32_t)((unsigned long long)((long long)t * mg + bias) >> 38);
+                r[u] = t - qt * p;  // low byte: the symmetric residue
             }
-            // four residues, then minus floor(p/2) per byte: the symmetric residues as int8
-            w[q] = __vsub4(__byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410), h4);
+            w[q] = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
         }
-        uint4* o4 = reinterpret_cast<uint4*>(planes + j * plane + mn * k_pad + k0);
+        if constexpr (E % 16 == 0) {
 #pragma unroll
-        for (int q = 0; q < E / 16; ++q) o4[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+            for (int q = 0; q < E / 16; ++q)
+                reinterpret_cast<uint4*>(out)[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+        } else {
+            *reinterpret_cast<uint2*>(out) = make_uint2(w[0], w[1]);
+        }
     }
 }
 
@@ -511,7 +524,7 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     if ((st = ozaki_amax(h, s, B, ldb, n, k, !tb, amaxB)) != DGT_SUCCESS) return st;
     auto split = [&](const double* X, int64_t ld, int64_t MN, int64_t mn_pad, bool kcontig,
                      const unsigned long long* am, int32_t* ex, int8_t* planes) -> dgt_status {
-        dim3 grid((unsigned)ceil_div(mn_pad, 128), (unsigned)(k_pad / RES_ELEMS));
+        dim3 grid((unsigned)ceil_div(mn_pad, RES_ROWS), (unsigned)(k_pad / RES_KSPAN));
         if (kcontig)
             split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, k, mn_pad, k_pad, nmod, bits, am, ex, planes, mt);
         else
