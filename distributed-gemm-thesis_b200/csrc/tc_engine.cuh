@@ -568,9 +568,6 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                 for (int ch = ch0; ch < ch0 + CHUNKS; ++ch) {
                     uint32_t v[32];
                     tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TN + ch * 32), v);
-                    if (!row_ok) continue;
-                    const int64_t rem_cols = DGT_TILE_FIELD(cx, n, n) - (n0 + ch * 32);
-                    const int ncols = rem_cols < 32 ? (int)rem_cols : 32;
                     if constexpr (EPI_MODE == 2) {
                         // acc mod p in integers.  |acc| <= k_pad 2^14 <= 2^31 - 2^21 (k_pad < 2^17),
                         // so x = acc + off (off = p floor(2^31 / p) >= 2^31 - 256, a multiple of p)
@@ -580,18 +577,38 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                         const uint32_t pm = (uint32_t)GROUPS[g].pad;
                         const uint32_t off = pm * (0x80000000u / pm), c16 = (1u << 16) % pm;
                         const uint32_t mg = (uint32_t)(0x100000000ull / pm) + 1u;
+                        // Each lane holds one row; the plane is column-major with rows
+                        // contiguous.  Four columns' bytes of this lane's row form one word; a
+                        // 4 x 4 byte transpose across the quad of lanes 4a .. 4a+3 (two shuffle
+                        // steps) leaves lane 4a+b with column 4i+b's bytes of rows 4a .. 4a+3,
+                        // so a warp stores four columns x 32 rows with one word per lane.
+                        // Every lane of the warp stores, rows past m and columns past n
+                        // included: the plane has m_pad rows and n_pad columns.
+                        const int bq = lane & 3;
+                        const uint32_t selA = (bq & 2) ? 0x3276u : 0x5410u;  // swap 16-bit halves with lane ^ 2
+                        const uint32_t selB = (bq & 1) ? 0x3715u : 0x6240u;  // swap bytes with lane ^ 1
+                        const int64_t rld = DGT_TILE_FIELD(cx, res_ld, res_ld);
                         uint8_t* rbase = DGT_TILE_FIELD(cx, res, res) + (int64_t)g * DGT_TILE_FIELD(cx, res_plane, res_plane) +
-                                         row + (n0 + ch * 32) * DGT_TILE_FIELD(cx, res_ld, res_ld);
+                                         (row - lane + 4 * (lane >> 2)) + (n0 + ch * 32 + bq) * rld;
 #pragma unroll
-                        for (int c = 0; c < 32; ++c) {
-                            if (c < ncols) {
-                                const uint32_t x = v[c] + off;
+                        for (int i = 0; i < 8; ++i) {
+                            uint32_t r[4];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                const uint32_t x = v[4 * i + u] + off;
                                 const uint32_t t = (x >> 16) * c16 + (x & 0xffffu);
-                                rbase[c * DGT_TILE_FIELD(cx, res_ld, res_ld)] = (uint8_t)(t - pm * __umulhi(t, mg));
+                                r[u] = t - pm * __umulhi(t, mg);
                             }
+                            uint32_t wd = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+                            wd = __byte_perm(wd, __shfl_xor_sync(0xffffffffu, wd, 2), selA);
+                            wd = __byte_perm(wd, __shfl_xor_sync(0xffffffffu, wd, 1), selB);
+                            *reinterpret_cast<uint32_t*>(rbase + (int64_t)(4 * i) * rld) = wd;
                         }
                         continue;
                     }
+                    if (!row_ok) continue;
+                    const int64_t rem_cols = DGT_TILE_FIELD(cx, n, n) - (n0 + ch * 32);
+                    const int ncols = rem_cols < 32 ? (int)rem_cols : 32;
                     if constexpr (EPI_MODE == 1) {
                         float* fbase = P.Cf + row + (n0 + ch * 32) * P.ldc;
                         float prevf[32];
