@@ -276,6 +276,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
+// 64 consecutive 32-bit columns of this warp's 32 TMEM lanes, load and wait in one asm (the
+// registers are written asynchronously until the wait, so nothing may touch them in between).
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&v)[64]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+        : "r"(taddr)
+        : "memory");
+}
+
 // 2^e for e in [-1022, 1023], built from the exponent field.
 __device__ __forceinline__ double pow2i(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
 
@@ -539,6 +550,17 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
         int32_t* col_exp_s = col_exp_all + (warp - 2) * TN;
         uint32_t gcount = 0;
         bool ok = true;
+        // EPI_MODE 2: lane g keeps group g's modulus constants (read with a shuffle), so the
+        // per-group work has no integer division
+        uint32_t k_off = 0, k_c16 = 0, k_mg = 0;
+        if constexpr (EPI_MODE == 2) {
+            if (lane < P.ngroups) {
+                const uint32_t pm = (uint32_t)GROUPS[lane].pad;
+                k_off = pm * (0x80000000u / pm);
+                k_c16 = (1u << 16) % pm;
+                k_mg = (uint32_t)(0x100000000ull / pm) + 1u;
+            }
+        }
         for (int tile = unit; tile < total_tiles && ok; tile += units) {
             const TileCtx cx = ctx_of(tile);
             const int tm = cx.tm, tn = cx.tn;
@@ -565,33 +587,42 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                 // with 8 epilogue warps, two warps share a lane quarter and split the columns
                 constexpr int CHUNKS = TN / 32 / (EPI / 4);
                 const int ch0 = ((warp - 2) / 4) * CHUNKS;
-                for (int ch = ch0; ch < ch0 + CHUNKS; ++ch) {
-                    uint32_t v[32];
-                    tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TN + ch * 32), v);
-                    if constexpr (EPI_MODE == 2) {
-                        // acc mod p in integers.  |acc| <= k_pad 2^14 <= 2^31 - 2^21 (k_pad < 2^17),
-                        // so x = acc + off (off = p floor(2^31 / p) >= 2^31 - 256, a multiple of p)
-                        // lies in (0, 2^32); t = (x >> 16)(2^16 mod p) + (x & 0xffff) < 2^24 is
-                        // congruent to acc, and t / p = umulhi(t, floor(2^32 / p) + 1) exactly for
-                        // t < 2^24 (Granlund & Montgomery 1994, thm 4.2)
-                        const uint32_t pm = (uint32_t)GROUPS[g].pad;
-                        const uint32_t off = pm * (0x80000000u / pm), c16 = (1u << 16) % pm;
-                        const uint32_t mg = (uint32_t)(0x100000000ull / pm) + 1u;
-                        // Each lane holds one row; the plane is column-major with rows
-                        // contiguous.  Four columns' bytes of this lane's row form one word; a
-                        // 4 x 4 byte transpose across the quad of lanes 4a .. 4a+3 (two shuffle
-                        // steps) leaves lane 4a+b with column 4i+b's bytes of rows 4a .. 4a+3,
-                        // so a warp stores four columns x 32 rows with one word per lane.
-                        // Every lane of the warp stores, rows past m and columns past n
-                        // included: the plane has m_pad rows and n_pad columns.
-                        const int bq = lane & 3;
-                        const uint32_t selA = (bq & 2) ? 0x3276u : 0x5410u;  // swap 16-bit halves with lane ^ 2
-                        const uint32_t selB = (bq & 1) ? 0x3715u : 0x6240u;  // swap bytes with lane ^ 1
-                        const int64_t rld = DGT_TILE_FIELD(cx, res_ld, res_ld);
-                        uint8_t* rbase = DGT_TILE_FIELD(cx, res, res) + (int64_t)g * DGT_TILE_FIELD(cx, res_plane, res_plane) +
-                                         (row - lane + 4 * (lane >> 2)) + (n0 + ch * 32 + bq) * rld;
+                if constexpr (EPI_MODE == 2) {
+                    // acc mod p in integers.  |acc| <= k_pad 2^14 <= 2^31 - 2^21 (k_pad < 2^17),
+                    // so x = acc + off (off = p floor(2^31 / p) >= 2^31 - 256, a multiple of p)
+                    // lies in (0, 2^32); t = (x >> 16)(2^16 mod p) + (x & 0xffff) < 2^24 is
+                    // congruent to acc, and t / p = umulhi(t, floor(2^32 / p) + 1) exactly for
+                    // t < 2^24 (Granlund & Montgomery 1994, thm 4.2)
+                    const uint32_t pm = (uint32_t)GROUPS[g].pad;
+                    uint32_t off, c16, mg;
+                    if (g < 32) {
+                        off = __shfl_sync(0xffffffffu, k_off, g);
+                        c16 = __shfl_sync(0xffffffffu, k_c16, g);
+                        mg = __shfl_sync(0xffffffffu, k_mg, g);
+                    } else {
+                        off = pm * (0x80000000u / pm);
+                        c16 = (1u << 16) % pm;
+                        mg = (uint32_t)(0x100000000ull / pm) + 1u;
+                    }
+                    // Each lane holds one row; the plane is column-major with rows contiguous.
+                    // Four columns' bytes of this lane's row form one word; a 4 x 4 byte
+                    // transpose across the quad of lanes 4a .. 4a+3 (two shuffle steps) leaves
+                    // lane 4a+b with column 4i+b's bytes of rows 4a .. 4a+3, so a warp stores
+                    // four columns x 32 rows with one word per lane.  Every lane stores, rows
+                    // past m and columns past n included: the plane has m_pad rows and n_pad
+                    // columns.
+                    const int bq = lane & 3;
+                    const uint32_t selA = (bq & 2) ? 0x3276u : 0x5410u;  // swap 16-bit halves with lane ^ 2
+                    const uint32_t selB = (bq & 1) ? 0x3715u : 0x6240u;  // swap bytes with lane ^ 1
+                    const int64_t rld = DGT_TILE_FIELD(cx, res_ld, res_ld);
+                    uint8_t* rbase = DGT_TILE_FIELD(cx, res, res) + (int64_t)g * DGT_TILE_FIELD(cx, res_plane, res_plane) +
+                                     (row - lane + 4 * (lane >> 2)) + (n0 + ch0 * 32 + bq) * rld;
+                    static_assert(CHUNKS % 2 == 0, "residue epilogue: 64-column TMEM loads");
+                    for (int c2 = 0; c2 < CHUNKS / 2; ++c2) {
+                        uint32_t v[64];
+                        tmem_ld64(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TN + (ch0 + 2 * c2) * 32), v);
 #pragma unroll
-                        for (int i = 0; i < 8; ++i) {
+                        for (int i = 0; i < 16; ++i) {
                             uint32_t r[4];
 #pragma unroll
                             for (int u = 0; u < 4; ++u) {
@@ -602,10 +633,13 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                             uint32_t wd = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
                             wd = __byte_perm(wd, __shfl_xor_sync(0xffffffffu, wd, 2), selA);
                             wd = __byte_perm(wd, __shfl_xor_sync(0xffffffffu, wd, 1), selB);
-                            *reinterpret_cast<uint32_t*>(rbase + (int64_t)(4 * i) * rld) = wd;
+                            *reinterpret_cast<uint32_t*>(rbase + (int64_t)(64 * c2 + 4 * i) * rld) = wd;
                         }
-                        continue;
                     }
+                }
+                for (int ch = ch0; ch < ch0 + CHUNKS && EPI_MODE != 2; ++ch) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TN + ch * 32), v);
                     if (!row_ok) continue;
                     const int64_t rem_cols = DGT_TILE_FIELD(cx, n, n) - (n0 + ch * 32);
                     const int ncols = rem_cols < 32 ? (int)rem_cols : 32;
