@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dgt", choices=["dgt", "reference"])
     ap.add_argument("--size", type=int, default=SIZE)
-    ap.add_argument("--path", default="ozaki", choices=["native", "ozaki", "ozaki2", "sgemm", "pack"],
+    ap.add_argument("--path", default="ozaki", choices=["native", "ozaki", "ozaki2", "sgemm", "pack", "grouped2"],
                     help="--workload once: which path to call")
     ap.add_argument("--variant", type=int, default=-1, help="--workload once: kernel variant (-1: default)")
     ap.add_argument("--slices", type=int, default=8, help="--workload once: Ozaki slice count")
@@ -593,7 +593,9 @@ def workload_batching(args):
 def workload_once(args):
     """Two calls of one path at --size (the first warms up), for profiler captures: native
     DGEMM, Ozaki INT8 DGEMM (--slices = slices), CRT INT8 DGEMM (--slices = moduli), 3xBF16
-    SGEMM, or a 4x4 block-cyclic pack with 256 blocks.  Prints the second call's time."""
+    SGEMM, a 4x4 block-cyclic pack with 256 blocks, or (grouped2) one grouped CRT call over
+    --size products with M, N, K log-uniform in [128, 4096] (the law of the 256-product
+    batching workload).  Prints the second call's time."""
     import numpy as np
 
     torch, dgt, h = _setup()
@@ -609,6 +611,19 @@ def workload_once(args):
         C = torch.zeros((n, n), dtype=torch.float32, device="cuda")
         f = lambda: h.sgemm("N", "N", n, n, n, 1.0, A.data_ptr(), n, B.data_ptr(), n, 0.0, C.data_ptr(), n)
         flops = 2.0 * n ** 3
+    elif args.path == "grouped2":
+        dims = np.exp(np.random.default_rng(SEED + 5).uniform(np.log(128), np.log(4096), (n, 3))).round().astype(int)
+        keep, descs, flops = [], [], 0.0
+        for m_, n_, k_ in dims:
+            m_, n_, k_ = int(m_), int(n_), int(k_)
+            Ai = torch.rand((k_, m_), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+            Bi = torch.rand((n_, k_), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+            Ci = torch.zeros((n_, m_), dtype=torch.float64, device="cuda")
+            keep.append((Ai, Bi, Ci))
+            descs.append(dict(m=m_, n=n_, k=k_, alpha=1.0, beta=0.0, A=Ai.data_ptr(), lda=m_, B=Bi.data_ptr(), ldb=k_,
+                              C=Ci.data_ptr(), ldc=m_))
+            flops += 2.0 * m_ * n_ * k_
+        f = lambda: h.dgemm_grouped(descs, mode=dgt.FP64_OZAKI2_INT8, slices=args.slices)
     elif args.path == "pack":
         p = q = 4
         G = torch.rand((n, n), dtype=torch.float64, device="cuda", generator=g)
