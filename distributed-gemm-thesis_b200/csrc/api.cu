@@ -55,7 +55,7 @@ dgt_status device_table(dgt_context* h, int n, const void* const* parts, const s
 }
 
 dgt_status ensure_workspace(dgt_context* h, size_t bytes, void** out, int slot) {
-    if (slot < 0 || slot > 2) return fail(h, DGT_ERROR_INVALID_VALUE, "bad workspace slot");
+    if (slot < 0 || slot > 3) return fail(h, DGT_ERROR_INVALID_VALUE, "bad workspace slot");
     void*& ptr = h->ws[slot];
     size_t& cap = h->ws_bytes[slot];
     if (bytes > cap) {
@@ -167,6 +167,19 @@ dgt_status run_problems_emulated(dgt_context* h, const std::vector<Problem>& pro
     return DGT_SUCCESS;
 }
 
+dgt_status validate_gemm(dgt_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k, const void* A,
+                         int64_t lda, const void* B, int64_t ldb, const void* C, int64_t ldc) {
+    if (!valid_op(ta) || !valid_op(tb)) return fail(h, DGT_ERROR_INVALID_VALUE, "transpose must be N, T or C");
+    if (m < 0 || n < 0 || k < 0) return fail(h, DGT_ERROR_INVALID_VALUE, "negative dimension");
+    int64_t rowsA = is_trans(ta) ? k : m, rowsB = is_trans(tb) ? n : k;
+    if (lda < std::max<int64_t>(1, rowsA)) return fail(h, DGT_ERROR_INVALID_VALUE, "lda < rows of A");
+    if (ldb < std::max<int64_t>(1, rowsB)) return fail(h, DGT_ERROR_INVALID_VALUE, "ldb < rows of B");
+    if (ldc < std::max<int64_t>(1, m)) return fail(h, DGT_ERROR_INVALID_VALUE, "ldc < m");
+    if (m > 0 && n > 0 && !C) return fail(h, DGT_ERROR_INVALID_VALUE, "C is null");
+    if (m > 0 && n > 0 && k > 0 && (!A || !B)) return fail(h, DGT_ERROR_INVALID_VALUE, "A or B is null");
+    return DGT_SUCCESS;
+}
+
 }  // namespace dgt
 
 using namespace dgt;
@@ -209,6 +222,10 @@ dgt_status dgt_destroy(dgt_handle_t h) {
     cudaStreamSynchronize(h->stream);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : h->copy_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& cs : h->copy_stream)
+        if (cs) cudaStreamDestroy(cs);
     for (void* w : h->ws)
         if (w) cudaFree(w);
     for (auto& t : h->tables) cudaFree(t.ptr);
@@ -345,18 +362,6 @@ int32_t dgt_cannon_schedule(int32_t p, int32_t c, int32_t i, int32_t j, int32_t 
 
 // ---- local GEMM -----------------------------------------------------------------------
 
-static dgt_status validate_gemm(dgt_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k,
-                                const void* A, int64_t lda, const void* B, int64_t ldb, const void* C, int64_t ldc) {
-    if (!valid_op(ta) || !valid_op(tb)) return fail(h, DGT_ERROR_INVALID_VALUE, "transpose must be N, T or C");
-    if (m < 0 || n < 0 || k < 0) return fail(h, DGT_ERROR_INVALID_VALUE, "negative dimension");
-    int64_t rowsA = is_trans(ta) ? k : m, rowsB = is_trans(tb) ? n : k;
-    if (lda < std::max<int64_t>(1, rowsA)) return fail(h, DGT_ERROR_INVALID_VALUE, "lda < rows of A");
-    if (ldb < std::max<int64_t>(1, rowsB)) return fail(h, DGT_ERROR_INVALID_VALUE, "ldb < rows of B");
-    if (ldc < std::max<int64_t>(1, m)) return fail(h, DGT_ERROR_INVALID_VALUE, "ldc < m");
-    if (m > 0 && n > 0 && !C) return fail(h, DGT_ERROR_INVALID_VALUE, "C is null");
-    if (m > 0 && n > 0 && k > 0 && (!A || !B)) return fail(h, DGT_ERROR_INVALID_VALUE, "A or B is null");
-    return DGT_SUCCESS;
-}
 
 static dgt_status native_single(dgt_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
                                 const double* A, int64_t lda, const double* B, int64_t ldb, double beta, double* C,

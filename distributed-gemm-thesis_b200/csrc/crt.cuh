@@ -106,4 +106,34 @@ cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, in
                                int nmod);
 
 }  // namespace oz2
+// CRT product pieces (ozaki2.cu), for callers that split op(A) once and run op(B) in column
+// panels (dgt_dgemm_host): shape and constants of one product (K <= 65536), the workspace
+// carve (bytes only when ws is null), one operand's amax + residue split, and the residue
+// GEMM + reconstruction of one op(B) panel.
+struct Oz2Shape {
+    int nmod, bits, variant;
+    bool pair;
+    int64_t m, k, m_pad, n_pad, k_pad;
+    oz2::CrtConst cc;
+    oz2::ModTable mt;
+};
+struct Oz2Work {
+    size_t bytes = 0;
+    int8_t* planesA = nullptr;
+    int8_t* planesB = nullptr;
+    unsigned long long* amaxA = nullptr;
+    unsigned long long* amaxB = nullptr;
+    int32_t* expA = nullptr;
+    int32_t* expB = nullptr;
+    uint8_t* res = nullptr;
+};
+dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmod, Oz2Shape& sh);
+Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws);
+int64_t ozaki2_n_pad(int64_t n);  // op(B) columns padded to the GEMM's tile width
+dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, const double* X, int64_t ld, int64_t MN,
+                        int64_t mn_pad, bool kcontig, unsigned long long* amax, int32_t* exps, int8_t* planes);
+dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+                           const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
+                           uint8_t* res, double alpha, double beta, double* C, int64_t ldc);
+
 }  // namespace dgt

@@ -48,9 +48,13 @@ struct dgt_context {
     std::string last_error;
     unsigned int* dev_error = nullptr;  // one word in device memory
     // workspace slots: 0 = split planes of the Ozaki / FP32 split paths, 1 = autotuner and
-    // probes, 2 = the 2.5D stacks' partial C tiles (live across the Ozaki calls of a Cannon step)
-    void* ws[3] = {nullptr, nullptr, nullptr};
-    size_t ws_bytes[3] = {0, 0, 0};
+    // probes, 2 = the 2.5D stacks' partial C tiles (live across the Ozaki calls of a Cannon
+    // step), 3 = device copies of host operands (dgt_dgemm_host)
+    void* ws[4] = {nullptr, nullptr, nullptr, nullptr};
+    size_t ws_bytes[4] = {0, 0, 0, 0};
+    // dgt_dgemm_host: copy-in and copy-out streams and its events, created on first use
+    cudaStream_t copy_stream[2] = {nullptr, nullptr};
+    cudaEvent_t copy_ev[10] = {};
     std::atomic<int64_t> launches{0};
     std::map<dgt::TuneKey, dgt::TuneEntry> tune;
     // device copies of launch tables (grouped problems, Ozaki jobs and schedules), keyed by
@@ -137,6 +141,9 @@ struct Problem {
 int dmma_variant_count();
 TuneKey tune_key(int mode, int64_t m, int64_t n, int64_t k);
 const TuneEntry* tune_lookup(dgt_context* h, int mode, int64_t m, int64_t n, int64_t k);
+// Argument checks shared by the GEMM entry points (api.cu).
+dgt_status validate_gemm(dgt_context* h, char ta, char tb, int64_t m, int64_t n, int64_t k, const void* A,
+                         int64_t lda, const void* B, int64_t ldb, const void* C, int64_t ldc);
 // Launches the persistent grouped FP64 DMMA kernel over problems/segments (host arrays,
 // copied to device workspace).  Validation is the caller's job.
 dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs);

@@ -479,9 +479,8 @@ dgt_status ozaki2_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, 
     return DGT_SUCCESS;
 }
 
-static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
-                                     double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
-                                     double beta, double* C, int64_t ldc, int nmod) {
+// Paddings and limits of one CRT product (one K-chunk) with op(B) panels of up to n columns.
+dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmod, Oz2Shape& sh) {
     using namespace oz2;
     if (nmod < MIN_MODULI || nmod > MAX_MODULI)
         return fail(h, DGT_ERROR_INVALID_VALUE, "modulus count must be in [8, 20]");
@@ -490,55 +489,55 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     // kernel variant: 0 (4 epilogue warps), 4 (CTA pair) or 1 (8 warps); all 128-byte stages
     const int variant = (h->ozaki_variant == 0 || h->ozaki_variant == 4) ? h->ozaki_variant : 1;
     const bool pair = variant == 4;
-    const int tkb = 128;
     const int64_t m_unit = pair ? 2 * oz::TM : oz::TM;
-    const int64_t m_pad = ceil_div(m, m_unit) * m_unit, n_pad = ceil_div(n, oz::TN) * oz::TN;
-    const int64_t k_pad = ceil_div(k, oz::KPAD) * oz::KPAD;
-    if (k_pad >= (int64_t)1 << 17)  // k_pad * 128^2 must stay below 2^31
+    sh.nmod = nmod;
+    sh.bits = bits;
+    sh.variant = variant;
+    sh.pair = pair;
+    sh.m = m;
+    sh.k = k;
+    sh.m_pad = ceil_div(m, m_unit) * m_unit;
+    sh.n_pad = ceil_div(n, oz::TN) * oz::TN;
+    sh.k_pad = ceil_div(k, oz::KPAD) * oz::KPAD;
+    if (sh.k_pad >= (int64_t)1 << 17)  // k_pad * 128^2 must stay below 2^31
         return fail(h, DGT_ERROR_UNSUPPORTED, "K too long for exact INT32 residue products");
-    if ((int64_t)nmod * std::max(m_pad, n_pad) > INT32_MAX)
+    if ((int64_t)nmod * std::max(sh.m_pad, sh.n_pad) > INT32_MAX)
         return fail(h, DGT_ERROR_UNSUPPORTED, "matrix too large for 32-bit TMA coordinates");
-    auto up = [](size_t x) { return (x + 1023) / 1024 * 1024; };
-    const size_t pa = up((size_t)nmod * m_pad * k_pad), pb = up((size_t)nmod * n_pad * k_pad);
-    const size_t xa = up((size_t)m * 8), xb = up((size_t)n * 8), ea = up((size_t)m * 4), eb = up((size_t)n * 4);
-    const size_t rs = up((size_t)nmod * m_pad * n_pad);
-    void* ws = nullptr;
-    dgt_status st = ensure_workspace(h, pa + pb + xa + xb + ea + eb + rs, &ws, 0);
+    crt_constants(nmod, sh.cc, sh.mt);
+    return DGT_SUCCESS;
+}
+
+// amax and residue planes of one operand: the MN rows of op(A) (kcontig = transa) or the MN
+// columns of op(B) (kcontig = !transb), planes padded to mn_pad rows.
+dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, const double* X, int64_t ld, int64_t MN,
+                        int64_t mn_pad, bool kcontig, unsigned long long* amax, int32_t* exps, int8_t* planes) {
+    using namespace oz2;
+    dgt_status st = ozaki_amax(h, s, X, ld, MN, sh.k, kcontig, amax);
     if (st != DGT_SUCCESS) return st;
-    char* p = (char*)ws;
-    int8_t* planesA = (int8_t*)p;
-    int8_t* planesB = (int8_t*)(p + pa);
-    auto* amaxA = (unsigned long long*)(p + pa + pb);
-    auto* amaxB = (unsigned long long*)(p + pa + pb + xa);
-    auto* expA = (int32_t*)(p + pa + pb + xa + xb);
-    auto* expB = (int32_t*)(p + pa + pb + xa + xb + ea);
-    auto* res = (uint8_t*)(p + pa + pb + xa + xb + ea + eb);
+    dim3 grid((unsigned)ceil_div(mn_pad, RES_ROWS), (unsigned)(sh.k_pad / RES_KSPAN));
+    if (kcontig)
+        split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sh.bits, amax, exps,
+                                                  planes, sh.mt);
+    else
+        split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sh.bits, amax, exps,
+                                                   planes, sh.mt);
+    h->launches.fetch_add(1);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DGT_SUCCESS : cuda_fail(h, e, "residue split");
+}
 
-    CrtConst cc;
-    ModTable mt;
-    crt_constants(nmod, cc, mt);
-    cudaStream_t s = h->stream;
-    mark(h, 0);
-    // op(A) is m x k: 'N' -> MN-contiguous; op(B) as its transpose n x k: 'N' -> K-contiguous
-    if ((st = ozaki_amax(h, s, A, lda, m, k, ta, amaxA)) != DGT_SUCCESS) return st;
-    if ((st = ozaki_amax(h, s, B, ldb, n, k, !tb, amaxB)) != DGT_SUCCESS) return st;
-    auto split = [&](const double* X, int64_t ld, int64_t MN, int64_t mn_pad, bool kcontig,
-                     const unsigned long long* am, int32_t* ex, int8_t* planes) -> dgt_status {
-        dim3 grid((unsigned)ceil_div(mn_pad, RES_ROWS), (unsigned)(k_pad / RES_KSPAN));
-        if (kcontig)
-            split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, k, mn_pad, k_pad, nmod, bits, am, ex, planes, mt);
-        else
-            split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, k, mn_pad, k_pad, nmod, bits, am, ex, planes, mt);
-        h->launches.fetch_add(1);
-        cudaError_t e = cudaGetLastError();
-        return e == cudaSuccess ? DGT_SUCCESS : cuda_fail(h, e, "residue split");
-    };
-    if ((st = split(A, lda, m, m_pad, ta, amaxA, expA, planesA)) != DGT_SUCCESS) return st;
-    if ((st = split(B, ldb, n, n_pad, !tb, amaxB, expB, planesB)) != DGT_SUCCESS) return st;
-
+// Residue GEMM of split operands (op(A) planes for sh.m rows, op(B) planes for n columns
+// padded to n_pad) and the reconstruction C = alpha C' + beta C.
+dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+                           const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
+                           uint8_t* res, double alpha, double beta, double* C, int64_t ldc) {
+    using namespace oz2;
+    const int nmod = sh.nmod, tkb = 128;
+    const int64_t m = sh.m, m_pad = sh.m_pad, k_pad = sh.k_pad;
+    const int64_t m_unit = sh.pair ? 2 * oz::TM : oz::TM;
     CUtensorMap tmA, tmB;
-    if (!oz::make_plane_map(&tmA, planesA, (int64_t)nmod * m_pad, k_pad, oz::TM, tkb) ||
-        !oz::make_plane_map(&tmB, planesB, (int64_t)nmod * n_pad, k_pad, pair ? oz::TN / 2 : oz::TN, tkb))
+    if (!oz::make_plane_map(&tmA, (void*)planesA, (int64_t)nmod * m_pad, k_pad, oz::TM, tkb) ||
+        !oz::make_plane_map(&tmB, (void*)planesB, (int64_t)nmod * n_pad, k_pad, sh.pair ? oz::TN / 2 : oz::TN, tkb))
         return fail(h, DGT_ERROR_CUDA, "cuTensorMapEncodeTiled failed");
     static thread_local oz::Params prm;
     prm = oz::Params{};
@@ -552,7 +551,7 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     prm.ngroups = nmod;
     for (int j = 0; j < nmod; ++j) {  // one group per modulus: the residue product over all of K
         prm.segs[j] = oz::Seg{j, j, 0, (int32_t)(k_pad / tkb)};
-        prm.groups[j] = oz::Group{j, j + 1, 0, mt.p[j]};
+        prm.groups[j] = oz::Group{j, j + 1, 0, sh.mt.p[j]};
     }
     prm.res = res;
     prm.res_ld = m_pad;
@@ -560,9 +559,9 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     prm.err = h->dev_error;
     mark(h, 1);
     cudaError_t le;
-    if (variant == 4)
+    if (sh.variant == 4)
         le = launch_residue_gemm<oz::OzCfg<8, 128, 6, true>>(tmA, tmB, prm, h->num_sms, s);
-    else if (variant == 0)
+    else if (sh.variant == 0)
         le = launch_residue_gemm<oz::OzCfg<4, 128, 4>>(tmA, tmB, prm, h->num_sms, s);
     else
         le = launch_residue_gemm<oz::OzCfg<8, 128, 4>>(tmA, tmB, prm, h->num_sms, s);
@@ -571,6 +570,8 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     mark(h, 2);
     const int64_t threads = ceil_div(m, 4) * n;
     const unsigned blocks = (unsigned)ceil_div(threads, 256);
+    const CrtConst& cc = sh.cc;
+    const int bits = sh.bits;
 #define DGT_CRT_LAUNCH(NW, NM)                                                                            \
     crt_reconstruct<NW, NM><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta, \
                                                    C, ldc, cc)
@@ -589,6 +590,46 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     h->launches.fetch_add(1);
     DGT_CUDA_TRY(h, cudaGetLastError());
     return DGT_SUCCESS;
+}
+
+int64_t ozaki2_n_pad(int64_t n) { return ceil_div(n, oz::TN) * oz::TN; }
+
+// Workspace carve of one CRT product: planes of op(A) (m_pad rows) and op(B) (n_pad rows),
+// amax words, exponents and the residue planes of C.
+Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws) {
+    auto up = [](size_t x) { return (x + 1023) / 1024 * 1024; };
+    const size_t pa = up((size_t)sh.nmod * sh.m_pad * sh.k_pad), pb = up((size_t)sh.nmod * n_pad * sh.k_pad);
+    const size_t xa = up((size_t)sh.m * 8), xb = up((size_t)n * 8), ea = up((size_t)sh.m * 4), eb = up((size_t)n * 4);
+    const size_t rs = up((size_t)sh.nmod * sh.m_pad * n_pad);
+    Oz2Work w;
+    w.bytes = pa + pb + xa + xb + ea + eb + rs;
+    char* p = (char*)ws;
+    if (!p) return w;
+    w.planesA = (int8_t*)p;
+    w.planesB = (int8_t*)(p + pa);
+    w.amaxA = (unsigned long long*)(p + pa + pb);
+    w.amaxB = (unsigned long long*)(p + pa + pb + xa);
+    w.expA = (int32_t*)(p + pa + pb + xa + xb);
+    w.expB = (int32_t*)(p + pa + pb + xa + xb + ea);
+    w.res = (uint8_t*)(p + pa + pb + xa + xb + ea + eb);
+    return w;
+}
+
+static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+                                     double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                     double beta, double* C, int64_t ldc, int nmod) {
+    Oz2Shape sh;
+    dgt_status st = ozaki2_shape(h, m, n, k, nmod, sh);
+    if (st != DGT_SUCCESS) return st;
+    void* ws = nullptr;
+    if ((st = ensure_workspace(h, ozaki2_carve(sh, n, sh.n_pad, nullptr).bytes, &ws, 0)) != DGT_SUCCESS) return st;
+    const Oz2Work w = ozaki2_carve(sh, n, sh.n_pad, ws);
+    cudaStream_t s = h->stream;
+    mark(h, 0);
+    // op(A) is m x k: 'N' -> MN-contiguous; op(B) as its transpose n x k: 'N' -> K-contiguous
+    if ((st = ozaki2_split(h, s, sh, A, lda, m, sh.m_pad, ta, w.amaxA, w.expA, w.planesA)) != DGT_SUCCESS) return st;
+    if ((st = ozaki2_split(h, s, sh, B, ldb, n, sh.n_pad, !tb, w.amaxB, w.expB, w.planesB)) != DGT_SUCCESS) return st;
+    return ozaki2_gemm_crt(h, s, sh, n, sh.n_pad, w.planesA, w.expA, w.planesB, w.expB, w.res, alpha, beta, C, ldc);
 }
 
 }  // namespace dgt

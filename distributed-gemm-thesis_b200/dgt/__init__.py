@@ -64,6 +64,8 @@ SIGNATURES = [
                            _dp, _vp, _c_i64]),
     ("dgt_dgemm_ex", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _dp, _vp, _c_i64, _vp,
                               _c_i64, _dp, _vp, _c_i64, _c_i32, ctypes.c_int]),
+    ("dgt_dgemm_host", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _dp, _vp, _c_i64, _vp,
+                                _c_i64, _dp, _vp, _c_i64, _c_i32, ctypes.c_int, _c_i64]),
     ("dgt_sgemm", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _fp, _vp, _c_i64, _vp, _c_i64,
                            _fp, _vp, _c_i64, _c_i32]),
     ("dgt_dgemm_grouped", _c_i32, [_vp, ctypes.c_int, ctypes.POINTER(GemmDesc), _c_i32, ctypes.c_int]),
@@ -210,6 +212,13 @@ class Handle:
             st = self.lib.dgt_dgemm_ex(self.h, ta.encode(), tb.encode(), m, n, k, ctypes.byref(a), _vp(A), lda,
                                        _vp(B), ldb, ctypes.byref(b), _vp(C), ldc, mode, slices)
         self._check(st)
+
+    def dgemm_host(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, mode=FP64_NATIVE, slices=7,
+                   panel_cols=0):
+        """dgt_dgemm_host: A, B, C are HOST addresses (page-locked for overlapped copies)."""
+        a, b = ctypes.c_double(alpha), ctypes.c_double(beta)
+        self._check(self.lib.dgt_dgemm_host(self.h, ta.encode(), tb.encode(), m, n, k, ctypes.byref(a), _vp(A), lda,
+                                            _vp(B), ldb, ctypes.byref(b), _vp(C), ldc, mode, slices, panel_cols))
 
     def sgemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, mode=FP32_BF16X3):
         a, b = ctypes.c_float(alpha), ctypes.c_float(beta)
