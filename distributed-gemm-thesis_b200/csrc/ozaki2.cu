@@ -269,7 +269,7 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
 #pragma unroll
     for (int j = 0; j < MAX_MODULI; ++j) {
         if (NM ? j < NM : j < cc.n) {
-            const uint32_t r = (rr[j] >> (8 * sel)) & 0xffu;
+            const uint32_t r = __byte_perm(rr[j], 0u, 0x4440u + (uint32_t)sel);  // byte sel
 #pragma unroll
             for (int l = 0; l < NW; ++l) acc[l] += (uint64_t)r * cc.W[j][l];  // < 20 * 2^40
         }
@@ -309,28 +309,34 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
 #pragma unroll
         for (int l = 0; l < NX; ++l) x[l] = z[l];
     }
-    int L = 0;
+    // The magnitude as 64-bit words; the top nonzero word and the one below it give the
+    // leading 64 bits, everything further down only a sticky bit, so the one rounding to 53
+    // bits is correct (round to nearest even).
+    constexpr int NWD = (NX + 1) / 2;
+    uint64_t wd[NWD];
 #pragma unroll
-    for (int l = 1; l < NX; ++l)
-        if (x[l] != 0u) L = l;
-    uint32_t a2 = 0, a1 = 0, a0 = 0;
+    for (int i = 0; i < NWD; ++i)
+        wd[i] = (uint64_t)x[2 * i] | (2 * i + 1 < NX ? (uint64_t)x[2 * i + 1] << 32 : 0ull);
+    uint64_t hi = wd[0], lo = 0;
     bool sticky = false;
+    int ti = 0;
 #pragma unroll
-    for (int l = 0; l < NX; ++l) {
-        if (l == L) a2 = x[l];
-        if (l == L - 1) a1 = x[l];
-        if (l == L - 2) a0 = x[l];
-        if (l < L - 2 && x[l] != 0u) sticky = true;
+    for (int i = 1; i < NWD; ++i) {
+        if (wd[i] != 0ull) {
+            hi = wd[i];
+            lo = wd[i - 1];
+            ti = i;
+        }
     }
-    if (a2 == 0u) return 0.0;
-    const int lz = __clz(a2);
-    const uint64_t top = ((uint64_t)a2 << 32) | a1;
-    const uint64_t top64 = lz ? (top << lz) | (uint64_t)(a0 >> (32 - lz)) : top;
-    sticky |= lz ? (uint32_t)(a0 << lz) != 0u : a0 != 0u;
-    // top64 carries the leading 64 bits; its bit 0 absorbs the rest as a sticky bit, so the
-    // one rounding to 53 bits is correct (round to nearest even)
+#pragma unroll
+    for (int i = 0; i + 2 < NWD; ++i)
+        if (i + 2 <= ti && wd[i] != 0ull) sticky = true;
+    if (hi == 0ull) return 0.0;
+    const int lz = __clzll((long long)hi);
+    const uint64_t top64 = lz ? (hi << lz) | (lo >> (64 - lz)) : hi;
+    sticky |= (lz ? (lo << lz) : lo) != 0ull;
     const double d = __ull2double_rn(top64 | (uint64_t)sticky);
-    const double mag = oz::scale2(d, 32 * (L - 1) - lz + shift);
+    const double mag = oz::scale2(d, 64 * ti - lz + shift);
     return neg ? -mag : mag;
 }
 
