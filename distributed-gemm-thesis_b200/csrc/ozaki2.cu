@@ -145,6 +145,20 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         if (by == 0 && seg == 0) exps[mn] = e;
     }
     const bool live = (mn < MN) && (e != oz::EXP_NONFINITE);
+    const int64_t plane = mn_pad * k_pad;
+    int8_t* out = planes + mn * k_pad + k0;
+    if (!live || k0 >= K) {  // padding (or a non-finite row): zero residues, no arithmetic
+#pragma unroll 4
+        for (int j = 0; j < nmod; ++j, out += plane) {
+            if constexpr (E % 16 == 0) {
+#pragma unroll
+                for (int q = 0; q < E / 16; ++q) reinterpret_cast<uint4*>(out)[q] = make_uint4(0u, 0u, 0u, 0u);
+            } else {
+                *reinterpret_cast<uint2*>(out) = make_uint2(0u, 0u);
+            }
+        }
+        return;
+    }
     int32_t x0[E], x1[E], x2[E];  // x = x2 2^40 + x1 2^20 + x0, x0 and x1 in [0, 2^20)
 #pragma unroll
     for (int i = 0; i < E; ++i) {
@@ -157,8 +171,6 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         x1[i] = (int32_t)((x >> 20) & 0xfffff);
         x2[i] = (int32_t)(x >> 40);
     }
-    int8_t* out = planes + mn * k_pad + k0;
-    const int64_t plane = mn_pad * k_pad;
     for (int j = 0; j < nmod; ++j, out += plane) {
         const int32_t p = mt.p[j], c20 = mt.c20[j], c40 = mt.c40[j], mg = mt.magic[j];
         const long long bias = mt.bias[j];
