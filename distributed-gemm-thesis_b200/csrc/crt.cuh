@@ -52,7 +52,7 @@ constexpr int MAX_MODULI = 20, MIN_MODULI = 8;
 constexpr int MAX_NW = 5;     // 32-bit limbs of W_p and P (P < 2^160)
 constexpr int MAX_BETA = 58;  // |A'| < 2^58
 
-// Residues of x = trunc(a 2^(beta-e)) (|x| <= 2^58) modulo p, in integers: x is cut into
+// Residues of x = rn(a 2^(beta-e)) (|x| <= 2^58) modulo p, in integers: x is cut into
 // 20-bit chunks x0, x1 (unsigned) and x2 = x >> 40 (arithmetic, |x2| <= 2^18), so
 // t = x2 c40 + x1 c20 + x0 (c20 = 2^20 mod p, c40 = 2^40 mod p) is congruent to x with
 // -2^26 < t < 2^29.  n = t + floor(p/2) + 2^18 p then lies in [0, 2^30), and with
@@ -97,7 +97,7 @@ struct CrtJob {
 };
 
 // host helpers (ozaki2.cu)
-int beta_for(int nmod, int64_t k);   // operand bits: largest beta with 2 k (2^beta - 1)^2 < P
+int beta_for(int nmod, int64_t k);   // operand bits: largest beta with 2 k 2^(2 beta) < P
 int limbs_for(int nmod);             // 32-bit limbs of P
 void crt_constants(int nmod, CrtConst& cc, ModTable& mt);
 cudaError_t launch_split_residues_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks,

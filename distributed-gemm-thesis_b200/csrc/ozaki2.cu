@@ -3,8 +3,9 @@
 // floating-point matrix multiplication using an integer modular technique").
 //
 //   1. Scale: row i of op(A) gets e_i with max_k |a_ik| in [2^(e_i-1), 2^e_i), column j of
-//      op(B) gets f_j likewise; A'_ik = trunc(a_ik 2^(beta-e_i)) and B'_kj = trunc(b_kj
-//      2^(beta-f_j)) are integers below 2^beta in magnitude (exact in FP64 for beta <= 58).
+//      op(B) gets f_j likewise; A'_ik = rn(a_ik 2^(beta-e_i)) and B'_kj = rn(b_kj
+//      2^(beta-f_j)) (rounded to nearest even) are integers of magnitude at most 2^beta
+//      (exact in FP64 for beta <= 58).
 //   2. Residues: for N pairwise coprime moduli p <= 256 with P = prod p > 2 k 2^(2 beta),
 //      A' mod p and B' mod p in the symmetric range [-(p/2), (p-1)/2] are INT8 planes.
 //   3. Multiply: (A' mod p)(B' mod p) is exact in INT32 (|sum| <= k 128^2 < 2^31) on the
@@ -86,7 +87,8 @@ static double log2_product(int n) {
     return s;
 }
 
-// Largest beta with 2 k (2^beta - 1)^2 < P (with a 1e-9 margin on the logarithms).
+// Largest beta with 2 k 2^(2 beta) < P (with a 1e-9 margin on the logarithms; operands are
+// rounded to nearest, so |A'|, |B'| <= 2^beta).
 int beta_for(int n, int64_t k) {
     const double b = (log2_product(n) - 1.0 - std::log2((double)std::max<int64_t>(k, 1))) / 2.0 - 1e-9;
     return std::min(MAX_BETA, (int)std::floor(b));
@@ -165,8 +167,10 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         const int64_t kk = k0 + i;
         double a = 0.0;
         if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
-        // an integer of magnitude <= 2^beta <= 2^58 (exact scaling, truncation toward 0)
-        const long long x = live ? __double2ll_rz(oz::scale2(a, beta - e)) : 0ll;
+        // an integer of magnitude <= 2^beta <= 2^58 (exact scaling, rounded to nearest even:
+        // half the quantisation error of truncation, and |x| <= 2^beta stays inside the
+        // operand-bit rule, which bounds k 2^(2 beta))
+        const long long x = live ? __double2ll_rn(oz::scale2(a, beta - e)) : 0ll;
         x0[i] = (int32_t)(x & 0xfffff);
         x1[i] = (int32_t)((x >> 20) & 0xfffff);
         x2[i] = (int32_t)(x >> 40);
@@ -295,7 +299,7 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
         c = t >> 32;
     }
     x[NW] = (uint32_t)c;
-    // X = q P + C' with |C'| <= k (2^beta - 1)^2 < (P / 2)(1 - 1.3e-9) by the operand-bit rule
+    // X = q P + C' with |C'| <= k 2^(2 beta) < (P / 2)(1 - 1.3e-9) by the operand-bit rule
     // (beta_for keeps a 1e-9 margin on its logarithms), so q is the integer nearest X / P, and
     // the estimate from the top three limbs is within 2^-37 of X / P (X < 2^13 P; the dropped
     // limbs are below 2^-37 P): rint gives q exactly, and X - q P is C' itself.

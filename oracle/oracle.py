@@ -418,7 +418,7 @@ OZAKI2_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
 
 def ozaki2_beta(nmod: int, k: int) -> int:
     """Operand bits for nmod moduli and inner dimension k: the largest beta (capped at 58)
-    with 2 k (2^beta - 1)^2 < P, chosen from logarithms with a 1e-9 margin."""
+    with 2 k 2^(2 beta) < P, chosen from logarithms with a 1e-9 margin."""
     import math
 
     lg = 0.0
@@ -437,7 +437,8 @@ def _exp_of_max(v: float) -> int:
 
 def ozaki2_exact(A, B, nmod: int, ta: str = "N", tb: str = "N"):
     """C = op(A) op(B) as the CRT emulation computes it: operands scaled per row of op(A) /
-    column of op(B) to beta-bit integers (truncated), their integer product taken exactly,
+    column of op(B) to integers of at most beta bits (rounded to nearest even), their integer
+    product taken exactly,
     rounded once to FP64 and scaled back.  Pure Python integers: small sizes only."""
     import math
 
@@ -448,11 +449,11 @@ def ozaki2_exact(A, B, nmod: int, ta: str = "N", tb: str = "N"):
     P = 1
     for p in OZAKI2_MODULI[:nmod]:
         P *= p
-    assert 2 * k * (2 ** beta - 1) ** 2 < P  # the CRT range covers every product
+    assert 2 * k * 2 ** (2 * beta) < P  # the CRT range covers every product (|A'|, |B'| <= 2^beta)
     ea = [_exp_of_max(float(np.max(np.abs(Aop[i, :])))) if k else 0 for i in range(m)]
     fb = [_exp_of_max(float(np.max(np.abs(Bop[:, j])))) if k else 0 for j in range(n)]
-    Ai = [[int(math.trunc(math.ldexp(float(Aop[i, t]), beta - ea[i]))) for t in range(k)] for i in range(m)]
-    Bi = [[int(math.trunc(math.ldexp(float(Bop[t, j]), beta - fb[j]))) for t in range(k)] for j in range(n)]
+    Ai = [[int(round(math.ldexp(float(Aop[i, t]), beta - ea[i]))) for t in range(k)] for i in range(m)]
+    Bi = [[int(round(math.ldexp(float(Bop[t, j]), beta - fb[j]))) for t in range(k)] for j in range(n)]
     C = np.empty((m, n))
     for i in range(m):
         for j in range(n):
@@ -474,9 +475,9 @@ def ozaki2_residue_check(A, B, nmod: int):
     P = math.prod(mods)
     ea = [_exp_of_max(float(np.max(np.abs(A[i, :])))) for i in range(m)]
     fb = [_exp_of_max(float(np.max(np.abs(B[:, j])))) for j in range(n)]
-    Ai = np.array([[int(math.trunc(math.ldexp(float(A[i, t]), beta - ea[i]))) for t in range(k)]
+    Ai = np.array([[int(round(math.ldexp(float(A[i, t]), beta - ea[i]))) for t in range(k)]
                    for i in range(m)], dtype=object)
-    Bi = np.array([[int(math.trunc(math.ldexp(float(B[t, j]), beta - fb[j]))) for j in range(n)]
+    Bi = np.array([[int(round(math.ldexp(float(B[t, j]), beta - fb[j]))) for j in range(n)]
                    for t in range(k)], dtype=object)
 
     def sym(x, p):
