@@ -26,8 +26,9 @@ struct SplitJob {
     int32_t split_bx;     // split blocks along mn (times k_pad / 32 along K)
     int64_t amax_begin;   // first block of this job in the amax launch
     int64_t split_begin;  // first block of this job in the split launch
-    int32_t bits;         // CRT scheme: operand bits of this product
+    int32_t bits;         // CRT scheme: sigma (row / column 2-norm bound 2^sigma) of this product
     int32_t unused;
+    unsigned long long* qn;  // CRT scheme: integer 2-norm bounds per row (see qnorm_*)
 };
 constexpr int AMAX_KCHUNK = 64;  // K rows per block of the MN-contiguous amax (fills the GPU)
 
@@ -97,9 +98,10 @@ struct CrtJob {
 };
 
 // host helpers (ozaki2.cu)
-int beta_for(int nmod, int64_t k);   // operand bits: largest beta with 2 k 2^(2 beta) < P
+int sigma_for(int nmod, int64_t k);  // 2-norm bound exponent of the scaled rows / columns
 int limbs_for(int nmod);             // 32-bit limbs of P
 void crt_constants(int nmod, CrtConst& cc, ModTable& mt);
+cudaError_t launch_qnorm_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks);
 cudaError_t launch_split_residues_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks,
                                           int nmod, const ModTable& mt);
 cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, int64_t threads, const CrtConst& cc,
@@ -123,6 +125,8 @@ struct Oz2Work {
     int8_t* planesB = nullptr;
     unsigned long long* amaxA = nullptr;
     unsigned long long* amaxB = nullptr;
+    unsigned long long* qnA = nullptr;
+    unsigned long long* qnB = nullptr;
     int32_t* expA = nullptr;
     int32_t* expB = nullptr;
     uint8_t* res = nullptr;
@@ -131,7 +135,8 @@ dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmo
 Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws);
 int64_t ozaki2_n_pad(int64_t n);  // op(B) columns padded to the GEMM's tile width
 dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, const double* X, int64_t ld, int64_t MN,
-                        int64_t mn_pad, bool kcontig, unsigned long long* amax, int32_t* exps, int8_t* planes);
+                        int64_t mn_pad, bool kcontig, unsigned long long* amax, unsigned long long* qn, int32_t* exps,
+                        int8_t* planes);
 dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
                            const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
                            uint8_t* res, double alpha, double beta, double* C, int64_t ldc);

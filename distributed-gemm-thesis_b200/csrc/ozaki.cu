@@ -515,8 +515,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
         o.m_pad = ceil_div(p.m, oz::TM) * oz::TM;
         o.n_pad = ceil_div(p.n, oz::TN) * oz::TN;
         o.k_pad = ceil_div(p.k, oz::KPAD) * oz::KPAD;
-        o.bits = crt ? oz2::beta_for(S, p.k) : 0;
-        if (crt && o.bits < 8) return DGT_ERROR_UNSUPPORTED;
+        o.bits = crt ? oz2::sigma_for(S, p.k) : 0;
         if ((int64_t)S * std::max(o.m_pad, o.n_pad) > INT32_MAX) return DGT_ERROR_UNSUPPORTED;
         o.pa = planes;
         planes += up((size_t)S * o.m_pad * o.k_pad, 1024);
@@ -533,7 +532,8 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
         o.eb = exp_words;
         exp_words += (size_t)p.n;
     }
-    const size_t amax_at = planes, exp_at = up(amax_at + amax_words * 8, 256);
+    // CRT: the rows' integer 2-norm bounds follow the amax words
+    const size_t amax_at = planes, exp_at = up(amax_at + amax_words * 8 * (crt ? 2 : 1), 256);
     const size_t total = up(exp_at + exp_words * 4, 256);
     void* ws = nullptr;
     dgt_status st = ensure_workspace(h, total, &ws, 0);
@@ -620,6 +620,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
             J.mn_pad = pad[t];
             J.k_pad = o.k_pad;
             J.amax = amax + xo[t];
+            J.qn = crt ? amax + amax_words + xo[t] : nullptr;
             J.exps = exps + eo[t];
             J.planes = pl[t];
             J.kcontig = kc[t] ? 1 : 0;
@@ -650,11 +651,13 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     const auto* d_crt = crt ? (const oz2::CrtJob*)((char*)table + offs[2]) : nullptr;
 
     mark(h, 0);
-    DGT_CUDA_TRY(h, cudaMemsetAsync(amax, 0, amax_words * 8, s));
+    DGT_CUDA_TRY(h, cudaMemsetAsync(amax, 0, amax_words * 8 * (crt ? 2 : 1), s));
     oz::amax_grouped<<<(unsigned)amax_blocks, 256, 0, s>>>(d_jobs, 2 * T);
     h->launches.fetch_add(1);
     DGT_CUDA_TRY(h, cudaGetLastError());
     if (crt) {
+        DGT_CUDA_TRY(h, oz2::launch_qnorm_grouped(s, d_jobs, 2 * T, amax_blocks));
+        h->launches.fetch_add(1);
         DGT_CUDA_TRY(h, oz2::launch_split_residues_grouped(s, d_jobs, 2 * T, split_blocks, S, mt));
     } else {
         oz::split_grouped<<<(unsigned)split_blocks, 128, 0, s>>>(d_jobs, 2 * T, S);

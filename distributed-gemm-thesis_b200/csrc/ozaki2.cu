@@ -2,18 +2,21 @@
 // Ozaki, Uchino, Imamura 2025, "Ozaki Scheme II: A GEMM-oriented emulation of
 // floating-point matrix multiplication using an integer modular technique").
 //
-//   1. Scale: row i of op(A) gets e_i with max_k |a_ik| in [2^(e_i-1), 2^e_i), column j of
-//      op(B) gets f_j likewise; A'_ik = rn(a_ik 2^(beta-e_i)) and B'_kj = rn(b_kj
-//      2^(beta-f_j)) (rounded to nearest even) are integers of magnitude at most 2^beta
-//      (exact in FP64 for beta <= 58).
-//   2. Residues: for N pairwise coprime moduli p <= 256 with P = prod p > 2 k 2^(2 beta),
+//   1. Scale: row i of op(A) gets s_i = min(sigma - g_i, 58 - e_i), where max_k |a_ik| <
+//      2^e_i and 2^g_i bounds the row's 2-norm; A'_ik = rn(a_ik 2^s_i) (rounded to nearest
+//      even) is an integer of magnitude at most 2^58 and the row's 2-norm is at most
+//      2^sigma + sqrt(k)/2; columns of op(B) likewise.  By Cauchy-Schwarz every |(A'B')_ij|
+//      is below (P/2)(1 - 2^-20) for sigma from sigma_for.  Scaling by the norm instead of
+//      the max spends the integer range where the row's mass is: rows with a few large
+//      entries among many small ones keep more bits.
+//   2. Residues: for N pairwise coprime moduli p <= 256 (P = prod p),
 //      A' mod p and B' mod p in the symmetric range [-(p/2), (p-1)/2] are INT8 planes.
 //   3. Multiply: (A' mod p)(B' mod p) is exact in INT32 (|sum| <= k 128^2 < 2^31) on the
 //      tcgen05 INT8 tensor cores -- one GEMM per modulus, N in all -- and its epilogue keeps
 //      only the residue of each element modulo p (one byte).
 //   4. Reconstruct: C'_ij = sum_p r_p W_p mod P (W_p = (P/p) ((P/p)^-1 mod p)), taken in
 //      the symmetric range, equals (A'B')_ij exactly; it is rounded once to FP64 (correctly)
-//      and scaled by 2^(e_i + f_j - 2 beta).  C = alpha C' + beta_C C.
+//      and scaled by 2^-(s_i + t_j).  C = alpha C' + beta_C C.
 //
 // Against the slice scheme (ozaki.cu), N GEMMs replace S(S+1)/2 digit products for the
 // same number of operand bits (N = 17 moduli: beta = 58 bits at K <= 16384, versus 36
@@ -87,11 +90,18 @@ static double log2_product(int n) {
     return s;
 }
 
-// Largest beta with 2 k 2^(2 beta) < P (with a 1e-9 margin on the logarithms; operands are
-// rounded to nearest, so |A'|, |B'| <= 2^beta).
-int beta_for(int n, int64_t k) {
-    const double b = (log2_product(n) - 1.0 - std::log2((double)std::max<int64_t>(k, 1))) / 2.0 - 1e-9;
-    return std::min(MAX_BETA, (int)std::floor(b));
+// Norm scaling.  Row i of op(A) is scaled by 2^s_i with s_i = min(sigma - g_i, 58 - e_i):
+// 2^g_i bounds the row's 2-norm (g_i from the integer bound of qnorm_*), e_i its max, so every
+// scaled row has 2-norm <= 2^sigma and every element magnitude below 2^58 (the split's range);
+// columns of op(B) likewise.  After rounding to nearest, ||A'_i|| <= 2^sigma + sqrt(k)/2, and
+// by Cauchy-Schwarz |C'_ij| <= (2^sigma + sqrt(k)/2)^2.  sigma is the largest integer keeping
+// that below (P/2)(1 - 2^-20), which the reconstruction's exact quotient needs (the sqrt(k)/2
+// terms are below 2^-40 of 2^sigma for every sigma used, well inside the margin).
+int sigma_for(int n, int64_t k) {
+    // sqrt((P / 2)(1 - 2^-20)) - sqrt(k) / 2, in the log domain for the first term
+    const double root = std::exp2((log2_product(n) - 1.0 + std::log2(1.0 - std::ldexp(1.0, -20))) / 2.0);
+    const double lim = root - std::sqrt((double)std::max<int64_t>(k, 1)) / 2.0;
+    return (int)std::floor(std::log2(lim) - 1e-9);
 }
 
 // Limbs of W_p and P for n moduli (P < 2^(32 nw)).
@@ -123,6 +133,83 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
     for (int l = 0; l <= MAX_NW; ++l) cc.kq[l] = std::ldexp(1.0, 32 * l) / pd;
 }
 
+// ---- device: row norms ---------------------------------------------------------------------------
+// Upper bound of a row's squared 2-norm relative to its max exponent e (max |x| < 2^e):
+// q = sum_k ceil(|x| 2^(20-e))^2, each term <= 2^40 and >= (|x| 2^(20-e))^2, summed in
+// integers (order-independent, so the bound and every result derived from it are
+// deterministic); ||x||_2 <= 2^(e-20) sqrt(q).
+__device__ __forceinline__ unsigned long long sq_term(double x, int e) {
+    const unsigned long long c = (unsigned long long)ceil(oz::scale2(fabs(x), 20 - e));
+    return c * c;
+}
+
+// MN-contiguous operand (element (mn, kk) at X[mn + kk ld]): thread per mn, K in chunks
+// across blocks, integer atomic sums (q zeroed by the caller).
+__device__ __forceinline__ void qnorm_mn_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                               int kchunk, const unsigned long long* __restrict__ amax,
+                                               unsigned long long* __restrict__ q, int64_t bx, int64_t by) {
+    const int64_t mn = bx * blockDim.x + threadIdx.x;
+    if (mn >= MN) return;
+    const unsigned long long am = amax[mn];
+    const int e = oz::exponent_of_max(am);
+    if (am == 0ull || e == oz::EXP_NONFINITE) return;
+    const int64_t k0 = by * kchunk, k1 = min(K, k0 + kchunk);
+    unsigned long long acc = 0;
+    for (int64_t kk = k0; kk < k1; ++kk) acc += sq_term(X[mn + kk * ld], e);
+    if (acc) atomicAdd(q + mn, acc);
+}
+
+// K-contiguous operand (element (mn, kk) at X[kk + mn ld]): warp per mn.
+__device__ __forceinline__ void qnorm_k_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                                              const unsigned long long* __restrict__ amax,
+                                              unsigned long long* __restrict__ q, int64_t bx) {
+    const int64_t mn = bx * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (mn >= MN) return;
+    const unsigned long long am = amax[mn];
+    const int e = oz::exponent_of_max(am);
+    unsigned long long acc = 0;
+    if (am != 0ull && e != oz::EXP_NONFINITE)
+        for (int64_t kk = lane; kk < K; kk += 32) acc += sq_term(X[kk + mn * ld], e);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) q[mn] = acc;
+}
+
+__global__ void qnorm_mn_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K, int kchunk,
+                                const unsigned long long* __restrict__ amax, unsigned long long* __restrict__ q) {
+    qnorm_mn_block(X, ld, MN, K, kchunk, amax, q, blockIdx.x, blockIdx.y);
+}
+__global__ void qnorm_k_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
+                               const unsigned long long* __restrict__ amax, unsigned long long* __restrict__ q) {
+    qnorm_k_block(X, ld, MN, K, amax, q, blockIdx.x);
+}
+// Every operand of a grouped call, on the amax launch's block layout.
+__global__ void __launch_bounds__(256) qnorm_grouped(const oz::SplitJob* __restrict__ jobs, int njobs) {
+    const int64_t blk = blockIdx.x;
+    const oz::SplitJob& J = jobs[oz::find_job(jobs, njobs, blk, false)];
+    const int64_t local = blk - J.amax_begin;
+    if (J.kcontig)
+        qnorm_k_block(J.X, J.ld, J.MN, J.K, J.amax, J.qn, local);
+    else
+        qnorm_mn_block(J.X, J.ld, J.MN, J.K, oz::AMAX_KCHUNK, J.amax, J.qn, local % J.amax_bx, local / J.amax_bx);
+}
+
+// Scale of row mn: exps[mn] = sigma - s with s = min(sigma - g, 58 - e) (see sigma_for);
+// EXP_NONFINITE for a row with an infinite or NaN element.
+__device__ __forceinline__ int row_scale_exp(unsigned long long am, unsigned long long qv, int sigma, int& s) {
+    const int e = oz::exponent_of_max(am);
+    if (e == oz::EXP_NONFINITE) return e;
+    if (am == 0ull || qv == 0ull) {
+        s = 0;
+        return sigma;
+    }
+    const int h = (64 - __clzll((long long)(qv - 1ull)) + 1) >> 1;  // 2^h >= sqrt(qv)
+    const int g = e - 20 + h;
+    s = min(sigma - g, 58 - e);
+    return sigma - s;
+}
+
 // ---- device: residue planes ----------------------------------------------------------------------
 // Plane j holds (A' mod p_j) in the symmetric range as int8 at [j][mn][kk] (K-major, row
 // length k_pad, mn_pad rows, zero padded).  A thread produces RES_ELEMS consecutive kk of one
@@ -131,8 +218,9 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
 // seg == 0, by == 0 threads also write exps[mn].
 template <bool K_CONTIG>
 __device__ __forceinline__ void residue_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                                              int64_t mn_pad, int64_t k_pad, int nmod, int beta,
-                                              const unsigned long long* __restrict__ amax, int32_t* __restrict__ exps,
+                                              int64_t mn_pad, int64_t k_pad, int nmod, int sigma,
+                                              const unsigned long long* __restrict__ amax,
+                                              const unsigned long long* __restrict__ qn, int32_t* __restrict__ exps,
                                               int8_t* __restrict__ planes, const ModTable& mt, int64_t bx,
                                               int64_t by) {
     constexpr int E = RES_ELEMS;
@@ -141,9 +229,9 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
     const int64_t mn = bx * RES_ROWS + row;
     const int64_t k0 = by * RES_KSPAN + seg * E;
     if (mn >= mn_pad) return;
-    int e = 0;
+    int e = 0, sc = 0;  // sc: this row's scale exponent s
     if (mn < MN) {
-        e = oz::exponent_of_max(amax[mn]);
+        e = row_scale_exp(amax[mn], qn[mn], sigma, sc);
         if (by == 0 && seg == 0) exps[mn] = e;
     }
     const bool live = (mn < MN) && (e != oz::EXP_NONFINITE);
@@ -167,10 +255,8 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         const int64_t kk = k0 + i;
         double a = 0.0;
         if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
-        // an integer of magnitude <= 2^beta <= 2^58 (exact scaling, rounded to nearest even:
-        // half the quantisation error of truncation, and |x| <= 2^beta stays inside the
-        // operand-bit rule, which bounds k 2^(2 beta))
-        const long long x = live ? __double2ll_rn(oz::scale2(a, beta - e)) : 0ll;
+        // an integer of magnitude <= 2^58 (exact scaling, rounded to nearest even)
+        const long long x = live ? __double2ll_rn(oz::scale2(a, sc)) : 0ll;
         x0[i] = (int32_t)(x & 0xfffff);
         x1[i] = (int32_t)((x >> 20) & 0xfffff);
         x2[i] = (int32_t)(x >> 40);
@@ -203,11 +289,13 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
 
 template <bool K_CONTIG>
 __global__ void __launch_bounds__(128) split_residues(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                                                      int64_t mn_pad, int64_t k_pad, int nmod, int beta,
+                                                      int64_t mn_pad, int64_t k_pad, int nmod, int sigma,
                                                       const unsigned long long* __restrict__ amax,
+                                                      const unsigned long long* __restrict__ qn,
                                                       int32_t* __restrict__ exps, int8_t* __restrict__ planes,
                                                       const __grid_constant__ ModTable mt) {
-    residue_block<K_CONTIG>(X, ld, MN, K, mn_pad, k_pad, nmod, beta, amax, exps, planes, mt, blockIdx.x, blockIdx.y);
+    residue_block<K_CONTIG>(X, ld, MN, K, mn_pad, k_pad, nmod, sigma, amax, qn, exps, planes, mt, blockIdx.x,
+                            blockIdx.y);
 }
 
 // Every operand of a grouped call in one launch (job table as for the digit split).
@@ -218,10 +306,10 @@ __global__ void __launch_bounds__(128) split_residues_grouped(const oz::SplitJob
     const int64_t local = blk - J.split_begin;
     const int64_t bx = local % J.split_bx, by = local / J.split_bx;
     if (J.kcontig)
-        residue_block<true>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, nmod, J.bits, J.amax, J.exps,
+        residue_block<true>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, nmod, J.bits, J.amax, J.qn, J.exps,
                             (int8_t*)J.planes, mt, bx, by);
     else
-        residue_block<false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, nmod, J.bits, J.amax, J.exps,
+        residue_block<false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, nmod, J.bits, J.amax, J.qn, J.exps,
                              (int8_t*)J.planes, mt, bx, by);
 }
 
@@ -299,8 +387,8 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
         c = t >> 32;
     }
     x[NW] = (uint32_t)c;
-    // X = q P + C' with |C'| <= k 2^(2 beta) < (P / 2)(1 - 1.3e-9) by the operand-bit rule
-    // (beta_for keeps a 1e-9 margin on its logarithms), so q is the integer nearest X / P, and
+    // X = q P + C' with |C'| <= (2^sigma + sqrt(k)/2)^2 < (P / 2)(1 - 2^-20) by the norm rule
+    // (sigma_for), so q is the integer nearest X / P, and
     // the estimate from the top three limbs is within 2^-37 of X / P (X < 2^13 P; the dropped
     // limbs are below 2^-37 P): rint gives q exactly, and X - q P is C' itself.
     double xq = 0.0;
@@ -419,6 +507,11 @@ __global__ void __launch_bounds__(256) crt_grouped(const CrtJob* __restrict__ jo
                  J.alpha, J.beta, J.C, J.ldc, cc);
 }
 
+cudaError_t launch_qnorm_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks) {
+    qnorm_grouped<<<(unsigned)blocks, 256, 0, s>>>(jobs, njobs);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_split_residues_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks,
                                           int nmod, const ModTable& mt) {
     split_residues_grouped<<<(unsigned)blocks, 128, 0, s>>>(jobs, njobs, nmod, mt);
@@ -506,8 +599,7 @@ dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmo
     using namespace oz2;
     if (nmod < MIN_MODULI || nmod > MAX_MODULI)
         return fail(h, DGT_ERROR_INVALID_VALUE, "modulus count must be in [8, 20]");
-    const int bits = beta_for(nmod, k);
-    if (bits < 8) return fail(h, DGT_ERROR_UNSUPPORTED, "K too long for this modulus count");
+    const int bits = sigma_for(nmod, k);
     // kernel variant: 0 (4 epilogue warps), 4 (CTA pair) or 1 (8 warps); all 128-byte stages
     const int variant = (h->ozaki_variant == 0 || h->ozaki_variant == 4) ? h->ozaki_variant : 1;
     const bool pair = variant == 4;
@@ -532,17 +624,27 @@ dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmo
 // amax and residue planes of one operand: the MN rows of op(A) (kcontig = transa) or the MN
 // columns of op(B) (kcontig = !transb), planes padded to mn_pad rows.
 dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, const double* X, int64_t ld, int64_t MN,
-                        int64_t mn_pad, bool kcontig, unsigned long long* amax, int32_t* exps, int8_t* planes) {
+                        int64_t mn_pad, bool kcontig, unsigned long long* amax, unsigned long long* qn, int32_t* exps,
+                        int8_t* planes) {
     using namespace oz2;
     dgt_status st = ozaki_amax(h, s, X, ld, MN, sh.k, kcontig, amax);
     if (st != DGT_SUCCESS) return st;
+    if (kcontig) {
+        qnorm_k_contig<<<(unsigned)ceil_div(MN, 8), 256, 0, s>>>(X, ld, MN, sh.k, amax, qn);
+    } else {
+        DGT_CUDA_TRY(h, cudaMemsetAsync(qn, 0, (size_t)MN * 8, s));
+        dim3 g((unsigned)ceil_div(MN, 256), (unsigned)ceil_div(sh.k, oz::AMAX_KCHUNK));
+        qnorm_mn_contig<<<g, 256, 0, s>>>(X, ld, MN, sh.k, oz::AMAX_KCHUNK, amax, qn);
+    }
+    h->launches.fetch_add(1);
+    DGT_CUDA_TRY(h, cudaGetLastError());
     dim3 grid((unsigned)ceil_div(mn_pad, RES_ROWS), (unsigned)(sh.k_pad / RES_KSPAN));
     if (kcontig)
-        split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sh.bits, amax, exps,
-                                                  planes, sh.mt);
+        split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sh.bits, amax, qn,
+                                                  exps, planes, sh.mt);
     else
-        split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sh.bits, amax, exps,
-                                                   planes, sh.mt);
+        split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sh.bits, amax, qn,
+                                                   exps, planes, sh.mt);
     h->launches.fetch_add(1);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DGT_SUCCESS : cuda_fail(h, e, "residue split");
@@ -624,16 +726,20 @@ Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws) {
     const size_t xa = up((size_t)sh.m * 8), xb = up((size_t)n * 8), ea = up((size_t)sh.m * 4), eb = up((size_t)n * 4);
     const size_t rs = up((size_t)sh.nmod * sh.m_pad * n_pad);
     Oz2Work w;
-    w.bytes = pa + pb + xa + xb + ea + eb + rs;
+    w.bytes = pa + pb + 2 * (xa + xb) + ea + eb + rs;
     char* p = (char*)ws;
     if (!p) return w;
     w.planesA = (int8_t*)p;
     w.planesB = (int8_t*)(p + pa);
-    w.amaxA = (unsigned long long*)(p + pa + pb);
-    w.amaxB = (unsigned long long*)(p + pa + pb + xa);
-    w.expA = (int32_t*)(p + pa + pb + xa + xb);
-    w.expB = (int32_t*)(p + pa + pb + xa + xb + ea);
-    w.res = (uint8_t*)(p + pa + pb + xa + xb + ea + eb);
+    p += pa + pb;
+    w.amaxA = (unsigned long long*)p;
+    w.amaxB = (unsigned long long*)(p + xa);
+    w.qnA = (unsigned long long*)(p + xa + xb);
+    w.qnB = (unsigned long long*)(p + 2 * xa + xb);
+    p += 2 * (xa + xb);
+    w.expA = (int32_t*)p;
+    w.expB = (int32_t*)(p + ea);
+    w.res = (uint8_t*)(p + ea + eb);
     return w;
 }
 
@@ -649,8 +755,10 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     cudaStream_t s = h->stream;
     mark(h, 0);
     // op(A) is m x k: 'N' -> MN-contiguous; op(B) as its transpose n x k: 'N' -> K-contiguous
-    if ((st = ozaki2_split(h, s, sh, A, lda, m, sh.m_pad, ta, w.amaxA, w.expA, w.planesA)) != DGT_SUCCESS) return st;
-    if ((st = ozaki2_split(h, s, sh, B, ldb, n, sh.n_pad, !tb, w.amaxB, w.expB, w.planesB)) != DGT_SUCCESS) return st;
+    if ((st = ozaki2_split(h, s, sh, A, lda, m, sh.m_pad, ta, w.amaxA, w.qnA, w.expA, w.planesA)) != DGT_SUCCESS)
+        return st;
+    if ((st = ozaki2_split(h, s, sh, B, ldb, n, sh.n_pad, !tb, w.amaxB, w.qnB, w.expB, w.planesB)) != DGT_SUCCESS)
+        return st;
     return ozaki2_gemm_crt(h, s, sh, n, sh.n_pad, w.planesA, w.expA, w.planesB, w.expB, w.res, alpha, beta, C, ldc);
 }
 

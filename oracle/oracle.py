@@ -416,16 +416,36 @@ OZAKI2_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                  223, 217, 211, 199, 197, 193, 191, 181, 179, 173)
 
 
-def ozaki2_beta(nmod: int, k: int) -> int:
-    """Operand bits for nmod moduli and inner dimension k: the largest beta (capped at 58)
-    with 2 k 2^(2 beta) < P, chosen from logarithms with a 1e-9 margin."""
+def ozaki2_sigma(nmod: int, k: int) -> int:
+    """Norm-bound exponent for nmod moduli and inner dimension k: the largest sigma with
+    (2^sigma + sqrt(k)/2)^2 < (P/2)(1 - 2^-20), computed as the kernels' host code does
+    (csrc/ozaki2.cu sigma_for)."""
     import math
 
     lg = 0.0
     for p in OZAKI2_MODULI[:nmod]:
         lg += math.log2(float(p))
-    b = (lg - 1.0 - math.log2(float(max(k, 1)))) / 2.0 - 1e-9
-    return min(58, math.floor(b))
+    root = 2.0 ** ((lg - 1.0 + math.log2(1.0 - 2.0 ** -20)) / 2.0)
+    lim = root - math.sqrt(float(max(k, 1))) / 2.0
+    return math.floor(math.log2(lim) - 1e-9)
+
+
+def _row_scale(v, sigma: int):
+    """Scale exponent s of one row (or column) v: s = min(sigma - g, 58 - e), e the exponent of
+    max |v| and 2^g >= the integer bound of ||v||_2, q = sum ceil(|v| 2^(20-e))^2
+    (csrc/ozaki2.cu qnorm_* and row_scale_exp).  None for a row with inf or NaN."""
+    import math
+
+    vals = [abs(float(x)) for x in v]
+    if any(not math.isfinite(x) for x in vals):
+        return None
+    mx = max(vals) if vals else 0.0
+    if mx == 0.0:
+        return 0
+    e = math.frexp(mx)[1]
+    q = sum(math.ceil(math.ldexp(x, 20 - e)) ** 2 for x in vals)
+    h = ((q - 1).bit_length() + 1) // 2
+    return min(sigma - (e - 20 + h), 58 - e)
 
 
 def _exp_of_max(v: float) -> int:
@@ -436,29 +456,29 @@ def _exp_of_max(v: float) -> int:
 
 
 def ozaki2_exact(A, B, nmod: int, ta: str = "N", tb: str = "N"):
-    """C = op(A) op(B) as the CRT emulation computes it: operands scaled per row of op(A) /
-    column of op(B) to integers of at most beta bits (rounded to nearest even), their integer
-    product taken exactly,
-    rounded once to FP64 and scaled back.  Pure Python integers: small sizes only."""
+    """C = op(A) op(B) as the CRT emulation computes it: each row of op(A) / column of op(B)
+    scaled by 2^s (its 2-norm bound, capped so no entry exceeds 2^58) and rounded to
+    integers (nearest even), their integer product taken exactly, rounded once to FP64 and
+    scaled back by 2^-(s_i + t_j).  Pure Python integers: small sizes only."""
     import math
 
     Aop, Bop = op(A, ta), op(B, tb)
     m, k = Aop.shape
     n = Bop.shape[1]
-    beta = ozaki2_beta(nmod, k)
+    sigma = ozaki2_sigma(nmod, k)
     P = 1
     for p in OZAKI2_MODULI[:nmod]:
         P *= p
-    assert 2 * k * 2 ** (2 * beta) < P  # the CRT range covers every product (|A'|, |B'| <= 2^beta)
-    ea = [_exp_of_max(float(np.max(np.abs(Aop[i, :])))) if k else 0 for i in range(m)]
-    fb = [_exp_of_max(float(np.max(np.abs(Bop[:, j])))) if k else 0 for j in range(n)]
-    Ai = [[int(round(math.ldexp(float(Aop[i, t]), beta - ea[i]))) for t in range(k)] for i in range(m)]
-    Bi = [[int(round(math.ldexp(float(Bop[t, j]), beta - fb[j]))) for t in range(k)] for j in range(n)]
+    sa = [_row_scale(Aop[i, :], sigma) for i in range(m)]
+    sb = [_row_scale(Bop[:, j], sigma) for j in range(n)]
+    Ai = [[int(round(math.ldexp(float(Aop[i, t]), sa[i]))) for t in range(k)] for i in range(m)]
+    Bi = [[int(round(math.ldexp(float(Bop[t, j]), sb[j]))) for t in range(k)] for j in range(n)]
     C = np.empty((m, n))
     for i in range(m):
         for j in range(n):
             exact = sum(a * b for a, b in zip(Ai[i], Bi[j]))
-            C[i, j] = math.ldexp(float(exact), ea[i] + fb[j] - 2 * beta)
+            assert 2 * abs(exact) < P  # the CRT range covers every product (Cauchy-Schwarz bound)
+            C[i, j] = math.ldexp(float(exact), -(sa[i] + sb[j]))
     return C
 
 
@@ -470,15 +490,16 @@ def ozaki2_residue_check(A, B, nmod: int):
 
     m, k = A.shape
     n = B.shape[1]
-    beta = ozaki2_beta(nmod, k)
+    sigma = ozaki2_sigma(nmod, k)
     mods = OZAKI2_MODULI[:nmod]
     P = math.prod(mods)
-    ea = [_exp_of_max(float(np.max(np.abs(A[i, :])))) for i in range(m)]
-    fb = [_exp_of_max(float(np.max(np.abs(B[:, j])))) for j in range(n)]
-    Ai = np.array([[int(round(math.ldexp(float(A[i, t]), beta - ea[i]))) for t in range(k)]
+    sa = [_row_scale(A[i, :], sigma) for i in range(m)]
+    sb = [_row_scale(B[:, j], sigma) for j in range(n)]
+    Ai = np.array([[int(round(math.ldexp(float(A[i, t]), sa[i]))) for t in range(k)]
                    for i in range(m)], dtype=object)
-    Bi = np.array([[int(round(math.ldexp(float(B[t, j]), beta - fb[j]))) for j in range(n)]
+    Bi = np.array([[int(round(math.ldexp(float(B[t, j]), sb[j]))) for j in range(n)]
                    for t in range(k)], dtype=object)
+    assert all(abs(x) <= 2 ** 58 for x in Ai.flat) and all(abs(x) <= 2 ** 58 for x in Bi.flat)
 
     def sym(x, p):
         r = x % p

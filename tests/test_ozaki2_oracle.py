@@ -15,29 +15,73 @@ def test_crt_identity_recovers_the_integer_product(nmod, k):
     assert (X == exact).all()
 
 
-def test_operand_bits_rule():
+def test_norm_rule():
+    """sigma: (2^sigma + sqrt(k)/2)^2 < (P/2)(1 - 2^-20), and sigma + 1 breaks it (checked in
+    integers with sqrt(k) bounded by isqrt)."""
     for nmod in range(8, 21):
         P = math.prod(O.OZAKI2_MODULI[:nmod])
         for k in (1, 7, 256, 4096, 16384, 65536):
-            b = O.ozaki2_beta(nmod, k)
-            if b < 1:
-                continue
-            assert 2 * k * 2 ** (2 * b) < P  # operands are rounded to nearest: |A'|, |B'| <= 2^beta
-            assert b == 58 or 2 * k * (2 ** (b + 1) - 1) ** 2 >= P // 2  # within a bit of the largest
-    assert O.ozaki2_beta(17, 16384) == 58 and O.ozaki2_beta(16, 16384) == 55
+            sg = O.ozaki2_sigma(nmod, k)
+            r = math.isqrt(k) + 1  # > sqrt(k)
+            lhs = (2 ** (sg + 1) + r) ** 2  # 4 (2^sigma + sqrt(k)/2)^2 < lhs
+            assert lhs * 2 ** 20 < 2 * P * (2 ** 20 - 1)
+            r0 = math.isqrt(k)  # <= sqrt(k)
+            assert (2 ** (sg + 2) + r0) ** 2 * 2 ** 20 >= 2 * P * (2 ** 20 - 1)  # sigma + 1 fails
     assert all(math.gcd(p, q) == 1 for i, p in enumerate(O.OZAKI2_MODULI) for q in O.OZAKI2_MODULI[:i])
 
 
-def test_rounded_operands_reach_the_bound():
-    """A row whose max rounds up gives |A'| = 2^beta exactly; the CRT identity still holds."""
+def test_row_scale_caps_entries():
+    """A row with one large entry among small ones: the norm bound is the max itself, so the
+    58-bit entry cap decides; a dense row of equal entries is scaled by its norm."""
     k = 64
-    A = np.full((3, k), 1.0 - 2.0 ** -60)  # just below 2^0: scaled to 2^beta - 2^(beta-60), rounds to 2^beta
+    single = np.zeros(k)
+    single[5] = 0.75
+    s1 = O._row_scale(single, O.ozaki2_sigma(20, k))
+    assert abs(int(round(math.ldexp(0.75, s1)))) <= 2 ** 58 and s1 == 58  # e = 0: cap 58 - e
+    dense = np.full(k, 0.75)
+    sg = O.ozaki2_sigma(12, k)
+    s2 = O._row_scale(dense, sg)
+    norm = math.sqrt(sum(math.ldexp(0.75, s2) ** 2 for _ in range(k)))
+    assert norm <= 2 ** sg < 2 * norm * 2  # within a factor 2 of the bound (power-of-two scales)
+
+
+def _exact_max_scaled(A, B, nmod):
+    """The same integer emulation with every row / column scaled by its max instead (the
+    bound k 2^(2 beta) < P/2): the reference point the norm scaling improves on."""
+    m, k = A.shape
+    n = B.shape[1]
+    lg = sum(math.log2(p) for p in O.OZAKI2_MODULI[:nmod])
+    beta = min(58, math.floor((lg - 1 - math.log2(k)) / 2 - 1e-9))
+    ea = [math.frexp(float(np.max(np.abs(A[i]))))[1] for i in range(m)]
+    fb = [math.frexp(float(np.max(np.abs(B[:, j]))))[1] for j in range(n)]
+    Ai = [[int(round(math.ldexp(float(A[i, t]), beta - ea[i]))) for t in range(k)] for i in range(m)]
+    Bi = [[int(round(math.ldexp(float(B[t, j]), beta - fb[j]))) for t in range(k)] for j in range(n)]
+    C = np.empty((m, n))
+    for i in range(m):
+        for j in range(n):
+            C[i, j] = math.ldexp(float(sum(x * y for x, y in zip(Ai[i], Bi[j]))), ea[i] + fb[j] - 2 * beta)
+    return C
+
+
+@pytest.mark.parametrize("phi", [0.5, 2.0])
+def test_norm_scaling_beats_max_scaling(phi):
+    """Entries (U - 0.5) exp(phi N(0,1)): a row's 2-norm is far below sqrt(k) times its max, so
+    scaling by the norm keeps more bits: at 12 moduli both errors are several times smaller."""
+    A, B = O.ozaki_matrix((20, 400), 21, phi), O.ozaki_matrix((400, 16), 22, phi)
+    want = O.dgemm(A, B)
+    norm = O.rel_errors(O.ozaki2_exact(A, B, 12), want)
+    mx = O.rel_errors(_exact_max_scaled(A, B, 12), want)
+    assert norm[1] < mx[1] / 3 and norm[0] < mx[0]
+
+
+def test_rows_at_the_norm_bound():
+    """Dense rows whose scaled entries round up: the CRT identity still holds."""
+    k = 64
+    A = np.full((3, k), 1.0 - 2.0 ** -60)
     A[1] *= -1.0
     B = O.uniform((k, 4), 9)
     X, exact = O.ozaki2_residue_check(A, B, 12)
     assert (X == exact).all()
-    beta = O.ozaki2_beta(12, k)
-    assert abs(int(round(math.ldexp(A[0, 0], beta - 0)))) == 2 ** beta
 
 
 def test_exact_restatement_accuracy():
