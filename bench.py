@@ -510,7 +510,8 @@ def workload_batching(args):
         want = A[rows, :] @ B
         cannon = {}
         for name, mode, S in (("native", dgt.FP64_NATIVE, 7), ("int8_s7", dgt.FP64_OZAKI_INT8, 7),
-                              ("int8_s8", dgt.FP64_OZAKI_INT8, 8), ("crt_n16", dgt.FP64_OZAKI2_INT8, 16)):
+                              ("int8_s8", dgt.FP64_OZAKI_INT8, 8), ("crt_n14", dgt.FP64_OZAKI2_INT8, 14),
+                              ("crt_n15", dgt.FP64_OZAKI2_INT8, 15), ("crt_n16", dgt.FP64_OZAKI2_INT8, 16)):
             f = lambda: h.cannon25d(M, p, c, 1.0, [x.data_ptr() for x in tA], [x.data_ptr() for x in tB], 0.0,
                                     [x.data_ptr() for x in tC], mode=mode, slices=S)
             f()
@@ -551,7 +552,8 @@ def workload_batching(args):
                 checks.append((i, rr, Ai[rr, :] @ Bi))
         grouped = {}
         for name, mode, S in (("native", dgt.FP64_NATIVE, 7), ("int8_s7", dgt.FP64_OZAKI_INT8, 7),
-                              ("int8_s8", dgt.FP64_OZAKI_INT8, 8), ("crt_n16", dgt.FP64_OZAKI2_INT8, 16)):
+                              ("int8_s8", dgt.FP64_OZAKI_INT8, 8), ("crt_n14", dgt.FP64_OZAKI2_INT8, 14),
+                              ("crt_n15", dgt.FP64_OZAKI2_INT8, 15), ("crt_n16", dgt.FP64_OZAKI2_INT8, 16)):
             f = lambda: h.dgemm_grouped(descs, mode=mode, slices=S)
             # kernel variant: the fastest of the library's variants for this batch
             knob = dgt.TUNE_DMMA_VARIANT if mode == dgt.FP64_NATIVE else dgt.TUNE_OZAKI_VARIANT

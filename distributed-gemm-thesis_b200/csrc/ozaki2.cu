@@ -135,16 +135,31 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
 
 // ---- device: row norms ---------------------------------------------------------------------------
 // Upper bound of a row's squared 2-norm relative to its max exponent e (max |x| < 2^e):
-// q = sum_k ceil(|x| 2^(20-e))^2, each term <= 2^40 and >= (|x| 2^(20-e))^2, summed in
-// integers (order-independent, so the bound and every result derived from it are
-// deterministic); ||x||_2 <= 2^(e-20) sqrt(q).
-__device__ __forceinline__ unsigned long long sq_term(double x, int e) {
-    const unsigned long long c = (unsigned long long)ceil(oz::scale2(fabs(x), 20 - e));
-    return c * c;
+// q = sum_k ceil(|x| 2^(20-e))^2, each term an integer <= 2^40 and >= (|x| 2^(20-e))^2.
+// Terms are added in FP64 in runs of at most 4096 (partial sums below 2^52: exact), each run
+// converted to an integer and summed in integers, so the bound and every result derived from
+// it are deterministic; ||x||_2 <= 2^(e-20) sqrt(q).  2^(20-e) is one double for e >= -1002
+// (the general scaling otherwise); a product that lands below the normal range only rounds
+// terms of size < 2^-2000, far inside the reconstruction's 2^-20 margin.
+struct QScale {
+    double f;
+    int sh;
+    bool direct;
+};
+__device__ __forceinline__ QScale qscale(int e) {
+    QScale q;
+    q.sh = 20 - e;
+    q.direct = q.sh <= 1023;
+    q.f = q.direct ? oz::pow2i(max(q.sh, -1022)) : 0.0;
+    return q;
+}
+__device__ __forceinline__ double sq_term(double x, const QScale& q) {
+    const double c = ceil(q.direct ? fabs(x) * q.f : oz::scale2(fabs(x), q.sh));
+    return c * c;  // exact: c <= 2^20
 }
 
-// MN-contiguous operand (element (mn, kk) at X[mn + kk ld]): thread per mn, K in chunks
-// across blocks, integer atomic sums (q zeroed by the caller).
+// MN-contiguous operand (element (mn, kk) at X[mn + kk ld]): thread per mn, K in chunks of
+// at most 64 across blocks, integer atomic sums (q zeroed by the caller).
 __device__ __forceinline__ void qnorm_mn_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
                                                int kchunk, const unsigned long long* __restrict__ amax,
                                                unsigned long long* __restrict__ q, int64_t bx, int64_t by) {
@@ -153,13 +168,15 @@ __device__ __forceinline__ void qnorm_mn_block(const double* __restrict__ X, int
     const unsigned long long am = amax[mn];
     const int e = oz::exponent_of_max(am);
     if (am == 0ull || e == oz::EXP_NONFINITE) return;
+    const QScale qs = qscale(e);
     const int64_t k0 = by * kchunk, k1 = min(K, k0 + kchunk);
-    unsigned long long acc = 0;
-    for (int64_t kk = k0; kk < k1; ++kk) acc += sq_term(X[mn + kk * ld], e);
-    if (acc) atomicAdd(q + mn, acc);
+    double acc = 0.0;
+    for (int64_t kk = k0; kk < k1; ++kk) acc += sq_term(X[mn + kk * ld], qs);
+    if (acc != 0.0) atomicAdd(q + mn, (unsigned long long)acc);
 }
 
-// K-contiguous operand (element (mn, kk) at X[kk + mn ld]): warp per mn.
+// K-contiguous operand (element (mn, kk) at X[kk + mn ld]): warp per mn; each lane's run is
+// at most ceil(K / 32) <= 4096 terms.
 __device__ __forceinline__ void qnorm_k_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
                                               const unsigned long long* __restrict__ amax,
                                               unsigned long long* __restrict__ q, int64_t bx) {
@@ -168,12 +185,16 @@ __device__ __forceinline__ void qnorm_k_block(const double* __restrict__ X, int6
     if (mn >= MN) return;
     const unsigned long long am = amax[mn];
     const int e = oz::exponent_of_max(am);
-    unsigned long long acc = 0;
-    if (am != 0ull && e != oz::EXP_NONFINITE)
-        for (int64_t kk = lane; kk < K; kk += 32) acc += sq_term(X[kk + mn * ld], e);
+    double acc = 0.0;
+    if (am != 0ull && e != oz::EXP_NONFINITE) {
+        const QScale qs = qscale(e);
+        const double* row = X + mn * ld;
+        for (int64_t kk = lane; kk < K; kk += 32) acc += sq_term(row[kk], qs);
+    }
+    unsigned long long t = (unsigned long long)acc;
 #pragma unroll
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) q[mn] = acc;
+    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) q[mn] = t;
 }
 
 __global__ void qnorm_mn_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K, int kchunk,
