@@ -256,6 +256,10 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         if (by == 0 && seg == 0) exps[mn] = e;
     }
     const bool live = (mn < MN) && (e != oz::EXP_NONFINITE);
+    // 2^sc as one double when it is one (the product is then exact, or below 2^-1022 where
+    // it rounds to the integer 0 either way); the general scaling otherwise
+    const bool direct = sc >= -1022 && sc <= 1023;
+    const double fsc = direct ? oz::pow2i(sc) : 0.0;
     const int64_t plane = mn_pad * k_pad;
     int8_t* out = planes + mn * k_pad + k0;
     if (!live || k0 >= K) {  // padding (or a non-finite row): zero residues, no arithmetic
@@ -277,7 +281,7 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         double a = 0.0;
         if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
         // an integer of magnitude <= 2^58 (exact scaling, rounded to nearest even)
-        const long long x = live ? __double2ll_rn(oz::scale2(a, sc)) : 0ll;
+        const long long x = live ? __double2ll_rn(direct ? a * fsc : oz::scale2(a, sc)) : 0ll;
         x0[i] = (int32_t)(x & 0xfffff);
         x1[i] = (int32_t)((x >> 20) & 0xfffff);
         x2[i] = (int32_t)(x >> 40);
