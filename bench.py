@@ -593,11 +593,11 @@ def workload_batching(args):
 
 
 def workload_once(args):
-    """Two calls of one path at --size (the first warms up), for profiler captures: native
+    """Four calls of one path at --size (three warm up), for profiler captures: native
     DGEMM, Ozaki INT8 DGEMM (--slices = slices), CRT INT8 DGEMM (--slices = moduli), 3xBF16
     SGEMM, a 4x4 block-cyclic pack with 256 blocks, or (grouped2) one grouped CRT call over
     --size products with M, N, K log-uniform in [128, 4096] (the law of the 256-product
-    batching workload).  Prints the second call's time."""
+    batching workload).  Prints the last call's time."""
     import numpy as np
 
     torch, dgt, h = _setup()
@@ -642,7 +642,8 @@ def workload_once(args):
         f = lambda: h.dgemm("N", "N", n, n, n, 1.0, A.data_ptr(), n, B.data_ptr(), n, 0.0, C.data_ptr(), n,
                             mode=mode, slices=args.slices)
         flops = 2.0 * n ** 3
-    f()
+    for _ in range(3):  # warm-up: allocation, first launches, clock ramp
+        f()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
