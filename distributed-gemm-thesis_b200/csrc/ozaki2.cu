@@ -546,7 +546,11 @@ cudaError_t launch_split_residues_grouped(cudaStream_t s, const oz::SplitJob* jo
 cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, int64_t threads, const CrtConst& cc,
                                int nmod) {
     const unsigned blocks = (unsigned)((threads + 255) / 256);
-    if (nmod == 16)
+    if (nmod == 14)
+        crt_grouped<4, 14><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
+    else if (nmod == 15)
+        crt_grouped<4, 15><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
+    else if (nmod == 16)
         crt_grouped<4, 16><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
     else if (nmod == 17)
         crt_grouped<5, 17><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
@@ -724,7 +728,11 @@ dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, i
 #define DGT_CRT_LAUNCH(NW, NM)                                                                            \
     crt_reconstruct<NW, NM><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta, \
                                                    C, ldc, cc)
-    if (nmod == 16)
+    if (nmod == 14)
+        DGT_CRT_LAUNCH(4, 14);
+    else if (nmod == 15)
+        DGT_CRT_LAUNCH(4, 15);
+    else if (nmod == 16)
         DGT_CRT_LAUNCH(4, 16);
     else if (nmod == 17)
         DGT_CRT_LAUNCH(5, 17);

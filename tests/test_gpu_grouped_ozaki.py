@@ -130,7 +130,8 @@ def test_grouped_ragged_batch_against_oracle():
         assert O.rel_errors(host(k[2], (it["m"], it["n"])), _want(it))[1] <= FRO_TOL
 
 
-def test_grouped_crt_matches_per_product_bitwise():
+@pytest.mark.parametrize("nmod", [14, 16])
+def test_grouped_crt_matches_per_product_bitwise(nmod):
     """The CRT scheme in one grouped pass (amax, norm bounds, residue split, residue GEMM, reconstruction)
     equals one CRT call per product bit for bit: same operand bits per product, same residues,
     same exact reconstruction."""
@@ -140,7 +141,7 @@ def test_grouped_crt_matches_per_product_bitwise():
     with dgt.Handle() as h:
         descs, keep = _descs(items)
         n0 = h.launch_count()
-        h.dgemm_grouped(descs, mode=dgt.FP64_OZAKI2_INT8, slices=16)
+        h.dgemm_grouped(descs, mode=dgt.FP64_OZAKI2_INT8, slices=nmod)
         torch.cuda.synchronize()
         h.check_device()
         assert h.launch_count() - n0 == 5  # amax, norm bounds, residue split, GEMM, reconstruction
@@ -148,7 +149,7 @@ def test_grouped_crt_matches_per_product_bitwise():
         for idx, (it, d) in enumerate(zip(items, descs)):
             dC = dev(it["C"])
             h.dgemm(it["ta"], it["tb"], it["m"], it["n"], it["k"], it["alpha"], d["A"], d["lda"], d["B"], d["ldb"],
-                    it["beta"], ptr(dC), it["m"], mode=dgt.FP64_OZAKI2_INT8, slices=16)
+                    it["beta"], ptr(dC), it["m"], mode=dgt.FP64_OZAKI2_INT8, slices=nmod)
             torch.cuda.synchronize()
             assert np.array_equal(host(dC, (it["m"], it["n"])), grouped[idx]), (it["m"], it["n"], it["k"])
     for it, got in zip(items, grouped):

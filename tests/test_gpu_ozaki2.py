@@ -46,6 +46,16 @@ def test_bitwise_equal_to_exact_restatement(h, ta, tb, shape):
     assert np.array_equal(got, O.ozaki2_exact(A, B, 17, ta, tb))
 
 
+@pytest.mark.parametrize("nmod", [8, 12, 14, 15, 16, 20])
+def test_bitwise_for_every_kernel_specialisation(h, nmod):
+    """The reconstruction has limb-count / modulus-count specialisations (14 to 17 unpredicated,
+    the rest generic): each equals the exact restatement bit for bit."""
+    m, n, k = 97, 60, 300
+    A, B, C = operands("N", "N", m, n, k, 50 + nmod, phi=1.0)
+    got = run(h, "N", "N", m, n, k, 1.0, 0.0, nmod, A, B, C)
+    assert np.array_equal(got, O.ozaki2_exact(A, B, nmod))
+
+
 @pytest.mark.parametrize("shape", [(300, 200, 1000), (513, 257, 4100)])
 def test_alpha_beta_against_fp64(h, shape):
     m, n, k = shape
