@@ -26,7 +26,7 @@ struct SplitJob {
     int32_t split_bx;     // split blocks along mn (times k_pad / 32 along K)
     int64_t amax_begin;   // first block of this job in the amax launch
     int64_t split_begin;  // first block of this job in the split launch
-    int32_t bits;         // CRT scheme: sigma (row / column 2-norm bound 2^sigma) of this product
+    int32_t bits;         // CRT scheme: sigma of this operand (scaled rows / columns have 2-norm <= 2^sigma)
     int32_t unused;
     unsigned long long* qn;  // CRT scheme: integer 2-norm bounds per row (see qnorm_*)
 };
@@ -93,12 +93,12 @@ struct CrtJob {
     double alpha, beta;
     double* C;
     int64_t ldc;
-    int32_t bits, unused;
+    int32_t bits, unused;  // bits: sigma_A + sigma_B (the reconstruction's shift is e + f - bits)
     int64_t thread_begin;
 };
 
 // host helpers (ozaki2.cu)
-int sigma_for(int nmod, int64_t k);  // 2-norm bound exponent of the scaled rows / columns
+int sigma_sum_for(int nmod, int64_t k);  // sigma_A + sigma_B (2-norm bound exponents of rows / columns)
 int limbs_for(int nmod);             // 32-bit limbs of P
 void crt_constants(int nmod, CrtConst& cc, ModTable& mt);
 cudaError_t launch_qnorm_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks);
@@ -113,7 +113,7 @@ cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, in
 // carve (bytes only when ws is null), one operand's amax + residue split, and the residue
 // GEMM + reconstruction of one op(B) panel.
 struct Oz2Shape {
-    int nmod, bits, variant;
+    int nmod, sa, sb, variant;  // sa, sb: sigma of op(A) rows and op(B) columns
     bool pair;
     int64_t m, k, m_pad, n_pad, k_pad;
     oz2::CrtConst cc;
@@ -134,9 +134,9 @@ struct Oz2Work {
 dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmod, Oz2Shape& sh);
 Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws);
 int64_t ozaki2_n_pad(int64_t n);  // op(B) columns padded to the GEMM's tile width
-dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, const double* X, int64_t ld, int64_t MN,
-                        int64_t mn_pad, bool kcontig, unsigned long long* amax, unsigned long long* qn, int32_t* exps,
-                        int8_t* planes);
+dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int sigma, const double* X, int64_t ld,
+                        int64_t MN, int64_t mn_pad, bool kcontig, unsigned long long* amax, unsigned long long* qn,
+                        int32_t* exps, int8_t* planes);
 dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
                            const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
                            uint8_t* res, double alpha, double beta, double* C, int64_t ldc);

@@ -133,7 +133,7 @@ extern "C" dgt_status dgt_dgemm_host(dgt_handle_t h, char transa, char transb, i
 
     if ((st = copy_in(0)) != DGT_SUCCESS) return st;
     DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[EV_A], 0));
-    if (crt && (st = ozaki2_split(h, s, sh, dA, rowsA, m, sh.m_pad, ta, w.amaxA, w.qnA, w.expA, w.planesA)) != DGT_SUCCESS)
+    if (crt && (st = ozaki2_split(h, s, sh, sh.sa, dA, rowsA, m, sh.m_pad, ta, w.amaxA, w.qnA, w.expA, w.planesA)) != DGT_SUCCESS)
         return st;
     for (int64_t j = 0; j < panels; ++j) {
         const int buf = (int)(j & 1);
@@ -143,7 +143,7 @@ extern "C" dgt_status dgt_dgemm_host(dgt_handle_t h, char transa, char transb, i
         if (j >= 2 && !read_c) DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[EV_OUT0 + buf], 0));
         if (crt) {
             const int64_t wpad = ozaki2_n_pad(wj);
-            if ((st = ozaki2_split(h, s, sh, dB[buf], ldb_d, wj, wpad, !tb, w.amaxB, w.qnB, w.expB, w.planesB)) != DGT_SUCCESS)
+            if ((st = ozaki2_split(h, s, sh, sh.sb, dB[buf], ldb_d, wj, wpad, !tb, w.amaxB, w.qnB, w.expB, w.planesB)) != DGT_SUCCESS)
                 return st;
             DGT_CUDA_TRY(h, cudaEventRecord(ev[EV_BFREE0 + buf], s));
             if ((st = ozaki2_gemm_crt(h, s, sh, wj, wpad, w.planesA, w.expA, w.planesB, w.expB, w.res, a, b, dC[buf],

@@ -515,7 +515,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
         o.m_pad = ceil_div(p.m, oz::TM) * oz::TM;
         o.n_pad = ceil_div(p.n, oz::TN) * oz::TN;
         o.k_pad = ceil_div(p.k, oz::KPAD) * oz::KPAD;
-        o.bits = crt ? oz2::sigma_for(S, p.k) : 0;
+        o.bits = crt ? oz2::sigma_sum_for(S, p.k) : 0;  // sigma_A + sigma_B
         if ((int64_t)S * std::max(o.m_pad, o.n_pad) > INT32_MAX) return DGT_ERROR_UNSUPPORTED;
         o.pa = planes;
         planes += up((size_t)S * o.m_pad * o.k_pad, 1024);
@@ -600,7 +600,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
             c.beta = p.beta;
             c.C = p.C;
             c.ldc = p.ldc;
-            c.bits = o.bits;
+            c.bits = o.bits;  // the reconstruction's shift takes the sum
             c.thread_begin = crt_threads;
             crt_threads += ceil_div(p.m, 4) * p.n;
         }
@@ -629,7 +629,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
             J.split_bx = (int32_t)ceil_div(pad[t], crt ? oz2::RES_ROWS : 128);
             J.amax_begin = amax_blocks;
             J.split_begin = split_blocks;
-            J.bits = o.bits;
+            J.bits = t == 0 ? (o.bits + 1) / 2 : o.bits / 2;  // op(A) takes the odd bit
             amax_blocks += (int64_t)J.amax_bx * J.amax_by;
             split_blocks += (int64_t)J.split_bx * (o.k_pad / (crt ? oz2::RES_KSPAN : 32));
         }

@@ -6,7 +6,8 @@
 //      2^e_i and 2^g_i bounds the row's 2-norm; A'_ik = rn(a_ik 2^s_i) (rounded to nearest
 //      even) is an integer of magnitude at most 2^58 and the row's 2-norm is at most
 //      2^sigma + sqrt(k)/2; columns of op(B) likewise.  By Cauchy-Schwarz every |(A'B')_ij|
-//      is below (P/2)(1 - 2^-20) for sigma from sigma_for.  Scaling by the norm instead of
+//      is below (P/2)(1 - 2^-20) for sigma_A + sigma_B from sigma_sum_for (op(A) takes the
+//      odd bit when the sum is odd).  Scaling by the norm instead of
 //      the max spends the integer range where the row's mass is: rows with a few large
 //      entries among many small ones keep more bits.
 //   2. Residues: for N pairwise coprime moduli p <= 256 (P = prod p),
@@ -97,11 +98,18 @@ static double log2_product(int n) {
 // by Cauchy-Schwarz |C'_ij| <= (2^sigma + sqrt(k)/2)^2.  sigma is the largest integer keeping
 // that below (P/2)(1 - 2^-20), which the reconstruction's exact quotient needs (the sqrt(k)/2
 // terms are below 2^-40 of 2^sigma for every sigma used, well inside the margin).
-int sigma_for(int n, int64_t k) {
-    // sqrt((P / 2)(1 - 2^-20)) - sqrt(k) / 2, in the log domain for the first term
-    const double root = std::exp2((log2_product(n) - 1.0 + std::log2(1.0 - std::ldexp(1.0, -20))) / 2.0);
-    const double lim = root - std::sqrt((double)std::max<int64_t>(k, 1)) / 2.0;
-    return (int)std::floor(std::log2(lim) - 1e-9);
+int sigma_sum_for(int n, int64_t k) {
+    // the largest s with (2^ceil(s/2) + r)(2^floor(s/2) + r) < (P / 2)(1 - 2^-20), r = sqrt(k) / 2,
+    // checked in the log domain with a 1e-9 margin (op(A) takes ceil(s/2), op(B) floor(s/2))
+    const double t = log2_product(n) - 1.0 + std::log2(1.0 - std::ldexp(1.0, -20));
+    const double r = std::sqrt((double)std::max<int64_t>(k, 1)) / 2.0;
+    int s = (int)std::floor(t);
+    while (s > 0) {
+        const double a = std::ldexp(1.0, (s + 1) / 2), b = std::ldexp(1.0, s / 2);
+        if (std::log2((a + r) * (b + r)) < t - 1e-9) break;
+        --s;
+    }
+    return s;
 }
 
 // Limbs of W_p and P for n moduli (P < 2^(32 nw)).
@@ -216,7 +224,8 @@ __global__ void __launch_bounds__(256) qnorm_grouped(const oz::SplitJob* __restr
         qnorm_mn_block(J.X, J.ld, J.MN, J.K, oz::AMAX_KCHUNK, J.amax, J.qn, local % J.amax_bx, local / J.amax_bx);
 }
 
-// Scale of row mn: exps[mn] = sigma - s with s = min(sigma - g, 58 - e) (see sigma_for);
+// Scale of row mn: exps[mn] = sigma - s with s = min(sigma - g, 58 - e) (sigma = sigma_A for
+// rows of op(A), sigma_B for columns of op(B); see sigma_sum_for);
 // EXP_NONFINITE for a row with an infinite or NaN element.
 __device__ __forceinline__ int row_scale_exp(unsigned long long am, unsigned long long qv, int sigma, int& s) {
     const int e = oz::exponent_of_max(am);
@@ -412,8 +421,8 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
         c = t >> 32;
     }
     x[NW] = (uint32_t)c;
-    // X = q P + C' with |C'| <= (2^sigma + sqrt(k)/2)^2 < (P / 2)(1 - 2^-20) by the norm rule
-    // (sigma_for), so q is the integer nearest X / P, and
+    // X = q P + C' with |C'| <= (2^sa + sqrt(k)/2)(2^sb + sqrt(k)/2) < (P / 2)(1 - 2^-20) by the norm rule
+    // (sigma_sum_for), so q is the integer nearest X / P, and
     // the estimate from the top three limbs is within 2^-37 of X / P (X < 2^13 P; the dropped
     // limbs are below 2^-37 P): rint gives q exactly, and X - q P is C' itself.
     double xq = 0.0;
@@ -474,7 +483,7 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
 template <int NW, int NM>
 __device__ __forceinline__ void crt_quad(const uint8_t* __restrict__ res, int64_t res_ld, int64_t res_plane,
                                          int64_t m, int64_t row0, int64_t col, const int32_t* __restrict__ row_exp,
-                                         const int32_t* __restrict__ col_exp, int beta, double alpha, double beta_c,
+                                         const int32_t* __restrict__ col_exp, int ssum, double alpha, double beta_c,
                                          double* __restrict__ C, int64_t ldc, const CrtConst& cc) {
     uint32_t rr[MAX_MODULI];  // four rows' residues per modulus, one byte each
 #pragma unroll
@@ -490,7 +499,7 @@ __device__ __forceinline__ void crt_quad(const uint8_t* __restrict__ res, int64_
         if (e == oz::EXP_NONFINITE || f == oz::EXP_NONFINITE)
             val = __longlong_as_double(0x7ff8000000000000ll);
         else
-            val = crt_value<NW, NM>(rr, e4, cc, e + f - 2 * beta);
+            val = crt_value<NW, NM>(rr, e4, cc, e + f - ssum);
         double* cp = C + row + col * ldc;
         *cp = beta_c != 0.0 ? fma(alpha, val, beta_c * *cp) : alpha * val;
     }
@@ -501,13 +510,13 @@ template <int NW, int NM>
 __global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
                                                        int64_t res_plane, int64_t m, int64_t n,
                                                        const int32_t* __restrict__ row_exp,
-                                                       const int32_t* __restrict__ col_exp, int beta, double alpha,
+                                                       const int32_t* __restrict__ col_exp, int ssum, double alpha,
                                                        double beta_c, double* __restrict__ C, int64_t ldc,
                                                        const __grid_constant__ CrtConst cc) {
     const int64_t quads = (m + 3) / 4;
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= quads * n) return;
-    crt_quad<NW, NM>(res, res_ld, res_plane, m, (idx % quads) * 4, idx / quads, row_exp, col_exp, beta, alpha, beta_c, C,
+    crt_quad<NW, NM>(res, res_ld, res_plane, m, (idx % quads) * 4, idx / quads, row_exp, col_exp, ssum, alpha, beta_c, C,
                  ldc, cc);
 }
 
@@ -628,13 +637,14 @@ dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmo
     using namespace oz2;
     if (nmod < MIN_MODULI || nmod > MAX_MODULI)
         return fail(h, DGT_ERROR_INVALID_VALUE, "modulus count must be in [8, 20]");
-    const int bits = sigma_for(nmod, k);
+    const int ssum = sigma_sum_for(nmod, k);
     // kernel variant: 0 (4 epilogue warps), 4 (CTA pair) or 1 (8 warps); all 128-byte stages
     const int variant = (h->ozaki_variant == 0 || h->ozaki_variant == 4) ? h->ozaki_variant : 1;
     const bool pair = variant == 4;
     const int64_t m_unit = pair ? 2 * oz::TM : oz::TM;
     sh.nmod = nmod;
-    sh.bits = bits;
+    sh.sa = (ssum + 1) / 2;
+    sh.sb = ssum / 2;
     sh.variant = variant;
     sh.pair = pair;
     sh.m = m;
@@ -652,9 +662,9 @@ dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmo
 
 // amax and residue planes of one operand: the MN rows of op(A) (kcontig = transa) or the MN
 // columns of op(B) (kcontig = !transb), planes padded to mn_pad rows.
-dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, const double* X, int64_t ld, int64_t MN,
-                        int64_t mn_pad, bool kcontig, unsigned long long* amax, unsigned long long* qn, int32_t* exps,
-                        int8_t* planes) {
+dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int sigma, const double* X, int64_t ld,
+                        int64_t MN, int64_t mn_pad, bool kcontig, unsigned long long* amax, unsigned long long* qn,
+                        int32_t* exps, int8_t* planes) {
     using namespace oz2;
     dgt_status st = ozaki_amax(h, s, X, ld, MN, sh.k, kcontig, amax);
     if (st != DGT_SUCCESS) return st;
@@ -669,10 +679,10 @@ dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, cons
     DGT_CUDA_TRY(h, cudaGetLastError());
     dim3 grid((unsigned)ceil_div(mn_pad, RES_ROWS), (unsigned)(sh.k_pad / RES_KSPAN));
     if (kcontig)
-        split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sh.bits, amax, qn,
+        split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sigma, amax, qn,
                                                   exps, planes, sh.mt);
     else
-        split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sh.bits, amax, qn,
+        split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sigma, amax, qn,
                                                    exps, planes, sh.mt);
     h->launches.fetch_add(1);
     cudaError_t e = cudaGetLastError();
@@ -724,7 +734,7 @@ dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, i
     const int64_t threads = ceil_div(m, 4) * n;
     const unsigned blocks = (unsigned)ceil_div(threads, 256);
     const CrtConst& cc = sh.cc;
-    const int bits = sh.bits;
+    const int bits = sh.sa + sh.sb;
 #define DGT_CRT_LAUNCH(NW, NM)                                                                            \
     crt_reconstruct<NW, NM><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta, \
                                                    C, ldc, cc)
@@ -788,9 +798,11 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     cudaStream_t s = h->stream;
     mark(h, 0);
     // op(A) is m x k: 'N' -> MN-contiguous; op(B) as its transpose n x k: 'N' -> K-contiguous
-    if ((st = ozaki2_split(h, s, sh, A, lda, m, sh.m_pad, ta, w.amaxA, w.qnA, w.expA, w.planesA)) != DGT_SUCCESS)
+    if ((st = ozaki2_split(h, s, sh, sh.sa, A, lda, m, sh.m_pad, ta, w.amaxA, w.qnA, w.expA, w.planesA)) !=
+        DGT_SUCCESS)
         return st;
-    if ((st = ozaki2_split(h, s, sh, B, ldb, n, sh.n_pad, !tb, w.amaxB, w.qnB, w.expB, w.planesB)) != DGT_SUCCESS)
+    if ((st = ozaki2_split(h, s, sh, sh.sb, B, ldb, n, sh.n_pad, !tb, w.amaxB, w.qnB, w.expB, w.planesB)) !=
+        DGT_SUCCESS)
         return st;
     return ozaki2_gemm_crt(h, s, sh, n, sh.n_pad, w.planesA, w.expA, w.planesB, w.expB, w.res, alpha, beta, C, ldc);
 }

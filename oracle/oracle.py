@@ -416,22 +416,30 @@ OZAKI2_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                  223, 217, 211, 199, 197, 193, 191, 181, 179, 173)
 
 
-def ozaki2_sigma(nmod: int, k: int) -> int:
-    """Norm-bound exponent for nmod moduli and inner dimension k: the largest sigma with
-    (2^sigma + sqrt(k)/2)^2 < (P/2)(1 - 2^-20), computed as the kernels' host code does
-    (csrc/ozaki2.cu sigma_for)."""
+def ozaki2_sigmas(nmod: int, k: int):
+    """(sigma_A, sigma_B) for nmod moduli and inner dimension k: s = sigma_A + sigma_B is the
+    largest with (2^ceil(s/2) + sqrt(k)/2)(2^floor(s/2) + sqrt(k)/2) < (P/2)(1 - 2^-20), checked
+    in the log domain with a 1e-9 margin as the kernels' host code does (csrc/ozaki2.cu
+    sigma_sum_for); op(A) takes the odd bit."""
     import math
 
     lg = 0.0
     for p in OZAKI2_MODULI[:nmod]:
         lg += math.log2(float(p))
-    root = 2.0 ** ((lg - 1.0 + math.log2(1.0 - 2.0 ** -20)) / 2.0)
-    lim = root - math.sqrt(float(max(k, 1))) / 2.0
-    return math.floor(math.log2(lim) - 1e-9)
+    t = lg - 1.0 + math.log2(1.0 - 2.0 ** -20)
+    r = math.sqrt(float(max(k, 1))) / 2.0
+    s = math.floor(t)
+    while s > 0:
+        a, b = 2.0 ** ((s + 1) // 2), 2.0 ** (s // 2)
+        if math.log2((a + r) * (b + r)) < t - 1e-9:
+            break
+        s -= 1
+    return (s + 1) // 2, s // 2
 
 
 def _row_scale(v, sigma: int):
-    """Scale exponent s of one row (or column) v: s = min(sigma - g, 58 - e), e the exponent of
+    """Scale exponent s of one row of op(A) (sigma = sigma_A) or column of op(B) (sigma_B):
+    s = min(sigma - g, 58 - e), e the exponent of
     max |v| and 2^g >= the integer bound of ||v||_2, q = sum ceil(|v| 2^(20-e))^2
     (csrc/ozaki2.cu qnorm_* and row_scale_exp).  None for a row with inf or NaN."""
     import math
@@ -465,12 +473,12 @@ def ozaki2_exact(A, B, nmod: int, ta: str = "N", tb: str = "N"):
     Aop, Bop = op(A, ta), op(B, tb)
     m, k = Aop.shape
     n = Bop.shape[1]
-    sigma = ozaki2_sigma(nmod, k)
+    sig_a, sig_b = ozaki2_sigmas(nmod, k)
     P = 1
     for p in OZAKI2_MODULI[:nmod]:
         P *= p
-    sa = [_row_scale(Aop[i, :], sigma) for i in range(m)]
-    sb = [_row_scale(Bop[:, j], sigma) for j in range(n)]
+    sa = [_row_scale(Aop[i, :], sig_a) for i in range(m)]
+    sb = [_row_scale(Bop[:, j], sig_b) for j in range(n)]
     Ai = [[int(round(math.ldexp(float(Aop[i, t]), sa[i]))) for t in range(k)] for i in range(m)]
     Bi = [[int(round(math.ldexp(float(Bop[t, j]), sb[j]))) for t in range(k)] for j in range(n)]
     C = np.empty((m, n))
@@ -490,11 +498,11 @@ def ozaki2_residue_check(A, B, nmod: int):
 
     m, k = A.shape
     n = B.shape[1]
-    sigma = ozaki2_sigma(nmod, k)
+    sig_a, sig_b = ozaki2_sigmas(nmod, k)
     mods = OZAKI2_MODULI[:nmod]
     P = math.prod(mods)
-    sa = [_row_scale(A[i, :], sigma) for i in range(m)]
-    sb = [_row_scale(B[:, j], sigma) for j in range(n)]
+    sa = [_row_scale(A[i, :], sig_a) for i in range(m)]
+    sb = [_row_scale(B[:, j], sig_b) for j in range(n)]
     Ai = np.array([[int(round(math.ldexp(float(A[i, t]), sa[i]))) for t in range(k)]
                    for i in range(m)], dtype=object)
     Bi = np.array([[int(round(math.ldexp(float(B[t, j]), sb[j]))) for j in range(n)]

@@ -16,17 +16,18 @@ def test_crt_identity_recovers_the_integer_product(nmod, k):
 
 
 def test_norm_rule():
-    """sigma: (2^sigma + sqrt(k)/2)^2 < (P/2)(1 - 2^-20), and sigma + 1 breaks it (checked in
-    integers with sqrt(k) bounded by isqrt)."""
+    """sigma_A + sigma_B: (2^sigma_A + sqrt(k)/2)(2^sigma_B + sqrt(k)/2) < (P/2)(1 - 2^-20), and one
+    more bit breaks it (checked in integers, sqrt(k) bounded by isqrt)."""
     for nmod in range(8, 21):
         P = math.prod(O.OZAKI2_MODULI[:nmod])
         for k in (1, 7, 256, 4096, 16384, 65536):
-            sg = O.ozaki2_sigma(nmod, k)
-            r = math.isqrt(k) + 1  # > sqrt(k)
-            lhs = (2 ** (sg + 1) + r) ** 2  # 4 (2^sigma + sqrt(k)/2)^2 < lhs
-            assert lhs * 2 ** 20 < 2 * P * (2 ** 20 - 1)
-            r0 = math.isqrt(k)  # <= sqrt(k)
-            assert (2 ** (sg + 2) + r0) ** 2 * 2 ** 20 >= 2 * P * (2 ** 20 - 1)  # sigma + 1 fails
+            sa, sb = O.ozaki2_sigmas(nmod, k)
+            assert sa - sb in (0, 1)
+            hi = math.isqrt(k) + 1  # > sqrt(k)
+            assert (2 ** (sa + 1) + hi) * (2 ** (sb + 1) + hi) * 2 ** 20 < 2 * P * (2 ** 20 - 1)
+            s1 = sa + sb + 1
+            lo = math.isqrt(k)  # <= sqrt(k)
+            assert (2 ** ((s1 + 1) // 2 + 1) + lo) * (2 ** (s1 // 2 + 1) + lo) * 2 ** 20 >= 2 * P * (2 ** 20 - 1)
     assert all(math.gcd(p, q) == 1 for i, p in enumerate(O.OZAKI2_MODULI) for q in O.OZAKI2_MODULI[:i])
 
 
@@ -36,10 +37,10 @@ def test_row_scale_caps_entries():
     k = 64
     single = np.zeros(k)
     single[5] = 0.75
-    s1 = O._row_scale(single, O.ozaki2_sigma(20, k))
+    s1 = O._row_scale(single, O.ozaki2_sigmas(20, k)[0])
     assert abs(int(round(math.ldexp(0.75, s1)))) <= 2 ** 58 and s1 == 58  # e = 0: cap 58 - e
     dense = np.full(k, 0.75)
-    sg = O.ozaki2_sigma(12, k)
+    sg = O.ozaki2_sigmas(12, k)[0]
     s2 = O._row_scale(dense, sg)
     norm = math.sqrt(sum(math.ldexp(0.75, s2) ** 2 for _ in range(k)))
     assert norm <= 2 ** sg < 2 * norm * 2  # within a factor 2 of the bound (power-of-two scales)
@@ -88,4 +89,4 @@ def test_exact_restatement_accuracy():
     A, B = O.ozaki_matrix((40, 300), 3, 0.5), O.ozaki_matrix((300, 30), 4, 0.5)
     want = O.dgemm(A, B)
     assert O.rel_errors(O.ozaki2_exact(A, B, 17), want)[1] <= 1e-15
-    assert O.rel_errors(O.ozaki2_exact(A, B, 12), want)[1] > 1e-13  # fewer moduli, fewer bits
+    assert O.rel_errors(O.ozaki2_exact(A, B, 12), want)[1] > 1e-14  # fewer moduli, fewer bits
