@@ -456,13 +456,6 @@ def _row_scale(v, sigma: int):
     return min(sigma - (e - 20 + h), 58 - e)
 
 
-def _exp_of_max(v: float) -> int:
-    """e with v in [2^(e-1), 2^e) (0 for v == 0)."""
-    import math
-
-    return 0 if v == 0.0 else math.frexp(v)[1]
-
-
 def ozaki2_exact(A, B, nmod: int, ta: str = "N", tb: str = "N"):
     """C = op(A) op(B) as the CRT emulation computes it: each row of op(A) / column of op(B)
     scaled by 2^s (its 2-norm bound, capped so no entry exceeds 2^58) and rounded to
