@@ -27,8 +27,27 @@ using namespace dgt;
 
 namespace {
 
-enum { EV_START, EV_A, EV_IN0, EV_IN1, EV_BFREE0, EV_BFREE1, EV_C0, EV_C1, EV_OUT0, EV_OUT1, EV_COUNT };
-static_assert(EV_COUNT <= 10, "dgt_context::copy_ev holds 10 events");
+enum {
+    EV_START, EV_A, EV_IN0, EV_IN1, EV_BFREE0, EV_BFREE1, EV_C0, EV_C1, EV_OUT0, EV_OUT1, EV_JOIN_IN, EV_JOIN_OUT,
+    EV_COUNT
+};
+static_assert(EV_COUNT <= 12, "dgt_context::copy_ev holds 12 events");
+
+// Once copies may be queued, every exit (success or error) orders the handle's stream after
+// all work of both copy streams, so nothing of this call can still be writing the handle's
+// workspace or the caller's C when the next work on the handle's stream starts.
+struct JoinCopyStreams {
+    cudaStream_t s = nullptr, si = nullptr, so = nullptr;
+    cudaEvent_t ei = nullptr, eo = nullptr;
+    bool armed = false;
+    ~JoinCopyStreams() {
+        if (!armed) return;
+        cudaEventRecord(ei, si);
+        cudaEventRecord(eo, so);
+        cudaStreamWaitEvent(s, ei, 0);
+        cudaStreamWaitEvent(s, eo, 0);
+    }
+};
 
 dgt_status ensure_copy_streams(dgt_context* h) {
     for (auto& cs : h->copy_stream)
@@ -103,7 +122,14 @@ extern "C" dgt_status dgt_dgemm_host(dgt_handle_t h, char transa, char transb, i
     }
 
     // copies start after the work already queued on the handle's stream
+    JoinCopyStreams join;
+    join.s = s;
+    join.si = si;
+    join.so = so;
+    join.ei = ev[EV_JOIN_IN];
+    join.eo = ev[EV_JOIN_OUT];
     DGT_CUDA_TRY(h, cudaEventRecord(ev[EV_START], s));
+    join.armed = true;
     DGT_CUDA_TRY(h, cudaStreamWaitEvent(si, ev[EV_START], 0));
     DGT_CUDA_TRY(h, cudaStreamWaitEvent(so, ev[EV_START], 0));
     if (k > 0) {
@@ -161,7 +187,6 @@ extern "C" dgt_status dgt_dgemm_host(dgt_handle_t h, char transa, char transb, i
         DGT_CUDA_TRY(h, cudaEventRecord(ev[EV_OUT0 + buf], so));
     }
     // the call is complete on the handle's stream once the last results have reached C
-    DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[EV_OUT0 + (int)((panels - 1) & 1)], 0));
-    if (panels > 1) DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[EV_OUT0 + (int)((panels - 2) & 1)], 0));
+    // (the join at scope exit)
     return DGT_SUCCESS;
 }
