@@ -426,6 +426,32 @@ dgt_status dgt_dgemm_ex(dgt_handle_t h, char ta, char tb, int64_t m, int64_t n, 
     return ozaki_dgemm(h, is_trans(ta), is_trans(tb), m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc, mode, slices);
 }
 
+dgt_status dgt_dgemm_workspace_size(int64_t m, int64_t n, int64_t k, dgt_fp64_mode mode, int slices,
+                                    size_t* bytes) {
+    if (!bytes) return DGT_ERROR_INVALID_VALUE;
+    *bytes = 0;
+    if (m < 0 || n < 0 || k < 0) return DGT_ERROR_INVALID_VALUE;
+    if (m == 0 || n == 0 || k == 0 || mode == DGT_FP64_NATIVE) return DGT_SUCCESS;
+    if (mode == DGT_FP64_OZAKI_INT8 || mode == DGT_FP64_OZAKI_BF16) {
+        if (!valid_slices(mode, slices)) return DGT_ERROR_INVALID_VALUE;
+        return ozaki_workspace_bound(slices, m, n, k, mode == DGT_FP64_OZAKI_BF16, bytes);
+    }
+    if (mode == DGT_FP64_OZAKI2_INT8) {
+        if (!valid_slices(mode, slices)) return DGT_ERROR_INVALID_VALUE;
+        return ozaki2_workspace_bound(slices, m, n, k, bytes);
+    }
+    if (mode == DGT_FP64_AUTO) {  // the autotuner's emulated candidates for this count
+        size_t a = 0, c = 0;
+        dgt_status sa = valid_slices(DGT_FP64_OZAKI_INT8, slices)
+                            ? ozaki_workspace_bound(slices, m, n, k, false, &a) : DGT_ERROR_INVALID_VALUE;
+        dgt_status sc = ozaki2_workspace_bound(valid_slices(DGT_FP64_OZAKI2_INT8, slices) ? slices : 16, m, n, k, &c);
+        if (sa != DGT_SUCCESS && sc != DGT_SUCCESS) return sa;
+        *bytes = std::max(a, c);
+        return DGT_SUCCESS;
+    }
+    return DGT_ERROR_INVALID_VALUE;
+}
+
 dgt_status dgt_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64_t n, int64_t k, const double* alpha,
                      const double* A, int64_t lda, const double* B, int64_t ldb, const double* beta, double* C,
                      int64_t ldc) {

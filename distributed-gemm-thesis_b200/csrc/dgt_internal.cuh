@@ -165,6 +165,9 @@ dgt_status launch_stack_reduce(dgt_context* h, int64_t elems_per_tile, int tiles
 // ---- Ozaki emulation (ozaki.cu) -----------------------------------------------------------
 // Scratch bytes one INT8 Ozaki call needs (0 if the shape is unsupported).
 size_t ozaki_scratch_bytes(int S, int64_t m, int64_t n, int64_t k);
+// Workspace upper bounds over kernel variants (dgt_dgemm_workspace_size).
+dgt_status ozaki_workspace_bound(int S, int64_t m, int64_t n, int64_t k, bool bf16, size_t* bytes);
+dgt_status ozaki2_workspace_bound(int nmod, int64_t m, int64_t n, int64_t k, size_t* bytes);
 // The INT8 Ozaki path on caller-provided scratch; no allocation, no handle.
 dgt_status ozaki_dgemm_on(cudaStream_t s, int num_sms, unsigned int* err, void* ws, size_t ws_bytes, bool ta,
                           bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A, int64_t lda,

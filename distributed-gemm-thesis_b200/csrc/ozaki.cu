@@ -266,6 +266,21 @@ static dgt_status ozaki_layout(dgt_context* h, int S, int64_t m, int64_t n, int6
     return DGT_SUCCESS;
 }
 
+// Largest workspace of the slice scheme over the kernel variants (0 .. 4) for this shape;
+// DGT_ERROR_UNSUPPORTED when no variant can run it.
+dgt_status ozaki_workspace_bound(int S, int64_t m, int64_t n, int64_t k, bool bf16, size_t* bytes) {
+    size_t best = 0;
+    bool any = false;
+    for (int v = 0; v <= 4; ++v) {
+        OzakiLayout L;
+        if (ozaki_layout(nullptr, S, m, n, k, v, bf16, L) != DGT_SUCCESS) continue;
+        best = std::max(best, L.total);
+        any = true;
+    }
+    *bytes = best;
+    return any ? DGT_SUCCESS : DGT_ERROR_UNSUPPORTED;
+}
+
 size_t ozaki_scratch_bytes(int S, int64_t m, int64_t n, int64_t k) {
     OzakiLayout L;
     return ozaki_layout(nullptr, S, m, n, k, 0, false, L) == DGT_SUCCESS ? L.total : 0;

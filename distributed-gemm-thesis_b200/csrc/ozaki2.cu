@@ -761,6 +761,27 @@ dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, i
 
 int64_t ozaki2_n_pad(int64_t n) { return ceil_div(n, oz::TN) * oz::TN; }
 
+// Largest workspace of the CRT scheme for this shape over the kernel variants (the CTA-pair
+// variant pads M to 256) and K-chunks (at most 65536 deep); DGT_ERROR_UNSUPPORTED as the call.
+dgt_status ozaki2_workspace_bound(int nmod, int64_t m, int64_t n, int64_t k, size_t* bytes) {
+    *bytes = 0;
+    if (nmod < oz2::MIN_MODULI || nmod > oz2::MAX_MODULI) return DGT_ERROR_INVALID_VALUE;
+    const int64_t kc = std::min<int64_t>(std::max<int64_t>(k, 1), 65536);
+    for (int pair = 0; pair < 2; ++pair) {
+        Oz2Shape sh{};
+        sh.nmod = nmod;
+        sh.m = m;
+        sh.k = kc;
+        const int64_t m_unit = pair ? 2 * oz::TM : oz::TM;
+        sh.m_pad = ceil_div(m, m_unit) * m_unit;
+        sh.n_pad = ceil_div(n, oz::TN) * oz::TN;
+        sh.k_pad = ceil_div(kc, oz::KPAD) * oz::KPAD;
+        if ((int64_t)nmod * std::max(sh.m_pad, sh.n_pad) > INT32_MAX) return DGT_ERROR_UNSUPPORTED;
+        *bytes = std::max(*bytes, ozaki2_carve(sh, n, sh.n_pad, nullptr).bytes);
+    }
+    return DGT_SUCCESS;
+}
+
 // Workspace carve of one CRT product: planes of op(A) (m_pad rows) and op(B) (n_pad rows),
 // amax words, exponents and the residue planes of C.
 Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws) {

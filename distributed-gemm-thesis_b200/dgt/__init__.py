@@ -64,6 +64,8 @@ SIGNATURES = [
                            _dp, _vp, _c_i64]),
     ("dgt_dgemm_ex", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _dp, _vp, _c_i64, _vp,
                               _c_i64, _dp, _vp, _c_i64, _c_i32, ctypes.c_int]),
+    ("dgt_dgemm_workspace_size", _c_i32, [_c_i64, _c_i64, _c_i64, _c_i32, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_size_t)]),
     ("dgt_dgemm_host", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _dp, _vp, _c_i64, _vp,
                                 _c_i64, _dp, _vp, _c_i64, _c_i32, ctypes.c_int, _c_i64]),
     ("dgt_sgemm", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _fp, _vp, _c_i64, _vp, _c_i64,
@@ -123,6 +125,16 @@ def _ptrs(ptrs):
 
 def _i64s(vals):
     return (_c_i64 * len(vals))(*[int(v) for v in vals])
+
+
+def dgemm_workspace_size(m, n, k, mode=FP64_NATIVE, slices=7):
+    """dgt_dgemm_workspace_size: device workspace bytes a dgt_dgemm_ex call of this shape needs
+    (an upper bound over kernel variants); no handle, no device call."""
+    out = ctypes.c_size_t()
+    st = load().dgt_dgemm_workspace_size(m, n, k, mode, slices, ctypes.byref(out))
+    if st != 0:
+        raise DgtError(st, "dgt_dgemm_workspace_size")
+    return out.value
 
 
 class Handle:
