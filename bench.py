@@ -279,7 +279,8 @@ def _setup():
 def workload_summa(args):
     """Plain FP64 SUMMA on virtual grids (4096^3 on 2x2 with 512 blocks; 15000x17000x9000 on
     4x4 with 256 blocks, alpha 1.5, beta -0.5), with the block-cyclic pack/unpack kernels
-    timed against HBM bandwidth (L2 flushed before each layout call)."""
+    timed against HBM bandwidth (L2 flushed before each layout call); cuBLAS DGEMM and the
+    reference's per-column layout copies are timed beside them as comparators."""
     import numpy as np
 
     torch, dgt, h = _setup()
@@ -347,9 +348,38 @@ def workload_summa(args):
         dC2 = torch.zeros_like(dC)
         glob_ms = _time_ms(torch, lambda: h.dgemm("N", "N", M, N, K, alpha, dA.data_ptr(), M, dB.data_ptr(), K, 0.0,
                                                    dC2.data_ptr(), M), 5)
+        # comparators, not the product: cuBLAS DGEMM (torch FP64 matmul) on the global matrices,
+        # and the reference's layout move -- one device copy per column of every block
+        # (src/Transfers/sharedTransfers.cpp:58-60) -- on a bounded sample of pack A's columns
+        At, Bt = dA.t(), dB.t()  # column-major A, B as torch views
+        cublas_ms = _time_ms(torch, lambda: torch.matmul(At, Bt), 5)
+        ncopies, sample_cols = 0, 4096
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for bj in range((K + b - 1) // b):
+            for bi in range((M + b - 1) // b):
+                owner = (bi % p) * q + (bj % q)
+                r0, c0, lr, lc = bi * b, bj * b, (bi // p) * b, (bj // q) * b
+                mr = min(b, M - r0)
+                for j in range(min(b, K - c0)):
+                    kA[owner][lc + j, lr:lr + mr].copy_(dA[c0 + j, r0:r0 + mr])
+                    ncopies += 1
+                    if ncopies == sample_cols:
+                        break
+                if ncopies == sample_cols:
+                    break
+            if ncopies == sample_cols:
+                break
+        torch.cuda.synchronize()
+        ref_s = time.perf_counter() - t0
+        ref_bytes = 16.0 * min(b, M) * ncopies
         out.append({"config": c["name"], "summa_tflops": flops / (summa_ms * 1e-3) / 1e12, "summa_ms": summa_ms,
                     "frac_of_dmma_peak": flops / (summa_ms * 1e-3) / 1e12 / dmma_peak,
                     "one_global_dgemm_tflops": flops / (glob_ms * 1e-3) / 1e12,
+                    "cublas_dgemm_tflops": flops / (cublas_ms * 1e-3) / 1e12,
+                    "reference_style_pack": {"column_copies": ncopies, "GB/s": ref_bytes / ref_s / 1e9,
+                                             "how": "one device copy per block column (torch slice copy_), "
+                                                    "first %d columns of pack A" % ncopies},
                     "max_rel": err[0], "fro_rel": err[1], "sampled_rows": len(rows),
                     "summa_crt16": {"tflops": flops / (crt_ms * 1e-3) / 1e12, "ms": crt_ms, "max_rel": err_crt[0],
                                     "fro_rel": err_crt[1]},
