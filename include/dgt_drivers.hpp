@@ -1,0 +1,250 @@
+// The reference's 2.5D Cannon benchmark drivers on top of the C++ mirror classes, with its
+// CSV execution logs (include/dgt_logging.hpp):
+//
+//   fullOffloadSumma25Dgemm     src/25DCannon.cpp:392-459   global A, B, C (host or device)
+//                                                            -> tiles -> runs -> gather
+//   preDistributedSumma25Dgemm  src/25DCannon.cpp:462-530   operands generated on the tiles
+//                                                            -> runs (-> gather)
+//
+// Same argument lists; two trailing defaults add what the virtual grid needs: the FP64
+// arithmetic (native DMMA or an emulation scheme) and where the log goes.  The whole
+// dRow x dCol x c grid runs on the current device, so a row's TotalGPUs is 1 and the
+// virtual grid is in dRow, dCol, StackSize.  Per row:
+//
+//   DecompositionTime  full offload: tile allocation, host->device copy of A, B, C and the
+//                      decompose2D pack; pre-distributed: tile allocation only (the
+//                      reference times only the decomposer's constructor, :483-485)
+//   ExecutionTime      one multiply, device time from CUDA events on the handle's stream
+//   GatherTime         reorderMatrix (device unpack, then the copy into C) when gathering
+//   CommunicationTime  0: the broadcast to the stacks and every shift are tile index
+//                      changes of the in-device schedule and move no data; the stack
+//                      reduction is a kernel of the multiply and counts in GemmCallTime
+//   GemmCallTime       = ExecutionTime
+//
+// Every run applies C <- alpha op(A) op(B) + beta C to the same tiles, as the reference's
+// run loop does.  Errors throw dgt::Error (the reference exits).
+#ifndef DGT_DRIVERS_HPP
+#define DGT_DRIVERS_HPP
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdint>
+#include <memory>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "dgt_logging.hpp"
+#include "dgt_mirror.hpp"
+
+namespace dgt {
+
+struct DriverOptions {
+    dgt_fp64_mode mode = DGT_FP64_NATIVE;
+    int slices = 7;          // emulation: slices (Ozaki I) or moduli (Ozaki II)
+    std::string logDir = ".";
+    std::string impl = "dgt";  // file-name suffix after "2.5DCANNON-"
+    std::string machine;       // empty: machineName()
+    uint64_t seed = 0;         // pre-distributed operands
+};
+
+namespace detail {
+
+inline void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Error(DGT_ERROR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct DevFree {
+    void operator()(double* p) const { cudaFree(p); }
+};
+using DevBuf = std::unique_ptr<double, DevFree>;
+
+inline DevBuf dev_alloc(size_t elems) {
+    double* p = nullptr;
+    cuda_check(cudaMalloc(&p, (elems ? elems : 1) * sizeof(double)), "cudaMalloc");
+    return DevBuf(p);
+}
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventPair() {
+        cuda_check(cudaEventCreate(&a), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&b), "cudaEventCreate");
+    }
+    ~EventPair() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    EventPair(const EventPair&) = delete;
+    EventPair& operator=(const EventPair&) = delete;
+};
+
+struct LogFile {
+    FILE* f = nullptr;
+    ~LogFile() {
+        if (f) std::fclose(f);
+    }
+};
+
+inline double seconds_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+inline std::string algo_name(const DriverOptions& o) {
+    switch (o.mode) {
+        case DGT_FP64_OZAKI_INT8: return "2.5D CANNON dgt OzakiI-INT8x" + std::to_string(o.slices);
+        case DGT_FP64_OZAKI_BF16: return "2.5D CANNON dgt OzakiI-BF16x" + std::to_string(o.slices);
+        case DGT_FP64_OZAKI2_INT8: return "2.5D CANNON dgt OzakiII-" + std::to_string(o.slices) + "moduli";
+        default: return "2.5D CANNON dgt";
+    }
+}
+
+// Decomposer, device tiles of the p x p stack-0 ranks, handle and log shared by both drivers.
+struct CannonRun {
+    Context ctx;
+    Summa25Decomposer dec;
+    std::vector<DevBuf> a, b, c;
+    std::vector<double*> pa, pb, pc;
+    LogFile log;
+    DriverOptions opt;
+    std::string algo;
+
+    CannonRun(long long M, long long N, long long K, int dRow, int dCol, int stacks, const DriverOptions& o)
+        : dec(ctx.get(), M, N, K, dRow, dCol, stacks), opt(o), algo(algo_name(o)) {
+        const size_t tile = size_t(dec.localM) * size_t(dec.localK);
+        for (int r = 0; r < dRow * dCol; ++r) {
+            a.push_back(dev_alloc(tile));
+            b.push_back(dev_alloc(tile));
+            c.push_back(dev_alloc(tile));
+            pa.push_back(a.back().get());
+            pb.push_back(b.back().get());
+            pc.push_back(c.back().get());
+        }
+    }
+
+    void open_log(bool preDistributed) {
+        const std::string machine = opt.machine.empty() ? machineName() : opt.machine;
+        const std::string path = opt.logDir + "/" + cannonLogFileName(preDistributed, machine, opt.impl);
+        log.f = createLogCsv(path, cannonLogHeader());
+        if (!log.f) throw Error(DGT_ERROR_INVALID_VALUE, "cannot open log file " + path);
+    }
+
+    // one multiply, device-timed (seconds)
+    double multiply(char TransA, char TransB, double alpha, double beta) {
+        dgt_stream_t s = nullptr;
+        check(ctx.get(), dgt_get_stream(ctx.get(), &s));
+        EventPair ev;
+        cuda_check(cudaEventRecord(ev.a, s), "cudaEventRecord");
+        dec.multiply(TransA, TransB, pa.data(), pb.data(), pc.data(), alpha, beta, opt.mode, opt.slices);
+        cuda_check(cudaEventRecord(ev.b, s), "cudaEventRecord");
+        cuda_check(cudaEventSynchronize(ev.b), "cudaEventSynchronize");
+        check(ctx.get(), dgt_check_device(ctx.get()));
+        float ms = 0.f;
+        cuda_check(cudaEventElapsedTime(&ms, ev.a, ev.b), "cudaEventElapsedTime");
+        return ms * 1e-3;
+    }
+
+    // reorderMatrix(0, C, localC): tiles -> dense device global -> C (host or device, ldc)
+    void gather(double* C, long long ldc) {
+        const long long M = dec.M;
+        DevBuf g = dev_alloc(size_t(M) * size_t(M));
+        dec.reorderMatrix(g.get(), pc.data());
+        cuda_check(cudaMemcpy2D(C, size_t(ldc) * 8, g.get(), size_t(M) * 8, size_t(M) * 8, size_t(M),
+                                cudaMemcpyDefault),
+                   "cudaMemcpy2D");
+    }
+
+    void write_row(double decomp, double exec, double gatherTime) {
+        if (!log.f) return;
+        const std::string line =
+            cannonCsvLine(algo.c_str(), dec.M, dec.N, dec.K, getSlurmNumNodes(), 1, dec.dRow, dec.dCol, dec.c,
+                          decomp, exec, gatherTime, calculateGflops(dec.M, dec.N, dec.K, exec), "devices", 0.0, exec);
+        writeLineToFile(log.f, line.c_str());
+    }
+};
+
+}  // namespace detail
+
+// src/25DCannon.cpp:392-459.  A, B, C: global column-major M x M matrices in host or
+// device memory (lda, ldb, ldc >= M).  With gatherResults every run's result is written
+// back into C.
+inline void fullOffloadSumma25Dgemm(char TransA, char TransB, long long M, long long N, long long K, double alpha,
+                                    const double* A, long long lda, const double* B, long long ldb, double beta,
+                                    double* C, long long ldc, int dRow, int dCol, int c, int numberOfRuns,
+                                    bool logging, bool gatherResults, const DriverOptions& opt = DriverOptions()) {
+    if (!A || !B || !C) throw Error(DGT_ERROR_INVALID_VALUE, "fullOffloadSumma25Dgemm: null matrix");
+    if (lda < M || ldb < M || ldc < M) throw Error(DGT_ERROR_INVALID_VALUE, "leading dimension < M");
+    const auto t0 = std::chrono::steady_clock::now();
+    detail::CannonRun run(M, N, K, dRow, dCol, c, opt);
+    {
+        const size_t MM = size_t(M) * size_t(M);
+        detail::DevBuf gA = detail::dev_alloc(MM), gB = detail::dev_alloc(MM), gC = detail::dev_alloc(MM);
+        const struct {
+            const double* src;
+            long long ld;
+            double* dst;
+        } ops[3] = {{A, lda, gA.get()}, {B, ldb, gB.get()}, {C, ldc, gC.get()}};
+        for (const auto& o : ops)
+            detail::cuda_check(cudaMemcpy2D(o.dst, size_t(M) * 8, o.src, size_t(o.ld) * 8, size_t(M) * 8, size_t(M),
+                                            cudaMemcpyDefault),
+                               "cudaMemcpy2D");
+        run.dec.decompose2D(gA.get(), gB.get(), gC.get(), run.pa.data(), run.pb.data(), run.pc.data());
+        detail::cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        check(run.ctx.get(), dgt_check_device(run.ctx.get()));
+    }
+    const double decomp = detail::seconds_since(t0);
+    if (logging) run.open_log(false);
+    for (int i = 0; i < numberOfRuns; ++i) {
+        const double exec = run.multiply(TransA, TransB, alpha, beta);
+        const auto g0 = std::chrono::steady_clock::now();
+        if (gatherResults) run.gather(C, ldc);
+        const double gatherTime = detail::seconds_since(g0);
+        if (logging) run.write_row(decomp, exec, gatherTime);
+    }
+}
+
+// src/25DCannon.cpp:462-530.  The stack-0 tiles are filled with U[-1, 1) values: global
+// column-major A, then B, then C, drawn in that order from std::mt19937_64(opt.seed) and
+// packed into the tiles (outside every timed region).  A and B are not read, as in the
+// reference; C (host or device, ldc >= M) receives the result when gatherResults is set.
+inline void preDistributedSumma25Dgemm(char TransA, char TransB, long long M, long long N, long long K, double alpha,
+                                       const double* A, long long lda, const double* B, long long ldb, double beta,
+                                       double* C, long long ldc, int dRow, int dCol, int c, int numberOfRuns,
+                                       bool logging, bool gatherResults, const DriverOptions& opt = DriverOptions()) {
+    (void)A;
+    (void)lda;
+    (void)B;
+    (void)ldb;
+    if (gatherResults && (!C || ldc < M)) throw Error(DGT_ERROR_INVALID_VALUE, "gather needs C with ldc >= M");
+    const auto t0 = std::chrono::steady_clock::now();
+    detail::CannonRun run(M, N, K, dRow, dCol, c, opt);
+    detail::cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    const double decomp = detail::seconds_since(t0);
+    {
+        const size_t MM = size_t(M) * size_t(M);
+        std::mt19937_64 rng(opt.seed);
+        std::uniform_real_distribution<double> U(-1.0, 1.0);
+        std::vector<double> host(MM);
+        detail::DevBuf g[3] = {detail::dev_alloc(MM), detail::dev_alloc(MM), detail::dev_alloc(MM)};
+        for (auto& d : g) {
+            for (auto& x : host) x = U(rng);
+            detail::cuda_check(cudaMemcpy(d.get(), host.data(), MM * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+        }
+        run.dec.decompose2D(g[0].get(), g[1].get(), g[2].get(), run.pa.data(), run.pb.data(), run.pc.data());
+        detail::cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        check(run.ctx.get(), dgt_check_device(run.ctx.get()));
+    }
+    if (logging) run.open_log(true);
+    for (int i = 0; i < numberOfRuns; ++i) {
+        const double exec = run.multiply(TransA, TransB, alpha, beta);
+        const auto g0 = std::chrono::steady_clock::now();
+        if (gatherResults) run.gather(C, ldc);
+        const double gatherTime = detail::seconds_since(g0);
+        if (logging) run.write_row(decomp, exec, gatherTime);
+    }
+}
+
+}  // namespace dgt
+
+#endif
