@@ -780,4 +780,16 @@ dgt_status dgt_copy_block(dgt_handle_t h, int64_t rows, int64_t cols, const doub
     return launch_strided_copies(h, {c});
 }
 
+dgt_status dgt_copy_block_f32(dgt_handle_t h, int64_t rows, int64_t cols, const float* src, float* dst, int64_t ldS,
+                              int64_t ldD, int32_t col_major) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (rows < 0 || cols < 0) return fail(h, DGT_ERROR_INVALID_VALUE, "negative size");
+    if (rows * cols == 0) return DGT_SUCCESS;
+    if (!src || !dst) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    if (((uintptr_t)src | (uintptr_t)dst) & 3) return fail(h, DGT_ERROR_INVALID_VALUE, "float pointer not 4-byte aligned");
+    if (!col_major) std::swap(rows, cols);
+    if (ldS < rows || ldD < rows) return fail(h, DGT_ERROR_INVALID_VALUE, "leading dimension < run length");
+    return launch_strided_copy_f32(h, src, dst, ldS, ldD, rows, cols);
+}
+
 }  // extern "C"

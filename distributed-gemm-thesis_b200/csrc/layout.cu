@@ -10,7 +10,8 @@
 //    (src/Decompositions/pblasDecomposition.cpp:73-221).  Global block (bi, bj) belongs to
 //    rank (bi mod p, bj mod q) at local offset ((bi div p)*mb, (bj div q)*nb) -- the
 //    closed form of the reference's modular rowOffset/columnOffset walk (:124-130).
-//  * strided block batches: copyBlock (src/Transfers/sharedTransfers.cpp:29-63) and the
+//  * strided block batches: copyBlock<double> and copyBlock<float>
+//    (src/Transfers/sharedTransfers.cpp:29-63, instantiations :84-88) and the
 //    MPI_Type_vector send/recv pairs (src/Transfers/mpiTransfers.cpp:16-57) used by
 //    deliverMatrix / gatherResult (2DBlockSequentialDecomposition.cpp:56-253) and
 //    decompose2D / reorderMatrix (src/25DCannon.cpp:87-149, :231-284).
@@ -67,6 +68,41 @@ __device__ __forceinline__ void warp_copy(const double* __restrict__ s, double* 
     }
 }
 
+// Copies n floats from s to d with one warp: the same scheme with four floats per 16-byte
+// vector, so the same-phase case peels up to three head and three tail elements.  Float
+// pointers are 4-byte aligned (checked by the caller), so after `head` elements both
+// addresses sit on a 16-byte boundary.
+__device__ __forceinline__ void warp_copy(const float* __restrict__ s, float* __restrict__ d, int64_t n, int lane) {
+    if ((((uintptr_t)s ^ (uintptr_t)d) & 15) == 0) {
+        const int64_t head = min(n, (int64_t)(((16 - ((uintptr_t)s & 15)) & 15) >> 2));
+        if (lane < head) d[lane] = s[lane];
+        const float4* s4 = reinterpret_cast<const float4*>(s + head);
+        float4* d4 = reinterpret_cast<float4*>(d + head);
+        const int64_t quads = (n - head) >> 2;
+        int64_t k = lane;
+        for (; k + 96 < quads; k += 128) {
+            float4 v0 = __ldcs(s4 + k), v1 = __ldcs(s4 + k + 32), v2 = __ldcs(s4 + k + 64), v3 = __ldcs(s4 + k + 96);
+            __stcs(d4 + k, v0);
+            __stcs(d4 + k + 32, v1);
+            __stcs(d4 + k + 64, v2);
+            __stcs(d4 + k + 96, v3);
+        }
+        for (; k < quads; k += 32) __stcs(d4 + k, __ldcs(s4 + k));
+        const int64_t i = head + quads * 4;
+        if (lane < n - i) d[i + lane] = s[i + lane];
+    } else {
+        int64_t k = lane;
+        for (; k + 96 < n; k += 128) {
+            float v0 = __ldcs(s + k), v1 = __ldcs(s + k + 32), v2 = __ldcs(s + k + 64), v3 = __ldcs(s + k + 96);
+            __stcs(d + k, v0);
+            __stcs(d + k + 32, v1);
+            __stcs(d + k + 64, v2);
+            __stcs(d + k + 96, v3);
+        }
+        for (; k < n; k += 32) __stcs(d + k, __ldcs(s + k));
+    }
+}
+
 struct CyclicParams {
     int64_t M, N, mb, nb, ldg;
     int32_t p, q;
@@ -100,20 +136,23 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) block_cyclic_kernel(const __gr
     }
 }
 
+template <typename T>
 struct CopyDesc {
-    const double* src;
-    double* dst;
+    const T* src;
+    T* dst;
     int64_t ldS, ldD, rows, cols;
     int64_t run_begin;  // prefix sum of cols
 };
 
+template <typename T>
 struct CopyParams {
     int ncopies;
     int64_t total_runs;
-    CopyDesc d[MAX_COPIES];
+    CopyDesc<T> d[MAX_COPIES];
 };
 
-__global__ void __launch_bounds__(LAYOUT_THREADS) strided_copy_kernel(const __grid_constant__ CopyParams P) {
+template <typename T>
+__global__ void __launch_bounds__(LAYOUT_THREADS) strided_copy_kernel(const __grid_constant__ CopyParams<T> P) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (LAYOUT_THREADS / 32);
     for (int64_t run = (int64_t)blockIdx.x * (LAYOUT_THREADS / 32) + (threadIdx.x >> 5); run < P.total_runs;
@@ -126,7 +165,7 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) strided_copy_kernel(const __gr
             else
                 hi = mid - 1;
         }
-        const CopyDesc& cd = P.d[lo];
+        const CopyDesc<T>& cd = P.d[lo];
         int64_t col = run - cd.run_begin;
         warp_copy(cd.src + col * cd.ldS, cd.dst + col * cd.ldD, cd.rows, lane);
     }
@@ -160,7 +199,8 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) stack_reduce_kernel(const __gr
 }
 
 thread_local CyclicParams t_cyc;
-thread_local CopyParams t_copy;
+thread_local CopyParams<double> t_copy;
+thread_local CopyParams<float> t_copy_f32;
 thread_local ReduceParams t_red;
 
 }  // namespace
@@ -197,22 +237,35 @@ dgt_status launch_block_cyclic(dgt_context* h, bool to_local, int64_t M, int64_t
 dgt_status launch_strided_copies(dgt_context* h, const std::vector<HostCopy>& copies) {
     size_t i = 0;
     while (i < copies.size()) {
-        CopyParams& P = t_copy;
+        CopyParams<double>& P = t_copy;
         int n = 0;
         int64_t runs = 0;
         for (; i < copies.size() && n < MAX_COPIES; ++i) {
             const HostCopy& c = copies[i];
             if (c.rows <= 0 || c.cols <= 0) continue;
-            P.d[n] = CopyDesc{c.src, c.dst, c.ldS, c.ldD, c.rows, c.cols, runs};
+            P.d[n] = CopyDesc<double>{c.src, c.dst, c.ldS, c.ldD, c.rows, c.cols, runs};
             runs += c.cols;
             ++n;
         }
         if (n == 0) continue;
         P.ncopies = n;
         P.total_runs = runs;
-        strided_copy_kernel<<<layout_grid(h, runs), LAYOUT_THREADS, 0, h->stream>>>(P);
+        strided_copy_kernel<double><<<layout_grid(h, runs), LAYOUT_THREADS, 0, h->stream>>>(P);
         DGT_LAUNCH_CHECK(h, "strided_copy_kernel");
     }
+    return DGT_SUCCESS;
+}
+
+// One strided float copy (copyBlock<float>): rows x cols, one warp per column.
+dgt_status launch_strided_copy_f32(dgt_context* h, const float* src, float* dst, int64_t ldS, int64_t ldD,
+                                   int64_t rows, int64_t cols) {
+    if (rows <= 0 || cols <= 0) return DGT_SUCCESS;
+    CopyParams<float>& P = t_copy_f32;
+    P.ncopies = 1;
+    P.total_runs = cols;
+    P.d[0] = CopyDesc<float>{src, dst, ldS, ldD, rows, cols, 0};
+    strided_copy_kernel<float><<<layout_grid(h, cols), LAYOUT_THREADS, 0, h->stream>>>(P);
+    DGT_LAUNCH_CHECK(h, "strided_copy_kernel<float>");
     return DGT_SUCCESS;
 }
 

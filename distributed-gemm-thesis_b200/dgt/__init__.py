@@ -86,6 +86,7 @@ SIGNATURES = [
     ("dgt_pack_cannon2d", _c_i32, [_vp, _c_i64, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("dgt_unpack_cannon2d", _c_i32, [_vp, _c_i64, _c_i32, _vp, _vp]),
     ("dgt_copy_block", _c_i32, [_vp, _c_i64, _c_i64, _vp, _vp, _c_i64, _c_i64, _c_i32]),
+    ("dgt_copy_block_f32", _c_i32, [_vp, _c_i64, _c_i64, _vp, _vp, _c_i64, _c_i64, _c_i32]),
     ("dgt_set_tuning", _c_i32, [_vp, _c_i32, _c_i32]),
     ("dgt_get_tuning", _c_i32, [_vp, _c_i32, ctypes.POINTER(_c_i32)]),
     ("dgt_autotune_dgemm", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _vp, _c_i64, _vp,
@@ -282,6 +283,10 @@ class Handle:
 
     def copy_block(self, rows, cols, src, dst, ldS, ldD, col_major=True):
         self._check(self.lib.dgt_copy_block(self.h, rows, cols, _vp(src), _vp(dst), ldS, ldD, int(col_major)))
+
+    def copy_block_f32(self, rows, cols, src, dst, ldS, ldD, col_major=True):
+        """copyBlock<float>: the same strided copy on 4-byte elements."""
+        self._check(self.lib.dgt_copy_block_f32(self.h, rows, cols, _vp(src), _vp(dst), ldS, ldD, int(col_major)))
 
 
 def numroc(n, nb, iproc, isrproc, nprocs) -> int:

@@ -44,6 +44,18 @@ class Context {
     dgt_handle_t h_ = nullptr;
 };
 
+// copyBlock<T> for the reference's two instantiations, double and float
+// (src/Transfers/sharedTransfers.cpp:29-63, :87-88): one strided copy on the handle's
+// stream.  Unlike the reference, a null pointer is an error rather than a printed no-op.
+inline void copyBlock(dgt_handle_t h, long long rows, long long columns, const double* src, double* dst,
+                      long long ldSource, long long ldDestination, bool columnMajor = true) {
+    check(h, dgt_copy_block(h, rows, columns, src, dst, ldSource, ldDestination, columnMajor));
+}
+inline void copyBlock(dgt_handle_t h, long long rows, long long columns, const float* src, float* dst,
+                      long long ldSource, long long ldDestination, bool columnMajor = true) {
+    check(h, dgt_copy_block_f32(h, rows, columns, src, dst, ldSource, ldDestination, columnMajor));
+}
+
 // ScaLAPACK block-cyclic layout of an M x N matrix on a dRow x dCol grid (row-major ranks).
 class pblasDecomposer {
   public:
