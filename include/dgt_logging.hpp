@@ -18,10 +18,10 @@
 #include <unistd.h>
 
 #include <climits>
+#include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
-#include <vector>
 
 namespace dgt {
 
@@ -82,21 +82,31 @@ inline std::string machineName() {
 #endif
 }
 
-// One row of the 2.5D Cannon log, times in seconds, with the reference's printf format
-// ("%s,%lld,%lld,%lld,%d,%d,%d,%d,%d,%lf,%lf,%lf,%lf,%s,%lf,%lf\n").
+// printf into a string of exactly the needed length.
+__attribute__((format(printf, 1, 2))) inline std::string formatString(const char* fmt, ...) {
+    va_list ap, ap2;
+    va_start(ap, fmt);
+    va_copy(ap2, ap);
+    const int n = std::vsnprintf(nullptr, 0, fmt, ap);
+    va_end(ap);
+    std::string out;
+    if (n > 0) {
+        out.resize(size_t(n) + 1);
+        std::vsnprintf(&out[0], out.size(), fmt, ap2);
+        out.resize(size_t(n));
+    }
+    va_end(ap2);
+    return out;
+}
+
+// One row of the 2.5D Cannon log, times in seconds, with the reference's printf format.
 inline std::string cannonCsvLine(const char* algo, long long M, long long N, long long K, int totalNodes,
                                  int totalGPUs, int dRow, int dCol, int stackSize, double decompositionTime,
                                  double executionTime, double gatherTime, double gflops, const char* dataLocation,
                                  double communicationTime, double gemmCallTime) {
-    const char* fmt = "%s,%lld,%lld,%lld,%d,%d,%d,%d,%d,%lf,%lf,%lf,%lf,%s,%lf,%lf\n";
-    int n = std::snprintf(nullptr, 0, fmt, algo, M, N, K, totalNodes, totalGPUs, dRow, dCol, stackSize,
-                          decompositionTime, executionTime, gatherTime, gflops, dataLocation, communicationTime,
-                          gemmCallTime);
-    if (n < 0) return std::string();
-    std::vector<char> buf(size_t(n) + 1);
-    std::snprintf(buf.data(), buf.size(), fmt, algo, M, N, K, totalNodes, totalGPUs, dRow, dCol, stackSize,
-                  decompositionTime, executionTime, gatherTime, gflops, dataLocation, communicationTime, gemmCallTime);
-    return std::string(buf.data(), size_t(n));
+    return formatString("%s,%lld,%lld,%lld,%d,%d,%d,%d,%d,%lf,%lf,%lf,%lf,%s,%lf,%lf\n", algo, M, N, K, totalNodes,
+                        totalGPUs, dRow, dCol, stackSize, decompositionTime, executionTime, gatherTime, gflops,
+                        dataLocation, communicationTime, gemmCallTime);
 }
 
 }  // namespace dgt

@@ -23,3 +23,19 @@ def zeros(rows, cols, dtype=None):
 
 def ptr(t):
     return t.data_ptr()
+
+
+def check_cannon_driver_logs(logs):
+    """CSV rows that tests/cpp/driver_test.cpp makes the 2.5D Cannon drivers write, read the
+    way the thesis notebooks read them (pandas.read_csv, header=0)."""
+    import pandas as pd
+
+    full = pd.read_csv(logs / "DGEMM_execution_logs-FullOffload_GEMM-b200test-2.5DCANNON-dgt.csv", header=0)
+    pre = pd.read_csv(logs / "DGEMM_execution_logs-PreDistributed_GEMM-b200test-2.5DCANNON-dgt.csv", header=0)
+    assert list(full["M"]) == [64, 64, 96] and list(full["StackSize"]) == [1, 1, 2]
+    assert list(pre["M"]) == [96] and list(pre["dRow"]) == [4]
+    for df in (full, pre):
+        assert (df["Algo"] == "2.5D CANNON dgt").all()
+        assert (df["DataLocation"] == "devices").all() and (df["TotalGPUs"] == 1).all()
+        assert (df["ExecutionTime"] > 0).all() and (df["GFlops"] > 0).all()
+        assert (df["GemmCallTime"] == df["ExecutionTime"]).all() and (df["CommunicationTime"] == 0).all()

@@ -4,6 +4,7 @@ import os
 import subprocess
 
 import pytest
+from devutil import check_cannon_driver_logs
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -26,8 +27,6 @@ def test_cpp_cannon_drivers_and_logs(tmp_path):
     """include/dgt_drivers.hpp: fullOffloadSumma25Dgemm / preDistributedSumma25Dgemm results
     against host triple loops (tests/cpp/driver_test.cpp), then their CSV rows read back
     the way the thesis notebooks read them."""
-    import pandas as pd
-
     lib = os.path.join(ROOT, "distributed-gemm-thesis_b200", "lib")
     exe = str(tmp_path / "driver_test")
     cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
@@ -41,12 +40,4 @@ def test_cpp_cannon_drivers_and_logs(tmp_path):
     assert out.returncode == 0, out.stdout + out.stderr
     assert "ALL OK" in out.stdout
 
-    full = pd.read_csv(logs / "DGEMM_execution_logs-FullOffload_GEMM-b200test-2.5DCANNON-dgt.csv", header=0)
-    pre = pd.read_csv(logs / "DGEMM_execution_logs-PreDistributed_GEMM-b200test-2.5DCANNON-dgt.csv", header=0)
-    assert list(full["M"]) == [64, 64, 96] and list(full["StackSize"]) == [1, 1, 2]
-    assert list(pre["M"]) == [96] and list(pre["dRow"]) == [4]
-    for df in (full, pre):
-        assert (df["Algo"] == "2.5D CANNON dgt").all()
-        assert (df["DataLocation"] == "devices").all() and (df["TotalGPUs"] == 1).all()
-        assert (df["ExecutionTime"] > 0).all() and (df["GFlops"] > 0).all()
-        assert (df["GemmCallTime"] == df["ExecutionTime"]).all() and (df["CommunicationTime"] == 0).all()
+    check_cannon_driver_logs(logs)
