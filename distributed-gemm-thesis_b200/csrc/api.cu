@@ -663,6 +663,57 @@ dgt_status dgt_unpack_block_cyclic(dgt_handle_t h, int64_t M, int64_t N, int64_t
     return launch_block_cyclic(h, false, M, N, mb, nb, p, q, global, ldg, (double* const*)locals, lld);
 }
 
+// Device alias of the page-locked host range [p, p + bytes), or nullptr when either end is
+// pageable, device memory or not mapped into the device's address space.  Both ends must
+// sit in mappings with the same host-to-device offset (one allocation or registration).
+static const void* host_range_alias(const void* p, size_t bytes) {
+    const char* first = static_cast<const char*>(p);
+    const char* last = first + bytes - 1;
+    cudaPointerAttributes a0{}, a1{};
+    if (cudaPointerGetAttributes(&a0, first) != cudaSuccess || cudaPointerGetAttributes(&a1, last) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a0.type != cudaMemoryTypeHost || a1.type != cudaMemoryTypeHost || !a0.devicePointer || !a1.devicePointer)
+        return nullptr;
+    if (static_cast<const char*>(a0.devicePointer) - first != static_cast<const char*>(a1.devicePointer) - last)
+        return nullptr;
+    return a0.devicePointer;
+}
+
+// Block-cyclic scatter / gather with the global matrix in page-locked host memory: the
+// block_cyclic kernel reads (or writes) the host matrix through its device mapping, so the
+// host-device transfer and the permutation are one pass and no device copy of the global
+// matrix is made (the reference's full-offload scatter from a host matrix,
+// src/Wrappers/cuBLASMp/cuBLASMpWrapped.cpp:633-636, and decompose2D from host A, B, C,
+// src/25DCannon.cpp:413-414).
+static dgt_status cyclic_host(dgt_context* h, bool to_local, int64_t M, int64_t N, int64_t mb, int64_t nb, int p,
+                              int q, const double* global, int64_t ldg, double* const* locals, const int64_t* lld) {
+    dgt_status st = check_cyclic(h, M, N, mb, nb, p, q, global, ldg, locals, lld);
+    if (st != DGT_SUCCESS) return st;
+    if (M == 0 || N == 0) return DGT_SUCCESS;
+    const size_t bytes = ((size_t)(N - 1) * (size_t)ldg + (size_t)M) * sizeof(double);
+    const void* alias = host_range_alias(global, bytes);
+    if (!alias)
+        return fail(h, DGT_ERROR_INVALID_VALUE,
+                    "global matrix is not page-locked host memory mapped for the device (cudaHostAlloc / cudaHostRegister)");
+    return launch_block_cyclic(h, to_local, M, N, mb, nb, p, q, (double*)alias, ldg, locals, lld);
+}
+
+dgt_status dgt_pack_block_cyclic_host(dgt_handle_t h, int64_t M, int64_t N, int64_t mb, int64_t nb, int32_t p,
+                                      int32_t q, const double* global, int64_t ldg, double* const* locals,
+                                      const int64_t* lld) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    return cyclic_host(h, true, M, N, mb, nb, p, q, global, ldg, locals, lld);
+}
+
+dgt_status dgt_unpack_block_cyclic_host(dgt_handle_t h, int64_t M, int64_t N, int64_t mb, int64_t nb, int32_t p,
+                                        int32_t q, double* global, int64_t ldg, const double* const* locals,
+                                        const int64_t* lld) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    return cyclic_host(h, false, M, N, mb, nb, p, q, global, ldg, (double* const*)locals, lld);
+}
+
 // One strided copy in the reference's convention: copyBlock swaps rows and columns
 // when not column-major (sharedTransfers.cpp:43-44), as does MPI_Type_vector's use.
 static HostCopy mk_copy(int64_t rows, int64_t cols, const double* src, int64_t ldS, double* dst, int64_t ldD,

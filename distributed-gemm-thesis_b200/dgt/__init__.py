@@ -81,6 +81,10 @@ SIGNATURES = [
     ("dgt_pack_block_cyclic", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _c_i64, _vp, _vp]),
     ("dgt_unpack_block_cyclic", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _c_i64, _vp,
                                          _vp]),
+    ("dgt_pack_block_cyclic_host", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _c_i64, _vp,
+                                            _vp]),
+    ("dgt_unpack_block_cyclic_host", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _c_i64,
+                                              _vp, _vp]),
     ("dgt_pack_block2d", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("dgt_unpack_block2d", _c_i32, [_vp, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _vp]),
     ("dgt_pack_cannon2d", _c_i32, [_vp, _c_i64, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -266,6 +270,15 @@ class Handle:
     def unpack_block_cyclic(self, M, N, mb, nb, p, q, G, ldg, locals_, lld):
         self._check(self.lib.dgt_unpack_block_cyclic(self.h, M, N, mb, nb, p, q, _vp(G), ldg, _ptrs(locals_),
                                                      _i64s(lld)))
+
+    def pack_block_cyclic_host(self, M, N, mb, nb, p, q, G, ldg, locals_, lld):
+        """Scatter from a page-locked host global matrix in one pass (no device copy of G)."""
+        self._check(self.lib.dgt_pack_block_cyclic_host(self.h, M, N, mb, nb, p, q, _vp(G), ldg, _ptrs(locals_),
+                                                        _i64s(lld)))
+
+    def unpack_block_cyclic_host(self, M, N, mb, nb, p, q, G, ldg, locals_, lld):
+        self._check(self.lib.dgt_unpack_block_cyclic_host(self.h, M, N, mb, nb, p, q, _vp(G), ldg, _ptrs(locals_),
+                                                          _i64s(lld)))
 
     def pack_block2d(self, M, N, K, P, col_major, A, B, C, lA, lB, lC):
         self._check(self.lib.dgt_pack_block2d(self.h, M, N, K, P, int(col_major), _vp(A), _vp(B), _vp(C), _ptrs(lA),

@@ -134,42 +134,3 @@ def test_copy_block(h, rows, cols, ldS, ldD, cm):
         want[j * ldD:j * ldD + r] = src[j * ldS:j * ldS + r]
     assert np.array_equal(dd.cpu().numpy(), want)
 
-
-# (rows, cols, ldS, ldD, source offset, destination offset in floats, column-major): the
-# offsets put the runs in every 16-byte phase, same and different on the two sides, so the
-# head / float4 body / tail split and the scalar path are all exercised.
-@pytest.mark.parametrize("rows,cols,ldS,ldD,so,do_,cm", [
-    (5, 7, 9, 6, 0, 0, True), (67, 5, 70, 68, 1, 3, True), (129, 4, 131, 133, 2, 2, True),
-    (3, 300, 3, 5, 1, 1, True), (64, 3, 64, 64, 3, 3, True), (3, 64, 70, 65, 0, 2, False),
-    (1, 1, 1, 1, 0, 0, True), (1031, 2, 1033, 1037, 1, 1, True), (2, 2, 2, 2, 3, 3, True),
-])
-def test_copy_block_f32(h, rows, cols, ldS, ldD, so, do_, cm):
-    """copyBlock<float>: bit-exact strided copy, the destination's other elements untouched."""
-    import torch
-
-    r, c = (rows, cols) if cm else (cols, rows)
-    rng = np.random.default_rng(rows * 7 + cols)
-    src = rng.standard_normal(so + ldS * c).astype(np.float32)
-    dst0 = rng.standard_normal(do_ + ldD * c).astype(np.float32)
-    ds, dd = torch.from_numpy(src).cuda(), torch.from_numpy(dst0.copy()).cuda()
-    h.copy_block_f32(rows, cols, ptr(ds) + 4 * so, ptr(dd) + 4 * do_, ldS, ldD, cm)
-    torch.cuda.synchronize()
-    h.check_device()
-    want = dst0.copy()
-    for j in range(c):
-        want[do_ + j * ldD:do_ + j * ldD + r] = src[so + j * ldS:so + j * ldS + r]
-    assert np.array_equal(dd.cpu().numpy().view(np.uint32), want.view(np.uint32))
-
-
-def test_copy_block_f32_rejects_bad_arguments(h):
-    """Host-side checks, before any launch: misaligned pointer, short leading dimension."""
-    import torch
-
-    x = torch.zeros(64, dtype=torch.float32, device="cuda")
-    with pytest.raises(dgt.DgtError) as e:
-        h.copy_block_f32(4, 4, ptr(x) + 2, ptr(x) + 32, 4, 4)
-    assert e.value.status == 1
-    with pytest.raises(dgt.DgtError) as e:
-        h.copy_block_f32(8, 2, ptr(x), ptr(x) + 128, 4, 8)
-    assert e.value.status == 1
-    h.copy_block_f32(0, 5, ptr(x), ptr(x), 1, 1)  # empty: no launch, no error

@@ -1,0 +1,146 @@
+"""GPU checks of the transfers at the edges of the hot path, through the C ABI:
+ * the block-cyclic scatter / gather with the global matrix in page-locked host memory
+   (dgt_pack_block_cyclic_host / dgt_unpack_block_cyclic_host), bit-exact against the
+   device-global entry points on the same inputs, and pageable memory refused;
+ * copyBlock<float> (dgt_copy_block_f32), bit-exact;
+ * the reference-shaped 2.5D Cannon benchmark drivers and their CSV logs
+   (include/dgt_drivers.hpp, tests/cpp/driver_test.cpp)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import dgt
+import oracle as O
+from devutil import check_cannon_driver_logs, dev, ptr
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def h():
+    with dgt.Handle() as handle:
+        yield handle
+
+
+def _pinned_global(G, ldg, fill):
+    """Column-major M x N matrix G in a page-locked host buffer with leading dimension ldg
+    (rows M..ldg-1 of every column hold `fill`), as a torch tensor and its address."""
+    import torch
+
+    M, N = G.shape
+    buf = np.full((N, ldg), fill, dtype=np.float64)
+    buf[:, :M] = G.T
+    t = torch.from_numpy(buf).pin_memory()
+    return t, t.data_ptr()
+
+
+def _locals(M, N, mb, nb, p, q):
+    import torch
+
+    rows = [dgt.numroc(M, mb, r // q, 0, p) for r in range(p * q)]
+    cols = [dgt.numroc(N, nb, r % q, 0, q) for r in range(p * q)]
+    lld = [max(x, 1) for x in rows]
+    locs = [torch.full((max(c, 1), l), -3.0, dtype=torch.float64, device="cuda") for c, l in zip(cols, lld)]
+    return locs, lld
+
+
+@pytest.mark.parametrize("M,N,mb,nb,p,q,ldg", [(300, 250, 32, 24, 2, 3, 300), (517, 389, 64, 64, 4, 4, 530),
+                                               (40, 70, 64, 16, 3, 2, 41)])
+def test_block_cyclic_from_host_equals_device_path(h, M, N, mb, nb, p, q, ldg):
+    import torch
+
+    G = O.uniform((M, N), M + N)
+    tG, pG = _pinned_global(G, ldg, 7.0)
+    # device path on the same matrix
+    dG = dev(np.asfortranarray(tG.numpy().T))  # ldg x N, column-major
+    want, lld = _locals(M, N, mb, nb, p, q)
+    h.pack_block_cyclic(M, N, mb, nb, p, q, ptr(dG), ldg, [ptr(t) for t in want], lld)
+    got, _ = _locals(M, N, mb, nb, p, q)
+    h.pack_block_cyclic_host(M, N, mb, nb, p, q, pG, ldg, [ptr(t) for t in got], lld)
+    torch.cuda.synchronize()
+    h.check_device()
+    for a, b in zip(got, want):
+        assert torch.equal(a.view(torch.int64), b.view(torch.int64))
+    # gather back into a second pinned buffer: the matrix, padding rows untouched
+    tB, pB = _pinned_global(np.zeros((M, N)), ldg, -9.0)
+    h.unpack_block_cyclic_host(M, N, mb, nb, p, q, pB, ldg, [ptr(t) for t in got], lld)
+    torch.cuda.synchronize()
+    h.check_device()
+    back = tB.numpy()
+    assert np.array_equal(back[:, :M].T, G)
+    assert (back[:, M:] == -9.0).all()
+
+
+def test_block_cyclic_host_refuses_pageable(h):
+    M, N, mb, nb, p, q = 64, 48, 16, 16, 2, 2
+    G = np.asfortranarray(O.uniform((M, N), 3))
+    locs, lld = _locals(M, N, mb, nb, p, q)
+    with pytest.raises(dgt.DgtError) as e:
+        h.pack_block_cyclic_host(M, N, mb, nb, p, q, G.ctypes.data, M, [ptr(t) for t in locs], lld)
+    assert e.value.status == 1
+    with pytest.raises(dgt.DgtError) as e:
+        h.unpack_block_cyclic_host(M, N, mb, nb, p, q, G.ctypes.data, M, [ptr(t) for t in locs], lld)
+    assert e.value.status == 1
+
+
+# (rows, cols, ldS, ldD, source offset, destination offset in floats, column-major): the
+# offsets put the runs in every 16-byte phase, same and different on the two sides, so the
+# head / float4 body / tail split and the scalar path are all exercised.
+@pytest.mark.parametrize("rows,cols,ldS,ldD,so,do_,cm", [
+    (5, 7, 9, 6, 0, 0, True), (67, 5, 70, 68, 1, 3, True), (129, 4, 131, 133, 2, 2, True),
+    (3, 300, 3, 5, 1, 1, True), (64, 3, 64, 64, 3, 3, True), (3, 64, 70, 65, 0, 2, False),
+    (1, 1, 1, 1, 0, 0, True), (1031, 2, 1033, 1037, 1, 1, True), (2, 2, 2, 2, 3, 3, True),
+])
+def test_copy_block_f32(h, rows, cols, ldS, ldD, so, do_, cm):
+    """copyBlock<float>: bit-exact strided copy, the destination's other elements untouched."""
+    import torch
+
+    r, c = (rows, cols) if cm else (cols, rows)
+    rng = np.random.default_rng(rows * 7 + cols)
+    src = rng.standard_normal(so + ldS * c).astype(np.float32)
+    dst0 = rng.standard_normal(do_ + ldD * c).astype(np.float32)
+    ds, dd = torch.from_numpy(src).cuda(), torch.from_numpy(dst0.copy()).cuda()
+    h.copy_block_f32(rows, cols, ptr(ds) + 4 * so, ptr(dd) + 4 * do_, ldS, ldD, cm)
+    torch.cuda.synchronize()
+    h.check_device()
+    want = dst0.copy()
+    for j in range(c):
+        want[do_ + j * ldD:do_ + j * ldD + r] = src[so + j * ldS:so + j * ldS + r]
+    assert np.array_equal(dd.cpu().numpy().view(np.uint32), want.view(np.uint32))
+
+
+def test_copy_block_f32_rejects_bad_arguments(h):
+    """Host-side checks, before any launch: misaligned pointer, short leading dimension."""
+    import torch
+
+    x = torch.zeros(64, dtype=torch.float32, device="cuda")
+    with pytest.raises(dgt.DgtError) as e:
+        h.copy_block_f32(4, 4, ptr(x) + 2, ptr(x) + 32, 4, 4)
+    assert e.value.status == 1
+    with pytest.raises(dgt.DgtError) as e:
+        h.copy_block_f32(8, 2, ptr(x), ptr(x) + 128, 4, 8)
+    assert e.value.status == 1
+    h.copy_block_f32(0, 5, ptr(x), ptr(x), 1, 1)  # empty: no launch, no error
+
+
+def test_cpp_cannon_drivers_and_logs(tmp_path):
+    """include/dgt_drivers.hpp: fullOffloadSumma25Dgemm / preDistributedSumma25Dgemm results
+    against host triple loops (tests/cpp/driver_test.cpp), then their CSV rows read back
+    the way the thesis notebooks read them."""
+    lib = os.path.join(ROOT, "distributed-gemm-thesis_b200", "lib")
+    exe = str(tmp_path / "driver_test")
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    subprocess.run(["g++", "-std=c++17", "-O2", os.path.join(ROOT, "tests", "cpp", "driver_test.cpp"),
+                    "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"), "-L", lib, "-ldgt",
+                    "-L", os.path.join(cuda, "lib64"), "-lcudart", f"-Wl,-rpath,{lib}", "-o", exe], check=True)
+    logs = tmp_path / "logs"
+    logs.mkdir()
+    out = subprocess.run([exe, str(logs)], capture_output=True, text=True, timeout=300)
+    print(out.stdout)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "ALL OK" in out.stdout
+
+    check_cannon_driver_logs(logs)
