@@ -21,8 +21,11 @@
 //                      reduction is a kernel of the multiply and counts in GemmCallTime
 //   GemmCallTime       = ExecutionTime
 //
-// Every run applies C <- alpha op(A) op(B) + beta C to the same tiles, as the reference's
-// run loop does.  Errors throw dgt::Error (the reference exits).
+// Every run applies C <- alpha op(A) op(B) + beta C to the tiles as packed.  The reference's
+// runs after the first start from the A and B tiles its previous multiply left skewed and
+// rotated (the shifts replace the tiles in place: src/25DCannon.cpp:305-307, :341-344), so
+// only its first run computes A B; the work per run, and so the timings, are the same.
+// Errors throw dgt::Error (the reference exits).
 #ifndef DGT_DRIVERS_HPP
 #define DGT_DRIVERS_HPP
 

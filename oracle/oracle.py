@@ -209,6 +209,8 @@ class _Ref:
         L.ref_cannon_reorder.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_void_p]
         L.ref_cannon_fulloffload.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, _dp, _dp, _dp]
+        L.ref_cannon_fulloffload_logged.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, ctypes.c_int]
         L.ref_cannon_trace.argtypes = [ctypes.c_int, ctypes.c_int, _ip]
         L.ref_set_dgemm.argtypes = [ctypes.c_void_p]
         self._blas = None
@@ -308,6 +310,16 @@ class _Ref:
         A, B = (np.array(x, dtype=np.float64, order="F") for x in (A, B))
         C = np.array(C, dtype=np.float64, order="F")
         self._check(self.L.ref_cannon_fulloffload(M, p, c, alpha, beta, _ptr(A), _ptr(B), _ptr(C)))
+        return C
+
+    def cannon_fulloffload_logged(self, log_dir, A, B, C, p, c, alpha, beta, runs):
+        """The reference's fullOffloadSumma25Dgemm with logging on, run in log_dir: returns C
+        after `runs` runs; the reference's own CSV log is left in log_dir."""
+        M = A.shape[0]
+        A, B = (np.array(x, dtype=np.float64, order="F") for x in (A, B))
+        C = np.array(C, dtype=np.float64, order="F")
+        self._check(self.L.ref_cannon_fulloffload_logged(str(log_dir).encode(), M, p, c, alpha, beta, _ptr(A), _ptr(B),
+                                                         _ptr(C), runs))
         return C
 
     def cannon_trace(self, p, c):

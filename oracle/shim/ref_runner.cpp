@@ -3,7 +3,10 @@
 // virtual rank.  Used only by tests/ (golden fixtures, pinning the restatement) and by
 // bench.py's CPU reference arm.  Every entry returns 0 on success, -1 on failure
 // (message via ref_last_error()).
+#include <unistd.h>
+
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <mutex>
@@ -177,6 +180,34 @@ extern "C" int ref_cannon_fulloffload(long long M, int p, int c, double alpha, d
         d.multiply('N', 'N', A, B, C, alpha, beta);
         d.reorderMatrix(0, C, d.localC);
     });
+}
+
+// The reference's full-offload driver itself, logging on (fullOffloadSumma25Dgemm,
+// src/25DCannon.cpp:392-459): run in `dir`, where its own createLogCsv / writeLineToFile
+// (src/Utilities/Logging.cpp) create or extend its CSV log, one row per run.  Its node count
+// comes from SLURM_JOB_NUM_NODES, set to 1 here when absent (the reference reads it
+// unchecked).  The working directory is the process's, so it is restored before returning.
+extern "C" int ref_cannon_fulloffload_logged(const char* dir, long long M, int p, int c, double alpha, double beta,
+                                             double* A, double* B, double* C, int runs) {
+    std::lock_guard<std::mutex> g(g_run_mutex);
+    if (!cannon_guard(M, p, c) || runs < 1 || !dir) {
+        g_err = "Cannon needs M % p == 0, p % c == 0, runs >= 1 and a directory";
+        return -1;
+    }
+    setenv("SLURM_JOB_NUM_NODES", "1", 0);
+    char old[4096];
+    if (!getcwd(old, sizeof(old)) || chdir(dir) != 0) {
+        g_err = "cannot enter the log directory";
+        return -1;
+    }
+    int rc = run_job(p * p * c, [&](int) {
+        fullOffloadSumma25Dgemm('N', 'N', M, M, M, alpha, A, M, B, M, beta, C, M, p, p, c, runs, true, true);
+    });
+    if (chdir(old) != 0 && rc == 0) {
+        g_err = "cannot return to the working directory";
+        rc = -1;
+    }
+    return rc;
 }
 
 // Step trace of the Cannon schedule: for every world rank and every local GEMM it

@@ -73,3 +73,59 @@ def test_drivers_header_compiles_and_links(tmp_path):
                     "-I", INC, "-I", os.path.join(CUDA, "include"), "-L", lib, "-ldgt",
                     "-L", os.path.join(CUDA, "lib64"), "-lcudart", f"-Wl,-rpath,{lib}", "-o", exe], check=True)
     assert os.path.getsize(exe) > 0
+
+
+def _csv_format(tmp_path):
+    exe = str(tmp_path / "csv_format")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", os.path.join(ROOT, "tests", "cpp", "csv_format.cpp"),
+                    "-I", INC, "-o", exe], check=True)
+    return lambda *args, stdin=None: subprocess.run([exe, *args], input=stdin, capture_output=True, text=True,
+                                                    timeout=60, check=True).stdout
+
+
+def test_logger_matches_reference_logging(tmp_path):
+    """Against the reference's own fullOffloadSumma25Dgemm with logging on (compiled from its
+    sources into oracle/_ref with MACHINE_NAME "oracle"): same file name, header written
+    once across two calls, every row it wrote printed identically by dgt::cannonCsvLine from
+    the row's own values, and the same file after createLogCsv on a log whose first line is
+    another header."""
+    import numpy as np
+
+    import oracle as O
+
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    fmt = _csv_format(tmp_path)
+    R = O.ref()
+    R.use_naive()
+    name = fmt("name", "full", "oracle", "cuBLAS").strip()
+    assert name == "DGEMM_execution_logs-FullOffload_GEMM-oracle-2.5DCANNON-cuBLAS.csv"
+
+    d1 = tmp_path / "ref1"
+    d1.mkdir()
+    A, B, C = (O.uniform((16, 16), s) for s in (1, 2, 3))
+    out = R.cannon_fulloffload_logged(d1, A, B, C, 2, 1, 1.0, 0.0, 2)
+    R.cannon_fulloffload_logged(d1, A, B, C, 4, 2, 1.0, 0.0, 1)
+    assert sorted(os.listdir(d1)) == [name]
+    text = (d1 / name).read_text()
+    lines = text.splitlines(keepends=True)
+    assert lines[0] == fmt("header")
+    assert text.count("Algo,") == 1 and len(lines) == 4
+    assert fmt("rows", stdin="".join(lines[1:])) == "".join(lines[1:])
+    # the reference's runs after the first start from tiles its previous multiply left
+    # rotated, so only a single run gives A B (the drivers here multiply the original tiles
+    # on every run)
+    single = R.cannon_fulloffload_logged(d1, A, B, C, 2, 1, 1.0, 0.0, 1)
+    assert np.abs(single - A @ B).max() < 1e-12 and np.abs(out - A @ B).max() > 1e-3
+
+    foreign = "Algo,M,N,K\nx,1,2,3\n"
+    d2 = tmp_path / "ref2"
+    d2.mkdir()
+    (d2 / name).write_text(foreign)
+    R.cannon_fulloffload_logged(d2, A, B, C, 2, 1, 1.0, 0.0, 1)
+    ours = tmp_path / "ours.csv"
+    ours.write_text(foreign)
+    fmt("open", str(ours))
+    ref_text, our_text = (d2 / name).read_text(), ours.read_text()
+    assert ref_text.startswith(our_text) and our_text == foreign + fmt("header")
+    assert ref_text[len(our_text):].count("\n") == 1
