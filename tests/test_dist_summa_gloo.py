@@ -1,0 +1,170 @@
+"""SUMMA across processes (dgt.dist.DistSumma) as four gloo ranks on the CPU: the step
+schedule -- panel owners, row and column broadcasts on the process-grid sub-groups, the
+ragged last panel, beta applied once, lookahead buffers -- with a host double standing in
+for the rank-local operations (on a GPU they are dgt_dgemm and dgt_copy_block).  Each rank
+starts from its block-cyclic locals (a scatter that equals the oracle's, which is pinned to
+the reference's pblasDecomposer, and that also covers grids leaving a process row empty);
+the gathered C must equal the host FP64 GEMM within 1e-13 (relative Frobenius; summation
+order differs)."""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# (p, q, mb, nb, kb, M, N, K, alpha, beta)
+CASES = [
+    (2, 2, 16, 24, 20, 150, 170, 90, 1.5, -0.5),   # ragged everywhere, 5 panels (last 10 wide)
+    (1, 4, 32, 16, 8, 64, 100, 77, 1.0, 0.0),      # one process row: no column broadcasts
+    (4, 1, 16, 32, 12, 40, 50, 61, -2.0, 1.0),     # process row 3 owns no rows of A or C
+    (2, 2, 16, 16, 16, 48, 40, 0, 1.0, 0.25),      # K = 0: C = beta C
+]
+
+
+class HostOps:
+    """Rank-local operations on CPU tensors (the test double of dgt.dist.DgtOps)."""
+
+    def empty(self, shape, like):
+        import torch
+
+        return torch.empty(shape, dtype=torch.float64)
+
+    def pack_rows(self, src, r0, rows, dst):
+        dst.copy_(src[:, r0:r0 + rows])
+
+    def gemm(self, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+        c = C.numpy()[:n, :m]  # column-major m x n view of C's storage
+        prod = A.numpy()[:k, :m].T @ B.numpy()[:n, :k].T if k > 0 else 0.0
+        c[...] = (alpha * prod + beta * c.T).T
+
+
+def _scatter(G, mb, nb, p, q):
+    """Block-cyclic locals of every rank (rank r = i q + j), empty ranks included."""
+    M, N = G.shape
+    out = []
+    for r in range(p * q):
+        i, j = r // q, r % q
+        rows = [x for b in range(i, -(-M // mb), p) for x in range(b * mb, min(M, (b + 1) * mb))]
+        cols = [x for b in range(j, -(-N // nb), q) for x in range(b * nb, min(N, (b + 1) * nb))]
+        out.append(np.asfortranarray(G[np.ix_(rows, cols)]))
+    return out
+
+
+def _gather(locs, M, N, mb, nb, p, q):
+    G = np.full((M, N), np.nan)
+    for r, loc in enumerate(locs):
+        i, j = r // q, r % q
+        rows = [x for b in range(i, -(-M // mb), p) for x in range(b * mb, min(M, (b + 1) * mb))]
+        cols = [x for b in range(j, -(-N // nb), q) for x in range(b * nb, min(N, (b + 1) * nb))]
+        G[np.ix_(rows, cols)] = loc
+    return G
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _local_tensor(x):
+    import torch
+
+    rows, cols = x.shape
+    t = torch.zeros((max(cols, 1), max(rows, 1)), dtype=torch.float64)
+    if rows and cols:
+        t.copy_(torch.from_numpy(np.ascontiguousarray(np.asfortranarray(x).T)))
+    return t
+
+
+def _rank_main(rank, world, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    for sub in ("", "oracle", "distributed-gemm-thesis_b200", "tests"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    import oracle as O
+    from dgt.dist import DistSumma
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
+            A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
+            la = _scatter(A, mb, kb, p, q)[rank]
+            lb = _scatter(B, kb, nb, p, q)[rank]
+            lc = _scatter(C, mb, nb, p, q)[rank]
+            tA, tB, tC = _local_tensor(la), _local_tensor(lb), _local_tensor(lc)
+            S = DistSumma(p, q, mb, nb, kb, ops=HostOps())
+            assert S.local_shapes(M, N, K) == (la.shape, lb.shape, lc.shape)
+            S.multiply(M, N, K, alpha, tA, tB, beta, tC)
+            rows, cols = lc.shape
+            got = tC.numpy()[:cols, :rows].T.copy() if rows and cols else np.zeros((rows, cols))
+            out.put((n_case, rank, got))
+        dist.barrier()
+    except Exception:
+        import traceback
+
+        out.put((-1, rank, traceback.format_exc()))
+        raise
+    finally:
+        dist.destroy_process_group()
+
+
+def test_dist_summa_four_gloo_ranks():
+    import torch.multiprocessing as mp
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    world = 4
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, out)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    results = {}
+    for _ in range(world * len(CASES)):
+        n_case, rank, got = out.get(timeout=180)
+        if n_case < 0:
+            for pr in procs:
+                pr.join(timeout=30)
+            pytest.fail(f"rank {rank} failed:\n{got}")
+        results[(n_case, rank)] = got
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
+        A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
+        G = _gather([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
+        ref = O.dgemm(A, B, alpha, beta, C) if K > 0 else beta * C
+        assert O.rel_errors(G, ref)[1] <= 1e-13, (n_case, O.rel_errors(G, ref))
+
+
+def test_scatter_helper_matches_oracle():
+    """The test's block-cyclic scatter equals the oracle's (pinned to the reference's
+    pblasDecomposer) wherever the oracle accepts the grid, and gather inverts it."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    for (M, N, mb, nb, p, q) in [(150, 90, 16, 20, 2, 2), (64, 77, 32, 8, 1, 4), (170, 61, 24, 12, 4, 1)]:
+        G = O.uniform((M, N), M)
+        mine = _scatter(G, mb, nb, p, q)
+        for a, b in zip(mine, O.orc().pblas_scatter(G, mb, nb, p, q)):
+            assert np.array_equal(a, b)
+        assert np.array_equal(_gather(mine, M, N, mb, nb, p, q), G)
+    G = O.uniform((40, 50), 1)
+    assert _scatter(G, 16, 32, 4, 1)[3].shape == (0, 50)  # a process row without rows
+
+
+def test_dist_summa_needs_matching_world():
+    """Outside an initialised process group, construction fails."""
+    sys.path.insert(0, os.path.join(ROOT, "distributed-gemm-thesis_b200"))
+    from dgt.dist import DistSumma
+
+    with pytest.raises(RuntimeError):
+        DistSumma(2, 2, 16, 16, 16)

@@ -4,7 +4,9 @@
    device-global entry points on the same inputs, and pageable memory refused;
  * copyBlock<float> (dgt_copy_block_f32), bit-exact;
  * the reference-shaped 2.5D Cannon benchmark drivers and their CSV logs
-   (include/dgt_drivers.hpp, tests/cpp/driver_test.cpp)."""
+   (include/dgt_drivers.hpp, tests/cpp/driver_test.cpp);
+ * SUMMA across processes (dgt.dist) with its device operations (dgt_copy_block panel
+   packing, dgt_dgemm steps) on one rank."""
 import os
 import subprocess
 
@@ -144,3 +146,33 @@ def test_cpp_cannon_drivers_and_logs(tmp_path):
     assert "ALL OK" in out.stdout
 
     check_cannon_driver_logs(logs)
+
+
+def test_dist_summa_device_ops_one_rank():
+    """dgt.dist.DistSumma on a 1 x 1 grid (a one-rank gloo group, so no collective runs):
+    every K panel goes through DgtOps -- B's panel rows packed by dgt_copy_block, the step
+    GEMM by dgt_dgemm with beta on the first panel only -- against the host FP64 GEMM."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    from dgt.dist import DistSumma
+
+    M, N, K, kb = 300, 200, 170, 32  # 6 panels, the last 10 wide
+    A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        tA, tB, tC = dev(A), dev(B), dev(C)  # (cols, rows) tensors: column-major, ld = rows
+        S = DistSumma(1, 1, 64, 64, kb)
+        S.multiply(M, N, K, 1.5, tA, tB, -0.5, tC)
+        torch.cuda.synchronize()
+        S.ops.h.check_device()
+        got = np.asfortranarray(tC.cpu().numpy().T)
+    finally:
+        dist.destroy_process_group()
+    assert O.rel_errors(got, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
