@@ -151,3 +151,119 @@ class DistSumma:
                 w.wait()
             if m > 0 and n > 0:
                 ops.gemm(m, n, kt, alpha, a, m, b, kt, beta if t == 0 else 1.0, C_loc, C_loc.shape[1])
+
+
+class DistCannon25D:
+    """2.5D Cannon on a p x p x c grid of processes (world of p*p*c ranks), the reference's
+    NCCL variant (Summa25Decomposer::multiplyNCCL, src/25DCannonNCCL.cpp:109-304) with the
+    tiles of square M = N = K split in (M/p)^2 blocks:
+
+      rank r = k p^2 + i p + j  (src/25DCannon.cpp:37-42)
+      1. stack broadcast: stack 0's A_ij, B_ij to every stack (broadcastToStackNCCL, :84-96)
+      2. skew: A_ij to column (j - i + k pc3) mod p, B_ij to row (i - j + k pc3) mod p (:120-126)
+      3. pc3 = p / c steps: C += A B, then A moves one column right and B one row down
+      4. stack reduce: C_ij(0) = sum over stacks (reduceResultNCCL, :306-320)
+
+    so rank (i, j, k) multiplies k-blocks (i + j - k pc3 - r) mod p, r = 0 .. pc3 - 1, and the
+    stacks together visit every k-block once.  The reference rotates by a growing amount
+    (column j + r at step r), which skips k-blocks on some grids (p = 3, c = 1); unit shifts
+    are the standard Cannon order and cover every grid.  Beta scales C on stack 0's first
+    step; the other stacks start their partial sums from zero.  The caller's A and B tiles
+    are read, never shifted in place (the reference's are, so its next call starts skewed).
+    Each rank passes (M/p, M/p) tensors: column-major tiles with ld = M/p; after the call
+    stack 0's C tiles hold the result.  Step r + 1's shifts are posted before step r's GEMM.
+    """
+
+    def __init__(self, p: int, c: int, ops=None):
+        import torch.distributed as dist
+
+        if not dist.is_initialized():
+            raise RuntimeError("DistCannon25D needs an initialised torch.distributed process group")
+        if p <= 0 or c <= 0 or p % c:
+            raise ValueError("need p >= 1, c >= 1 and p % c == 0")
+        world, rank = dist.get_world_size(), dist.get_rank()
+        if world != p * p * c:
+            raise ValueError(f"world size {world} != p*p*c = {p * p * c}")
+        self.p, self.c, self.pc3 = p, c, p // c
+        self.rank = rank
+        self.k, self.i, self.j = rank // (p * p), (rank // p) % p, rank % p
+        # every rank creates every stack fiber group, in the same order
+        self.fibers = ([dist.new_group([k * p * p + r for k in range(c)]) for r in range(p * p)] if c > 1 else None)
+        self.ops = ops
+
+    def _rank_of(self, i, j, k=None):
+        p = self.p
+        return (self.k if k is None else k) * p * p + (i % p) * p + (j % p)
+
+    def multiply(self, M: int, alpha: float, A_tile, B_tile, beta: float, C_tile) -> None:
+        import torch.distributed as dist
+
+        if self.ops is None:
+            import torch
+
+            self.ops = DgtOps(dgt.Handle(stream=torch.cuda.current_stream().cuda_stream))
+        ops, p, c, pc3, i, j, k = self.ops, self.p, self.c, self.pc3, self.i, self.j, self.k
+        if M <= 0 or M % p:
+            raise ValueError("need M > 0 and M % p == 0")
+        lm = M // p
+        for name, t in (("A", A_tile), ("B", B_tile), ("C", C_tile)):
+            if tuple(t.shape) != (lm, lm):
+                raise ValueError(f"{name} tile must have shape ({lm}, {lm}), got {tuple(t.shape)}")
+
+        # 1. stack broadcast of A and B (stack 0 sends its own tiles)
+        if c > 1:
+            fiber = self.fibers[i * p + j]
+            root = self._rank_of(i, j, 0)
+            if k == 0:
+                a0, b0 = A_tile, B_tile
+            else:
+                a0, b0 = ops.empty((lm, lm), C_tile), ops.empty((lm, lm), C_tile)
+            works = [dist.broadcast(a0, src=root, group=fiber, async_op=True),
+                     dist.broadcast(b0, src=root, group=fiber, async_op=True)]
+            for w in works:
+                w.wait()
+        else:
+            a0, b0 = A_tile, B_tile
+
+        ws_a = [ops.empty((lm, lm), C_tile), ops.empty((lm, lm), C_tile)] if p > 1 else None
+        ws_b = [ops.empty((lm, lm), C_tile), ops.empty((lm, lm), C_tile)] if p > 1 else None
+
+        def exchange(send_a, to_a, recv_a, from_a, send_b, to_b, recv_b, from_b):
+            """Post the A and B moves of one shift; a move to oneself is a local copy."""
+            ops_list = []
+            for snd, to, rcv, frm in ((send_a, to_a, recv_a, from_a), (send_b, to_b, recv_b, from_b)):
+                if to == self.rank and frm == self.rank:
+                    rcv.copy_(snd)
+                    continue
+                ops_list.append(dist.P2POp(dist.isend, snd, to))
+                ops_list.append(dist.P2POp(dist.irecv, rcv, frm))
+            return dist.batch_isend_irecv(ops_list) if ops_list else []
+
+        # 2. skew (reference convention); a tile that stays put is used in place
+        kp = k * pc3
+        if p > 1:
+            reqs = exchange(a0, self._rank_of(i, j - i + kp), ws_a[0], self._rank_of(i, j + i - kp),
+                            b0, self._rank_of(i - j + kp, j), ws_b[0], self._rank_of(i + j - kp, j))
+            for r in reqs:
+                r.wait()
+            cur_a, cur_b = ws_a[0], ws_b[0]
+        else:
+            cur_a, cur_b = a0, b0
+
+        # 3. steps, the next shift posted before this step's GEMM
+        for r in range(pc3):
+            reqs = []
+            if r + 1 < pc3:
+                nxt_a, nxt_b = ws_a[(r + 1) % 2], ws_b[(r + 1) % 2]
+                reqs = exchange(cur_a, self._rank_of(i, j + 1), nxt_a, self._rank_of(i, j - 1),
+                                cur_b, self._rank_of(i + 1, j), nxt_b, self._rank_of(i - 1, j))
+            step_beta = (beta if k == 0 else 0.0) if r == 0 else 1.0
+            ops.gemm(lm, lm, lm, alpha, cur_a, lm, cur_b, lm, step_beta, C_tile, lm)
+            for q_ in reqs:
+                q_.wait()
+            if r + 1 < pc3:
+                cur_a, cur_b = nxt_a, nxt_b
+
+        # 4. stack reduction into stack 0
+        if c > 1:
+            dist.reduce(C_tile, dst=self._rank_of(i, j, 0), op=dist.ReduceOp.SUM, group=self.fibers[i * p + j])

@@ -39,3 +39,22 @@ def check_cannon_driver_logs(logs):
         assert (df["DataLocation"] == "devices").all() and (df["TotalGPUs"] == 1).all()
         assert (df["ExecutionTime"] > 0).all() and (df["GFlops"] > 0).all()
         assert (df["GemmCallTime"] == df["ExecutionTime"]).all() and (df["CommunicationTime"] == 0).all()
+
+
+class HostOps:
+    """Rank-local operations on CPU tensors: the test double of dgt.dist.DgtOps for the
+    multi-process schedules run as gloo ranks.  Like dgt_dgemm, C is not read when beta
+    is 0."""
+
+    def empty(self, shape, like):
+        import torch
+
+        return torch.empty(shape, dtype=torch.float64)
+
+    def pack_rows(self, src, r0, rows, dst):
+        dst.copy_(src[:, r0:r0 + rows])
+
+    def gemm(self, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+        c = C.numpy()[:n, :m]  # column-major m x n view of C's storage
+        prod = A.numpy()[:k, :m].T @ B.numpy()[:n, :k].T if k > 0 else np.zeros((m, n))
+        c[...] = (alpha * prod).T if beta == 0.0 else (alpha * prod + beta * c.T).T

@@ -24,23 +24,6 @@ CASES = [
 ]
 
 
-class HostOps:
-    """Rank-local operations on CPU tensors (the test double of dgt.dist.DgtOps)."""
-
-    def empty(self, shape, like):
-        import torch
-
-        return torch.empty(shape, dtype=torch.float64)
-
-    def pack_rows(self, src, r0, rows, dst):
-        dst.copy_(src[:, r0:r0 + rows])
-
-    def gemm(self, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
-        c = C.numpy()[:n, :m]  # column-major m x n view of C's storage
-        prod = A.numpy()[:k, :m].T @ B.numpy()[:n, :k].T if k > 0 else 0.0
-        c[...] = (alpha * prod + beta * c.T).T
-
-
 def _scatter(G, mb, nb, p, q):
     """Block-cyclic locals of every rank (rank r = i q + j), empty ranks included."""
     M, N = G.shape
@@ -87,6 +70,7 @@ def _rank_main(rank, world, port, out):
     for sub in ("", "oracle", "distributed-gemm-thesis_b200", "tests"):
         sys.path.insert(0, os.path.join(ROOT, sub))
     import oracle as O
+    from devutil import HostOps
     from dgt.dist import DistSumma
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
