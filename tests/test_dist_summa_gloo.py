@@ -152,3 +152,57 @@ def test_dist_summa_needs_matching_world():
 
     with pytest.raises(RuntimeError):
         DistSumma(2, 2, 16, 16, 16)
+
+
+class _PtrHandle:
+    """dgt.Handle's copy_block and dgemm acting on host addresses, so DgtOps's pointer and
+    leading-dimension arithmetic runs unchanged on CPU tensors."""
+
+    @staticmethod
+    def _mat(addr, rows, cols, ld):
+        import ctypes
+
+        n = ld * (cols - 1) + rows if rows and cols else 0
+        buf = np.frombuffer((ctypes.c_double * max(n, 1)).from_address(addr), dtype=np.float64)
+        return np.lib.stride_tricks.as_strided(buf, shape=(rows, cols), strides=(8, 8 * ld))
+
+    def copy_block(self, rows, cols, src, dst, ldS, ldD, col_major=True):
+        assert col_major and ldS >= rows and ldD >= rows
+        self._mat(dst, rows, cols, ldD)[...] = self._mat(src, rows, cols, ldS)
+
+    def dgemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, mode=None, slices=7):
+        assert ta == tb == "N" and lda >= max(1, m) and ldb >= max(1, k) and ldc >= max(1, m)
+        c = self._mat(C, m, n, ldc)
+        prod = self._mat(A, m, k, lda) @ self._mat(B, k, n, ldb) if k else 0.0
+        c[...] = alpha * prod if beta == 0.0 else alpha * prod + beta * c
+
+
+def test_device_ops_argument_arithmetic():
+    """DistSumma on a 1 x 1 grid (one-rank gloo group) through DgtOps -- the product's
+    pointer offsets, leading dimensions and beta-on-the-first-panel rule -- with the handle
+    replaced by a host-address double."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    for sub in ("oracle", "distributed-gemm-thesis_b200"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    import oracle as O
+    from dgt.dist import DgtOps, DistCannon25D, DistSumma
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        M, N, K = 70, 50, 45
+        A, B, C = O.uniform((M, K), 4), O.uniform((K, N), 5), O.uniform((M, N), 6)
+        tA, tB, tC = (_local_tensor(x) for x in (A, B, C))
+        DistSumma(1, 1, 16, 16, 8, ops=DgtOps(_PtrHandle())).multiply(M, N, K, 1.5, tA, tB, -0.5, tC)
+        got = tC.numpy().T
+        assert O.rel_errors(got, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
+        S = O.uniform((40, 40), 7)
+        tS, tT, tU = _local_tensor(S), _local_tensor(S.T.copy()), _local_tensor(S)
+        DistCannon25D(1, 1, ops=DgtOps(_PtrHandle())).multiply(40, 2.0, tS, tT, 0.5, tU)
+        assert O.rel_errors(tU.numpy().T, O.dgemm(S, S.T, 2.0, 0.5, S))[1] <= 1e-13
+    finally:
+        dist.destroy_process_group()
