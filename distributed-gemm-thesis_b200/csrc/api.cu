@@ -493,6 +493,83 @@ dgt_status dgt_dgemm_grouped(dgt_handle_t h, int count, const dgt_gemm_desc* d, 
 
 // ---- SUMMA on block-cyclic local buffers -------------------------------------------------
 
+// Shape checks of a SUMMA call (dgt_summa, dgt_summa_rank, dgt_summa_schedule); nullptr if
+// the call is valid, else the reason.  lldC, when given, is checked for every rank.
+static const char* summa_check(const dgt_grid_layout* L, int64_t M, int64_t N, int64_t K, const int64_t* lldA,
+                               const int64_t* lldB, const int64_t* lldC) {
+    const int p = L->p, q = L->q;
+    if (p <= 0 || q <= 0 || L->c != 1) return "SUMMA needs p, q >= 1 and c == 1";
+    if (L->mb <= 0 || L->nb <= 0 || L->kb <= 0) return "block sizes must be > 0";
+    if (M < 0 || N < 0 || K < 0 || M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return "dimension out of range";
+    auto roc = [](int64_t n, int64_t b, int i, int np) { return (int64_t)dgt_numroc((int)n, (int)b, i, 0, np); };
+    for (int r = 0; r < p * q; ++r) {
+        int i = r / q;
+        if (lldC && lldC[r] < std::max<int64_t>(1, roc(M, L->mb, i, p))) return "lldC < rows";
+        if (lldA[r] < std::max<int64_t>(1, roc(M, L->mb, i, p))) return "lldA < rows";
+        if (lldB[r] < std::max<int64_t>(1, roc(K, L->kb, i, p))) return "lldB < rows";
+    }
+    return nullptr;
+}
+
+// Virtual rank (i, j)'s SUMMA problem: its C block and the K segments its GEMM walks.  Panel
+// t reads A's block column t from process column t mod q (local column (t div q) kb) and
+// B's block row t from process row t mod p (local row (t div p) kb), through A_loc / B_loc,
+// which may point into other devices' memory.  Panels are visited owner pair by owner pair
+// (t mod q, t mod p) so that runs contiguous in both owners' buffers merge into one segment.
+static Problem summa_problem(const dgt_grid_layout* L, int i, int j, int64_t M, int64_t N, int64_t K, double alpha,
+                             double beta, const double* const* A_loc, const int64_t* lldA,
+                             const double* const* B_loc, const int64_t* lldB, double* C, int64_t ldc,
+                             std::vector<KSegment>& segs) {
+    const int p = L->p, q = L->q;
+    const int64_t mb = L->mb, nb = L->nb, kb = L->kb;
+    auto roc = [](int64_t n, int64_t b, int i, int np) { return (int64_t)dgt_numroc((int)n, (int)b, i, 0, np); };
+    const int64_t kblocks = ceil_div(K, kb);
+    Problem pr{};
+    pr.m = roc(M, mb, i, p);
+    pr.n = roc(N, nb, j, q);
+    pr.alpha = K == 0 ? 0.0 : alpha;
+    pr.beta = beta;
+    pr.C = C;
+    pr.ldc = ldc;
+    pr.seg_begin = (int32_t)segs.size();
+    std::vector<std::vector<int64_t>> classes;
+    std::vector<std::pair<int, int>> keys;
+    for (int64_t t = 0; t < kblocks; ++t) {
+        std::pair<int, int> key((int)(t % q), (int)(t % p));
+        auto it = std::find(keys.begin(), keys.end(), key);
+        if (it == keys.end()) {
+            keys.push_back(key);
+            classes.push_back({t});
+        } else {
+            classes[it - keys.begin()].push_back(t);
+        }
+    }
+    for (auto& cls : classes) {
+        for (int64_t t : cls) {
+            int ra = i * q + (int)(t % q);
+            int rb = (int)(t % p) * q + j;
+            int64_t kt = std::min(kb, K - t * kb);
+            const double* a = A_loc[ra] + (t / q) * kb * lldA[ra];
+            const double* b = B_loc[rb] + (t / p) * kb;
+            if (pr.seg_count > 0) {
+                KSegment& last = segs.back();
+                if (last.lda == lldA[ra] && last.ldb == lldB[rb] && last.A + last.k * last.lda == a &&
+                    last.B + last.k == b) {
+                    last.k += kt;
+                    continue;
+                }
+            }
+            segs.push_back(KSegment{a, b, lldA[ra], lldB[rb], kt});
+            pr.seg_count++;
+        }
+    }
+    if (pr.seg_count == 0) {  // K == 0: C = beta*C
+        segs.push_back(KSegment{nullptr, nullptr, 1, 1, 0});
+        pr.seg_count = 1;
+    }
+    return pr;
+}
+
 dgt_status dgt_summa(dgt_handle_t h, const dgt_grid_layout* L, int64_t M, int64_t N, int64_t K, double alpha,
                      const double* const* A_loc, const int64_t* lldA, const double* const* B_loc,
                      const int64_t* lldB, double beta, double* const* C_loc, const int64_t* lldC, dgt_fp64_mode mode,
@@ -500,78 +577,54 @@ dgt_status dgt_summa(dgt_handle_t h, const dgt_grid_layout* L, int64_t M, int64_
     if (!h) return DGT_ERROR_NOT_INITIALIZED;
     if (!L || !A_loc || !B_loc || !C_loc || !lldA || !lldB || !lldC)
         return fail(h, DGT_ERROR_INVALID_VALUE, "null argument");
-    const int p = L->p, q = L->q;
-    if (p <= 0 || q <= 0 || L->c != 1) return fail(h, DGT_ERROR_INVALID_VALUE, "SUMMA needs p, q >= 1 and c == 1");
-    if (L->mb <= 0 || L->nb <= 0 || L->kb <= 0) return fail(h, DGT_ERROR_INVALID_VALUE, "block sizes must be > 0");
-    if (M < 0 || N < 0 || K < 0 || M > INT32_MAX || N > INT32_MAX || K > INT32_MAX)
-        return fail(h, DGT_ERROR_INVALID_VALUE, "dimension out of range");
-    const int64_t mb = L->mb, nb = L->nb, kb = L->kb;
-    auto roc = [](int64_t n, int64_t b, int i, int np) { return (int64_t)dgt_numroc((int)n, (int)b, i, 0, np); };
-    for (int r = 0; r < p * q; ++r) {
-        int i = r / q;
-        if (lldC[r] < std::max<int64_t>(1, roc(M, mb, i, p))) return fail(h, DGT_ERROR_INVALID_VALUE, "lldC < rows");
-        if (lldA[r] < std::max<int64_t>(1, roc(M, mb, i, p))) return fail(h, DGT_ERROR_INVALID_VALUE, "lldA < rows");
-        if (lldB[r] < std::max<int64_t>(1, roc(K, kb, i, p))) return fail(h, DGT_ERROR_INVALID_VALUE, "lldB < rows");
-    }
+    if (const char* why = summa_check(L, M, N, K, lldA, lldB, lldC)) return fail(h, DGT_ERROR_INVALID_VALUE, why);
     if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
-    const int64_t kblocks = ceil_div(K, kb);
     std::vector<Problem> probs;
     std::vector<KSegment> segs;
-    for (int i = 0; i < p; ++i) {
-        for (int j = 0; j < q; ++j) {
-            const int r = i * q + j;
-            Problem pr{};
-            pr.m = roc(M, mb, i, p);
-            pr.n = roc(N, nb, j, q);
-            pr.alpha = K == 0 ? 0.0 : alpha;
-            pr.beta = beta;
-            pr.C = C_loc[r];
-            pr.ldc = lldC[r];
-            pr.seg_begin = (int32_t)segs.size();
-            // Panel t: A's block column t lives on process column t mod q at local column
-            // (t div q)*kb; B's block row t on process row t mod p at local row (t div p)*kb.
-            // Panels are visited owner pair by owner pair (t mod q, t mod p) so that runs
-            // that are contiguous in both local buffers merge into one segment.
-            std::vector<std::vector<int64_t>> classes;
-            std::vector<std::pair<int, int>> keys;
-            for (int64_t t = 0; t < kblocks; ++t) {
-                std::pair<int, int> key((int)(t % q), (int)(t % p));
-                auto it = std::find(keys.begin(), keys.end(), key);
-                if (it == keys.end()) {
-                    keys.push_back(key);
-                    classes.push_back({t});
-                } else {
-                    classes[it - keys.begin()].push_back(t);
-                }
-            }
-            for (auto& cls : classes) {
-                for (int64_t t : cls) {
-                    int ra = i * q + (int)(t % q);
-                    int rb = (int)(t % p) * q + j;
-                    int64_t kt = std::min(kb, K - t * kb);
-                    const double* a = A_loc[ra] + (t / q) * kb * lldA[ra];
-                    const double* b = B_loc[rb] + (t / p) * kb;
-                    if (pr.seg_count > 0) {
-                        KSegment& last = segs.back();
-                        if (last.lda == lldA[ra] && last.ldb == lldB[rb] && last.A + last.k * last.lda == a &&
-                            last.B + last.k == b) {
-                            last.k += kt;
-                            continue;
-                        }
-                    }
-                    segs.push_back(KSegment{a, b, lldA[ra], lldB[rb], kt});
-                    pr.seg_count++;
-                }
-            }
-            if (pr.seg_count == 0) {  // K == 0: C = beta*C
-                segs.push_back(KSegment{nullptr, nullptr, 1, 1, 0});
-                pr.seg_count = 1;
-            }
-            probs.push_back(pr);
+    for (int i = 0; i < L->p; ++i)
+        for (int j = 0; j < L->q; ++j) {
+            const int r = i * L->q + j;
+            probs.push_back(summa_problem(L, i, j, M, N, K, alpha, beta, A_loc, lldA, B_loc, lldB, C_loc[r], lldC[r],
+                                          segs));
         }
-    }
     if (mode == DGT_FP64_NATIVE) return launch_dmma_grouped(h, probs, segs);
     return run_problems_emulated(h, probs, segs, mode, slices);
+}
+
+dgt_status dgt_summa_rank(dgt_handle_t h, const dgt_grid_layout* L, int32_t rank, int64_t M, int64_t N, int64_t K,
+                          double alpha, const double* const* A_loc, const int64_t* lldA, const double* const* B_loc,
+                          const int64_t* lldB, double beta, double* C, int64_t ldc, dgt_fp64_mode mode, int slices) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!L || !A_loc || !B_loc || !C || !lldA || !lldB) return fail(h, DGT_ERROR_INVALID_VALUE, "null argument");
+    if (const char* why = summa_check(L, M, N, K, lldA, lldB, nullptr)) return fail(h, DGT_ERROR_INVALID_VALUE, why);
+    if (rank < 0 || rank >= L->p * L->q) return fail(h, DGT_ERROR_INVALID_VALUE, "rank outside the grid");
+    const int i = rank / L->q, j = rank % L->q;
+    if (ldc < std::max<int64_t>(1, dgt_numroc((int)M, (int)L->mb, i, 0, L->p)))
+        return fail(h, DGT_ERROR_INVALID_VALUE, "ldc < rows");
+    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
+    std::vector<KSegment> segs;
+    std::vector<Problem> probs{summa_problem(L, i, j, M, N, K, alpha, beta, A_loc, lldA, B_loc, lldB, C, ldc, segs)};
+    if (probs[0].m == 0 || probs[0].n == 0) return DGT_SUCCESS;
+    if (mode == DGT_FP64_NATIVE) return launch_dmma_grouped(h, probs, segs);
+    return run_problems_emulated(h, probs, segs, mode, slices);
+}
+
+int32_t dgt_summa_schedule(const dgt_grid_layout* L, int32_t rank, int64_t M, int64_t N, int64_t K,
+                           const double* const* A_loc, const int64_t* lldA, const double* const* B_loc,
+                           const int64_t* lldB, int64_t* out, int32_t max_segments) {
+    if (!L || !A_loc || !B_loc || !lldA || !lldB || summa_check(L, M, N, K, lldA, lldB, nullptr)) return -1;
+    if (rank < 0 || rank >= L->p * L->q) return -1;
+    std::vector<KSegment> segs;
+    double* no_c = nullptr;
+    summa_problem(L, rank / L->q, rank % L->q, M, N, K, 1.0, 0.0, A_loc, lldA, B_loc, lldB, no_c, 1, segs);
+    for (size_t s = 0; s < segs.size() && out && (int32_t)s < max_segments; ++s) {
+        out[5 * s + 0] = (int64_t)(uintptr_t)segs[s].A;
+        out[5 * s + 1] = (int64_t)(uintptr_t)segs[s].B;
+        out[5 * s + 2] = segs[s].lda;
+        out[5 * s + 3] = segs[s].ldb;
+        out[5 * s + 4] = segs[s].k;
+    }
+    return (int32_t)segs.size();
 }
 
 // ---- 2.5D Cannon -----------------------------------------------------------------------------

@@ -75,6 +75,10 @@ SIGNATURES = [
     ("dgt_block2d_grid", _c_i32, [_c_i32, ctypes.POINTER(_c_i32), ctypes.POINTER(_c_i32)]),
     ("dgt_summa", _c_i32, [_vp, ctypes.POINTER(GridLayout), _c_i64, _c_i64, _c_i64, ctypes.c_double, _vp, _vp, _vp,
                            _vp, ctypes.c_double, _vp, _vp, _c_i32, ctypes.c_int]),
+    ("dgt_summa_rank", _c_i32, [_vp, ctypes.POINTER(GridLayout), _c_i32, _c_i64, _c_i64, _c_i64, ctypes.c_double,
+                                _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _c_i64, _c_i32, ctypes.c_int]),
+    ("dgt_summa_schedule", _c_i32, [ctypes.POINTER(GridLayout), _c_i32, _c_i64, _c_i64, _c_i64, _vp, _vp, _vp, _vp,
+                                    _vp, _c_i32]),
     ("dgt_cannon25d", _c_i32, [_vp, _c_i64, _c_i32, _c_i32, ctypes.c_char, ctypes.c_char, ctypes.c_double, _vp, _vp,
                                ctypes.c_double, _vp, _c_i32, ctypes.c_int]),
     ("dgt_cannon_schedule", _c_i32, [_c_i32] * 5 + [ctypes.POINTER(_c_i32)]),
@@ -257,6 +261,14 @@ class Handle:
                                        _ptrs(B_locals), _i64s(lldB), beta, _ptrs(C_locals), _i64s(lldC), mode,
                                        slices))
 
+    def summa_rank(self, rank, p, q, mb, nb, kb, M, N, K, alpha, A_locals, lldA, B_locals, lldB, beta, C, ldc,
+                   mode=FP64_NATIVE, slices=7):
+        """Rank `rank`'s C block of the SUMMA; A_locals / B_locals may be peer-mapped pointers."""
+        L = GridLayout(p, q, 1, mb, nb, kb)
+        self._check(self.lib.dgt_summa_rank(self.h, ctypes.byref(L), rank, M, N, K, alpha, _ptrs(A_locals),
+                                            _i64s(lldA), _ptrs(B_locals), _i64s(lldB), beta, _vp(C), ldc, mode,
+                                            slices))
+
     def cannon25d(self, M, p, c, alpha, A_tiles, B_tiles, beta, C_tiles, ta="N", tb="N", mode=FP64_NATIVE,
                   slices=7):
         self._check(self.lib.dgt_cannon25d(self.h, M, p, c, ta.encode(), tb.encode(), alpha, _ptrs(A_tiles),
@@ -312,6 +324,20 @@ def block2d_grid(P):
     if st != SUCCESS:
         raise DgtError(st, "block2d_grid")
     return a.value, b.value
+
+
+def summa_schedule(rank, p, q, mb, nb, kb, M, N, K, A_locals, lldA, B_locals, lldB):
+    """[(A address, B address, lda, ldb, k), ...]: the K segments rank `rank`'s SUMMA GEMM
+    walks (host only; the addresses are not dereferenced)."""
+    lib = load()
+    L = GridLayout(p, q, 1, mb, nb, kb)
+    args = (ctypes.byref(L), rank, M, N, K, _ptrs(A_locals), _i64s(lldA), _ptrs(B_locals), _i64s(lldB))
+    n = lib.dgt_summa_schedule(*args, None, 0)
+    if n < 0:
+        raise DgtError(INVALID_VALUE, "dgt_summa_schedule")
+    out = (ctypes.c_int64 * (5 * max(n, 1)))()
+    lib.dgt_summa_schedule(*args, out, n)
+    return [tuple(out[5 * s:5 * s + 5]) for s in range(n)]
 
 
 def cannon_schedule(p, c, i, j, k):

@@ -6,7 +6,9 @@
  * the reference-shaped 2.5D Cannon benchmark drivers and their CSV logs
    (include/dgt_drivers.hpp, tests/cpp/driver_test.cpp);
  * SUMMA across processes (dgt.dist) with its device operations (dgt_copy_block panel
-   packing, dgt_dgemm steps) on one rank."""
+   packing, dgt_dgemm steps) on one rank;
+ * one rank's share of the SUMMA (dgt_summa_rank), the form a multi-GPU run uses with other
+   GPUs' buffers in its pointer arrays, against the whole-grid dgt_summa."""
 import os
 import subprocess
 
@@ -15,7 +17,7 @@ import pytest
 
 import dgt
 import oracle as O
-from devutil import check_cannon_driver_logs, dev, ptr
+from devutil import check_cannon_driver_logs, dev, host, ptr
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -176,3 +178,39 @@ def test_dist_summa_device_ops_one_rank():
     finally:
         dist.destroy_process_group()
     assert O.rel_errors(got, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
+
+
+@pytest.mark.parametrize("M,N,K,b,p,q", [(257, 131, 199, 32, 2, 3), (500, 400, 300, 64, 4, 4)])
+def test_summa_rank_matches_whole_grid(h, M, N, K, b, p, q):
+    """Every rank's dgt_summa_rank equals its block of the whole-grid dgt_summa (same
+    segments, same kernel; relative Frobenius <= 1e-14), and the assembled result the host
+    FP64 GEMM (<= 1e-13)."""
+    import torch
+
+    A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
+    o = O.orc()
+
+    def pack(X, rows, cols):
+        shapes = o.pblas_shapes(rows, cols, b, b, p, q)
+        locs = [torch.zeros((max(c, 1), max(r, 1)), dtype=torch.float64, device="cuda") for r, c, _ in shapes]
+        lld = [max(r, 1) for r, _, _ in shapes]
+        dX = dev(X)
+        h.pack_block_cyclic(rows, cols, b, b, p, q, ptr(dX), rows, [ptr(l) for l in locs], lld)
+        return dX, locs, lld
+
+    _, lA, lldA = pack(A, M, K)
+    _, lB, lldB = pack(B, K, N)
+    dC, lC, lldC = pack(C, M, N)
+    lC_rank = [x.clone() for x in lC]
+    pA, pB = [ptr(x) for x in lA], [ptr(x) for x in lB]
+    h.summa(p, q, b, b, b, M, N, K, 1.5, pA, lldA, pB, lldB, -0.5, [ptr(x) for x in lC], lldC)
+    for r in range(p * q):
+        h.summa_rank(r, p, q, b, b, b, M, N, K, 1.5, pA, lldA, pB, lldB, -0.5, ptr(lC_rank[r]), lldC[r])
+    torch.cuda.synchronize()
+    h.check_device()
+    for r in range(p * q):
+        whole, mine = lC[r].cpu().numpy(), lC_rank[r].cpu().numpy()
+        assert O.rel_errors(mine, whole)[1] <= 1e-14, r
+    h.unpack_block_cyclic(M, N, b, b, p, q, ptr(dC), M, [ptr(x) for x in lC_rank], lldC)
+    torch.cuda.synchronize()
+    assert O.rel_errors(host(dC, (M, N)), O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
