@@ -627,6 +627,60 @@ int32_t dgt_summa_schedule(const dgt_grid_layout* L, int32_t rank, int64_t M, in
     return (int32_t)segs.size();
 }
 
+// ---- buffers shared between processes (CUDA IPC) --------------------------------------------
+
+static_assert(sizeof(dgt_ipc_handle) == sizeof(cudaIpcMemHandle_t), "IPC handle size");
+
+dgt_status dgt_ipc_alloc(size_t bytes, void** ptr, dgt_ipc_handle* handle) {
+    if (!ptr || !handle || bytes == 0) return DGT_ERROR_INVALID_VALUE;
+    *ptr = nullptr;
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return DGT_ERROR_ALLOC;
+    }
+    cudaIpcMemHandle_t h;
+    if (cudaIpcGetMemHandle(&h, p) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p);
+        return DGT_ERROR_CUDA;
+    }
+    std::memcpy(handle->bytes, &h, sizeof(h));
+    *ptr = p;
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_ipc_open(const dgt_ipc_handle* handle, void** ptr) {
+    if (!ptr || !handle) return DGT_ERROR_INVALID_VALUE;
+    *ptr = nullptr;
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, handle->bytes, sizeof(h));
+    if (cudaIpcOpenMemHandle(ptr, h, cudaIpcMemLazyEnablePeerAccess) != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
+        return DGT_ERROR_CUDA;
+    }
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_ipc_close(void* ptr) {
+    if (!ptr) return DGT_ERROR_INVALID_VALUE;
+    if (cudaIpcCloseMemHandle(ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return DGT_ERROR_CUDA;
+    }
+    return DGT_SUCCESS;
+}
+
+dgt_status dgt_ipc_free(void* ptr) {
+    if (!ptr) return DGT_ERROR_INVALID_VALUE;
+    if (cudaFree(ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return DGT_ERROR_CUDA;
+    }
+    return DGT_SUCCESS;
+}
+
 // ---- 2.5D Cannon -----------------------------------------------------------------------------
 
 dgt_status dgt_cannon25d(dgt_handle_t h, int64_t M, int32_t p, int32_t c, char ta, char tb, double alpha,

@@ -77,6 +77,10 @@ SIGNATURES = [
                            _vp, ctypes.c_double, _vp, _vp, _c_i32, ctypes.c_int]),
     ("dgt_summa_rank", _c_i32, [_vp, ctypes.POINTER(GridLayout), _c_i32, _c_i64, _c_i64, _c_i64, ctypes.c_double,
                                 _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _c_i64, _c_i32, ctypes.c_int]),
+    ("dgt_ipc_alloc", _c_i32, [ctypes.c_size_t, ctypes.POINTER(_vp), ctypes.c_char_p]),
+    ("dgt_ipc_open", _c_i32, [ctypes.c_char_p, ctypes.POINTER(_vp)]),
+    ("dgt_ipc_close", _c_i32, [_vp]),
+    ("dgt_ipc_free", _c_i32, [_vp]),
     ("dgt_summa_schedule", _c_i32, [ctypes.POINTER(GridLayout), _c_i32, _c_i64, _c_i64, _c_i64, _vp, _vp, _vp, _vp,
                                     _vp, _c_i32]),
     ("dgt_cannon25d", _c_i32, [_vp, _c_i64, _c_i32, _c_i32, ctypes.c_char, ctypes.c_char, ctypes.c_double, _vp, _vp,

@@ -267,3 +267,125 @@ class DistCannon25D:
         # 4. stack reduction into stack 0
         if c > 1:
             dist.reduce(C_tile, dst=self._rank_of(i, j, 0), op=dist.ReduceOp.SUM, group=self.fibers[i * p + j])
+
+
+class DeviceIpc:
+    """Device buffers shared between the processes of a node through the C ABI's CUDA IPC
+    entry points (dgt_ipc_*): a mapped peer buffer is read over NVLink by the kernels."""
+
+    def __init__(self):
+        self.lib = dgt.load()
+
+    def alloc(self, nbytes: int):
+        import ctypes
+
+        ptr, h = ctypes.c_void_p(), ctypes.create_string_buffer(64)
+        st = self.lib.dgt_ipc_alloc(max(int(nbytes), 8), ctypes.byref(ptr), h)
+        if st != dgt.SUCCESS:
+            raise dgt.DgtError(st, "dgt_ipc_alloc")
+        return ptr.value, h.raw
+
+    def open(self, handle: bytes) -> int:
+        import ctypes
+
+        ptr = ctypes.c_void_p()
+        st = self.lib.dgt_ipc_open(ctypes.create_string_buffer(handle, 64), ctypes.byref(ptr))
+        if st != dgt.SUCCESS:
+            raise dgt.DgtError(st, "dgt_ipc_open")
+        return ptr.value
+
+    def close(self, ptr: int) -> None:
+        self.lib.dgt_ipc_close(ptr)
+
+    def free(self, ptr: int) -> None:
+        self.lib.dgt_ipc_free(ptr)
+
+    def tensor(self, ptr: int, shape):
+        """A float64 torch tensor over device memory at ptr (no copy)."""
+        import torch
+
+        class _Buf:
+            __cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                        "strides": None}
+
+        return torch.as_tensor(_Buf(), device="cuda")
+
+    def synchronize(self) -> None:
+        import torch
+
+        torch.cuda.synchronize()
+
+
+class PeerSumma:
+    """SUMMA across processes with the panel broadcasts fused into the GEMM: every rank's
+    local A and B live in buffers the other ranks map (DeviceIpc), and each rank's
+    dgt_summa_rank reads the owners' panels straight from their memory, tile by tile, as it
+    multiplies -- no broadcast, no staging copy.  Same layout and result as DistSumma.
+
+        S = PeerSumma(p, q, mb, nb, kb, M, N, K)      # collective: allocates and maps
+        S.A_loc[...] = ...; S.B_loc[...] = ...          # this rank's block-cyclic locals
+        S.multiply(alpha, beta, C_loc)                  # C_loc: (n, m) tensor, column-major
+        S.close()                                       # collective
+
+    Host barriers bracket each multiply (every owner's A and B are written before any rank
+    reads them, and no owner rewrites them while a peer still reads); no kernel waits on
+    another process.
+    """
+
+    def __init__(self, p, q, mb, nb, kb, M, N, K, ipc=None, handle=None, mode=dgt.FP64_NATIVE, slices=7):
+        import torch.distributed as dist
+
+        if not dist.is_initialized():
+            raise RuntimeError("PeerSumma needs an initialised torch.distributed process group")
+        if min(p, q, mb, nb, kb) <= 0 or min(M, N, K) < 0:
+            raise ValueError("grid, block sizes and dimensions must be valid")
+        world, rank = dist.get_world_size(), dist.get_rank()
+        if world != p * q:
+            raise ValueError(f"world size {world} != p*q = {p * q}")
+        self.p, self.q, self.mb, self.nb, self.kb, self.M, self.N, self.K = p, q, mb, nb, kb, M, N, K
+        self.rank, self.mode, self.slices = rank, mode, slices
+        self.ipc = ipc or DeviceIpc()
+        if handle is None:
+            import torch
+
+            handle = dgt.Handle(stream=torch.cuda.current_stream().cuda_stream)
+        self.h = handle
+        P = p * q
+        self.lldA = [max(1, local_rows(M, mb, r // q, p)) for r in range(P)]
+        self.lldB = [max(1, local_rows(K, kb, r // q, p)) for r in range(P)]
+        colsA = max(1, local_rows(K, kb, rank % q, q))
+        colsB = max(1, local_rows(N, nb, rank % q, q))
+        self._own = [self.ipc.alloc(8 * self.lldA[rank] * colsA), self.ipc.alloc(8 * self.lldB[rank] * colsB)]
+        handles = [None] * world
+        dist.all_gather_object(handles, (self._own[0][1], self._own[1][1]))
+        self.A_ptrs = [self._own[0][0] if r == rank else self.ipc.open(handles[r][0]) for r in range(P)]
+        self.B_ptrs = [self._own[1][0] if r == rank else self.ipc.open(handles[r][1]) for r in range(P)]
+        self.A_loc = self.ipc.tensor(self._own[0][0], (colsA, self.lldA[rank]))
+        self.B_loc = self.ipc.tensor(self._own[1][0], (colsB, self.lldB[rank]))
+        self.m = local_rows(M, mb, rank // q, p)
+        self.n = local_rows(N, nb, rank % q, q)
+
+    def multiply(self, alpha: float, beta: float, C_loc) -> None:
+        import torch.distributed as dist
+
+        if tuple(C_loc.shape) != (max(self.n, 1), max(self.m, 1)):
+            raise ValueError(f"C_loc must have shape ({max(self.n, 1)}, {max(self.m, 1)})")
+        self.ipc.synchronize()
+        dist.barrier()
+        self.h.summa_rank(self.rank, self.p, self.q, self.mb, self.nb, self.kb, self.M, self.N, self.K, alpha,
+                          self.A_ptrs, self.lldA, self.B_ptrs, self.lldB, beta, C_loc.data_ptr(), max(self.m, 1),
+                          mode=self.mode, slices=self.slices)
+        self.ipc.synchronize()
+        dist.barrier()
+
+    def close(self) -> None:
+        import torch.distributed as dist
+
+        for r, (a, b) in enumerate(zip(self.A_ptrs, self.B_ptrs)):
+            if r != self.rank:
+                self.ipc.close(a)
+                self.ipc.close(b)
+        dist.barrier()
+        for ptr, _ in self._own:
+            self.ipc.free(ptr)
+        self._own = []

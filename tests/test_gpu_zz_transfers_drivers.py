@@ -8,9 +8,12 @@
  * SUMMA across processes (dgt.dist) with its device operations (dgt_copy_block panel
    packing, dgt_dgemm steps) on one rank;
  * one rank's share of the SUMMA (dgt_summa_rank), the form a multi-GPU run uses with other
-   GPUs' buffers in its pointer arrays, against the whole-grid dgt_summa."""
+   GPUs' buffers in its pointer arrays, against the whole-grid dgt_summa;
+ * PeerSumma over CUDA IPC buffers (dgt_ipc_*): one process, and two processes sharing the
+   GPU that read each other's panels."""
 import os
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -214,3 +217,85 @@ def test_summa_rank_matches_whole_grid(h, M, N, K, b, p, q):
     h.unpack_block_cyclic(M, N, b, b, p, q, ptr(dC), M, [ptr(x) for x in lC_rank], lldC)
     torch.cuda.synchronize()
     assert O.rel_errors(host(dC, (M, N)), O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
+
+
+def _peer_rank(rank, world, p, q, port, out):
+    """One rank of PeerSumma over real CUDA IPC (every rank on cuda:0)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    for sub in ("", "oracle", "distributed-gemm-thesis_b200", "tests"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    import oracle as O
+    from dgt.dist import PeerSumma
+    from test_dist_summa_gloo import _local_tensor, _scatter
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        torch.cuda.set_device(0)
+        M, N, K, mb, nb, kb = 300, 260, 170, 32, 48, 40
+        A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
+        S = PeerSumma(p, q, mb, nb, kb, M, N, K)
+        la, lb, lc = _scatter(A, mb, kb, p, q)[rank], _scatter(B, kb, nb, p, q)[rank], _scatter(C, mb, nb, p, q)[rank]
+        S.A_loc.copy_(_local_tensor(la).cuda())
+        S.B_loc.copy_(_local_tensor(lb).cuda())
+        tC = _local_tensor(lc).cuda()
+        S.multiply(1.5, -0.5, tC)
+        S.h.check_device()
+        rows, cols = lc.shape
+        out.put((rank, tC.cpu().numpy()[:cols, :rows].T.copy()))
+        S.close()
+    except Exception:
+        import traceback
+
+        out.put((-1, traceback.format_exc()))
+        raise
+    finally:
+        dist.destroy_process_group()
+
+
+def _run_peer(world, p, q):
+    import socket
+
+    import torch.multiprocessing as mp
+    from test_dist_summa_gloo import _gather
+
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = [ctx.Process(target=_peer_rank, args=(r, world, p, q, port, out)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    got = {}
+    for _ in range(world):
+        rank, res = out.get(timeout=300)
+        if rank < 0:
+            for pr in procs:
+                pr.join(timeout=60)
+            pytest.fail(res)
+        got[rank] = res
+    for pr in procs:
+        pr.join(timeout=120)
+        assert pr.exitcode == 0
+    M, N, K, mb, nb, kb = 300, 260, 170, 32, 48, 40
+    A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
+    G = _gather([got[r] for r in range(world)], M, N, mb, nb, p, q)
+    assert O.rel_errors(G, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
+
+
+def test_peer_summa_one_process():
+    """PeerSumma on a 1 x 1 grid: dgt_ipc_alloc buffers viewed as tensors, dgt_summa_rank on
+    them, dgt_ipc_free."""
+    _run_peer(1, 1, 1)
+
+
+def test_peer_summa_two_processes_share_one_gpu():
+    """Two processes on one GPU, each mapping the other's A and B through dgt_ipc_open: each
+    rank's dgt_summa_rank reads its peer's panels directly.  The kernels only read data that
+    host barriers have published; neither waits on the other."""
+    _run_peer(2, 1, 2)

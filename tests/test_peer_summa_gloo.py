@@ -1,0 +1,162 @@
+"""SUMMA with the broadcasts fused into the GEMM (dgt.dist.PeerSumma) as four gloo ranks on
+the CPU.  Process-shared memory (multiprocessing.shared_memory) stands in for CUDA IPC, and
+a handle double runs, on those addresses, exactly the K segments dgt_summa_schedule gives
+each rank -- the segment list dgt_summa_rank's kernel walks.  So the test exercises the
+whole host side of the fused path across real processes: buffer sizes, handle exchange,
+the peer pointer arrays, the barriers, and each rank reading its panels straight out of the
+owners' memory.  The gathered C must equal the host FP64 GEMM within 1e-13."""
+import ctypes
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CASES = [  # (p, q, mb, nb, kb, M, N, K, alpha, beta)
+    (2, 2, 16, 24, 20, 150, 170, 90, 1.5, -0.5),
+    (1, 4, 32, 16, 8, 64, 100, 77, 1.0, 0.0),
+]
+
+
+class ShmIpc:
+    """Host shared memory with DeviceIpc's interface (alloc / open / close / free / tensor)."""
+
+    def __init__(self):
+        self.segments = {}
+
+    def _addr(self, shm):
+        return np.frombuffer(shm.buf, dtype=np.uint8).ctypes.data
+
+    def alloc(self, nbytes):
+        from multiprocessing import shared_memory
+
+        shm = shared_memory.SharedMemory(create=True, size=max(int(nbytes), 8))
+        addr = self._addr(shm)
+        self.segments[addr] = shm
+        return addr, shm.name.encode().ljust(64, b"\0")
+
+    def open(self, handle):
+        from multiprocessing import shared_memory
+
+        shm = shared_memory.SharedMemory(name=handle.rstrip(b"\0").decode())
+        addr = self._addr(shm)
+        self.segments[addr] = shm
+        return addr
+
+    def close(self, ptr):
+        pass  # mappings go with the process
+
+    def free(self, ptr):
+        self.segments[ptr].unlink()
+
+    def tensor(self, ptr, shape):
+        import torch
+
+        n = int(np.prod(shape))
+        return torch.from_numpy(np.frombuffer((ctypes.c_double * n).from_address(ptr), dtype=np.float64).reshape(shape))
+
+    def synchronize(self):
+        pass
+
+
+class ScheduleHandle:
+    """dgt.Handle.summa_rank executed on host addresses: the segments dgt_summa_schedule
+    returns, each a rank-local GEMM reading the owners' memory."""
+
+    @staticmethod
+    def _mat(addr, rows, cols, ld):
+        n = ld * (cols - 1) + rows if rows and cols else 1
+        buf = np.frombuffer((ctypes.c_double * n).from_address(addr), dtype=np.float64)
+        return np.lib.stride_tricks.as_strided(buf, shape=(rows, cols), strides=(8, 8 * ld))
+
+    def summa_rank(self, rank, p, q, mb, nb, kb, M, N, K, alpha, A_ptrs, lldA, B_ptrs, lldB, beta, C, ldc,
+                   mode=None, slices=7):
+        import dgt
+
+        m, n = dgt.numroc(M, mb, rank // q, 0, p), dgt.numroc(N, nb, rank % q, 0, q)
+        if m == 0 or n == 0:
+            return
+        c = self._mat(C, m, n, ldc)
+        first = True
+        for a, b, lda, ldb, k in dgt.summa_schedule(rank, p, q, mb, nb, kb, M, N, K, A_ptrs, lldA, B_ptrs, lldB):
+            prod = self._mat(a, m, k, lda) @ self._mat(b, k, n, ldb) if k else 0.0
+            c[...] = alpha * prod + (beta if first else 1.0) * c
+            first = False
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    for sub in ("", "oracle", "distributed-gemm-thesis_b200", "tests"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    import oracle as O
+    from dgt.dist import PeerSumma
+    from test_dist_summa_gloo import _local_tensor, _scatter
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
+            A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
+            S = PeerSumma(p, q, mb, nb, kb, M, N, K, ipc=ShmIpc(), handle=ScheduleHandle())
+            la, lb, lc = _scatter(A, mb, kb, p, q)[rank], _scatter(B, kb, nb, p, q)[rank], _scatter(C, mb, nb, p, q)[rank]
+            S.A_loc.copy_(_local_tensor(la))
+            S.B_loc.copy_(_local_tensor(lb))
+            tC = _local_tensor(lc)
+            S.multiply(alpha, beta, tC)
+            # the owners' A and B are untouched by the peers' reads
+            assert torch.equal(S.A_loc, _local_tensor(la)) and torch.equal(S.B_loc, _local_tensor(lb))
+            rows, cols = lc.shape
+            out.put((n_case, rank, tC.numpy()[:cols, :rows].T.copy()))
+            S.close()
+        dist.barrier()
+    except Exception:
+        import traceback
+
+        out.put((-1, rank, traceback.format_exc()))
+        raise
+    finally:
+        dist.destroy_process_group()
+
+
+def test_peer_summa_four_gloo_ranks():
+    import torch.multiprocessing as mp
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as O
+    from test_dist_summa_gloo import _gather
+
+    world = 4
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, out)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    results = {}
+    for _ in range(world * len(CASES)):
+        n_case, rank, got = out.get(timeout=180)
+        if n_case < 0:
+            for pr in procs:
+                pr.join(timeout=30)
+            pytest.fail(f"rank {rank} failed:\n{got}")
+        results[(n_case, rank)] = got
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
+        A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
+        G = _gather([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
+        assert O.rel_errors(G, O.dgemm(A, B, alpha, beta, C))[1] <= 1e-13, n_case
