@@ -355,11 +355,29 @@ class PeerSumma:
         self.lldB = [max(1, local_rows(K, kb, r // q, p)) for r in range(P)]
         colsA = max(1, local_rows(K, kb, rank % q, q))
         colsB = max(1, local_rows(N, nb, rank % q, q))
-        self._own = [self.ipc.alloc(8 * self.lldA[rank] * colsA), self.ipc.alloc(8 * self.lldB[rank] * colsB)]
-        handles = [None] * world
-        dist.all_gather_object(handles, (self._own[0][1], self._own[1][1]))
-        self.A_ptrs = [self._own[0][0] if r == rank else self.ipc.open(handles[r][0]) for r in range(P)]
-        self.B_ptrs = [self._own[1][0] if r == rank else self.ipc.open(handles[r][1]) for r in range(P)]
+        self._own, opened = [], []
+        try:
+            self._own.append(self.ipc.alloc(8 * self.lldA[rank] * colsA))
+            self._own.append(self.ipc.alloc(8 * self.lldB[rank] * colsB))
+            handles = [None] * world
+            dist.all_gather_object(handles, (self._own[0][1], self._own[1][1]))
+            self.A_ptrs, self.B_ptrs = [], []
+            for r in range(P):
+                for ptrs, own, h in ((self.A_ptrs, self._own[0][0], handles[r][0]),
+                                     (self.B_ptrs, self._own[1][0], handles[r][1])):
+                    if r == rank:
+                        ptrs.append(own)
+                    else:
+                        ptrs.append(self.ipc.open(h))
+                        opened.append(ptrs[-1])
+        except Exception:
+            # give back what this rank took; peers see the failure at their next collective
+            for ptr in opened:
+                self.ipc.close(ptr)
+            for ptr, _ in self._own:
+                self.ipc.free(ptr)
+            self._own = []
+            raise
         self.A_loc = self.ipc.tensor(self._own[0][0], (colsA, self.lldA[rank]))
         self.B_loc = self.ipc.tensor(self._own[1][0], (colsB, self.lldB[rank]))
         self.m = local_rows(M, mb, rank // q, p)

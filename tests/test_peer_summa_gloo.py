@@ -160,3 +160,61 @@ def test_peer_summa_four_gloo_ranks():
         A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
         G = _gather([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
         assert O.rel_errors(G, O.dgemm(A, B, alpha, beta, C))[1] <= 1e-13, n_case
+
+
+class _FailingOpenIpc(ShmIpc):
+    def __init__(self):
+        super().__init__()
+        self.freed = []
+
+    def open(self, handle):
+        raise RuntimeError("mapping refused")
+
+    def free(self, ptr):
+        self.freed.append(ptr)  # unlinked after the barrier: the peer may still be mapping it
+
+
+def _failing_rank(rank, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    for sub in ("", "distributed-gemm-thesis_b200", "tests"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    from dgt.dist import PeerSumma
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=2, timeout=datetime.timedelta(seconds=60))
+    try:
+        ipc = _FailingOpenIpc() if rank == 1 else ShmIpc()
+        own = []
+        try:
+            S = PeerSumma(1, 2, 16, 16, 16, 32, 32, 32, ipc=ipc, handle=ScheduleHandle())
+            own = [ptr for ptr, _ in S._own]
+            out.put((rank, "built", len(S.A_ptrs)))
+        except RuntimeError as e:
+            out.put((rank, str(e), len(ipc.freed)))
+        dist.barrier()
+        for ptr in own + getattr(ipc, "freed", []):
+            ShmIpc.free(ipc, ptr)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_peer_summa_setup_failure_releases_buffers():
+    """A rank that cannot map a peer's buffer raises, after freeing the two buffers it
+    allocated; the group is still usable (a barrier completes)."""
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_rank, args=(r, port, out)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    got = dict((r, (msg, n)) for r, msg, n in (out.get(timeout=120) for _ in procs))
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    assert got[0] == ("built", 2)
+    assert got[1] == ("mapping refused", 2)
