@@ -10,7 +10,8 @@
  * one rank's share of the SUMMA (dgt_summa_rank), the form a multi-GPU run uses with other
    GPUs' buffers in its pointer arrays, against the whole-grid dgt_summa;
  * PeerSumma over CUDA IPC buffers (dgt_ipc_*): one process, and two processes sharing the
-   GPU that read each other's panels."""
+   GPU that read each other's panels;
+ * the benchmark command line (bin/dgt_cublas25d_benchmark) with its CSV rows."""
 import os
 import subprocess
 import sys
@@ -299,3 +300,21 @@ def test_peer_summa_two_processes_share_one_gpu():
     rank's dgt_summa_rank reads its peer's panels directly.  The kernels only read data that
     host barriers have published; neither waits on the other."""
     _run_peer(2, 1, 2)
+
+
+def test_benchmark_cli_on_gpu(tmp_path):
+    """The built dgt_cublas25d_benchmark (the reference's cuBLAS25Benchmark command line):
+    a pre-distributed run and a full-offload run append their CSV rows."""
+    import pandas as pd
+
+    exe = os.path.join(ROOT, "distributed-gemm-thesis_b200", "bin", "dgt_cublas25d_benchmark")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "distributed-gemm-thesis_b200")], check=True)
+    for extra in ([], ["1"]):
+        r = subprocess.run([exe, "NN", "512", "512", "512", "1.0", "0.0", "4", "4", "2", "2", "devices", *extra,
+                            "--machine", "b200test", "--logdir", str(tmp_path)], capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+    for kind in ("PreDistributed", "FullOffload"):
+        df = pd.read_csv(tmp_path / f"DGEMM_execution_logs-{kind}_GEMM-b200test-2.5DCANNON-dgt.csv", header=0)
+        assert len(df) == 2 and (df["GFlops"] > 0).all() and (df["StackSize"] == 2).all()
