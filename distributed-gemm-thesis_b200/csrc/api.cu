@@ -737,6 +737,52 @@ dgt_status dgt_cannon25d(dgt_handle_t h, int64_t M, int32_t p, int32_t c, char t
     return launch_stack_reduce(h, tile, p * p, c - 1, C_tiles, W, (int64_t)p * p * tile);
 }
 
+dgt_status dgt_cannon25d_rank(dgt_handle_t h, int64_t M, int32_t p, int32_t c, int32_t rank, char ta, char tb,
+                              double alpha, const double* const* A_tiles, const double* const* B_tiles, double beta,
+                              double* C_tile, dgt_fp64_mode mode, int slices) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (!A_tiles || !B_tiles || !C_tile) return fail(h, DGT_ERROR_INVALID_VALUE, "null tile array or C tile");
+    if (p <= 0 || c <= 0 || p % c != 0) return fail(h, DGT_ERROR_INVALID_VALUE, "need p % c == 0");
+    if (M <= 0 || M % p != 0) return fail(h, DGT_ERROR_INVALID_VALUE, "need M % p == 0");
+    if (!valid_op(ta) || !valid_op(tb)) return fail(h, DGT_ERROR_INVALID_VALUE, "transpose must be N, T or C");
+    if (rank < 0 || rank >= p * p * c) return fail(h, DGT_ERROR_INVALID_VALUE, "rank outside the grid");
+    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
+    const int64_t lm = M / p;
+    const int pc3 = p / c;
+    const int k = rank / (p * p), i = (rank / p) % p, j = rank % p;
+    std::vector<int> order(pc3);
+    cannon_order(p, c, i, j, k, order.data());
+    Problem pr{};
+    pr.m = lm;
+    pr.n = lm;
+    pr.alpha = alpha;
+    pr.beta = (k == 0) ? beta : 0.0;  // the other stacks' partial sums start at 0
+    pr.C = C_tile;
+    pr.ldc = lm;
+    pr.transa = is_trans(ta);
+    pr.transb = is_trans(tb);
+    pr.seg_begin = 0;
+    pr.seg_count = pc3;
+    std::vector<KSegment> segs;
+    for (int s = 0; s < pc3; ++s) {
+        int t = order[s];
+        segs.push_back(KSegment{A_tiles[i * p + t], B_tiles[t * p + j], lm, lm, lm});
+    }
+    std::vector<Problem> probs{pr};
+    return (mode == DGT_FP64_NATIVE) ? launch_dmma_grouped(h, probs, segs)
+                                     : run_problems_emulated(h, probs, segs, mode, slices);
+}
+
+dgt_status dgt_reduce_tiles(dgt_handle_t h, double* C, const double* const* parts, int32_t nparts, int64_t elems) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (elems < 0 || nparts < 0) return fail(h, DGT_ERROR_INVALID_VALUE, "negative size");
+    if (elems == 0 || nparts == 0) return DGT_SUCCESS;
+    if (!C || !parts) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    for (int s = 0; s < nparts; ++s)
+        if (!parts[s]) return fail(h, DGT_ERROR_INVALID_VALUE, "null part");
+    return launch_tile_sum(h, C, parts, nparts, elems);
+}
+
 // ---- layout ------------------------------------------------------------------------------------
 
 static dgt_status check_cyclic(dgt_context* h, int64_t M, int64_t N, int64_t mb, int64_t nb, int p, int q,

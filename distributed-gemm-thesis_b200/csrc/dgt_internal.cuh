@@ -160,6 +160,8 @@ dgt_status launch_block_cyclic(dgt_context* h, bool to_local, int64_t M, int64_t
 dgt_status launch_strided_copies(dgt_context* h, const std::vector<HostCopy>& copies);
 dgt_status launch_strided_copy_f32(dgt_context* h, const float* src, float* dst, int64_t ldS, int64_t ldD,
                                    int64_t rows, int64_t cols);
+// C[e] += parts[0][e] + ... + parts[nparts-1][e] (plain loads: parts may be peer memory).
+dgt_status launch_tile_sum(dgt_context* h, double* C, const double* const* parts, int nparts, int64_t elems);
 // C[t] += sum_{s < stacks} W[s*stack_stride + t*elems_per_tile + e] for every tile t.
 dgt_status launch_stack_reduce(dgt_context* h, int64_t elems_per_tile, int tiles, int stacks, double* const* C,
                                const double* W, int64_t stack_stride);

@@ -198,7 +198,26 @@ __global__ void __launch_bounds__(LAYOUT_THREADS) stack_reduce_kernel(const __gr
     }
 }
 
+struct TileSumParams {
+    int64_t elems;
+    int nparts;
+    double* C;
+    const double* parts[MAX_RANKS];
+};
+
+// C[e] += parts[0][e] + parts[1][e] + ... in that order (the stack reduction's order), with
+// plain loads, so the parts may be other GPUs' memory mapped into this one.
+__global__ void __launch_bounds__(LAYOUT_THREADS) tile_sum_kernel(const __grid_constant__ TileSumParams P) {
+    for (int64_t e = (int64_t)blockIdx.x * LAYOUT_THREADS + threadIdx.x; e < P.elems;
+         e += (int64_t)gridDim.x * LAYOUT_THREADS) {
+        double v = P.C[e];
+        for (int s = 0; s < P.nparts; ++s) v += P.parts[s][e];
+        P.C[e] = v;
+    }
+}
+
 thread_local CyclicParams t_cyc;
+thread_local TileSumParams t_sum;
 thread_local CopyParams<double> t_copy;
 thread_local CopyParams<float> t_copy_f32;
 thread_local ReduceParams t_red;
@@ -266,6 +285,19 @@ dgt_status launch_strided_copy_f32(dgt_context* h, const float* src, float* dst,
     P.d[0] = CopyDesc<float>{src, dst, ldS, ldD, rows, cols, 0};
     strided_copy_kernel<float><<<layout_grid(h, cols), LAYOUT_THREADS, 0, h->stream>>>(P);
     DGT_LAUNCH_CHECK(h, "strided_copy_kernel<float>");
+    return DGT_SUCCESS;
+}
+
+dgt_status launch_tile_sum(dgt_context* h, double* C, const double* const* parts, int nparts, int64_t elems) {
+    if (nparts > MAX_RANKS) return fail(h, DGT_ERROR_UNSUPPORTED, "more than 256 parts");
+    TileSumParams& P = t_sum;
+    P.elems = elems;
+    P.nparts = nparts;
+    P.C = C;
+    for (int s = 0; s < nparts; ++s) P.parts[s] = parts[s];
+    int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(elems, LAYOUT_THREADS), (int64_t)h->num_sms * 8));
+    tile_sum_kernel<<<grid, LAYOUT_THREADS, 0, h->stream>>>(P);
+    DGT_LAUNCH_CHECK(h, "tile_sum_kernel");
     return DGT_SUCCESS;
 }
 

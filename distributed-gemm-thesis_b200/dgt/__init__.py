@@ -77,6 +77,9 @@ SIGNATURES = [
                            _vp, ctypes.c_double, _vp, _vp, _c_i32, ctypes.c_int]),
     ("dgt_summa_rank", _c_i32, [_vp, ctypes.POINTER(GridLayout), _c_i32, _c_i64, _c_i64, _c_i64, ctypes.c_double,
                                 _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _c_i64, _c_i32, ctypes.c_int]),
+    ("dgt_cannon25d_rank", _c_i32, [_vp, _c_i64, _c_i32, _c_i32, _c_i32, ctypes.c_char, ctypes.c_char,
+                                    ctypes.c_double, _vp, _vp, ctypes.c_double, _vp, _c_i32, ctypes.c_int]),
+    ("dgt_reduce_tiles", _c_i32, [_vp, _vp, _vp, _c_i32, _c_i64]),
     ("dgt_ipc_alloc", _c_i32, [ctypes.c_size_t, ctypes.POINTER(_vp), ctypes.c_char_p]),
     ("dgt_ipc_open", _c_i32, [ctypes.c_char_p, ctypes.POINTER(_vp)]),
     ("dgt_ipc_close", _c_i32, [_vp]),
@@ -272,6 +275,16 @@ class Handle:
         self._check(self.lib.dgt_summa_rank(self.h, ctypes.byref(L), rank, M, N, K, alpha, _ptrs(A_locals),
                                             _i64s(lldA), _ptrs(B_locals), _i64s(lldB), beta, _vp(C), ldc, mode,
                                             slices))
+
+    def cannon25d_rank(self, M, p, c, rank, alpha, A_tiles, B_tiles, beta, C_tile, ta="N", tb="N",
+                       mode=FP64_NATIVE, slices=7):
+        """Rank `rank`'s stack partial of the 2.5D Cannon; A_tiles / B_tiles may be peer-mapped."""
+        self._check(self.lib.dgt_cannon25d_rank(self.h, M, p, c, rank, ta.encode(), tb.encode(), alpha,
+                                                _ptrs(A_tiles), _ptrs(B_tiles), beta, _vp(C_tile), mode, slices))
+
+    def reduce_tiles(self, C, parts, elems):
+        """C[e] += sum of parts[s][e], in order (parts may be peer-mapped)."""
+        self._check(self.lib.dgt_reduce_tiles(self.h, _vp(C), _ptrs(parts), len(parts), elems))
 
     def cannon25d(self, M, p, c, alpha, A_tiles, B_tiles, beta, C_tiles, ta="N", tb="N", mode=FP64_NATIVE,
                   slices=7):

@@ -407,3 +407,105 @@ class PeerSumma:
         for ptr, _ in self._own:
             self.ipc.free(ptr)
         self._own = []
+
+
+class PeerCannon25D:
+    """2.5D Cannon across p*p*c processes with its communication fused into the kernels: the
+    stack-0 ranks hold A_ij and B_ij in buffers every rank maps (DeviceIpc), each rank's
+    dgt_cannon25d_rank reads the tiles of its k-blocks straight from their owners (no stack
+    broadcast, no skew, no shifts), and each stack-0 rank sums the other stacks' partials
+    by reading them from their ranks (dgt_reduce_tiles) -- the reduction reads the partial
+    sums where the GEMMs left them.  Same k-block order and summation order as the in-device
+    dgt_cannon25d.
+
+        S = PeerCannon25D(p, c, M)            # collective
+        S.A_tile[...] = ...; S.B_tile[...] = ...  (stack-0 ranks: tile (i, j), column-major)
+        S.multiply(alpha, beta, C_tile)       # stack 0: the C tile, result in place
+        S.close()                             # collective
+
+    Host barriers separate publishing the tiles, the GEMMs, and the reduction; no kernel
+    waits on another process.
+    """
+
+    def __init__(self, p, c, M, ipc=None, handle=None, mode=dgt.FP64_NATIVE, slices=7):
+        import torch.distributed as dist
+
+        if not dist.is_initialized():
+            raise RuntimeError("PeerCannon25D needs an initialised torch.distributed process group")
+        if p <= 0 or c <= 0 or p % c or M <= 0 or M % p:
+            raise ValueError("need p % c == 0 and M % p == 0")
+        world, rank = dist.get_world_size(), dist.get_rank()
+        if world != p * p * c:
+            raise ValueError(f"world size {world} != p*p*c = {p * p * c}")
+        self.p, self.c, self.M, self.lm, self.rank = p, c, M, M // p, rank
+        self.k, self.i, self.j = rank // (p * p), (rank // p) % p, rank % p
+        self.mode, self.slices = mode, slices
+        self.ipc = ipc or DeviceIpc()
+        if handle is None:
+            import torch
+
+            handle = dgt.Handle(stream=torch.cuda.current_stream().cuda_stream)
+        self.h = handle
+        nbytes = 8 * self.lm * self.lm
+        self._own, opened = [], []
+        try:
+            # stack 0 owns the A and B tiles; the other stacks own their partial C
+            names = ("A", "B") if self.k == 0 else ("P",)
+            mine = {}
+            for name in names:
+                ptr, hnd = self.ipc.alloc(nbytes)
+                self._own.append((ptr, hnd))
+                mine[name] = (ptr, hnd)
+            handles = [None] * world
+            dist.all_gather_object(handles, {n: h for n, (_, h) in mine.items()})
+
+            def mapped(r, name):
+                if r == rank:
+                    return mine[name][0]
+                ptr = self.ipc.open(handles[r][name])
+                opened.append(ptr)
+                return ptr
+
+            self.A_ptrs = [mapped(r, "A") for r in range(p * p)]
+            self.B_ptrs = [mapped(r, "B") for r in range(p * p)]
+            base = self.i * p + self.j
+            self.P_ptrs = [mapped(k * p * p + base, "P") for k in range(1, c)] if self.k == 0 else []
+        except Exception:
+            for ptr in opened:
+                self.ipc.close(ptr)
+            for ptr, _ in self._own:
+                self.ipc.free(ptr)
+            self._own = []
+            raise
+        self._opened = opened
+        self.A_tile = self.ipc.tensor(mine["A"][0], (self.lm, self.lm)) if self.k == 0 else None
+        self.B_tile = self.ipc.tensor(mine["B"][0], (self.lm, self.lm)) if self.k == 0 else None
+        self._partial = mine["P"][0] if self.k > 0 else None
+
+    def multiply(self, alpha: float, beta: float, C_tile=None) -> None:
+        import torch.distributed as dist
+
+        if self.k == 0 and (C_tile is None or tuple(C_tile.shape) != (self.lm, self.lm)):
+            raise ValueError(f"stack-0 ranks pass their ({self.lm}, {self.lm}) C tile")
+        c_ptr = C_tile.data_ptr() if self.k == 0 else self._partial
+        self.ipc.synchronize()
+        dist.barrier()  # every stack-0 tile is published
+        self.h.cannon25d_rank(self.M, self.p, self.c, self.rank, alpha, self.A_ptrs, self.B_ptrs, beta, c_ptr,
+                              mode=self.mode, slices=self.slices)
+        self.ipc.synchronize()
+        dist.barrier()  # every partial is complete
+        if self.k == 0 and self.P_ptrs:
+            self.h.reduce_tiles(c_ptr, self.P_ptrs, self.lm * self.lm)
+            self.ipc.synchronize()
+        dist.barrier()  # no partial or tile is read any more
+
+    def close(self) -> None:
+        import torch.distributed as dist
+
+        for ptr in self._opened:
+            self.ipc.close(ptr)
+        self._opened = []
+        dist.barrier()
+        for ptr, _ in self._own:
+            self.ipc.free(ptr)
+        self._own = []

@@ -11,7 +11,9 @@
    GPUs' buffers in its pointer arrays, against the whole-grid dgt_summa;
  * PeerSumma over CUDA IPC buffers (dgt_ipc_*): one process, and two processes sharing the
    GPU that read each other's panels;
- * the benchmark command line (bin/dgt_cublas25d_benchmark) with its CSV rows."""
+ * the benchmark command line (bin/dgt_cublas25d_benchmark) with its CSV rows;
+ * the 2.5D Cannon per rank (dgt_cannon25d_rank + dgt_reduce_tiles) against the in-device
+   dgt_cannon25d, and PeerCannon25D as eight processes sharing the GPU."""
 import os
 import subprocess
 import sys
@@ -318,3 +320,108 @@ def test_benchmark_cli_on_gpu(tmp_path):
     for kind in ("PreDistributed", "FullOffload"):
         df = pd.read_csv(tmp_path / f"DGEMM_execution_logs-{kind}_GEMM-b200test-2.5DCANNON-dgt.csv", header=0)
         assert len(df) == 2 and (df["GFlops"] > 0).all() and (df["StackSize"] == 2).all()
+
+
+def test_cannon_rank_and_reduce_match_in_device(h):
+    """Every rank's dgt_cannon25d_rank (stack partials in separate buffers) followed by
+    dgt_reduce_tiles into the stack-0 tiles equals the in-device dgt_cannon25d: same
+    k-block order, same summation order (relative Frobenius <= 1e-14 per tile)."""
+    import torch
+
+    M, p, c = 512, 4, 2
+    lm = M // p
+    A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), O.uniform((M, M), 3)
+    dA, dB, dC = dev(A), dev(B), dev(C)
+    tiles = lambda: [torch.zeros((lm, lm), dtype=torch.float64, device="cuda") for _ in range(p * p)]
+    tA, tB, tC = tiles(), tiles(), tiles()
+    h.pack_cannon2d(M, p, ptr(dA), ptr(dB), ptr(dC), [ptr(x) for x in tA], [ptr(x) for x in tB],
+                    [ptr(x) for x in tC])
+    mine = [x.clone() for x in tC]
+    partials = [torch.full((lm, lm), float("nan"), dtype=torch.float64, device="cuda") for _ in range(p * p * (c - 1))]
+    pA, pB = [ptr(x) for x in tA], [ptr(x) for x in tB]
+    h.cannon25d(M, p, c, 1.5, pA, pB, -0.5, [ptr(x) for x in tC])
+    for rank in range(p * p * c):
+        k, r = rank // (p * p), rank % (p * p)
+        out = mine[r] if k == 0 else partials[(k - 1) * p * p + r]
+        h.cannon25d_rank(M, p, c, rank, 1.5, pA, pB, -0.5, ptr(out))
+    for r in range(p * p):
+        h.reduce_tiles(ptr(mine[r]), [ptr(partials[(k - 1) * p * p + r]) for k in range(1, c)], lm * lm)
+    torch.cuda.synchronize()
+    h.check_device()
+    for r in range(p * p):
+        assert O.rel_errors(mine[r].cpu().numpy(), tC[r].cpu().numpy())[1] <= 1e-14, r
+
+
+def _peer_cannon_rank(rank, p, c, M, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    for sub in ("", "oracle", "distributed-gemm-thesis_b200", "tests"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    import oracle as O
+    from dgt.dist import PeerCannon25D
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=p * p * c, timeout=datetime.timedelta(seconds=180))
+    try:
+        torch.cuda.set_device(0)
+        lm = M // p
+        k, i, j = rank // (p * p), (rank // p) % p, rank % p
+        A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), O.uniform((M, M), 3)
+        tile = lambda X: torch.from_numpy(np.ascontiguousarray(X[i * lm:(i + 1) * lm, j * lm:(j + 1) * lm].T)).cuda()
+        S = PeerCannon25D(p, c, M)
+        C_tile = None
+        if k == 0:
+            S.A_tile.copy_(tile(A))
+            S.B_tile.copy_(tile(B))
+            C_tile = tile(C)
+        S.multiply(1.5, -0.5, C_tile)
+        S.h.check_device()
+        if k == 0:
+            out.put((rank, C_tile.cpu().numpy().T.copy()))
+        S.close()
+    except Exception:
+        import traceback
+
+        out.put((-1, traceback.format_exc()))
+        raise
+    finally:
+        dist.destroy_process_group()
+
+
+def test_peer_cannon_eight_processes_share_one_gpu():
+    """PeerCannon25D on a 2 x 2 x 2 grid, eight processes on one GPU: tiles read from their
+    owners through dgt_ipc_open, the stack-1 partials summed into stack 0 by reading them
+    from their ranks.  Kernels only read data host barriers have published."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    p, c, M = 2, 2, 256
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = [ctx.Process(target=_peer_cannon_rank, args=(r, p, c, M, port, out)) for r in range(p * p * c)]
+    for pr in procs:
+        pr.start()
+    tiles = {}
+    for _ in range(p * p):
+        rank, got = out.get(timeout=400)
+        if rank < 0:
+            for pr in procs:
+                pr.join(timeout=60)
+            pytest.fail(got)
+        tiles[rank] = got
+    for pr in procs:
+        pr.join(timeout=180)
+        assert pr.exitcode == 0
+    lm = M // p
+    G = np.zeros((M, M))
+    for r, t in tiles.items():
+        G[(r // p) * lm:(r // p + 1) * lm, (r % p) * lm:(r % p + 1) * lm] = t
+    A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), O.uniform((M, M), 3)
+    assert O.rel_errors(G, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
