@@ -689,8 +689,71 @@ def workload_once(args):
     h.close()
 
 
+def workload_edges(args):
+    """Transfers at the edges of the path, each checked bit for bit:
+    (1) the block-cyclic scatter and gather of the 15000 x 17000 C of the ragged SUMMA
+        configuration (4 x 4 grid, 256 blocks) with the global matrix in page-locked host
+        memory (dgt_pack_block_cyclic_host / dgt_unpack_block_cyclic_host: one pass over the
+        host link, permuted on the way), against a plain page-locked copy of the same bytes
+        by the copy engine, the host link's own rate;
+    (2) the float strided copy (dgt_copy_block_f32) of a 32768 x 16384 float matrix from
+        leading dimension 32768 to 32772 (every run off the 16-byte phase), against HBM
+        bandwidth (L2 flushed before each call)."""
+    torch, dgt, h = _setup()
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    sampler = ClockSampler(0)
+    sampler.start()
+    # (1) host-memory scatter / gather
+    M, N, b, p, q = 15000, 17000, 256, 4, 4
+    G = torch.empty((N, M), dtype=torch.float64).uniform_(-1.0, 1.0, generator=torch.Generator().manual_seed(SEED))
+    Gp = G.pin_memory()
+    back = torch.zeros_like(Gp).pin_memory()
+    dG = torch.empty((N, M), dtype=torch.float64, device="cuda")
+    rows = [dgt.numroc(M, b, r // q, 0, p) for r in range(p * q)]
+    cols = [dgt.numroc(N, b, r % q, 0, q) for r in range(p * q)]
+    lld = [max(x, 1) for x in rows]
+    mk = lambda: [torch.empty((max(c, 1), l), dtype=torch.float64, device="cuda") for c, l in zip(cols, lld)]
+    locs, ref = mk(), mk()
+    lp, rp = [x.data_ptr() for x in locs], [x.data_ptr() for x in ref]
+    nbytes = 8 * M * N
+    pack_ms = _time_ms(torch, lambda: h.pack_block_cyclic_host(M, N, b, b, p, q, Gp.data_ptr(), M, lp, lld), 5)
+    h2d_ms = _time_ms(torch, lambda: dG.copy_(Gp, non_blocking=True), 5)
+    h.pack_block_cyclic(M, N, b, b, p, q, dG.data_ptr(), M, rp, lld)
+    unpack_ms = _time_ms(torch, lambda: h.unpack_block_cyclic_host(M, N, b, b, p, q, back.data_ptr(), M, lp, lld), 5)
+    d2h_ms = _time_ms(torch, lambda: back.copy_(dG, non_blocking=True), 5)
+    h.unpack_block_cyclic_host(M, N, b, b, p, q, back.data_ptr(), M, lp, lld)
+    torch.cuda.synchronize()
+    h.check_device()
+    same = all(torch.equal(a.view(torch.int64), r.view(torch.int64)) for a, r in zip(locs, ref)) and torch.equal(back, G)
+    gbs = lambda ms: nbytes / (ms * 1e-3) / 1e9
+    host = {"matrix": "15000 x 17000 f64 (C of the ragged SUMMA configuration), 4 x 4 grid, 256 blocks",
+            "bytes": nbytes, "scatter_from_host_GB/s": gbs(pack_ms), "plain_h2d_copy_GB/s": gbs(h2d_ms),
+            "gather_to_host_GB/s": gbs(unpack_ms), "plain_d2h_copy_GB/s": gbs(d2h_ms),
+            "scatter_frac_of_copy": h2d_ms / pack_ms, "gather_frac_of_copy": d2h_ms / unpack_ms, "bitwise": same}
+    del G, Gp, back, dG, locs, ref
+    torch.cuda.empty_cache()
+    # (2) float strided copy
+    R, C, ldD = 32768, 16384, 32772
+    S = torch.empty((C, R), dtype=torch.float32, device="cuda").uniform_(-1.0, 1.0)
+    D = torch.zeros((C, ldD), dtype=torch.float32, device="cuda")
+    f_ms = _time_ms(torch, lambda: h.copy_block_f32(R, C, S.data_ptr(), D.data_ptr(), R, ldD), 10, flush=flush)
+    torch.cuda.synchronize()
+    h.check_device()
+    f_bytes = 2 * 4 * R * C
+    fcopy = {"matrix": "32768 x 16384 f32, ld 32768 -> 32772", "bytes": f_bytes, "ms": f_ms,
+             "GB/s": f_bytes / (f_ms * 1e-3) / 1e9, "frac_of_hbm": f_bytes / (f_ms * 1e-3) / 1e9 / hbm,
+             "bitwise": bool(torch.equal(D[:, :R], S)) and bool((D[:, R:] == 0).all())}
+    clocks = sampler.stop()
+    print(json.dumps({"workload": "edges", "hbm_peak_gbs": hbm,
+                      "hbm_peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                      "host_memory_scatter": host, "copy_block_f32": fcopy, "clocks": clocks}))
+    h.close()
+
+
 WORKLOADS = {"summa": workload_summa, "precision": workload_precision, "fp32": workload_fp32,
-             "batching": workload_batching, "once": workload_once}
+             "batching": workload_batching, "once": workload_once, "edges": workload_edges}
 
 
 # ---- dgt arm ------------------------------------------------------------------------------------
