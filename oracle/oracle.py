@@ -212,6 +212,9 @@ class _Ref:
         L.ref_cannon_fulloffload_logged.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                                     ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, ctypes.c_int]
         L.ref_cannon_trace.argtypes = [ctypes.c_int, ctypes.c_int, _ip]
+        for name in ("ref_copy_block_f64", "ref_copy_block_f32"):
+            getattr(L, name).argtypes = [ctypes.c_longlong] * 2 + [ctypes.c_void_p] * 2 + [ctypes.c_longlong] * 2 + [
+                ctypes.c_int]
         L.ref_set_dgemm.argtypes = [ctypes.c_void_p]
         self._blas = None
 
@@ -321,6 +324,15 @@ class _Ref:
         self._check(self.L.ref_cannon_fulloffload_logged(str(log_dir).encode(), M, p, c, alpha, beta, _ptr(A), _ptr(B),
                                                          _ptr(C), runs))
         return C
+
+    def copy_block(self, rows, cols, src, dst, ldS, ldD, col_major=True):
+        """The reference's copyBlock<double> or <float> (by src's dtype) on flat host arrays;
+        returns the destination after the copy."""
+        src = np.ascontiguousarray(src)
+        dst = np.array(dst, dtype=src.dtype)
+        fn = self.L.ref_copy_block_f32 if src.dtype == np.float32 else self.L.ref_copy_block_f64
+        self._check(fn(rows, cols, src.ctypes.data, dst.ctypes.data, ldS, ldD, int(col_major)))
+        return dst
 
     def cannon_trace(self, p, c):
         pc3 = int((p * p * c / c ** 3) ** 0.5 + 1e-9)

@@ -16,6 +16,7 @@
 #include "2DBlockSequentialDecomposition.hpp"
 #include "25DCannon.hpp"
 #include "pblasDecomposition.hpp"
+#include "transfers.hpp"
 
 int fake_mpi_run(int size, const std::function<void(int)>& fn, std::string* err);
 extern "C" void ref_set_process_grid(int dRow, int dCol);
@@ -208,6 +209,19 @@ extern "C" int ref_cannon_fulloffload_logged(const char* dir, long long M, int p
         rc = -1;
     }
     return rc;
+}
+
+// The reference's copyBlock in its two instantiations (src/Transfers/sharedTransfers.cpp:29-63,
+// :87-88), on host memory through the CUDA test double: its contiguous shortcut included.
+extern "C" int ref_copy_block_f64(long long rows, long long cols, double* src, double* dst, long long ldS,
+                                  long long ldD, int colMajor) {
+    copyBlock<double>(rows, cols, src, dst, ldS, ldD, colMajor != 0);
+    return 0;
+}
+extern "C" int ref_copy_block_f32(long long rows, long long cols, float* src, float* dst, long long ldS,
+                                  long long ldD, int colMajor) {
+    copyBlock<float>(rows, cols, src, dst, ldS, ldD, colMajor != 0);
+    return 0;
 }
 
 // Step trace of the Cannon schedule: for every world rank and every local GEMM it

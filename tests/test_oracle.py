@@ -184,3 +184,36 @@ def test_block2d_live_against_reference(case):
             for x, y in zip(xs, ys):
                 assert np.array_equal(x, y)
         assert np.array_equal(O.orc().block2d_gather(a[2], M, N, P, cm), O.ref().block2d_gather(b[2], M, N, K, P, cm))
+
+
+def _strided(rows, cols, src, dst, ldS, ldD, col_major=True):
+    r, c = (rows, cols) if col_major else (cols, rows)
+    out = dst.copy()
+    for j in range(c):
+        out[j * ldD:j * ldD + r] = src[j * ldS:j * ldS + r]
+    return out
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference sources absent)")
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_reference_copy_block_instantiations(dtype):
+    """The reference's own copyBlock<float> and copyBlock<double> (the float instantiation is
+    what dgt_copy_block_f32 replaces) copy a strided block exactly as the strided restatement
+    the GPU tests hold the product to, except under their contiguous shortcut
+    (sharedTransfers.cpp:51: rows == ldS and columns == ldD after the swap), which copies
+    rows*columns contiguous elements whatever ldD is -- reproduced here, fixed in the product."""
+    R = O.ref()
+    rng = np.random.default_rng(3)
+    for rows, cols, ldS, ldD, cm in [(5, 7, 9, 6, True), (64, 3, 64, 64, True), (3, 64, 70, 65, False),
+                                     (1, 1, 1, 1, True), (17, 4, 20, 17, True), (4, 17, 20, 19, False)]:
+        r, c = (rows, cols) if cm else (cols, rows)
+        src = rng.standard_normal(ldS * c).astype(dtype)
+        dst = rng.standard_normal(ldD * c).astype(dtype)
+        assert np.array_equal(R.copy_block(rows, cols, src, dst, ldS, ldD, cm), _strided(rows, cols, src, dst, ldS, ldD, cm))
+    # the shortcut: rows == ldS, cols == ldD, but ldD != rows
+    rows, cols, ldS, ldD = 4, 6, 4, 6
+    src = rng.standard_normal(ldS * cols).astype(dtype)
+    dst = np.zeros(ldD * cols, dtype=dtype)
+    got = R.copy_block(rows, cols, src, dst, ldS, ldD, True)
+    assert np.array_equal(got[:rows * cols], src[:rows * cols])
+    assert not np.array_equal(got, _strided(rows, cols, src, dst, ldS, ldD, True))
