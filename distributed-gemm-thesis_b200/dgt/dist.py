@@ -51,6 +51,11 @@ class DgtOps:
         cols, ld = src.shape
         self.h.copy_block(rows, cols, src.data_ptr() + 8 * r0, dst.data_ptr(), ld, rows)
 
+    def copy(self, src, dst):
+        """dst <- src for two contiguous tensors of the same shape (one strided-copy launch)."""
+        cols, rows = src.shape
+        self.h.copy_block(rows, cols, src.data_ptr(), dst.data_ptr(), rows, rows)
+
     def gemm(self, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
         """C = alpha A B + beta C on column-major device buffers (tensors' storage)."""
         self.h.dgemm("N", "N", m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb, beta, C.data_ptr(), ldc,
@@ -233,7 +238,7 @@ class DistCannon25D:
             ops_list = []
             for snd, to, rcv, frm in ((send_a, to_a, recv_a, from_a), (send_b, to_b, recv_b, from_b)):
                 if to == self.rank and frm == self.rank:
-                    rcv.copy_(snd)
+                    ops.copy(snd, rcv)
                     continue
                 ops_list.append(dist.P2POp(dist.isend, snd, to))
                 ops_list.append(dist.P2POp(dist.irecv, rcv, frm))

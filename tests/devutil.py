@@ -54,6 +54,9 @@ class HostOps:
     def pack_rows(self, src, r0, rows, dst):
         dst.copy_(src[:, r0:r0 + rows])
 
+    def copy(self, src, dst):
+        dst.copy_(src)
+
     def gemm(self, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
         c = C.numpy()[:n, :m]  # column-major m x n view of C's storage
         prod = A.numpy()[:k, :m].T @ B.numpy()[:n, :k].T if k > 0 else np.zeros((m, n))

@@ -204,5 +204,8 @@ def test_device_ops_argument_arithmetic():
         tS, tT, tU = _local_tensor(S), _local_tensor(S.T.copy()), _local_tensor(S)
         DistCannon25D(1, 1, ops=DgtOps(_PtrHandle())).multiply(40, 2.0, tS, tT, 0.5, tU)
         assert O.rel_errors(tU.numpy().T, O.dgemm(S, S.T, 2.0, 0.5, S))[1] <= 1e-13
+        dst = torch.zeros_like(tS)
+        DgtOps(_PtrHandle()).copy(tS, dst)  # the skew's copy of a tile that stays put
+        assert torch.equal(dst, tS)
     finally:
         dist.destroy_process_group()
