@@ -17,6 +17,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CASES = [  # (p, q, mb, nb, kb, M, N, K, alpha, beta)
     (2, 2, 16, 24, 20, 150, 170, 90, 1.5, -0.5),
     (1, 4, 32, 16, 8, 64, 100, 77, 1.0, 0.0),
+    (4, 1, 16, 32, 12, 40, 50, 61, -2.0, 1.0),  # process row 3 owns no rows of A or C
+    (2, 2, 16, 16, 16, 48, 40, 0, 1.0, 0.25),   # K = 0: C = beta C
 ]
 
 
@@ -159,7 +161,8 @@ def test_peer_summa_four_gloo_ranks():
     for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
         A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
         G = _gather([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
-        assert O.rel_errors(G, O.dgemm(A, B, alpha, beta, C))[1] <= 1e-13, n_case
+        ref = O.dgemm(A, B, alpha, beta, C) if K > 0 else beta * C
+        assert O.rel_errors(G, ref)[1] <= 1e-13, n_case
 
 
 class _FailingOpenIpc(ShmIpc):
