@@ -209,3 +209,50 @@ def test_device_ops_argument_arithmetic():
         assert torch.equal(dst, tS)
     finally:
         dist.destroy_process_group()
+
+
+def _dying_rank_main(rank, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    for sub in ("", "oracle", "distributed-gemm-thesis_b200", "tests"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    import oracle as O
+    from devutil import HostOps
+    from dgt.dist import DistSumma
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=4, timeout=datetime.timedelta(seconds=10))
+    p, q, b, M, N, K = 2, 2, 16, 64, 64, 64
+    A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
+    tA, tB, tC = (_local_tensor(_scatter(X, b, b, p, q)[rank]) for X in (A, B, C))
+    S = DistSumma(p, q, b, b, b, ops=HostOps())
+    if rank == 3:
+        os._exit(1)  # leaves between steps: none of its collectives is in flight
+    try:
+        S.multiply(M, N, K, 1.0, tA, tB, 0.0, tC)
+        out.put((rank, "finished"))
+    except Exception:
+        out.put((rank, "error"))
+
+
+def test_dist_summa_rank_failure_ends_in_errors_not_a_hang():
+    """A rank that exits before the step loop: every other rank's step loop ends with an
+    error instead of waiting for ever -- the ranks sharing its process row or column at their
+    next broadcast (gloo notices the closed connection, or the 10 s group timeout ends the
+    wait), and rank 0, which shares no group with it, once those ranks have left its own
+    row and column broadcasts in turn."""
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dying_rank_main, args=(r, port, out)) for r in range(4)]
+    for pr in procs:
+        pr.start()
+    got = dict(out.get(timeout=120) for _ in range(3))
+    for pr in procs:
+        pr.join(timeout=60)
+    assert got == {0: "error", 1: "error", 2: "error"}
+    assert procs[3].exitcode == 1
