@@ -13,7 +13,8 @@
    GPU that read each other's panels;
  * the benchmark command line (bin/dgt_cublas25d_benchmark) with its CSV rows;
  * the 2.5D Cannon per rank (dgt_cannon25d_rank + dgt_reduce_tiles) against the in-device
-   dgt_cannon25d, and PeerCannon25D as eight processes sharing the GPU."""
+   dgt_cannon25d, and PeerCannon25D as eight processes sharing the GPU;
+ * guard bands around dgt_dgemm's operands in every FP64 mode (nothing written outside C)."""
 import os
 import subprocess
 import sys
@@ -425,3 +426,52 @@ def test_peer_cannon_eight_processes_share_one_gpu():
         G[(r // p) * lm:(r // p + 1) * lm, (r % p) * lm:(r % p + 1) * lm] = t
     A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), O.uniform((M, M), 3)
     assert O.rel_errors(G, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
+
+
+GUARD = 4096  # doubles of canary before and after every buffer (same allocation: a stray write cannot fault)
+CANARY = np.array([0x7FF4DEADBEEF0001], dtype=np.uint64).view(np.float64)[0]  # a signalling-NaN bit pattern
+
+
+def _guarded(X, ld):
+    """Device buffer: GUARD canaries, X column-major with leading dimension ld (padding rows
+    canary too), GUARD canaries.  Returns (tensor, pointer to X, host image of the buffer)."""
+    import torch
+
+    rows, cols = X.shape
+    img = np.full(2 * GUARD + ld * max(cols, 1), CANARY)
+    for j in range(cols):
+        img[GUARD + j * ld:GUARD + j * ld + rows] = X[:, j]
+    t = torch.from_numpy(img.copy()).cuda()
+    return t, t.data_ptr() + 8 * GUARD, img
+
+
+@pytest.mark.parametrize("mode,S", [(dgt.FP64_NATIVE, 7), (dgt.FP64_OZAKI_INT8, 7), (dgt.FP64_OZAKI2_INT8, 14)])
+def test_gemm_guard_bands(h, mode, S):
+    """dgt_dgemm writes C's m x n block and nothing else: the canaries around A, B and C and
+    the padding rows of C (ldc > m) are bit for bit unchanged, A and B are not modified, and C
+    matches the host FP64 GEMM -- for ragged, tiny and transposed shapes (the substitute for a
+    memory sanitizer on this pool)."""
+    import torch
+
+    for m, n, k, ta, tb in [(257, 131, 199, "N", "N"), (1, 1, 1, "N", "N"), (7, 13, 5, "T", "N"),
+                            (130, 129, 300, "N", "T"), (65, 33, 17, "T", "T")]:
+        A = O.uniform((k, m) if ta == "T" else (m, k), m + 1)
+        B = O.uniform((n, k) if tb == "T" else (k, n), n + 2)
+        C = O.uniform((m, n), k + 3)
+        lda, ldb, ldc = A.shape[0] + 3, B.shape[0] + 1, m + 5
+        tA, pA, iA = _guarded(A, lda)
+        tB, pB, iB = _guarded(B, ldb)
+        tC, pC, iC = _guarded(C, ldc)
+        h.dgemm(ta, tb, m, n, k, 1.5, pA, lda, pB, ldb, -0.5, pC, ldc, mode=mode, slices=S)
+        torch.cuda.synchronize()
+        h.check_device()
+        for t, img in ((tA, iA), (tB, iB)):
+            assert np.array_equal(t.cpu().numpy().view(np.uint64), img.view(np.uint64)), (m, n, k, ta, tb)
+        got = tC.cpu().numpy()
+        outside = np.ones(got.shape, dtype=bool)
+        for j in range(n):
+            outside[GUARD + j * ldc:GUARD + j * ldc + m] = False
+        assert np.array_equal(got[outside].view(np.uint64), iC[outside].view(np.uint64)), (m, n, k, ta, tb)
+        res = np.stack([got[GUARD + j * ldc:GUARD + j * ldc + m] for j in range(n)], axis=1)
+        tol = 1e-13 if mode != dgt.FP64_OZAKI_INT8 else 1e-12
+        assert O.rel_errors(res, O.dgemm(A, B, 1.5, -0.5, C, ta, tb))[1] <= tol, (m, n, k, ta, tb)
