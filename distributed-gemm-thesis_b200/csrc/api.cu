@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <initializer_list>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -971,6 +972,64 @@ dgt_status dgt_unpack_cannon2d(dgt_handle_t h, int64_t M, int32_t p, double* C, 
     for (int i = 0; i < p; ++i)
         for (int j = 0; j < p; ++j) copies.push_back(HostCopy{lC[i * p + j], C + lm * (j * M + i), lm, M, lm, lm});
     return launch_strided_copies(h, copies);
+}
+
+// The Cannon and 2D-block layouts with the global matrices in page-locked host memory: the
+// same strided-copy kernels read (or write) the host matrices through their device mapping,
+// so the host-device transfer and the permutation are one pass (decompose2D from host A, B,
+// C in the full-offload driver, src/25DCannon.cpp:413-414; deliverMatrix / gatherResult
+// from a host matrix).  A matrix of 0 bytes is passed through untouched (nothing is read).
+static bool alias_all(std::initializer_list<std::pair<const double**, size_t>> xs) {
+    for (auto& x : xs) {
+        if (x.second == 0) continue;
+        const void* a = host_range_alias(*x.first, x.second);
+        if (!a) return false;
+        *x.first = static_cast<const double*>(a);
+    }
+    return true;
+}
+static const char* kNotPinned =
+    "global matrix is not page-locked host memory mapped for the device (cudaHostAlloc / cudaHostRegister)";
+
+dgt_status dgt_pack_cannon2d_host(dgt_handle_t h, int64_t M, int32_t p, const double* A, const double* B,
+                                  const double* C, double* const* lA, double* const* lB, double* const* lC) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (p <= 0 || M <= 0 || M % p != 0) return fail(h, DGT_ERROR_INVALID_VALUE, "need M % p == 0");
+    if (!A || !B || !C || !lA || !lB || !lC) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    const size_t bytes = (size_t)M * (size_t)M * sizeof(double);
+    if (!alias_all({{&A, bytes}, {&B, bytes}, {&C, bytes}})) return fail(h, DGT_ERROR_INVALID_VALUE, kNotPinned);
+    return dgt_pack_cannon2d(h, M, p, A, B, C, lA, lB, lC);
+}
+
+dgt_status dgt_unpack_cannon2d_host(dgt_handle_t h, int64_t M, int32_t p, double* C, const double* const* lC) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (p <= 0 || M <= 0 || M % p != 0) return fail(h, DGT_ERROR_INVALID_VALUE, "need M % p == 0");
+    if (!C || !lC) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    const double* c = C;
+    if (!alias_all({{&c, (size_t)M * (size_t)M * sizeof(double)}})) return fail(h, DGT_ERROR_INVALID_VALUE, kNotPinned);
+    return dgt_unpack_cannon2d(h, M, p, const_cast<double*>(c), lC);
+}
+
+dgt_status dgt_pack_block2d_host(dgt_handle_t h, int64_t M, int64_t N, int64_t K, int32_t P, int32_t col_major,
+                                 const double* A, const double* B, const double* C, double* const* lA,
+                                 double* const* lB, double* const* lC) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (M < 0 || N < 0 || K < 0 || P <= 0) return fail(h, DGT_ERROR_INVALID_VALUE, "bad sizes");
+    if (!A || !B || !C || !lA || !lB || !lC) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    const size_t e = sizeof(double);
+    if (!alias_all({{&A, (size_t)M * K * e}, {&B, (size_t)K * N * e}, {&C, (size_t)M * N * e}}))
+        return fail(h, DGT_ERROR_INVALID_VALUE, kNotPinned);
+    return dgt_pack_block2d(h, M, N, K, P, col_major, A, B, C, lA, lB, lC);
+}
+
+dgt_status dgt_unpack_block2d_host(dgt_handle_t h, int64_t M, int64_t N, int32_t P, int32_t col_major, double* C,
+                                   const double* const* lC) {
+    if (!h) return DGT_ERROR_NOT_INITIALIZED;
+    if (M < 0 || N < 0 || P <= 0) return fail(h, DGT_ERROR_INVALID_VALUE, "bad sizes");
+    if (!C || !lC) return fail(h, DGT_ERROR_INVALID_VALUE, "null pointer");
+    const double* c = C;
+    if (!alias_all({{&c, (size_t)M * N * sizeof(double)}})) return fail(h, DGT_ERROR_INVALID_VALUE, kNotPinned);
+    return dgt_unpack_block2d(h, M, N, P, col_major, const_cast<double*>(c), lC);
 }
 
 dgt_status dgt_copy_block(dgt_handle_t h, int64_t rows, int64_t cols, const double* src, double* dst, int64_t ldS,

@@ -96,6 +96,10 @@ SIGNATURES = [
                                             _vp]),
     ("dgt_unpack_block_cyclic_host", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _c_i64,
                                               _vp, _vp]),
+    ("dgt_pack_cannon2d_host", _c_i32, [_vp, _c_i64, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("dgt_unpack_cannon2d_host", _c_i32, [_vp, _c_i64, _c_i32, _vp, _vp]),
+    ("dgt_pack_block2d_host", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp]),
+    ("dgt_unpack_block2d_host", _c_i32, [_vp, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _vp]),
     ("dgt_pack_block2d", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp]),
     ("dgt_unpack_block2d", _c_i32, [_vp, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _vp]),
     ("dgt_pack_cannon2d", _c_i32, [_vp, _c_i64, _c_i32, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -308,6 +312,22 @@ class Handle:
     def unpack_block_cyclic_host(self, M, N, mb, nb, p, q, G, ldg, locals_, lld):
         self._check(self.lib.dgt_unpack_block_cyclic_host(self.h, M, N, mb, nb, p, q, _vp(G), ldg, _ptrs(locals_),
                                                           _i64s(lld)))
+
+    def pack_cannon2d_host(self, M, p, A, B, C, lA, lB, lC):
+        """decompose2D from page-locked host A, B, C in one pass."""
+        self._check(self.lib.dgt_pack_cannon2d_host(self.h, M, p, _vp(A), _vp(B), _vp(C), _ptrs(lA), _ptrs(lB),
+                                                    _ptrs(lC)))
+
+    def unpack_cannon2d_host(self, M, p, C, lC):
+        self._check(self.lib.dgt_unpack_cannon2d_host(self.h, M, p, _vp(C), _ptrs(lC)))
+
+    def pack_block2d_host(self, M, N, K, P, col_major, A, B, C, lA, lB, lC):
+        """deliverMatrix from page-locked host A, B, C in one pass."""
+        self._check(self.lib.dgt_pack_block2d_host(self.h, M, N, K, P, int(col_major), _vp(A), _vp(B), _vp(C),
+                                                   _ptrs(lA), _ptrs(lB), _ptrs(lC)))
+
+    def unpack_block2d_host(self, M, N, P, col_major, C, lC):
+        self._check(self.lib.dgt_unpack_block2d_host(self.h, M, N, P, int(col_major), _vp(C), _ptrs(lC)))
 
     def pack_block2d(self, M, N, K, P, col_major, A, B, C, lA, lB, lC):
         self._check(self.lib.dgt_pack_block2d(self.h, M, N, K, P, int(col_major), _vp(A), _vp(B), _vp(C), _ptrs(lA),

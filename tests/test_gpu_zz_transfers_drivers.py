@@ -475,3 +475,65 @@ def test_gemm_guard_bands(h, mode, S):
         res = np.stack([got[GUARD + j * ldc:GUARD + j * ldc + m] for j in range(n)], axis=1)
         tol = 1e-13 if mode != dgt.FP64_OZAKI_INT8 else 1e-12
         assert O.rel_errors(res, O.dgemm(A, B, 1.5, -0.5, C, ta, tb))[1] <= tol, (m, n, k, ta, tb)
+
+
+def _pinned_flat(x, order):
+    import torch
+
+    t = torch.from_numpy(np.ascontiguousarray(np.asarray(x, order=order).ravel(order=order))).pin_memory()
+    return t, t.data_ptr()
+
+
+@pytest.mark.parametrize("M,N,K,P", [(13, 11, 5, 6), (333, 171, 80, 5)])
+@pytest.mark.parametrize("cm", [True, False])
+def test_block2d_from_host_equals_device_path(h, M, N, K, P, cm):
+    """deliverMatrix / gatherResult with A, B, C in page-locked host memory: the same locals
+    as the device-memory entries, bit for bit, and C restored by the gather."""
+    import torch
+
+    order = "F" if cm else "C"
+    A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
+    lA, lB, lC = O.orc().block2d_deliver(A, B, C, P, cm)
+    (hA, pA), (hB, pB), (hC, pC) = (_pinned_flat(x, order) for x in (A, B, C))
+    dA, dB, dC = hA.cuda(), hB.cuda(), hC.cuda()
+    mk = lambda ls: [torch.zeros(x.size, dtype=torch.float64, device="cuda") for x in ls]
+    oA, oB, oC, rA, rB, rC = mk(lA), mk(lB), mk(lC), mk(lA), mk(lB), mk(lC)
+    ps = lambda ts: [ptr(t) for t in ts]
+    h.pack_block2d_host(M, N, K, P, cm, pA, pB, pC, ps(oA), ps(oB), ps(oC))
+    h.pack_block2d(M, N, K, P, cm, ptr(dA), ptr(dB), ptr(dC), ps(rA), ps(rB), ps(rC))
+    back, pBk = _pinned_flat(np.zeros((M, N)), order)
+    h.unpack_block2d_host(M, N, P, cm, pBk, ps(oC))
+    torch.cuda.synchronize()
+    h.check_device()
+    for got, want in zip(oA + oB + oC, rA + rB + rC):
+        assert torch.equal(got, want)
+    assert torch.equal(back, hC)
+
+
+@pytest.mark.parametrize("M,p", [(300, 3), (512, 4)])
+def test_cannon2d_from_host_equals_device_path(h, M, p):
+    """decompose2D / reorderMatrix with A, B, C in page-locked host memory (the full-offload
+    driver's path): the same tiles as the device-memory entries, C restored, pageable
+    memory refused."""
+    import torch
+
+    A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), O.uniform((M, M), 3)
+    (hA, pA), (hB, pB), (hC, pC) = (_pinned_flat(x, "F") for x in (A, B, C))
+    dA, dB, dC = hA.cuda(), hB.cuda(), hC.cuda()
+    lm = M // p
+    mk = lambda: [torch.zeros((lm, lm), dtype=torch.float64, device="cuda") for _ in range(p * p)]
+    oA, oB, oC, rA, rB, rC = mk(), mk(), mk(), mk(), mk(), mk()
+    ps = lambda ts: [ptr(t) for t in ts]
+    h.pack_cannon2d_host(M, p, pA, pB, pC, ps(oA), ps(oB), ps(oC))
+    h.pack_cannon2d(M, p, ptr(dA), ptr(dB), ptr(dC), ps(rA), ps(rB), ps(rC))
+    back, pBk = _pinned_flat(np.zeros((M, M)), "F")
+    h.unpack_cannon2d_host(M, p, pBk, ps(oC))
+    torch.cuda.synchronize()
+    h.check_device()
+    for got, want in zip(oA + oB + oC, rA + rB + rC):
+        assert torch.equal(got, want)
+    assert torch.equal(back, hC)
+    pageable = np.asfortranarray(A)
+    with pytest.raises(dgt.DgtError) as e:
+        h.pack_cannon2d_host(M, p, pageable.ctypes.data, pA, pC, ps(oA), ps(oB), ps(oC))
+    assert e.value.status == dgt.INVALID_VALUE
