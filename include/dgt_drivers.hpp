@@ -11,9 +11,10 @@
 // dRow x dCol x c grid runs on the current device, so a row's TotalGPUs is 1 and the
 // virtual grid is in dRow, dCol, StackSize.  Per row:
 //
-//   DecompositionTime  full offload: tile allocation, host->device copy of A, B, C and the
-//                      decompose2D pack; pre-distributed: tile allocation only (the
-//                      reference times only the decomposer's constructor, :483-485)
+//   DecompositionTime  full offload: tile allocation and decompose2D -- one pass from host
+//                      memory when A, B, C are page-locked with ld = M, else a copy of A, B,
+//                      C to the device and the pack there; pre-distributed: tile allocation
+//                      only (the reference times only the decomposer's constructor, :483-485)
 //   ExecutionTime      one multiply, device time from CUDA events on the handle's stream
 //   GatherTime         reorderMatrix (device unpack, then the copy into C) when gathering
 //   CommunicationTime  0: the broadcast to the stacks and every shift are tile index
@@ -148,9 +149,16 @@ struct CannonRun {
         return ms * 1e-3;
     }
 
-    // reorderMatrix(0, C, localC): tiles -> dense device global -> C (host or device, ldc)
+    bool direct = false;  // A, B, C page-locked with ld == M: packed and gathered in one pass
+
+    // reorderMatrix(0, C, localC): tiles -> C (host or device, ldc)
     void gather(double* C, long long ldc) {
         const long long M = dec.M;
+        if (direct) {
+            check(ctx.get(), dgt_unpack_cannon2d_host(ctx.get(), M, dec.dRow, C, pc.data()));
+            cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+            return;
+        }
         DevBuf g = dev_alloc(size_t(M) * size_t(M));
         dec.reorderMatrix(g.get(), pc.data());
         cuda_check(cudaMemcpy2D(C, size_t(ldc) * 8, g.get(), size_t(M) * 8, size_t(M) * 8, size_t(M),
@@ -180,7 +188,15 @@ inline void fullOffloadSumma25Dgemm(char TransA, char TransB, long long M, long 
     if (lda < M || ldb < M || ldc < M) throw Error(DGT_ERROR_INVALID_VALUE, "leading dimension < M");
     const auto t0 = std::chrono::steady_clock::now();
     detail::CannonRun run(M, N, K, dRow, dCol, c, opt);
-    {
+    // page-locked A, B, C (as the reference's test allocates them) are read straight from host
+    // memory by the pack kernel; anything else is staged on the device first
+    run.direct = lda == M && ldb == M && ldc == M &&
+                 dgt_pack_cannon2d_host(run.ctx.get(), M, dRow, A, B, C, run.pa.data(), run.pb.data(),
+                                        run.pc.data()) == DGT_SUCCESS;
+    if (run.direct) {
+        detail::cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        check(run.ctx.get(), dgt_check_device(run.ctx.get()));
+    } else {
         const size_t MM = size_t(M) * size_t(M);
         detail::DevBuf gA = detail::dev_alloc(MM), gB = detail::dev_alloc(MM), gC = detail::dev_alloc(MM);
         const struct {

@@ -3,9 +3,10 @@
 //  * fullOffloadSumma25Dgemm from pageable host matrices (lda > M for A) with gather: after
 //    R runs, C = alpha A B (1 + beta + ... + beta^(R-1)) + beta^R C0 (every run applies the
 //    GEMM to the same tiles), checked against a host triple loop to 12 digits;
+//  * the same from page-locked A, B, C (ld = M): packed and gathered straight from host memory;
 //  * preDistributedSumma25Dgemm with gather: the operands are the documented seeded
 //    stream (global A, B, C from std::mt19937_64(seed)), so the host recomputes the result;
-//  * the CSV rows each run appends (read back by tests/test_gpu_mirror.py with pandas);
+//  * the CSV rows each run appends (read back with pandas by the Python tests that run this);
 //  * a non-square problem is rejected with DGT_ERROR_INVALID_VALUE, as the reference's
 //    constructor rejects it.
 #include <cuda_runtime.h>
@@ -66,6 +67,35 @@ static int test_full_offload(const char* dir, long long M, int p, int c, int run
     return e <= 1e-12 ? 0 : 1;
 }
 
+// A, B, C in page-locked host memory with ld = M, as the reference's test allocates them
+// (src/Tests/summa25Dtest.cpp:40-42): the driver packs and gathers straight from host memory.
+static int test_full_offload_pinned(const char* dir, long long M, int p, int c) {
+    double *A = nullptr, *B = nullptr, *C = nullptr;
+    const size_t n = size_t(M) * size_t(M);
+    if (cudaMallocHost((void**)&A, n * 8) != cudaSuccess || cudaMallocHost((void**)&B, n * 8) != cudaSuccess ||
+        cudaMallocHost((void**)&C, n * 8) != cudaSuccess)
+        return 1;
+    std::mt19937_64 rng(13);
+    std::uniform_real_distribution<double> U(-1.0, 1.0);
+    for (size_t i = 0; i < n; ++i) A[i] = U(rng);
+    for (size_t i = 0; i < n; ++i) B[i] = U(rng);
+    for (size_t i = 0; i < n; ++i) C[i] = U(rng);
+    std::vector<double> Av(A, A + n), Bv(B, B + n), AB(n), ref(n);
+    host_gemm(Av, M, Bv, AB, M);
+    for (size_t i = 0; i < n; ++i) ref[i] = 1.5 * AB[i] - 0.5 * C[i];
+    dgt::DriverOptions opt;
+    opt.logDir = dir;
+    opt.machine = "b200test";
+    dgt::fullOffloadSumma25Dgemm('N', 'N', M, M, M, 1.5, A, M, B, M, -0.5, C, M, p, p, c, 1, true, true, opt);
+    std::vector<double> got(C, C + n);
+    const double e = rel_fro(ref, got, M, M);
+    std::printf("full offload from page-locked memory M=%lld grid %dx%dx%d: rel Frobenius %.3e\n", M, p, p, c, e);
+    cudaFreeHost(A);
+    cudaFreeHost(B);
+    cudaFreeHost(C);
+    return e <= 1e-12 ? 0 : 1;
+}
+
 static int test_pre_distributed(const char* dir, long long M, int p, int c) {
     const uint64_t seed = 11;
     const double alpha = 1.0, beta = 0.25;
@@ -94,6 +124,7 @@ int main(int argc, char** argv) {
         int fails = 0;
         fails += test_full_offload(argv[1], 64, 2, 1, 2);
         fails += test_full_offload(argv[1], 96, 4, 2, 1);
+        fails += test_full_offload_pinned(argv[1], 64, 2, 1);
         fails += test_pre_distributed(argv[1], 96, 4, 2);
         bool threw = false;
         std::vector<double> X(64 * 64, 0.0);

@@ -2,7 +2,8 @@
 // Cannon drivers (include/dgt_drivers.hpp) make, so that their host logic -- allocation
 // sizes, copy pitches, the run loop, the result and the CSV rows -- runs and is checked on
 // a machine without a GPU (tests/test_csv_log.py links tests/cpp/driver_test.cpp against
-// this file instead of libcudart and libdgt).  "Device" memory is host memory; kernels are
+// this file instead of libcudart and libdgt).  "Device" memory is host memory, and
+// cudaMallocHost marks an allocation page-locked for the *_host entries; kernels are
 // plain loops: the Cannon pack / unpack move tile (i, j) <-> &X[lm (j M + i)] with ld M
 // (src/25DCannon.cpp:113-136, :254-271) and the multiply computes every C tile as
 // alpha sum_t A(i,t) B(t,j) + beta C(i,j), the 2.5D algorithm's result.
@@ -11,6 +12,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <set>
 #include <vector>
 
 #include "dgt.h"
@@ -33,6 +35,19 @@ cudaError_t cudaMalloc(void** p, size_t bytes) {
     return *p ? cudaSuccess : cudaErrorMemoryAllocation;
 }
 cudaError_t cudaFree(void* p) {
+    std::free(p);
+    return cudaSuccess;
+}
+// page-locked allocations, so the *_host entries can tell them from pageable memory
+static std::set<const void*> g_pinned;
+cudaError_t cudaMallocHost(void** p, size_t bytes) {
+    *p = std::malloc(bytes);
+    if (!*p) return cudaErrorMemoryAllocation;
+    g_pinned.insert(*p);
+    return cudaSuccess;
+}
+cudaError_t cudaFreeHost(void* p) {
+    g_pinned.erase(p);
     std::free(p);
     return cudaSuccess;
 }
@@ -108,6 +123,17 @@ dgt_status dgt_unpack_cannon2d(dgt_handle_t, int64_t M, int32_t p, double* C, co
             for (int64_t c = 0; c < lm; ++c)
                 for (int64_t r = 0; r < lm; ++r) C[lm * (j * M + i) + r + c * M] = lC[i * p + j][r + c * lm];
     return DGT_SUCCESS;
+}
+
+dgt_status dgt_pack_cannon2d_host(dgt_handle_t h, int64_t M, int32_t p, const double* A, const double* B,
+                                  const double* C, double* const* lA, double* const* lB, double* const* lC) {
+    if (!g_pinned.count(A) || !g_pinned.count(B) || !g_pinned.count(C)) return DGT_ERROR_INVALID_VALUE;
+    return dgt_pack_cannon2d(h, M, p, A, B, C, lA, lB, lC);
+}
+
+dgt_status dgt_unpack_cannon2d_host(dgt_handle_t h, int64_t M, int32_t p, double* C, const double* const* lC) {
+    if (!g_pinned.count(C)) return DGT_ERROR_INVALID_VALUE;
+    return dgt_unpack_cannon2d(h, M, p, C, lC);
 }
 
 dgt_status dgt_cannon25d(dgt_handle_t, int64_t M, int32_t p, int32_t c, char ta, char tb, double alpha,

@@ -32,7 +32,7 @@ def check_cannon_driver_logs(logs):
 
     full = pd.read_csv(logs / "DGEMM_execution_logs-FullOffload_GEMM-b200test-2.5DCANNON-dgt.csv", header=0)
     pre = pd.read_csv(logs / "DGEMM_execution_logs-PreDistributed_GEMM-b200test-2.5DCANNON-dgt.csv", header=0)
-    assert list(full["M"]) == [64, 64, 96] and list(full["StackSize"]) == [1, 1, 2]
+    assert list(full["M"]) == [64, 64, 96, 64] and list(full["StackSize"]) == [1, 1, 2, 1]
     assert list(pre["M"]) == [96] and list(pre["dRow"]) == [4]
     for df in (full, pre):
         assert (df["Algo"] == "2.5D CANNON dgt").all()
