@@ -1,5 +1,8 @@
 """Device-buffer helpers for the GPU tests: column-major numpy <-> device memory owned
 by torch (torch only owns the memory; every computation goes through libdgt)."""
+import ctypes
+import socket
+
 import numpy as np
 
 
@@ -61,3 +64,82 @@ class HostOps:
         c = C.numpy()[:n, :m]  # column-major m x n view of C's storage
         prod = A.numpy()[:k, :m].T @ B.numpy()[:n, :k].T if k > 0 else np.zeros((m, n))
         c[...] = (alpha * prod).T if beta == 0.0 else (alpha * prod + beta * c.T).T
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def scatter_block_cyclic(G, mb, nb, p, q):
+    """Block-cyclic locals of every rank of a p x q grid (rank r = i q + j), empty ranks
+    included (the oracle's scatter refuses grids that leave a rank empty)."""
+    M, N = G.shape
+    out = []
+    for r in range(p * q):
+        i, j = r // q, r % q
+        rows = [x for b in range(i, -(-M // mb), p) for x in range(b * mb, min(M, (b + 1) * mb))]
+        cols = [x for b in range(j, -(-N // nb), q) for x in range(b * nb, min(N, (b + 1) * nb))]
+        out.append(np.asfortranarray(G[np.ix_(rows, cols)]))
+    return out
+
+
+def gather_block_cyclic(locs, M, N, mb, nb, p, q):
+    G = np.full((M, N), np.nan)
+    for r, loc in enumerate(locs):
+        i, j = r // q, r % q
+        rows = [x for b in range(i, -(-M // mb), p) for x in range(b * mb, min(M, (b + 1) * mb))]
+        cols = [x for b in range(j, -(-N // nb), q) for x in range(b * nb, min(N, (b + 1) * nb))]
+        G[np.ix_(rows, cols)] = loc
+    return G
+
+
+def local_tensor(x):
+    import torch
+
+    rows, cols = x.shape
+    t = torch.zeros((max(cols, 1), max(rows, 1)), dtype=torch.float64)
+    if rows and cols:
+        t.copy_(torch.from_numpy(np.ascontiguousarray(np.asfortranarray(x).T)))
+    return t
+
+
+class ShmIpc:
+    """Host shared memory with DeviceIpc's interface (alloc / open / close / free / tensor)."""
+
+    def __init__(self):
+        self.segments = {}
+
+    def _addr(self, shm):
+        return np.frombuffer(shm.buf, dtype=np.uint8).ctypes.data
+
+    def alloc(self, nbytes):
+        from multiprocessing import shared_memory
+
+        shm = shared_memory.SharedMemory(create=True, size=max(int(nbytes), 8))
+        addr = self._addr(shm)
+        self.segments[addr] = shm
+        return addr, shm.name.encode().ljust(64, b"\0")
+
+    def open(self, handle):
+        from multiprocessing import shared_memory
+
+        shm = shared_memory.SharedMemory(name=handle.rstrip(b"\0").decode())
+        addr = self._addr(shm)
+        self.segments[addr] = shm
+        return addr
+
+    def close(self, ptr):
+        pass  # mappings go with the process
+
+    def free(self, ptr):
+        self.segments[ptr].unlink()
+
+    def tensor(self, ptr, shape):
+        import torch
+
+        n = int(np.prod(shape))
+        return torch.from_numpy(np.frombuffer((ctypes.c_double * n).from_address(ptr), dtype=np.float64).reshape(shape))
+
+    def synchronize(self):
+        pass

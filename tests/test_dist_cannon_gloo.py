@@ -11,14 +11,9 @@ import sys
 
 import numpy as np
 import pytest
+from devutil import free_port
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-
-
-def _free_port():
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        return s.getsockname()[1]
 
 
 def _tile(X, i, j, lm):
@@ -78,7 +73,7 @@ def test_dist_cannon_gloo(p, c, M):
     world = p * p * c
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
-    port = _free_port()
+    port = free_port()
     procs = [ctx.Process(target=_rank_main, args=(r, p, c, M, alpha, beta, port, out)) for r in range(world)]
     for pr in procs:
         pr.start()

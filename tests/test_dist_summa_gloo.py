@@ -12,6 +12,7 @@ import sys
 
 import numpy as np
 import pytest
+from devutil import free_port, gather_block_cyclic, local_tensor, scatter_block_cyclic
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -22,44 +23,6 @@ CASES = [
     (4, 1, 16, 32, 12, 40, 50, 61, -2.0, 1.0),     # process row 3 owns no rows of A or C
     (2, 2, 16, 16, 16, 48, 40, 0, 1.0, 0.25),      # K = 0: C = beta C
 ]
-
-
-def _scatter(G, mb, nb, p, q):
-    """Block-cyclic locals of every rank (rank r = i q + j), empty ranks included."""
-    M, N = G.shape
-    out = []
-    for r in range(p * q):
-        i, j = r // q, r % q
-        rows = [x for b in range(i, -(-M // mb), p) for x in range(b * mb, min(M, (b + 1) * mb))]
-        cols = [x for b in range(j, -(-N // nb), q) for x in range(b * nb, min(N, (b + 1) * nb))]
-        out.append(np.asfortranarray(G[np.ix_(rows, cols)]))
-    return out
-
-
-def _gather(locs, M, N, mb, nb, p, q):
-    G = np.full((M, N), np.nan)
-    for r, loc in enumerate(locs):
-        i, j = r // q, r % q
-        rows = [x for b in range(i, -(-M // mb), p) for x in range(b * mb, min(M, (b + 1) * mb))]
-        cols = [x for b in range(j, -(-N // nb), q) for x in range(b * nb, min(N, (b + 1) * nb))]
-        G[np.ix_(rows, cols)] = loc
-    return G
-
-
-def _free_port():
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        return s.getsockname()[1]
-
-
-def _local_tensor(x):
-    import torch
-
-    rows, cols = x.shape
-    t = torch.zeros((max(cols, 1), max(rows, 1)), dtype=torch.float64)
-    if rows and cols:
-        t.copy_(torch.from_numpy(np.ascontiguousarray(np.asfortranarray(x).T)))
-    return t
 
 
 def _rank_main(rank, world, port, out):
@@ -78,10 +41,10 @@ def _rank_main(rank, world, port, out):
     try:
         for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
             A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
-            la = _scatter(A, mb, kb, p, q)[rank]
-            lb = _scatter(B, kb, nb, p, q)[rank]
-            lc = _scatter(C, mb, nb, p, q)[rank]
-            tA, tB, tC = _local_tensor(la), _local_tensor(lb), _local_tensor(lc)
+            la = scatter_block_cyclic(A, mb, kb, p, q)[rank]
+            lb = scatter_block_cyclic(B, kb, nb, p, q)[rank]
+            lc = scatter_block_cyclic(C, mb, nb, p, q)[rank]
+            tA, tB, tC = local_tensor(la), local_tensor(lb), local_tensor(lc)
             S = DistSumma(p, q, mb, nb, kb, ops=HostOps())
             assert S.local_shapes(M, N, K) == (la.shape, lb.shape, lc.shape)
             S.multiply(M, N, K, alpha, tA, tB, beta, tC)
@@ -107,7 +70,7 @@ def test_dist_summa_four_gloo_ranks():
     world = 4
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
-    port = _free_port()
+    port = free_port()
     procs = [ctx.Process(target=_rank_main, args=(r, world, port, out)) for r in range(world)]
     for pr in procs:
         pr.start()
@@ -124,7 +87,7 @@ def test_dist_summa_four_gloo_ranks():
         assert pr.exitcode == 0
     for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
         A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
-        G = _gather([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
+        G = gather_block_cyclic([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
         ref = O.dgemm(A, B, alpha, beta, C) if K > 0 else beta * C
         assert O.rel_errors(G, ref)[1] <= 1e-13, (n_case, O.rel_errors(G, ref))
 
@@ -137,12 +100,12 @@ def test_scatter_helper_matches_oracle():
 
     for (M, N, mb, nb, p, q) in [(150, 90, 16, 20, 2, 2), (64, 77, 32, 8, 1, 4), (170, 61, 24, 12, 4, 1)]:
         G = O.uniform((M, N), M)
-        mine = _scatter(G, mb, nb, p, q)
+        mine = scatter_block_cyclic(G, mb, nb, p, q)
         for a, b in zip(mine, O.orc().pblas_scatter(G, mb, nb, p, q)):
             assert np.array_equal(a, b)
-        assert np.array_equal(_gather(mine, M, N, mb, nb, p, q), G)
+        assert np.array_equal(gather_block_cyclic(mine, M, N, mb, nb, p, q), G)
     G = O.uniform((40, 50), 1)
-    assert _scatter(G, 16, 32, 4, 1)[3].shape == (0, 50)  # a process row without rows
+    assert scatter_block_cyclic(G, 16, 32, 4, 1)[3].shape == (0, 50)  # a process row without rows
 
 
 def test_dist_summa_needs_matching_world():
@@ -191,17 +154,17 @@ def test_device_ops_argument_arithmetic():
     import oracle as O
     from dgt.dist import DgtOps, DistCannon25D, DistSumma
 
-    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{free_port()}", rank=0, world_size=1,
                             timeout=datetime.timedelta(seconds=60))
     try:
         M, N, K = 70, 50, 45
         A, B, C = O.uniform((M, K), 4), O.uniform((K, N), 5), O.uniform((M, N), 6)
-        tA, tB, tC = (_local_tensor(x) for x in (A, B, C))
+        tA, tB, tC = (local_tensor(x) for x in (A, B, C))
         DistSumma(1, 1, 16, 16, 8, ops=DgtOps(_PtrHandle())).multiply(M, N, K, 1.5, tA, tB, -0.5, tC)
         got = tC.numpy().T
         assert O.rel_errors(got, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
         S = O.uniform((40, 40), 7)
-        tS, tT, tU = _local_tensor(S), _local_tensor(S.T.copy()), _local_tensor(S)
+        tS, tT, tU = local_tensor(S), local_tensor(S.T.copy()), local_tensor(S)
         DistCannon25D(1, 1, ops=DgtOps(_PtrHandle())).multiply(40, 2.0, tS, tT, 0.5, tU)
         assert O.rel_errors(tU.numpy().T, O.dgemm(S, S.T, 2.0, 0.5, S))[1] <= 1e-13
         dst = torch.zeros_like(tS)
@@ -226,7 +189,7 @@ def _dying_rank_main(rank, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=4, timeout=datetime.timedelta(seconds=10))
     p, q, b, M, N, K = 2, 2, 16, 64, 64, 64
     A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
-    tA, tB, tC = (_local_tensor(_scatter(X, b, b, p, q)[rank]) for X in (A, B, C))
+    tA, tB, tC = (local_tensor(scatter_block_cyclic(X, b, b, p, q)[rank]) for X in (A, B, C))
     S = DistSumma(p, q, b, b, b, ops=HostOps())
     if rank == 3:
         os._exit(1)  # leaves between steps: none of its collectives is in flight
@@ -247,7 +210,7 @@ def test_dist_summa_rank_failure_ends_in_errors_not_a_hang():
 
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
-    port = _free_port()
+    port = free_port()
     procs = [ctx.Process(target=_dying_rank_main, args=(r, port, out)) for r in range(4)]
     for pr in procs:
         pr.start()

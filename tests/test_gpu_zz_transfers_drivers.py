@@ -234,7 +234,7 @@ def _peer_rank(rank, world, p, q, port, out):
         sys.path.insert(0, os.path.join(ROOT, sub))
     import oracle as O
     from dgt.dist import PeerSumma
-    from test_dist_summa_gloo import _local_tensor, _scatter
+    from devutil import local_tensor, scatter_block_cyclic
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
@@ -243,10 +243,10 @@ def _peer_rank(rank, world, p, q, port, out):
         M, N, K, mb, nb, kb = 300, 260, 170, 32, 48, 40
         A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
         S = PeerSumma(p, q, mb, nb, kb, M, N, K)
-        la, lb, lc = _scatter(A, mb, kb, p, q)[rank], _scatter(B, kb, nb, p, q)[rank], _scatter(C, mb, nb, p, q)[rank]
-        S.A_loc.copy_(_local_tensor(la).cuda())
-        S.B_loc.copy_(_local_tensor(lb).cuda())
-        tC = _local_tensor(lc).cuda()
+        la, lb, lc = scatter_block_cyclic(A, mb, kb, p, q)[rank], scatter_block_cyclic(B, kb, nb, p, q)[rank], scatter_block_cyclic(C, mb, nb, p, q)[rank]
+        S.A_loc.copy_(local_tensor(la).cuda())
+        S.B_loc.copy_(local_tensor(lb).cuda())
+        tC = local_tensor(lc).cuda()
         S.multiply(1.5, -0.5, tC)
         S.h.check_device()
         rows, cols = lc.shape
@@ -265,7 +265,7 @@ def _run_peer(world, p, q):
     import socket
 
     import torch.multiprocessing as mp
-    from test_dist_summa_gloo import _gather
+    from devutil import gather_block_cyclic
 
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
@@ -288,7 +288,7 @@ def _run_peer(world, p, q):
         assert pr.exitcode == 0
     M, N, K, mb, nb, kb = 300, 260, 170, 32, 48, 40
     A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
-    G = _gather([got[r] for r in range(world)], M, N, mb, nb, p, q)
+    G = gather_block_cyclic([got[r] for r in range(world)], M, N, mb, nb, p, q)
     assert O.rel_errors(G, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
 
 

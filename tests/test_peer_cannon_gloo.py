@@ -14,6 +14,7 @@ import sys
 
 import numpy as np
 import pytest
+from devutil import free_port
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -46,12 +47,6 @@ class CannonHandle:
             c += self._mat(part, elems, 1, elems)
 
 
-def _free_port():
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        return s.getsockname()[1]
-
-
 def _rank_main(rank, p, c, M, port, out):
     import datetime
 
@@ -62,7 +57,7 @@ def _rank_main(rank, p, c, M, port, out):
         sys.path.insert(0, os.path.join(ROOT, sub))
     import oracle as O
     from dgt.dist import PeerCannon25D
-    from test_peer_summa_gloo import ShmIpc
+    from devutil import ShmIpc
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=p * p * c, timeout=datetime.timedelta(seconds=60))
@@ -103,7 +98,7 @@ def test_peer_cannon_gloo(p, c, M):
     world = p * p * c
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
-    port = _free_port()
+    port = free_port()
     procs = [ctx.Process(target=_rank_main, args=(r, p, c, M, port, out)) for r in range(world)]
     for pr in procs:
         pr.start()

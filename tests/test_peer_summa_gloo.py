@@ -12,6 +12,7 @@ import sys
 
 import numpy as np
 import pytest
+from devutil import ShmIpc, free_port
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CASES = [  # (p, q, mb, nb, kb, M, N, K, alpha, beta)
@@ -20,47 +21,6 @@ CASES = [  # (p, q, mb, nb, kb, M, N, K, alpha, beta)
     (4, 1, 16, 32, 12, 40, 50, 61, -2.0, 1.0),  # process row 3 owns no rows of A or C
     (2, 2, 16, 16, 16, 48, 40, 0, 1.0, 0.25),   # K = 0: C = beta C
 ]
-
-
-class ShmIpc:
-    """Host shared memory with DeviceIpc's interface (alloc / open / close / free / tensor)."""
-
-    def __init__(self):
-        self.segments = {}
-
-    def _addr(self, shm):
-        return np.frombuffer(shm.buf, dtype=np.uint8).ctypes.data
-
-    def alloc(self, nbytes):
-        from multiprocessing import shared_memory
-
-        shm = shared_memory.SharedMemory(create=True, size=max(int(nbytes), 8))
-        addr = self._addr(shm)
-        self.segments[addr] = shm
-        return addr, shm.name.encode().ljust(64, b"\0")
-
-    def open(self, handle):
-        from multiprocessing import shared_memory
-
-        shm = shared_memory.SharedMemory(name=handle.rstrip(b"\0").decode())
-        addr = self._addr(shm)
-        self.segments[addr] = shm
-        return addr
-
-    def close(self, ptr):
-        pass  # mappings go with the process
-
-    def free(self, ptr):
-        self.segments[ptr].unlink()
-
-    def tensor(self, ptr, shape):
-        import torch
-
-        n = int(np.prod(shape))
-        return torch.from_numpy(np.frombuffer((ctypes.c_double * n).from_address(ptr), dtype=np.float64).reshape(shape))
-
-    def synchronize(self):
-        pass
 
 
 class ScheduleHandle:
@@ -88,12 +48,6 @@ class ScheduleHandle:
             first = False
 
 
-def _free_port():
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        return s.getsockname()[1]
-
-
 def _rank_main(rank, world, port, out):
     import datetime
 
@@ -104,7 +58,7 @@ def _rank_main(rank, world, port, out):
         sys.path.insert(0, os.path.join(ROOT, sub))
     import oracle as O
     from dgt.dist import PeerSumma
-    from test_dist_summa_gloo import _local_tensor, _scatter
+    from devutil import local_tensor, scatter_block_cyclic
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
@@ -112,13 +66,13 @@ def _rank_main(rank, world, port, out):
         for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
             A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
             S = PeerSumma(p, q, mb, nb, kb, M, N, K, ipc=ShmIpc(), handle=ScheduleHandle())
-            la, lb, lc = _scatter(A, mb, kb, p, q)[rank], _scatter(B, kb, nb, p, q)[rank], _scatter(C, mb, nb, p, q)[rank]
-            S.A_loc.copy_(_local_tensor(la))
-            S.B_loc.copy_(_local_tensor(lb))
-            tC = _local_tensor(lc)
+            la, lb, lc = scatter_block_cyclic(A, mb, kb, p, q)[rank], scatter_block_cyclic(B, kb, nb, p, q)[rank], scatter_block_cyclic(C, mb, nb, p, q)[rank]
+            S.A_loc.copy_(local_tensor(la))
+            S.B_loc.copy_(local_tensor(lb))
+            tC = local_tensor(lc)
             S.multiply(alpha, beta, tC)
             # the owners' A and B are untouched by the peers' reads
-            assert torch.equal(S.A_loc, _local_tensor(la)) and torch.equal(S.B_loc, _local_tensor(lb))
+            assert torch.equal(S.A_loc, local_tensor(la)) and torch.equal(S.B_loc, local_tensor(lb))
             rows, cols = lc.shape
             out.put((n_case, rank, tC.numpy()[:cols, :rows].T.copy()))
             S.close()
@@ -138,12 +92,12 @@ def test_peer_summa_four_gloo_ranks():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle as O
-    from test_dist_summa_gloo import _gather
+    from devutil import gather_block_cyclic
 
     world = 4
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
-    port = _free_port()
+    port = free_port()
     procs = [ctx.Process(target=_rank_main, args=(r, world, port, out)) for r in range(world)]
     for pr in procs:
         pr.start()
@@ -160,7 +114,7 @@ def test_peer_summa_four_gloo_ranks():
         assert pr.exitcode == 0
     for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
         A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
-        G = _gather([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
+        G = gather_block_cyclic([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
         ref = O.dgemm(A, B, alpha, beta, C) if K > 0 else beta * C
         assert O.rel_errors(G, ref)[1] <= 1e-13, n_case
 
@@ -211,7 +165,7 @@ def test_peer_summa_setup_failure_releases_buffers():
 
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
-    port = _free_port()
+    port = free_port()
     procs = [ctx.Process(target=_failing_rank, args=(r, port, out)) for r in range(2)]
     for pr in procs:
         pr.start()
