@@ -1,5 +1,7 @@
-"""Device-buffer helpers for the GPU tests: column-major numpy <-> device memory owned
-by torch (torch only owns the memory; every computation goes through libdgt)."""
+"""Helpers shared by the tests: column-major numpy <-> device memory owned by torch (torch
+only owns the memory; every computation goes through libdgt), the CSV-log checks of the
+C++ drivers, and the host doubles of the multi-process tests (rank-local operations,
+process-shared memory standing in for CUDA IPC, block-cyclic scatter / gather, free ports)."""
 import ctypes
 import socket
 
