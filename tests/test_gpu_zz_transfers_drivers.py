@@ -537,3 +537,39 @@ def test_cannon2d_from_host_equals_device_path(h, M, p):
     with pytest.raises(dgt.DgtError) as e:
         h.pack_cannon2d_host(M, p, pageable.ctypes.data, pA, pC, ps(oA), ps(oB), ps(oC))
     assert e.value.status == dgt.INVALID_VALUE
+
+
+def test_summa_guard_bands(h):
+    """dgt_summa on a 2 x 3 grid with every rank's A, B and C local between canaries and
+    padded leading dimensions: only the C blocks' valid rows change, and the gathered result
+    is the host FP64 GEMM."""
+    import torch
+
+    from devutil import gather_block_cyclic, scatter_block_cyclic
+
+    p, q, b, M, N, K = 2, 3, 32, 257, 131, 199
+    A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
+    la, lb, lc = scatter_block_cyclic(A, b, b, p, q), scatter_block_cyclic(B, b, b, p, q), scatter_block_cyclic(C, b, b, p, q)
+    gA = [_guarded(x, max(x.shape[0], 1) + 2) for x in la]
+    gB = [_guarded(x, max(x.shape[0], 1) + 1) for x in lb]
+    gC = [_guarded(x, max(x.shape[0], 1) + 3) for x in lc]
+    ld = lambda xs, g: [max(x.shape[0], 1) + g for x in xs]
+    h.summa(p, q, b, b, b, M, N, K, 1.5, [g[1] for g in gA], ld(la, 2), [g[1] for g in gB], ld(lb, 1), -0.5,
+            [g[1] for g in gC], ld(lc, 3))
+    torch.cuda.synchronize()
+    h.check_device()
+    for (t, _, img) in gA + gB:
+        assert np.array_equal(t.cpu().numpy().view(np.uint64), img.view(np.uint64))
+    res = []
+    for x, (t, _, img) in zip(lc, gC):
+        rows, cols = x.shape
+        ldc = max(rows, 1) + 3
+        got = t.cpu().numpy()
+        inside = np.zeros(got.shape, dtype=bool)
+        for j in range(cols):
+            inside[GUARD + j * ldc:GUARD + j * ldc + rows] = True
+        assert np.array_equal(got[~inside].view(np.uint64), img[~inside].view(np.uint64))
+        res.append(np.stack([got[GUARD + j * ldc:GUARD + j * ldc + rows] for j in range(cols)], axis=1)
+                   if rows and cols else np.zeros((rows, cols)))
+    G = gather_block_cyclic(res, M, N, b, b, p, q)
+    assert O.rel_errors(G, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
