@@ -243,7 +243,7 @@ def _peer_rank(rank, world, p, q, port, out):
         M, N, K, mb, nb, kb = 300, 260, 170, 32, 48, 40
         A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
         S = PeerSumma(p, q, mb, nb, kb, M, N, K)
-        la, lb, lc = scatter_block_cyclic(A, mb, kb, p, q)[rank], scatter_block_cyclic(B, kb, nb, p, q)[rank], scatter_block_cyclic(C, mb, nb, p, q)[rank]
+        la, lb, lc = (scatter_block_cyclic(X, r, c, p, q)[rank] for X, r, c in ((A, mb, kb), (B, kb, nb), (C, mb, nb)))
         S.A_loc.copy_(local_tensor(la).cuda())
         S.B_loc.copy_(local_tensor(lb).cuda())
         tC = local_tensor(lc).cuda()
@@ -549,7 +549,7 @@ def test_summa_guard_bands(h):
 
     p, q, b, M, N, K = 2, 3, 32, 257, 131, 199
     A, B, C = O.uniform((M, K), 1), O.uniform((K, N), 2), O.uniform((M, N), 3)
-    la, lb, lc = scatter_block_cyclic(A, b, b, p, q), scatter_block_cyclic(B, b, b, p, q), scatter_block_cyclic(C, b, b, p, q)
+    la, lb, lc = (scatter_block_cyclic(X, b, b, p, q) for X in (A, B, C))
     gA = [_guarded(x, max(x.shape[0], 1) + 2) for x in la]
     gB = [_guarded(x, max(x.shape[0], 1) + 1) for x in lb]
     gC = [_guarded(x, max(x.shape[0], 1) + 3) for x in lc]

@@ -64,9 +64,9 @@ def _rank_main(rank, world, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
-            A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
+            A, B, C = (O.uniform(shape, 10 * n_case + s) for s, shape in ((1, (M, K)), (2, (K, N)), (3, (M, N))))
             S = PeerSumma(p, q, mb, nb, kb, M, N, K, ipc=ShmIpc(), handle=ScheduleHandle())
-            la, lb, lc = scatter_block_cyclic(A, mb, kb, p, q)[rank], scatter_block_cyclic(B, kb, nb, p, q)[rank], scatter_block_cyclic(C, mb, nb, p, q)[rank]
+            la, lb, lc = (scatter_block_cyclic(X, r, c, p, q)[rank] for X, r, c in ((A, mb, kb), (B, kb, nb), (C, mb, nb)))
             S.A_loc.copy_(local_tensor(la))
             S.B_loc.copy_(local_tensor(lb))
             tC = local_tensor(lc)
@@ -113,7 +113,7 @@ def test_peer_summa_four_gloo_ranks():
         pr.join(timeout=60)
         assert pr.exitcode == 0
     for n_case, (p, q, mb, nb, kb, M, N, K, alpha, beta) in enumerate(CASES):
-        A, B, C = O.uniform((M, K), 10 * n_case + 1), O.uniform((K, N), 10 * n_case + 2), O.uniform((M, N), 10 * n_case + 3)
+        A, B, C = (O.uniform(shape, 10 * n_case + s) for s, shape in ((1, (M, K)), (2, (K, N)), (3, (M, N))))
         G = gather_block_cyclic([results[(n_case, r)] for r in range(world)], M, N, mb, nb, p, q)
         ref = O.dgemm(A, B, alpha, beta, C) if K > 0 else beta * C
         assert O.rel_errors(G, ref)[1] <= 1e-13, n_case
