@@ -58,3 +58,15 @@ def test_status_strings():
     lib = dgt.load()
     assert lib.dgt_status_string(0) == b"DGT_SUCCESS"
     assert lib.dgt_status_string(4) == b"DGT_ERROR_TIMEOUT"
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/dgt.h is a C header: a C99 translation unit that includes it compiles with
+    -pedantic -Werror (no C++ in the boundary's types or signatures)."""
+    import subprocess
+
+    src = tmp_path / "use_dgt.c"
+    src.write_text('#include "dgt.h"\nint main(void) { dgt_ipc_handle h; dgt_grid_layout g; (void)h; (void)g; '
+                   'return (int)DGT_SUCCESS; }\n')
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    "-c", str(src), "-o", str(tmp_path / "use_dgt.o")], check=True)
