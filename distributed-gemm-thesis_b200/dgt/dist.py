@@ -27,6 +27,7 @@ ops to run the same schedule as gloo ranks on the CPU.
 from __future__ import annotations
 
 import math
+import os
 
 import dgt
 
@@ -514,3 +515,90 @@ class PeerCannon25D:
         for ptr, _ in self._own:
             self.ipc.free(ptr)
         self._own = []
+
+
+def pre_distributed_cannon25_nccl(p, c, M, runs, alpha=1.0, beta=0.0, logging=True, gather_results=False,
+                                  log_dir=".", machine=None, fused=False, seed=0, ops=None, ipc=None, handle=None,
+                                  sync=None):
+    """The reference's NCCL benchmark driver (preDistributedCannon25NCCL,
+    src/25DCannonNCCL.cpp:322-399) over the multi-process 2.5D Cannon: one process per GPU,
+    p*p*c ranks.  DecompositionTime is the decomposer's construction, as in the reference
+    (:343-345); the stack-0 tiles are then filled with U[-1, 1) values (global A, B, C from
+    numpy's PCG64(seed), tile (i, j) of each); every run is one multiply, timed between two
+    barriers (the slowest rank's time); with gather_results the stack-0 C tiles are
+    collected on rank 0 (reorderMatrix).  Rank 0 appends one row per run in the reference's
+    NCCL schema (Algo "2.5D CANNON dgt NCCL", or "2.5D CANNON dgt peer" for the fused form;
+    TotalGPUs = the number of ranks, one GPU each).  Returns C on rank 0 when gathering,
+    else None.  `fused` selects PeerCannon25D (kernels read the owners' tiles) instead of
+    DistCannon25D (NCCL broadcasts and shifts); ops / ipc / handle / sync stand in for the
+    device in tests."""
+    import time
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from . import csvlog
+
+    rank, world = dist.get_rank(), dist.get_world_size()
+    if sync is None:
+        sync = torch.cuda.synchronize
+    log = None
+    if logging and rank == 0:
+        name = csvlog.cannon_nccl_log_name(machine or csvlog.machine_name())
+        log = csvlog.create_log_csv(os.path.join(log_dir, name), csvlog.CANNON_NCCL_HEADER)
+    try:
+        t0 = time.perf_counter()
+        S = (PeerCannon25D(p, c, M, ipc=ipc, handle=handle) if fused else DistCannon25D(p, c, ops=ops))
+        decomp = time.perf_counter() - t0
+        lm = M // p
+        k, i, j = rank // (p * p), (rank // p) % p, rank % p
+        device = "cpu" if (ops is not None or ipc is not None) else "cuda"
+        rng = np.random.Generator(np.random.PCG64(seed))
+        G = [rng.uniform(-1.0, 1.0, (M, M)) for _ in range(3)]
+        tile = lambda X: torch.from_numpy(np.ascontiguousarray(X[i * lm:(i + 1) * lm, j * lm:(j + 1) * lm].T)).to(device)
+        if fused:
+            C_tile = None
+            if k == 0:
+                S.A_tile.copy_(tile(G[0]))
+                S.B_tile.copy_(tile(G[1]))
+                C_tile = tile(G[2])
+            A_tile = B_tile = None
+        else:
+            A_tile, B_tile = (tile(G[0]), tile(G[1])) if k == 0 else (torch.empty((lm, lm), dtype=torch.float64,
+                                                                                   device=device),) * 2
+            C_tile = tile(G[2]) if k == 0 else torch.empty((lm, lm), dtype=torch.float64, device=device)
+        result = None
+        for _ in range(runs):
+            sync()
+            dist.barrier()
+            t0 = time.perf_counter()
+            if fused:
+                S.multiply(alpha, beta, C_tile)
+            else:
+                S.multiply(M, alpha, A_tile, B_tile, beta, C_tile)
+            sync()
+            dist.barrier()
+            execution = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            if gather_results:
+                mine = C_tile.cpu().numpy().T.copy() if k == 0 else None
+                tiles = [None] * world if rank == 0 else None
+                dist.gather_object(mine, tiles, dst=0)
+                if rank == 0:
+                    result = np.zeros((M, M))
+                    for r in range(p * p):
+                        ri, rj = r // p, r % p
+                        result[ri * lm:(ri + 1) * lm, rj * lm:(rj + 1) * lm] = tiles[r]
+            gather = time.perf_counter() - t0
+            if log is not None:
+                algo = "2.5D CANNON dgt peer" if fused else "2.5D CANNON dgt NCCL"
+                csvlog.write_line_to_file(log, csvlog.cannon_nccl_row(
+                    algo, M, M, M, csvlog.slurm_num_nodes(), world, p, p, c, decomp, execution, gather,
+                    csvlog.calculate_gflops(M, M, M, execution)))
+        if fused:
+            S.close()
+        return result
+    finally:
+        if log is not None:
+            log.close()

@@ -145,3 +145,31 @@ class ShmIpc:
 
     def synchronize(self):
         pass
+
+
+class CannonHandle:
+    """dgt.Handle.cannon25d_rank and reduce_tiles executed on host addresses."""
+
+    @staticmethod
+    def _mat(addr, rows, cols, ld):
+        n = ld * (cols - 1) + rows
+        buf = np.frombuffer((ctypes.c_double * n).from_address(addr), dtype=np.float64)
+        return np.lib.stride_tricks.as_strided(buf, shape=(rows, cols), strides=(8, 8 * ld))
+
+    def cannon25d_rank(self, M, p, c, rank, alpha, A_tiles, B_tiles, beta, C_tile, ta="N", tb="N", mode=None,
+                       slices=7):
+        import dgt
+
+        lm = M // p
+        k, i, j = rank // (p * p), (rank // p) % p, rank % p
+        order, _ = dgt.cannon_schedule(p, c, i, j, k)
+        acc = np.zeros((lm, lm))
+        for t in order:
+            acc += self._mat(A_tiles[i * p + t], lm, lm, lm) @ self._mat(B_tiles[t * p + j], lm, lm, lm)
+        C = self._mat(C_tile, lm, lm, lm)
+        C[...] = alpha * acc + (beta * C if k == 0 and beta != 0.0 else 0.0)
+
+    def reduce_tiles(self, C, parts, elems):
+        c = self._mat(C, elems, 1, elems)
+        for part in parts:
+            c += self._mat(part, elems, 1, elems)

@@ -95,3 +95,88 @@ def test_dist_cannon_gloo(p, c, M):
         G[i * lm:(i + 1) * lm, j * lm:(j + 1) * lm] = t
     A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), O.uniform((M, M), 3)
     assert O.rel_errors(G, O.dgemm(A, B, alpha, beta, C))[1] <= 1e-13
+
+
+def _driver_rank(rank, p, c, fused, log_dir, port, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    for sub in ("", "oracle", "distributed-gemm-thesis_b200", "tests"):
+        sys.path.insert(0, os.path.join(ROOT, sub))
+    from devutil import CannonHandle, HostOps, ShmIpc
+    from dgt.dist import pre_distributed_cannon25_nccl
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=p * p * c, timeout=datetime.timedelta(seconds=60))
+    try:
+        kw = dict(ipc=ShmIpc(), handle=CannonHandle()) if fused else dict(ops=HostOps())
+        C = pre_distributed_cannon25_nccl(p, c, 40, 2, alpha=1.5, beta=-0.5, gather_results=True, log_dir=log_dir,
+                                          machine="b200test", fused=fused, seed=5, sync=lambda: None, **kw)
+        if rank == 0:
+            out.put((rank, C))
+        dist.barrier()
+    except Exception:
+        import traceback
+
+        out.put((-1, traceback.format_exc()))
+        raise
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("p,c,fused", [(2, 1, False), (2, 2, True)])
+def test_nccl_driver_log_and_result(p, c, fused, tmp_path):
+    """pre_distributed_cannon25_nccl (the reference's preDistributedCannon25NCCL) on gloo
+    ranks: rank 0 gathers C after two runs (C <- alpha A B + beta C each run) and appends
+    one row per run in the reference's NCCL schema."""
+    import torch.multiprocessing as mp
+
+    pd = pytest.importorskip("pandas")
+    sys.path.insert(0, os.path.join(ROOT, "distributed-gemm-thesis_b200"))
+    from dgt import csvlog
+
+    world = p * p * c
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_driver_rank, args=(r, p, c, fused, str(tmp_path), port, out)) for r in range(world)]
+    for pr in procs:
+        pr.start()
+    rank, C = out.get(timeout=180)
+    for pr in procs:
+        pr.join(timeout=60)
+    assert rank == 0, C
+    assert all(pr.exitcode == 0 for pr in procs)
+    rng = np.random.Generator(np.random.PCG64(5))
+    A, B, C0 = (rng.uniform(-1.0, 1.0, (40, 40)) for _ in range(3))
+    AB = A @ B
+    want = 1.5 * AB + -0.5 * (1.5 * AB + -0.5 * C0)
+    assert np.abs(C - want).max() <= 1e-12
+    path = tmp_path / csvlog.cannon_nccl_log_name("b200test")
+    assert path.name == "DGEMM_execution_logs-PreDistributed_GEMM-b200test-2.5DCANNON-dgt-NCCL.csv"
+    df = pd.read_csv(path, header=0)
+    assert list(df.columns) == csvlog.CANNON_NCCL_HEADER.split(",")
+    assert len(df) == 2 and (df["TotalGPUs"] == world).all() and (df["StackSize"] == c).all()
+    assert (df["Algo"] == ("2.5D CANNON dgt peer" if fused else "2.5D CANNON dgt NCCL")).all()
+
+
+def test_csvlog_rules(tmp_path):
+    """The Python log helpers keep the reference's rules: header once, a foreign first line
+    gets the header appended, %lf-style rows."""
+    sys.path.insert(0, os.path.join(ROOT, "distributed-gemm-thesis_b200"))
+    from dgt import csvlog
+
+    row = csvlog.cannon_nccl_row("2.5D CANNON dgt NCCL", 8192, 8192, 8192, 1, 32, 4, 4, 2, 0.5, 0.03125, 0.125,
+                                 csvlog.calculate_gflops(8192, 8192, 8192, 0.03125))
+    assert row == "2.5D CANNON dgt NCCL,8192,8192,8192,1,32,4,4,2,0.500000,0.031250,0.125000,35184.372089,devices\n"
+    path = tmp_path / "log.csv"
+    for _ in range(2):
+        f = csvlog.create_log_csv(str(path), csvlog.CANNON_NCCL_HEADER)
+        csvlog.write_line_to_file(f, row)
+        f.close()
+    assert path.read_text() == csvlog.CANNON_NCCL_HEADER + "\n" + row + row
+    other = tmp_path / "other.csv"
+    other.write_text("Algo,M\nx,1\n")
+    csvlog.create_log_csv(str(other), csvlog.CANNON_NCCL_HEADER).close()
+    assert other.read_text() == "Algo,M\nx,1\n" + csvlog.CANNON_NCCL_HEADER + "\n"

@@ -7,44 +7,15 @@ ranks.  Grids 2x2x1, 2x2x2 and 3x3x1 (where the reference's rotations skip k-blo
 shift-by-one order is used); the partial buffers of stacks above 0 start as NaN, so any
 read of an unwritten partial would show.  Stack 0's tiles must equal the host FP64 GEMM
 within 1e-13 (relative Frobenius)."""
-import ctypes
 import os
 import socket
 import sys
 
 import numpy as np
 import pytest
-from devutil import free_port
+from devutil import CannonHandle, free_port
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-
-
-class CannonHandle:
-    """dgt.Handle.cannon25d_rank and reduce_tiles executed on host addresses."""
-
-    @staticmethod
-    def _mat(addr, rows, cols, ld):
-        n = ld * (cols - 1) + rows
-        buf = np.frombuffer((ctypes.c_double * n).from_address(addr), dtype=np.float64)
-        return np.lib.stride_tricks.as_strided(buf, shape=(rows, cols), strides=(8, 8 * ld))
-
-    def cannon25d_rank(self, M, p, c, rank, alpha, A_tiles, B_tiles, beta, C_tile, ta="N", tb="N", mode=None,
-                       slices=7):
-        import dgt
-
-        lm = M // p
-        k, i, j = rank // (p * p), (rank // p) % p, rank % p
-        order, _ = dgt.cannon_schedule(p, c, i, j, k)
-        acc = np.zeros((lm, lm))
-        for t in order:
-            acc += self._mat(A_tiles[i * p + t], lm, lm, lm) @ self._mat(B_tiles[t * p + j], lm, lm, lm)
-        C = self._mat(C_tile, lm, lm, lm)
-        C[...] = alpha * acc + (beta * C if k == 0 and beta != 0.0 else 0.0)
-
-    def reduce_tiles(self, C, parts, elems):
-        c = self._mat(C, elems, 1, elems)
-        for part in parts:
-            c += self._mat(part, elems, 1, elems)
 
 
 def _rank_main(rank, p, c, M, port, out):
