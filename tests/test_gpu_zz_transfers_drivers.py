@@ -573,3 +573,33 @@ def test_summa_guard_bands(h):
                    if rows and cols else np.zeros((rows, cols)))
     G = gather_block_cyclic(res, M, N, b, b, p, q)
     assert O.rel_errors(G, O.dgemm(A, B, 1.5, -0.5, C))[1] <= 1e-13
+
+
+def test_nccl_driver_one_rank_on_gpu(tmp_path):
+    """pre_distributed_cannon25_nccl on a 1 x 1 x 1 grid (a one-rank gloo group, no collective
+    runs): the multiply through DgtOps on the GPU, two runs, the gathered C and the log."""
+    import datetime
+    import socket
+
+    import pandas as pd
+    import torch.distributed as dist
+    from dgt import csvlog
+    from dgt.dist import pre_distributed_cannon25_nccl
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        C = pre_distributed_cannon25_nccl(1, 1, 256, 2, alpha=1.5, beta=-0.5, gather_results=True,
+                                          log_dir=str(tmp_path), machine="b200test", seed=5)
+    finally:
+        dist.destroy_process_group()
+    rng = np.random.Generator(np.random.PCG64(5))
+    A, B, C0 = (rng.uniform(-1.0, 1.0, (256, 256)) for _ in range(3))
+    AB = A @ B
+    want = 1.5 * AB - 0.5 * (1.5 * AB - 0.5 * C0)
+    assert O.rel_errors(C, want)[1] <= 1e-13
+    df = pd.read_csv(tmp_path / csvlog.cannon_nccl_log_name("b200test"), header=0)
+    assert len(df) == 2 and (df["GFlops"] > 0).all()
