@@ -70,3 +70,31 @@ def test_header_is_plain_c(tmp_path):
                    'return (int)DGT_SUCCESS; }\n')
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
                     "-c", str(src), "-o", str(tmp_path / "use_dgt.o")], check=True)
+
+
+def test_new_entries_report_bad_arguments_without_a_device():
+    """The boundary returns a status and never aborts: every handle entry given a null handle
+    answers DGT_ERROR_NOT_INITIALIZED, and the IPC entries refuse null or empty arguments
+    with DGT_ERROR_INVALID_VALUE -- all before any CUDA call, so this runs without a GPU."""
+    import ctypes
+
+    lib = dgt.load()
+    z = ctypes.c_void_p(0)
+    NI = dgt.NOT_INITIALIZED
+    assert lib.dgt_copy_block_f32(None, 4, 4, z, z, 4, 4, 1) == NI
+    assert lib.dgt_pack_block_cyclic_host(None, 4, 4, 2, 2, 1, 1, z, 4, z, z) == NI
+    assert lib.dgt_unpack_block_cyclic_host(None, 4, 4, 2, 2, 1, 1, z, 4, z, z) == NI
+    assert lib.dgt_pack_cannon2d_host(None, 4, 2, z, z, z, z, z, z) == NI
+    assert lib.dgt_unpack_cannon2d_host(None, 4, 2, z, z) == NI
+    assert lib.dgt_pack_block2d_host(None, 4, 4, 4, 2, 1, z, z, z, z, z, z) == NI
+    assert lib.dgt_unpack_block2d_host(None, 4, 4, 2, 1, z, z) == NI
+    L = dgt.GridLayout(1, 1, 1, 16, 16, 16)
+    assert lib.dgt_summa_rank(None, ctypes.byref(L), 0, 4, 4, 4, 1.0, z, z, z, z, 0.0, z, 4, 0, 7) == NI
+    assert lib.dgt_cannon25d_rank(None, 4, 1, 1, 0, b"N", b"N", 1.0, z, z, 0.0, z, 0, 7) == NI
+    assert lib.dgt_reduce_tiles(None, z, z, 1, 4) == NI
+    ptr, h = ctypes.c_void_p(), ctypes.create_string_buffer(64)
+    assert lib.dgt_ipc_alloc(0, ctypes.byref(ptr), h) == dgt.INVALID_VALUE
+    assert lib.dgt_ipc_alloc(64, None, h) == dgt.INVALID_VALUE
+    assert lib.dgt_ipc_open(None, ctypes.byref(ptr)) == dgt.INVALID_VALUE
+    assert lib.dgt_ipc_close(None) == dgt.INVALID_VALUE
+    assert lib.dgt_ipc_free(None) == dgt.INVALID_VALUE
