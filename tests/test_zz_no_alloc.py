@@ -4,7 +4,8 @@ memory, in allocation-free real-time loops).  Its scratch is
 a fixed 64 MiB device array inside the library.  Checked through the C ABI against the
 handle-based entry point (dgt_dgemm_ex, same slice count) on two calls in a row, so the
 second call runs on scratch the first one left behind; the tolerance is the one the Ozaki
-tests use (relative Frobenius <= 1e-13).  Collected last on purpose."""
+tests use (relative Frobenius <= 1e-13).  Collected after the rest of the validated GPU
+suite, before the tests of the newest entries."""
 import ctypes
 
 import numpy as np
