@@ -11,6 +11,8 @@
 // is the schedule the reference intends.
 #include "mpi.h"
 
+#include "host_pool.h"
+
 #include <algorithm>
 #include <array>
 #include <atomic>
@@ -50,7 +52,7 @@ namespace {
 
 struct Message {
     int context, src, dst, tag, epoch;
-    std::vector<unsigned char> bytes;
+    PoolBytes bytes;  // packed payload (pool memory: no zero fill, no fresh pages per message)
 };
 
 struct TypeInfo {
@@ -106,10 +108,15 @@ TypeInfo type_info(MPI_Datatype t) {
 // extent in elements of one instance of the type
 long long type_extent(const TypeInfo& ti) { return (long long)(ti.count - 1) * ti.stride + ti.blocklen; }
 
-std::vector<unsigned char> pack(const void* buf, int count, MPI_Datatype type) {
+PoolBytes pack(const void* buf, int count, MPI_Datatype type) {
     TypeInfo ti = type_info(type);
-    std::vector<unsigned char> out((size_t)count * ti.count * ti.blocklen * ti.elem);
+    PoolBytes out((size_t)count * ti.count * ti.blocklen * ti.elem);
+    if (!out.data()) throw FakeAbort("out of host memory for a message");
     const unsigned char* b = static_cast<const unsigned char*>(buf);
+    if (ti.count == 1 || ti.stride == ti.blocklen) {  // contiguous: one copy
+        host_copy(out.data(), b, out.size());
+        return out;
+    }
     size_t o = 0;
     for (int c = 0; c < count; ++c) {
         const unsigned char* base = b + (size_t)c * type_extent(ti) * ti.elem;
@@ -122,11 +129,15 @@ std::vector<unsigned char> pack(const void* buf, int count, MPI_Datatype type) {
     return out;
 }
 
-void unpack(const std::vector<unsigned char>& in, void* buf, int count, MPI_Datatype type) {
+void unpack(const PoolBytes& in, void* buf, int count, MPI_Datatype type) {
     TypeInfo ti = type_info(type);
     size_t need = (size_t)count * ti.count * ti.blocklen * ti.elem;
     if (in.size() != need) throw FakeAbort("message size mismatch");
     unsigned char* b = static_cast<unsigned char*>(buf);
+    if (ti.count == 1 || ti.stride == ti.blocklen) {  // contiguous: one copy
+        host_copy(b, in.data(), need);
+        return;
+    }
     size_t o = 0;
     for (int c = 0; c < count; ++c) {
         unsigned char* base = b + (size_t)c * type_extent(ti) * ti.elem;
@@ -396,8 +407,9 @@ int MPI_Reduce(const void* sendbuf, void* recvbuf, int count, MPI_Datatype type,
         return MPI_SUCCESS;
     }
     size_t es = predefined_size(type);
-    if (sendbuf != MPI_IN_PLACE) std::memcpy(recvbuf, sendbuf, (size_t)count * es);
-    std::vector<unsigned char> tmp((size_t)count * es);
+    if (sendbuf != MPI_IN_PLACE) host_copy(recvbuf, sendbuf, (size_t)count * es);
+    PoolBytes tmp((size_t)count * es);
+    if (!tmp.data()) return MPI_ERR_OTHER;
     for (int r = 0; r < (int)comm->members.size(); ++r) {
         if (r == root) continue;
         recv_blocking(tmp.data(), count, type, r, TAG_REDUCE, comm);
