@@ -2,13 +2,14 @@
 vs native FP64 DMMA, at equal error against the host FP64 oracle.
 
 Workload (the FP64-emulation configuration): C = alpha*A*B + beta*C with
-M = N = K = 16384, column-major, entries (U[0,1) - 0.5) * exp(phi * N(0,1)), phi = 0.5
-(phi = 4.0 is measured for error only: the kernels are data-independent), seeded
-synthetic data.  One step = one dgt_dgemm call through the C ABI.  Two emulation schemes
-compete: CRT over INT8 residues (count = moduli) and INT8 digit slices (count = slices);
-each takes the smallest count whose max- and Frobenius-relative errors vs the oracle are
-<= the native DMMA kernel's ("equal error"), and the faster one is the headline (the
-other is reported beside it).  Inputs (2 GiB each) are larger than L2, so no flush.
+M = N = K = 16384, column-major, entries (U[0,1) - 0.5) * exp(phi * N(0,1)), phi = 0.5 for
+the headline value and phi = 4.0 timed beside it ("phi4"), seeded synthetic data.  One
+step = one dgt_dgemm call through the C ABI.  Two emulation schemes compete: CRT over INT8
+residues (count = moduli) and INT8 digit slices (count = slices); each takes the smallest
+count whose max- and Frobenius-relative errors against the exact product (sampled rows in
+double-double) are <= the native DMMA kernel's ("equal error"), and the faster one is the
+headline (the other is reported beside it).  Inputs (2 GiB each) are larger than L2, so no
+flush.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -34,6 +35,7 @@ SIZE = 16384
 PHI = 0.5
 ALPHA, BETA = 1.0, 0.0
 SEED = 20261203
+ROWS = 32  # sampled rows of C checked against the exact product (all N columns of each)
 
 
 def parse():
@@ -190,18 +192,18 @@ def reference_arm(args):
     M = 2048
     A, B, C = O.uniform((M, M), 1), O.uniform((M, M), 2), np.zeros((M, M), order="F")
     t0 = time.perf_counter()
-    r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA)
+    r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA, in_place=True)
     dt = time.perf_counter() - t0
     rate = 2 * M ** 3 / max(dt, 1e-6)
     M = int(min(args.size, max(2048, (3.0 * rate / 2) ** (1 / 3))) // 256 * 256)
     A, B = O.ozaki_matrix((M, M), SEED, PHI), O.ozaki_matrix((M, M), SEED + 1, PHI)
     C = np.zeros((M, M), order="F")
     for _ in range(args.warmup):
-        r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA)
+        r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA, in_place=True)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA)
+        r.cannon_fulloffload(A, B, C, 1, 1, ALPHA, BETA, in_place=True)
         times.append(time.perf_counter() - t0)
     ms = 1e3 * statistics.mean(times)
     v = 2 * M ** 3 / (ms * 1e-3) / 1e12
@@ -408,14 +410,18 @@ def _ozaki_inputs(n, seed, phi, k=None):
 
 def workload_precision(args):
     """FP64 emulation at M = N = K = 16384 for phi in {0.5, 4.0}: native DMMA, INT8 slices
-    4..8 (and 9, 10 for phi = 4), CRT with 12..17 moduli, BF16 slices 7 and 8; error vs the
-    host FP64 GEMM on 48 sampled rows; whole-call TFLOP/s (split + GEMM + reconstruction)."""
+    4..8 (and 9, 10 for phi = 4), CRT with 12..20 moduli, BF16 slices 7 and 8; errors against
+    the exact product (ROWS sampled rows x all columns in double-double on the host) and, for
+    context, the host FP64 GEMM's own error; whole-call TFLOP/s (split + GEMM +
+    reconstruction)."""
     import numpy as np
+
+    import oracle as O
 
     torch, dgt, h = _setup()
     n = args.size
     flops = 2.0 * n ** 3
-    rows = np.sort(np.random.default_rng(1).choice(n, 48, replace=False))
+    rows = np.sort(np.random.default_rng(1).choice(n, ROWS, replace=False))
     out = []
     sampler = ClockSampler(0)
     sampler.start()
@@ -423,11 +429,13 @@ def workload_precision(args):
         A, B = _ozaki_inputs(n, SEED + int(phi * 10), phi)
         dA, dB = _dev(torch, A), _dev(torch, B)
         dC = torch.zeros((n, n), dtype=torch.float64, device="cuda")
-        want = A[rows, :] @ B
+        exact = O.orc().dd_rows(A[rows, :], B)
+        blas = _rel(A[rows, :] @ B, exact)
+        out.append({"phi": phi, "method": "host_openblas", "max_rel": blas[0], "fro_rel": blas[1]})
         runs = [("native", dgt.FP64_NATIVE, 0)] + [(f"int8_s{S}", dgt.FP64_OZAKI_INT8, S) for S in (4, 5, 6, 7, 8)]
         if phi > 1:
             runs += [(f"int8_s{S}", dgt.FP64_OZAKI_INT8, S) for S in (9, 10)]
-        runs += [(f"crt_n{N}", dgt.FP64_OZAKI2_INT8, N) for N in (12, 13, 14, 15, 16, 17)]
+        runs += [(f"crt_n{N}", dgt.FP64_OZAKI2_INT8, N) for N in range(12, 21)]
         runs += [(f"bf16_s{S}", dgt.FP64_OZAKI_BF16, S) for S in (7, 8)]
         for name, mode, S in runs:
             f = lambda: h.dgemm("N", "N", n, n, n, 1.0, dA.data_ptr(), n, dB.data_ptr(), n, 0.0, dC.data_ptr(), n,
@@ -435,7 +443,7 @@ def workload_precision(args):
             f()
             torch.cuda.synchronize()
             h.check_device()
-            err = _rel(_rows_of(dC, rows, (n, n)), want)
+            err = _rel(_rows_of(dC, rows, (n, n)), exact)
             bf16 = mode == dgt.FP64_OZAKI_BF16
             ms = _time_ms(torch, f, 1 if bf16 else 3, warm=0 if bf16 else 1)
             out.append({"phi": phi, "method": name, "slices": S, "tflops": flops / (ms * 1e-3) / 1e12, "ms": ms,
@@ -445,6 +453,7 @@ def workload_precision(args):
     clocks = sampler.stop()
     print(json.dumps({"workload": "precision", "unit": "TFLOP/s (FP64-equivalent, 2*M*N*K)", "M": n, "N": n, "K": n,
                       "dtype": "f64", "data": "synthetic (U[0,1)-0.5)*exp(phi*N(0,1)) seeded",
+                      "errors_vs": f"exact product, {len(rows)} sampled rows x {n} columns in double-double",
                       "sampled_rows": len(rows), "ozaki_variant": h.get_tuning(dgt.TUNE_OZAKI_VARIANT),
                       "results": out, "clocks": clocks}))
     h.close()
@@ -752,8 +761,122 @@ def workload_edges(args):
     h.close()
 
 
+def workload_layout(args):
+    """Every device-memory layout kernel against HBM bandwidth (L2 flushed before each timed
+    call, median of 10), each result checked bit for bit against its inverse or a second path:
+    block-cyclic pack of A, B, C and unpack of C of the ragged SUMMA configuration
+    (15000 x 17000 x 9000, 4 x 4 grid, 256 blocks; pblasDecomposer::scatterMatrix /
+    gatherMatrix); 2D-block deliver and gather on the same shapes over 16 ranks
+    (BlockSequentialDecomposer::deliverMatrix / gatherResult: A row panels, B column panels, C
+    blocks); Cannon decompose and reorder of 8192^2 matrices on a 4 x 4 grid
+    (Summa25Decomposer::decompose2D / reorderMatrix); the strided block copy (copyBlock).
+    Algorithmic bytes = 8 read + 8 written per element moved."""
+    torch, dgt, h = _setup()
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    rnd = lambda shape: torch.rand(shape, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    out = {}
+
+    def rec(name, fn, elems, check):
+        ms = _time_ms(torch, fn, 10, flush=flush)
+        torch.cuda.synchronize()
+        h.check_device()
+        gbs = 16.0 * elems / (ms * 1e-3) / 1e9
+        out[name] = {"elements": elems, "ms": ms, "GB/s": gbs, "frac_of_hbm": gbs / hbm, "bitwise": bool(check())}
+
+    sampler = ClockSampler(0)
+    sampler.start()
+    # block-cyclic (config 2)
+    M, N, K, b, p, q = 15000, 17000, 9000, 256, 4, 4
+
+    def cyclic(rows, cols):
+        shp = [(dgt.numroc(rows, b, r // q, 0, p), dgt.numroc(cols, b, r % q, 0, q)) for r in range(p * q)]
+        bufs = [torch.empty((max(c, 1), max(r_, 1)), dtype=torch.float64, device="cuda") for r_, c in shp]
+        return bufs, [x.data_ptr() for x in bufs], [max(r_, 1) for r_, _ in shp]
+
+    for name, rows, cols in (("A", M, K), ("B", K, N), ("C", M, N)):
+        G = rnd((cols, rows))
+        bufs, ptrs, lld = cyclic(rows, cols)
+        back = torch.zeros_like(G)
+        pack = lambda: h.pack_block_cyclic(rows, cols, b, b, p, q, G.data_ptr(), rows, ptrs, lld)
+        unpack = lambda: h.unpack_block_cyclic(rows, cols, b, b, p, q, back.data_ptr(), rows, ptrs, lld)
+        rec(f"block_cyclic pack {name} {rows}x{cols}", pack, rows * cols,
+            lambda: (unpack(), torch.cuda.synchronize(), torch.equal(back, G))[2])
+        if name == "C":
+            back.zero_()
+            rec(f"block_cyclic unpack C {rows}x{cols}", unpack, rows * cols, lambda: torch.equal(back, G))
+        del G, bufs, back
+    torch.cuda.empty_cache()
+    # 2D block (config 2 shapes, 16 ranks)
+    P = 16
+    dr, dc = dgt.block2d_grid(P)
+    A, B, C = rnd((K, M)), rnd((N, K)), rnd((N, M))
+    tm = [M // dr + (M % dr if i == dr - 1 else 0) for i in range(dr)]
+    tn = [N // dc + (N % dc if j == dc - 1 else 0) for j in range(dc)]
+    lA = [torch.empty((K, tm[r // dc]), dtype=torch.float64, device="cuda") for r in range(P)]
+    lB = [torch.empty((tn[r % dc], K), dtype=torch.float64, device="cuda") for r in range(P)]
+    lC = [torch.empty((tn[r % dc], tm[r // dc]), dtype=torch.float64, device="cuda") for r in range(P)]
+    ptrs = lambda xs: [x.data_ptr() for x in xs]
+    deliver = lambda: h.pack_block2d(M, N, K, P, 1, A.data_ptr(), B.data_ptr(), C.data_ptr(), ptrs(lA), ptrs(lB),
+                                     ptrs(lC))
+    Cb = torch.zeros_like(C)
+    gather = lambda: h.unpack_block2d(M, N, P, 1, Cb.data_ptr(), ptrs(lC))
+
+    def check_deliver():
+        ok = True
+        for r in range(P):
+            i, j = r // dc, r % dc
+            r0, c0 = i * (M // dr), j * (N // dc)
+            ok &= torch.equal(lA[r], A[:, r0:r0 + tm[i]]) and torch.equal(lB[r], B[c0:c0 + tn[j], :])
+            ok &= torch.equal(lC[r], C[c0:c0 + tn[j], r0:r0 + tm[i]])
+        return ok
+
+    elems = M * K * dc + K * N * dr + M * N
+    rec(f"block2d deliver A,B,C ({dr}x{dc} ranks, A panels x{dc}, B panels x{dr})", deliver, elems, check_deliver)
+    rec(f"block2d gather C {M}x{N}", gather, M * N, lambda: torch.equal(Cb, C))
+    del A, B, C, lA, lB, lC, Cb
+    torch.cuda.empty_cache()
+    # Cannon 2D (8192^2 on 4 x 4)
+    S, pc = 8192, 4
+    A, B, C = rnd((S, S)), rnd((S, S)), rnd((S, S))
+    ts = S // pc
+    tiles = lambda: [torch.empty((ts, ts), dtype=torch.float64, device="cuda") for _ in range(pc * pc)]
+    tA, tB, tC = tiles(), tiles(), tiles()
+    dec = lambda: h.pack_cannon2d(S, pc, A.data_ptr(), B.data_ptr(), C.data_ptr(), ptrs(tA), ptrs(tB), ptrs(tC))
+    Cb = torch.zeros_like(C)
+    reo = lambda: h.unpack_cannon2d(S, pc, Cb.data_ptr(), ptrs(tC))
+
+    def check_dec():
+        ok = True
+        for r in range(pc * pc):
+            i, j = r // pc, r % pc
+            ok &= torch.equal(tA[r], A[j * ts:(j + 1) * ts, i * ts:(i + 1) * ts])
+            ok &= torch.equal(tB[r], B[j * ts:(j + 1) * ts, i * ts:(i + 1) * ts])
+        return ok
+
+    rec(f"cannon decompose A,B,C {S}^2 on {pc}x{pc}", dec, 3 * S * S, check_dec)
+    rec(f"cannon reorder C {S}^2 on {pc}x{pc}", reo, S * S, lambda: torch.equal(Cb, C))
+    # strided block copy (copyBlock): a 16384 x 16384 block from ld 16384 to ld 16388
+    R2, C2 = 16384, 16384
+    src = rnd((C2, R2))
+    dst = torch.zeros((C2, R2 + 4), dtype=torch.float64, device="cuda")
+    rec(f"copy_block {R2}x{C2} ld {R2}->{R2 + 4}", lambda: h.copy_block(R2, C2, src.data_ptr(), dst.data_ptr(), R2,
+                                                                        R2 + 4), R2 * C2,
+        lambda: torch.equal(dst[:, :R2], src))
+    clocks = sampler.stop()
+    print(json.dumps({"workload": "layout", "unit": "GB/s", "hbm_peak_gbs": hbm,
+                      "hbm_peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                      "bytes_rule": "16 B per element moved (8 read + 8 written)", "l2": "flushed before each call",
+                      "results": out, "clocks": clocks}))
+    h.close()
+
+
 WORKLOADS = {"summa": workload_summa, "precision": workload_precision, "fp32": workload_fp32,
-             "batching": workload_batching, "once": workload_once, "edges": workload_edges}
+             "batching": workload_batching, "once": workload_once, "edges": workload_edges,
+             "layout": workload_layout}
 
 
 # ---- dgt arm ------------------------------------------------------------------------------------
@@ -791,36 +914,50 @@ def main():
     C_nat = torch.zeros_like(C)
     pa, pb, pc = A.data_ptr(), B.data_ptr(), C.data_ptr()
 
-    def run(mode, S, out=pc):
-        h.dgemm("N", "N", n, n, n, ALPHA, pa, n, pb, n, BETA, out, n, mode=mode, slices=S)
+    def run(mode, S, out=pc, a=pa, b=pb):
+        h.dgemm("N", "N", n, n, n, ALPHA, a, n, b, n, BETA, out, n, mode=mode, slices=S)
 
-    # ---- accuracy: sampled rows vs the host FP64 oracle (OpenBLAS) ----
-    rows = np.sort(np.random.default_rng(1).choice(n, 48, replace=False))
+    # ---- accuracy against the exact product ----
+    # ROWS sampled rows of alpha*A*B over all n columns, in double-double on the host (TwoSum /
+    # TwoProduct: exact to far below FP64 rounding), rounded once.  Every result -- native,
+    # each emulation count, and the host FP64 GEMM for context -- is measured against it, so
+    # "equal error" compares each method's own error, not its disagreement with another
+    # rounded FP64 GEMM.
+    rows = np.sort(np.random.default_rng(1).choice(n, ROWS, replace=False))
     rows_t = torch.from_numpy(rows).cuda()
-    want = ALPHA * (A_np[rows, :] @ B_np)
 
-    def rows_err(t):  # tensor column r holds matrix row r: gather the sampled rows on device
+    def exact_rows(An, Bn):
+        return O.orc().dd_rows(An[rows, :], Bn, ALPHA)
+
+    def rows_err(t, ex):  # tensor column r holds matrix row r: gather the sampled rows on device
         got = t[:, rows_t].cpu().numpy().T
-        return O.rel_errors(got, want)
+        return O.rel_errors(got, ex)
 
+    def scan(schemes, ex, nat_err, a, b):
+        """Errors of every count of every scheme vs the exact rows; per scheme the smallest
+        count whose max- and Frobenius-relative errors are both <= the native kernel's."""
+        errs, chosen = {}, {}
+        for name, (mode, counts) in schemes.items():
+            for cnt in counts:
+                run(mode, cnt, pc, a, b)
+                torch.cuda.synchronize()
+                h.check_device()
+                e = rows_err(C, ex)
+                errs[(name, cnt)] = e
+                if name not in chosen and e[0] <= nat_err[0] and e[1] <= nat_err[1]:
+                    chosen[name] = cnt
+        return errs, chosen
+
+    exact = exact_rows(A_np, B_np)
+    blas_err = O.rel_errors(ALPHA * (A_np[rows, :] @ B_np), exact)  # host OpenBLAS dgemm, for context
     run(dgt.FP64_NATIVE, 0, C_nat.data_ptr())
     torch.cuda.synchronize()
-    nat_err = rows_err(C_nat)
+    nat_err = rows_err(C_nat, exact)
     # Two emulation schemes are candidates: CRT over INT8 residues (count = moduli) and INT8
-    # digit slices (count = slices).  For each, the smallest count whose max- and Frobenius-
-    # relative errors are both <= the native kernel's ("equal error"); the faster of the two
-    # (after tuning kernel variants) is the headline.
-    schemes = {"crt": (dgt.FP64_OZAKI2_INT8, (14, 15, 16, 17)), "slices": (dgt.FP64_OZAKI_INT8, (6, 7, 8))}
-    errs, chosen = {}, {}
-    for name, (mode, counts) in schemes.items():
-        for cnt in counts:
-            run(mode, cnt)
-            torch.cuda.synchronize()
-            h.check_device()
-            errs[(name, cnt)] = rows_err(C)
-            e = errs[(name, cnt)]
-            if name not in chosen and e[0] <= nat_err[0] and e[1] <= nat_err[1]:
-                chosen[name] = cnt
+    # digit slices (count = slices).  For each, the smallest count at equal error; the faster
+    # of the two (after tuning kernel variants) is the headline.
+    schemes = {"crt": (dgt.FP64_OZAKI2_INT8, (14, 15, 16, 17, 18)), "slices": (dgt.FP64_OZAKI_INT8, (6, 7, 8, 9))}
+    errs, chosen = scan(schemes, exact, nat_err, pa, pb)
     equal_error = bool(chosen)
     for name, (mode, counts) in schemes.items():
         chosen.setdefault(name, counts[-1])
@@ -834,22 +971,6 @@ def main():
     eligible = [nm for nm in schemes if (lambda e: e[0] <= nat_err[0] and e[1] <= nat_err[1])(errs[(nm, chosen[nm])])]
     best = min(eligible or list(schemes), key=lambda nm: scheme_ms[nm])
     MODE, S = schemes[best][0], chosen[best]
-    # phi = 4.0 error (same kernels; data-dependent accuracy only)
-    A4 = O.ozaki_matrix((n, 2048), SEED + 99, 4.0)
-    B4 = O.ozaki_matrix((2048, 1024), SEED + 98, 4.0)
-    dA4 = torch.from_numpy(np.ascontiguousarray(A4.T)).cuda()
-    dB4 = torch.from_numpy(np.ascontiguousarray(B4.T)).cuda()
-    dC4 = torch.zeros((1024, n), dtype=torch.float64, device="cuda")
-    want4 = A4 @ B4
-    phi4 = {}
-    for label, mode, SS in (("native", dgt.FP64_NATIVE, 2), (f"crt_n{chosen['crt']}", dgt.FP64_OZAKI2_INT8,
-                                                              chosen["crt"]), ("crt_n17", dgt.FP64_OZAKI2_INT8, 17),
-                            (f"slices_s{chosen['slices']}", dgt.FP64_OZAKI_INT8, chosen["slices"])):
-        h.dgemm("N", "N", n, 1024, 2048, 1.0, dA4.data_ptr(), n, dB4.data_ptr(), 2048, 0.0, dC4.data_ptr(), n,
-                mode=mode, slices=SS)
-        torch.cuda.synchronize()
-        phi4[label] = O.rel_errors(dC4.cpu().numpy().T, want4)
-    del dA4, dB4, dC4
 
     def timed(fn, steps, warm):
         for _ in range(warm):
@@ -953,6 +1074,31 @@ def main():
     torch.cuda.synchronize()
     e2e_same = bool(np.array_equal(C_h.numpy()[:, rows], C[:, rows_t].cpu().numpy()))
 
+    # ---- phi = 4.0: the same 16384^3 product on the wide-dynamic-range input, timed ----
+    # (U - 0.5) exp(4 N(0,1)) entries span ~14 decades; CRT counts are scanned against the exact
+    # rows as above (the INT8 slice scheme's errors are listed beside), the smallest count at
+    # equal error is timed like the headline, and native DMMA is timed on the same matrices.
+    A4_np = O.ozaki_matrix((n, n), SEED + 7 * rank + 40, 4.0)
+    B4_np = O.ozaki_matrix((n, n), SEED + 7 * rank + 41, 4.0)
+    A4 = torch.from_numpy(np.ascontiguousarray(A4_np.T)).cuda()
+    B4 = torch.from_numpy(np.ascontiguousarray(B4_np.T)).cuda()
+    pa4, pb4 = A4.data_ptr(), B4.data_ptr()
+    exact4 = exact_rows(A4_np, B4_np)
+    blas4_err = O.rel_errors(ALPHA * (A4_np[rows, :] @ B4_np), exact4)
+    run(dgt.FP64_NATIVE, 0, C_nat.data_ptr(), pa4, pb4)
+    torch.cuda.synchronize()
+    nat4_err = rows_err(C_nat, exact4)
+    schemes4 = {"crt": (dgt.FP64_OZAKI2_INT8, (15, 16, 17, 18, 19, 20)),
+                "slices": (dgt.FP64_OZAKI_INT8, (8, 9, 10))}
+    errs4, chosen4 = scan(schemes4, exact4, nat4_err, pa4, pb4)
+    S4 = chosen4.get("crt", schemes4["crt"][1][-1])
+    equal4 = "crt" in chosen4
+    nat4_ms = max_over_ranks(timed(lambda: run(dgt.FP64_NATIVE, 0, C_nat.data_ptr(), pa4, pb4),
+                                   max(2, args.steps // 2), 1), world)
+    emu4_ms = max_over_ranks(timed(lambda: run(dgt.FP64_OZAKI2_INT8, S4, pc, pa4, pb4), args.steps, args.warmup),
+                             world)
+    del A4, B4
+
     # ---- CPU baseline: the reference's validation GEMM (OpenBLAS dgemm), bounded sample ----
     cpu = None
     if rank == 0 and world == 1:
@@ -970,6 +1116,20 @@ def main():
                "sample": f"host OpenBLAS dgemm (numpy, {cores} threads) on the first {ms_rows} rows of A "
                          f"times B ({ms_rows}x{n}x{n}), the reference's validation GEMM "
                          f"(src/Wrappers/cuBLASMp/cuBLASMpValidator.cpp:48)"}
+
+    # ---- N > 1: the physical step loop on the ragged SUMMA configuration ----
+    # (15000 x 17000 x 9000, 256 blocks, alpha 1.5, beta -0.5) over the world's most-square
+    # grid: panel broadcasts over NCCL (collective) and owners' panels read in place over
+    # NVLink (fused), each timed on the device, max over ranks, beside the replicas' value
+    distributed = None
+    if world > 1:
+        from dgt.dist import summa_benchmark
+
+        try:
+            distributed = summa_benchmark(15000, 17000, 9000, 256, 256, 256, steps=3, warmup=1, alpha=1.5, beta=-0.5,
+                                          seed=SEED)
+        except Exception as e:  # reported in the line; the replicas' value stands
+            distributed = {"error": f"{type(e).__name__}: {e}"}
 
     peaks = measured_peaks()
     if rank == 0:
@@ -993,8 +1153,20 @@ def main():
                              "value": job_tflops(world, flops, other_ms), "ms_per_step": other_ms,
                              "max_rel": errs[(other, chosen[other])][0], "fro_rel": errs[(other, chosen[other])][1],
                              "kernel_variant": tuned[other]["variant"]},
+            "errors_vs": f"exact product: {ROWS} sampled rows x all {n} columns of alpha*A*B in double-double "
+                         f"on the host (oracle orc_dd_rows), rounded once; max = max elementwise |x - e| / |e|, "
+                         f"fro = ||x - e||_F / ||e||_F",
+            "host_blas_error": {"max_rel": blas_err[0], "fro_rel": blas_err[1]},
             "errors_by_count": {f"{k[0]}_{k[1]}": v for k, v in errs.items()},
-            "phi4_errors": {k: {"max_rel": v[0], "fro_rel": v[1]} for k, v in phi4.items()},
+            "phi4": {"value": job_tflops(world, flops, emu4_ms), "ms_per_step": emu4_ms, "scheme": "crt",
+                     "count": S4, "equal_error": equal4, "speedup_vs_native": nat4_ms / emu4_ms,
+                     "max_rel": errs4[("crt", S4)][0], "fro_rel": errs4[("crt", S4)][1],
+                     "native_dmma": {"value": job_tflops(world, flops, nat4_ms), "ms_per_step": nat4_ms,
+                                     "max_rel": nat4_err[0], "fro_rel": nat4_err[1]},
+                     "host_blas_error": {"max_rel": blas4_err[0], "fro_rel": blas4_err[1]},
+                     "slices_equal_error_count": chosen4.get("slices"),
+                     "errors_by_count": {f"{k[0]}_{k[1]}": v for k, v in errs4.items()},
+                     "inputs": f"(U-0.5)*exp(4.0*N(0,1)), M=N=K={n}, seeded"},
             "roofline": {"bound": "tensor", "kernel": "oz::digit_gemm (INT8 tcgen05 GEMM of the emulation)",
                          "achieved": achieved, "peak": int8_peak,
                          "unit": "TOP/s (INT8)", "frac": achieved / int8_peak, "traffic": traffic,
@@ -1007,6 +1179,7 @@ def main():
                     "rows_equal_device_result": e2e_same},
             "gpu_launches": launches,
             "clocks": clocks,
+            "distributed": distributed,
             "cpu_baseline": cpu,
             "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
         }

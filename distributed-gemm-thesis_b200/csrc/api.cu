@@ -277,6 +277,9 @@ dgt_status dgt_set_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t value) {
             if (value < 0 || value > 4) return fail(h, DGT_ERROR_INVALID_VALUE, "unknown Ozaki kernel variant");
             h->ozaki_variant = value;
             return DGT_SUCCESS;
+        case DGT_TUNE_TEST_STALL:
+            h->test_stall = value != 0;
+            return DGT_SUCCESS;
     }
     return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
 }
@@ -300,6 +303,7 @@ dgt_status dgt_get_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t* value) {
         case DGT_TUNE_OZAKI_SLICES: *value = h->slices; return DGT_SUCCESS;
         case DGT_TUNE_PROFILE: *value = h->profile ? 1 : 0; return DGT_SUCCESS;
         case DGT_TUNE_OZAKI_VARIANT: *value = h->ozaki_variant; return DGT_SUCCESS;
+        case DGT_TUNE_TEST_STALL: *value = h->test_stall; return DGT_SUCCESS;
     }
     return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
 }

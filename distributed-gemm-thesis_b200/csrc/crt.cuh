@@ -51,22 +51,27 @@ namespace oz2 {
 
 constexpr int MAX_MODULI = 20, MIN_MODULI = 8;
 constexpr int MAX_NW = 5;     // 32-bit limbs of W_p and P (P < 2^160)
-constexpr int MAX_BETA = 58;  // |A'| < 2^58
+constexpr int SPLIT_BITS = 79;  // scaled operands are integers of magnitude below 2^79
 
-// Residues of x = rn(a 2^(beta-e)) (|x| <= 2^58) modulo p, in integers: x is cut into
-// 20-bit chunks x0, x1 (unsigned) and x2 = x >> 40 (arithmetic, |x2| <= 2^18), so
-// t = x2 c40 + x1 c20 + x0 (c20 = 2^20 mod p, c40 = 2^40 mod p) is congruent to x with
-// -2^26 < t < 2^29.  n = t + floor(p/2) + 2^18 p then lies in [0, 2^30), and with
-// magic = floor(2^38 / p) + 1 = 2^38 / p + e (0 < e <= 1), floor(n magic / 2^38) = floor(n / p)
-// because n e / 2^38 < 2^30 / 2^38 <= 1 / p (p <= 256).  One 32 x 32 -> 64-bit multiply-add
-// gives n magic = t magic + bias.  r = t - floor(n / p) p is the symmetric residue
-// ((x + floor(p/2)) mod p) - floor(p/2) minus 2^18 p, a multiple of 256, so the low byte of r
+// Residues of Y = rn(a 2^s) modulo p, in integers.  The norm rule keeps |Y| <= 2^sigma +
+// sqrt(k)/2 < 2^78 (sigma <= 77 for 20 moduli).  Y is taken as yh 2^40 + yl with
+// yh = rn(y 2^-40) and yl = rn(y - yh 2^40), |yh|, |yl| <= 2^39 (y - yh 2^40 is exact in
+// FP64, and yh 2^40 is an even integer, so the two roundings give rn(y) with its tie
+// rule).  Both are cut into 20-bit chunks, x0 = yl mod 2^20, x1 = yl >> 20, x2 = yh mod 2^20,
+// x3 = yh >> 20 (arithmetic shifts: |x1|, |x3| <= 2^19), and with c20, c40, c60 = 2^20, 2^40,
+// 2^60 mod p in the symmetric range (|c| <= 127; 0 for p = 256)
+// t = x3 c60 + x2 c40 + x1 c20 + x0 is congruent to Y with |t| < 127 2^21 + 2^20 < 2^28.
+// n = t + floor(p/2) + 2^21 p then lies in (0, 2^30), and with magic = floor(2^38 / p) + 1 =
+// 2^38 / p + e (0 < e <= 1), floor(n magic / 2^38) = floor(n / p) because
+// n e / 2^38 < 2^30 / 2^38 <= 1 / p (p <= 256).  One 32 x 32 -> 64-bit multiply-add gives
+// n magic = t magic + bias.  r = t - floor(n / p) p is the symmetric residue
+// ((Y + floor(p/2)) mod p) - floor(p/2) minus 2^21 p, a multiple of 256, so the low byte of r
 // is the symmetric residue as int8.
 struct ModTable {
     int32_t p[MAX_MODULI];
-    int32_t c20[MAX_MODULI], c40[MAX_MODULI];  // 2^20 mod p, 2^40 mod p
-    int32_t magic[MAX_MODULI];                 // floor(2^38 / p) + 1 (< 2^31 for p > 128)
-    long long bias[MAX_MODULI];                // (floor(p/2) + 2^18 p) magic
+    int32_t c20[MAX_MODULI], c40[MAX_MODULI], c60[MAX_MODULI];  // 2^20, 2^40, 2^60 mod p, symmetric
+    int32_t magic[MAX_MODULI];                                 // floor(2^38 / p) + 1 (< 2^31 for p > 128)
+    long long bias[MAX_MODULI];                                // (floor(p/2) + 2^21 p) magic
 };
 // Residue split geometry: a block of 128 threads covers RES_ROWS rows (mn) and RES_KSPAN
 // consecutive kk, one 32-byte sector of every plane row; RES_TPR threads share a row, each

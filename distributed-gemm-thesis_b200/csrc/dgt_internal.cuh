@@ -43,6 +43,7 @@ struct dgt_context {
     int dmma_variant = 2;  // native FP64 kernel variant (see dgemm_dmma.cu); 2 measured fastest
     int ozaki_variant = 1; // INT8 Ozaki kernel variant (see ozaki.cu); 1 measured fastest
     bool profile = false;  // record phase events (DGT_TUNE_PROFILE)
+    int test_stall = 0;    // failure-path test hook (DGT_TUNE_TEST_STALL)
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // split start, gemm start, gemm end
     bool ev_split = false;  // last call had a split phase
     std::string last_error;
@@ -70,6 +71,29 @@ struct dgt_context {
 };
 
 namespace dgt {
+
+// Opts Kernel into `bytes` of dynamic shared memory on the current device.  The attribute
+// belongs to the device's context, so it is set once per (kernel, device) -- a process that
+// launches on several devices sets it on each -- under a mutex, since host threads may
+// launch concurrently.
+template <auto Kernel>
+cudaError_t smem_opt_in(int bytes) {
+    constexpr int kMaxDev = 64;
+    static std::mutex mu;
+    static bool done[kMaxDev] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDev)
+        return cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    std::lock_guard<std::mutex> g(mu);
+    if (!done[dev]) {
+        e = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+        done[dev] = true;
+    }
+    return cudaSuccess;
+}
 
 inline dgt_status fail(dgt_context* h, dgt_status s, const std::string& msg) {
     if (h) h->last_error = msg;

@@ -289,13 +289,8 @@ size_t ozaki_scratch_bytes(int S, int64_t m, int64_t n, int64_t k) {
 template <class CF, int KIND>
 static cudaError_t launch_ozaki_variant(const CUtensorMap& tmA, const CUtensorMap& tmB, const oz::Params& prm,
                                         int num_sms, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(oz::digit_gemm<CF, KIND, 0>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t e = smem_opt_in<oz::digit_gemm<CF, KIND, 0>>((int)CF::SMEM);
+    if (e != cudaSuccess) return e;
     const int tiles = prm.tiles_m * prm.tiles_n;
     if constexpr (CF::PAIR) {
         // one 2-CTA cluster per 256 x 256 tile, persistent over half the SMs' worth of clusters
@@ -410,6 +405,7 @@ static dgt_status ozaki_run(dgt_context* h, cudaStream_t s, int num_sms, unsigne
         prm.groups_ext = dgroups;
     }
     prm.err = err;
+    prm.test_stall = h ? h->test_stall : 0;
     const int tiles = prm.tiles_m * prm.tiles_n;
     const int grid = std::min(tiles, num_sms);
     if (h) mark(h, 1);
@@ -461,13 +457,8 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
 
 template <class CF, int EPI>
 static cudaError_t launch_ozaki_grouped(const oz::Params& prm, int grid, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(oz::digit_gemm<CF, 0, EPI, true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CF::SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t e = smem_opt_in<oz::digit_gemm<CF, 0, EPI, true>>((int)CF::SMEM);
+    if (e != cudaSuccess) return e;
     static const CUtensorMap unused = {};  // grouped mode reads each problem's maps from its table
     oz::digit_gemm<CF, 0, EPI, true><<<grid, CF::THREADS, CF::SMEM, s>>>(unused, unused, prm);
     return cudaGetLastError();
@@ -688,6 +679,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     prm.segs_ext = nullptr;
     prm.groups_ext = nullptr;
     prm.err = h->dev_error;
+    prm.test_stall = h->test_stall;
     prm.gprobs = d_gp;
     prm.nprob = T;
     prm.total_tiles = tiles;

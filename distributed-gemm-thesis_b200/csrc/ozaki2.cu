@@ -2,10 +2,9 @@
 // Ozaki, Uchino, Imamura 2025, "Ozaki Scheme II: A GEMM-oriented emulation of
 // floating-point matrix multiplication using an integer modular technique").
 //
-//   1. Scale: row i of op(A) gets s_i = min(sigma - g_i, 58 - e_i), where max_k |a_ik| <
-//      2^e_i and 2^g_i bounds the row's 2-norm; A'_ik = rn(a_ik 2^s_i) (rounded to nearest
-//      even) is an integer of magnitude at most 2^58 and the row's 2-norm is at most
-//      2^sigma + sqrt(k)/2; columns of op(B) likewise.  By Cauchy-Schwarz every |(A'B')_ij|
+//   1. Scale: row i of op(A) gets s_i = sigma - g_i, where 2^g_i bounds the row's 2-norm;
+//      A'_ik = rn(a_ik 2^s_i) (rounded to nearest even) is an integer and the row's 2-norm is
+//      at most 2^sigma + sqrt(k)/2 (so every entry is below 2^78); columns of op(B) likewise.  By Cauchy-Schwarz every |(A'B')_ij|
 //      is below (P/2)(1 - 2^-20) for sigma_A + sigma_B from sigma_sum_for (op(A) takes the
 //      odd bit when the sum is odd).  Scaling by the norm instead of
 //      the max spends the integer range where the row's mass is: rows with a few large
@@ -19,8 +18,11 @@
 //      the symmetric range, equals (A'B')_ij exactly; it is rounded once to FP64 (correctly)
 //      and scaled by 2^-(s_i + t_j).  C = alpha C' + beta_C C.
 //
+// Entries of a scaled row are not capped below its norm bound: on heavy-tailed rows the
+// largest entries exceed 2^53 (they are integers already) and the small ones keep their
+// bits down to 2^0, so every added modulus still buys about 4 bits per operand.
 // Against the slice scheme (ozaki.cu), N GEMMs replace S(S+1)/2 digit products for the
-// same number of operand bits (N = 17 moduli: beta = 58 bits at K <= 16384, versus 36
+// same number of operand bits (N = 17 moduli: sigma = 65-66 bits at K <= 16384, versus 36
 // products for S = 8 slices of 7 bits), and the output is read and written once instead of
 // once per flush group.  The FLOP count reported for this path is 2*M*N*K.
 #include <cuda.h>
@@ -91,10 +93,9 @@ static double log2_product(int n) {
     return s;
 }
 
-// Norm scaling.  Row i of op(A) is scaled by 2^s_i with s_i = min(sigma - g_i, 58 - e_i):
-// 2^g_i bounds the row's 2-norm (g_i from the integer bound of qnorm_*), e_i its max, so every
-// scaled row has 2-norm <= 2^sigma and every element magnitude below 2^58 (the split's range);
-// columns of op(B) likewise.  After rounding to nearest, ||A'_i|| <= 2^sigma + sqrt(k)/2, and
+// Norm scaling.  Row i of op(A) is scaled by 2^s_i with s_i = sigma - g_i: 2^g_i bounds the
+// row's 2-norm (g_i from the integer bound of qnorm_*), so every scaled row has 2-norm
+// <= 2^sigma; columns of op(B) likewise.  After rounding to nearest, ||A'_i|| <= 2^sigma + sqrt(k)/2, and
 // by Cauchy-Schwarz |C'_ij| <= (2^sigma + sqrt(k)/2)^2.  sigma is the largest integer keeping
 // that below (P/2)(1 - 2^-20), which the reconstruction's exact quotient needs (the sqrt(k)/2
 // terms are below 2^-40 of 2^sigma for every sigma used, well inside the margin).
@@ -124,10 +125,12 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
     for (int i = 0; i < n; ++i) {
         const uint32_t p = (uint32_t)kModuli[i];
         mt.p[i] = (int32_t)p;
-        mt.c20[i] = (int32_t)((1ull << 20) % p);
-        mt.c40[i] = (int32_t)((1ull << 40) % p);
+        auto sym = [p](unsigned long long v) { return (int32_t)(v > p / 2 ? (long long)v - p : (long long)v); };
+        mt.c20[i] = sym((1ull << 20) % p);
+        mt.c40[i] = sym((1ull << 40) % p);
+        mt.c60[i] = sym((1ull << 60) % p);
         mt.magic[i] = (int32_t)((1ull << 38) / p + 1);
-        mt.bias[i] = ((long long)(p >> 1) + ((long long)p << 18)) * mt.magic[i];
+        mt.bias[i] = ((long long)(p >> 1) + ((long long)p << 21)) * mt.magic[i];
         Big M = P;
         big_div_small(M, p);  // M = P / p
         Big Mm = M;
@@ -224,9 +227,9 @@ __global__ void __launch_bounds__(256) qnorm_grouped(const oz::SplitJob* __restr
         qnorm_mn_block(J.X, J.ld, J.MN, J.K, oz::AMAX_KCHUNK, J.amax, J.qn, local % J.amax_bx, local / J.amax_bx);
 }
 
-// Scale of row mn: exps[mn] = sigma - s with s = min(sigma - g, 58 - e) (sigma = sigma_A for
-// rows of op(A), sigma_B for columns of op(B); see sigma_sum_for);
-// EXP_NONFINITE for a row with an infinite or NaN element.
+// Scale of row mn: exps[mn] = sigma - s = g with s = sigma - g (sigma = sigma_A for rows of
+// op(A), sigma_B for columns of op(B); see sigma_sum_for); EXP_NONFINITE for a row with an
+// infinite or NaN element.
 __device__ __forceinline__ int row_scale_exp(unsigned long long am, unsigned long long qv, int sigma, int& s) {
     const int e = oz::exponent_of_max(am);
     if (e == oz::EXP_NONFINITE) return e;
@@ -236,8 +239,8 @@ __device__ __forceinline__ int row_scale_exp(unsigned long long am, unsigned lon
     }
     const int h = (64 - __clzll((long long)(qv - 1ull)) + 1) >> 1;  // 2^h >= sqrt(qv)
     const int g = e - 20 + h;
-    s = min(sigma - g, 58 - e);
-    return sigma - s;
+    s = sigma - g;
+    return g;
 }
 
 // ---- device: residue planes ----------------------------------------------------------------------
@@ -283,20 +286,24 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         }
         return;
     }
-    int32_t x0[E], x1[E], x2[E];  // x = x2 2^40 + x1 2^20 + x0, x0 and x1 in [0, 2^20)
+    // Y = x3 2^60 + x2 2^40 + x1 2^20 + x0 (crt.cuh ModTable): x0, x2 in [0, 2^20), |x1|, |x3| <= 2^19
+    int32_t x0[E], x1[E], x2[E], x3[E];
 #pragma unroll
     for (int i = 0; i < E; ++i) {
         const int64_t kk = k0 + i;
         double a = 0.0;
         if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
-        // an integer of magnitude <= 2^58 (exact scaling, rounded to nearest even)
-        const long long x = live ? __double2ll_rn(direct ? a * fsc : oz::scale2(a, sc)) : 0ll;
-        x0[i] = (int32_t)(x & 0xfffff);
-        x1[i] = (int32_t)((x >> 20) & 0xfffff);
-        x2[i] = (int32_t)(x >> 40);
+        // y = a 2^sc exactly; Y = rn(y) = yh 2^40 + yl, |yh|, |yl| <= 2^39
+        const double y = live ? (direct ? a * fsc : oz::scale2(a, sc)) : 0.0;
+        const double yh = rint(y * 0x1p-40);
+        const long long hi = __double2ll_rn(yh), lo = __double2ll_rn(fma(-yh, 0x1p40, y));
+        x0[i] = (int32_t)(lo & 0xfffff);
+        x1[i] = (int32_t)(lo >> 20);
+        x2[i] = (int32_t)(hi & 0xfffff);
+        x3[i] = (int32_t)(hi >> 20);
     }
     for (int j = 0; j < nmod; ++j, out += plane) {
-        const int32_t p = mt.p[j], c20 = mt.c20[j], c40 = mt.c40[j], mg = mt.magic[j];
+        const int32_t p = mt.p[j], c20 = mt.c20[j], c40 = mt.c40[j], c60 = mt.c60[j], mg = mt.magic[j];
         const long long bias = mt.bias[j];
         uint32_t w[E / 4];
 #pragma unroll
@@ -305,7 +312,7 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int i = 4 * q + u;
-                const int32_t t = x2[i] * c40 + x1[i] * c20 + x0[i];               // = x mod p, in (-2^26, 2^29)
+                const int32_t t = x3[i] * c60 + x2[i] * c40 + x1[i] * c20 + x0[i];  // = Y mod p, |t| < 2^28
                 const int32_t qt = (int32_t)((unsigned long long)((long long)t * mg + bias) >> 38);
                 r[u] = t - qt * p;  // low byte: the symmetric residue
             }
@@ -563,6 +570,12 @@ cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, in
         crt_grouped<4, 16><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
     else if (nmod == 17)
         crt_grouped<5, 17><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
+    else if (nmod == 18)
+        crt_grouped<5, 18><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
+    else if (nmod == 19)
+        crt_grouped<5, 19><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
+    else if (nmod == 20)
+        crt_grouped<5, 20><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc);
     else
         switch (limbs_for(nmod)) {
             case 2: crt_grouped<2, 0><<<blocks, 256, 0, s>>>(jobs, njobs, threads, cc); break;
@@ -580,13 +593,8 @@ cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, in
 template <class CF>
 static cudaError_t launch_residue_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const oz::Params& prm,
                                        int num_sms, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(oz::digit_gemm<CF, 0, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)CF::SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t e = smem_opt_in<oz::digit_gemm<CF, 0, 2>>((int)CF::SMEM);
+    if (e != cudaSuccess) return e;
     const int tiles = prm.tiles_m * prm.tiles_n;
     if constexpr (CF::PAIR) {
         cudaLaunchConfig_t cfg = {};
@@ -720,6 +728,7 @@ dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, i
     prm.res_ld = m_pad;
     prm.res_plane = m_pad * n_pad;
     prm.err = h->dev_error;
+    prm.test_stall = h->test_stall;
     mark(h, 1);
     cudaError_t le;
     if (sh.variant == 4)
@@ -746,6 +755,12 @@ dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, i
         DGT_CRT_LAUNCH(4, 16);
     else if (nmod == 17)
         DGT_CRT_LAUNCH(5, 17);
+    else if (nmod == 18)
+        DGT_CRT_LAUNCH(5, 18);
+    else if (nmod == 19)
+        DGT_CRT_LAUNCH(5, 19);
+    else if (nmod == 20)
+        DGT_CRT_LAUNCH(5, 20);
     else
         switch (limbs_for(nmod)) {
             case 2: DGT_CRT_LAUNCH(2, 0); break;

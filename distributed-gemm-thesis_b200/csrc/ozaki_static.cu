@@ -10,18 +10,21 @@
 // holds until the process exits.
 //
 // The array's name is only a host-side stand-in in host code, so the first call on each
-// device looks up its device address with cudaGetSymbolAddress (with that device current)
-// and caches it; make that first call before any stream capture begins.  Every
-// call on a device shares the array and finds the previous call's contents in it: the
-// parts that must start at zero are cleared on the stream each time, and calls whose
-// work overlaps on the GPU (two streams, or two host threads) race on the scratch.
+// device looks up its device address with cudaGetSymbolAddress (with that device current),
+// clears the error word and caches both; make that first call before any stream capture
+// begins.  Later calls outside a capture look the address up again, so a context that was
+// reset (cudaDeviceReset) and recreated is picked up.  Every call on a device shares the
+// array and finds the previous call's contents in it: the parts that must start at zero are
+// cleared on the stream each time, and calls whose work overlaps on the GPU (two streams,
+// or two host threads) race on the scratch.
+//
+// The error word is sticky: a bounded device wait that ran out in any call sets a bit that
+// stays until dgt_ozaki_static_check reads and clears it.
 #include <cuda_runtime.h>
 
 #include <mutex>
 
 #include "dgt_internal.cuh"
-
-#define DGT_OZAKI_STATIC_SCRATCH_BYTES (64ull << 20)
 
 namespace {
 
@@ -33,22 +36,40 @@ std::mutex g_setup_mutex;
 void* g_scratch_addr[kMaxDevices] = {};
 int g_num_sms[kMaxDevices] = {};
 
-// Once per device, with that device current: the array's device address and SM count.
-dgt_status setup_device(int dev, void** addr, int* sms) {
+// With device `dev` current: the array's device address and the SM count.  A device seen for
+// the first time (or whose array moved, after a context reset) gets its error word cleared.
+// Inside a stream capture only the cached address is used.
+dgt_status setup_device(int dev, cudaStream_t s, void** addr, int* sms) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return DGT_ERROR_CUDA;
+    if (cs == cudaStreamCaptureStatusNone || !g_scratch_addr[dev]) {
+        if (cs != cudaStreamCaptureStatusNone) return DGT_ERROR_NOT_INITIALIZED;  // first call inside a capture
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_ozaki_scratch);
         if (e != cudaSuccess || !p) return DGT_ERROR_CUDA;
-        int n = 0;
-        e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (e != cudaSuccess) return DGT_ERROR_CUDA;
-        g_num_sms[dev] = n;
-        g_scratch_addr[dev] = p;
+        if (p != g_scratch_addr[dev]) {
+            int n = 0;
+            e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess) return DGT_ERROR_CUDA;
+            if (cudaMemset(p, 0, sizeof(unsigned int)) != cudaSuccess) return DGT_ERROR_CUDA;
+            g_num_sms[dev] = n;
+            g_scratch_addr[dev] = p;
+        }
     }
     *addr = g_scratch_addr[dev];
     *sms = g_num_sms[dev];
     return DGT_SUCCESS;
+}
+
+// C = beta C for k = 0 (BLAS: C is not read when beta is 0).
+__global__ void scale_c(double* __restrict__ C, int64_t ldc, int64_t m, int64_t n, double beta) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
+        double* c = C + i + j * ldc;
+        *c = beta == 0.0 ? 0.0 : beta * *c;
+    }
 }
 
 }  // namespace
@@ -67,26 +88,44 @@ extern "C" dgt_status dgt_dgemm_ozaki_static(dgt_stream_t stream, char transa, c
         return DGT_ERROR_INVALID_VALUE;
     if (m == 0 || n == 0) return DGT_SUCCESS;
     if (!C || (k > 0 && (!A || !B))) return DGT_ERROR_INVALID_VALUE;
-    if (k == 0) return DGT_ERROR_UNSUPPORTED;  // nothing to emulate; use dgt_dgemm
-    const size_t need = ozaki_scratch_bytes(slices, m, n, k);
-    if (need == 0) return DGT_ERROR_UNSUPPORTED;
-    if (need > DGT_OZAKI_STATIC_SCRATCH_BYTES - kErrBytes) {
-        std::fprintf(stderr,
-                     "dgt_dgemm_ozaki_static: m=%lld n=%lld k=%lld with %d slices needs %zu bytes of scratch; the "
-                     "static scratch holds %llu bytes\n",
-                     (long long)m, (long long)n, (long long)k, slices, need,
-                     (unsigned long long)(DGT_OZAKI_STATIC_SCRATCH_BYTES - kErrBytes));
-        return DGT_ERROR_INVALID_VALUE;
+    size_t need = 0;
+    if (k > 0) {
+        need = ozaki_scratch_bytes(slices, m, n, k);
+        if (need == 0) return DGT_ERROR_UNSUPPORTED;
+        // too large for the fixed array: the caller's problem, reported by status alone
+        if (need > DGT_OZAKI_STATIC_SCRATCH_BYTES - kErrBytes) return DGT_ERROR_INVALID_VALUE;
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return DGT_ERROR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
     void* base = nullptr;
     int sms = 0;
-    dgt_status st = setup_device(dev, &base, &sms);
+    dgt_status st = setup_device(dev, s, &base, &sms);
     if (st != DGT_SUCCESS) return st;
-    cudaStream_t s = (cudaStream_t)stream;
+    if (k == 0) {  // nothing to multiply: C = beta C
+        const dim3 grid((unsigned)((m + 255) / 256), (unsigned)std::min<int64_t>(n, 4096));
+        scale_c<<<grid, 256, 0, s>>>(C, ldc, m, n, *beta);
+        return cudaGetLastError() == cudaSuccess ? DGT_SUCCESS : DGT_ERROR_CUDA;
+    }
     unsigned int* err = (unsigned int*)base;
-    if (cudaMemsetAsync(err, 0, sizeof(unsigned int), s) != cudaSuccess) return DGT_ERROR_CUDA;
     return ozaki_dgemm_on(s, sms, err, (char*)base + kErrBytes, DGT_OZAKI_STATIC_SCRATCH_BYTES - kErrBytes, ta, tb,
                           m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc, slices);
+}
+
+extern "C" dgt_status dgt_ozaki_static_check(dgt_stream_t stream) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return DGT_ERROR_CUDA;
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        base = g_scratch_addr[dev];
+    }
+    if (!base) return DGT_SUCCESS;  // no call on this device yet: nothing to report
+    if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return DGT_ERROR_CUDA;
+    unsigned int word = 0;
+    if (cudaMemcpy(&word, base, sizeof(word), cudaMemcpyDeviceToHost) != cudaSuccess) return DGT_ERROR_CUDA;
+    if (word == 0) return DGT_SUCCESS;
+    if (cudaMemset(base, 0, sizeof(word)) != cudaSuccess) return DGT_ERROR_CUDA;
+    if (word & DGT_DEVERR_TIMEOUT) return DGT_ERROR_TIMEOUT;
+    return DGT_ERROR_INVALID_VALUE;  // a device-side bounds check failed
 }

@@ -169,12 +169,8 @@ static dgt_status sgemm_split(dgt_context* h, bool ta, bool tb, int64_t m, int64
         !oz::make_plane_map(&tmB, planesB, (int64_t)planes * n_pad, k_pad * 2, oz::TN, 128))
         return fail(h, DGT_ERROR_CUDA, "cuTensorMapEncodeTiled failed");
     using CF = oz::OzCfg<4, 128, 4>;
-    static bool attr = false;
-    if (!attr) {
-        DGT_CUDA_TRY(h, cudaFuncSetAttribute(oz::digit_gemm<CF, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)CF::SMEM));
-        attr = true;
-    }
+    const cudaError_t opt = smem_opt_in<oz::digit_gemm<CF, 1, 1>>((int)CF::SMEM);
+    DGT_CUDA_TRY(h, opt);
     static thread_local oz::Params prm;  // ~21 KB: keep it off the stack
     prm = oz::Params{};
     prm.m = m;
@@ -188,6 +184,7 @@ static dgt_status sgemm_split(dgt_context* h, bool ta, bool tb, int64_t m, int64
     std::copy(segs.begin(), segs.end(), prm.segs);
     std::copy(groups.begin(), groups.end(), prm.groups);
     prm.err = h->dev_error;
+    prm.test_stall = h->test_stall;
     prm.Cf = C;
     prm.alpha_f = alpha;
     prm.beta_f = beta;

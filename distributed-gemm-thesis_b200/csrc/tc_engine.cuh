@@ -78,6 +78,11 @@ struct Params {
     // grouped mode: per-problem descriptors in device memory, tiles numbered problem by problem
     const struct GProb* gprobs;
     int32_t nprob, total_tiles;
+    // Failure-path test hook (DGT_TUNE_TEST_STALL): nonzero makes every CTA's producer
+    // withhold the operand loads of its first pipeline stage, a barrier phase nothing
+    // completes, so the MMA issuer's first wait runs out of its budget.  No load or MMA is in
+    // flight for that stage, so the abort path drains and returns as on a real stall.
+    int32_t test_stall;
 };
 constexpr int MAX_SEGS = 640, MAX_GROUPS = 640;
 
@@ -448,6 +453,10 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                                 ok = false;
                                 break;
                             }
+                            if (P.test_stall && it == 0) {  // withheld: stage 0 never fills
+                                ++it;
+                                continue;
+                            }
                             if constexpr (PAIR) {
                                 const uint32_t lbar = map_to_rank(full(s), 0);
                                 if (leader) mbar_expect_tx(full(s), 2 * (A_STAGE + B_STAGE));
@@ -468,6 +477,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
             // drain: wait for this CTA's own loads still in flight (bounded)
             if (!ok && leader) {
                 for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
+                    if (P.test_stall && j == 0) continue;  // the withheld stage has nothing in flight
                     long long t0 = clock64();
                     while (!mbar_try(full(j % STAGES), (j / STAGES) & 1) && clock64() - t0 < WAIT_BUDGET) {
                     }

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libdgt.so")
 SUCCESS, INVALID_VALUE, UNSUPPORTED, CUDA_ERROR, TIMEOUT, ALLOC, NOT_INITIALIZED = range(7)
 FP64_NATIVE, FP64_OZAKI_INT8, FP64_OZAKI_BF16, FP64_AUTO, FP64_OZAKI2_INT8 = range(5)
 FP32_SIMT, FP32_BF16X1, FP32_BF16X3 = range(3)
-TUNE_DMMA_VARIANT, TUNE_OZAKI_SLICES, TUNE_PROFILE, TUNE_OZAKI_VARIANT = range(4)
+TUNE_DMMA_VARIANT, TUNE_OZAKI_SLICES, TUNE_PROFILE, TUNE_OZAKI_VARIANT, TUNE_TEST_STALL = range(5)
 
 _c_i64 = ctypes.c_int64
 _c_i32 = ctypes.c_int32
@@ -117,6 +117,7 @@ SIGNATURES = [
     ("dgt_launch_count", _c_i64, [_vp]),
     ("dgt_dgemm_ozaki_static", _c_i32, [_vp, ctypes.c_char, ctypes.c_char, _c_i64, _c_i64, _c_i64, _dp, _vp, _c_i64,
                                          _vp, _c_i64, _dp, _vp, _c_i64, _c_i32]),
+    ("dgt_ozaki_static_check", _c_i32, [_vp]),
 ]
 
 _lib = None

@@ -602,3 +602,149 @@ def pre_distributed_cannon25_nccl(p, c, M, runs, alpha=1.0, beta=0.0, logging=Tr
     finally:
         if log is not None:
             log.close()
+
+
+# ---- benchmark of the physical step loop --------------------------------------------------------
+
+class DeviceClock:
+    """Device time of a region on torch's current stream (the stream the library's kernels
+    and, ordered against it, NCCL's run on): CUDA events, synchronized on both sides."""
+
+    def start(self) -> None:
+        import torch
+
+        torch.cuda.synchronize()
+        self.e0, self.e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        self.e0.record()
+
+    def stop(self) -> float:
+        import torch
+
+        self.e1.record()
+        torch.cuda.synchronize()
+        return self.e0.elapsed_time(self.e1)
+
+
+class HostClock:
+    """Wall time of a region (the host doubles' clock)."""
+
+    def start(self) -> None:
+        import time
+
+        self.t0 = time.perf_counter()
+
+    def stop(self) -> float:
+        import time
+
+        return (time.perf_counter() - self.t0) * 1e3
+
+
+def _max_over_ranks(x: float) -> float:
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def summa_benchmark(M: int, N: int, K: int, mb: int, nb: int, kb: int, steps: int = 3, warmup: int = 1,
+                    alpha: float = 1.0, beta: float = 0.0, ops=None, ipc=None, handle=None, clock=None,
+                    device: str = "cuda", seed: int = 0) -> dict:
+    """Times the physical SUMMA step loop on this process group: the world's p x q grid is the
+    reference's most-square factorisation (calculateVirtualDeviceGrid,
+    src/Decompositions/2DBlockSequentialDecomposition.cpp:27-54), every rank fills its
+    block-cyclic locals of A, B and C from its own seeded generator, and two forms run the
+    same product:
+
+      * collective -- DistSumma: panels broadcast on the process-row / -column sub-groups
+        (NCCL on B200), one panel of lookahead, the local GEMMs through the C ABI;
+      * fused      -- PeerSumma: every rank's dgt_summa_rank reads the owners' panels from
+        their memory (CUDA IPC, plain loads), no broadcast.
+
+    Each form: `warmup` untimed multiplies, then `steps` timed ones between barriers; the time
+    is the maximum over ranks.  The compute reference is the same rank's m x n x K product as
+    one local GEMM with no communication (dense local operands), so exposed communication =
+    form time - compute time.  Returns a dict with, per form, ms per multiply, whole-job
+    TFLOP/s (2 M N K / time), the compute reference and the exposed communication, plus the
+    fused result's relative Frobenius distance from the collective one on this rank (max over
+    ranks; the two differ only in summation order).  `ops`, `ipc`, `handle` and `clock` take
+    the host doubles on CPU; on a GPU they default to the library (DgtOps, DeviceIpc,
+    dgt.Handle on torch's current stream) and CUDA events."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size()
+    rank = dist.get_rank()
+    p, q = dgt.block2d_grid(world)
+    clock = clock or DeviceClock()
+    own_handle = device == "cuda" and handle is None
+    if own_handle:
+        handle = dgt.Handle(stream=torch.cuda.current_stream().cuda_stream)
+    try:
+        return _summa_benchmark(M, N, K, mb, nb, kb, steps, warmup, alpha, beta, ops or DgtOps(handle), ipc, handle,
+                                clock, device, seed, world, rank, p, q)
+    finally:
+        if own_handle:
+            handle.close()
+
+
+def _summa_benchmark(M, N, K, mb, nb, kb, steps, warmup, alpha, beta, ops, ipc, handle, clock, device, seed, world,
+                     rank, p, q):
+    import torch
+    import torch.distributed as dist
+
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed * 1000 + rank)
+
+    def rand(shape):
+        return torch.rand(shape, dtype=torch.float64, device=device, generator=gen) * 2 - 1
+
+    def timed(fn) -> float:
+        for _ in range(warmup):
+            fn()
+        dist.barrier()
+        clock.start()
+        for _ in range(steps):
+            fn()
+        ms = clock.stop() / max(steps, 1)
+        dist.barrier()
+        return _max_over_ranks(ms)
+
+    S = DistSumma(p, q, mb, nb, kb, ops=ops)
+    (ma, ka), (kr, nc), (m, n) = S.local_shapes(M, N, K)
+    A_loc, B_loc = rand((max(ka, 1), max(ma, 1))), rand((max(nc, 1), max(kr, 1)))
+    C0 = rand((max(n, 1), max(m, 1)))
+    C_coll = C0.clone()
+    # both forms run warmup + steps multiplies from the same C0, so their results compare
+    coll_ms = timed(lambda: S.multiply(M, N, K, alpha, A_loc, B_loc, beta, C_coll))
+
+    # compute reference: this rank's m x n x K as one local GEMM on dense local operands
+    if m > 0 and n > 0 and K > 0:
+        A_full, B_full, C_full = rand((K, m)), rand((n, K)), C0.clone()
+        comp_ms = timed(lambda: ops.gemm(m, n, K, alpha, A_full, m, B_full, K, beta, C_full, m))
+        del A_full, B_full, C_full
+    else:
+        comp_ms = timed(lambda: None)
+
+    P = PeerSumma(p, q, mb, nb, kb, M, N, K, ipc=ipc, handle=handle)
+    try:
+        P.A_loc.copy_(A_loc)
+        P.B_loc.copy_(B_loc)
+        C_fused = C0.clone()
+        fused_ms = timed(lambda: P.multiply(alpha, beta, C_fused))
+        if device == "cuda":
+            torch.cuda.synchronize()
+        den = float(torch.linalg.norm(C_coll)) or 1.0
+        diff = _max_over_ranks(float(torch.linalg.norm(C_fused - C_coll)) / den)
+    finally:
+        P.close()
+    flops = 2.0 * M * N * K
+
+    def form(ms):
+        return {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12 if ms > 0 else 0.0, "compute_ms": comp_ms,
+                "exposed_comm_ms": max(ms - comp_ms, 0.0)}
+
+    return {"grid": [p, q], "M": M, "N": N, "K": K, "blocks": [mb, nb, kb], "ranks": world,
+            "collective": form(coll_ms), "fused": form(fused_ms), "fused_vs_collective_rel": diff}

@@ -74,6 +74,8 @@ class _Orc:
         L.orc_dgemm_dd_sample.argtypes = [ctypes.c_char, ctypes.c_char, ctypes.c_int64, ctypes.c_double, _dp,
                                           ctypes.c_int64, _dp, ctypes.c_int64, ctypes.c_double, _dp, ctypes.c_int64,
                                           ctypes.c_int64, _i64p, _i64p, _dp]
+        L.orc_dd_rows.argtypes = [ctypes.c_int64, ctypes.c_int64, _dp, ctypes.c_int64, ctypes.c_int64, _dp,
+                                  ctypes.c_int64, ctypes.c_double, _dp, ctypes.c_int64, ctypes.c_int]
 
     # -- block-cyclic --------------------------------------------------------------
     def numroc(self, n, nb, iproc, isrproc, nprocs):
@@ -187,6 +189,19 @@ class _Orc:
         self.L.orc_dgemm_dd_sample(ta.encode(), tb.encode(), K, alpha, _ptr(A), A.shape[0], _ptr(B), B.shape[0],
                                    beta, C0p, ldc, len(rows), rows.ctypes.data_as(_i64p),
                                    cols.ctypes.data_as(_i64p), _ptr(out))
+        return out
+
+
+    def dd_rows(self, A_rows, B, alpha=1.0, threads=0):
+        """alpha * A_rows @ B in double-double (TwoSum / TwoProduct), rounded once to double:
+        the exact product of a few sampled rows (A_rows: r x K) with all of B (K x n), on
+        `threads` host threads (0: every online core)."""
+        At = np.ascontiguousarray(A_rows, dtype=np.float64)  # row s K-contiguous at At[s]
+        B = np.asfortranarray(B, dtype=np.float64)
+        r, K = At.shape
+        n = B.shape[1]
+        out = np.zeros((r, n), order="F")
+        self.L.orc_dd_rows(K, r, _ptr(At), K, n, _ptr(B), B.shape[0], alpha, _ptr(out), r, int(threads))
         return out
 
 
@@ -308,10 +323,18 @@ class _Ref:
         self._check(self.L.ref_cannon_reorder(M, p, c, _ptr(C), _ptr_array(tiles)))
         return C
 
-    def cannon_fulloffload(self, A, B, C, p, c, alpha, beta):
+    def cannon_fulloffload(self, A, B, C, p, c, alpha, beta, in_place=False):
+        """The reference's decompose2D -> multiply -> reorderMatrix on host matrices.  A and B
+        are read where they lie when they are column-major doubles already; C is updated in
+        place when in_place is set (C must then be a column-major double array), else a copy
+        is updated and returned."""
         M = A.shape[0]
-        A, B = (np.array(x, dtype=np.float64, order="F") for x in (A, B))
-        C = np.array(C, dtype=np.float64, order="F")
+        A, B = (np.asfortranarray(x, dtype=np.float64) for x in (A, B))
+        if in_place:
+            if not (C.flags.f_contiguous and C.dtype == np.float64):
+                raise ValueError("in_place needs a column-major float64 C")
+        else:
+            C = np.array(C, dtype=np.float64, order="F")
         self._check(self.L.ref_cannon_fulloffload(M, p, c, alpha, beta, _ptr(A), _ptr(B), _ptr(C)))
         return C
 
@@ -440,6 +463,33 @@ OZAKI2_MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                  223, 217, 211, 199, 197, 193, 191, 181, 179, 173)
 
 
+def ozaki2_split_residues(y, p: int):
+    """The kernels' integer residue split (csrc/crt.cuh ModTable, csrc/ozaki2.cu
+    residue_block) restated in numpy: y = a 2^s as float64 (|y| < 2^78), returned as the int8
+    symmetric residues of rn(y) modulo p.  Steps: yh = rint(y 2^-40), yl = rint(y - yh 2^40)
+    (both exact), 20-bit chunks x0..x3, t = x3 c60 + x2 c40 + x1 c20 + x0 with symmetric
+    constants, then the quotient of t + floor(p/2) + 2^21 p by p from one multiply by
+    floor(2^38/p) + 1 and a shift, and the low byte of t minus quotient times p."""
+    y = np.asarray(y, dtype=np.float64)
+    yh = np.rint(y * 2.0 ** -40)
+    hi = yh.astype(np.int64)
+    lo = np.rint(y - yh * 2.0 ** 40).astype(np.int64)  # exact in float64 (|y - yh 2^40| <= 2^39)
+    x0, x1 = lo & 0xFFFFF, lo >> 20
+    x2, x3 = hi & 0xFFFFF, hi >> 20
+
+    def sym(v):
+        return v - p if v > p // 2 else v
+
+    c20, c40, c60 = sym(2 ** 20 % p), sym(2 ** 40 % p), sym(2 ** 60 % p)
+    t = x3 * c60 + x2 * c40 + x1 * c20 + x0
+    assert np.all(np.abs(t) < 2 ** 28)
+    magic = (1 << 38) // p + 1
+    bias = (p // 2 + (p << 21)) * magic
+    q = ((t * magic + bias) >> 38).astype(np.int64)
+    r = t - q * p
+    return (r & 0xFF).astype(np.uint8).view(np.int8)
+
+
 def ozaki2_sigmas(nmod: int, k: int):
     """(sigma_A, sigma_B) for nmod moduli and inner dimension k: s = sigma_A + sigma_B is the
     largest with (2^ceil(s/2) + sqrt(k)/2)(2^floor(s/2) + sqrt(k)/2) < (P/2)(1 - 2^-20), checked
@@ -463,9 +513,9 @@ def ozaki2_sigmas(nmod: int, k: int):
 
 def _row_scale(v, sigma: int):
     """Scale exponent s of one row of op(A) (sigma = sigma_A) or column of op(B) (sigma_B):
-    s = min(sigma - g, 58 - e), e the exponent of
-    max |v| and 2^g >= the integer bound of ||v||_2, q = sum ceil(|v| 2^(20-e))^2
-    (csrc/ozaki2.cu qnorm_* and row_scale_exp).  None for a row with inf or NaN."""
+    s = sigma - g, where 2^g >= the integer bound of ||v||_2 from q = sum ceil(|v| 2^(20-e))^2,
+    e the exponent of max |v| (csrc/ozaki2.cu qnorm_* and row_scale_exp).  No entry cap: the
+    scaled row's 2-norm is at most 2^sigma + sqrt(k)/2.  None for a row with inf or NaN."""
     import math
 
     vals = [abs(float(x)) for x in v]
@@ -477,13 +527,13 @@ def _row_scale(v, sigma: int):
     e = math.frexp(mx)[1]
     q = sum(math.ceil(math.ldexp(x, 20 - e)) ** 2 for x in vals)
     h = ((q - 1).bit_length() + 1) // 2
-    return min(sigma - (e - 20 + h), 58 - e)
+    return sigma - (e - 20 + h)
 
 
 def ozaki2_exact(A, B, nmod: int, ta: str = "N", tb: str = "N"):
     """C = op(A) op(B) as the CRT emulation computes it: each row of op(A) / column of op(B)
-    scaled by 2^s (its 2-norm bound, capped so no entry exceeds 2^58) and rounded to
-    integers (nearest even), their integer product taken exactly, rounded once to FP64 and
+    scaled by 2^s (so that its 2-norm is at most 2^sigma) and rounded to integers (nearest
+    even), their integer product taken exactly, rounded once to FP64 and
     scaled back by 2^-(s_i + t_j).  Pure Python integers: small sizes only."""
     import math
 
@@ -524,7 +574,9 @@ def ozaki2_residue_check(A, B, nmod: int):
                    for i in range(m)], dtype=object)
     Bi = np.array([[int(round(math.ldexp(float(B[t, j]), sb[j]))) for j in range(n)]
                    for t in range(k)], dtype=object)
-    assert all(abs(x) <= 2 ** 58 for x in Ai.flat) and all(abs(x) <= 2 ** 58 for x in Bi.flat)
+    # the kernels' integer split takes |x| < 2^78 (every entry is below its row's norm bound)
+    assert all(abs(x) <= 2 ** sig_a + math.isqrt(k) for x in Ai.flat)
+    assert all(abs(x) <= 2 ** sig_b + math.isqrt(k) for x in Bi.flat)
 
     def sym(x, p):
         r = x % p

@@ -4,7 +4,11 @@
  * cited loops so that tests can check the CUDA product against it bit for bit, and
  * the restatement itself against the reference's own code (oracle/_ref).
  */
+#define _DEFAULT_SOURCE /* sysconf(_SC_NPROCESSORS_ONLN) under -std=c11 */
 #include "orc.h"
+
+#include <pthread.h>
+#include <unistd.h>
 
 #include <math.h>
 #include <string.h>
@@ -318,4 +322,65 @@ void orc_dgemm_dd_sample(char ta, char tb, int64_t K, double alpha, const double
         if (beta != 0.0 && C0) r = dd_add_prod(r, beta, C0[i + j * ldc]);
         out[s] = r.hi + r.lo;
     }
+}
+
+/* Sampled rows of alpha*op(A)*B in double-double, for the whole width of B: row s of op(A)
+ * is At[0..K) + s*ldat (K-contiguous), column j of B is B + j*ldb, and the result (rounded
+ * once to double) goes to out[s + j*ldo].  Columns are split across nthreads POSIX threads
+ * (<= 0: one per online core); each thread carries four rows' accumulators at once so the
+ * dependent TwoSum chains overlap. */
+typedef struct {
+    int64_t K, nrows, ldat, ldb, ldo, j0, j1;
+    const double *At, *B;
+    double alpha, *out;
+} dd_rows_job;
+
+static void* dd_rows_worker(void* arg) {
+    const dd_rows_job* J = (const dd_rows_job*)arg;
+    for (int64_t j = J->j0; j < J->j1; ++j) {
+        const double* b = J->B + j * J->ldb;
+        for (int64_t s = 0; s < J->nrows; s += 4) {
+            const int64_t nr = J->nrows - s < 4 ? J->nrows - s : 4;
+            dd acc[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+            const double* a[4];
+            for (int r = 0; r < 4; ++r) a[r] = J->At + (s + (r < nr ? r : 0)) * J->ldat;
+            for (int64_t p = 0; p < J->K; ++p) {
+                const double bp = b[p];
+                for (int r = 0; r < 4; ++r) acc[r] = dd_add_prod(acc[r], a[r][p], bp);
+            }
+            for (int r = 0; r < nr; ++r) {
+                double h = J->alpha * acc[r].hi;
+                double he = fma(J->alpha, acc[r].hi, -h);
+                dd v = two_sum(h, he + J->alpha * acc[r].lo);
+                J->out[(s + r) + j * J->ldo] = v.hi + v.lo;
+            }
+        }
+    }
+    return NULL;
+}
+
+void orc_dd_rows(int64_t K, int64_t nrows, const double* At, int64_t ldat, int64_t ncols, const double* B,
+                 int64_t ldb, double alpha, double* out, int64_t ldo, int nthreads) {
+    if (nthreads <= 0) {
+        long c = sysconf(_SC_NPROCESSORS_ONLN);
+        nthreads = c > 0 ? (int)c : 1;
+    }
+    if (nthreads > 256) nthreads = 256;
+    if (nthreads > ncols) nthreads = ncols > 0 ? (int)ncols : 1;
+    pthread_t tid[256];
+    dd_rows_job jobs[256];
+    for (int t = 0; t < nthreads; ++t) {
+        dd_rows_job J = {K, nrows, ldat, ldb, ldo, ncols * t / nthreads, ncols * (t + 1) / nthreads, At, B, alpha, out};
+        jobs[t] = J;
+    }
+    int started = 0;
+    for (int t = 1; t < nthreads; ++t)
+        if (pthread_create(&tid[t], NULL, dd_rows_worker, &jobs[t]) == 0)
+            started = t;
+        else
+            break;
+    /* threads that could not start run here, after this thread's own share */
+    dd_rows_worker(&jobs[0]);
+    for (int t = started + 1; t < nthreads; ++t) dd_rows_worker(&jobs[t]);
+    for (int t = 1; t <= started; ++t) pthread_join(tid[t], NULL);
 }

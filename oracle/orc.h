@@ -70,6 +70,12 @@ void orc_dgemm_dd_sample(char ta, char tb, int64_t K, double alpha, const double
                          int64_t ldb, double beta, const double* C0, int64_t ldc, int64_t n, const int64_t* rows,
                          const int64_t* cols, double* out);
 
+/* Sampled rows of alpha*op(A)*B in double-double over every column of B (the exact-product
+ * yardstick of the FP64 emulation's error): At holds the rows K-contiguously (row s at
+ * At + s*ldat), out[s + j*ldo]; work split over nthreads threads (<= 0: all online cores). */
+void orc_dd_rows(int64_t K, int64_t nrows, const double* At, int64_t ldat, int64_t ncols, const double* B,
+                 int64_t ldb, double alpha, double* out, int64_t ldo, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

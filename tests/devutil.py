@@ -173,3 +173,28 @@ class CannonHandle:
         c = self._mat(C, elems, 1, elems)
         for part in parts:
             c += self._mat(part, elems, 1, elems)
+
+
+class ScheduleHandle:
+    """dgt.Handle.summa_rank executed on host addresses: the segments dgt_summa_schedule
+    returns, each a rank-local GEMM reading the owners' memory."""
+
+    @staticmethod
+    def _mat(addr, rows, cols, ld):
+        n = ld * (cols - 1) + rows if rows and cols else 1
+        buf = np.frombuffer((ctypes.c_double * n).from_address(addr), dtype=np.float64)
+        return np.lib.stride_tricks.as_strided(buf, shape=(rows, cols), strides=(8, 8 * ld))
+
+    def summa_rank(self, rank, p, q, mb, nb, kb, M, N, K, alpha, A_ptrs, lldA, B_ptrs, lldB, beta, C, ldc,
+                   mode=None, slices=7):
+        import dgt
+
+        m, n = dgt.numroc(M, mb, rank // q, 0, p), dgt.numroc(N, nb, rank % q, 0, q)
+        if m == 0 or n == 0:
+            return
+        c = self._mat(C, m, n, ldc)
+        first = True
+        for a, b, lda, ldb, k in dgt.summa_schedule(rank, p, q, mb, nb, kb, M, N, K, A_ptrs, lldA, B_ptrs, lldB):
+            prod = self._mat(a, m, k, lda) @ self._mat(b, k, n, ldb) if k else 0.0
+            c[...] = alpha * prod + (beta if first else 1.0) * c
+            first = False

@@ -53,9 +53,11 @@ def test_block_cyclic_shapes(h, case):
     _cyclic_roundtrip(h, *case, seed=5)
 
 
-def test_block_cyclic_config2_full_size(h):
-    """15000 x 9000 (A of config 2) on a 4 x 4 grid, block 256: bit-exact vs the oracle."""
-    _cyclic_roundtrip(h, 15000, 9000, 256, 256, 4, 4, seed=42)
+@pytest.mark.parametrize("name,M,N", [("A", 15000, 9000), ("B", 9000, 17000), ("C", 15000, 17000)])
+def test_block_cyclic_config2_full_size(h, name, M, N):
+    """All three matrices of the ragged SUMMA configuration (M = 15000, N = 17000, K = 9000) on
+    a 4 x 4 grid with 256 blocks, packed and unpacked at full size: bit-exact vs the oracle."""
+    _cyclic_roundtrip(h, M, N, 256, 256, 4, 4, seed={"A": 42, "B": 43, "C": 44}[name])
 
 
 def test_block_cyclic_rejects_bad_lld(h):

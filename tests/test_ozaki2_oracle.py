@@ -31,19 +31,44 @@ def test_norm_rule():
     assert all(math.gcd(p, q) == 1 for i, p in enumerate(O.OZAKI2_MODULI) for q in O.OZAKI2_MODULI[:i])
 
 
-def test_row_scale_caps_entries():
-    """A row with one large entry among small ones: the norm bound is the max itself, so the
-    58-bit entry cap decides; a dense row of equal entries is scaled by its norm."""
+def test_row_scale_has_no_entry_cap():
+    """A row with one large entry among small ones: its norm bound is the max itself, so the
+    scaled entry reaches 2^sigma, beyond the FP64 mantissa (an integer already) while the
+    small entries keep their bits down to 2^0; a dense row of equal entries is scaled by its
+    norm."""
     k = 64
-    single = np.zeros(k)
+    single = np.full(k, 2.0 ** -30)
     single[5] = 0.75
-    s1 = O._row_scale(single, O.ozaki2_sigmas(20, k)[0])
-    assert abs(int(round(math.ldexp(0.75, s1)))) <= 2 ** 58 and s1 == 58  # e = 0: cap 58 - e
+    sg = O.ozaki2_sigmas(20, k)[0]
+    s1 = O._row_scale(single, sg)
+    big = abs(int(round(math.ldexp(0.75, s1))))
+    assert 2 ** 76 <= big <= 2 ** sg and s1 == sg  # g = 0: 2^0 bounds the norm (about 0.75)
+    assert int(round(math.ldexp(2.0 ** -30, s1))) == 2 ** (s1 - 30)  # small entries stay exact
     dense = np.full(k, 0.75)
     sg = O.ozaki2_sigmas(12, k)[0]
     s2 = O._row_scale(dense, sg)
     norm = math.sqrt(sum(math.ldexp(0.75, s2) ** 2 for _ in range(k)))
     assert norm <= 2 ** sg < 2 * norm * 2  # within a factor 2 of the bound (power-of-two scales)
+
+
+def test_residue_split_arithmetic():
+    """The kernels' integer split (ozaki2_split_residues, a restatement of its steps) gives the
+    symmetric residue of rn(y) for every modulus: at the range edges (|y| up to 2^78, ties at
+    .5, values next to 2^40 multiples) and on random magnitudes from 2^-3 to 2^78."""
+    rng = np.random.default_rng(5)
+    edges = []
+    for e in (0, 1, 19, 20, 39, 40, 41, 52, 53, 59, 60, 61, 77):
+        for d in (-1.0, -0.5, 0.0, 0.5, 1.0):
+            edges += [2.0 ** e + d, -(2.0 ** e + d)]
+    edges += [2.0 ** 78 - 2.0 ** 25, -(2.0 ** 78 - 2.0 ** 25), 0.5, -0.5, 1.5, -1.5, 2.5, -2.5, 0.0]
+    mags = np.ldexp(rng.random(20000) + 0.5, rng.integers(-3, 78, 20000))
+    y = np.concatenate([np.array(edges), mags * np.where(rng.random(20000) < 0.5, -1.0, 1.0)])
+    assert np.all(np.abs(y) < 2.0 ** 78)
+    exact = [int(round(float(v))) for v in y]  # rn, ties to even
+    for p in O.OZAKI2_MODULI:
+        got = O.ozaki2_split_residues(y, p)
+        want = [((x + p // 2) % p) - p // 2 for x in exact]
+        assert got.tolist() == want, p
 
 
 def _exact_max_scaled(A, B, nmod):
@@ -52,7 +77,7 @@ def _exact_max_scaled(A, B, nmod):
     m, k = A.shape
     n = B.shape[1]
     lg = sum(math.log2(p) for p in O.OZAKI2_MODULI[:nmod])
-    beta = min(58, math.floor((lg - 1 - math.log2(k)) / 2 - 1e-9))
+    beta = math.floor((lg - 1 - math.log2(k)) / 2 - 1e-9)
     ea = [math.frexp(float(np.max(np.abs(A[i]))))[1] for i in range(m)]
     fb = [math.frexp(float(np.max(np.abs(B[:, j]))))[1] for j in range(n)]
     Ai = [[int(round(math.ldexp(float(A[i, t]), beta - ea[i]))) for t in range(k)] for i in range(m)]

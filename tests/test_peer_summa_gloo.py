@@ -5,14 +5,13 @@ each rank -- the segment list dgt_summa_rank's kernel walks.  So the test exerci
 whole host side of the fused path across real processes: buffer sizes, handle exchange,
 the peer pointer arrays, the barriers, and each rank reading its panels straight out of the
 owners' memory.  The gathered C must equal the host FP64 GEMM within 1e-13."""
-import ctypes
 import os
 import socket
 import sys
 
 import numpy as np
 import pytest
-from devutil import ShmIpc, free_port
+from devutil import ScheduleHandle, ShmIpc, free_port
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CASES = [  # (p, q, mb, nb, kb, M, N, K, alpha, beta)
@@ -21,31 +20,6 @@ CASES = [  # (p, q, mb, nb, kb, M, N, K, alpha, beta)
     (4, 1, 16, 32, 12, 40, 50, 61, -2.0, 1.0),  # process row 3 owns no rows of A or C
     (2, 2, 16, 16, 16, 48, 40, 0, 1.0, 0.25),   # K = 0: C = beta C
 ]
-
-
-class ScheduleHandle:
-    """dgt.Handle.summa_rank executed on host addresses: the segments dgt_summa_schedule
-    returns, each a rank-local GEMM reading the owners' memory."""
-
-    @staticmethod
-    def _mat(addr, rows, cols, ld):
-        n = ld * (cols - 1) + rows if rows and cols else 1
-        buf = np.frombuffer((ctypes.c_double * n).from_address(addr), dtype=np.float64)
-        return np.lib.stride_tricks.as_strided(buf, shape=(rows, cols), strides=(8, 8 * ld))
-
-    def summa_rank(self, rank, p, q, mb, nb, kb, M, N, K, alpha, A_ptrs, lldA, B_ptrs, lldB, beta, C, ldc,
-                   mode=None, slices=7):
-        import dgt
-
-        m, n = dgt.numroc(M, mb, rank // q, 0, p), dgt.numroc(N, nb, rank % q, 0, q)
-        if m == 0 or n == 0:
-            return
-        c = self._mat(C, m, n, ldc)
-        first = True
-        for a, b, lda, ldb, k in dgt.summa_schedule(rank, p, q, mb, nb, kb, M, N, K, A_ptrs, lldA, B_ptrs, lldB):
-            prod = self._mat(a, m, k, lda) @ self._mat(b, k, n, ldb) if k else 0.0
-            c[...] = alpha * prod + (beta if first else 1.0) * c
-            first = False
 
 
 def _rank_main(rank, world, port, out):

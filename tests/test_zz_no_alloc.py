@@ -1,11 +1,12 @@
 """dgt_dgemm_ozaki_static: the FP64-accurate (INT8 Ozaki) GEMM for callers that cannot
 allocate device memory when they multiply (under a foreign allocator that owns the device
-memory, in allocation-free real-time loops).  Its scratch is
-a fixed 64 MiB device array inside the library.  Checked through the C ABI against the
-handle-based entry point (dgt_dgemm_ex, same slice count) on two calls in a row, so the
-second call runs on scratch the first one left behind; the tolerance is the one the Ozaki
-tests use (relative Frobenius <= 1e-13).  Collected after the rest of the validated GPU
-suite, before the tests of the newest entries."""
+memory, in allocation-free real-time loops).  Its scratch is a fixed 64 MiB device array
+inside the library.  Checked through the C ABI against the handle-based entry point
+(dgt_dgemm_ex, same slice count) on calls in a row, so each later call runs on scratch an
+earlier, larger one left behind; the tolerance is the one the Ozaki tests use (relative
+Frobenius <= 1e-13).  Both operand layouts are covered (op(A) K-contiguous with 'T'), with
+odd sizes.  After the calls, dgt_ozaki_static_check reads the sticky device error word:
+clean.  This file is collected last of the GPU suite."""
 import ctypes
 
 import numpy as np
@@ -26,6 +27,14 @@ def _entry():
     fn.argtypes = [ctypes.c_void_p, ctypes.c_char, ctypes.c_char, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                    ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
                    ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int]
+    return fn
+
+
+def _check_entry():
+    lib = dgt.load()
+    fn = lib.dgt_ozaki_static_check
+    fn.restype = ctypes.c_int32
+    fn.argtypes = [ctypes.c_void_p]
     return fn
 
 
@@ -50,11 +59,32 @@ def _case(fn, h, ta, tb, m, n, k, alpha, beta, S, seed):
     assert O.rel_errors(got, O.dgemm(A, B, alpha, beta, C, ta, tb))[1] <= TOL
 
 
-def test_static_scratch_matches_handle_entry_twice():
-    fn = _entry()
+def test_static_scratch_matches_handle_entry_in_a_row():
+    import torch
+
+    fn, check = _entry(), _check_entry()
     with dgt.Handle() as h:
         _case(fn, h, "N", "T", 300, 200, 100, 1.5, -0.5, 7, 11)
         _case(fn, h, "N", "N", 256, 513, 640, 1.0, 0.0, 8, 21)
+        _case(fn, h, "T", "N", 129, 77, 301, -0.75, 0.25, 7, 31)  # smaller, on the larger call's leftovers
+        _case(fn, h, "T", "T", 65, 143, 97, 1.0, 2.0, 8, 41)
+    assert check(torch.cuda.current_stream().cuda_stream) == dgt.SUCCESS
+
+
+def test_static_k_zero_scales_c():
+    import torch
+
+    fn = _entry()
+    m, n = 37, 21
+    C = O.uniform((m, n), 51)
+    dC = dev(C)
+    a, b = ctypes.c_double(1.0), ctypes.c_double(-0.5)
+    x = torch.zeros(1, dtype=torch.float64, device="cuda")
+    st = fn(torch.cuda.current_stream().cuda_stream, b"N", b"N", m, n, 0, ctypes.byref(a), ptr(x), m, ptr(x), 1,
+            ctypes.byref(b), ptr(dC), m, 7)
+    assert st == dgt.SUCCESS
+    torch.cuda.synchronize()
+    assert np.array_equal(host(dC, (m, n)), -0.5 * C)
 
 
 def test_static_scratch_rejects_oversize():
