@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "dgt_internal.cuh"
+#include "tc_engine.cuh"
 
 namespace dgt {
 namespace {
@@ -188,13 +189,143 @@ __device__ __forceinline__ int find_problem(const Problem* P, int nprob, int til
     return lo;
 }
 
+// One BK-deep k-tile of the CTA tile from shared memory: every warp multiplies its 64 x 32
+// (or 32 x 32) block with DMMA fragments read from the stage (layouts as in load_tile).
+template <class CF>
+__device__ __forceinline__ void mma_ktile(const double* __restrict__ a, const double* __restrict__ b, bool a_mn,
+                                          bool b_mn, double (&acc)[CF::MT][4][4], int wm, int wn, int g, int t) {
+    constexpr int BK = CF::BK, LD_K = CF::LD_K, LD_KB = CF::LD_KB, LDMN = CF::LDMN;
+    constexpr int MMAK = CF::MMAK, MT = CF::MT, WTM = MT * 16;
+    constexpr bool PERM = CF::PERM;
+    if constexpr (PERM) {
+        // physical k of fragment element h (logical k = t + 4h), see Cfg
+        auto kp = [&](int h) { return 8 * (h >> 1) + 2 * t + (h & 1); };
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += MMAK) {
+            double bf[4][MMAK / 4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int n = wn * 32 + j * 8 + g;
+                if (b_mn) {
+#pragma unroll
+                    for (int h = 0; h < MMAK / 4; ++h) bf[j][h] = b[(kk + kp(h)) * LDMN + n];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < MMAK / 8; ++q) {
+                        const double2 v = *reinterpret_cast<const double2*>(b + n * LD_KB + kk + 8 * q + 2 * t);
+                        bf[j][2 * q] = v.x;
+                        bf[j][2 * q + 1] = v.y;
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < MT; ++i) {
+                const int mr = wm * WTM + i * 16 + 2 * g;  // physical rows of MMA rows g, g + 8
+                double af[MMAK / 2];
+                if (a_mn) {
+#pragma unroll
+                    for (int h = 0; h < MMAK / 4; ++h) {
+                        const double2 v = *reinterpret_cast<const double2*>(a + (kk + kp(h)) * LDMN + mr);
+                        af[2 * h] = v.x;
+                        af[2 * h + 1] = v.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < MMAK / 8; ++q) {
+                        const double2 v0 = *reinterpret_cast<const double2*>(a + mr * LD_K + kk + 8 * q + 2 * t);
+                        const double2 v1 =
+                            *reinterpret_cast<const double2*>(a + (mr + 1) * LD_K + kk + 8 * q + 2 * t);
+                        af[4 * q] = v0.x;
+                        af[4 * q + 1] = v1.x;
+                        af[4 * q + 2] = v0.y;
+                        af[4 * q + 3] = v1.y;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if constexpr (MMAK == 8)
+                        dmma_16x8x8(acc[i][j], af, bf[j]);
+                    else
+                        dmma_16x8x16(acc[i][j], af, bf[j]);
+                }
+            }
+        }
+    } else {
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += MMAK) {
+        // B fragments of the warp's four n8 tiles, then one m16 tile of A at a time
+        double bf[4][MMAK / 4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = wn * 32 + j * 8 + g;
+#pragma unroll
+            for (int h = 0; h < MMAK / 4; ++h)
+                bf[j][h] = b_mn ? b[(kk + t + 4 * h) * LDMN + n] : b[n * LD_KB + kk + t + 4 * h];
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i) {
+            const int m = wm * WTM + i * 16 + g;
+            double af[MMAK / 2];
+#pragma unroll
+            for (int h = 0; h < MMAK / 4; ++h) {
+                if (a_mn) {
+                    af[2 * h] = a[(kk + t + 4 * h) * LDMN + m];
+                    af[2 * h + 1] = a[(kk + t + 4 * h) * LDMN + m + 8];
+                } else {
+                    af[2 * h] = a[m * LD_K + kk + t + 4 * h];
+                    af[2 * h + 1] = a[(m + 8) * LD_K + kk + t + 4 * h];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if constexpr (MMAK == 4) {
+                    dmma_16x8x4(acc[i][j], af[0], af[1], bf[j][0]);
+                } else if constexpr (MMAK == 8) {
+                    dmma_16x8x8(acc[i][j], af, bf[j]);
+                } else {
+                    dmma_16x8x16(acc[i][j], af, bf[j]);
+                }
+            }
+        }
+    }
+    }  // PERM
+}
+
+// C = alpha acc + beta C for the warp's fragment of tile (m0, n0) (beta == 0: C is not read).
+template <class CF>
+__device__ __forceinline__ void store_tile(const double (&acc)[CF::MT][4][4], double* C, int64_t ldc, int64_t m,
+                                           int64_t n, int64_t m0, int64_t n0, double alpha, double beta, int wm,
+                                           int wn, int g, int t) {
+    constexpr int MT = CF::MT, WTM = MT * 16;
+    constexpr bool PERM = CF::PERM;
+#pragma unroll
+    for (int i = 0; i < MT; ++i) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                int64_t row = m0 + wm * WTM + i * 16 + (PERM ? 2 * g + h : g + h * 8);
+                if (row >= m) continue;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    int64_t col = n0 + wn * 32 + j * 8 + 2 * t + e;
+                    if (col >= n) continue;
+                    double* cp = C + row + col * ldc;
+                    double v = alpha * acc[i][j][h * 2 + e];
+                    if (beta != 0.0) v = fma(beta, *cp, v);
+                    *cp = v;
+                }
+            }
+        }
+    }
+}
+
 template <class CF>
 __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __grid_constant__ GroupedParams prm) {
     constexpr int BK = CF::BK, STAGES = CF::STAGES, LD_K = CF::LD_K, LD_KB = CF::LD_KB, LDMN = CF::LDMN;
     constexpr int STAGE_A = CF::STAGE_A, STAGE_B = CF::STAGE_B;
-    constexpr int MMAK = CF::MMAK, THREADS = CF::THREADS, MT = CF::MT, WTM = MT * 16;
-    constexpr bool PERM = CF::PERM;
-    static_assert(!PERM || MMAK >= 8, "128-bit fragment loads need the k8 or k16 shape");
+    constexpr int THREADS = CF::THREADS, MT = CF::MT;
+    static_assert(!CF::PERM || CF::MMAK >= 8, "128-bit fragment loads need the k8 or k16 shape");
     extern __shared__ __align__(16) double smem[];
     double* sA = smem;
     double* sB = smem + STAGES * STAGE_A;
@@ -273,125 +404,169 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
             issue((kt + STAGES - 1) % STAGES);
             const double* a = sA + (kt % STAGES) * STAGE_A;
             const double* b = sB + (kt % STAGES) * STAGE_B;
-            if constexpr (PERM) {
-                // physical k of fragment element h (logical k = t + 4h), see Cfg
-                auto kp = [&](int h) { return 8 * (h >> 1) + 2 * t + (h & 1); };
-#pragma unroll
-                for (int kk = 0; kk < BK; kk += MMAK) {
-                    double bf[4][MMAK / 4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int n = wn * 32 + j * 8 + g;
-                        if (b_mn) {
-#pragma unroll
-                            for (int h = 0; h < MMAK / 4; ++h) bf[j][h] = b[(kk + kp(h)) * LDMN + n];
-                        } else {
-#pragma unroll
-                            for (int q = 0; q < MMAK / 8; ++q) {
-                                const double2 v = *reinterpret_cast<const double2*>(b + n * LD_KB + kk + 8 * q + 2 * t);
-                                bf[j][2 * q] = v.x;
-                                bf[j][2 * q + 1] = v.y;
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int i = 0; i < MT; ++i) {
-                        const int mr = wm * WTM + i * 16 + 2 * g;  // physical rows of MMA rows g, g + 8
-                        double af[MMAK / 2];
-                        if (a_mn) {
-#pragma unroll
-                            for (int h = 0; h < MMAK / 4; ++h) {
-                                const double2 v = *reinterpret_cast<const double2*>(a + (kk + kp(h)) * LDMN + mr);
-                                af[2 * h] = v.x;
-                                af[2 * h + 1] = v.y;
-                            }
-                        } else {
-#pragma unroll
-                            for (int q = 0; q < MMAK / 8; ++q) {
-                                const double2 v0 = *reinterpret_cast<const double2*>(a + mr * LD_K + kk + 8 * q + 2 * t);
-                                const double2 v1 =
-                                    *reinterpret_cast<const double2*>(a + (mr + 1) * LD_K + kk + 8 * q + 2 * t);
-                                af[4 * q] = v0.x;
-                                af[4 * q + 1] = v1.x;
-                                af[4 * q + 2] = v0.y;
-                                af[4 * q + 3] = v1.y;
-                            }
-                        }
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            if constexpr (MMAK == 8)
-                                dmma_16x8x8(acc[i][j], af, bf[j]);
-                            else
-                                dmma_16x8x16(acc[i][j], af, bf[j]);
-                        }
-                    }
-                }
-            } else {
-#pragma unroll
-            for (int kk = 0; kk < BK; kk += MMAK) {
-                // B fragments of the warp's four n8 tiles, then one m16 tile of A at a time
-                double bf[4][MMAK / 4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int n = wn * 32 + j * 8 + g;
-#pragma unroll
-                    for (int h = 0; h < MMAK / 4; ++h)
-                        bf[j][h] = b_mn ? b[(kk + t + 4 * h) * LDMN + n] : b[n * LD_KB + kk + t + 4 * h];
-                }
-#pragma unroll
-                for (int i = 0; i < MT; ++i) {
-                    const int m = wm * WTM + i * 16 + g;
-                    double af[MMAK / 2];
-#pragma unroll
-                    for (int h = 0; h < MMAK / 4; ++h) {
-                        if (a_mn) {
-                            af[2 * h] = a[(kk + t + 4 * h) * LDMN + m];
-                            af[2 * h + 1] = a[(kk + t + 4 * h) * LDMN + m + 8];
-                        } else {
-                            af[2 * h] = a[m * LD_K + kk + t + 4 * h];
-                            af[2 * h + 1] = a[(m + 8) * LD_K + kk + t + 4 * h];
-                        }
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        if constexpr (MMAK == 4) {
-                            dmma_16x8x4(acc[i][j], af[0], af[1], bf[j][0]);
-                        } else if constexpr (MMAK == 8) {
-                            dmma_16x8x8(acc[i][j], af, bf[j]);
-                        } else {
-                            dmma_16x8x16(acc[i][j], af, bf[j]);
-                        }
-                    }
-                }
-            }
-            }  // PERM
+            mma_ktile<CF>(a, b, a_mn, b_mn, acc, wm, wn, g, t);
         }
         cp_async_wait<0>();
         __syncthreads();  // the next tile's prologue reuses the ring
 
         // epilogue: C = alpha*acc + beta*C (beta == 0: C not read)
-        const double alpha = pb.alpha, beta = pb.beta;
+        store_tile<CF>(acc, pb.C, pb.ldc, pb.m, pb.n, m0, n0, pb.alpha, pb.beta, wm, wn, g, t);
+    }
+}
+
+// ---- TMA-fed form for one plain GEMM ---------------------------------------------------------
+// The same CTA tile, warps and fragment code, with the operand tiles brought into shared memory
+// by the tensor memory accelerator instead of per-thread cp.async: thread 0 issues two 2D
+// bulk-tensor loads per stage (no multicast) that complete on the stage's mbarrier, so no
+// thread spends issue slots on load addresses.  The boxes carry the padding of the cp.async
+// layout: a mn-major operand box is {BM + 4, BK} (rows of 132 doubles, the extra 4 columns are
+// never read) and a K-major one {BK + 4, BM}; ragged edges and the end of K come back
+// zero-filled from the out-of-range part of the box.  The stage counter runs across tiles,
+// so the next tile's first stages load while this tile's epilogue stores C.  Every mbarrier
+// wait is bounded; on expiry the CTA records DGT_DEVERR_TIMEOUT, stops, waits (bounded) for
+// its own loads and returns.
+struct TmaGemmParams {
+    CUtensorMap tmA, tmB;  // 64-byte aligned inside the parameter block
+    int64_t m, n, ldc;
+    double alpha, beta;
+    double* C;
+    int32_t tiles_m, tiles_n, total_tiles, ktiles;
+    int32_t a_mn, b_mn;  // operand layouts: 1 = mn-major box {BM + 4, BK}, 0 = K-major box {BK + 4, BM}
+    unsigned int* err;
+};
+
+template <class CF>
+__global__ void __launch_bounds__(CF::THREADS, 1) dmma_tma_kernel(const __grid_constant__ TmaGemmParams P) {
+    constexpr int BK = CF::BK, STAGES = CF::STAGES, STAGE_A = CF::STAGE_A, STAGE_B = CF::STAGE_B, MT = CF::MT;
+    static_assert(!CF::PERM, "the TMA boxes reproduce the unpermuted padded layouts");
+    static_assert(CF::LDMN == BM + 4 && CF::LD_K == BK + 4 && CF::LD_KB == BK + 4, "box shapes follow the layouts");
+    constexpr uint32_t BYTES_MN = (BM + 4) * BK * 8, BYTES_K = (BK + 4) * BM * 8;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    double* smem = reinterpret_cast<double*>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    double* sA = smem;
+    double* sB = smem + STAGES * STAGE_A;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * STAGE_B);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(full + STAGES);
+    // thread 0's load cursor lives in shared memory, out of the MMA warps' registers:
+    // cur[0] = tile, cur[1] = k-tile of the next stage to fill, cur[2] = stages issued
+    int* cur = const_cast<int*>(abort_flag) + 1;
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 2, wn = warp & 3;
+    const int g = lane >> 2, t = lane & 3;
+    const uint32_t tx_bytes = (P.a_mn ? BYTES_MN : BYTES_K) + (P.b_mn ? BYTES_MN : BYTES_K);
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) oz::mbar_init(oz::su32(full + s), 1);
+        *abort_flag = 0;
+        cur[0] = blockIdx.x;
+        cur[1] = 0;
+        cur[2] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    auto tile_mn = [&](int tile, int64_t& m0, int64_t& n0) {
+        const int in_group = GROUP_M * P.tiles_n;
+        const int first_m = (tile / in_group) * GROUP_M;
+        const int gsize = min(P.tiles_m - first_m, GROUP_M);
+        m0 = (int64_t)(first_m + (tile % in_group) % gsize) * BM;
+        n0 = (int64_t)((tile % in_group) / gsize) * BN;
+    };
+    auto issue_next = [&]() {
+        const int ld_tile = cur[0], ld_kt = cur[1];
+        if (ld_tile >= P.total_tiles) return;
+        const int s = cur[2] % STAGES;
+        int64_t m0, n0;
+        tile_mn(ld_tile, m0, n0);
+        const int32_t k0 = ld_kt * BK;
+        const uint32_t bar = oz::su32(full + s);
+        oz::mbar_expect_tx(bar, tx_bytes);
+        const uint32_t da = oz::su32(sA + s * STAGE_A), db = oz::su32(sB + s * STAGE_B);
+        if (P.a_mn)
+            oz::tma_load_2d(da, &P.tmA, (int32_t)m0, k0, bar);
+        else
+            oz::tma_load_2d(da, &P.tmA, k0, (int32_t)m0, bar);
+        if (P.b_mn)
+            oz::tma_load_2d(db, &P.tmB, (int32_t)n0, k0, bar);
+        else
+            oz::tma_load_2d(db, &P.tmB, k0, (int32_t)n0, bar);
+        cur[2] += 1;
+        if (ld_kt + 1 == P.ktiles) {
+            cur[1] = 0;
+            cur[0] = ld_tile + gridDim.x;
+        } else {
+            cur[1] = ld_kt + 1;
+        }
+    };
+    if (tid == 0)
+        for (int s = 0; s < STAGES - 1; ++s) issue_next();
+
+    uint32_t it = 0;  // stages consumed
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < P.total_tiles && ok; tile += gridDim.x) {
+        int64_t m0, n0;
+        tile_mn(tile, m0, n0);
+        double acc[MT][4][4];
 #pragma unroll
-        for (int i = 0; i < MT; ++i) {
+        for (int i = 0; i < MT; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < 4; ++j)
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    int64_t row = m0 + wm * WTM + i * 16 + (PERM ? 2 * g + h : g + h * 8);
-                    if (row >= pb.m) continue;
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        int64_t col = n0 + wn * 32 + j * 8 + 2 * t + e;
-                        if (col >= pb.n) continue;
-                        double* cp = pb.C + row + col * pb.ldc;
-                        double v = alpha * acc[i][j][h * 2 + e];
-                        if (beta != 0.0) v = fma(beta, *cp, v);
-                        *cp = v;
-                    }
-                }
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+        for (int kt = 0; kt < P.ktiles; ++kt, ++it) {
+            const int s = (int)(it % STAGES);
+            const bool got = oz::mbar_wait(oz::su32(full + s), (it / STAGES) & 1, abort_flag, P.err);
+            // every warp is done with stage it - 1 (refilled below), and all agree on aborting
+            if (__syncthreads_or(!got)) {
+                ok = false;
+                break;
+            }
+            if (tid == 0) issue_next();
+            mma_ktile<CF>(sA + s * STAGE_A, sB + s * STAGE_B, P.a_mn != 0, P.b_mn != 0, acc, wm, wn, g, t);
+        }
+        if (!ok) break;
+        store_tile<CF>(acc, P.C, P.ldc, P.m, P.n, m0, n0, P.alpha, P.beta, wm, wn, g, t);
+    }
+    // loads issued but not consumed (the lookahead past the last tile, or an abort) must land
+    // before the CTA's shared memory is released
+    if (tid == 0) {
+        for (uint32_t j = it; j < (uint32_t)cur[2]; ++j) {
+            long long t0 = clock64();
+            while (!oz::mbar_try(oz::su32(full + (j % STAGES)), (j / STAGES) & 1) && clock64() - t0 < oz::WAIT_BUDGET) {
             }
         }
     }
+    __syncthreads();
+}
+
+// 2D FP64 tensor map over a column-major operand: inner extent `inner` (contiguous), `outer`
+// columns of stride ld doubles, box {box_inner, box_outer}, no swizzle, zero fill outside.
+static bool make_f64_map(CUtensorMap* map, const double* base, int64_t inner, int64_t outer, int64_t ld,
+                         int box_inner, int box_outer) {
+    auto enc = oz::get_encode();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * 8)};
+    cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_outer};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <class CF>
+constexpr size_t tma_smem_bytes() {
+    return 128 + CF::SMEM + (size_t)CF::STAGES * 8 + 32;  // ring, full barriers, abort flag + cursor
+}
+
+template <class CF>
+cudaError_t launch_tma_variant(const TmaGemmParams& prm, int grid, cudaStream_t stream) {
+    cudaError_t e = smem_opt_in<dmma_tma_kernel<CF>>((int)tma_smem_bytes<CF>());
+    if (e != cudaSuccess) return e;
+    dmma_tma_kernel<CF><<<grid, CF::THREADS, tma_smem_bytes<CF>(), stream>>>(prm);
+    return cudaGetLastError();
 }
 
 using V0 = Cfg<4, 16, 4>;
@@ -411,20 +586,58 @@ using V13 = Cfg<16, 32, 2, 8, true>;
 
 template <class CF>
 cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stream) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(dmma_grouped_kernel<CF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)CF::SMEM);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    cudaError_t e = smem_opt_in<dmma_grouped_kernel<CF>>((int)CF::SMEM);
+    if (e != cudaSuccess) return e;
     dmma_grouped_kernel<CF><<<grid, CF::THREADS, CF::SMEM, stream>>>(prm);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-int dmma_variant_count() { return 14; }
+// Variants 14-17: the TMA-fed kernel with the tile shapes of variants 2, 1, 7 and a 5-deep
+// BK = 16 ring.  A call the TMA form does not cover (several problems or K-segments, operands
+// not 16-byte aligned or with an odd leading dimension, or small) runs the cp.async kernel of
+// the same shape instead.
+using T14 = V2;
+using T15 = V1;
+using T16 = V7;
+using T17 = Cfg<8, 16, 5>;
+
+int dmma_variant_count() { return 18; }
+
+// The TMA form for one plain GEMM, when the operands allow it; *used says whether it ran.
+template <class CF>
+static cudaError_t try_tma(dgt_context* h, const Problem& p, const KSegment& sg, int grid, bool* used) {
+    *used = false;
+    const bool a_mn = p.transa == 0, b_mn = p.transb != 0;
+    const int64_t k = sg.k;
+    if (p.m < 256 || p.n < 256 || k < 64) return cudaSuccess;
+    if (((uintptr_t)sg.A & 15) || ((uintptr_t)sg.B & 15) || (sg.lda & 1) || (sg.ldb & 1)) return cudaSuccess;
+    static thread_local TmaGemmParams prm;
+    prm = TmaGemmParams{};
+    // op(A) is m x k: 'N' -> mn-major (inner m), 'T' -> K-major (inner k); op(B)^T is n x k:
+    // 'N' -> K-major (inner k), 'T' -> mn-major (inner n)
+    const bool okA = a_mn ? make_f64_map(&prm.tmA, sg.A, p.m, k, sg.lda, BM + 4, CF::BK)
+                          : make_f64_map(&prm.tmA, sg.A, k, p.m, sg.lda, CF::BK + 4, BM);
+    const bool okB = b_mn ? make_f64_map(&prm.tmB, sg.B, p.n, k, sg.ldb, BN + 4, CF::BK)
+                          : make_f64_map(&prm.tmB, sg.B, k, p.n, sg.ldb, CF::BK + 4, BN);
+    if (!okA || !okB) return cudaSuccess;
+    prm.m = p.m;
+    prm.n = p.n;
+    prm.ldc = p.ldc;
+    prm.alpha = p.alpha;
+    prm.beta = p.beta;
+    prm.C = p.C;
+    prm.tiles_m = p.tiles_m;
+    prm.tiles_n = p.tiles_n;
+    prm.total_tiles = p.tiles_m * p.tiles_n;
+    prm.ktiles = (int32_t)ceil_div(k, CF::BK);
+    prm.a_mn = a_mn;
+    prm.b_mn = b_mn;
+    prm.err = h->dev_error;
+    *used = true;
+    return launch_tma_variant<CF>(prm, grid, h->stream);
+}
 
 dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs) {
     // drop empty problems, lay out the tile prefix
@@ -463,8 +676,27 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
         prm.segs = (const KSegment*)((char*)table + offs[1]);
     }
     int grid = (int)std::min<int64_t>(tiles, h->num_sms);
-    cudaError_t e;
-    switch (h->dmma_variant) {
+    cudaError_t e = cudaSuccess;
+    int variant = h->dmma_variant;
+    if (variant >= 14) {
+        bool used = false;
+        if (live.size() == 1 && segs.size() == 1) {
+            switch (variant) {
+                case 14: e = try_tma<T14>(h, live[0], segs[0], grid, &used); break;
+                case 15: e = try_tma<T15>(h, live[0], segs[0], grid, &used); break;
+                case 16: e = try_tma<T16>(h, live[0], segs[0], grid, &used); break;
+                default: e = try_tma<T17>(h, live[0], segs[0], grid, &used); break;
+            }
+        }
+        if (used) {
+            h->launches.fetch_add(1);
+            if (e != cudaSuccess) return cuda_fail(h, e, "dmma_tma_kernel launch");
+            return DGT_SUCCESS;
+        }
+        variant = variant == 14 ? 2 : variant == 15 ? 1 : variant == 16 ? 7 : 17;
+    }
+    switch (variant) {
+        case 17: e = launch_variant<T17>(prm, grid, h->stream); break;
         case 1: e = launch_variant<V1>(prm, grid, h->stream); break;
         case 2: e = launch_variant<V2>(prm, grid, h->stream); break;
         case 3: e = launch_variant<V3>(prm, grid, h->stream); break;

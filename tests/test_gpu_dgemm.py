@@ -131,7 +131,7 @@ def test_double_double_sample_error(h):
     assert np.median(gpu_err) <= 4 * max(np.median(cpu_err), 1e-17)
 
 
-@pytest.mark.parametrize("variant", list(range(14)))
+@pytest.mark.parametrize("variant", list(range(18)))
 def test_dmma_kernel_variants(variant):
     """Every tuning variant of the native kernel (DMMA shape m16n8k4/k8/k16, K depth, ring
     depth, 8 or 16 warps, 64- or 128-bit fragment loads) on ragged shapes, all four
@@ -145,3 +145,36 @@ def test_dmma_kernel_variants(variant):
         assert fro <= FRO_TOL
         _, fro = run(hh, "N", "T", 129, 131, 77, 2.0, 1.0, pad=(1, 1, 1), offset=1)
         assert fro <= FRO_TOL
+
+
+def _raw(h, ta, tb, m, n, k, alpha, beta, A, B, C, lda, ldb):
+    import torch
+
+    dA, dB, dC = dev(A), dev(B), dev(C)
+    h.dgemm(ta, tb, m, n, k, alpha, ptr(dA), lda, ptr(dB), ldb, beta, ptr(dC), m)
+    torch.cuda.synchronize()
+    h.check_device()
+    return host(dC, (m, n))
+
+
+@pytest.mark.parametrize("tma,base", [(14, 2), (15, 1), (16, 7), (17, 1)])
+def test_tma_variants_bit_identical_to_cp_async(tma, base):
+    """Variants 14-17 bring the operand tiles in by TMA (bulk-tensor loads completing on an
+    mbarrier per stage) into the same padded shared-memory layout the cp.async loader writes,
+    so with the same DMMA shape and K depth the result is bit for bit the cp.async kernel's:
+    ragged edges (zero-filled out-of-range boxes), all four transpose pairs, beta != 0, a K
+    that is not a multiple of the stage depth, and a problem spanning several waves of tiles."""
+    for (m, n, k), (ta, tb) in (((513, 385, 300), ("N", "N")), ((513, 385, 300), ("N", "T")),
+                                ((513, 385, 300), ("T", "N")), ((513, 385, 300), ("T", "T")),
+                                ((256, 256, 64), ("N", "N")), ((2304, 2048, 1000), ("N", "N"))):
+        ra, ca = (k, m) if ta == "T" else (m, k)
+        rb, cb = (n, k) if tb == "T" else (k, n)
+        A, B, C = O.uniform((ra, ca), m + 1), O.uniform((rb, cb), n + 2), O.uniform((m, n), k + 3)
+        out = {}
+        for v in (tma, base):
+            with dgt.Handle() as hh:
+                hh.set_tuning(dgt.TUNE_DMMA_VARIANT, v)
+                out[v] = _raw(hh, ta, tb, m, n, k, 1.5, -0.5, A, B, C, ra, rb)
+        assert np.array_equal(out[tma], out[base]), (tma, m, n, k, ta, tb)
+        assert O.rel_errors(out[tma], O.dgemm(A, B, 1.5, -0.5, C, ta, tb))[1] <= FRO_TOL
+
