@@ -119,7 +119,7 @@ cudaError_t launch_crt_grouped(cudaStream_t s, const CrtJob* jobs, int njobs, in
 // GEMM + reconstruction of one op(B) panel.
 struct Oz2Shape {
     int nmod, sa, sb, variant;  // sa, sb: sigma of op(A) rows and op(B) columns
-    bool pair;
+    bool pair, dyn;             // CTA-pair kernel; dynamic (tile, modulus) unit order
     int64_t m, k, m_pad, n_pad, k_pad;
     oz2::CrtConst cc;
     oz2::ModTable mt;
@@ -135,6 +135,7 @@ struct Oz2Work {
     int32_t* expA = nullptr;
     int32_t* expB = nullptr;
     uint8_t* res = nullptr;
+    int32_t* sched = nullptr;  // unit counter of the residue GEMM's dynamic order
 };
 dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmod, Oz2Shape& sh);
 Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws);
@@ -144,6 +145,7 @@ dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int 
                         int32_t* exps, int8_t* planes);
 dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
                            const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
-                           uint8_t* res, double alpha, double beta, double* C, int64_t ldc);
+                           uint8_t* res, double alpha, double beta, double* C, int64_t ldc,
+                           int32_t* sched = nullptr);
 
 }  // namespace dgt

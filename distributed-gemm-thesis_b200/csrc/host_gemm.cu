@@ -173,7 +173,7 @@ extern "C" dgt_status dgt_dgemm_host(dgt_handle_t h, char transa, char transb, i
                 return st;
             DGT_CUDA_TRY(h, cudaEventRecord(ev[EV_BFREE0 + buf], s));
             if ((st = ozaki2_gemm_crt(h, s, sh, wj, wpad, w.planesA, w.expA, w.planesB, w.expB, w.res, a, b, dC[buf],
-                                      m)) != DGT_SUCCESS)
+                                      m, w.sched)) != DGT_SUCCESS)
                 return st;
         } else {
             if ((st = dgt_dgemm_ex(h, transa, transb, m, wj, k, alpha, dA, std::max<int64_t>(rowsA, 1), dB[buf], ldb_d,

@@ -443,7 +443,9 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
     if (mode != DGT_FP64_OZAKI_INT8 && mode != DGT_FP64_OZAKI_BF16)
         return fail(h, DGT_ERROR_UNSUPPORTED, "unknown Ozaki mode");
     OzakiLayout L;
-    dgt_status st = ozaki_layout(h, S, m, n, k, h->ozaki_variant, mode == DGT_FP64_OZAKI_BF16, L);
+    // variants 5 and 6 differ from 1 and 4 only in the CRT residue GEMM's unit order
+    const int ov = h->ozaki_variant == 5 ? 1 : h->ozaki_variant == 6 ? 4 : h->ozaki_variant;
+    dgt_status st = ozaki_layout(h, S, m, n, k, ov, mode == DGT_FP64_OZAKI_BF16, L);
     if (st != DGT_SUCCESS) return st;
     void* ws = nullptr;
     st = ensure_workspace(h, L.total, &ws, 0);

@@ -646,9 +646,12 @@ dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmo
     if (nmod < MIN_MODULI || nmod > MAX_MODULI)
         return fail(h, DGT_ERROR_INVALID_VALUE, "modulus count must be in [8, 20]");
     const int ssum = sigma_sum_for(nmod, k);
-    // kernel variant: 0 (4 epilogue warps), 4 (CTA pair) or 1 (8 warps); all 128-byte stages
-    const int variant = (h->ozaki_variant == 0 || h->ozaki_variant == 4) ? h->ozaki_variant : 1;
+    // kernel variant: 0 (4 epilogue warps), 4 (CTA pair) or 1 (8 warps); all 128-byte stages;
+    // 5 and 6 are 1 and 4 with the (tile, modulus) units taken in a dynamic order
+    const int ov = h->ozaki_variant;
+    const int variant = ov == 5 ? 1 : ov == 6 ? 4 : (ov == 0 || ov == 4) ? ov : 1;
     const bool pair = variant == 4;
+    sh.dyn = ov == 5 || ov == 6;
     const int64_t m_unit = pair ? 2 * oz::TM : oz::TM;
     sh.nmod = nmod;
     sh.sa = (ssum + 1) / 2;
@@ -701,7 +704,7 @@ dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int 
 // padded to n_pad) and the reconstruction C = alpha C' + beta C.
 dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
                            const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
-                           uint8_t* res, double alpha, double beta, double* C, int64_t ldc) {
+                           uint8_t* res, double alpha, double beta, double* C, int64_t ldc, int32_t* sched) {
     using namespace oz2;
     const int nmod = sh.nmod, tkb = 128;
     const int64_t m = sh.m, m_pad = sh.m_pad, k_pad = sh.k_pad;
@@ -729,6 +732,10 @@ dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, i
     prm.res_plane = m_pad * n_pad;
     prm.err = h->dev_error;
     prm.test_stall = h->test_stall;
+    if (sh.dyn && sched) {  // the unit counter starts at zero for every launch
+        DGT_CUDA_TRY(h, cudaMemsetAsync(sched, 0, sizeof(int32_t), s));
+        prm.sched = sched;
+    }
     mark(h, 1);
     cudaError_t le;
     if (sh.variant == 4)
@@ -804,8 +811,9 @@ Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws) {
     const size_t pa = up((size_t)sh.nmod * sh.m_pad * sh.k_pad), pb = up((size_t)sh.nmod * n_pad * sh.k_pad);
     const size_t xa = up((size_t)sh.m * 8), xb = up((size_t)n * 8), ea = up((size_t)sh.m * 4), eb = up((size_t)n * 4);
     const size_t rs = up((size_t)sh.nmod * sh.m_pad * n_pad);
+    const size_t sc = 1024;  // the residue GEMM's unit counter (dynamic order)
     Oz2Work w;
-    w.bytes = pa + pb + 2 * (xa + xb) + ea + eb + rs;
+    w.bytes = pa + pb + 2 * (xa + xb) + ea + eb + rs + sc;
     char* p = (char*)ws;
     if (!p) return w;
     w.planesA = (int8_t*)p;
@@ -819,6 +827,7 @@ Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws) {
     w.expA = (int32_t*)p;
     w.expB = (int32_t*)(p + ea);
     w.res = (uint8_t*)(p + ea + eb);
+    w.sched = (int32_t*)(p + ea + eb + rs);
     return w;
 }
 
@@ -840,7 +849,8 @@ static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m
     if ((st = ozaki2_split(h, s, sh, sh.sb, B, ldb, n, sh.n_pad, !tb, w.amaxB, w.qnB, w.expB, w.planesB)) !=
         DGT_SUCCESS)
         return st;
-    return ozaki2_gemm_crt(h, s, sh, n, sh.n_pad, w.planesA, w.expA, w.planesB, w.expB, w.res, alpha, beta, C, ldc);
+    return ozaki2_gemm_crt(h, s, sh, n, sh.n_pad, w.planesA, w.expA, w.planesB, w.expB, w.res, alpha, beta, C, ldc,
+                           w.sched);
 }
 
 }  // namespace dgt

@@ -37,8 +37,9 @@ struct OzCfg {
     static constexpr int THREADS = 64 + 32 * EPI;
     static constexpr int A_STAGE = TM * TKB, B_STAGE = (PAIR ? TN / 2 : TN) * TKB;
     static constexpr int TILE_M = PAIR ? 2 * TM : TM;  // rows of output per (cluster) tile
-    static constexpr size_t SMEM = 1024 + (size_t)STAGES * (A_STAGE + B_STAGE) + 256 + (size_t)EPI * TN * 4;
+    static constexpr size_t SMEM = 1024 + (size_t)STAGES * (A_STAGE + B_STAGE) + 256 + (size_t)EPI * TN * 4 + 256;
 };
+constexpr int UNIT_RING = 8;  // depth of the dynamic scheduler's unit ring (see digit_gemm)
 constexpr int EXP_NONFINITE = 0x7fff;
 constexpr long long WAIT_BUDGET = 4000000000LL;  // clock64 cycles (~2 s) per wait
 constexpr int GROUP_M = 8;
@@ -83,6 +84,9 @@ struct Params {
     // completes, so the MMA issuer's first wait runs out of its budget.  No load or MMA is in
     // flight for that stage, so the abort path drains and returns as on a real stall.
     int32_t test_stall;
+    // Dynamic unit order: when set, the clusters take work units from this zeroed counter
+    // (atomicAdd) in ascending order instead of a static round robin.
+    int32_t* sched;
 };
 constexpr int MAX_SEGS = 640, MAX_GROUPS = 640;
 
@@ -146,6 +150,37 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
         }
     }
     return true;
+}
+
+// Cluster-scope forms for barriers that the other CTA of a pair may arrive on.
+__device__ __forceinline__ bool mbar_try_cluster(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(1000000u)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                                  unsigned int* err) {
+    long long t0 = clock64();
+    while (!mbar_try_cluster(bar, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > WAIT_BUDGET) {
+            *abort_flag = 1;
+            atomicOr(err, DGT_DEVERR_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+// Arrive (release, cluster scope) on a barrier given by its shared::cluster address.
+__device__ __forceinline__ void mbar_arrive_release_cluster(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ void st_cluster_s32(uint32_t cluster_addr, int32_t v) {
+    asm volatile("st.shared::cluster.s32 [%0], %1;\n" ::"r"(cluster_addr), "r"(v) : "memory");
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int32_t x, int32_t y,
@@ -352,6 +387,10 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
     uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 5);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     int32_t* col_exp_all = (int32_t*)(tmem_slot + 4);  // TN entries per epilogue warp
+    // dynamic unit order (P.sched): the leader's producer takes units from the global counter
+    // and publishes them through this ring to every role of both CTAs of the cluster
+    volatile int32_t* uring = col_exp_all + EPI * TN;            // UNIT_RING unit ids
+    uint64_t* ubars = (uint64_t*)(col_exp_all + EPI * TN + UNIT_RING);  // ufull[R], uempty[R]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     auto full = [&](int s) { return su32(bars + s); };
@@ -359,6 +398,9 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
     auto accf = [&](int b) { return su32(bars + 2 * STAGES + b); };
     auto acce = [&](int b) { return su32(bars + 2 * STAGES + 2 + b); };
     const uint32_t done_bar = su32(bars + 2 * STAGES + 4);
+    auto ufull = [&](int r) { return su32(ubars + r); };
+    auto uempty = [&](int r) { return su32(ubars + UNIT_RING + r); };
+    const bool dyn = P.sched != nullptr;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -370,6 +412,12 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
             mbar_init(acce(b), PAIR ? 2 * EPI : EPI);  // the leader's counts both CTAs' epilogue warps
         }
         mbar_init(done_bar, 1);
+        for (int r = 0; r < UNIT_RING; ++r) {
+            mbar_init(ufull(r), 1);
+            // readers of a slot: the leader's MMA issuer and epilogue warps, and in a pair the
+            // other CTA's producer and epilogue warps (the leader's producer writes it)
+            mbar_init(uempty(r), PAIR ? 2 + 2 * EPI : 1 + EPI);
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -393,6 +441,70 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
     const uint32_t tmem_base = *tmem_slot;
 
     const int total_tiles = GROUPED ? P.total_tiles : P.tiles_m * P.tiles_n;
+    // Work units.  The residue epilogue (EPI_MODE 2) stores every group -- one CRT modulus --
+    // to its own plane, so a unit is one (tile, group) pair, groups outermost: the CTAs then
+    // run one modulus at a time over the whole output and share its planes' panels in L2,
+    // and the tail after the last full wave is at most one modulus of one tile.  The other
+    // modes fold a tile's groups into C in order, so a unit is a whole tile.
+    constexpr bool UNIT_PER_GROUP = EPI_MODE == 2;
+    const int total_units = UNIT_PER_GROUP ? total_tiles * P.ngroups : total_tiles;
+    auto unit_of = [&](int u, int& tile, int& g0, int& g1) {
+        if constexpr (UNIT_PER_GROUP) {
+            g0 = u / total_tiles;
+            tile = u - g0 * total_tiles;
+            g1 = g0 + 1;
+        } else {
+            tile = u;
+            g0 = 0;
+            g1 = P.ngroups;
+        }
+    };
+    // The j-th unit this CTA (or cluster) works on, or -1 past the last.  Static order: a
+    // round robin.  Dynamic order: read from ring slot j once the scheduler has filled it; the
+    // slot is then released to the scheduler at once (the id is in a register).
+    auto unit_static = [&](uint32_t j) -> int {
+        const int un = unit + (int)j * units;
+        return un < total_units ? un : -1;
+    };
+    auto unit_take = [&](uint32_t j, bool& ok) -> int {  // one thread
+        const int r = (int)(j % UNIT_RING);
+        if (!mbar_wait_cluster(ufull(r), (j / UNIT_RING) & 1, abort_flag, P.err)) {
+            ok = false;
+            return -1;
+        }
+        const int un = uring[r];
+        mbar_arrive_release_cluster(PAIR ? map_to_rank(uempty(r), 0) : uempty(r));
+        return un;
+    };
+    auto unit_take_warp = [&](uint32_t j, bool& ok) -> int {  // a whole warp: lane 0 takes it
+        int un = -1, got = 1;
+        if ((threadIdx.x & 31) == 0) {
+            bool lok = true;
+            un = unit_take(j, lok);
+            got = lok;
+        }
+        un = __shfl_sync(0xffffffffu, un, 0);
+        if (!__shfl_sync(0xffffffffu, got, 0)) ok = false;
+        return un;
+    };
+    // The scheduler (the leader's producer lane): the next unit from the counter, published to
+    // both CTAs' rings; -1 once the units are exhausted.
+    auto unit_publish = [&](uint32_t j, bool& ok) -> int {
+        const int r = (int)(j % UNIT_RING);
+        if (!mbar_wait_cluster(uempty(r), ((j / UNIT_RING) & 1) ^ 1, abort_flag, P.err)) {
+            ok = false;
+            return -1;
+        }
+        int un = atomicAdd(P.sched, 1);
+        if (un >= total_units) un = -1;
+        uring[r] = un;
+        mbar_arrive_release_cluster(ufull(r));
+        if constexpr (PAIR) {
+            st_cluster_s32(map_to_rank(su32((const void*)(uring + r)), 1), un);
+            mbar_arrive_release_cluster(map_to_rank(ufull(r), 1));
+        }
+        return un;
+    };
     auto raster = [](int tile, int tiles_m, int tiles_n) -> int2 {
         int in_group = GROUP_M * tiles_n;
         int grp = tile / in_group;
@@ -429,7 +541,11 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
-            for (int tile = unit; tile < total_tiles && ok; tile += units) {
+            for (uint32_t j = 0; ok; ++j) {
+                const int un = !dyn ? unit_static(j) : leader ? unit_publish(j, ok) : unit_take(j, ok);
+                if (un < 0) break;
+                int tile, g0, g1;
+                unit_of(un, tile, g0, g1);
                 const TileCtx cx = ctx_of(tile);
                 const int tm = cx.tm, tn = cx.tn;
                 const CUtensorMap* tA = GROUPED ? &cx.gp->tmA : &tmA;
@@ -441,7 +557,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                     tensormap_acquire(tB);
                 }
                 const int m_pad = DGT_TILE_FIELD(cx, m_pad, m_pad), n_pad = DGT_TILE_FIELD(cx, n_pad, n_pad);
-                for (int g = 0; g < P.ngroups && ok; ++g) {
+                for (int g = g0; g < g1 && ok; ++g) {
                     const Group G = GROUPS[g];
                     for (int si = G.seg0; si < G.seg1 && ok; ++si) {
                         const Seg sg = SEGS[si];
@@ -489,9 +605,13 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
         if (lane == 0 && leader) {
             uint32_t it = 0, gcount = 0;
             bool ok = true;
-            for (int tile = unit; tile < total_tiles && ok; tile += units) {
+            for (uint32_t j = 0; ok; ++j) {
+                const int un = dyn ? unit_take(j, ok) : unit_static(j);
+                if (un < 0) break;
+                int tile, g0, g1;
+                unit_of(un, tile, g0, g1);
                 const TileCtx cx = ctx_of(tile);
-                for (int g = 0; g < P.ngroups && ok; ++g, ++gcount) {
+                for (int g = g0; g < g1 && ok; ++g, ++gcount) {
                     const Group G = GROUPS[g];
                     const int b = gcount & 1;
                     const uint32_t u = gcount >> 1;
@@ -575,7 +695,11 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                 k_mg = (uint32_t)(0x100000000ull / pm) + 1u;
             }
         }
-        for (int tile = unit; tile < total_tiles && ok; tile += units) {
+        for (uint32_t j = 0; ok; ++j) {
+            const int un = dyn ? unit_take_warp(j, ok) : unit_static(j);
+            if (un < 0) break;
+            int tile, g0, g1;
+            unit_of(un, tile, g0, g1);
             const TileCtx cx = ctx_of(tile);
             const int tm = cx.tm, tn = cx.tn;
             const int64_t row = (int64_t)tm * TILE_M + (int64_t)crank * TM + r_in;
@@ -589,7 +713,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
             __syncwarp();
             const bool row_ok = row < DGT_TILE_FIELD(cx, m, m);
             const int e_row = (EPI_MODE == 0 && row_ok) ? DGT_TILE_FIELD(cx, row_exp, row_exp)[row] : 0;
-            for (int g = 0; g < P.ngroups; ++g, ++gcount) {
+            for (int g = g0; g < g1; ++g, ++gcount) {
                 const int b = gcount & 1;
                 const uint32_t u = gcount >> 1;
                 if (!mbar_wait(accf(b), u & 1, abort_flag, P.err)) {

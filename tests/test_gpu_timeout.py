@@ -36,6 +36,7 @@ def _stalled_then_exact(h, call, check_result):
 
 
 @pytest.mark.parametrize("mode,count,variant", [(dgt.FP64_OZAKI2_INT8, 14, 1), (dgt.FP64_OZAKI2_INT8, 14, 4),
+                                                (dgt.FP64_OZAKI2_INT8, 14, 5), (dgt.FP64_OZAKI2_INT8, 14, 6),
                                                 (dgt.FP64_OZAKI_INT8, 7, 0)])
 def test_fp64_emulation_wait_runs_out_then_recovers(mode, count, variant):
     m, n, k = 200, 300, 256

@@ -27,7 +27,8 @@ def _crt_bytes(nmod, m, n, k):
         pa, pb = _up(nmod * m_pad * k_pad), _up(nmod * n_pad * k_pad)
         xa, xb, ea, eb = _up(m * 8), _up(n * 8), _up(m * 4), _up(n * 4)
         rs = _up(nmod * m_pad * n_pad)
-        best = max(best, pa + pb + 2 * (xa + xb) + ea + eb + rs)
+        sc = 1024  # the residue GEMM's unit counter
+        best = max(best, pa + pb + 2 * (xa + xb) + ea + eb + rs + sc)
     return best
 
 
