@@ -274,7 +274,7 @@ dgt_status dgt_set_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t value) {
             h->profile = value != 0;
             return DGT_SUCCESS;
         case DGT_TUNE_OZAKI_VARIANT:
-            if (value < 0 || value > 6) return fail(h, DGT_ERROR_INVALID_VALUE, "unknown Ozaki kernel variant");
+            if (value < 0 || value > 7) return fail(h, DGT_ERROR_INVALID_VALUE, "unknown Ozaki kernel variant");
             h->ozaki_variant = value;
             return DGT_SUCCESS;
         case DGT_TUNE_TEST_STALL:

@@ -166,7 +166,7 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
             if (S == 0) return DGT_SUCCESS;  // no count reaches tol: not eligible
         }
         std::vector<int> cands;
-        const std::vector<int> all = crt ? std::vector<int>{0, 1, 4, 5, 6} : std::vector<int>{0, 1, 2, 3, 4};
+        const std::vector<int> all = crt ? std::vector<int>{0, 1, 4, 5, 6, 7} : std::vector<int>{0, 1, 2, 3, 4};
         for (int v : all) {
             h->ozaki_variant = v;
             float t;

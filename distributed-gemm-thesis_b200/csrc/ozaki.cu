@@ -443,9 +443,13 @@ dgt_status ozaki_dgemm(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, i
     if (mode != DGT_FP64_OZAKI_INT8 && mode != DGT_FP64_OZAKI_BF16)
         return fail(h, DGT_ERROR_UNSUPPORTED, "unknown Ozaki mode");
     OzakiLayout L;
-    // variants 5 and 6 differ from 1 and 4 only in the CRT residue GEMM's unit order
-    const int ov = h->ozaki_variant == 5 ? 1 : h->ozaki_variant == 6 ? 4 : h->ozaki_variant;
-    dgt_status st = ozaki_layout(h, S, m, n, k, ov, mode == DGT_FP64_OZAKI_BF16, L);
+    // variants 5, 6 and 7 differ from 1, 4 and 0 only in the CRT residue GEMM's unit order; the BF16
+    // kernel has a single form (8 epilogue warps, 128-byte stages, one CTA per tile), so its
+    // layout is variant 1's whatever the handle's INT8 choice
+    const bool bf16 = mode == DGT_FP64_OZAKI_BF16;
+    const int hv = h->ozaki_variant;
+    const int ov = bf16 ? 1 : hv == 5 ? 1 : hv == 6 ? 4 : hv == 7 ? 0 : hv;
+    dgt_status st = ozaki_layout(h, S, m, n, k, ov, bf16, L);
     if (st != DGT_SUCCESS) return st;
     void* ws = nullptr;
     st = ensure_workspace(h, L.total, &ws, 0);
@@ -471,8 +475,11 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     if (T == 0) return DGT_SUCCESS;
     if (!valid_slices(crt ? DGT_FP64_OZAKI2_INT8 : DGT_FP64_OZAKI_INT8, S))
         return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16] (moduli: [8, 20])");
-    // variants 0 and 1 (4 or 8 epilogue warps, 128-byte stages); the others run as variant 1
-    const int variant = h->ozaki_variant == 0 ? 0 : 1;
+    // variants 0 and 1 (4 or 8 epilogue warps, 128-byte stages); 7 runs as 0 and the others as 1,
+    // 5, 6 and 7 with the GEMM's units taken in a dynamic order (the heaviest products' tiles are
+    // numbered first, and a CTA that finishes early takes the next unit)
+    const int variant = (h->ozaki_variant == 0 || h->ozaki_variant == 7) ? 0 : 1;
+    const bool dyn = h->ozaki_variant >= 5;
     const int tkb = 128;
     auto up = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
 
@@ -542,13 +549,15 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     }
     // CRT: the rows' integer 2-norm bounds follow the amax words
     const size_t amax_at = planes, exp_at = up(amax_at + amax_words * 8 * (crt ? 2 : 1), 256);
-    const size_t total = up(exp_at + exp_words * 4, 256);
+    const size_t sched_at = up(exp_at + exp_words * 4, 256);  // the GEMM's unit counter (dynamic order)
+    const size_t total = sched_at + 256;
     void* ws = nullptr;
     dgt_status st = ensure_workspace(h, total, &ws, 0);
     if (st != DGT_SUCCESS) return st;
     char* base = (char*)ws;
     auto* amax = (unsigned long long*)(base + amax_at);
     auto* exps = (int32_t*)(base + exp_at);
+    auto* sched = (int32_t*)(base + sched_at);
 
     // host tables: GProb[T] (tensor maps inside, 64-byte aligned), SplitJob[2T] and, for CRT,
     // CrtJob[T], zeroed byte for byte so that padding hashes the same on every call
@@ -647,16 +656,20 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
 
     // device copy of the tables from the handle's cache (a repeated call, e.g. from a
     // replayed CUDA graph, needs no copy)
-    const void* parts[3] = {gp, jobs, cj};
-    const size_t part_bytes[3] = {(size_t)T * sizeof(oz::GProb), job_bytes, crt_bytes};
-    size_t offs[3];
+    static thread_local std::vector<int32_t> host_tiles;
+    host_tiles.resize(T);
+    for (int r = 0; r < T; ++r) host_tiles[r] = gp[r].tile_begin;
+    const void* parts[4] = {gp, jobs, host_tiles.data(), cj};
+    const size_t part_bytes[4] = {(size_t)T * sizeof(oz::GProb), job_bytes, (size_t)T * sizeof(int32_t), crt_bytes};
+    size_t offs[4];
     void* table = nullptr;
-    st = device_table(h, crt ? 3 : 2, parts, part_bytes, &table, offs);
+    st = device_table(h, crt ? 4 : 3, parts, part_bytes, &table, offs);
     if (st != DGT_SUCCESS) return st;
     cudaStream_t s = h->stream;
     const auto* d_gp = (const oz::GProb*)((char*)table + offs[0]);
     const auto* d_jobs = (const oz::SplitJob*)((char*)table + offs[1]);
-    const auto* d_crt = crt ? (const oz2::CrtJob*)((char*)table + offs[2]) : nullptr;
+    const auto* d_tiles = (const int32_t*)((char*)table + offs[2]);
+    const auto* d_crt = crt ? (const oz2::CrtJob*)((char*)table + offs[3]) : nullptr;
 
     mark(h, 0);
     DGT_CUDA_TRY(h, cudaMemsetAsync(amax, 0, amax_words * 8 * (crt ? 2 : 1), s));
@@ -683,9 +696,16 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     prm.err = h->dev_error;
     prm.test_stall = h->test_stall;
     prm.gprobs = d_gp;
+    prm.prob_tiles = d_tiles;
     prm.nprob = T;
     prm.total_tiles = tiles;
-    const int grid = std::min<int>(tiles, h->num_sms);
+    if (dyn) {
+        DGT_CUDA_TRY(h, cudaMemsetAsync(sched, 0, sizeof(int32_t), s));
+        prm.sched = sched;
+    }
+    // the residue epilogue works in (tile, modulus) units: as many CTAs as units, up to the SMs
+    const int64_t units = crt ? (int64_t)tiles * (int64_t)groups.size() : (int64_t)tiles;
+    const int grid = (int)std::min<int64_t>(units, h->num_sms);
     mark(h, 1);
     cudaError_t le;
     if (crt)

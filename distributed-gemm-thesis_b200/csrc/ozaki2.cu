@@ -595,10 +595,11 @@ static cudaError_t launch_residue_gemm(const CUtensorMap& tmA, const CUtensorMap
                                        int num_sms, cudaStream_t s) {
     cudaError_t e = smem_opt_in<oz::digit_gemm<CF, 0, 2>>((int)CF::SMEM);
     if (e != cudaSuccess) return e;
-    const int tiles = prm.tiles_m * prm.tiles_n;
+    // (tile, modulus) units: as many CTAs (or clusters) as units, up to the SMs
+    const int64_t units = (int64_t)prm.tiles_m * prm.tiles_n * prm.ngroups;
     if constexpr (CF::PAIR) {
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(2 * std::min(tiles, num_sms / 2)));
+        cfg.gridDim = dim3((unsigned)(2 * std::min<int64_t>(units, num_sms / 2)));
         cfg.blockDim = dim3(CF::THREADS);
         cfg.dynamicSmemBytes = CF::SMEM;
         cfg.stream = s;
@@ -611,7 +612,8 @@ static cudaError_t launch_residue_gemm(const CUtensorMap& tmA, const CUtensorMap
         cfg.numAttrs = 1;
         return cudaLaunchKernelEx(&cfg, oz::digit_gemm<CF, 0, 2>, tmA, tmB, prm);
     } else {
-        oz::digit_gemm<CF, 0, 2><<<std::min(tiles, num_sms), CF::THREADS, CF::SMEM, s>>>(tmA, tmB, prm);
+        oz::digit_gemm<CF, 0, 2><<<(unsigned)std::min<int64_t>(units, num_sms), CF::THREADS, CF::SMEM, s>>>(tmA, tmB,
+                                                                                                    prm);
         return cudaGetLastError();
     }
 }
@@ -647,11 +649,11 @@ dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmo
         return fail(h, DGT_ERROR_INVALID_VALUE, "modulus count must be in [8, 20]");
     const int ssum = sigma_sum_for(nmod, k);
     // kernel variant: 0 (4 epilogue warps), 4 (CTA pair) or 1 (8 warps); all 128-byte stages;
-    // 5 and 6 are 1 and 4 with the (tile, modulus) units taken in a dynamic order
+    // 5, 6 and 7 are 1, 4 and 0 with the (tile, modulus) units taken in a dynamic order
     const int ov = h->ozaki_variant;
-    const int variant = ov == 5 ? 1 : ov == 6 ? 4 : (ov == 0 || ov == 4) ? ov : 1;
+    const int variant = ov == 5 ? 1 : ov == 6 ? 4 : ov == 7 ? 0 : (ov == 0 || ov == 4) ? ov : 1;
     const bool pair = variant == 4;
-    sh.dyn = ov == 5 || ov == 6;
+    sh.dyn = ov == 5 || ov == 6 || ov == 7;
     const int64_t m_unit = pair ? 2 * oz::TM : oz::TM;
     sh.nmod = nmod;
     sh.sa = (ssum + 1) / 2;

@@ -37,7 +37,7 @@ struct OzCfg {
     static constexpr int THREADS = 64 + 32 * EPI;
     static constexpr int A_STAGE = TM * TKB, B_STAGE = (PAIR ? TN / 2 : TN) * TKB;
     static constexpr int TILE_M = PAIR ? 2 * TM : TM;  // rows of output per (cluster) tile
-    static constexpr size_t SMEM = 1024 + (size_t)STAGES * (A_STAGE + B_STAGE) + 256 + (size_t)EPI * TN * 4 + 256;
+    static constexpr size_t SMEM = 1024 + (size_t)STAGES * (A_STAGE + B_STAGE) + 256 + (size_t)EPI * TN * 4 + 512;
 };
 constexpr int UNIT_RING = 8;  // depth of the dynamic scheduler's unit ring (see digit_gemm)
 constexpr int EXP_NONFINITE = 0x7fff;
@@ -76,8 +76,11 @@ struct Params {
     // no host-to-device copy); MAX_SEGS / MAX_GROUPS keep the block under 32 KB.
     Seg segs[640];
     Group groups[640];
-    // grouped mode: per-problem descriptors in device memory, tiles numbered problem by problem
+    // grouped mode: per-problem descriptors in device memory, tiles numbered problem by problem;
+    // prob_tiles[p] = gprobs[p].tile_begin as a compact array (the binary search per work unit
+    // stays in one or two cache lines)
     const struct GProb* gprobs;
+    const int32_t* prob_tiles;
     int32_t nprob, total_tiles;
     // Failure-path test hook (DGT_TUNE_TEST_STALL): nonzero makes every CTA's producer
     // withhold the operand loads of its first pipeline stage, a barrier phase nothing
@@ -391,6 +394,9 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
     // and publishes them through this ring to every role of both CTAs of the cluster
     volatile int32_t* uring = col_exp_all + EPI * TN;            // UNIT_RING unit ids
     uint64_t* ubars = (uint64_t*)(col_exp_all + EPI * TN + UNIT_RING);  // ufull[R], uempty[R]
+    // grouped mode: problems whose tensor maps this CTA's producer has already acquired
+    constexpr int ACQ_BITS = 2048;
+    uint32_t* acquired = (uint32_t*)(ubars + 2 * UNIT_RING);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     auto full = [&](int s) { return su32(bars + s); };
@@ -518,7 +524,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
             int lo = 0, hi = P.nprob - 1;  // last problem whose first tile is <= tile
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
-                if (P.gprobs[mid].tile_begin <= tile)
+                if ((P.prob_tiles ? P.prob_tiles[mid] : P.gprobs[mid].tile_begin) <= tile)
                     lo = mid;
                 else
                     hi = mid - 1;
@@ -541,6 +547,8 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
+            if constexpr (GROUPED)
+                for (int w = 0; w < ACQ_BITS / 32; ++w) acquired[w] = 0u;
             for (uint32_t j = 0; ok; ++j) {
                 const int un = !dyn ? unit_static(j) : leader ? unit_publish(j, ok) : unit_take(j, ok);
                 if (un < 0) break;
@@ -552,9 +560,14 @@ __global__ void __launch_bounds__(CF::THREADS, 1)
                 const CUtensorMap* tB = GROUPED ? &cx.gp->tmB : &tmB;
                 if constexpr (GROUPED) {
                     // the problem's maps reached global memory by a host copy: order them for
-                    // the tensor-map proxy before the TMA unit reads them
-                    tensormap_acquire(tA);
-                    tensormap_acquire(tB);
+                    // the tensor-map proxy before the TMA unit reads them, once per problem
+                    const int pi = (int)(cx.gp - P.gprobs);
+                    const uint32_t bit = 1u << (pi & 31);
+                    if (pi >= ACQ_BITS || !(acquired[pi >> 5] & bit)) {
+                        tensormap_acquire(tA);
+                        tensormap_acquire(tB);
+                        if (pi < ACQ_BITS) acquired[pi >> 5] |= bit;
+                    }
                 }
                 const int m_pad = DGT_TILE_FIELD(cx, m_pad, m_pad), n_pad = DGT_TILE_FIELD(cx, n_pad, n_pad);
                 for (int g = g0; g < g1 && ok; ++g) {

@@ -130,15 +130,18 @@ def test_grouped_ragged_batch_against_oracle():
         assert O.rel_errors(host(k[2], (it["m"], it["n"])), _want(it))[1] <= FRO_TOL
 
 
+@pytest.mark.parametrize("variant", [1, 6])
 @pytest.mark.parametrize("nmod", [14, 16])
-def test_grouped_crt_matches_per_product_bitwise(nmod):
+def test_grouped_crt_matches_per_product_bitwise(nmod, variant):
     """The CRT scheme in one grouped pass (amax, norm bounds, residue split, residue GEMM, reconstruction)
     equals one CRT call per product bit for bit: same operand bits per product, same residues,
-    same exact reconstruction."""
+    same exact reconstruction -- with the grouped GEMM's (tile, modulus) units in the static
+    order (variant 1) and taken from the atomic counter (variant 6)."""
     import torch
 
     items = _batch(13, 20, 1, 700) + _batch(14, 4, 200, 5000)
     with dgt.Handle() as h:
+        h.set_tuning(dgt.TUNE_OZAKI_VARIANT, variant)
         descs, keep = _descs(items)
         n0 = h.launch_count()
         h.dgemm_grouped(descs, mode=dgt.FP64_OZAKI2_INT8, slices=nmod)

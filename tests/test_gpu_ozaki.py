@@ -109,7 +109,7 @@ def test_ozaki_large_4096(h):
     assert O.rel_errors(got[rows, :], A[rows, :] @ B)[1] <= 1e-13
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_ozaki_kernel_variants(variant):
     """Every tuning variant of the INT8 kernel (epilogue warps x stage depth, and the CTA-pair
     kernel with 256 x 256 tiles) gives the same digits-exact products: identical to variant 0,

@@ -73,7 +73,7 @@ def test_error_falls_with_moduli(h):
     assert errs[-1] <= 1e-15  # the residual is the host FP64 GEMM's own rounding
 
 
-@pytest.mark.parametrize("variant", [0, 1, 4, 5, 6])
+@pytest.mark.parametrize("variant", [0, 1, 4, 5, 6, 7])
 def test_kernel_variants_identical(variant):
     """Every residue-GEMM variant gives the same bits: 4 / 8 epilogue warps, the CTA pair, and
     (5, 6) the dynamic (tile, modulus) unit order, where clusters take units from an atomic
