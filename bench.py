@@ -1070,8 +1070,9 @@ def main():
                 traffic = float(ln.split(":")[1].split()[0])
 
     # ---- end to end through the C ABI: pinned host in, host out, every step ----
-    # dgt_dgemm_host takes the host buffers: op(A) is copied once, op(B) and C travel in
-    # column panels on the library's copy streams, overlapped with the computation
+    # dgt_dgemm_host takes the host buffers: in the CRT mode op(A) row panels and op(B) column
+    # panels travel alternately on the library's copy streams and every C block computes as
+    # soon as its two panels are split, overlapped with the input stream
     def e2e_step():
         h.dgemm_host("N", "N", n, n, n, ALPHA, A_h.data_ptr(), n, B_h.data_ptr(), n, BETA, C_h.data_ptr(), n,
                      mode=MODE, slices=S)
@@ -1184,7 +1185,9 @@ def main():
                          "peak_burst": int8_burst, "frac_of_burst": achieved / int8_burst,
                          "algorithmic": f"{products} INT8 products x 2*M*N*K_pad ops"},
             "e2e": {"value": e2e_v, "unit": "TFLOP/s", "h2d_bytes_per_step": 2 * 8 * n * n,
-                    "d2h_bytes_per_step": 8 * n * n, "entry": "dgt_dgemm_host (copies overlapped in column panels)",
+                    "d2h_bytes_per_step": 8 * n * n,
+                    "entry": "dgt_dgemm_host (op(A) row panels and op(B) column panels cross the host link "
+                             "alternately, each split on arrival; completed C blocks return while others compute)",
                     "rows_equal_device_result": e2e_same},
             "gpu_launches": launches,
             "clocks": clocks,

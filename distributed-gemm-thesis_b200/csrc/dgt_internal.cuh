@@ -55,7 +55,7 @@ struct dgt_context {
     size_t ws_bytes[4] = {0, 0, 0, 0};
     // dgt_dgemm_host: copy-in and copy-out streams and its events, created on first use
     cudaStream_t copy_stream[2] = {nullptr, nullptr};
-    cudaEvent_t copy_ev[12] = {};
+    cudaEvent_t copy_ev[24] = {};
     std::atomic<int64_t> launches{0};
     std::map<dgt::TuneKey, dgt::TuneEntry> tune;
     // device copies of launch tables (grouped problems, Ozaki jobs and schedules), keyed by

@@ -31,7 +31,7 @@ enum {
     EV_START, EV_A, EV_IN0, EV_IN1, EV_BFREE0, EV_BFREE1, EV_C0, EV_C1, EV_OUT0, EV_OUT1, EV_JOIN_IN, EV_JOIN_OUT,
     EV_COUNT
 };
-static_assert(EV_COUNT <= 12, "dgt_context::copy_ev holds 12 events");
+static_assert(EV_COUNT <= 24, "dgt_context::copy_ev holds 24 events");
 
 // Once copies may be queued, every exit (success or error) orders the handle's stream after
 // all work of both copy streams, so nothing of this call can still be writing the handle's
@@ -52,14 +52,170 @@ struct JoinCopyStreams {
 dgt_status ensure_copy_streams(dgt_context* h) {
     for (auto& cs : h->copy_stream)
         if (!cs) DGT_CUDA_TRY(h, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    for (int i = 0; i < EV_COUNT; ++i)
-        if (!h->copy_ev[i]) DGT_CUDA_TRY(h, cudaEventCreateWithFlags(&h->copy_ev[i], cudaEventDisableTiming));
+    for (auto& e : h->copy_ev)
+        if (!e) DGT_CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return DGT_SUCCESS;
 }
 
 size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 
 }  // namespace
+
+// CRT mode in a 2D block order.  op(A) moves in row panels and op(B) in column panels,
+// alternately (A_0, B_0, A_1, B_1, ...); each panel is split into residue planes as soon as it
+// arrives, and every C block whose row and column panels are both split is computed (residue
+// GEMM and reconstruction) and sent back.  The host link's input stream therefore overlaps
+// the arithmetic from the second panel on, instead of op(A) crossing whole before the first
+// panel computes.  The residue planes of every panel stay resident (each row panel meets every
+// column panel); the FP64 staging buffers and the C blocks are double buffered.  Row scaling
+// depends on op(A)'s rows alone and column scaling on op(B)'s columns alone, so every block
+// equals the whole-matrix device call's bit for bit.
+enum {
+    E2_START, E2_AIN0, E2_AIN1, E2_AFREE0, E2_AFREE1, E2_BIN0, E2_BIN1, E2_BFREE0, E2_BFREE1, E2_CIN0, E2_CIN1,
+    E2_CREADY0, E2_CREADY1, E2_COUT0, E2_COUT1, E2_JOIN_IN, E2_JOIN_OUT, E2_COUNT
+};
+static_assert(E2_COUNT <= 24, "dgt_context::copy_ev holds 24 events");
+
+static dgt_status crt_host_2d(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                              double beta, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+                              int64_t ldc, int nmod, int64_t mb, int64_t nb) {
+    const bool read_c = beta != 0.0;
+    const int64_t R = ceil_div(m, mb), Q = ceil_div(n, nb);
+    Oz2Shape shf, shl;  // the full row panels' shape and the last (ragged) one's
+    dgt_status st;
+    if ((st = ozaki2_shape(h, mb, nb, k, nmod, shf)) != DGT_SUCCESS) return st;
+    if ((st = ozaki2_shape(h, m - (R - 1) * mb, nb, k, nmod, shl)) != DGT_SUCCESS) return st;
+    auto shape_of = [&](int64_t i) -> const Oz2Shape& { return i + 1 < R ? shf : shl; };
+    const int64_t k_pad = shf.k_pad;
+    // workspace: planes of every row and column panel, per-row / per-column scale data, one
+    // block's residue planes, the unit counter, two FP64 staging buffers per operand, two C blocks
+    auto up = [](size_t x) { return (x + 1023) / 1024 * 1024; };
+    std::vector<size_t> offA(R), offB(Q);
+    size_t at = 0;
+    for (int64_t i = 0; i < R; ++i) {
+        offA[i] = at;
+        at += up((size_t)nmod * shape_of(i).m_pad * k_pad);
+    }
+    for (int64_t j = 0; j < Q; ++j) {
+        offB[j] = at;
+        at += up((size_t)nmod * ozaki2_n_pad(std::min(nb, n - j * nb)) * k_pad);
+    }
+    const size_t o_amaxA = at, o_qnA = o_amaxA + up((size_t)m * 8), o_expA = o_qnA + up((size_t)m * 8);
+    const size_t o_amaxB = o_expA + up((size_t)m * 4), o_qnB = o_amaxB + up((size_t)n * 8),
+                 o_expB = o_qnB + up((size_t)n * 8);
+    const size_t o_res = o_expB + up((size_t)n * 4);
+    const size_t o_sched = o_res + up((size_t)nmod * shf.m_pad * ozaki2_n_pad(nb));
+    const size_t stA = up((size_t)mb * k * 8), stB = up((size_t)nb * k * 8), cb = up((size_t)mb * nb * 8);
+    const size_t o_stA = o_sched + 1024, o_stB = o_stA + 2 * stA, o_cb = o_stB + 2 * stB, total = o_cb + 2 * cb;
+    void* ws = nullptr;
+    if ((st = ensure_workspace(h, total, &ws, 3)) != DGT_SUCCESS) return st;
+    if ((st = ensure_copy_streams(h)) != DGT_SUCCESS) return st;
+    char* base = (char*)ws;
+    auto* amaxA = (unsigned long long*)(base + o_amaxA);
+    auto* qnA = (unsigned long long*)(base + o_qnA);
+    auto* expA = (int32_t*)(base + o_expA);
+    auto* amaxB = (unsigned long long*)(base + o_amaxB);
+    auto* qnB = (unsigned long long*)(base + o_qnB);
+    auto* expB = (int32_t*)(base + o_expB);
+    auto* res = (uint8_t*)(base + o_res);
+    auto* sched = (int32_t*)(base + o_sched);
+    double* stageA[2] = {(double*)(base + o_stA), (double*)(base + o_stA + stA)};
+    double* stageB[2] = {(double*)(base + o_stB), (double*)(base + o_stB + stB)};
+    double* cblk[2] = {(double*)(base + o_cb), (double*)(base + o_cb + cb)};
+    cudaStream_t s = h->stream, si = h->copy_stream[0], so = h->copy_stream[1];
+    cudaEvent_t* ev = h->copy_ev;
+
+    JoinCopyStreams join;
+    join.s = s;
+    join.si = si;
+    join.so = so;
+    join.ei = ev[E2_JOIN_IN];
+    join.eo = ev[E2_JOIN_OUT];
+    DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_START], s));
+    join.armed = true;
+    DGT_CUDA_TRY(h, cudaStreamWaitEvent(si, ev[E2_START], 0));
+    DGT_CUDA_TRY(h, cudaStreamWaitEvent(so, ev[E2_START], 0));
+
+    // op(A) row panel i: 'N' rows r0.. of the m x k matrix; 'T' columns r0.. of the k x m one
+    auto take_a = [&](int64_t i) -> dgt_status {
+        const int slot = (int)(i & 1);
+        const int64_t r0 = i * mb, mi = std::min(mb, m - r0);
+        if (i >= 2) DGT_CUDA_TRY(h, cudaStreamWaitEvent(si, ev[E2_AFREE0 + slot], 0));
+        if (ta)
+            DGT_CUDA_TRY(h, cudaMemcpy2DAsync(stageA[slot], k * 8, A + r0 * lda, lda * 8, k * 8, mi, cudaMemcpyDefault,
+                                              si));
+        else
+            DGT_CUDA_TRY(h, cudaMemcpy2DAsync(stageA[slot], mi * 8, A + r0, lda * 8, mi * 8, k, cudaMemcpyDefault, si));
+        DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_AIN0 + slot], si));
+        DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[E2_AIN0 + slot], 0));
+        const Oz2Shape& sh = shape_of(i);
+        if ((st = ozaki2_split(h, s, sh, sh.sa, stageA[slot], ta ? k : mi, mi, sh.m_pad, ta, amaxA + r0, qnA + r0,
+                               expA + r0, (int8_t*)(base + offA[i]))) != DGT_SUCCESS)
+            return st;
+        DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_AFREE0 + slot], s));
+        return DGT_SUCCESS;
+    };
+    // op(B) column panel j: 'N' columns c0.. of the k x n matrix; 'T' rows c0.. of the n x k one
+    auto take_b = [&](int64_t j) -> dgt_status {
+        const int slot = (int)(j & 1);
+        const int64_t c0 = j * nb, wj = std::min(nb, n - c0);
+        if (j >= 2) DGT_CUDA_TRY(h, cudaStreamWaitEvent(si, ev[E2_BFREE0 + slot], 0));
+        if (tb)
+            DGT_CUDA_TRY(h, cudaMemcpy2DAsync(stageB[slot], wj * 8, B + c0, ldb * 8, wj * 8, k, cudaMemcpyDefault, si));
+        else
+            DGT_CUDA_TRY(h, cudaMemcpy2DAsync(stageB[slot], k * 8, B + c0 * ldb, ldb * 8, k * 8, wj, cudaMemcpyDefault,
+                                              si));
+        DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_BIN0 + slot], si));
+        DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[E2_BIN0 + slot], 0));
+        if ((st = ozaki2_split(h, s, shf, shf.sb, stageB[slot], tb ? wj : k, wj, ozaki2_n_pad(wj), !tb, amaxB + c0,
+                               qnB + c0, expB + c0, (int8_t*)(base + offB[j]))) != DGT_SUCCESS)
+            return st;
+        DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_BFREE0 + slot], s));
+        return DGT_SUCCESS;
+    };
+    int64_t blocks = 0;
+    auto compute = [&](int64_t i, int64_t j) -> dgt_status {
+        const int slot = (int)(blocks & 1);
+        const int64_t r0 = i * mb, mi = std::min(mb, m - r0), c0 = j * nb, wj = std::min(nb, n - c0);
+        if (blocks >= 2) {  // the buffer's previous block has left
+            DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[E2_COUT0 + slot], 0));
+            if (read_c) DGT_CUDA_TRY(h, cudaStreamWaitEvent(si, ev[E2_COUT0 + slot], 0));
+        }
+        if (read_c) {
+            DGT_CUDA_TRY(h, cudaMemcpy2DAsync(cblk[slot], mi * 8, C + r0 + c0 * ldc, ldc * 8, mi * 8, wj,
+                                              cudaMemcpyDefault, si));
+            DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_CIN0 + slot], si));
+            DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[E2_CIN0 + slot], 0));
+        }
+        if ((st = ozaki2_gemm_crt(h, s, shape_of(i), wj, ozaki2_n_pad(wj), (const int8_t*)(base + offA[i]),
+                                  expA + r0, (const int8_t*)(base + offB[j]), expB + c0, res, alpha, beta,
+                                  cblk[slot], mi, sched)) != DGT_SUCCESS)
+            return st;
+        DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_CREADY0 + slot], s));
+        DGT_CUDA_TRY(h, cudaStreamWaitEvent(so, ev[E2_CREADY0 + slot], 0));
+        DGT_CUDA_TRY(h, cudaMemcpy2DAsync(C + r0 + c0 * ldc, ldc * 8, cblk[slot], mi * 8, mi * 8, wj, cudaMemcpyDefault,
+                                          so));
+        DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_COUT0 + slot], so));
+        ++blocks;
+        return DGT_SUCCESS;
+    };
+    // growing rectangle: after each panel, every block it completes
+    int64_t ia = 0, jb = 0;
+    while (ia < R || jb < Q) {
+        if (ia < R && (ia <= jb || jb >= Q)) {
+            if ((st = take_a(ia)) != DGT_SUCCESS) return st;
+            for (int64_t j = 0; j < jb; ++j)
+                if ((st = compute(ia, j)) != DGT_SUCCESS) return st;
+            ++ia;
+        } else {
+            if ((st = take_b(jb)) != DGT_SUCCESS) return st;
+            for (int64_t i = 0; i < ia; ++i)
+                if ((st = compute(i, jb)) != DGT_SUCCESS) return st;
+            ++jb;
+        }
+    }
+    return DGT_SUCCESS;
+}
 
 extern "C" dgt_status dgt_dgemm_host(dgt_handle_t h, char transa, char transb, int64_t m, int64_t n, int64_t k,
                                      const double* alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
@@ -93,6 +249,11 @@ extern "C" dgt_status dgt_dgemm_host(dgt_handle_t h, char transa, char transb, i
     }
     nb = std::min(nb, n);
     const int64_t panels = ceil_div(n, nb);
+    // CRT with a tall op(A) (several row panels of about m/8 rows, at least 1024): 2D block order
+    if (mode == DGT_FP64_OZAKI2_INT8 && k > 0 && k <= 65536) {
+        const int64_t mb = std::max<int64_t>(1024, ceil_div(ceil_div(m, 8), 256) * 256);
+        if (mb < m) return crt_host_2d(h, ta, tb, m, n, k, a, b, A, lda, B, ldb, C, ldc, slices, mb, nb);
+    }
 
     // device copies: op(A) as stored (rowsA x colsA, dense), two op(B) panels, two C panels
     const int64_t rowsA = ta ? k : m, colsA = ta ? m : k;

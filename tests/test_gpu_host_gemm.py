@@ -1,5 +1,5 @@
 """dgt_dgemm_host: A, B and C in host memory, copies pipelined with the computation in column
-panels.  In the CRT mode op(A) is split once and every panel's result equals the
+panels (and, in the CRT mode with a tall op(A), in a 2D order of row and column panels).  In the CRT mode op(A) is split once and every panel's result equals the
 whole-matrix device call bit for bit (row scaling depends on op(A)'s rows alone, column
 scaling on op(B)'s columns alone); other modes run the device GEMM per panel.  Page-locked and
 pageable host buffers give the same results (pageable ones only serialize the copies)."""
@@ -73,6 +73,24 @@ def test_crt_host_equals_device_bitwise(m, n, k, ta, tb, beta, panel):
     assert np.array_equal(got, want)
     ref = O.dgemm(A, B, 1.5, beta, C, ta, tb)
     assert O.rel_errors(got, ref)[1] <= FRO_TOL
+
+
+@pytest.mark.parametrize("m,n,k,ta,tb,beta,panel", [
+    (2600, 2300, 777, "N", "N", -0.5, 512),   # 3 row panels x 5 column panels, both ragged, C read
+    (2100, 1000, 300, "T", "T", 0.0, 0),      # automatic column width
+    (3000, 700, 2049, "N", "T", 1.25, 256),
+    (2049, 1300, 1000, "T", "N", 0.0, 384),   # a one-row last panel
+])
+def test_crt_host_2d_block_order_equals_device_bitwise(m, n, k, ta, tb, beta, panel):
+    """A tall op(A) runs in 2D block order: row panels of op(A) and column panels of op(B)
+    arrive alternately, each is split on arrival, and every completed C block is computed and
+    sent back.  Bit for bit the whole-matrix device call."""
+    A, B, C = _case(m, n, k, ta, tb, 3 * m + n)
+    with dgt.Handle() as h:
+        want = _device_result(h, A, B, C, ta, tb, m, n, k, 1.5, beta, dgt.FP64_OZAKI2_INT8, 15)
+        got = _host_result(h, A, B, C, ta, tb, m, n, k, 1.5, beta, dgt.FP64_OZAKI2_INT8, 15, panel)
+    assert np.array_equal(got, want)
+    assert O.rel_errors(got, O.dgemm(A, B, 1.5, beta, C, ta, tb))[1] <= FRO_TOL
 
 
 def test_host_pageable_equals_pinned():
