@@ -77,7 +77,7 @@ struct ModTable {
 // consecutive kk, one 32-byte sector of every plane row; RES_TPR threads share a row, each
 // turning RES_ELEMS consecutive kk into bytes.
 constexpr int RES_KSPAN = 32;
-constexpr int RES_TPR = 2;
+constexpr int RES_TPR = 4;
 constexpr int RES_ELEMS = RES_KSPAN / RES_TPR;
 constexpr int RES_ROWS = 128 / RES_TPR;
 
@@ -86,6 +86,7 @@ struct CrtConst {
     uint32_t W[MAX_MODULI][MAX_NW];
     uint32_t P[MAX_NW + 1];
     double kq[MAX_NW + 1];                      // 2^(32 l) / P: X / P ~ sum_l x_l kq_l
+    double Wd[MAX_MODULI][MAX_NW];              // W as doubles (exact: every limb < 2^32)
 };
 
 // One product of a grouped reconstruction: its residue planes, exponents, scaling and output;

@@ -136,7 +136,10 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
         Big Mm = M;
         const uint32_t m_mod = big_div_small(Mm, p);
         big_mul_small(M, inv_mod(m_mod, p));  // W = M * (M^-1 mod p) < P
-        for (int l = 0; l < MAX_NW; ++l) cc.W[i][l] = l < (int)M.size() ? M[l] : 0;
+        for (int l = 0; l < MAX_NW; ++l) {
+            cc.W[i][l] = l < (int)M.size() ? M[l] : 0;
+            cc.Wd[i][l] = (double)cc.W[i][l];
+        }
     }
     for (int l = 0; l <= MAX_NW; ++l) cc.P[l] = l < (int)P.size() ? P[l] : 0;
     double pd = 0;
@@ -408,17 +411,30 @@ template <int NW, int NM>
 __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
                                             int shift) {
     constexpr int NX = NW + 1;
+    // The low NI limbs accumulate in 64-bit integers, the high ones in FP64, which is exact:
+    // r W_l < 2^40 and at most 20 of them sum below 2^45 < 2^53.  Splitting the multiply-adds
+    // between the integer and the (otherwise idle) FP64 pipe halves the longest pipe's work.
+    constexpr int NI = NW / 2;
     uint64_t acc[NW];
+    double accd[NW - NI];
 #pragma unroll
     for (int l = 0; l < NW; ++l) acc[l] = 0;
+#pragma unroll
+    for (int l = 0; l < NW - NI; ++l) accd[l] = 0.0;
 #pragma unroll
     for (int j = 0; j < MAX_MODULI; ++j) {
         if (NM ? j < NM : j < cc.n) {
             const uint32_t r = __byte_perm(rr[j], 0u, 0x4440u + (uint32_t)sel);  // byte sel
 #pragma unroll
-            for (int l = 0; l < NW; ++l) acc[l] += (uint64_t)r * cc.W[j][l];  // < 20 * 2^40
+            for (int l = 0; l < NI; ++l) acc[l] += (uint64_t)r * cc.W[j][l];  // < 20 * 2^40
+            // r as a double: 2^52 + r has r in its low mantissa bits, then subtract 2^52 (exact)
+            const double rd = __hiloint2double(0x43300000, (int)r) - 4503599627370496.0;
+#pragma unroll
+            for (int l = NI; l < NW; ++l) accd[l - NI] = fma(rd, cc.Wd[j][l], accd[l - NI]);
         }
     }
+#pragma unroll
+    for (int l = NI; l < NW; ++l) acc[l] = (uint64_t)accd[l - NI];  // an integer below 2^45: exact
     uint32_t x[NX];
     uint64_t c = 0;
 #pragma unroll
@@ -495,8 +511,31 @@ __device__ __forceinline__ void crt_quad(const uint8_t* __restrict__ res, int64_
     uint32_t rr[MAX_MODULI];  // four rows' residues per modulus, one byte each
 #pragma unroll
     for (int j = 0; j < MAX_MODULI; ++j)
-        rr[j] = j < cc.n ? *reinterpret_cast<const uint32_t*>(res + j * res_plane + col * res_ld + row0) : 0u;
+        rr[j] = (NM ? j < NM : j < cc.n) ? *reinterpret_cast<const uint32_t*>(res + j * res_plane + col * res_ld + row0)
+                                         : 0u;
     const int f = col_exp[col];
+    double* cq = C + row0 + col * ldc;
+    if (row0 + 3 < m && (((uintptr_t)cq | (uintptr_t)(row_exp + row0)) & 15) == 0) {
+        // a whole quad with 16-byte-aligned exponents and C: one int4 load, two double2 stores
+        const int4 e = *reinterpret_cast<const int4*>(row_exp + row0);
+        const int ev[4] = {e.x, e.y, e.z, e.w};
+        double v[4];
+#pragma unroll
+        for (int e4 = 0; e4 < 4; ++e4)
+            v[e4] = (ev[e4] == oz::EXP_NONFINITE || f == oz::EXP_NONFINITE)
+                        ? __longlong_as_double(0x7ff8000000000000ll)
+                        : crt_value<NW, NM>(rr, e4, cc, ev[e4] + f - ssum);
+        double2* c2 = reinterpret_cast<double2*>(cq);
+        double2 lo = make_double2(alpha * v[0], alpha * v[1]), hi = make_double2(alpha * v[2], alpha * v[3]);
+        if (beta_c != 0.0) {
+            const double2 p0 = c2[0], p1 = c2[1];
+            lo = make_double2(fma(alpha, v[0], beta_c * p0.x), fma(alpha, v[1], beta_c * p0.y));
+            hi = make_double2(fma(alpha, v[2], beta_c * p1.x), fma(alpha, v[3], beta_c * p1.y));
+        }
+        c2[0] = lo;
+        c2[1] = hi;
+        return;
+    }
 #pragma unroll
     for (int e4 = 0; e4 < 4; ++e4) {
         const int64_t row = row0 + e4;
