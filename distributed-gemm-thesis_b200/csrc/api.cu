@@ -110,17 +110,46 @@ static bool cannon_order(int p, int c, int i, int j, int k, int* out) {
     return covers;
 }
 
-// Emulated-FP64 execution of a step schedule.  Step t of every product is its t-th
-// segment with K > 0 (the reference issues one cublasDgemm per step too); the first step
-// applies the product's beta, later steps accumulate.  Each step splits its own operands,
-// so every step is scaled on its own panel -- the numerics of a per-step local GEMM.  With
-// INT8 slices or CRT residues all products' step t run as one grouped pass (the products of
-// one step write distinct C); a step the grouped form does not support runs product by
-// product.
+// Emulated-FP64 execution of a step schedule.  CRT residues with steps fused (the default,
+// DGT_TUNE_FUSE_STEPS 1): every product is one product over the concatenation of its
+// K-segments -- as the native kernel, which keeps one accumulator across the segments -- and
+// all products run in one grouped pass.  Otherwise (INT8 slices, steps unfused, or a batch
+// the grouped form cannot hold) step t of every product is its t-th segment with K > 0 (the
+// reference issues one cublasDgemm per step too); the first step applies the product's beta,
+// later steps accumulate, each step splits its own operands (scaled on its own panel: the
+// numerics of a per-step local GEMM), and all products' step t run as one grouped pass (the
+// products of one step write distinct C); a step the grouped form does not support runs
+// product by product.
 dgt_status run_problems_emulated(dgt_context* h, const std::vector<Problem>& probs,
-                                 const std::vector<KSegment>& segs, dgt_fp64_mode mode, int slices) {
+                                 const std::vector<KSegment>& segs, dgt_fp64_mode mode, int slices,
+                                 bool allow_fused = true) {
     if (!valid_slices(mode, slices))
         return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16] (moduli: [8, 20])");
+    if (mode == DGT_FP64_OZAKI2_INT8 && allow_fused && h->fuse_steps) {
+        // CRT, fused: every product is ONE product over the concatenation of its K-segments
+        // (rows and columns scaled over the whole K, the residue products summed exactly across
+        // steps), all products in one grouped pass
+        std::vector<OzProblem> batch;
+        bool whole = true;
+        for (const Problem& pr : probs) {
+            if (pr.m <= 0 || pr.n <= 0) continue;
+            int64_t kt = 0;
+            for (int s = 0; s < pr.seg_count; ++s) kt += std::max<int64_t>(0, segs[pr.seg_begin + s].k);
+            if (kt == 0) {
+                whole = false;  // C = beta C: the step-by-step form handles it
+                break;
+            }
+            OzProblem b{pr.transa != 0, pr.transb != 0, pr.m, pr.n, kt, pr.alpha, pr.beta, nullptr, 0, nullptr, 0,
+                        pr.C, pr.ldc};
+            b.segs = &segs[pr.seg_begin];
+            b.nseg = pr.seg_count;
+            batch.push_back(b);
+        }
+        if (whole) {
+            dgt_status st = ozaki_dgemm_grouped(h, batch, slices, true);
+            if (st != DGT_ERROR_UNSUPPORTED) return st;
+        }
+    }
     std::vector<std::vector<const KSegment*>> steps(probs.size());
     size_t max_steps = 0;
     for (size_t i = 0; i < probs.size(); ++i) {
@@ -178,6 +207,33 @@ dgt_status validate_gemm(dgt_context* h, char ta, char tb, int64_t m, int64_t n,
     if (ldc < std::max<int64_t>(1, m)) return fail(h, DGT_ERROR_INVALID_VALUE, "ldc < m");
     if (m > 0 && n > 0 && !C) return fail(h, DGT_ERROR_INVALID_VALUE, "C is null");
     if (m > 0 && n > 0 && k > 0 && (!A || !B)) return fail(h, DGT_ERROR_INVALID_VALUE, "A or B is null");
+    return DGT_SUCCESS;
+}
+
+// Problems (one per grouped descriptor) for the grouped entry points; descriptors validated.
+dgt_status desc_problems(dgt_context* h, int count, const dgt_gemm_desc* d, std::vector<Problem>& probs,
+                                std::vector<KSegment>& segs) {
+    if (count < 0 || (count > 0 && !d)) return fail(h, DGT_ERROR_INVALID_VALUE, "bad descriptor array");
+    for (int i = 0; i < count; ++i) {
+        dgt_status st = validate_gemm(h, d[i].transa, d[i].transb, d[i].m, d[i].n, d[i].k, d[i].A, d[i].lda, d[i].B,
+                                      d[i].ldb, d[i].C, d[i].ldc);
+        if (st != DGT_SUCCESS) return st;
+    }
+    for (int i = 0; i < count; ++i) {
+        Problem p{};
+        p.m = d[i].m;
+        p.n = d[i].n;
+        p.alpha = d[i].k == 0 ? 0.0 : d[i].alpha;
+        p.beta = d[i].beta;
+        p.C = d[i].C;
+        p.ldc = d[i].ldc;
+        p.seg_begin = (int32_t)segs.size();
+        p.seg_count = 1;
+        p.transa = is_trans(d[i].transa);
+        p.transb = is_trans(d[i].transb);
+        segs.push_back(KSegment{d[i].A, d[i].B, d[i].lda, d[i].ldb, d[i].k});
+        probs.push_back(p);
+    }
     return DGT_SUCCESS;
 }
 
@@ -280,6 +336,9 @@ dgt_status dgt_set_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t value) {
         case DGT_TUNE_TEST_STALL:
             h->test_stall = value != 0;
             return DGT_SUCCESS;
+        case DGT_TUNE_FUSE_STEPS:
+            h->fuse_steps = value != 0;
+            return DGT_SUCCESS;
     }
     return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
 }
@@ -304,6 +363,7 @@ dgt_status dgt_get_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t* value) {
         case DGT_TUNE_PROFILE: *value = h->profile ? 1 : 0; return DGT_SUCCESS;
         case DGT_TUNE_OZAKI_VARIANT: *value = h->ozaki_variant; return DGT_SUCCESS;
         case DGT_TUNE_TEST_STALL: *value = h->test_stall; return DGT_SUCCESS;
+        case DGT_TUNE_FUSE_STEPS: *value = h->fuse_steps ? 1 : 0; return DGT_SUCCESS;
     }
     return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
 }
@@ -466,32 +526,13 @@ dgt_status dgt_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64_t n, int
 
 dgt_status dgt_dgemm_grouped(dgt_handle_t h, int count, const dgt_gemm_desc* d, dgt_fp64_mode mode, int slices) {
     if (!h) return DGT_ERROR_NOT_INITIALIZED;
-    if (count < 0 || (count > 0 && !d)) return fail(h, DGT_ERROR_INVALID_VALUE, "bad descriptor array");
-    for (int i = 0; i < count; ++i) {
-        dgt_status st = validate_gemm(h, d[i].transa, d[i].transb, d[i].m, d[i].n, d[i].k, d[i].A, d[i].lda, d[i].B,
-                                      d[i].ldb, d[i].C, d[i].ldc);
-        if (st != DGT_SUCCESS) return st;
-    }
-    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
     std::vector<Problem> probs;
     std::vector<KSegment> segs;
-    probs.reserve(count);
-    segs.reserve(count);
-    for (int i = 0; i < count; ++i) {
-        Problem p{};
-        p.m = d[i].m;
-        p.n = d[i].n;
-        p.alpha = d[i].k == 0 ? 0.0 : d[i].alpha;
-        p.beta = d[i].beta;
-        p.C = d[i].C;
-        p.ldc = d[i].ldc;
-        p.seg_begin = (int32_t)segs.size();
-        p.seg_count = 1;
-        p.transa = is_trans(d[i].transa);
-        p.transb = is_trans(d[i].transb);
-        segs.push_back(KSegment{d[i].A, d[i].B, d[i].lda, d[i].ldb, d[i].k});
-        probs.push_back(p);
-    }
+    probs.reserve(count > 0 ? count : 0);
+    segs.reserve(count > 0 ? count : 0);
+    dgt_status st = desc_problems(h, count, d, probs, segs);
+    if (st != DGT_SUCCESS) return st;
+    if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
     if (mode != DGT_FP64_NATIVE) return run_problems_emulated(h, probs, segs, mode, slices);
     return launch_dmma_grouped(h, probs, segs);
 }
@@ -691,6 +732,13 @@ dgt_status dgt_ipc_free(void* ptr) {
 dgt_status dgt_cannon25d(dgt_handle_t h, int64_t M, int32_t p, int32_t c, char ta, char tb, double alpha,
                          const double* const* A_tiles, const double* const* B_tiles, double beta,
                          double* const* C_tiles, dgt_fp64_mode mode, int slices) {
+    return dgt_cannon25d_batch(h, M, p, c, ta, tb, alpha, A_tiles, B_tiles, beta, C_tiles, 0, nullptr, mode, slices);
+}
+
+dgt_status dgt_cannon25d_batch(dgt_handle_t h, int64_t M, int32_t p, int32_t c, char ta, char tb, double alpha,
+                               const double* const* A_tiles, const double* const* B_tiles, double beta,
+                               double* const* C_tiles, int32_t count, const dgt_gemm_desc* descs,
+                               dgt_fp64_mode mode, int slices) {
     if (!h) return DGT_ERROR_NOT_INITIALIZED;
     if (!A_tiles || !B_tiles || !C_tiles) return fail(h, DGT_ERROR_INVALID_VALUE, "null tile array");
     // Summa25Decomposer ctor checks (src/25DCannon.cpp:7-23), as status codes
@@ -699,47 +747,144 @@ dgt_status dgt_cannon25d(dgt_handle_t h, int64_t M, int32_t p, int32_t c, char t
     if (!valid_op(ta) || !valid_op(tb)) return fail(h, DGT_ERROR_INVALID_VALUE, "transpose must be N, T or C");
     if (p * p > 256) return fail(h, DGT_ERROR_UNSUPPORTED, "more than 256 tiles per stack");
     if (mode == DGT_FP64_AUTO) mode = DGT_FP64_NATIVE;
+    if (mode != DGT_FP64_NATIVE && !valid_slices(mode, slices))
+        return fail(h, DGT_ERROR_INVALID_VALUE, "slice count must be in [2, 16] (moduli: [8, 20])");
+    std::vector<Problem> extra;
+    std::vector<KSegment> extra_segs;
+    dgt_status st = desc_problems(h, count, descs, extra, extra_segs);
+    if (st != DGT_SUCCESS) return st;
     const int64_t lm = M / p, tile = lm * lm;
     const int pc3 = p / c;
+    const bool native = mode == DGT_FP64_NATIVE;
+    const bool fuse = h->fuse_steps && (native ? (c > 1 || count > 0) : mode == DGT_FP64_OZAKI2_INT8);
+    // native stacks 1..c-1 write partial tiles W; fused, the stack-0 tiles wait on counters
+    // after W for them
+    const int64_t tiles_per = native ? dmma_tile_count(lm, lm) : 0;
     double* W = nullptr;
-    if (c > 1) {
+    int32_t* flags = nullptr;
+    const size_t w_bytes = (size_t)(c - 1) * p * p * tile * sizeof(double);
+    const size_t flag_count = (size_t)p * p * tiles_per;
+    if (c > 1 && (native || !fuse)) {
         void* ws = nullptr;
-        dgt_status st = ensure_workspace(h, (size_t)(c - 1) * p * p * tile * sizeof(double), &ws, 2);
+        st = ensure_workspace(h, w_bytes + (fuse ? flag_count * sizeof(int32_t) : 0), &ws, 2);
         if (st != DGT_SUCCESS) return st;
         W = (double*)ws;
+        flags = fuse ? (int32_t*)((char*)ws + w_bytes) : nullptr;
     }
+    // every virtual rank (i, j, k): one problem whose K-segments are its k-blocks in Cannon
+    // order; stack 0 carries beta*C (src/25DCannon.cpp:322), the other stacks start at 0
+    std::vector<int> order(pc3);
+    auto rank_problem = [&](int i, int j, int k, std::vector<Problem>& probs, std::vector<KSegment>& segs) {
+        cannon_order(p, c, i, j, k, order.data());
+        Problem pr{};
+        pr.m = lm;
+        pr.n = lm;
+        pr.alpha = alpha;
+        pr.beta = (k == 0) ? beta : 0.0;
+        pr.C = (k == 0 || !W) ? C_tiles[i * p + j] : W + ((int64_t)(k - 1) * p * p + i * p + j) * tile;
+        pr.ldc = lm;
+        pr.transa = is_trans(ta);
+        pr.transb = is_trans(tb);
+        pr.seg_begin = (int32_t)segs.size();
+        pr.seg_count = pc3;
+        for (int s = 0; s < pc3; ++s) {
+            const int t = order[s];
+            segs.push_back(KSegment{A_tiles[i * p + t], B_tiles[t * p + j], lm, lm, lm});
+        }
+        probs.push_back(pr);
+    };
     std::vector<Problem> probs;
     std::vector<KSegment> segs;
-    std::vector<int> order(pc3);
-    for (int k = 0; k < c; ++k) {
-        for (int i = 0; i < p; ++i) {
-            for (int j = 0; j < p; ++j) {
-                cannon_order(p, c, i, j, k, order.data());
-                Problem pr{};
-                pr.m = lm;
-                pr.n = lm;
-                pr.alpha = alpha;
-                // stack 0 carries beta*C (src/25DCannon.cpp:322); other stacks start at 0
-                pr.beta = (k == 0) ? beta : 0.0;
-                pr.C = (k == 0) ? C_tiles[i * p + j] : W + ((int64_t)(k - 1) * p * p + i * p + j) * tile;
-                pr.ldc = lm;
-                pr.transa = is_trans(ta);
-                pr.transb = is_trans(tb);
-                pr.seg_begin = (int32_t)segs.size();
-                pr.seg_count = pc3;
-                for (int s = 0; s < pc3; ++s) {
-                    int t = order[s];
-                    segs.push_back(KSegment{A_tiles[i * p + t], B_tiles[t * p + j], lm, lm, lm});
+    if (fuse && native) {
+        // ONE persistent launch: every partial tile first (they only store and count
+        // themselves), then the extra products, then the stack-0 tiles, which add their
+        // partials in stack order once counted (reduceResult, src/25DCannon.cpp:203-228)
+        for (int k = 1; k < c; ++k)
+            for (int i = 0; i < p; ++i)
+                for (int j = 0; j < p; ++j) {
+                    rank_problem(i, j, k, probs, segs);
+                    probs.back().red_role = 1;
+                    probs.back().red_slot = (int32_t)((i * p + j) * tiles_per);
                 }
-                probs.push_back(pr);
+        for (Problem e : extra) {
+            e.seg_begin += (int32_t)segs.size();
+            probs.push_back(e);
+        }
+        segs.insert(segs.end(), extra_segs.begin(), extra_segs.end());
+        // rank_problem's segments go after the extras' (seg_begin is taken at the push)
+        for (int i = 0; i < p; ++i)
+            for (int j = 0; j < p; ++j) {
+                rank_problem(i, j, 0, probs, segs);
+                if (c == 1) continue;
+                Problem& pr = probs.back();
+                pr.red_role = 2;
+                pr.red_slot = (int32_t)((i * p + j) * tiles_per);
+                pr.red_wait = c - 1;
+                pr.red_src = W + (int64_t)(i * p + j) * tile;
+                pr.red_stride = (int64_t)p * p * tile;
+                pr.red_ld = lm;
             }
+        return launch_dmma_grouped(h, probs, segs, flags, flag_count);
+    }
+    if (fuse) {
+        // CRT: one grouped pass; each (i, j) is a stack group -- stack 0's product, then stacks
+        // 1..c-1 as further stacks of the same output -- and every rank's k-blocks are one K
+        for (int i = 0; i < p; ++i)
+            for (int j = 0; j < p; ++j)
+                for (int k = 0; k < c; ++k) rank_problem(i, j, k, probs, segs);
+        const size_t cannon_probs = probs.size();
+        for (Problem e : extra) {
+            e.seg_begin += (int32_t)segs.size();
+            probs.push_back(e);
+        }
+        segs.insert(segs.end(), extra_segs.begin(), extra_segs.end());
+        std::vector<OzProblem> batch;
+        for (size_t r = 0; r < probs.size(); ++r) {
+            const Problem& pr = probs[r];
+            if (pr.m <= 0 || pr.n <= 0) continue;
+            int64_t kt = 0;
+            for (int s = 0; s < pr.seg_count; ++s) kt += segs[pr.seg_begin + s].k;
+            if (kt == 0) {  // an extra product without K: C = beta C (the native kernel, alpha 0)
+                std::vector<Problem> one{pr};
+                std::vector<KSegment> none{KSegment{nullptr, nullptr, 1, 1, 0}};
+                one[0].seg_begin = 0;
+                st = launch_dmma_grouped(h, one, none);
+                if (st != DGT_SUCCESS) return st;
+                continue;
+            }
+            OzProblem b{pr.transa != 0, pr.transb != 0, pr.m, pr.n, kt, pr.alpha, pr.beta, nullptr, 0, nullptr, 0,
+                        pr.C, pr.ldc};
+            b.segs = &segs[pr.seg_begin];
+            b.nseg = pr.seg_count;
+            b.stack = (r < cannon_probs && r % c != 0) ? 1 : 0;
+            batch.push_back(b);
+        }
+        st = ozaki_dgemm_grouped(h, batch, slices, true);
+        if (st != DGT_ERROR_UNSUPPORTED) return st;
+        // too large for one pass: the step-by-step form below
+        probs.clear();
+        segs.clear();
+        if (c > 1) {
+            void* ws = nullptr;
+            st = ensure_workspace(h, w_bytes, &ws, 2);
+            if (st != DGT_SUCCESS) return st;
+            W = (double*)ws;
         }
     }
-    dgt_status st = (mode == DGT_FP64_NATIVE) ? launch_dmma_grouped(h, probs, segs)
-                                              : run_problems_emulated(h, probs, segs, mode, slices);
-    if (st != DGT_SUCCESS || c == 1) return st;
+    // step-by-step form: the virtual ranks in one grouped call, then the stack reduction, then
+    // the extra products as a second grouped call
+    for (int k = 0; k < c; ++k)
+        for (int i = 0; i < p; ++i)
+            for (int j = 0; j < p; ++j) rank_problem(i, j, k, probs, segs);
+    st = native ? launch_dmma_grouped(h, probs, segs) : run_problems_emulated(h, probs, segs, mode, slices, false);
+    if (st != DGT_SUCCESS) return st;
     // stack reduction (reduceResult, src/25DCannon.cpp:203-228) into the stack-0 tiles
-    return launch_stack_reduce(h, tile, p * p, c - 1, C_tiles, W, (int64_t)p * p * tile);
+    if (c > 1) {
+        st = launch_stack_reduce(h, tile, p * p, c - 1, C_tiles, W, (int64_t)p * p * tile);
+        if (st != DGT_SUCCESS) return st;
+    }
+    if (extra.empty()) return DGT_SUCCESS;
+    return native ? launch_dmma_grouped(h, extra, extra_segs) : run_problems_emulated(h, extra, extra_segs, mode, slices);
 }
 
 dgt_status dgt_cannon25d_rank(dgt_handle_t h, int64_t M, int32_t p, int32_t c, int32_t rank, char ta, char tb,

@@ -29,6 +29,11 @@ struct SplitJob {
     int32_t bits;         // CRT scheme: sigma of this operand (scaled rows / columns have 2-norm <= 2^sigma)
     int32_t unused;
     unsigned long long* qn;  // CRT scheme: integer 2-norm bounds per row (see qnorm_*)
+    // Row stride of the planes (the product's padded K).  A product whose K is the
+    // concatenation of several pieces (K-segments) has one job per piece: planes then points
+    // at the piece's first column, K / k_pad are the piece's, and every piece's job updates
+    // the row's amax and norm bound with atomics.
+    int64_t plane_ld;
 };
 constexpr int AMAX_KCHUNK = 64;  // K rows per block of the MN-contiguous amax (fills the GPU)
 
@@ -90,7 +95,10 @@ struct CrtConst {
 };
 
 // One product of a grouped reconstruction: its residue planes, exponents, scaling and output;
-// it owns threads [thread_begin, thread_begin + ceil(m/4) n) of the launch.
+// it owns threads [thread_begin, thread_begin + ceil(m/4) n) of the launch.  count > 1 makes
+// it the lead of a stack group: the count - 1 jobs after it (same m, n, C) are further stacks
+// of the same output, own no threads (their thread_begin is the next lead's), and the lead's
+// threads write C = (alpha v + beta C) + alpha_1 v_1 + alpha_2 v_2 + ... in that order.
 struct CrtJob {
     const uint8_t* res;
     int64_t res_ld, res_plane, m, n;
@@ -99,7 +107,7 @@ struct CrtJob {
     double alpha, beta;
     double* C;
     int64_t ldc;
-    int32_t bits, unused;  // bits: sigma_A + sigma_B (the reconstruction's shift is e + f - bits)
+    int32_t bits, count;  // bits: sigma_A + sigma_B (the reconstruction's shift is e + f - bits)
     int64_t thread_begin;
 };
 

@@ -7,8 +7,10 @@
 // One persistent kernel serves every caller: a plain GEMM is one problem with one
 // K-segment; a SUMMA / Cannon virtual rank is one problem whose K-segments are its step
 // schedule (panel reads replace the reference's broadcasts and shifts); a grouped
-// workload is many problems.  CTAs walk a static round-robin tile list (no inter-CTA
-// waits), so the launch cannot deadlock.
+// workload is many problems.  CTAs walk a static round-robin tile list.  The one inter-CTA
+// wait is the 2.5D stack reduction's: a stack-0 tile waits for partial tiles numbered before
+// it, the launch is cooperative (every CTA resident), so the lowest unfinished tile can always
+// proceed; the wait is bounded all the same.
 //
 // Tile: 128 x 128 x 16, 8 warps (2 x 4), warp tile 64 x 32 of m16n8k4 DMMAs, a 4-stage
 // cp.async ring in shared memory padded so fragment loads are bank-conflict free.
@@ -58,6 +60,8 @@ struct GroupedParams {
     int total_tiles;
     const Problem* probs;  // global table, or null -> inline
     const KSegment* segs;
+    int32_t* red_flags;    // stack-reduction counters (null: no problem reduces)
+    unsigned int* err;     // sticky device error word
     Problem inl_probs[MAX_INLINE_PROBS];
     KSegment inl_segs[MAX_INLINE_SEGS];
 };
@@ -177,6 +181,15 @@ __device__ __forceinline__ void load_tile_full(double* s, const double* base, in
     }
 }
 
+__device__ __forceinline__ int32_t ld_acquire_gpu(const int32_t* p) {
+    int32_t v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add_gpu(int32_t* p, int32_t v) {
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ int find_problem(const Problem* P, int nprob, int tile) {
     int lo = 0, hi = nprob - 1;
     while (lo < hi) {
@@ -292,10 +305,14 @@ __device__ __forceinline__ void mma_ktile(const double* __restrict__ a, const do
 }
 
 // C = alpha acc + beta C for the warp's fragment of tile (m0, n0) (beta == 0: C is not read).
+// With nred > 0 the nred partial tiles red + s * red_stride (leading dimension red_ld) are
+// added to the result afterwards, in order s = 0, 1, ... (the stack reduction's order); they were
+// written by other CTAs of this launch, so they are read from L2.
 template <class CF>
 __device__ __forceinline__ void store_tile(const double (&acc)[CF::MT][4][4], double* C, int64_t ldc, int64_t m,
                                            int64_t n, int64_t m0, int64_t n0, double alpha, double beta, int wm,
-                                           int wn, int g, int t) {
+                                           int wn, int g, int t, const double* red = nullptr,
+                                           int64_t red_stride = 0, int64_t red_ld = 0, int nred = 0) {
     constexpr int MT = CF::MT, WTM = MT * 16;
     constexpr bool PERM = CF::PERM;
 #pragma unroll
@@ -313,6 +330,8 @@ __device__ __forceinline__ void store_tile(const double (&acc)[CF::MT][4][4], do
                     double* cp = C + row + col * ldc;
                     double v = alpha * acc[i][j][h * 2 + e];
                     if (beta != 0.0) v = fma(beta, *cp, v);
+                    // explicit adds: alpha acc + partial must not contract into one FMA
+                    for (int s = 0; s < nred; ++s) v = __dadd_rn(v, __ldcg(red + s * red_stride + row + col * red_ld));
                     *cp = v;
                 }
             }
@@ -409,8 +428,37 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
         cp_async_wait<0>();
         __syncthreads();  // the next tile's prologue reuses the ring
 
-        // epilogue: C = alpha*acc + beta*C (beta == 0: C not read)
-        store_tile<CF>(acc, pb.C, pb.ldc, pb.m, pb.n, m0, n0, pb.alpha, pb.beta, wm, wn, g, t);
+        // epilogue: C = alpha*acc + beta*C (beta == 0: C not read), plus the stack partials
+        int nred = 0;
+        if (pb.red_role == 2) {
+            // a stack-0 tile: its partial tiles come from CTAs that took them earlier in the
+            // tile order; one thread waits (bounded) for their count, then the CTA reads them
+            __shared__ int s_ready;
+            if (tid == 0) {
+                const int32_t* f = prm.red_flags + pb.red_slot + local;
+                const long long t0 = clock64();
+                int ready = 1;
+                while (ld_acquire_gpu(f) < pb.red_wait) {
+                    if (clock64() - t0 > oz::WAIT_BUDGET) {
+                        atomicOr(prm.err, DGT_DEVERR_TIMEOUT);
+                        ready = 0;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+                s_ready = ready;
+            }
+            __syncthreads();
+            nred = s_ready ? pb.red_wait : 0;
+        }
+        store_tile<CF>(acc, pb.C, pb.ldc, pb.m, pb.n, m0, n0, pb.alpha, pb.beta, wm, wn, g, t, pb.red_src,
+                       pb.red_stride, pb.red_ld, nred);
+        if (pb.red_role == 1) {
+            // a partial tile: every thread's stores reach L2 before the tile is counted
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) red_release_add_gpu(prm.red_flags + pb.red_slot + local, 1);
+        }
     }
 }
 
@@ -585,11 +633,25 @@ using V12 = Cfg<8, 32, 2, 8, true>;
 using V13 = Cfg<16, 32, 2, 8, true>;
 
 template <class CF>
-cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stream) {
+cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stream, bool coop) {
     cudaError_t e = smem_opt_in<dmma_grouped_kernel<CF>>((int)CF::SMEM);
     if (e != cudaSuccess) return e;
-    dmma_grouped_kernel<CF><<<grid, CF::THREADS, CF::SMEM, stream>>>(prm);
-    return cudaGetLastError();
+    if (!coop) {
+        dmma_grouped_kernel<CF><<<grid, CF::THREADS, CF::SMEM, stream>>>(prm);
+        return cudaGetLastError();
+    }
+    // a stack reduction waits across CTAs: a cooperative launch keeps them all resident
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(CF::THREADS);
+    cfg.dynamicSmemBytes = CF::SMEM;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, dmma_grouped_kernel<CF>, prm);
 }
 
 }  // namespace
@@ -604,6 +666,7 @@ using T16 = V7;
 using T17 = Cfg<8, 16, 5>;
 
 int dmma_variant_count() { return 18; }
+int64_t dmma_tile_count(int64_t m, int64_t n) { return ceil_div(m, BM) * ceil_div(n, BN); }
 
 // The TMA form for one plain GEMM, when the operands allow it; *used says whether it ran.
 template <class CF>
@@ -639,13 +702,23 @@ static cudaError_t try_tma(dgt_context* h, const Problem& p, const KSegment& sg,
     return launch_tma_variant<CF>(prm, grid, h->stream);
 }
 
-dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs) {
+dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs,
+                               int32_t* red_flags, size_t red_count) {
     // drop empty problems, lay out the tile prefix
     std::vector<Problem> live;
     live.reserve(probs.size());
     int64_t tiles = 0;
+    bool reduces = false, stack0_seen = false;
     for (auto p : probs) {
         if (p.m <= 0 || p.n <= 0) continue;
+        if (p.red_role != 0) {
+            if (!red_flags) return fail(h, DGT_ERROR_INVALID_VALUE, "stack reduction without counters");
+            // a partial numbered after a stack-0 tile could be waited for by a CTA it needs
+            if (p.red_role == 1 && stack0_seen)
+                return fail(h, DGT_ERROR_INVALID_VALUE, "partial problem after a stack-0 problem");
+            stack0_seen |= p.red_role == 2;
+            reduces = true;
+        }
         p.tiles_m = (int32_t)ceil_div(p.m, BM);
         p.tiles_n = (int32_t)ceil_div(p.n, BN);
         p.tile_begin = (int32_t)tiles;
@@ -658,6 +731,8 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
     static thread_local GroupedParams prm;  // large; filled per launch (launch copies the value)
     prm.nprob = (int)live.size();
     prm.total_tiles = (int)tiles;
+    prm.red_flags = reduces ? red_flags : nullptr;
+    prm.err = h->dev_error;
     if ((int)live.size() <= MAX_INLINE_PROBS && (int)segs.size() <= MAX_INLINE_SEGS) {
         prm.probs = nullptr;
         prm.segs = nullptr;
@@ -677,10 +752,11 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
     }
     int grid = (int)std::min<int64_t>(tiles, h->num_sms);
     cudaError_t e = cudaSuccess;
+    if (reduces) DGT_CUDA_TRY(h, cudaMemsetAsync(red_flags, 0, red_count * sizeof(int32_t), h->stream));
     int variant = h->dmma_variant;
     if (variant >= 14) {
         bool used = false;
-        if (live.size() == 1 && segs.size() == 1) {
+        if (live.size() == 1 && segs.size() == 1 && !reduces) {
             switch (variant) {
                 case 14: e = try_tma<T14>(h, live[0], segs[0], grid, &used); break;
                 case 15: e = try_tma<T15>(h, live[0], segs[0], grid, &used); break;
@@ -696,21 +772,21 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
         variant = variant == 14 ? 2 : variant == 15 ? 1 : variant == 16 ? 7 : 17;
     }
     switch (variant) {
-        case 17: e = launch_variant<T17>(prm, grid, h->stream); break;
-        case 1: e = launch_variant<V1>(prm, grid, h->stream); break;
-        case 2: e = launch_variant<V2>(prm, grid, h->stream); break;
-        case 3: e = launch_variant<V3>(prm, grid, h->stream); break;
-        case 4: e = launch_variant<V4>(prm, grid, h->stream); break;
-        case 5: e = launch_variant<V5>(prm, grid, h->stream); break;
-        case 6: e = launch_variant<V6>(prm, grid, h->stream); break;
-        case 7: e = launch_variant<V7>(prm, grid, h->stream); break;
-        case 8: e = launch_variant<V8>(prm, grid, h->stream); break;
-        case 9: e = launch_variant<V9>(prm, grid, h->stream); break;
-        case 10: e = launch_variant<V10>(prm, grid, h->stream); break;
-        case 11: e = launch_variant<V11>(prm, grid, h->stream); break;
-        case 12: e = launch_variant<V12>(prm, grid, h->stream); break;
-        case 13: e = launch_variant<V13>(prm, grid, h->stream); break;
-        default: e = launch_variant<V0>(prm, grid, h->stream); break;
+        case 17: e = launch_variant<T17>(prm, grid, h->stream, reduces); break;
+        case 1: e = launch_variant<V1>(prm, grid, h->stream, reduces); break;
+        case 2: e = launch_variant<V2>(prm, grid, h->stream, reduces); break;
+        case 3: e = launch_variant<V3>(prm, grid, h->stream, reduces); break;
+        case 4: e = launch_variant<V4>(prm, grid, h->stream, reduces); break;
+        case 5: e = launch_variant<V5>(prm, grid, h->stream, reduces); break;
+        case 6: e = launch_variant<V6>(prm, grid, h->stream, reduces); break;
+        case 7: e = launch_variant<V7>(prm, grid, h->stream, reduces); break;
+        case 8: e = launch_variant<V8>(prm, grid, h->stream, reduces); break;
+        case 9: e = launch_variant<V9>(prm, grid, h->stream, reduces); break;
+        case 10: e = launch_variant<V10>(prm, grid, h->stream, reduces); break;
+        case 11: e = launch_variant<V11>(prm, grid, h->stream, reduces); break;
+        case 12: e = launch_variant<V12>(prm, grid, h->stream, reduces); break;
+        case 13: e = launch_variant<V13>(prm, grid, h->stream, reduces); break;
+        default: e = launch_variant<V0>(prm, grid, h->stream, reduces); break;
     }
     h->launches.fetch_add(1);
     if (e != cudaSuccess) return cuda_fail(h, e, "dmma_grouped_kernel launch");

@@ -44,6 +44,7 @@ struct dgt_context {
     int ozaki_variant = 6; // INT8 Ozaki kernel variant (dgt.h); 6 measured fastest at 16384^3
     bool profile = false;  // record phase events (DGT_TUNE_PROFILE)
     int test_stall = 0;    // failure-path test hook (DGT_TUNE_TEST_STALL)
+    bool fuse_steps = true; // DGT_TUNE_FUSE_STEPS
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // split start, gemm start, gemm end
     bool ev_split = false;  // last call had a split phase
     std::string last_error;
@@ -160,9 +161,19 @@ struct Problem {
     int32_t transa, transb;        // 0 = 'N', 1 = 'T'
     int32_t tile_begin;            // prefix sum of tiles (filled by the launcher)
     int32_t tiles_m, tiles_n;
+    // Stack reduction inside the launch (2.5D Cannon).  red_role 1: a partial problem; it stores
+    // its tiles, then counts each in red_flags[red_slot + local tile].  red_role 2: a stack-0
+    // problem; it waits until its tile's count reaches red_wait and adds the red_wait partial
+    // tiles red_src + s * red_stride (leading dimension red_ld), s = 0, 1, ..., to its own
+    // result in that order.  Partial problems' tiles are numbered before every stack-0 tile,
+    // which, with all CTAs resident, keeps every wait finite.  red_role 0: no reduction.
+    const double* red_src;
+    int64_t red_stride, red_ld;
+    int32_t red_role, red_slot, red_wait, red_pad;
 };
 
 int dmma_variant_count();
+int64_t dmma_tile_count(int64_t m, int64_t n);  // CTA tiles of one m x n problem of the grouped kernel
 TuneKey tune_key(int mode, int64_t m, int64_t n, int64_t k);
 const TuneEntry* tune_lookup(dgt_context* h, int mode, int64_t m, int64_t n, int64_t k);
 // Argument checks shared by the GEMM entry points (api.cu).
@@ -170,7 +181,10 @@ dgt_status validate_gemm(dgt_context* h, char ta, char tb, int64_t m, int64_t n,
                          int64_t lda, const void* B, int64_t ldb, const void* C, int64_t ldc);
 // Launches the persistent grouped FP64 DMMA kernel over problems/segments (host arrays,
 // copied to device workspace).  Validation is the caller's job.
-dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs);
+// red_flags: the stack-reduction counters (zeroed by the launcher), or null when no problem
+// reduces.
+dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs,
+                               int32_t* red_flags = nullptr, size_t red_count = 0);
 
 // ---- layout engine (layout.cu) ---------------------------------------------------------
 // One strided copy: rows x cols, column-major (rows contiguous on both sides).
@@ -224,6 +238,15 @@ struct OzProblem {
     int64_t ldb;
     double* C;
     int64_t ldc;
+    // CRT scheme only.  nseg > 0: K is the concatenation of the pieces segs[0 .. nseg) (each
+    // with its own A, B, lda, ldb and k > 0; k above is their total, A and B are unused): one
+    // product, its rows and columns scaled over the whole K, so a step schedule's steps
+    // become one exact residue sum.  stack 1: a further stack of the preceding product's
+    // output (same m, n, C and ldc, beta 0); alpha times its result is added to the preceding
+    // stacks' sum, in order (the 2.5D stack reduction).
+    const KSegment* segs = nullptr;
+    int32_t nseg = 0;
+    int32_t stack = 0;
 };
 // All products in one INT8 emulation pass: one amax launch, one split launch, one persistent
 // GEMM launch over every product's tiles (and, for the CRT scheme, one reconstruction

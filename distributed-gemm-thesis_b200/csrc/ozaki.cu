@@ -60,9 +60,11 @@ __global__ void amax_mn_contig(const double* __restrict__ X, int64_t ld, int64_t
     amax_mn_block(X, ld, MN, K, kchunk, amax, blockIdx.x, blockIdx.y);
 }
 
-// K-contiguous operand: element (mn, kk) at X[kk + mn*ld]; one warp per mn.
+// K-contiguous operand: element (mn, kk) at X[kk + mn*ld]; one warp per mn.  atomic: the row
+// may have other pieces (amax zeroed by the caller), so the result goes in by atomicMax.
 __device__ __forceinline__ void amax_k_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                                             unsigned long long* __restrict__ amax, int64_t bx) {
+                                             unsigned long long* __restrict__ amax, int64_t bx,
+                                             bool atomic = false) {
     int64_t mn = bx * (blockDim.x / 32) + threadIdx.x / 32;
     int lane = threadIdx.x & 31;
     if (mn >= MN) return;
@@ -77,7 +79,12 @@ __device__ __forceinline__ void amax_k_block(const double* __restrict__ X, int64
         unsigned long long other = __shfl_xor_sync(0xffffffffu, mx, o);
         mx = other > mx ? other : mx;
     }
-    if (lane == 0) amax[mn] = mx;
+    if (lane == 0) {
+        if (!atomic)
+            amax[mn] = mx;
+        else if (mx)
+            atomicMax(amax + mn, mx);
+    }
 }
 
 __global__ void amax_k_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
@@ -160,7 +167,7 @@ __global__ void __launch_bounds__(256) amax_grouped(const SplitJob* __restrict__
     const SplitJob& J = jobs[find_job(jobs, njobs, blk, false)];
     const int64_t local = blk - J.amax_begin;
     if (J.kcontig)
-        amax_k_block(J.X, J.ld, J.MN, J.K, J.amax, local);
+        amax_k_block(J.X, J.ld, J.MN, J.K, J.amax, local, true);
     else
         amax_mn_block(J.X, J.ld, J.MN, J.K, AMAX_KCHUNK, J.amax, local % J.amax_bx, local / J.amax_bx);
 }
@@ -483,8 +490,45 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     const int tkb = 128;
     auto up = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
 
+    // every product's K pieces: one (A, B, k), or its K-segments (CRT only), each padded to KPAD
+    struct Piece {
+        const double* A;
+        const double* B;
+        int64_t lda, ldb, k, k_off, k_pad;
+    };
+    std::vector<Piece> pieces;
+    std::vector<int32_t> piece_begin(T + 1);
+    std::vector<int64_t> k_total(T), k_pads(T);
     int64_t k_pad_max = 0;
-    for (const OzProblem& p : probs) k_pad_max = std::max(k_pad_max, ceil_div(p.k, oz::KPAD) * oz::KPAD);
+    for (int i = 0; i < T; ++i) {
+        const OzProblem& p = probs[i];
+        if (!crt && (p.nseg > 0 || p.stack)) return DGT_ERROR_UNSUPPORTED;
+        if (p.stack) {  // a further stack of the preceding output
+            if (i == 0 || p.beta != 0.0) return fail(h, DGT_ERROR_INVALID_VALUE, "stack product without its output");
+            const OzProblem& q = probs[i - 1];
+            if (q.m != p.m || q.n != p.n || q.C != p.C || q.ldc != p.ldc)
+                return fail(h, DGT_ERROR_INVALID_VALUE, "stack product with another output");
+        }
+        piece_begin[i] = (int32_t)pieces.size();
+        int64_t kt = 0, kp = 0;
+        const int ns = p.nseg > 0 ? p.nseg : 1;
+        for (int s = 0; s < ns; ++s) {
+            Piece pc = p.nseg > 0 ? Piece{p.segs[s].A, p.segs[s].B, p.segs[s].lda, p.segs[s].ldb, p.segs[s].k, 0, 0}
+                                  : Piece{p.A, p.B, p.lda, p.ldb, p.k, 0, 0};
+            if (pc.k <= 0) continue;
+            pc.k_off = kp;
+            pc.k_pad = ceil_div(pc.k, oz::KPAD) * oz::KPAD;
+            kt += pc.k;
+            kp += pc.k_pad;
+            pieces.push_back(pc);
+        }
+        if (kt == 0) return fail(h, DGT_ERROR_INVALID_VALUE, "grouped product without K");
+        k_total[i] = kt;
+        k_pads[i] = kp;
+        k_pad_max = std::max(k_pad_max, kp);
+    }
+    piece_begin[T] = (int32_t)pieces.size();
+    const int NJ = 2 * (int)pieces.size();  // split jobs: every piece of op(A), then of op(B), per product
     std::vector<oz::Seg> segs;
     std::vector<oz::Group> groups;
     oz2::CrtConst cc;
@@ -513,7 +557,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     // round-robin takes the heaviest tiles early.
     std::vector<int> order(T);
     for (int i = 0; i < T; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return probs[a].k > probs[b].k; });
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return k_total[a] > k_total[b]; });
 
     // scratch: per product planes A | planes B | residues (CRT) (1 KB aligned), then all amax
     // words, all exponents
@@ -529,8 +573,8 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
         Off& o = off[i];
         o.m_pad = ceil_div(p.m, oz::TM) * oz::TM;
         o.n_pad = ceil_div(p.n, oz::TN) * oz::TN;
-        o.k_pad = ceil_div(p.k, oz::KPAD) * oz::KPAD;
-        o.bits = crt ? oz2::sigma_sum_for(S, p.k) : 0;  // sigma_A + sigma_B
+        o.k_pad = k_pads[i];
+        o.bits = crt ? oz2::sigma_sum_for(S, k_total[i]) : 0;  // sigma_A + sigma_B
         if ((int64_t)S * std::max(o.m_pad, o.n_pad) > INT32_MAX) return DGT_ERROR_UNSUPPORTED;
         o.pa = planes;
         planes += up((size_t)S * o.m_pad * o.k_pad, 1024);
@@ -559,15 +603,15 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     auto* exps = (int32_t*)(base + exp_at);
     auto* sched = (int32_t*)(base + sched_at);
 
-    // host tables: GProb[T] (tensor maps inside, 64-byte aligned), SplitJob[2T] and, for CRT,
+    // host tables: GProb[T] (tensor maps inside, 64-byte aligned), SplitJob[NJ] and, for CRT,
     // CrtJob[T], zeroed byte for byte so that padding hashes the same on every call
-    const size_t job_bytes = (size_t)2 * T * sizeof(oz::SplitJob);
+    const size_t job_bytes = (size_t)NJ * sizeof(oz::SplitJob);
     const size_t crt_bytes = crt ? (size_t)T * sizeof(oz2::CrtJob) : 0;
     static thread_local std::vector<oz::GProb> host_gp;
     static thread_local std::vector<oz::SplitJob> host_jobs;
     static thread_local std::vector<oz2::CrtJob> host_crt;
     host_gp.resize(T);
-    host_jobs.resize(2 * (size_t)T);
+    host_jobs.resize((size_t)NJ);
     host_crt.resize(crt ? T : 1);
     std::memset((void*)host_gp.data(), 0, (size_t)T * sizeof(oz::GProb));
     std::memset((void*)host_jobs.data(), 0, job_bytes);
@@ -577,6 +621,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     oz2::CrtJob* cj = host_crt.data();
     int64_t amax_blocks = 0, split_blocks = 0, crt_threads = 0;
     int32_t tiles = 0;
+    int nj = 0;
     for (int r = 0; r < T; ++r) {
         const int i = order[r];
         const OzProblem& p = probs[i];
@@ -605,50 +650,65 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
             g.res = (uint8_t*)(base + o.rs);
             g.res_ld = o.m_pad;
             g.res_plane = o.m_pad * o.n_pad;
-            oz2::CrtJob& c = cj[r];
-            c.res = g.res;
-            c.res_ld = g.res_ld;
-            c.res_plane = g.res_plane;
-            c.m = p.m;
-            c.n = p.n;
-            c.row_exp = g.row_exp;
-            c.col_exp = g.col_exp;
-            c.alpha = p.alpha;
-            c.beta = p.beta;
-            c.C = p.C;
-            c.ldc = p.ldc;
-            c.bits = o.bits;  // the reconstruction's shift takes the sum
-            c.thread_begin = crt_threads;
-            crt_threads += ceil_div(p.m, 4) * p.n;
         }
         tiles += g.tiles_m * g.tiles_n;
         // op(A) is m x k: 'N' -> MN-contiguous; op(B) as its transpose n x k: 'N' -> K-contiguous
         const bool kc[2] = {p.ta, !p.tb};
-        const double* X[2] = {p.A, p.B};
-        const int64_t ld[2] = {p.lda, p.ldb}, MN[2] = {p.m, p.n}, pad[2] = {o.m_pad, o.n_pad};
+        const int64_t MN[2] = {p.m, p.n}, pad[2] = {o.m_pad, o.n_pad};
         const size_t xo[2] = {o.xa, o.xb}, eo[2] = {o.ea, o.eb};
-        void* pl[2] = {pA, pB};
+        char* pl[2] = {(char*)pA, (char*)pB};
         for (int t = 0; t < 2; ++t) {
-            oz::SplitJob& J = jobs[2 * r + t];
-            J.X = X[t];
-            J.ld = ld[t];
-            J.MN = MN[t];
-            J.K = p.k;
-            J.mn_pad = pad[t];
-            J.k_pad = o.k_pad;
-            J.amax = amax + xo[t];
-            J.qn = crt ? amax + amax_words + xo[t] : nullptr;
-            J.exps = exps + eo[t];
-            J.planes = pl[t];
-            J.kcontig = kc[t] ? 1 : 0;
-            J.amax_bx = (int32_t)(kc[t] ? ceil_div(MN[t], 8) : ceil_div(MN[t], 256));
-            J.amax_by = (int32_t)(kc[t] ? 1 : ceil_div(p.k, oz::AMAX_KCHUNK));
-            J.split_bx = (int32_t)ceil_div(pad[t], crt ? oz2::RES_ROWS : 128);
-            J.amax_begin = amax_blocks;
-            J.split_begin = split_blocks;
-            J.bits = t == 0 ? (o.bits + 1) / 2 : o.bits / 2;  // op(A) takes the odd bit
-            amax_blocks += (int64_t)J.amax_bx * J.amax_by;
-            split_blocks += (int64_t)J.split_bx * (o.k_pad / (crt ? oz2::RES_KSPAN : 32));
+            for (int pi = piece_begin[i]; pi < piece_begin[i + 1]; ++pi) {
+                const Piece& pc = pieces[pi];
+                oz::SplitJob& J = jobs[nj++];
+                J.X = t == 0 ? pc.A : pc.B;
+                J.ld = t == 0 ? pc.lda : pc.ldb;
+                J.MN = MN[t];
+                J.K = pc.k;
+                J.mn_pad = pad[t];
+                J.k_pad = pc.k_pad;
+                J.plane_ld = o.k_pad;
+                J.amax = amax + xo[t];
+                J.qn = crt ? amax + amax_words + xo[t] : nullptr;
+                J.exps = exps + eo[t];
+                J.planes = pl[t] + pc.k_off;  // the piece's first column of every plane row
+                J.kcontig = kc[t] ? 1 : 0;
+                J.amax_bx = (int32_t)(kc[t] ? ceil_div(MN[t], 8) : ceil_div(MN[t], 256));
+                J.amax_by = (int32_t)(kc[t] ? 1 : ceil_div(pc.k, oz::AMAX_KCHUNK));
+                J.split_bx = (int32_t)ceil_div(pad[t], crt ? oz2::RES_ROWS : 128);
+                J.amax_begin = amax_blocks;
+                J.split_begin = split_blocks;
+                J.bits = t == 0 ? (o.bits + 1) / 2 : o.bits / 2;  // op(A) takes the odd bit
+                amax_blocks += (int64_t)J.amax_bx * J.amax_by;
+                split_blocks += (int64_t)J.split_bx * (pc.k_pad / (crt ? oz2::RES_KSPAN : 32));
+            }
+        }
+    }
+    // reconstruction jobs in the caller's order, so a stack group's members follow its lead
+    int lead = -1;
+    for (int i = 0; crt && i < T; ++i) {
+        const OzProblem& p = probs[i];
+        const Off& o = off[i];
+        oz2::CrtJob& c = cj[i];
+        c.res = (const uint8_t*)(base + o.rs);
+        c.res_ld = o.m_pad;
+        c.res_plane = o.m_pad * o.n_pad;
+        c.m = p.m;
+        c.n = p.n;
+        c.row_exp = exps + o.ea;
+        c.col_exp = exps + o.eb;
+        c.alpha = p.alpha;
+        c.beta = p.beta;
+        c.C = p.C;
+        c.ldc = p.ldc;
+        c.bits = o.bits;  // the reconstruction's shift takes the sum
+        c.thread_begin = crt_threads;
+        if (p.stack) {
+            cj[lead].count += 1;  // owns no threads: thread_begin is the next lead's
+        } else {
+            lead = i;
+            c.count = 1;
+            crt_threads += ceil_div(p.m, 4) * p.n;
         }
     }
     if (amax_blocks > INT32_MAX || split_blocks > INT32_MAX || crt_threads / 256 > INT32_MAX)
@@ -673,15 +733,15 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
 
     mark(h, 0);
     DGT_CUDA_TRY(h, cudaMemsetAsync(amax, 0, amax_words * 8 * (crt ? 2 : 1), s));
-    oz::amax_grouped<<<(unsigned)amax_blocks, 256, 0, s>>>(d_jobs, 2 * T);
+    oz::amax_grouped<<<(unsigned)amax_blocks, 256, 0, s>>>(d_jobs, NJ);
     h->launches.fetch_add(1);
     DGT_CUDA_TRY(h, cudaGetLastError());
     if (crt) {
-        DGT_CUDA_TRY(h, oz2::launch_qnorm_grouped(s, d_jobs, 2 * T, amax_blocks));
+        DGT_CUDA_TRY(h, oz2::launch_qnorm_grouped(s, d_jobs, NJ, amax_blocks));
         h->launches.fetch_add(1);
-        DGT_CUDA_TRY(h, oz2::launch_split_residues_grouped(s, d_jobs, 2 * T, split_blocks, S, mt));
+        DGT_CUDA_TRY(h, oz2::launch_split_residues_grouped(s, d_jobs, NJ, split_blocks, S, mt));
     } else {
-        oz::split_grouped<<<(unsigned)split_blocks, 128, 0, s>>>(d_jobs, 2 * T, S);
+        oz::split_grouped<<<(unsigned)split_blocks, 128, 0, s>>>(d_jobs, NJ, S);
         DGT_CUDA_TRY(h, cudaGetLastError());
     }
     h->launches.fetch_add(1);

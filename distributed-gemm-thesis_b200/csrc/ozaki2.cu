@@ -191,9 +191,10 @@ __device__ __forceinline__ void qnorm_mn_block(const double* __restrict__ X, int
 
 // K-contiguous operand (element (mn, kk) at X[kk + mn ld]): warp per mn; each lane's run is
 // at most ceil(K / 32) <= 4096 terms.
+// atomic: the row may have other pieces (q zeroed by the caller), so the sum goes in by atomicAdd.
 __device__ __forceinline__ void qnorm_k_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
                                               const unsigned long long* __restrict__ amax,
-                                              unsigned long long* __restrict__ q, int64_t bx) {
+                                              unsigned long long* __restrict__ q, int64_t bx, bool atomic = false) {
     const int64_t mn = bx * (blockDim.x / 32) + threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     if (mn >= MN) return;
@@ -208,7 +209,12 @@ __device__ __forceinline__ void qnorm_k_block(const double* __restrict__ X, int6
     unsigned long long t = (unsigned long long)acc;
 #pragma unroll
     for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (lane == 0) q[mn] = t;
+    if (lane == 0) {
+        if (!atomic)
+            q[mn] = t;
+        else if (t)
+            atomicAdd(q + mn, t);
+    }
 }
 
 __global__ void qnorm_mn_contig(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K, int kchunk,
@@ -225,7 +231,7 @@ __global__ void __launch_bounds__(256) qnorm_grouped(const oz::SplitJob* __restr
     const oz::SplitJob& J = jobs[oz::find_job(jobs, njobs, blk, false)];
     const int64_t local = blk - J.amax_begin;
     if (J.kcontig)
-        qnorm_k_block(J.X, J.ld, J.MN, J.K, J.amax, J.qn, local);
+        qnorm_k_block(J.X, J.ld, J.MN, J.K, J.amax, J.qn, local, true);
     else
         qnorm_mn_block(J.X, J.ld, J.MN, J.K, oz::AMAX_KCHUNK, J.amax, J.qn, local % J.amax_bx, local / J.amax_bx);
 }
@@ -248,13 +254,14 @@ __device__ __forceinline__ int row_scale_exp(unsigned long long am, unsigned lon
 
 // ---- device: residue planes ----------------------------------------------------------------------
 // Plane j holds (A' mod p_j) in the symmetric range as int8 at [j][mn][kk] (K-major, row
-// length k_pad, mn_pad rows, zero padded).  A thread produces RES_ELEMS consecutive kk of one
+// stride pld >= k_pad, mn_pad rows, zero padded to k_pad; pld > k_pad for one piece of a
+// concatenated K).  A thread produces RES_ELEMS consecutive kk of one
 // mn; the RES_TPR adjacent lanes of a row write one whole 32-byte sector per plane together
 // (lanes that wrote parts of a sector each made L2 fetch the sector from DRAM first).  The
 // seg == 0, by == 0 threads also write exps[mn].
 template <bool K_CONTIG>
 __device__ __forceinline__ void residue_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                                              int64_t mn_pad, int64_t k_pad, int nmod, int sigma,
+                                              int64_t mn_pad, int64_t k_pad, int64_t pld, int nmod, int sigma,
                                               const unsigned long long* __restrict__ amax,
                                               const unsigned long long* __restrict__ qn, int32_t* __restrict__ exps,
                                               int8_t* __restrict__ planes, const ModTable& mt, int64_t bx,
@@ -275,8 +282,8 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
     // it rounds to the integer 0 either way); the general scaling otherwise
     const bool direct = sc >= -1022 && sc <= 1023;
     const double fsc = direct ? oz::pow2i(sc) : 0.0;
-    const int64_t plane = mn_pad * k_pad;
-    int8_t* out = planes + mn * k_pad + k0;
+    const int64_t plane = mn_pad * pld;
+    int8_t* out = planes + mn * pld + k0;
     if (!live || k0 >= K) {  // padding (or a non-finite row): zero residues, no arithmetic
 #pragma unroll 4
         for (int j = 0; j < nmod; ++j, out += plane) {
@@ -338,7 +345,7 @@ __global__ void __launch_bounds__(128) split_residues(const double* __restrict__
                                                       const unsigned long long* __restrict__ qn,
                                                       int32_t* __restrict__ exps, int8_t* __restrict__ planes,
                                                       const __grid_constant__ ModTable mt) {
-    residue_block<K_CONTIG>(X, ld, MN, K, mn_pad, k_pad, nmod, sigma, amax, qn, exps, planes, mt, blockIdx.x,
+    residue_block<K_CONTIG>(X, ld, MN, K, mn_pad, k_pad, k_pad, nmod, sigma, amax, qn, exps, planes, mt, blockIdx.x,
                             blockIdx.y);
 }
 
@@ -350,10 +357,10 @@ __global__ void __launch_bounds__(128) split_residues_grouped(const oz::SplitJob
     const int64_t local = blk - J.split_begin;
     const int64_t bx = local % J.split_bx, by = local / J.split_bx;
     if (J.kcontig)
-        residue_block<true>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, nmod, J.bits, J.amax, J.qn, J.exps,
+        residue_block<true>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, J.plane_ld, nmod, J.bits, J.amax, J.qn, J.exps,
                             (int8_t*)J.planes, mt, bx, by);
     else
-        residue_block<false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, nmod, J.bits, J.amax, J.qn, J.exps,
+        residue_block<false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, J.plane_ld, nmod, J.bits, J.amax, J.qn, J.exps,
                              (int8_t*)J.planes, mt, bx, by);
 }
 
@@ -551,6 +558,28 @@ __device__ __forceinline__ void crt_quad(const uint8_t* __restrict__ res, int64_
     }
 }
 
+// The four values of rows row0 .. row0+3 of column col of one product, before alpha (rows at
+// or past m: 0).
+template <int NW, int NM>
+__device__ __forceinline__ void crt_vals(const CrtJob& J, int64_t row0, int64_t col, const CrtConst& cc,
+                                         double (&v)[4]) {
+    uint32_t rr[MAX_MODULI];
+#pragma unroll
+    for (int j = 0; j < MAX_MODULI; ++j)
+        rr[j] = (NM ? j < NM : j < cc.n)
+                    ? *reinterpret_cast<const uint32_t*>(J.res + j * J.res_plane + col * J.res_ld + row0)
+                    : 0u;
+    const int f = J.col_exp[col];
+#pragma unroll
+    for (int e4 = 0; e4 < 4; ++e4) {
+        v[e4] = 0.0;
+        if (row0 + e4 >= J.m) continue;
+        const int e = J.row_exp[row0 + e4];
+        v[e4] = (e == oz::EXP_NONFINITE || f == oz::EXP_NONFINITE) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                                  : crt_value<NW, NM>(rr, e4, cc, e + f - J.bits);
+    }
+}
+
 // Thread per 4 consecutive rows of one column of C.
 template <int NW, int NM>
 __global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
@@ -583,8 +612,32 @@ __global__ void __launch_bounds__(256) crt_grouped(const CrtJob* __restrict__ jo
     const CrtJob& J = jobs[lo];
     const int64_t local = idx - J.thread_begin, quads = (J.m + 3) / 4;
     if (local >= quads * J.n) return;
-    crt_quad<NW, NM>(J.res, J.res_ld, J.res_plane, J.m, (local % quads) * 4, local / quads, J.row_exp, J.col_exp, J.bits,
-                 J.alpha, J.beta, J.C, J.ldc, cc);
+    const int64_t row0 = (local % quads) * 4, col = local / quads;
+    if (J.count <= 1) {
+        crt_quad<NW, NM>(J.res, J.res_ld, J.res_plane, J.m, row0, col, J.row_exp, J.col_exp, J.bits, J.alpha, J.beta,
+                         J.C, J.ldc, cc);
+        return;
+    }
+    // a stack group: stack 0 as a plain product (alpha v + beta C), then each further stack's
+    // alpha v added in stack order -- the stack reduction's order
+    double v[4], out[4];
+    crt_vals<NW, NM>(J, row0, col, cc, v);
+    // (explicitly rounded products and sums: a contracted alpha v + out would skip the rounding
+    // of alpha v that the stack-by-stack form makes)
+    double* cp = J.C + row0 + col * J.ldc;
+#pragma unroll
+    for (int e4 = 0; e4 < 4; ++e4)
+        out[e4] = (J.beta != 0.0 && row0 + e4 < J.m) ? fma(J.alpha, v[e4], __dmul_rn(J.beta, cp[e4]))
+                                                     : __dmul_rn(J.alpha, v[e4]);
+    for (int g = 1; g < J.count; ++g) {
+        const CrtJob& G = jobs[lo + g];
+        crt_vals<NW, NM>(G, row0, col, cc, v);
+#pragma unroll
+        for (int e4 = 0; e4 < 4; ++e4) out[e4] = __dadd_rn(out[e4], __dmul_rn(G.alpha, v[e4]));
+    }
+#pragma unroll
+    for (int e4 = 0; e4 < 4; ++e4)
+        if (row0 + e4 < J.m) cp[e4] = out[e4];
 }
 
 cudaError_t launch_qnorm_grouped(cudaStream_t s, const oz::SplitJob* jobs, int njobs, int64_t blocks) {

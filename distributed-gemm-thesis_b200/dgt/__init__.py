@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libdgt.so")
 SUCCESS, INVALID_VALUE, UNSUPPORTED, CUDA_ERROR, TIMEOUT, ALLOC, NOT_INITIALIZED = range(7)
 FP64_NATIVE, FP64_OZAKI_INT8, FP64_OZAKI_BF16, FP64_AUTO, FP64_OZAKI2_INT8 = range(5)
 FP32_SIMT, FP32_BF16X1, FP32_BF16X3 = range(3)
-TUNE_DMMA_VARIANT, TUNE_OZAKI_SLICES, TUNE_PROFILE, TUNE_OZAKI_VARIANT, TUNE_TEST_STALL = range(5)
+TUNE_DMMA_VARIANT, TUNE_OZAKI_SLICES, TUNE_PROFILE, TUNE_OZAKI_VARIANT, TUNE_TEST_STALL, TUNE_FUSE_STEPS = range(6)
 
 _c_i64 = ctypes.c_int64
 _c_i32 = ctypes.c_int32
@@ -88,6 +88,9 @@ SIGNATURES = [
                                     _vp, _c_i32]),
     ("dgt_cannon25d", _c_i32, [_vp, _c_i64, _c_i32, _c_i32, ctypes.c_char, ctypes.c_char, ctypes.c_double, _vp, _vp,
                                ctypes.c_double, _vp, _c_i32, ctypes.c_int]),
+    ("dgt_cannon25d_batch", _c_i32, [_vp, _c_i64, _c_i32, _c_i32, ctypes.c_char, ctypes.c_char, ctypes.c_double,
+                                     _vp, _vp, ctypes.c_double, _vp, _c_i32, ctypes.POINTER(GemmDesc), _c_i32,
+                                     ctypes.c_int]),
     ("dgt_cannon_schedule", _c_i32, [_c_i32] * 5 + [ctypes.POINTER(_c_i32)]),
     ("dgt_pack_block_cyclic", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _c_i64, _vp, _vp]),
     ("dgt_unpack_block_cyclic", _c_i32, [_vp, _c_i64, _c_i64, _c_i64, _c_i64, _c_i32, _c_i32, _vp, _c_i64, _vp,
@@ -258,13 +261,17 @@ class Handle:
         self._check(self.lib.dgt_sgemm(self.h, ta.encode(), tb.encode(), m, n, k, ctypes.byref(a), _vp(A), lda,
                                        _vp(B), ldb, ctypes.byref(b), _vp(C), ldc, mode))
 
-    def dgemm_grouped(self, descs, mode=FP64_NATIVE, slices=7):
-        arr = (GemmDesc * len(descs))()
+    @staticmethod
+    def _desc_array(descs):
+        arr = (GemmDesc * max(1, len(descs)))()
         for i, d in enumerate(descs):
             arr[i] = GemmDesc(d["m"], d["n"], d["k"], d.get("alpha", 1.0), d.get("beta", 0.0), d["A"], d["lda"],
                               d["B"], d["ldb"], d["C"], d["ldc"], d.get("transa", "N").encode(),
                               d.get("transb", "N").encode())
-        self._check(self.lib.dgt_dgemm_grouped(self.h, len(descs), arr, mode, slices))
+        return arr
+
+    def dgemm_grouped(self, descs, mode=FP64_NATIVE, slices=7):
+        self._check(self.lib.dgt_dgemm_grouped(self.h, len(descs), self._desc_array(descs), mode, slices))
 
     def summa(self, p, q, mb, nb, kb, M, N, K, alpha, A_locals, lldA, B_locals, lldB, beta, C_locals, lldC,
               mode=FP64_NATIVE, slices=7):
@@ -295,6 +302,13 @@ class Handle:
                   slices=7):
         self._check(self.lib.dgt_cannon25d(self.h, M, p, c, ta.encode(), tb.encode(), alpha, _ptrs(A_tiles),
                                            _ptrs(B_tiles), beta, _ptrs(C_tiles), mode, slices))
+
+    def cannon25d_batch(self, M, p, c, alpha, A_tiles, B_tiles, beta, C_tiles, descs, ta="N", tb="N",
+                        mode=FP64_NATIVE, slices=7):
+        """The 2.5D Cannon multiply plus the grouped products `descs` in one grouped launch."""
+        self._check(self.lib.dgt_cannon25d_batch(self.h, M, p, c, ta.encode(), tb.encode(), alpha, _ptrs(A_tiles),
+                                                 _ptrs(B_tiles), beta, _ptrs(C_tiles), len(descs),
+                                                 self._desc_array(descs), mode, slices))
 
     # -- layout ----------------------------------------------------------------------------
     def pack_block_cyclic(self, M, N, mb, nb, p, q, G, ldg, locals_, lld):

@@ -92,6 +92,7 @@ def test_new_entries_report_bad_arguments_without_a_device():
     assert lib.dgt_summa_rank(None, ctypes.byref(L), 0, 4, 4, 4, 1.0, z, z, z, z, 0.0, z, 4, 0, 7) == NI
     assert lib.dgt_cannon25d_rank(None, 4, 1, 1, 0, b"N", b"N", 1.0, z, z, 0.0, z, 0, 7) == NI
     assert lib.dgt_reduce_tiles(None, z, z, 1, 4) == NI
+    assert lib.dgt_cannon25d_batch(None, 4, 1, 1, b"N", b"N", 1.0, z, z, 0.0, z, 0, None, 0, 7) == NI
     ptr, h = ctypes.c_void_p(), ctypes.create_string_buffer(64)
     assert lib.dgt_ipc_alloc(0, ctypes.byref(ptr), h) == dgt.INVALID_VALUE
     assert lib.dgt_ipc_alloc(64, None, h) == dgt.INVALID_VALUE
