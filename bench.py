@@ -511,9 +511,11 @@ def workload_fp32(args):
 
 def workload_batching(args):
     """Batching: virtual 2.5D Cannon 4x4x2 on M = N = K = 8192 and 256 independent products
-    with M, N, K log-uniform in [128, 4096], U[-1,1) entries; native DMMA and INT8 Ozaki
-    (S = 7 and 8), each as one grouped call; eager vs CUDA-graph replay; per-product
-    emulation shown for contrast; errors vs the host FP64 GEMM on sampled rows."""
+    with M, N, K log-uniform in [128, 4096], U[-1,1) entries; native DMMA, INT8 slices
+    (S = 7 and 8) and CRT residues (14-16 moduli), each as one grouped call, and then both
+    workloads together in one dgt_cannon25d_batch call (native: one persistent launch); eager
+    vs CUDA-graph replay; per-product emulation shown for contrast; errors vs the host FP64
+    GEMM on sampled rows."""
     import numpy as np
 
     torch, dgt, h = _setup()
@@ -576,8 +578,6 @@ def workload_batching(args):
                             "graph_tflops": 2.0 * M ** 3 / (gms * 1e-3) / 1e12, "kernel_launches": launches,
                             "kernel_variant": best[0], "max_rel": err[0], "fro_rel": err[1]}
         res["cannon_4x4x2_8192"] = cannon
-        del dA, dB, dC, tA, tB, tC
-        torch.cuda.empty_cache()
 
         # ---- 256 independent products ----
         rng = np.random.default_rng(SEED + 5)
@@ -632,6 +632,44 @@ def workload_batching(args):
         ms = _time_ms(torch, per, 3, warm=1)
         grouped["int8_s8_one_call_per_product"] = {"tflops": flops / (ms * 1e-3) / 1e12, "ms": ms}
         res["grouped_256"] = {"flops": flops, "methods": grouped}
+
+        # ---- both in ONE grouped launch (dgt_cannon25d_batch): natively one persistent launch
+        # with the stack reduction inside; CRT one grouped pass; slices as two calls ----
+        both = {}
+        total = flops + 2.0 * M ** 3
+        pA, pB, pC = [x.data_ptr() for x in tA], [x.data_ptr() for x in tB], [x.data_ptr() for x in tC]
+        for name, mode, S in (("native", dgt.FP64_NATIVE, 7), ("int8_s8", dgt.FP64_OZAKI_INT8, 8),
+                              ("crt_n14", dgt.FP64_OZAKI2_INT8, 14), ("crt_n15", dgt.FP64_OZAKI2_INT8, 15),
+                              ("crt_n16", dgt.FP64_OZAKI2_INT8, 16)):
+            f = lambda: h.cannon25d_batch(M, p, c, 1.0, pA, pB, 0.0, pC, descs, mode=mode, slices=S)
+            # tile shape / kernel variant: the fastest for this batch
+            knob = dgt.TUNE_DMMA_VARIANT if mode == dgt.FP64_NATIVE else dgt.TUNE_OZAKI_VARIANT
+            cands = (0, 1, 2, 7, 10, 12) if mode == dgt.FP64_NATIVE else (0, 1, 5, 7)
+            best = None
+            for v in cands:
+                h.set_tuning(knob, v)
+                t = _time_ms(torch, f, 2, warm=1)
+                if best is None or t < best[1]:
+                    best = (v, t)
+            h.set_tuning(knob, best[0])
+            f()
+            h.unpack_cannon2d(M, p, dC.data_ptr(), pC)
+            torch.cuda.synchronize()
+            h.check_device()
+            errs = [_rel(_rows_of(dC, rows, (M, M)), want)]
+            errs += [_rel(_rows_of(outs[i], rr, (int(dims[i][0]), int(dims[i][1]))), w) for i, rr, w in checks]
+            n0 = h.launch_count()
+            f()
+            launches = h.launch_count() - n0
+            ms = _time_ms(torch, f, 5)
+            gms = graph_ms(f)
+            both[name] = {"tflops": total / (ms * 1e-3) / 1e12, "ms": ms, "graph_ms": gms,
+                          "graph_tflops": total / (gms * 1e-3) / 1e12, "kernel_launches": launches,
+                          "kernel_variant": best[0], "max_rel": max(e[0] for e in errs),
+                          "fro_rel": max(e[1] for e in errs)}
+        res["cannon_plus_256_one_launch"] = {"flops": total, "methods": both}
+        del dA, dB, dC, tA, tB, tC
+        torch.cuda.empty_cache()
     h.set_stream(0)
     clocks = sampler.stop()
     print(json.dumps({"workload": "batching", "unit": "TFLOP/s (FP64-equivalent)", "dtype": "f64",

@@ -283,6 +283,10 @@ dgt_status dgt_destroy(dgt_handle_t h) {
         if (e) cudaEventDestroy(e);
     for (auto& cs : h->copy_stream)
         if (cs) cudaStreamDestroy(cs);
+    for (auto& e : h->work_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& ws : h->work_stream)
+        if (ws) cudaStreamDestroy(ws);
     for (void* w : h->ws)
         if (w) cudaFree(w);
     for (auto& t : h->tables) cudaFree(t.ptr);
@@ -339,6 +343,10 @@ dgt_status dgt_set_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t value) {
         case DGT_TUNE_FUSE_STEPS:
             h->fuse_steps = value != 0;
             return DGT_SUCCESS;
+        case DGT_TUNE_CRT_PANELS:
+            if (value < 0 || value > 8) return fail(h, DGT_ERROR_INVALID_VALUE, "CRT panel count must be in [0, 8]");
+            h->crt_panels = value;
+            return DGT_SUCCESS;
     }
     return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
 }
@@ -364,6 +372,7 @@ dgt_status dgt_get_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t* value) {
         case DGT_TUNE_OZAKI_VARIANT: *value = h->ozaki_variant; return DGT_SUCCESS;
         case DGT_TUNE_TEST_STALL: *value = h->test_stall; return DGT_SUCCESS;
         case DGT_TUNE_FUSE_STEPS: *value = h->fuse_steps ? 1 : 0; return DGT_SUCCESS;
+        case DGT_TUNE_CRT_PANELS: *value = h->crt_panels; return DGT_SUCCESS;
     }
     return fail(h, DGT_ERROR_INVALID_VALUE, "unknown tuning knob");
 }

@@ -45,6 +45,7 @@ struct dgt_context {
     bool profile = false;  // record phase events (DGT_TUNE_PROFILE)
     int test_stall = 0;    // failure-path test hook (DGT_TUNE_TEST_STALL)
     bool fuse_steps = true; // DGT_TUNE_FUSE_STEPS
+    int crt_panels = 0;     // DGT_TUNE_CRT_PANELS (0: the library's choice)
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // split start, gemm start, gemm end
     bool ev_split = false;  // last call had a split phase
     std::string last_error;
@@ -57,6 +58,10 @@ struct dgt_context {
     // dgt_dgemm_host: copy-in and copy-out streams and its events, created on first use
     cudaStream_t copy_stream[2] = {nullptr, nullptr};
     cudaEvent_t copy_ev[24] = {};
+    // the CRT product in op(B) panels: split and reconstruction streams and their events,
+    // created on first use
+    cudaStream_t work_stream[2] = {nullptr, nullptr};
+    cudaEvent_t work_ev[1 + 3 * 8] = {};
     std::atomic<int64_t> launches{0};
     std::map<dgt::TuneKey, dgt::TuneEntry> tune;
     // device copies of launch tables (grouped problems, Ozaki jobs and schedules), keyed by

@@ -271,6 +271,24 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
     const int row = threadIdx.x / RES_TPR, seg = threadIdx.x % RES_TPR;
     const int64_t mn = bx * RES_ROWS + row;
     const int64_t k0 = by * RES_KSPAN + seg * E;
+    // MN-contiguous operand: the block's RES_ROWS x RES_KSPAN tile comes in through shared
+    // memory, every warp load one kk over RES_ROWS consecutive mn (a thread's own kk run would
+    // touch one 8-byte word per row); rows of RES_ROWS + 1 doubles keep the reads at two
+    // wavefronts per warp
+    constexpr int TLD = RES_ROWS + 1;
+    __shared__ double tile[K_CONTIG ? 1 : RES_KSPAN * TLD];
+    if constexpr (!K_CONTIG) {
+        static_assert(128 % RES_ROWS == 0 && RES_KSPAN % (128 / RES_ROWS) == 0, "residue split: tile shape");
+        constexpr int KSTEP = 128 / RES_ROWS;
+        const int lm = threadIdx.x % RES_ROWS, kq = threadIdx.x / RES_ROWS;
+        const int64_t tm = bx * RES_ROWS + lm, tk0 = by * RES_KSPAN;
+#pragma unroll
+        for (int i = 0; i < RES_KSPAN / KSTEP; ++i) {
+            const int kl = kq + KSTEP * i;
+            tile[kl * TLD + lm] = (tm < MN && tk0 + kl < K) ? X[tm + (tk0 + kl) * ld] : 0.0;
+        }
+        __syncthreads();
+    }
     if (mn >= mn_pad) return;
     int e = 0, sc = 0;  // sc: this row's scale exponent s
     if (mn < MN) {
@@ -302,7 +320,7 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
     for (int i = 0; i < E; ++i) {
         const int64_t kk = k0 + i;
         double a = 0.0;
-        if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : X[mn + kk * ld];
+        if (live && kk < K) a = K_CONTIG ? X[kk + mn * ld] : tile[(seg * E + i) * TLD + row];
         // y = a 2^sc exactly; Y = rn(y) = yh 2^40 + yl, |yh|, |yl| <= 2^39
         const double y = live ? (direct ? a * fsc : oz::scale2(a, sc)) : 0.0;
         const double yh = rint(y * 0x1p-40);
@@ -582,7 +600,7 @@ __device__ __forceinline__ void crt_vals(const CrtJob& J, int64_t row0, int64_t 
 
 // Thread per 4 consecutive rows of one column of C.
 template <int NW, int NM>
-__global__ void __launch_bounds__(256) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
+__global__ void __launch_bounds__(128) crt_reconstruct(const uint8_t* __restrict__ res, int64_t res_ld,
                                                        int64_t res_plane, int64_t m, int64_t n,
                                                        const int32_t* __restrict__ row_exp,
                                                        const int32_t* __restrict__ col_exp, int ssum, double alpha,
@@ -795,10 +813,9 @@ dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int 
 }
 
 // Residue GEMM of split operands (op(A) planes for sh.m rows, op(B) planes for n columns
-// padded to n_pad) and the reconstruction C = alpha C' + beta C.
-dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
-                           const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
-                           uint8_t* res, double alpha, double beta, double* C, int64_t ldc, int32_t* sched) {
+// padded to n_pad) into res.
+static dgt_status ozaki2_residue_gemm(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+                                      const int8_t* planesA, const int8_t* planesB, uint8_t* res, int32_t* sched) {
     using namespace oz2;
     const int nmod = sh.nmod, tkb = 128;
     const int64_t m = sh.m, m_pad = sh.m_pad, k_pad = sh.k_pad;
@@ -840,13 +857,22 @@ dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, i
         le = launch_residue_gemm<oz::OzCfg<8, 128, 4>>(tmA, tmB, prm, h->num_sms, s);
     h->launches.fetch_add(1);
     if (le != cudaSuccess) return cuda_fail(h, le, "residue GEMM launch");
-    mark(h, 2);
+    return DGT_SUCCESS;
+}
+
+// The reconstruction C = alpha C' + beta C of n columns from their residues.
+static dgt_status ozaki2_reconstruct(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+                                     const uint8_t* res, const int32_t* expA, const int32_t* expB, double alpha,
+                                     double beta, double* C, int64_t ldc) {
+    using namespace oz2;
+    const int nmod = sh.nmod;
+    const int64_t m = sh.m, m_pad = sh.m_pad;
     const int64_t threads = ceil_div(m, 4) * n;
-    const unsigned blocks = (unsigned)ceil_div(threads, 256);
+    const unsigned blocks = (unsigned)ceil_div(threads, 128);
     const CrtConst& cc = sh.cc;
     const int bits = sh.sa + sh.sb;
 #define DGT_CRT_LAUNCH(NW, NM)                                                                            \
-    crt_reconstruct<NW, NM><<<blocks, 256, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta, \
+    crt_reconstruct<NW, NM><<<blocks, 128, 0, s>>>(res, m_pad, m_pad * n_pad, m, n, expA, expB, bits, alpha, beta, \
                                                    C, ldc, cc)
     if (nmod == 14)
         DGT_CRT_LAUNCH(4, 14);
@@ -873,6 +899,16 @@ dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, i
     h->launches.fetch_add(1);
     DGT_CUDA_TRY(h, cudaGetLastError());
     return DGT_SUCCESS;
+}
+
+// Residue GEMM and reconstruction of one op(B) panel on one stream.
+dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+                           const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
+                           uint8_t* res, double alpha, double beta, double* C, int64_t ldc, int32_t* sched) {
+    dgt_status st = ozaki2_residue_gemm(h, s, sh, n, n_pad, planesA, planesB, res, sched);
+    if (st != DGT_SUCCESS) return st;
+    mark(h, 2);
+    return ozaki2_reconstruct(h, s, sh, n, n_pad, res, expA, expB, alpha, beta, C, ldc);
 }
 
 int64_t ozaki2_n_pad(int64_t n) { return ceil_div(n, oz::TN) * oz::TN; }
@@ -925,12 +961,112 @@ Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws) {
     return w;
 }
 
+static dgt_status ensure_work_streams(dgt_context* h) {
+    for (auto& ws : h->work_stream)
+        if (!ws) DGT_CUDA_TRY(h, cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
+    for (auto& e : h->work_ev)
+        if (!e) DGT_CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return DGT_SUCCESS;
+}
+
+// Panels of op(B) for a device-resident CRT product: the knob's count, else one piece.  (At
+// 16384^3, 14 moduli, the CTA-pair kernel: 54.1 ms in one piece, 55.1 ms in 2 or 4 panels,
+// 57.1 ms in 8 -- the split and reconstruction blocks that share the SMs slow the residue
+// GEMM about as much as they take off the critical path; its 167 registers x 320 threads leave
+// room for one 128-thread side block per SM.)
+static int crt_panel_count(const dgt_context* h, int64_t, int64_t, int64_t) {
+    return h->crt_panels > 0 ? h->crt_panels : 1;
+}
+
+// The CRT product with op(B) in np column panels of whole GEMM tiles.  On the handle's
+// stream: the split of op(A), then panel by panel the residue GEMM.  On side streams: the
+// splits of op(B)'s panels, in order (panel p + 1's while the GEMM runs panel p), and each
+// panel's reconstruction once its GEMM is done, while the GEMM runs the next panel.  The
+// ALU-bound split and reconstruction kernels so share the SMs with the tensor-bound GEMM
+// instead of running before and after it.  Two residue buffers alternate: panel p's GEMM
+// waits for panel p - 2's reconstruction.  The side streams fork from and join back into the
+// handle's stream through events, so the whole call can be captured in a CUDA graph.  Every
+// kernel computes what the one-piece form does for its columns: the results are identical.
+static dgt_status ozaki2_dgemm_panels(dgt_context* h, const Oz2Shape& sh, int np, bool ta, bool tb, int64_t n,
+                                      double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
+                                      double beta, double* C, int64_t ldc) {
+    const int64_t pw = ceil_div(ceil_div(n, np), oz::TN) * oz::TN;  // panel width: whole tiles
+    np = (int)ceil_div(n, pw);
+    auto up = [](size_t x) { return (x + 1023) / 1024 * 1024; };
+    const size_t pa = up((size_t)sh.nmod * sh.m_pad * sh.k_pad), pbp = up((size_t)sh.nmod * pw * sh.k_pad);
+    const size_t xa = up((size_t)sh.m * 8), xb = up((size_t)n * 8), ea = up((size_t)sh.m * 4), eb = up((size_t)n * 4);
+    const size_t rs = up((size_t)sh.nmod * sh.m_pad * pw);
+    const size_t bytes = pa + np * pbp + 2 * (xa + xb) + ea + eb + 2 * rs + 1024;
+    if (bytes > ozaki2_carve(sh, n, sh.n_pad, nullptr).bytes) return DGT_ERROR_UNSUPPORTED;  // one piece instead
+    void* ws = nullptr;
+    dgt_status st = ensure_workspace(h, bytes, &ws, 0);
+    if (st != DGT_SUCCESS) return st;
+    if ((st = ensure_work_streams(h)) != DGT_SUCCESS) return st;
+    char* p = (char*)ws;
+    int8_t* planesA = (int8_t*)p;
+    int8_t* planesB = (int8_t*)(p + pa);
+    p += pa + np * pbp;
+    auto* amaxA = (unsigned long long*)p;
+    auto* amaxB = (unsigned long long*)(p + xa);
+    auto* qnA = (unsigned long long*)(p + xa + xb);
+    auto* qnB = (unsigned long long*)(p + 2 * xa + xb);
+    p += 2 * (xa + xb);
+    auto* expA = (int32_t*)p;
+    auto* expB = (int32_t*)(p + ea);
+    uint8_t* res[2] = {(uint8_t*)(p + ea + eb), (uint8_t*)(p + ea + eb + rs)};
+    auto* sched = (int32_t*)(p + ea + eb + 2 * rs);
+
+    cudaStream_t s = h->stream, ss = h->work_stream[0], sr = h->work_stream[1];
+    cudaEvent_t* fork = &h->work_ev[0];
+    cudaEvent_t* split_done = &h->work_ev[1];
+    cudaEvent_t* gemm_done = &h->work_ev[1 + 8];
+    cudaEvent_t* recon_done = &h->work_ev[1 + 16];
+    mark(h, 0);
+    DGT_CUDA_TRY(h, cudaEventRecord(*fork, s));
+    DGT_CUDA_TRY(h, cudaStreamWaitEvent(ss, *fork, 0));
+    DGT_CUDA_TRY(h, cudaStreamWaitEvent(sr, *fork, 0));
+    // op(B)'s panels: 'N' -> columns n0.. at B + n0 ldb (K-contiguous), 'T' -> rows n0.. at B + n0
+    for (int q = 0; q < np; ++q) {
+        const int64_t n0 = q * pw, w = std::min(pw, n - n0);
+        const double* X = tb ? B + n0 : B + n0 * ldb;
+        st = ozaki2_split(h, ss, sh, sh.sb, X, ldb, w, pw, !tb, amaxB + n0, qnB + n0, expB + n0,
+                          planesB + q * pbp);
+        if (st != DGT_SUCCESS) return st;
+        DGT_CUDA_TRY(h, cudaEventRecord(split_done[q], ss));
+    }
+    st = ozaki2_split(h, s, sh, sh.sa, A, lda, sh.m, sh.m_pad, ta, amaxA, qnA, expA, planesA);
+    if (st != DGT_SUCCESS) return st;
+    for (int q = 0; q < np; ++q) {
+        const int64_t n0 = q * pw, w = std::min(pw, n - n0);
+        DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, split_done[q], 0));
+        if (q >= 2) DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, recon_done[q - 2], 0));
+        st = ozaki2_residue_gemm(h, s, sh, w, pw, planesA, planesB + q * pbp, res[q & 1], sched);
+        if (st != DGT_SUCCESS) return st;
+        DGT_CUDA_TRY(h, cudaEventRecord(gemm_done[q], s));
+        DGT_CUDA_TRY(h, cudaStreamWaitEvent(sr, gemm_done[q], 0));
+        st = ozaki2_reconstruct(h, sr, sh, w, pw, res[q & 1], expA, expB + n0, alpha, beta, C + n0 * ldc, ldc);
+        if (st != DGT_SUCCESS) return st;
+        DGT_CUDA_TRY(h, cudaEventRecord(recon_done[q], sr));
+    }
+    // join: the last reconstruction (every earlier one precedes it on its stream; the splits
+    // precede the GEMMs that waited for them)
+    DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, recon_done[np - 1], 0));
+    mark(h, 2);
+    return DGT_SUCCESS;
+}
+
 static dgt_status ozaki2_dgemm_chunk(dgt_context* h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
                                      double alpha, const double* A, int64_t lda, const double* B, int64_t ldb,
                                      double beta, double* C, int64_t ldc, int nmod) {
     Oz2Shape sh;
     dgt_status st = ozaki2_shape(h, m, n, k, nmod, sh);
     if (st != DGT_SUCCESS) return st;
+    const int np = crt_panel_count(h, m, n, k);
+    if (np > 1 && n > oz::TN) {
+        // (within the one-piece form's workspace: dgt_dgemm_workspace_size stays a bound)
+        st = ozaki2_dgemm_panels(h, sh, std::min(np, 8), ta, tb, n, alpha, A, lda, B, ldb, beta, C, ldc);
+        if (st != DGT_ERROR_UNSUPPORTED) return st;
+    }
     void* ws = nullptr;
     if ((st = ensure_workspace(h, ozaki2_carve(sh, n, sh.n_pad, nullptr).bytes, &ws, 0)) != DGT_SUCCESS) return st;
     const Oz2Work w = ozaki2_carve(sh, n, sh.n_pad, ws);

@@ -16,7 +16,8 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libdgt.so")
 SUCCESS, INVALID_VALUE, UNSUPPORTED, CUDA_ERROR, TIMEOUT, ALLOC, NOT_INITIALIZED = range(7)
 FP64_NATIVE, FP64_OZAKI_INT8, FP64_OZAKI_BF16, FP64_AUTO, FP64_OZAKI2_INT8 = range(5)
 FP32_SIMT, FP32_BF16X1, FP32_BF16X3 = range(3)
-TUNE_DMMA_VARIANT, TUNE_OZAKI_SLICES, TUNE_PROFILE, TUNE_OZAKI_VARIANT, TUNE_TEST_STALL, TUNE_FUSE_STEPS = range(6)
+TUNE_DMMA_VARIANT, TUNE_OZAKI_SLICES, TUNE_PROFILE, TUNE_OZAKI_VARIANT, TUNE_TEST_STALL, TUNE_FUSE_STEPS, \
+    TUNE_CRT_PANELS = range(7)
 
 _c_i64 = ctypes.c_int64
 _c_i32 = ctypes.c_int32

@@ -1,9 +1,10 @@
 """CUDA-graph capture of the step schedules: after eager warm-up passes of the sequence
 (the first sizes the handle's workspace, the second runs with the final workspace and so
-leaves every launch table resident), dgt_dgemm (native and Ozaki),
-dgt_cannon25d (native, and emulated as one grouped Ozaki pass per step) and
-dgt_dgemm_grouped (native and grouped Ozaki) issue only capturable work, so the whole batch
-can be captured once and replayed; replay results equal the eager results bit for bit."""
+leaves every launch table resident), dgt_dgemm (native, Ozaki slices, and CRT in op(B)
+panels on forked side streams), dgt_cannon25d (native: one cooperative launch with the stack
+reduction inside; slices: one grouped pass per step), dgt_cannon25d_batch (native and CRT)
+and dgt_dgemm_grouped (native and grouped Ozaki) issue only capturable work, so the whole
+batch can be captured once and replayed; replay results equal the eager results bit for bit."""
 import numpy as np
 import pytest
 
@@ -20,7 +21,7 @@ def test_capture_and_replay_all_paths():
     m = n = k = 512
     A, B, C = O.uniform((m, k), 1), O.uniform((k, n), 2), O.uniform((m, n), 3)
     dA, dB = dev(A), dev(B)
-    outs = {name: dev(C) for name in ("native", "ozaki")}
+    outs = {name: dev(C) for name in ("native", "ozaki", "crt_panels")}
     # Cannon 4x4x2 on M = 512
     M, p, c = 512, 4, 2
     lm = M // p
@@ -46,6 +47,11 @@ def test_capture_and_replay_all_paths():
     rkeep = [dev(O.uniform((d["m"], d["n"]), 700 + i)) for i, d in enumerate(gdesc)]
     rdesc = [dict(d, C=ptr(c)) for d, c in zip(gdesc, rkeep)]
     rC0 = [x.clone() for x in rkeep]
+    # Cannon plus 6 of the products in one call, native and CRT (own outputs)
+    bT = {mode: [dev(x) for x in tC0] for mode in (dgt.FP64_NATIVE, dgt.FP64_OZAKI2_INT8)}
+    bkeep = {mode: [dev(O.uniform((d["m"], d["n"]), 900 + i)) for i, d in enumerate(gdesc[:6])] for mode in bT}
+    bdesc = {mode: [dict(d, C=ptr(c)) for d, c in zip(gdesc[:6], bkeep[mode])] for mode in bT}
+    bC0 = {mode: [x.clone() for x in bkeep[mode]] for mode in bT}
 
     def batch(h):
         h.dgemm("N", "N", m, n, k, 1.0, ptr(dA), m, ptr(dB), k, 0.5, ptr(outs["native"]), m, mode=dgt.FP64_NATIVE)
@@ -57,6 +63,13 @@ def test_capture_and_replay_all_paths():
         h.dgemm_grouped(gdesc)
         h.dgemm_grouped(edesc, mode=dgt.FP64_OZAKI_INT8, slices=7)
         h.dgemm_grouped(rdesc, mode=dgt.FP64_OZAKI2_INT8, slices=16)
+        h.set_tuning(dgt.TUNE_CRT_PANELS, 3)
+        h.dgemm("N", "N", m, n, k, 1.0, ptr(dA), m, ptr(dB), k, 0.5, ptr(outs["crt_panels"]), m,
+                mode=dgt.FP64_OZAKI2_INT8, slices=14)
+        h.set_tuning(dgt.TUNE_CRT_PANELS, 0)
+        for mode in bT:
+            h.cannon25d_batch(M, p, c, 1.0, [ptr(x) for x in tA], [ptr(x) for x in tB], 0.5, [ptr(x) for x in bT[mode]],
+                              bdesc[mode], mode=mode, slices=14)
 
     def reset():
         for name in outs:
@@ -71,6 +84,11 @@ def test_capture_and_replay_all_paths():
             x.copy_(x0)
         for x, x0 in zip(rkeep, rC0):
             x.copy_(x0)
+        for mode in bT:
+            for x, x0 in zip(bT[mode], tC0):
+                x.copy_(dev(x0))
+            for x, x0 in zip(bkeep[mode], bC0[mode]):
+                x.copy_(x0)
 
     with dgt.Handle() as h:
         side = torch.cuda.Stream()
@@ -80,8 +98,10 @@ def test_capture_and_replay_all_paths():
             reset()
             batch(h)  # eager again, now with the final workspace: every table is resident
         torch.cuda.synchronize()
-        eager = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
-                 [x.clone() for x in ekeep] + [x.clone() for x in tE] + [x.clone() for x in rkeep])
+        snap = lambda: ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
+                        [x.clone() for x in ekeep] + [x.clone() for x in tE] + [x.clone() for x in rkeep] +
+                        [x.clone() for mode in bT for x in bT[mode] + bkeep[mode]])
+        eager = snap()
         reset()
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
@@ -92,8 +112,7 @@ def test_capture_and_replay_all_paths():
         g.replay()
         torch.cuda.synchronize()
         h.check_device()
-        replay = ([t.clone() for t in outs.values()] + [x.clone() for x in tC] + [x[2].clone() for x in gkeep] +
-                  [x.clone() for x in ekeep] + [x.clone() for x in tE] + [x.clone() for x in rkeep])
+        replay = snap()
         for a, b in zip(eager, replay):
             assert torch.equal(a, b)
         # and a second replay after another reset gives the same again

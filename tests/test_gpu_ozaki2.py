@@ -138,6 +138,22 @@ def test_long_k_runs_in_chunks(h):
     assert O.rel_errors(got_t, O.dgemm(A, B, 1.5, -0.5, C))[1] <= FRO_TOL
 
 
+@pytest.mark.parametrize("panels", [2, 3, 8])
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T"), ("N", "T")])
+def test_panels_change_nothing(h, panels, ta, tb):
+    """op(B) in column panels (split and reconstruction on side streams beside the residue
+    GEMM): the same result, bit for bit, as the product in one piece; ragged last panel."""
+    m, n, k = 700, 1500, 900
+    A, B, C = operands(ta, tb, m, n, k, 80 + panels, phi=1.0)
+    h.set_tuning(dgt.TUNE_CRT_PANELS, 1)
+    one = run(h, ta, tb, m, n, k, 1.5, -0.5, 14, A, B, C)
+    h.set_tuning(dgt.TUNE_CRT_PANELS, panels)
+    got = run(h, ta, tb, m, n, k, 1.5, -0.5, 14, A, B, C)
+    h.set_tuning(dgt.TUNE_CRT_PANELS, 0)
+    assert np.array_equal(got, one)
+    assert O.rel_errors(got, O.dgemm(A, B, 1.5, -0.5, C, ta, tb))[1] <= FRO_TOL
+
+
 def test_grouped_and_cannon_through_crt(h):
     import torch
 
