@@ -604,6 +604,158 @@ static bool make_f64_map(CUtensorMap* map, const double* base, int64_t inner, in
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The same TMA-fed kernel without the per-k-tile __syncthreads.  Every stage has a full
+// barrier (the TMA bytes land) and an empty barrier (one arrival per warp once its DMMAs have
+// read the stage).  Thread 0, after consuming k-tile `it`, waits (bounded) until every warp has
+// released k-tile it - 1 and refills that stage with load it + STAGES - 1; the other warps never
+// wait for each other, only for data, so a warp that falls behind on one k-tile catches up on
+// the next instead of holding all eight at a barrier.
+// EARLY: thread 0 refills before its own DMMAs of k-tile `it` (the load goes out up to one
+// k-tile sooner; warp 0 may wait for the slowest warp first).
+template <class CF, bool EARLY = false>
+__global__ void __launch_bounds__(CF::THREADS, 1) dmma_tma_dec_kernel(const __grid_constant__ TmaGemmParams P) {
+    constexpr int BK = CF::BK, STAGES = CF::STAGES, STAGE_A = CF::STAGE_A, STAGE_B = CF::STAGE_B, MT = CF::MT;
+    constexpr int NWARPS = CF::THREADS / 32;
+    static_assert(!CF::PERM, "the TMA boxes reproduce the unpermuted padded layouts");
+    static_assert(CF::LDMN == BM + 4 && CF::LD_K == BK + 4 && CF::LD_KB == BK + 4, "box shapes follow the layouts");
+    constexpr uint32_t BYTES_MN = (BM + 4) * BK * 8, BYTES_K = (BK + 4) * BM * 8;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    double* smem = reinterpret_cast<double*>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    double* sA = smem;
+    double* sB = smem + STAGES * STAGE_A;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * STAGE_B);
+    uint64_t* empty = full + STAGES;
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + STAGES);
+    int* cur = const_cast<int*>(abort_flag) + 1;  // thread 0's load cursor, as in dmma_tma_kernel
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 2, wn = warp & 3;
+    const int g = lane >> 2, t = lane & 3;
+    const uint32_t tx_bytes = (P.a_mn ? BYTES_MN : BYTES_K) + (P.b_mn ? BYTES_MN : BYTES_K);
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            oz::mbar_init(oz::su32(full + s), 1);
+            oz::mbar_init(oz::su32(empty + s), NWARPS);
+        }
+        *abort_flag = 0;
+        cur[0] = blockIdx.x;
+        cur[1] = 0;
+        cur[2] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    auto tile_mn = [&](int tile, int64_t& m0, int64_t& n0) {
+        const int in_group = GROUP_M * P.tiles_n;
+        const int first_m = (tile / in_group) * GROUP_M;
+        const int gsize = min(P.tiles_m - first_m, GROUP_M);
+        m0 = (int64_t)(first_m + (tile % in_group) % gsize) * BM;
+        n0 = (int64_t)((tile % in_group) / gsize) * BN;
+    };
+    auto issue_next = [&]() {
+        const int ld_tile = cur[0], ld_kt = cur[1];
+        if (ld_tile >= P.total_tiles) return;
+        const int s = cur[2] % STAGES;
+        int64_t m0, n0;
+        tile_mn(ld_tile, m0, n0);
+        const int32_t k0 = ld_kt * BK;
+        const uint32_t bar = oz::su32(full + s);
+        oz::mbar_expect_tx(bar, tx_bytes);
+        const uint32_t da = oz::su32(sA + s * STAGE_A), db = oz::su32(sB + s * STAGE_B);
+        if (P.a_mn)
+            oz::tma_load_2d(da, &P.tmA, (int32_t)m0, k0, bar);
+        else
+            oz::tma_load_2d(da, &P.tmA, k0, (int32_t)m0, bar);
+        if (P.b_mn)
+            oz::tma_load_2d(db, &P.tmB, (int32_t)n0, k0, bar);
+        else
+            oz::tma_load_2d(db, &P.tmB, k0, (int32_t)n0, bar);
+        cur[2] += 1;
+        if (ld_kt + 1 == P.ktiles) {
+            cur[1] = 0;
+            cur[0] = ld_tile + gridDim.x;
+        } else {
+            cur[1] = ld_kt + 1;
+        }
+    };
+    if (tid == 0)
+        for (int s = 0; s < STAGES - 1; ++s) issue_next();
+
+    uint32_t it = 0;  // stages consumed by this warp
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < P.total_tiles && ok; tile += gridDim.x) {
+        int64_t m0, n0;
+        tile_mn(tile, m0, n0);
+        double acc[MT][4][4];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+        for (int kt = 0; kt < P.ktiles; ++kt, ++it) {
+            const int s = (int)(it % STAGES);
+            // every lane waits (bounded); the warp leaves together if any lane gave up
+            const bool got = oz::mbar_wait(oz::su32(full + s), (it / STAGES) & 1, abort_flag, P.err);
+            if (!__all_sync(0xffffffffu, got)) {
+                ok = false;
+                break;
+            }
+            // thread 0 refills the stage of k-tile it - 1 once every warp has released it
+            auto refill = [&]() -> bool {
+                bool good = true;
+                if (lane == 0) {
+                    if (it > 0) {
+                        const uint32_t prev = it - 1;
+                        good = oz::mbar_wait(oz::su32(empty + prev % STAGES), (prev / STAGES) & 1, abort_flag, P.err);
+                    }
+                    if (good) issue_next();
+                }
+                return __shfl_sync(0xffffffffu, good, 0);
+            };
+            if (EARLY && warp == 0 && !refill()) {
+                ok = false;
+                break;
+            }
+            mma_ktile<CF>(sA + s * STAGE_A, sB + s * STAGE_B, P.a_mn != 0, P.b_mn != 0, acc, wm, wn, g, t);
+            __syncwarp();  // every lane's fragment reads of the stage are done
+            if (lane == 0) oz::mbar_arrive(oz::su32(empty + s));
+            if (!EARLY && warp == 0 && !refill()) {
+                ok = false;
+                break;
+            }
+        }
+        if (!ok) break;
+        store_tile<CF>(acc, P.C, P.ldc, P.m, P.n, m0, n0, P.alpha, P.beta, wm, wn, g, t);
+    }
+    // loads issued but not consumed (the lookahead past the last tile, or an abort) must land
+    // before the CTA's shared memory is released
+    if (tid == 0) {
+        for (uint32_t j = it; j < (uint32_t)cur[2]; ++j) {
+            long long t0 = clock64();
+            while (!oz::mbar_try(oz::su32(full + (j % STAGES)), (j / STAGES) & 1) && clock64() - t0 < oz::WAIT_BUDGET) {
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <class CF>
+constexpr size_t tma_dec_smem_bytes() {
+    return 128 + CF::SMEM + (size_t)CF::STAGES * 16 + 32;  // ring, full + empty barriers, abort flag + cursor
+}
+
+template <class CF, bool EARLY = false>
+cudaError_t launch_tma_dec_variant(const TmaGemmParams& prm, int grid, cudaStream_t stream) {
+    static_assert(tma_dec_smem_bytes<CF>() <= 232448, "shared memory per CTA");
+    cudaError_t e = smem_opt_in<dmma_tma_dec_kernel<CF, EARLY>>((int)tma_dec_smem_bytes<CF>());
+    if (e != cudaSuccess) return e;
+    dmma_tma_dec_kernel<CF, EARLY><<<grid, CF::THREADS, tma_dec_smem_bytes<CF>(), stream>>>(prm);
+    return cudaGetLastError();
+}
+
 template <class CF>
 constexpr size_t tma_smem_bytes() {
     return 128 + CF::SMEM + (size_t)CF::STAGES * 8 + 32;  // ring, full barriers, abort flag + cursor
@@ -664,12 +816,18 @@ using T14 = V2;
 using T15 = V1;
 using T16 = V7;
 using T17 = Cfg<8, 16, 5>;
+// Variants 18-22: the decoupled TMA kernel (empty barriers, no per-k-tile __syncthreads) with
+// the tile shapes of 14, 17 and 16, a 4-deep BK = 24 ring (21), and 14's shape refilling
+// before warp 0's DMMAs (22); outside the TMA form's cover, the cp.async kernel of variant 2,
+// 17, 7, 2 and 2.  (BK = 24 is a TMA-only depth: its cp.async stand-in is variant 2.)
+using T21 = Cfg<8, 24, 4>;
 
-int dmma_variant_count() { return 18; }
+int dmma_variant_count() { return 23; }
 int64_t dmma_tile_count(int64_t m, int64_t n) { return ceil_div(m, BM) * ceil_div(n, BN); }
 
 // The TMA form for one plain GEMM, when the operands allow it; *used says whether it ran.
-template <class CF>
+// DEC: the decoupled kernel (dmma_tma_dec_kernel).
+template <class CF, bool DEC = false, bool EARLY = false>
 static cudaError_t try_tma(dgt_context* h, const Problem& p, const KSegment& sg, int grid, bool* used) {
     *used = false;
     const bool a_mn = p.transa == 0, b_mn = p.transb != 0;
@@ -699,7 +857,10 @@ static cudaError_t try_tma(dgt_context* h, const Problem& p, const KSegment& sg,
     prm.b_mn = b_mn;
     prm.err = h->dev_error;
     *used = true;
-    return launch_tma_variant<CF>(prm, grid, h->stream);
+    if constexpr (DEC)
+        return launch_tma_dec_variant<CF, EARLY>(prm, grid, h->stream);
+    else
+        return launch_tma_variant<CF>(prm, grid, h->stream);
 }
 
 dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, const std::vector<KSegment>& segs,
@@ -761,7 +922,12 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
                 case 14: e = try_tma<T14>(h, live[0], segs[0], grid, &used); break;
                 case 15: e = try_tma<T15>(h, live[0], segs[0], grid, &used); break;
                 case 16: e = try_tma<T16>(h, live[0], segs[0], grid, &used); break;
-                default: e = try_tma<T17>(h, live[0], segs[0], grid, &used); break;
+                case 17: e = try_tma<T17>(h, live[0], segs[0], grid, &used); break;
+                case 18: e = try_tma<T14, true>(h, live[0], segs[0], grid, &used); break;
+                case 19: e = try_tma<T17, true>(h, live[0], segs[0], grid, &used); break;
+                case 20: e = try_tma<T16, true>(h, live[0], segs[0], grid, &used); break;
+                case 21: e = try_tma<T21, true>(h, live[0], segs[0], grid, &used); break;
+                default: e = try_tma<T14, true, true>(h, live[0], segs[0], grid, &used); break;
             }
         }
         if (used) {
@@ -769,7 +935,10 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
             if (e != cudaSuccess) return cuda_fail(h, e, "dmma_tma_kernel launch");
             return DGT_SUCCESS;
         }
-        variant = variant == 14 ? 2 : variant == 15 ? 1 : variant == 16 ? 7 : 17;
+        variant = (variant == 14 || variant == 18 || variant == 21 || variant == 22) ? 2
+                  : variant == 15                                    ? 1
+                  : (variant == 16 || variant == 20)                 ? 7
+                                                                     : 17;
     }
     switch (variant) {
         case 17: e = launch_variant<T17>(prm, grid, h->stream, reduces); break;

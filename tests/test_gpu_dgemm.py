@@ -131,7 +131,7 @@ def test_double_double_sample_error(h):
     assert np.median(gpu_err) <= 4 * max(np.median(cpu_err), 1e-17)
 
 
-@pytest.mark.parametrize("variant", list(range(18)))
+@pytest.mark.parametrize("variant", list(range(23)))
 def test_dmma_kernel_variants(variant):
     """Every tuning variant of the native kernel (DMMA shape m16n8k4/k8/k16, K depth, ring
     depth, 8 or 16 warps, 64- or 128-bit fragment loads) on ragged shapes, all four
@@ -157,10 +157,11 @@ def _raw(h, ta, tb, m, n, k, alpha, beta, A, B, C, lda, ldb):
     return host(dC, (m, n))
 
 
-@pytest.mark.parametrize("tma,base", [(14, 2), (15, 1), (16, 7), (17, 1)])
+@pytest.mark.parametrize("tma,base", [(14, 2), (15, 1), (16, 7), (17, 1), (18, 2), (19, 1), (20, 7), (21, 2), (22, 2)])
 def test_tma_variants_bit_identical_to_cp_async(tma, base):
-    """Variants 14-17 bring the operand tiles in by TMA (bulk-tensor loads completing on an
-    mbarrier per stage) into the same padded shared-memory layout the cp.async loader writes,
+    """Variants 14-22 bring the operand tiles in by TMA (bulk-tensor loads completing on an
+    mbarrier per stage; 18-22 release stages through per-stage empty barriers instead of a CTA
+    barrier per k-tile) into the same padded shared-memory layout the cp.async loader writes,
     so with the same DMMA shape and K depth the result is bit for bit the cp.async kernel's:
     ragged edges (zero-filled out-of-range boxes), all four transpose pairs, beta != 0, a K
     that is not a multiple of the stage depth, and a problem spanning several waves of tiles."""
