@@ -558,7 +558,7 @@ def workload_batching(args):
             # kernel variant of the steps' grouped passes: the fastest of the library's variants
             knob = dgt.TUNE_DMMA_VARIANT if mode == dgt.FP64_NATIVE else dgt.TUNE_OZAKI_VARIANT
             best = None
-            for v in ((2,) if mode == dgt.FP64_NATIVE else (0, 1, 5, 7)):
+            for v in ((2, 23, 24) if mode == dgt.FP64_NATIVE else (0, 1, 5, 7)):
                 h.set_tuning(knob, v)
                 t = _time_ms(torch, f, 2, warm=1)
                 if best is None or t < best[1]:
@@ -605,7 +605,7 @@ def workload_batching(args):
             f = lambda: h.dgemm_grouped(descs, mode=mode, slices=S)
             # kernel variant: the fastest of the library's variants for this batch
             knob = dgt.TUNE_DMMA_VARIANT if mode == dgt.FP64_NATIVE else dgt.TUNE_OZAKI_VARIANT
-            cands = range(7) if mode == dgt.FP64_NATIVE else (0, 1, 5, 7)  # static and dynamic unit order
+            cands = (0, 1, 2, 23, 24, 25) if mode == dgt.FP64_NATIVE else (0, 1, 5, 7)  # static and dynamic unit order
             best = None
             for v in cands:
                 h.set_tuning(knob, v)
@@ -644,7 +644,7 @@ def workload_batching(args):
             f = lambda: h.cannon25d_batch(M, p, c, 1.0, pA, pB, 0.0, pC, descs, mode=mode, slices=S)
             # tile shape / kernel variant: the fastest for this batch
             knob = dgt.TUNE_DMMA_VARIANT if mode == dgt.FP64_NATIVE else dgt.TUNE_OZAKI_VARIANT
-            cands = (0, 1, 2, 7, 10, 12) if mode == dgt.FP64_NATIVE else (0, 1, 5, 7)
+            cands = (1, 2, 23, 24, 25) if mode == dgt.FP64_NATIVE else (0, 1, 5, 7)
             best = None
             for v in cands:
                 h.set_tuning(knob, v)

@@ -462,6 +462,194 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
     }
 }
 
+// ---- the grouped kernel without CTA barriers in its main loop -------------------------------
+// cp.async copies signal a stage's full mbarrier when they land (cp.async.mbarrier.arrive.noinc,
+// one arrival per thread), every warp releases the stage through its empty mbarrier after its
+// DMMAs, and every thread refills a stage (its share of the copies) once lane 0 of its warp saw
+// the stage released.  The load cursor (tile, problem, K-segment, K offset; the same in every
+// thread) runs across tiles, so the next tile's first stages load while this tile's last
+// k-tiles multiply and its epilogue stores, and no tile starts on an empty ring.  Every wait is
+// bounded; a warp that gives up leaves its k-loop, and the CTA agrees on the abort at the tile
+// boundary (one __syncthreads_and per tile).  Same fragments, same k order: the results equal
+// dmma_grouped_kernel's of the same shape bit for bit.
+__device__ __forceinline__ void cp_async_mbar_arrive(uint32_t bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+
+// Tile `local` of a problem: grouped rasterisation (GROUP_M tile rows at a time).
+__device__ __forceinline__ void tile_origin(const Problem& pb, int local, int64_t& m0, int64_t& n0) {
+    const int in_group = GROUP_M * pb.tiles_n;
+    const int first_m = (local / in_group) * GROUP_M;
+    const int gsize = min(pb.tiles_m - first_m, GROUP_M);
+    m0 = (int64_t)(first_m + (local % in_group) % gsize) * BM;
+    n0 = (int64_t)((local % in_group) / gsize) * BN;
+}
+
+template <class CF>
+constexpr size_t grouped_dec_smem_bytes() {
+    return CF::SMEM + (size_t)CF::STAGES * 16 + 16;  // ring, full + empty barriers, abort flag
+}
+
+template <class CF>
+__global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_dec_kernel(const __grid_constant__ GroupedParams prm) {
+    constexpr int BK = CF::BK, STAGES = CF::STAGES, LD_K = CF::LD_K, LD_KB = CF::LD_KB, LDMN = CF::LDMN;
+    constexpr int STAGE_A = CF::STAGE_A, STAGE_B = CF::STAGE_B;
+    constexpr int THREADS = CF::THREADS, MT = CF::MT, NWARPS = THREADS / 32;
+    static_assert(!CF::PERM || CF::MMAK >= 8, "128-bit fragment loads need the k8 or k16 shape");
+    extern __shared__ __align__(16) double smem[];
+    double* sA = smem;
+    double* sB = smem + STAGES * STAGE_A;
+    uint64_t* full = reinterpret_cast<uint64_t*>(sB + STAGES * STAGE_B);
+    uint64_t* empty = full + STAGES;
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + STAGES);
+    __shared__ int s_ready;
+
+    const Problem* probs = prm.probs ? prm.probs : prm.inl_probs;
+    const KSegment* segs = prm.segs ? prm.segs : prm.inl_segs;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp >> 2, wn = warp & 3;
+    const int g = lane >> 2, t = lane & 3;
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            oz::mbar_init(oz::su32(full + s), THREADS);
+            oz::mbar_init(oz::su32(empty + s), NWARPS);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    // the load cursor
+    int ld_tile = blockIdx.x, ld_pi = 0, ld_seg = 0;
+    int64_t ld_k0 = 0, ld_m0 = 0, ld_n0 = 0;
+    auto ld_enter = [&]() {  // the first non-empty K-segment of ld_tile or a later tile
+        while (ld_tile < prm.total_tiles) {
+            ld_pi = find_problem(probs, prm.nprob, ld_tile);
+            const Problem& pb = probs[ld_pi];
+            tile_origin(pb, ld_tile - pb.tile_begin, ld_m0, ld_n0);
+            ld_k0 = 0;
+            ld_seg = 0;
+            while (ld_seg < pb.seg_count && segs[pb.seg_begin + ld_seg].k <= 0) ++ld_seg;
+            if (ld_seg < pb.seg_count) return;
+            ld_tile += gridDim.x;  // no K at all: its consumer multiplies nothing
+        }
+    };
+    ld_enter();
+    uint32_t issued = 0;
+    // this thread's share of the next stage; false if its warp gave up waiting for the stage
+    auto issue = [&]() -> bool {
+        if (ld_tile >= prm.total_tiles) return true;
+        const int s = (int)(issued % STAGES);
+        if (issued >= STAGES) {  // the stage's previous k-tile, released by every warp
+            bool good = true;
+            if (lane == 0)
+                good = oz::mbar_wait(oz::su32(empty + s), ((issued - STAGES) / STAGES) & 1, abort_flag, prm.err);
+            if (!__shfl_sync(0xffffffffu, good, 0)) return false;
+        }
+        const Problem& pb = probs[ld_pi];
+        const KSegment sg = segs[pb.seg_begin + ld_seg];
+        const bool a_mn = (pb.transa == 0), b_mn = (pb.transb != 0);
+        const int64_t klim = sg.k - ld_k0;
+        const bool va = (((uintptr_t)sg.A & 15) == 0) && ((sg.lda & 1) == 0);
+        const bool vb = (((uintptr_t)sg.B & 15) == 0) && ((sg.ldb & 1) == 0);
+        if (va && klim >= BK && pb.m - ld_m0 >= BM)
+            load_tile_full<BK, LD_K, THREADS, LDMN>(sA + s * STAGE_A, sg.A, sg.lda, a_mn, ld_m0, ld_k0, tid);
+        else
+            load_tile<BK, LD_K, THREADS, LDMN>(sA + s * STAGE_A, sg.A, sg.lda, a_mn, ld_m0, ld_k0, pb.m - ld_m0, klim,
+                                               va, tid);
+        if (vb && klim >= BK && pb.n - ld_n0 >= BN)
+            load_tile_full<BK, LD_KB, THREADS, LDMN>(sB + s * STAGE_B, sg.B, sg.ldb, b_mn, ld_n0, ld_k0, tid);
+        else
+            load_tile<BK, LD_KB, THREADS, LDMN>(sB + s * STAGE_B, sg.B, sg.ldb, b_mn, ld_n0, ld_k0, pb.n - ld_n0,
+                                                klim, vb, tid);
+        cp_async_mbar_arrive(oz::su32(full + s));
+        ++issued;
+        ld_k0 += BK;
+        if (ld_k0 >= sg.k) {
+            ld_k0 = 0;
+            ++ld_seg;
+            while (ld_seg < pb.seg_count && segs[pb.seg_begin + ld_seg].k <= 0) ++ld_seg;
+            if (ld_seg >= pb.seg_count) {
+                ld_tile += gridDim.x;
+                ld_enter();
+            }
+        }
+        return true;
+    };
+
+    bool ok = true;
+    for (int s = 0; s < STAGES - 1 && ok; ++s) ok = issue();
+    uint32_t it = 0;  // stages consumed
+    for (int tile = blockIdx.x; tile < prm.total_tiles; tile += gridDim.x) {
+        const int pi = find_problem(probs, prm.nprob, tile);
+        const Problem& pb = probs[pi];
+        const int local = tile - pb.tile_begin;
+        int64_t m0, n0;
+        tile_origin(pb, local, m0, n0);
+        const bool a_mn = (pb.transa == 0), b_mn = (pb.transb != 0);
+        int total_kt = 0;
+        for (int s = 0; s < pb.seg_count; ++s) {
+            const int64_t k = segs[pb.seg_begin + s].k;
+            if (k > 0) total_kt += (int)ceil_div(k, BK);
+        }
+        double acc[MT][4][4];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+        for (int kt = 0; kt < total_kt && ok; ++kt, ++it) {
+            const int s = (int)(it % STAGES);
+            const bool got = oz::mbar_wait(oz::su32(full + s), (it / STAGES) & 1, abort_flag, prm.err);
+            if (!__all_sync(0xffffffffu, got)) {
+                ok = false;
+                break;
+            }
+            mma_ktile<CF>(sA + s * STAGE_A, sB + s * STAGE_B, a_mn, b_mn, acc, wm, wn, g, t);
+            __syncwarp();  // every lane's fragment reads of the stage are done
+            if (lane == 0) oz::mbar_arrive(oz::su32(empty + s));
+            if (!issue()) {
+                ok = false;
+                break;
+            }
+        }
+        if (!__syncthreads_and(ok)) break;  // the CTA leaves a failed tile together
+
+        // epilogue: as dmma_grouped_kernel's (stack partials waited for and added in order)
+        int nred = 0;
+        if (pb.red_role == 2) {
+            if (tid == 0) {
+                const int32_t* f = prm.red_flags + pb.red_slot + local;
+                const long long t0 = clock64();
+                int ready = 1;
+                while (ld_acquire_gpu(f) < pb.red_wait) {
+                    if (clock64() - t0 > oz::WAIT_BUDGET) {
+                        atomicOr(prm.err, DGT_DEVERR_TIMEOUT);
+                        ready = 0;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+                s_ready = ready;
+            }
+            __syncthreads();
+            nred = s_ready ? pb.red_wait : 0;
+        }
+        store_tile<CF>(acc, pb.C, pb.ldc, pb.m, pb.n, m0, n0, pb.alpha, pb.beta, wm, wn, g, t, pb.red_src,
+                       pb.red_stride, pb.red_ld, nred);
+        if (pb.red_role == 1) {
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) red_release_add_gpu(prm.red_flags + pb.red_slot + local, 1);
+        }
+    }
+    cp_async_wait<0>();  // this thread's copies still in flight (the lookahead past the last tile)
+    __syncthreads();
+}
+
 // ---- TMA-fed form for one plain GEMM ---------------------------------------------------------
 // The same CTA tile, warps and fragment code, with the operand tiles brought into shared memory
 // by the tensor memory accelerator instead of per-thread cp.async: thread 0 issues two 2D
@@ -784,26 +972,37 @@ using V11 = Cfg<16, 16, 4, 8, true>;
 using V12 = Cfg<8, 32, 2, 8, true>;
 using V13 = Cfg<16, 32, 2, 8, true>;
 
-template <class CF>
-cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stream, bool coop) {
-    cudaError_t e = smem_opt_in<dmma_grouped_kernel<CF>>((int)CF::SMEM);
+template <auto Kernel, int THREADS, size_t SMEM>
+cudaError_t launch_grouped(const GroupedParams& prm, int grid, cudaStream_t stream, bool coop) {
+    static_assert(SMEM <= 232448 - 16, "shared memory per CTA");
+    cudaError_t e = smem_opt_in<Kernel>((int)SMEM);
     if (e != cudaSuccess) return e;
     if (!coop) {
-        dmma_grouped_kernel<CF><<<grid, CF::THREADS, CF::SMEM, stream>>>(prm);
+        Kernel<<<grid, THREADS, SMEM, stream>>>(prm);
         return cudaGetLastError();
     }
     // a stack reduction waits across CTAs: a cooperative launch keeps them all resident
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)grid);
-    cfg.blockDim = dim3(CF::THREADS);
-    cfg.dynamicSmemBytes = CF::SMEM;
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = SMEM;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, dmma_grouped_kernel<CF>, prm);
+    return cudaLaunchKernelEx(&cfg, Kernel, prm);
+}
+
+// DEC: the grouped kernel without CTA barriers in its main loop.
+template <class CF, bool DEC = false>
+cudaError_t launch_variant(const GroupedParams& prm, int grid, cudaStream_t stream, bool coop) {
+    if constexpr (DEC)
+        return launch_grouped<dmma_grouped_dec_kernel<CF>, CF::THREADS, grouped_dec_smem_bytes<CF>()>(prm, grid, stream,
+                                                                                                    coop);
+    else
+        return launch_grouped<dmma_grouped_kernel<CF>, CF::THREADS, CF::SMEM>(prm, grid, stream, coop);
 }
 
 }  // namespace
@@ -818,11 +1017,15 @@ using T16 = V7;
 using T17 = Cfg<8, 16, 5>;
 // Variants 18-22: the decoupled TMA kernel (empty barriers, no per-k-tile __syncthreads) with
 // the tile shapes of 14, 17 and 16, a 4-deep BK = 24 ring (21), and 14's shape refilling
-// before warp 0's DMMAs (22); outside the TMA form's cover, the cp.async kernel of variant 2,
-// 17, 7, 2 and 2.  (BK = 24 is a TMA-only depth: its cp.async stand-in is variant 2.)
+// before warp 0's DMMAs (22); outside the TMA form's cover, the cp.async kernel of variant 23
+// (the decoupled grouped kernel of 18's shape), 17, 7, 2 and 2.  (BK = 24 is a TMA-only
+// depth: its cp.async stand-in is variant 2.)
 using T21 = Cfg<8, 24, 4>;
+// Variants 23-25: the grouped kernel without CTA barriers in its main loop
+// (dmma_grouped_dec_kernel) with the shapes of variants 2, 1 and 17; every call, grouped or
+// not, runs it.
 
-int dmma_variant_count() { return 23; }
+int dmma_variant_count() { return 26; }
 int64_t dmma_tile_count(int64_t m, int64_t n) { return ceil_div(m, BM) * ceil_div(n, BN); }
 
 // The TMA form for one plain GEMM, when the operands allow it; *used says whether it ran.
@@ -915,7 +1118,7 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
     cudaError_t e = cudaSuccess;
     if (reduces) DGT_CUDA_TRY(h, cudaMemsetAsync(red_flags, 0, red_count * sizeof(int32_t), h->stream));
     int variant = h->dmma_variant;
-    if (variant >= 14) {
+    if (variant >= 14 && variant <= 22) {
         bool used = false;
         if (live.size() == 1 && segs.size() == 1 && !reduces) {
             switch (variant) {
@@ -935,12 +1138,16 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
             if (e != cudaSuccess) return cuda_fail(h, e, "dmma_tma_kernel launch");
             return DGT_SUCCESS;
         }
-        variant = (variant == 14 || variant == 18 || variant == 21 || variant == 22) ? 2
-                  : variant == 15                                    ? 1
-                  : (variant == 16 || variant == 20)                 ? 7
-                                                                     : 17;
+        variant = variant == 18                                      ? 23
+                  : (variant == 14 || variant == 21 || variant == 22) ? 2
+                  : variant == 15                                     ? 1
+                  : (variant == 16 || variant == 20)                  ? 7
+                                                                      : 17;
     }
     switch (variant) {
+        case 23: e = launch_variant<V2, true>(prm, grid, h->stream, reduces); break;
+        case 24: e = launch_variant<V1, true>(prm, grid, h->stream, reduces); break;
+        case 25: e = launch_variant<T17, true>(prm, grid, h->stream, reduces); break;
         case 17: e = launch_variant<T17>(prm, grid, h->stream, reduces); break;
         case 1: e = launch_variant<V1>(prm, grid, h->stream, reduces); break;
         case 2: e = launch_variant<V2>(prm, grid, h->stream, reduces); break;

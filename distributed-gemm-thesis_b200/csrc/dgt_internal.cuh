@@ -41,7 +41,7 @@ struct dgt_context {
     dgt_fp64_mode fp64_mode = DGT_FP64_NATIVE;
     int slices = 7;
     int dmma_variant = 18; // native FP64 kernel variant (see dgemm_dmma.cu): 18 measured fastest for
-                           // one plain GEMM; calls outside its TMA form run variant 2, the fastest cp.async one
+                           // one plain GEMM; calls outside its TMA form run variant 23 (grouped, decoupled)
     int ozaki_variant = 6; // INT8 Ozaki kernel variant (dgt.h); 6 measured fastest at 16384^3
     bool profile = false;  // record phase events (DGT_TUNE_PROFILE)
     int test_stall = 0;    // failure-path test hook (DGT_TUNE_TEST_STALL)

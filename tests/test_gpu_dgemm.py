@@ -131,7 +131,7 @@ def test_double_double_sample_error(h):
     assert np.median(gpu_err) <= 4 * max(np.median(cpu_err), 1e-17)
 
 
-@pytest.mark.parametrize("variant", list(range(23)))
+@pytest.mark.parametrize("variant", list(range(26)))
 def test_dmma_kernel_variants(variant):
     """Every tuning variant of the native kernel (DMMA shape m16n8k4/k8/k16, K depth, ring
     depth, 8 or 16 warps, 64- or 128-bit fragment loads) on ragged shapes, all four
@@ -179,3 +179,46 @@ def test_tma_variants_bit_identical_to_cp_async(tma, base):
         assert np.array_equal(out[tma], out[base]), (tma, m, n, k, ta, tb)
         assert O.rel_errors(out[tma], O.dgemm(A, B, 1.5, -0.5, C, ta, tb))[1] <= FRO_TOL
 
+
+
+@pytest.mark.parametrize("dec,base", [(23, 2), (24, 1), (25, 17)])
+def test_grouped_dec_variants_bit_identical(dec, base):
+    """Variants 23-25 run the grouped kernel without CTA barriers in its main loop (stages
+    signalled by cp.async mbarrier arrivals, released per warp, the load cursor running across
+    tiles and problems): bit for bit the barrier kernel of the same shape, on 48 ragged grouped
+    products (transposes, misaligned operands, K = 0, a one-element product, several waves),
+    and against host FP64."""
+    import torch
+
+    rng = np.random.default_rng(dec)
+    specs = []
+    for i in range(48):
+        m, n, k = (int(x) for x in rng.integers(1, 700, 3))
+        if i == 0:
+            m, n, k = 1, 1, 1
+        if i == 1:
+            k = 0
+        ta, tb = str(rng.choice(["N", "T"])), str(rng.choice(["N", "T"]))
+        ra, ca = (k, m) if ta == "T" else (m, k)
+        rb, cb = (n, k) if tb == "T" else (k, n)
+        specs.append((m, n, k, ta, tb, O.uniform((max(ra, 1), max(ca, 1)), 3 * i + 1),
+                      O.uniform((max(rb, 1), max(cb, 1)), 3 * i + 2), O.uniform((m, n), 3 * i + 3)))
+    outs = {}
+    for v in (dec, base):
+        keep, descs = [], []
+        for m, n, k, ta, tb, A, B, C in specs:
+            dA, dB, dC = dev(A), dev(B), dev(C)
+            keep.append((dA, dB, dC))
+            descs.append(dict(m=m, n=n, k=k, alpha=1.25, beta=-0.5, A=ptr(dA), lda=A.shape[0], B=ptr(dB),
+                              ldb=B.shape[0], C=ptr(dC), ldc=m, transa=ta, transb=tb))
+        with dgt.Handle() as hh:
+            hh.set_tuning(dgt.TUNE_DMMA_VARIANT, v)
+            hh.dgemm_grouped(descs)
+            torch.cuda.synchronize()
+            hh.check_device()
+        outs[v] = [host(x[2], (sp[0], sp[1])) for x, sp in zip(keep, specs)]
+    for i, (m, n, k, ta, tb, A, B, C) in enumerate(specs):
+        assert np.array_equal(outs[dec][i], outs[base][i]), i
+        want = O.dgemm(A[:, :k] if ta == "N" else A[:k, :], B[:k, :] if tb == "N" else B[:, :k], 1.25, -0.5, C,
+                       ta, tb) if k > 0 else -0.5 * C
+        assert O.rel_errors(outs[dec][i], want)[1] <= FRO_TOL, i

@@ -97,7 +97,7 @@ def test_native_cannon_reduces_inside_its_launch(h, M, p, c, beta):
     assert O.rel_errors(host(dC, (M, M)), O.dgemm(A, B, 1.5, beta, C))[1] <= FRO_TOL
 
 
-@pytest.mark.parametrize("variant", [1, 10])
+@pytest.mark.parametrize("variant", [1, 10, 23, 25])
 def test_native_batch_is_one_launch(h, variant):
     """Cannon 4 x 4 x 2 plus 40 ragged products in one launch: both parts bit for bit as run
     apart (the Cannon step-by-step, the products through dgt_dgemm_grouped)."""
