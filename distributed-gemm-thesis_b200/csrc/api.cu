@@ -338,7 +338,8 @@ dgt_status dgt_set_tuning(dgt_handle_t h, dgt_tune_knob knob, int32_t value) {
             h->ozaki_variant = value;
             return DGT_SUCCESS;
         case DGT_TUNE_TEST_STALL:
-            h->test_stall = value != 0;
+            if (value < 0 || value > 2) return fail(h, DGT_ERROR_INVALID_VALUE, "test stall mode must be 0, 1 or 2");
+            h->test_stall = value;
             return DGT_SUCCESS;
         case DGT_TUNE_FUSE_STEPS:
             h->fuse_steps = value != 0;

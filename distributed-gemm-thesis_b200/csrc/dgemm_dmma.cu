@@ -62,6 +62,8 @@ struct GroupedParams {
     const KSegment* segs;
     int32_t* red_flags;    // stack-reduction counters (null: no problem reduces)
     unsigned int* err;     // sticky device error word
+    int32_t test_stall;    // DGT_TUNE_TEST_STALL: 1 withholds the first stage (decoupled kernel),
+                           // 2 keeps partial tiles from counting themselves
     Problem inl_probs[MAX_INLINE_PROBS];
     KSegment inl_segs[MAX_INLINE_SEGS];
 };
@@ -439,7 +441,9 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
                 const long long t0 = clock64();
                 int ready = 1;
                 while (ld_acquire_gpu(f) < pb.red_wait) {
-                    if (clock64() - t0 > oz::WAIT_BUDGET) {
+                    // a wait that already ran out anywhere in the launch ends this one too, so
+                    // the whole launch spends one budget, not one per stack-0 tile
+                    if (clock64() - t0 > oz::WAIT_BUDGET || (*(volatile unsigned int*)prm.err & DGT_DEVERR_TIMEOUT)) {
                         atomicOr(prm.err, DGT_DEVERR_TIMEOUT);
                         ready = 0;
                         break;
@@ -457,7 +461,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_kernel(const __gr
             // a partial tile: every thread's stores reach L2 before the tile is counted
             __threadfence();
             __syncthreads();
-            if (tid == 0) red_release_add_gpu(prm.red_flags + pb.red_slot + local, 1);
+            if (tid == 0 && prm.test_stall != 2) red_release_add_gpu(prm.red_flags + pb.red_slot + local, 1);
         }
     }
 }
@@ -538,6 +542,20 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_dec_kernel(const 
     };
     ld_enter();
     uint32_t issued = 0;
+    // moves the cursor past the stage just issued (K offset, then segment, then tile)
+    auto advance = [&](const KSegment& sg, const Problem& pb) -> bool {
+        ld_k0 += BK;
+        if (ld_k0 >= sg.k) {
+            ld_k0 = 0;
+            ++ld_seg;
+            while (ld_seg < pb.seg_count && segs[pb.seg_begin + ld_seg].k <= 0) ++ld_seg;
+            if (ld_seg >= pb.seg_count) {
+                ld_tile += gridDim.x;
+                ld_enter();
+            }
+        }
+        return true;
+    };
     // this thread's share of the next stage; false if its warp gave up waiting for the stage
     auto issue = [&]() -> bool {
         if (ld_tile >= prm.total_tiles) return true;
@@ -551,6 +569,10 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_dec_kernel(const 
         const Problem& pb = probs[ld_pi];
         const KSegment sg = segs[pb.seg_begin + ld_seg];
         const bool a_mn = (pb.transa == 0), b_mn = (pb.transb != 0);
+        if (prm.test_stall == 1 && issued == 0) {  // the test hook: the first stage never fills
+            ++issued;
+            return advance(sg, pb);
+        }
         const int64_t klim = sg.k - ld_k0;
         const bool va = (((uintptr_t)sg.A & 15) == 0) && ((sg.lda & 1) == 0);
         const bool vb = (((uintptr_t)sg.B & 15) == 0) && ((sg.ldb & 1) == 0);
@@ -566,17 +588,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_dec_kernel(const 
                                                 klim, vb, tid);
         cp_async_mbar_arrive(oz::su32(full + s));
         ++issued;
-        ld_k0 += BK;
-        if (ld_k0 >= sg.k) {
-            ld_k0 = 0;
-            ++ld_seg;
-            while (ld_seg < pb.seg_count && segs[pb.seg_begin + ld_seg].k <= 0) ++ld_seg;
-            if (ld_seg >= pb.seg_count) {
-                ld_tile += gridDim.x;
-                ld_enter();
-            }
-        }
-        return true;
+        return advance(sg, pb);
     };
 
     bool ok = true;
@@ -626,7 +638,9 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_dec_kernel(const 
                 const long long t0 = clock64();
                 int ready = 1;
                 while (ld_acquire_gpu(f) < pb.red_wait) {
-                    if (clock64() - t0 > oz::WAIT_BUDGET) {
+                    // a wait that already ran out anywhere in the launch ends this one too, so
+                    // the whole launch spends one budget, not one per stack-0 tile
+                    if (clock64() - t0 > oz::WAIT_BUDGET || (*(volatile unsigned int*)prm.err & DGT_DEVERR_TIMEOUT)) {
                         atomicOr(prm.err, DGT_DEVERR_TIMEOUT);
                         ready = 0;
                         break;
@@ -643,7 +657,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_grouped_dec_kernel(const 
         if (pb.red_role == 1) {
             __threadfence();
             __syncthreads();
-            if (tid == 0) red_release_add_gpu(prm.red_flags + pb.red_slot + local, 1);
+            if (tid == 0 && prm.test_stall != 2) red_release_add_gpu(prm.red_flags + pb.red_slot + local, 1);
         }
     }
     cp_async_wait<0>();  // this thread's copies still in flight (the lookahead past the last tile)
@@ -669,6 +683,7 @@ struct TmaGemmParams {
     int32_t tiles_m, tiles_n, total_tiles, ktiles;
     int32_t a_mn, b_mn;  // operand layouts: 1 = mn-major box {BM + 4, BK}, 0 = K-major box {BK + 4, BM}
     unsigned int* err;
+    int32_t test_stall;  // DGT_TUNE_TEST_STALL 1: the first stage is never loaded
 };
 
 template <class CF>
@@ -718,16 +733,18 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_tma_kernel(const __grid_c
         tile_mn(ld_tile, m0, n0);
         const int32_t k0 = ld_kt * BK;
         const uint32_t bar = oz::su32(full + s);
-        oz::mbar_expect_tx(bar, tx_bytes);
-        const uint32_t da = oz::su32(sA + s * STAGE_A), db = oz::su32(sB + s * STAGE_B);
-        if (P.a_mn)
-            oz::tma_load_2d(da, &P.tmA, (int32_t)m0, k0, bar);
-        else
-            oz::tma_load_2d(da, &P.tmA, k0, (int32_t)m0, bar);
-        if (P.b_mn)
-            oz::tma_load_2d(db, &P.tmB, (int32_t)n0, k0, bar);
-        else
-            oz::tma_load_2d(db, &P.tmB, k0, (int32_t)n0, bar);
+        if (!(P.test_stall == 1 && cur[2] == 0)) {  // (the test hook withholds the first stage)
+            oz::mbar_expect_tx(bar, tx_bytes);
+            const uint32_t da = oz::su32(sA + s * STAGE_A), db = oz::su32(sB + s * STAGE_B);
+            if (P.a_mn)
+                oz::tma_load_2d(da, &P.tmA, (int32_t)m0, k0, bar);
+            else
+                oz::tma_load_2d(da, &P.tmA, k0, (int32_t)m0, bar);
+            if (P.b_mn)
+                oz::tma_load_2d(db, &P.tmB, (int32_t)n0, k0, bar);
+            else
+                oz::tma_load_2d(db, &P.tmB, k0, (int32_t)n0, bar);
+        }
         cur[2] += 1;
         if (ld_kt + 1 == P.ktiles) {
             cur[1] = 0;
@@ -769,6 +786,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_tma_kernel(const __grid_c
     // before the CTA's shared memory is released
     if (tid == 0) {
         for (uint32_t j = it; j < (uint32_t)cur[2]; ++j) {
+            if (P.test_stall == 1 && j == 0) continue;  // the withheld stage has nothing in flight
             long long t0 = clock64();
             while (!oz::mbar_try(oz::su32(full + (j % STAGES)), (j / STAGES) & 1) && clock64() - t0 < oz::WAIT_BUDGET) {
             }
@@ -850,16 +868,18 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_tma_dec_kernel(const __gr
         tile_mn(ld_tile, m0, n0);
         const int32_t k0 = ld_kt * BK;
         const uint32_t bar = oz::su32(full + s);
-        oz::mbar_expect_tx(bar, tx_bytes);
-        const uint32_t da = oz::su32(sA + s * STAGE_A), db = oz::su32(sB + s * STAGE_B);
-        if (P.a_mn)
-            oz::tma_load_2d(da, &P.tmA, (int32_t)m0, k0, bar);
-        else
-            oz::tma_load_2d(da, &P.tmA, k0, (int32_t)m0, bar);
-        if (P.b_mn)
-            oz::tma_load_2d(db, &P.tmB, (int32_t)n0, k0, bar);
-        else
-            oz::tma_load_2d(db, &P.tmB, k0, (int32_t)n0, bar);
+        if (!(P.test_stall == 1 && cur[2] == 0)) {  // (the test hook withholds the first stage)
+            oz::mbar_expect_tx(bar, tx_bytes);
+            const uint32_t da = oz::su32(sA + s * STAGE_A), db = oz::su32(sB + s * STAGE_B);
+            if (P.a_mn)
+                oz::tma_load_2d(da, &P.tmA, (int32_t)m0, k0, bar);
+            else
+                oz::tma_load_2d(da, &P.tmA, k0, (int32_t)m0, bar);
+            if (P.b_mn)
+                oz::tma_load_2d(db, &P.tmB, (int32_t)n0, k0, bar);
+            else
+                oz::tma_load_2d(db, &P.tmB, k0, (int32_t)n0, bar);
+        }
         cur[2] += 1;
         if (ld_kt + 1 == P.ktiles) {
             cur[1] = 0;
@@ -922,6 +942,7 @@ __global__ void __launch_bounds__(CF::THREADS, 1) dmma_tma_dec_kernel(const __gr
     // before the CTA's shared memory is released
     if (tid == 0) {
         for (uint32_t j = it; j < (uint32_t)cur[2]; ++j) {
+            if (P.test_stall == 1 && j == 0) continue;  // the withheld stage has nothing in flight
             long long t0 = clock64();
             while (!oz::mbar_try(oz::su32(full + (j % STAGES)), (j / STAGES) & 1) && clock64() - t0 < oz::WAIT_BUDGET) {
             }
@@ -1059,6 +1080,7 @@ static cudaError_t try_tma(dgt_context* h, const Problem& p, const KSegment& sg,
     prm.a_mn = a_mn;
     prm.b_mn = b_mn;
     prm.err = h->dev_error;
+    prm.test_stall = h->test_stall;
     *used = true;
     if constexpr (DEC)
         return launch_tma_dec_variant<CF, EARLY>(prm, grid, h->stream);
@@ -1097,6 +1119,7 @@ dgt_status launch_dmma_grouped(dgt_context* h, std::vector<Problem>& probs, cons
     prm.total_tiles = (int)tiles;
     prm.red_flags = reduces ? red_flags : nullptr;
     prm.err = h->dev_error;
+    prm.test_stall = h->test_stall;
     if ((int)live.size() <= MAX_INLINE_PROBS && (int)segs.size() <= MAX_INLINE_SEGS) {
         prm.probs = nullptr;
         prm.segs = nullptr;

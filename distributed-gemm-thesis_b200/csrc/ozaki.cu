@@ -412,7 +412,7 @@ static dgt_status ozaki_run(dgt_context* h, cudaStream_t s, int num_sms, unsigne
         prm.groups_ext = dgroups;
     }
     prm.err = err;
-    prm.test_stall = h ? h->test_stall : 0;
+    prm.test_stall = (h && h->test_stall == 1) ? 1 : 0;
     const int tiles = prm.tiles_m * prm.tiles_n;
     const int grid = std::min(tiles, num_sms);
     if (h) mark(h, 1);
@@ -754,7 +754,7 @@ dgt_status ozaki_dgemm_grouped(dgt_context* h, const std::vector<OzProblem>& pro
     prm.segs_ext = nullptr;
     prm.groups_ext = nullptr;
     prm.err = h->dev_error;
-    prm.test_stall = h->test_stall;
+    prm.test_stall = h->test_stall == 1 ? 1 : 0;
     prm.gprobs = d_gp;
     prm.prob_tiles = d_tiles;
     prm.nprob = T;

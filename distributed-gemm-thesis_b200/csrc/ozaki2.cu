@@ -842,7 +842,7 @@ static dgt_status ozaki2_residue_gemm(dgt_context* h, cudaStream_t s, const Oz2S
     prm.res_ld = m_pad;
     prm.res_plane = m_pad * n_pad;
     prm.err = h->dev_error;
-    prm.test_stall = h->test_stall;
+    prm.test_stall = h->test_stall == 1 ? 1 : 0;
     if (sh.dyn && sched) {  // the unit counter starts at zero for every launch
         DGT_CUDA_TRY(h, cudaMemsetAsync(sched, 0, sizeof(int32_t), s));
         prm.sched = sched;

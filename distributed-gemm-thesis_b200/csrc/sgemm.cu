@@ -184,7 +184,7 @@ static dgt_status sgemm_split(dgt_context* h, bool ta, bool tb, int64_t m, int64
     std::copy(segs.begin(), segs.end(), prm.segs);
     std::copy(groups.begin(), groups.end(), prm.groups);
     prm.err = h->dev_error;
-    prm.test_stall = h->test_stall;
+    prm.test_stall = h->test_stall == 1 ? 1 : 0;
     prm.Cf = C;
     prm.alpha_f = alpha;
     prm.beta_f = beta;
