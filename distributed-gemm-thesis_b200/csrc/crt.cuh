@@ -72,11 +72,27 @@ constexpr int SPLIT_BITS = 79;  // scaled operands are integers of magnitude bel
 // n magic = t magic + bias.  r = t - floor(n / p) p is the symmetric residue
 // ((Y + floor(p/2)) mod p) - floor(p/2) minus 2^21 p, a multiple of 256, so the low byte of r
 // is the symmetric residue as int8.
+//
+// The first nfp moduli take the same residue through the FP64 pipe instead (the integer pipe
+// is the split's bound): t = fma(yh, c40, yl) is exact (|t| < 2^39 127 + 2^39 < 2^47),
+// q = rint(t / p) from one FMA with fl(1/p) and the round-to-integer constant 1.5 2^52
+// (|t / p| < 2^40, so the product is within 2^-12 of t / p, while t / p lies at least
+// 1 / (2p) >= 2^-9 from a half-integer for odd p; for p = 256 the product is exact and a tie
+// gives r = +-128), r = t - q p exactly, and r + 1.5 2^52 carries r in its low 32 bits.  For
+// odd p, r is the symmetric residue; for p = 256 its byte is the integer path's 0x80 at a
+// tie: the planes are the same bytes either way.  At 16384^2, 14 moduli, both operands'
+// amax + norm bound + split took 7.0-7.4 ms with every modulus on the integer path, 6.0-6.5
+// with 5 on the FP64 path, 5.6-5.7 with 9, 5.8 with 11 and 5.6-5.8 with all 14.
+#ifndef DGT_SPLIT_FP64_MODULI
+#define DGT_SPLIT_FP64_MODULI 9
+#endif
 struct ModTable {
     int32_t p[MAX_MODULI];
     int32_t c20[MAX_MODULI], c40[MAX_MODULI], c60[MAX_MODULI];  // 2^20, 2^40, 2^60 mod p, symmetric
     int32_t magic[MAX_MODULI];                                 // floor(2^38 / p) + 1 (< 2^31 for p > 128)
     long long bias[MAX_MODULI];                                // (floor(p/2) + 2^21 p) magic
+    double c40d[MAX_MODULI], invp[MAX_MODULI], pd[MAX_MODULI];  // the FP64 path's c40, fl(1/p), p
+    int32_t nfp;                                               // moduli [0, nfp) take the FP64 path
 };
 // Residue split geometry: a block of 128 threads covers RES_ROWS rows (mn) and RES_KSPAN
 // consecutive kk, one 32-byte sector of every plane row; RES_TPR threads share a row, each

@@ -131,6 +131,9 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
         mt.c60[i] = sym((1ull << 60) % p);
         mt.magic[i] = (int32_t)((1ull << 38) / p + 1);
         mt.bias[i] = ((long long)(p >> 1) + ((long long)p << 21)) * mt.magic[i];
+        mt.c40d[i] = (double)mt.c40[i];
+        mt.invp[i] = 1.0 / (double)p;
+        mt.pd[i] = (double)p;
         Big M = P;
         big_div_small(M, p);  // M = P / p
         Big Mm = M;
@@ -141,6 +144,7 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
             cc.Wd[i][l] = (double)cc.W[i][l];
         }
     }
+    mt.nfp = std::min(n, DGT_SPLIT_FP64_MODULI);
     for (int l = 0; l <= MAX_NW; ++l) cc.P[l] = l < (int)P.size() ? P[l] : 0;
     double pd = 0;
     for (int l = MAX_NW; l >= 0; --l) pd = pd * 4294967296.0 + (double)cc.P[l];
@@ -316,6 +320,7 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
     }
     // Y = x3 2^60 + x2 2^40 + x1 2^20 + x0 (crt.cuh ModTable): x0, x2 in [0, 2^20), |x1|, |x3| <= 2^19
     int32_t x0[E], x1[E], x2[E], x3[E];
+    double yhd[E], yld[E];  // Y = yh 2^40 + yl as doubles, for the FP64 path
 #pragma unroll
     for (int i = 0; i < E; ++i) {
         const int64_t kk = k0 + i;
@@ -324,13 +329,41 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
         // y = a 2^sc exactly; Y = rn(y) = yh 2^40 + yl, |yh|, |yl| <= 2^39
         const double y = live ? (direct ? a * fsc : oz::scale2(a, sc)) : 0.0;
         const double yh = rint(y * 0x1p-40);
-        const long long hi = __double2ll_rn(yh), lo = __double2ll_rn(fma(-yh, 0x1p40, y));
+        const double yl = rint(fma(-yh, 0x1p40, y));  // the second rounding: Y = yh 2^40 + yl
+        yhd[i] = yh;
+        yld[i] = yl;
+        const long long hi = __double2ll_rn(yh), lo = __double2ll_rn(yl);
         x0[i] = (int32_t)(lo & 0xfffff);
         x1[i] = (int32_t)(lo >> 20);
         x2[i] = (int32_t)(hi & 0xfffff);
         x3[i] = (int32_t)(hi >> 20);
     }
-    for (int j = 0; j < nmod; ++j, out += plane) {
+    constexpr double RINT = 6755399441055744.0;  // 1.5 2^52: adding it rounds to an integer
+    const int nfp = min(mt.nfp, nmod);
+    for (int j = 0; j < nfp; ++j, out += plane) {
+        const double c40 = mt.c40d[j], ip = mt.invp[j], pd = mt.pd[j];
+        uint32_t w[E / 4];
+#pragma unroll
+        for (int q = 0; q < E / 4; ++q) {
+            int32_t r[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = 4 * q + u;
+                const double t = fma(yhd[i], c40, yld[i]);       // = Y mod p, |t| < 2^47, exact
+                const double qd = fma(t, ip, RINT) - RINT;       // rint(t / p)
+                r[u] = __double2loint(fma(-qd, pd, t) + RINT);  // t - q p, exact, in its low word
+            }
+            w[q] = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+        }
+        if constexpr (E % 16 == 0) {
+#pragma unroll
+            for (int q = 0; q < E / 16; ++q)
+                reinterpret_cast<uint4*>(out)[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+        } else {
+            *reinterpret_cast<uint2*>(out) = make_uint2(w[0], w[1]);
+        }
+    }
+    for (int j = nfp; j < nmod; ++j, out += plane) {
         const int32_t p = mt.p[j], c20 = mt.c20[j], c40 = mt.c40[j], c60 = mt.c60[j], mg = mt.magic[j];
         const long long bias = mt.bias[j];
         uint32_t w[E / 4];
