@@ -490,6 +490,32 @@ def ozaki2_split_residues(y, p: int):
     return (r & 0xFF).astype(np.uint8).view(np.int8)
 
 
+def _fma(a: float, b: float, c: float) -> float:
+    """a b + c rounded once to the nearest double (ties to even): exact rational arithmetic,
+    then Python's correctly rounded float()."""
+    from fractions import Fraction
+
+    return float(Fraction(a) * Fraction(b) + Fraction(c))
+
+
+def ozaki2_split_residues_fp64(y, p: int):
+    """The kernels' FP64 residue path (csrc/crt.cuh ModTable, the first moduli of
+    csrc/ozaki2.cu residue_block) restated step by step with exactly rounded FMAs: yh =
+    rint(y 2^-40), yl = rint(y - yh 2^40), t = fma(yh, c40, yl), q = fma(t, fl(1/p), 1.5 2^52)
+    - 1.5 2^52, r = fma(-q, p, t); the int8 byte of r.  Small samples only (pure Python)."""
+    RINT = 6755399441055744.0
+    c40 = float((2 ** 40 % p) - p if 2 ** 40 % p > p // 2 else 2 ** 40 % p)
+    out = []
+    for v in np.asarray(y, dtype=np.float64).ravel():
+        yh = float(np.rint(float(v) * 2.0 ** -40))
+        yl = float(np.rint(_fma(-yh, 2.0 ** 40, float(v))))
+        t = _fma(yh, c40, yl)
+        q = _fma(t, 1.0 / p, RINT) - RINT
+        r = int(_fma(-q, float(p), t))
+        out.append(((r & 0xFF) ^ 0x80) - 0x80)
+    return np.array(out, dtype=np.int8)
+
+
 def ozaki2_sigmas(nmod: int, k: int):
     """(sigma_A, sigma_B) for nmod moduli and inner dimension k: s = sigma_A + sigma_B is the
     largest with (2^ceil(s/2) + sqrt(k)/2)(2^floor(s/2) + sqrt(k)/2) < (P/2)(1 - 2^-20), checked

@@ -71,6 +71,23 @@ def test_residue_split_arithmetic():
         assert got.tolist() == want, p
 
 
+def test_fp64_residue_path_gives_the_same_bytes():
+    """The split's FP64 path (ozaki2_split_residues_fp64: exact t = yh c40 + yl, q = rint(t/p)
+    by one FMA with fl(1/p), r = t - q p) writes the integer path's bytes for every modulus:
+    non-integer y (the second rounding), exact ties of p = 256 (r = +-128, byte 0x80), and the
+    range edges."""
+    rng = np.random.default_rng(9)
+    edges = []
+    for e in (0, 1, 8, 39, 40, 41, 52, 53, 77):
+        for d in (-1.0, -0.5, 0.0, 0.5, 1.0):
+            edges += [2.0 ** e + d, -(2.0 ** e + d)]
+    ties = [128.0 + 256.0 * j for j in range(-3, 4)] + [2.0 ** 40 * 3 + 128.0, -(2.0 ** 45) - 128.0]
+    mags = np.ldexp(rng.random(300) + 0.5, rng.integers(-3, 78, 300))
+    y = np.concatenate([np.array(edges + ties), mags * np.where(rng.random(300) < 0.5, -1.0, 1.0)])
+    for p in O.OZAKI2_MODULI:
+        assert O.ozaki2_split_residues_fp64(y, p).tolist() == O.ozaki2_split_residues(y, p).tolist(), p
+
+
 def _exact_max_scaled(A, B, nmod):
     """The same integer emulation with every row / column scaled by its max instead (the
     bound k 2^(2 beta) < P/2): the reference point the norm scaling improves on."""
