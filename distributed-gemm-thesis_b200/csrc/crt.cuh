@@ -108,7 +108,12 @@ struct CrtConst {
     uint32_t P[MAX_NW + 1];
     double kq[MAX_NW + 1];                      // 2^(32 l) / P: X / P ~ sum_l x_l kq_l
     double Wd[MAX_MODULI][MAX_NW];              // W as doubles (exact: every limb < 2^32)
+    // the FP64 reconstruction (at most F3_MAX moduli): W and P in three 41-bit limbs as
+    // doubles, and fl(2^(41 l) / P)
+    double Wf[MAX_MODULI][3];
+    double Pf[3], Kf[3];
 };
+constexpr int F3_MAX = 15;  // 15 terms r W_l < 2^49 sum below 2^53; P < 2^123 for 15 moduli
 
 // One product of a grouped reconstruction: its residue planes, exponents, scaling and output;
 // it owns threads [thread_begin, thread_begin + ceil(m/4) n) of the launch.  count > 1 makes

@@ -149,6 +149,27 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
     double pd = 0;
     for (int l = MAX_NW; l >= 0; --l) pd = pd * 4294967296.0 + (double)cc.P[l];
     for (int l = 0; l <= MAX_NW; ++l) cc.kq[l] = std::ldexp(1.0, 32 * l) / pd;
+    // 41-bit limbs (bits [41 l, 41 l + 41)) for the FP64 reconstruction
+    auto limb41 = [](const Big& x, int l) {
+        uint64_t v = 0;
+        for (int b = 0; b < 41; ++b) {
+            const int bit = 41 * l + b, w = bit / 32;
+            if (w < (int)x.size() && ((x[w] >> (bit % 32)) & 1u)) v |= 1ull << b;
+        }
+        return (double)v;
+    };
+    for (int i = 0; i < n; ++i) {
+        Big M = P;
+        big_div_small(M, (uint32_t)kModuli[i]);
+        Big Mm = M;
+        const uint32_t m_mod = big_div_small(Mm, (uint32_t)kModuli[i]);
+        big_mul_small(M, inv_mod(m_mod, (uint32_t)kModuli[i]));  // W_i, as above
+        for (int l = 0; l < 3; ++l) cc.Wf[i][l] = limb41(M, l);
+    }
+    for (int l = 0; l < 3; ++l) {
+        cc.Pf[l] = limb41(P, l);
+        cc.Kf[l] = std::ldexp(1.0, 41 * l) / pd;
+    }
 }
 
 // ---- device: row norms ---------------------------------------------------------------------------
@@ -461,6 +482,62 @@ __device__ __forceinline__ void limbs_addsub(uint32_t (&x)[N], const uint32_t (&
     }
 }
 
+// x + y rounded to odd: the exact sum when it is a double, else the neighbour of the exact
+// sum (toward zero or away) whose last mantissa bit is 1 -- the round-toward-zero result with
+// that bit set.  TwoSum (Knuth) tells exact from inexact.
+__device__ __forceinline__ double add_round_odd(double x, double y) {
+    const double s = __dadd_rn(x, y);
+    const double bb = __dsub_rn(s, x);
+    const double e = __dadd_rn(__dsub_rn(x, __dsub_rn(s, bb)), __dsub_rn(y, bb));
+    if (e == 0.0) return s;
+    return __longlong_as_double(__double_as_longlong(__dadd_rz(x, y)) | 1ll);
+}
+// a + b + c rounded once to the nearest double (ties to even): Boldo and Melquiond's adder
+// ("Emulation of FMA and correctly rounded sums: proved algorithms using rounding to odd",
+// IEEE Trans. Computers 57(4), 2008): two TwoSums, the two error terms added with rounding to
+// odd, then one rounding to nearest.  Valid for doubles without underflow or overflow.
+__device__ __forceinline__ double sum3_rn(double a, double b, double c) {
+    const double uh = __dadd_rn(b, c);
+    const double ub = __dsub_rn(uh, b);
+    const double ul = __dadd_rn(__dsub_rn(b, __dsub_rn(uh, ub)), __dsub_rn(c, ub));
+    const double th = __dadd_rn(a, uh);
+    const double tb = __dsub_rn(th, a);
+    const double tl = __dadd_rn(__dsub_rn(a, __dsub_rn(th, tb)), __dsub_rn(uh, tb));
+    return __dadd_rn(th, add_round_odd(tl, ul));
+}
+
+// The same value as crt_value, through the FP64 pipe, for at most F3_MAX moduli.  X = S0 +
+// S1 2^41 + S2 2^82 with S_l = sum_j r_j w_jl (w_jl the 41-bit limbs of W_j: every term below
+// 2^49, the sum below 2^53, exact).  q = round(X / P) from S_l fl(2^(41 l) / P) (X / P < 2^12,
+// the estimate within 2^-38, inside the 2^-20 margin), and d_l = S_l - q P_l is exact (both
+// below 2^53), so C' = X - q P = d0 + d1 2^41 + d2 2^82 exactly, rounded once by sum3_rn.  The
+// scaling then runs on the mantissa and exponent crt_value would hand it, so the result is
+// the same double in every case, subnormal results included.
+template <int NM>
+__device__ __forceinline__ double crt_value_f3(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
+                                               int shift) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+    for (int j = 0; j < MAX_MODULI; ++j) {
+        if (NM ? j < NM : j < cc.n) {
+            const uint32_t r = __byte_perm(rr[j], 0u, 0x4440u + (uint32_t)sel);  // byte sel
+            const double rd = __hiloint2double(0x43300000, (int)r) - 4503599627370496.0;
+            s0 = fma(rd, cc.Wf[j][0], s0);
+            s1 = fma(rd, cc.Wf[j][1], s1);
+            s2 = fma(rd, cc.Wf[j][2], s2);
+        }
+    }
+    const double q = rint(fma(s2, cc.Kf[2], fma(s1, cc.Kf[1], s0 * cc.Kf[0])));
+    const double d0 = fma(-q, cc.Pf[0], s0), d1 = fma(-q, cc.Pf[1], s1), d2 = fma(-q, cc.Pf[2], s2);
+    const double z = sum3_rn(d2 * 0x1p82, d1 * 0x1p41, d0);
+    if (z == 0.0) return 0.0;
+    // z = m 2^ez with m in [1, 2): hand scale2 the mantissa in [2^63, 2^64) as crt_value does
+    const long long bits = __double_as_longlong(z);
+    const int ez = (int)((bits >> 52) & 0x7ff) - 1023;
+    const double zm = __longlong_as_double((bits & ~(0x7ffll << 52)) | ((long long)(1023 + 63) << 52));
+    return oz::scale2(zm, ez - 63 + shift);
+}
+
 // X = sum_j r_j W_j (NW-limb W, NX = NW + 1 limbs for X < 2^13 P) reduced mod P into the
 // symmetric range, rounded to FP64 once (round to nearest even), times 2^shift.  r_j is byte
 // `sel` of rr[j]; NM is the modulus count when known at compile time (0: cc.n).  Constant trip
@@ -468,6 +545,10 @@ __device__ __forceinline__ void limbs_addsub(uint32_t (&x)[N], const uint32_t (&
 template <int NW, int NM>
 __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
                                             int shift) {
+    if constexpr (NM != 0 && NM <= F3_MAX) {
+        return crt_value_f3<NM>(rr, sel, cc, shift);  // the FP64 form (same value)
+    } else {
+    if (NM == 0 && cc.n <= F3_MAX) return crt_value_f3<0>(rr, sel, cc, shift);
     constexpr int NX = NW + 1;
     // The low NI limbs accumulate in 64-bit integers, the high ones in FP64, which is exact:
     // r W_l < 2^40 and at most 20 of them sum below 2^45 < 2^53.  Splitting the multiply-adds
@@ -557,6 +638,7 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
     const double d = __ull2double_rn(top64 | (uint64_t)sticky);
     const double mag = oz::scale2(d, 64 * ti - lz + shift);
     return neg ? -mag : mag;
+    }
 }
 
 // Rows row0 .. row0+3 of column col of one product: residue planes [j][col][row] with leading

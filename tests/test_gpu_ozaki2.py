@@ -56,6 +56,21 @@ def test_bitwise_for_every_kernel_specialisation(h, nmod):
     assert np.array_equal(got, O.ozaki2_exact(A, B, nmod))
 
 
+@pytest.mark.parametrize("nmod", [9, 14, 15, 17])
+@pytest.mark.parametrize("scale", [-540, 0, 500])
+def test_bitwise_across_the_exponent_range(h, nmod, scale):
+    """Products that land in the subnormal range (~2^-1080), near 1 and near the overflow
+    threshold (~2^1000), with a wide dynamic range inside each row: bit for bit the exact
+    restatement (the exact integer product rounded once, then scaled) for both reconstruction
+    forms -- three FP64 limbs and a correctly rounded three-term sum up to 15 moduli, 32-bit
+    integer limbs above."""
+    m, n, k = 37, 29, 90
+    A, B, _ = operands("N", "N", m, n, k, 70 + nmod, phi=2.0)
+    A, B = np.ldexp(A, scale), np.ldexp(B, scale)
+    got = run(h, "N", "N", m, n, k, 1.0, 0.0, nmod, A, B, np.zeros((m, n)))
+    assert np.array_equal(got, O.ozaki2_exact(A, B, nmod))
+
+
 @pytest.mark.parametrize("shape", [(300, 200, 1000), (513, 257, 4100)])
 def test_alpha_beta_against_fp64(h, shape):
     m, n, k = shape
