@@ -516,6 +516,33 @@ def ozaki2_split_residues_fp64(y, p: int):
     return np.array(out, dtype=np.int8)
 
 
+def sum3_rn(a: float, b: float, c: float) -> float:
+    """The reconstruction's correctly rounded sum of three doubles (csrc/ozaki2.cu sum3_rn,
+    Boldo and Melquiond's adder with rounding to odd) restated step by step: two TwoSums, the
+    error terms added with rounding to odd (the round-toward-zero sum with its last bit set
+    when inexact), one rounding to nearest."""
+    import math
+    import struct
+    from fractions import Fraction
+
+    def two_sum(x, y):
+        s = x + y
+        bb = s - x
+        return s, (x - (s - bb)) + (y - bb)
+
+    def add_round_odd(x, y):
+        s, e = two_sum(x, y)
+        if e == 0.0:
+            return s
+        t = s if abs(Fraction(s)) <= abs(Fraction(x) + Fraction(y)) else math.nextafter(s, 0.0)  # toward zero
+        bits = struct.unpack("<q", struct.pack("<d", t))[0] | 1
+        return struct.unpack("<d", struct.pack("<q", bits))[0]
+
+    uh, ul = two_sum(b, c)
+    th, tl = two_sum(a, uh)
+    return th + add_round_odd(tl, ul)
+
+
 def ozaki2_sigmas(nmod: int, k: int):
     """(sigma_A, sigma_B) for nmod moduli and inner dimension k: s = sigma_A + sigma_B is the
     largest with (2^ceil(s/2) + sqrt(k)/2)(2^floor(s/2) + sqrt(k)/2) < (P/2)(1 - 2^-20), checked

@@ -88,6 +88,34 @@ def test_fp64_residue_path_gives_the_same_bytes():
         assert O.ozaki2_split_residues_fp64(y, p).tolist() == O.ozaki2_split_residues(y, p).tolist(), p
 
 
+def test_three_term_sum_is_correctly_rounded():
+    """The reconstruction's final rounding (oracle.sum3_rn restates the kernel's steps): the
+    sum d2 2^82 + d1 2^41 + d0 of three limb differences (integers below 2^53, overlapping)
+    rounds once to nearest-even -- random limbs, heavy cancellation, and values an ulp around
+    exact ties -- against exact rationals."""
+    import random
+    from fractions import Fraction
+
+    rnd = random.Random(11)
+    cases = []
+    for i in range(6000):
+        d0, d1 = rnd.randint(-2 ** 53 + 1, 2 ** 53 - 1), rnd.randint(-2 ** 53 + 1, 2 ** 53 - 1)
+        d2 = rnd.randint(-2 ** 53 + 1, 2 ** 53 - 1) if i % 3 == 0 else rnd.randint(-2 ** 12, 2 ** 12)
+        cases.append((d0, d1, d2))
+    for i in range(3000):  # C = (odd K) 2^(s-1) + delta: one bit past the 53rd, ties and neighbours
+        s_ = rnd.randint(54, 100)
+        C = (2 * rnd.randint(2 ** 52, 2 ** 53 - 1) + 1) * 2 ** (s_ - 54) + rnd.choice([-1, 0, 1])
+        C *= rnd.choice([-1, 1])
+        d2, rem = divmod(C, 2 ** 82)
+        d1, d0 = divmod(rem, 2 ** 41)
+        t = rnd.randint(-2 ** 10, 2 ** 10)  # an overlapping split of the same value
+        cases.append((d0 + t * 2 ** 41, d1 - t, d2))
+    for d0, d1, d2 in cases:
+        a, b, c = float(d2) * 2.0 ** 82, float(d1) * 2.0 ** 41, float(d0)
+        assert (Fraction(a), Fraction(b), Fraction(c)) == (d2 * Fraction(2) ** 82, d1 * Fraction(2) ** 41, d0)
+        assert O.sum3_rn(a, b, c) == float(Fraction(a) + Fraction(b) + Fraction(c)), (d0, d1, d2)
+
+
 def _exact_max_scaled(A, B, nmod):
     """The same integer emulation with every row / column scaled by its max instead (the
     bound k 2^(2 beta) < P/2): the reference point the norm scaling improves on."""
