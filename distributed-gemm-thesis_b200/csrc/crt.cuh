@@ -170,9 +170,19 @@ struct Oz2Work {
 dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmod, Oz2Shape& sh);
 Oz2Work ozaki2_carve(const Oz2Shape& sh, int64_t n, int64_t n_pad, void* ws);
 int64_t ozaki2_n_pad(int64_t n);  // op(B) columns padded to the GEMM's tile width
+// plane_rows: rows between the operand's modulus planes (0: mn_pad), for a panel written into
+// a larger operand's planes (planes then points at the panel's first row of plane 0).
 dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int sigma, const double* X, int64_t ld,
                         int64_t MN, int64_t mn_pad, bool kcontig, unsigned long long* amax, unsigned long long* qn,
-                        int32_t* exps, int8_t* planes);
+                        int32_t* exps, int8_t* planes, int64_t plane_rows = 0);
+// The residue GEMM alone (planes strided as for ozaki2_split's plane_rows; spans are the rows
+// addressable from each planes pointer) and the reconstruction alone.
+dgt_status ozaki2_residue_gemm(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+                               const int8_t* planesA, const int8_t* planesB, uint8_t* res, int32_t* sched,
+                               int64_t a_rows = 0, int64_t a_span = 0, int64_t b_rows = 0, int64_t b_span = 0);
+dgt_status ozaki2_reconstruct(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+                              const uint8_t* res, const int32_t* expA, const int32_t* expB, double alpha, double beta,
+                              double* C, int64_t ldc);
 dgt_status ozaki2_gemm_crt(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
                            const int8_t* planesA, const int32_t* expA, const int8_t* planesB, const int32_t* expB,
                            uint8_t* res, double alpha, double beta, double* C, int64_t ldc,

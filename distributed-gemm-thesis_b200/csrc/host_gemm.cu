@@ -63,13 +63,16 @@ size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 
 // CRT mode in a 2D block order.  op(A) moves in row panels and op(B) in column panels,
 // alternately (A_0, B_0, A_1, B_1, ...); each panel is split into residue planes as soon as it
-// arrives, and every C block whose row and column panels are both split is computed (residue
-// GEMM and reconstruction) and sent back.  The host link's input stream therefore overlaps
-// the arithmetic from the second panel on, instead of op(A) crossing whole before the first
-// panel computes.  The residue planes of every panel stay resident (each row panel meets every
-// column panel); the FP64 staging buffers and the C blocks are double buffered.  Row scaling
-// depends on op(A)'s rows alone and column scaling on op(B)'s columns alone, so every block
-// equals the whole-matrix device call's bit for bit.
+// arrives, straight into its rows of its operand's planes (one [modulus][rows][k] array per
+// operand, so any run of panels is one operand for the GEMM), and the blocks it completes --
+// the new row panel times every column panel so far, or every row panel so far times the new
+// column panel -- run as ONE residue GEMM and one reconstruction, whose result goes back to
+// the host in one strided copy.  The host link's input stream therefore overlaps the
+// arithmetic from the second panel on, instead of op(A) crossing whole before the first panel
+// computes, and the arithmetic runs in 2 R + 2 Q - 2 launches of full-width GEMMs rather than a
+// launch per block.  The FP64 staging buffers and the results are double buffered.  Row
+// scaling depends on op(A)'s rows alone and column scaling on op(B)'s columns alone, so every
+// block equals the whole-matrix device call's bit for bit.
 enum {
     E2_START, E2_AIN0, E2_AIN1, E2_AFREE0, E2_AFREE1, E2_BIN0, E2_BIN1, E2_BFREE0, E2_BFREE1, E2_CIN0, E2_CIN1,
     E2_CREADY0, E2_CREADY1, E2_COUT0, E2_COUT1, E2_JOIN_IN, E2_JOIN_OUT, E2_COUNT
@@ -80,37 +83,36 @@ static dgt_status crt_host_2d(dgt_context* h, bool ta, bool tb, int64_t m, int64
                               double beta, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
                               int64_t ldc, int nmod, int64_t mb, int64_t nb) {
     const bool read_c = beta != 0.0;
+    nb = ozaki2_n_pad(nb);  // column panels of whole 256-wide tiles
     const int64_t R = ceil_div(m, mb), Q = ceil_div(n, nb);
-    Oz2Shape shf, shl;  // the full row panels' shape and the last (ragged) one's
+    Oz2Shape shp;  // constants, scales and kernel variant (the same for every panel)
     dgt_status st;
-    if ((st = ozaki2_shape(h, mb, nb, k, nmod, shf)) != DGT_SUCCESS) return st;
-    if ((st = ozaki2_shape(h, m - (R - 1) * mb, nb, k, nmod, shl)) != DGT_SUCCESS) return st;
-    auto shape_of = [&](int64_t i) -> const Oz2Shape& { return i + 1 < R ? shf : shl; };
-    const int64_t k_pad = shf.k_pad;
-    // workspace: planes of every row and column panel, per-row / per-column scale data, one
-    // block's residue planes, the unit counter, two FP64 staging buffers per operand, two C blocks
+    if ((st = ozaki2_shape(h, m, n, k, nmod, shp)) != DGT_SUCCESS) return st;
+    const int64_t m_unit = shp.pair ? 2 * 128 : 128, k_pad = shp.k_pad;
+    // op(A)'s planes hold every row panel, [modulus][MS rows][k_pad], row panel i at row i mb;
+    // op(B)'s likewise, [modulus][NS rows][k_pad], column panel j at row j nb
+    const int64_t MS = ceil_div(m, m_unit) * m_unit, NS = ozaki2_n_pad(n);
+    if (mb % m_unit) return fail(h, DGT_ERROR_INVALID_VALUE, "row panels of whole tiles");
+    // workspace: both operands' planes, per-row / per-column scale data, the residues and the
+    // FP64 result of the largest merged GEMM (a column of row panels, or a row of column panels),
+    // the unit counter, two FP64 staging buffers per operand, two result buffers
     auto up = [](size_t x) { return (x + 1023) / 1024 * 1024; };
-    std::vector<size_t> offA(R), offB(Q);
-    size_t at = 0;
-    for (int64_t i = 0; i < R; ++i) {
-        offA[i] = at;
-        at += up((size_t)nmod * shape_of(i).m_pad * k_pad);
-    }
-    for (int64_t j = 0; j < Q; ++j) {
-        offB[j] = at;
-        at += up((size_t)nmod * ozaki2_n_pad(std::min(nb, n - j * nb)) * k_pad);
-    }
-    const size_t o_amaxA = at, o_qnA = o_amaxA + up((size_t)m * 8), o_expA = o_qnA + up((size_t)m * 8);
+    const size_t blk = std::max((size_t)MS * nb, (size_t)mb * NS);  // elements of the largest merged result
+    const size_t o_pA = 0, o_pB = up((size_t)nmod * MS * k_pad);
+    const size_t o_amaxA = o_pB + up((size_t)nmod * NS * k_pad), o_qnA = o_amaxA + up((size_t)m * 8),
+                 o_expA = o_qnA + up((size_t)m * 8);
     const size_t o_amaxB = o_expA + up((size_t)m * 4), o_qnB = o_amaxB + up((size_t)n * 8),
                  o_expB = o_qnB + up((size_t)n * 8);
     const size_t o_res = o_expB + up((size_t)n * 4);
-    const size_t o_sched = o_res + up((size_t)nmod * shf.m_pad * ozaki2_n_pad(nb));
-    const size_t stA = up((size_t)mb * k * 8), stB = up((size_t)nb * k * 8), cb = up((size_t)mb * nb * 8);
+    const size_t o_sched = o_res + up((size_t)nmod * blk);
+    const size_t stA = up((size_t)mb * k * 8), stB = up((size_t)nb * k * 8), cb = up(blk * 8);
     const size_t o_stA = o_sched + 1024, o_stB = o_stA + 2 * stA, o_cb = o_stB + 2 * stB, total = o_cb + 2 * cb;
     void* ws = nullptr;
     if ((st = ensure_workspace(h, total, &ws, 3)) != DGT_SUCCESS) return st;
     if ((st = ensure_copy_streams(h)) != DGT_SUCCESS) return st;
     char* base = (char*)ws;
+    auto* planesA = (int8_t*)(base + o_pA);
+    auto* planesB = (int8_t*)(base + o_pB);
     auto* amaxA = (unsigned long long*)(base + o_amaxA);
     auto* qnA = (unsigned long long*)(base + o_qnA);
     auto* expA = (int32_t*)(base + o_expA);
@@ -148,9 +150,9 @@ static dgt_status crt_host_2d(dgt_context* h, bool ta, bool tb, int64_t m, int64
             DGT_CUDA_TRY(h, cudaMemcpy2DAsync(stageA[slot], mi * 8, A + r0, lda * 8, mi * 8, k, cudaMemcpyDefault, si));
         DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_AIN0 + slot], si));
         DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[E2_AIN0 + slot], 0));
-        const Oz2Shape& sh = shape_of(i);
-        if ((st = ozaki2_split(h, s, sh, sh.sa, stageA[slot], ta ? k : mi, mi, sh.m_pad, ta, amaxA + r0, qnA + r0,
-                               expA + r0, (int8_t*)(base + offA[i]))) != DGT_SUCCESS)
+        const int64_t pad = std::min(mb, MS - r0);
+        if ((st = ozaki2_split(h, s, shp, shp.sa, stageA[slot], ta ? k : mi, mi, pad, ta, amaxA + r0, qnA + r0,
+                               expA + r0, planesA + r0 * k_pad, MS)) != DGT_SUCCESS)
             return st;
         DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_AFREE0 + slot], s));
         return DGT_SUCCESS;
@@ -167,50 +169,58 @@ static dgt_status crt_host_2d(dgt_context* h, bool ta, bool tb, int64_t m, int64
                                               si));
         DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_BIN0 + slot], si));
         DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[E2_BIN0 + slot], 0));
-        if ((st = ozaki2_split(h, s, shf, shf.sb, stageB[slot], tb ? wj : k, wj, ozaki2_n_pad(wj), !tb, amaxB + c0,
-                               qnB + c0, expB + c0, (int8_t*)(base + offB[j]))) != DGT_SUCCESS)
+        if ((st = ozaki2_split(h, s, shp, shp.sb, stageB[slot], tb ? wj : k, wj, ozaki2_n_pad(wj), !tb, amaxB + c0,
+                               qnB + c0, expB + c0, planesB + c0 * k_pad, NS)) != DGT_SUCCESS)
             return st;
         DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_BFREE0 + slot], s));
         return DGT_SUCCESS;
     };
-    int64_t blocks = 0;
-    auto compute = [&](int64_t i, int64_t j) -> dgt_status {
-        const int slot = (int)(blocks & 1);
-        const int64_t r0 = i * mb, mi = std::min(mb, m - r0), c0 = j * nb, wj = std::min(nb, n - c0);
-        if (blocks >= 2) {  // the buffer's previous block has left
+    // One merged GEMM: C rows [r0, r0 + rows) x columns [c0, c0 + cols), every block of it
+    // already split -- the row panels up to ia times a new column panel, or a new row panel
+    // times the column panels up to jb -- residue GEMM, reconstruction, result to the host.
+    int64_t merged = 0;
+    auto compute = [&](int64_t r0, int64_t rows, int64_t c0, int64_t cols) -> dgt_status {
+        const int slot = (int)(merged & 1);
+        if (merged >= 2) {  // the buffer's previous result has left
             DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[E2_COUT0 + slot], 0));
             if (read_c) DGT_CUDA_TRY(h, cudaStreamWaitEvent(si, ev[E2_COUT0 + slot], 0));
         }
         if (read_c) {
-            DGT_CUDA_TRY(h, cudaMemcpy2DAsync(cblk[slot], mi * 8, C + r0 + c0 * ldc, ldc * 8, mi * 8, wj,
+            DGT_CUDA_TRY(h, cudaMemcpy2DAsync(cblk[slot], rows * 8, C + r0 + c0 * ldc, ldc * 8, rows * 8, cols,
                                               cudaMemcpyDefault, si));
             DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_CIN0 + slot], si));
             DGT_CUDA_TRY(h, cudaStreamWaitEvent(s, ev[E2_CIN0 + slot], 0));
         }
-        if ((st = ozaki2_gemm_crt(h, s, shape_of(i), wj, ozaki2_n_pad(wj), (const int8_t*)(base + offA[i]),
-                                  expA + r0, (const int8_t*)(base + offB[j]), expB + c0, res, alpha, beta,
-                                  cblk[slot], mi, sched)) != DGT_SUCCESS)
+        Oz2Shape sh = shp;  // the merged GEMM's rows
+        sh.m = rows;
+        sh.m_pad = ceil_div(rows, m_unit) * m_unit;
+        const int64_t cpad = ozaki2_n_pad(cols);
+        if ((st = ozaki2_residue_gemm(h, s, sh, cols, cpad, planesA + r0 * k_pad, planesB + c0 * k_pad, res, sched,
+                                      MS, (int64_t)nmod * MS - r0, NS, (int64_t)nmod * NS - c0)) != DGT_SUCCESS)
+            return st;
+        if ((st = ozaki2_reconstruct(h, s, sh, cols, cpad, res, expA + r0, expB + c0, alpha, beta, cblk[slot],
+                                     rows)) != DGT_SUCCESS)
             return st;
         DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_CREADY0 + slot], s));
         DGT_CUDA_TRY(h, cudaStreamWaitEvent(so, ev[E2_CREADY0 + slot], 0));
-        DGT_CUDA_TRY(h, cudaMemcpy2DAsync(C + r0 + c0 * ldc, ldc * 8, cblk[slot], mi * 8, mi * 8, wj, cudaMemcpyDefault,
-                                          so));
+        DGT_CUDA_TRY(h, cudaMemcpy2DAsync(C + r0 + c0 * ldc, ldc * 8, cblk[slot], rows * 8, rows * 8, cols,
+                                          cudaMemcpyDefault, so));
         DGT_CUDA_TRY(h, cudaEventRecord(ev[E2_COUT0 + slot], so));
-        ++blocks;
+        ++merged;
         return DGT_SUCCESS;
     };
-    // growing rectangle: after each panel, every block it completes
+    // growing rectangle: after each panel, the row or column of blocks it completes, as one GEMM
     int64_t ia = 0, jb = 0;
     while (ia < R || jb < Q) {
         if (ia < R && (ia <= jb || jb >= Q)) {
             if ((st = take_a(ia)) != DGT_SUCCESS) return st;
-            for (int64_t j = 0; j < jb; ++j)
-                if ((st = compute(ia, j)) != DGT_SUCCESS) return st;
+            if (jb > 0 && (st = compute(ia * mb, std::min(mb, m - ia * mb), 0, std::min(jb * nb, n))) != DGT_SUCCESS)
+                return st;
             ++ia;
         } else {
             if ((st = take_b(jb)) != DGT_SUCCESS) return st;
-            for (int64_t i = 0; i < ia; ++i)
-                if ((st = compute(i, jb)) != DGT_SUCCESS) return st;
+            if (ia > 0 && (st = compute(0, std::min(ia * mb, m), jb * nb, std::min(nb, n - jb * nb))) != DGT_SUCCESS)
+                return st;
             ++jb;
         }
     }

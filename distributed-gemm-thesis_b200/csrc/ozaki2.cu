@@ -280,14 +280,15 @@ __device__ __forceinline__ int row_scale_exp(unsigned long long am, unsigned lon
 // ---- device: residue planes ----------------------------------------------------------------------
 // Plane j holds (A' mod p_j) in the symmetric range as int8 at [j][mn][kk] (K-major, row
 // stride pld >= k_pad, mn_pad rows, zero padded to k_pad; pld > k_pad for one piece of a
-// concatenated K).  A thread produces RES_ELEMS consecutive kk of one
+// concatenated K), planes pstride bytes apart (>= mn_pad pld; more for a panel of a larger
+// operand's planes).  A thread produces RES_ELEMS consecutive kk of one
 // mn; the RES_TPR adjacent lanes of a row write one whole 32-byte sector per plane together
 // (lanes that wrote parts of a sector each made L2 fetch the sector from DRAM first).  The
 // seg == 0, by == 0 threads also write exps[mn].
 template <bool K_CONTIG>
 __device__ __forceinline__ void residue_block(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                                              int64_t mn_pad, int64_t k_pad, int64_t pld, int nmod, int sigma,
-                                              const unsigned long long* __restrict__ amax,
+                                              int64_t mn_pad, int64_t k_pad, int64_t pld, int64_t pstride, int nmod,
+                                              int sigma, const unsigned long long* __restrict__ amax,
                                               const unsigned long long* __restrict__ qn, int32_t* __restrict__ exps,
                                               int8_t* __restrict__ planes, const ModTable& mt, int64_t bx,
                                               int64_t by) {
@@ -325,7 +326,7 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
     // it rounds to the integer 0 either way); the general scaling otherwise
     const bool direct = sc >= -1022 && sc <= 1023;
     const double fsc = direct ? oz::pow2i(sc) : 0.0;
-    const int64_t plane = mn_pad * pld;
+    const int64_t plane = pstride;
     int8_t* out = planes + mn * pld + k0;
     if (!live || k0 >= K) {  // padding (or a non-finite row): zero residues, no arithmetic
 #pragma unroll 4
@@ -412,13 +413,13 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
 
 template <bool K_CONTIG>
 __global__ void __launch_bounds__(128) split_residues(const double* __restrict__ X, int64_t ld, int64_t MN, int64_t K,
-                                                      int64_t mn_pad, int64_t k_pad, int nmod, int sigma,
-                                                      const unsigned long long* __restrict__ amax,
+                                                      int64_t mn_pad, int64_t k_pad, int64_t pstride, int nmod,
+                                                      int sigma, const unsigned long long* __restrict__ amax,
                                                       const unsigned long long* __restrict__ qn,
                                                       int32_t* __restrict__ exps, int8_t* __restrict__ planes,
                                                       const __grid_constant__ ModTable mt) {
-    residue_block<K_CONTIG>(X, ld, MN, K, mn_pad, k_pad, k_pad, nmod, sigma, amax, qn, exps, planes, mt, blockIdx.x,
-                            blockIdx.y);
+    residue_block<K_CONTIG>(X, ld, MN, K, mn_pad, k_pad, k_pad, pstride, nmod, sigma, amax, qn, exps, planes, mt,
+                            blockIdx.x, blockIdx.y);
 }
 
 // Every operand of a grouped call in one launch (job table as for the digit split).
@@ -429,10 +430,10 @@ __global__ void __launch_bounds__(128) split_residues_grouped(const oz::SplitJob
     const int64_t local = blk - J.split_begin;
     const int64_t bx = local % J.split_bx, by = local / J.split_bx;
     if (J.kcontig)
-        residue_block<true>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, J.plane_ld, nmod, J.bits, J.amax, J.qn, J.exps,
+        residue_block<true>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, J.plane_ld, J.mn_pad * J.plane_ld, nmod, J.bits, J.amax, J.qn, J.exps,
                             (int8_t*)J.planes, mt, bx, by);
     else
-        residue_block<false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, J.plane_ld, nmod, J.bits, J.amax, J.qn, J.exps,
+        residue_block<false>(J.X, J.ld, J.MN, J.K, J.mn_pad, J.k_pad, J.plane_ld, J.mn_pad * J.plane_ld, nmod, J.bits, J.amax, J.qn, J.exps,
                              (int8_t*)J.planes, mt, bx, by);
 }
 
@@ -902,7 +903,8 @@ dgt_status ozaki2_shape(dgt_context* h, int64_t m, int64_t n, int64_t k, int nmo
 // columns of op(B) (kcontig = !transb), planes padded to mn_pad rows.
 dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int sigma, const double* X, int64_t ld,
                         int64_t MN, int64_t mn_pad, bool kcontig, unsigned long long* amax, unsigned long long* qn,
-                        int32_t* exps, int8_t* planes) {
+                        int32_t* exps, int8_t* planes, int64_t plane_rows) {
+    const int64_t pstride = (plane_rows > 0 ? plane_rows : mn_pad) * sh.k_pad;
     using namespace oz2;
     dgt_status st = ozaki_amax(h, s, X, ld, MN, sh.k, kcontig, amax);
     if (st != DGT_SUCCESS) return st;
@@ -917,11 +919,11 @@ dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int 
     DGT_CUDA_TRY(h, cudaGetLastError());
     dim3 grid((unsigned)ceil_div(mn_pad, RES_ROWS), (unsigned)(sh.k_pad / RES_KSPAN));
     if (kcontig)
-        split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sigma, amax, qn,
-                                                  exps, planes, sh.mt);
+        split_residues<true><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, pstride, sh.nmod, sigma, amax,
+                                                  qn, exps, planes, sh.mt);
     else
-        split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, sh.nmod, sigma, amax, qn,
-                                                   exps, planes, sh.mt);
+        split_residues<false><<<grid, 128, 0, s>>>(X, ld, MN, sh.k, mn_pad, sh.k_pad, pstride, sh.nmod, sigma, amax,
+                                                   qn, exps, planes, sh.mt);
     h->launches.fetch_add(1);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? DGT_SUCCESS : cuda_fail(h, e, "residue split");
@@ -929,23 +931,30 @@ dgt_status ozaki2_split(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int 
 
 // Residue GEMM of split operands (op(A) planes for sh.m rows, op(B) planes for n columns
 // padded to n_pad) into res.
-static dgt_status ozaki2_residue_gemm(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
-                                      const int8_t* planesA, const int8_t* planesB, uint8_t* res, int32_t* sched) {
+// Plane strides: op(A)'s planes a_rows rows apart (0: m_pad), a_span rows addressable from
+// planesA (0: nmod a_rows) -- a row panel of a larger operand's planes starts inside them;
+// likewise op(B).  The GEMM covers sh.m_pad rows and n_pad columns.
+dgt_status ozaki2_residue_gemm(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+                               const int8_t* planesA, const int8_t* planesB, uint8_t* res, int32_t* sched,
+                               int64_t a_rows, int64_t a_span, int64_t b_rows, int64_t b_span) {
     using namespace oz2;
     const int nmod = sh.nmod, tkb = 128;
     const int64_t m = sh.m, m_pad = sh.m_pad, k_pad = sh.k_pad;
     const int64_t m_unit = sh.pair ? 2 * oz::TM : oz::TM;
+    const int64_t ars = a_rows > 0 ? a_rows : m_pad, brs = b_rows > 0 ? b_rows : n_pad;
+    const int64_t aspan = a_span > 0 ? a_span : (int64_t)nmod * ars, bspan = b_span > 0 ? b_span : (int64_t)nmod * brs;
+    if (ars > INT32_MAX || brs > INT32_MAX) return fail(h, DGT_ERROR_UNSUPPORTED, "planes too large");
     CUtensorMap tmA, tmB;
-    if (!oz::make_plane_map(&tmA, (void*)planesA, (int64_t)nmod * m_pad, k_pad, oz::TM, tkb) ||
-        !oz::make_plane_map(&tmB, (void*)planesB, (int64_t)nmod * n_pad, k_pad, sh.pair ? oz::TN / 2 : oz::TN, tkb))
+    if (!oz::make_plane_map(&tmA, (void*)planesA, aspan, k_pad, oz::TM, tkb) ||
+        !oz::make_plane_map(&tmB, (void*)planesB, bspan, k_pad, sh.pair ? oz::TN / 2 : oz::TN, tkb))
         return fail(h, DGT_ERROR_CUDA, "cuTensorMapEncodeTiled failed");
     static thread_local oz::Params prm;
     prm = oz::Params{};
     prm.m = m;
     prm.n = n;
     prm.ldc = m_pad;
-    prm.m_pad = (int32_t)m_pad;
-    prm.n_pad = (int32_t)n_pad;
+    prm.m_pad = (int32_t)ars;
+    prm.n_pad = (int32_t)brs;
     prm.tiles_m = (int32_t)(m_pad / m_unit);
     prm.tiles_n = (int32_t)(n_pad / oz::TN);
     prm.ngroups = nmod;
@@ -976,7 +985,7 @@ static dgt_status ozaki2_residue_gemm(dgt_context* h, cudaStream_t s, const Oz2S
 }
 
 // The reconstruction C = alpha C' + beta C of n columns from their residues.
-static dgt_status ozaki2_reconstruct(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
+dgt_status ozaki2_reconstruct(dgt_context* h, cudaStream_t s, const Oz2Shape& sh, int64_t n, int64_t n_pad,
                                      const uint8_t* res, const int32_t* expA, const int32_t* expB, double alpha,
                                      double beta, double* C, int64_t ldc) {
     using namespace oz2;
