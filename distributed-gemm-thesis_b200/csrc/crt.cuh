@@ -78,20 +78,22 @@ constexpr int SPLIT_BITS = 79;  // scaled operands are integers of magnitude bel
 // q = rint(t / p) from one FMA with fl(1/p) and the round-to-integer constant 1.5 2^52
 // (|t / p| < 2^40, so the product is within 2^-12 of t / p, while t / p lies at least
 // 1 / (2p) >= 2^-9 from a half-integer for odd p; for p = 256 the product is exact and a tie
-// gives r = +-128), r = t - q p exactly, and r + 1.5 2^52 carries r in its low 32 bits.  For
-// odd p, r is the symmetric residue; for p = 256 its byte is the integer path's 0x80 at a
-// tie: the planes are the same bytes either way.  At 16384^2, 14 moduli, both operands'
-// amax + norm bound + split took 7.0-7.4 ms with every modulus on the integer path, 6.0-6.5
-// with 5 on the FP64 path, 5.6-5.7 with 9, 5.8 with 11 and 5.6-5.8 with all 14.
+// gives r = +-128), and r = t - q p is taken in 32-bit integers from the low words of the
+// exact t + 1.5 2^52 and q + 1.5 2^52 (the byte needs r mod 256 only).  For odd p, r is the
+// symmetric residue; for p = 256 its byte is the integer path's 0x80 at a tie: the planes are
+// the same bytes either way.  At 16384^2, 14 moduli, both operands' amax + norm bound + split
+// took 7.0-7.4 ms with every modulus on the integer path, 5.6 with 9 on the FP64 path and 5.4
+// with all of them (the 256-product grouped pass at 15 moduli: 15.8 and 15.2 ms), so every
+// modulus takes the FP64 path; the integer path stays for builds that set a smaller count.
 #ifndef DGT_SPLIT_FP64_MODULI
-#define DGT_SPLIT_FP64_MODULI 9
+#define DGT_SPLIT_FP64_MODULI 20
 #endif
 struct ModTable {
     int32_t p[MAX_MODULI];
     int32_t c20[MAX_MODULI], c40[MAX_MODULI], c60[MAX_MODULI];  // 2^20, 2^40, 2^60 mod p, symmetric
     int32_t magic[MAX_MODULI];                                 // floor(2^38 / p) + 1 (< 2^31 for p > 128)
     long long bias[MAX_MODULI];                                // (floor(p/2) + 2^21 p) magic
-    double c40d[MAX_MODULI], invp[MAX_MODULI], pd[MAX_MODULI];  // the FP64 path's c40, fl(1/p), p
+    double c40d[MAX_MODULI], invp[MAX_MODULI];                 // the FP64 path's c40 and fl(1/p)
     int32_t nfp;                                               // moduli [0, nfp) take the FP64 path
 };
 // Residue split geometry: a block of 128 threads covers RES_ROWS rows (mn) and RES_KSPAN

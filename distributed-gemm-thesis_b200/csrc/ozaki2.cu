@@ -133,7 +133,6 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
         mt.bias[i] = ((long long)(p >> 1) + ((long long)p << 21)) * mt.magic[i];
         mt.c40d[i] = (double)mt.c40[i];
         mt.invp[i] = 1.0 / (double)p;
-        mt.pd[i] = (double)p;
         Big M = P;
         big_div_small(M, p);  // M = P / p
         Big Mm = M;
@@ -363,7 +362,8 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
     constexpr double RINT = 6755399441055744.0;  // 1.5 2^52: adding it rounds to an integer
     const int nfp = min(mt.nfp, nmod);
     for (int j = 0; j < nfp; ++j, out += plane) {
-        const double c40 = mt.c40d[j], ip = mt.invp[j], pd = mt.pd[j];
+        const double c40 = mt.c40d[j], ip = mt.invp[j];
+        const int32_t p = mt.p[j];
         uint32_t w[E / 4];
 #pragma unroll
         for (int q = 0; q < E / 4; ++q) {
@@ -371,9 +371,12 @@ __device__ __forceinline__ void residue_block(const double* __restrict__ X, int6
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const int i = 4 * q + u;
-                const double t = fma(yhd[i], c40, yld[i]);       // = Y mod p, |t| < 2^47, exact
-                const double qd = fma(t, ip, RINT) - RINT;       // rint(t / p)
-                r[u] = __double2loint(fma(-qd, pd, t) + RINT);  // t - q p, exact, in its low word
+                const double t = fma(yhd[i], c40, yld[i]);  // = Y mod p, |t| < 2^47, exact
+                // t + 1.5 2^52 and 1.5 2^52 + rint(t / p) are exact and carry t and q in their
+                // low words (mod 2^32); only the low byte of r = t - q p is kept, so the low
+                // words suffice
+                const int32_t tl = __double2loint(t + RINT), ql = __double2loint(fma(t, ip, RINT));
+                r[u] = tl - ql * p;
             }
             w[q] = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
         }

@@ -501,8 +501,11 @@ def _fma(a: float, b: float, c: float) -> float:
 def ozaki2_split_residues_fp64(y, p: int):
     """The kernels' FP64 residue path (csrc/crt.cuh ModTable, the first moduli of
     csrc/ozaki2.cu residue_block) restated step by step with exactly rounded FMAs: yh =
-    rint(y 2^-40), yl = rint(y - yh 2^40), t = fma(yh, c40, yl), q = fma(t, fl(1/p), 1.5 2^52)
-    - 1.5 2^52, r = fma(-q, p, t); the int8 byte of r.  Small samples only (pure Python)."""
+    rint(y 2^-40), yl = rint(y - yh 2^40), t = fma(yh, c40, yl), the low 32-bit words of
+    t + 1.5 2^52 and of fma(t, fl(1/p), 1.5 2^52) (t and q = rint(t/p) modulo 2^32), r = their
+    32-bit difference t - q p; the int8 byte of r.  Small samples only (pure Python)."""
+    import struct
+
     RINT = 6755399441055744.0
     c40 = float((2 ** 40 % p) - p if 2 ** 40 % p > p // 2 else 2 ** 40 % p)
     out = []
@@ -510,8 +513,9 @@ def ozaki2_split_residues_fp64(y, p: int):
         yh = float(np.rint(float(v) * 2.0 ** -40))
         yl = float(np.rint(_fma(-yh, 2.0 ** 40, float(v))))
         t = _fma(yh, c40, yl)
-        q = _fma(t, 1.0 / p, RINT) - RINT
-        r = int(_fma(-q, float(p), t))
+        lo = lambda d: struct.unpack("<q", struct.pack("<d", d))[0] & 0xFFFFFFFF  # the low word
+        tl, ql = lo(t + RINT), lo(_fma(t, 1.0 / p, RINT))
+        r = (tl - ql * p) & 0xFFFFFFFF
         out.append(((r & 0xFF) ^ 0x80) - 0x80)
     return np.array(out, dtype=np.int8)
 
