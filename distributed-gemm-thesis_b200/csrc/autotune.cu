@@ -83,10 +83,35 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
         cudaEventElapsedTime(ms, e0, e1);
         return DGT_SUCCESS;
     };
-    // Candidates run once untimed, then in ROUNDS interleaved rounds (each candidate once per
-    // round, best of the rounds), so a clock that drifts under the power cap while the tuner
-    // runs favours no candidate by its position in the list.
-    constexpr int ROUNDS = 3;
+    // Candidates are timed in blocks of back-to-back calls, as a step loop runs them: untimed
+    // calls for at least WARM_MS, then the mean of timed calls for at least BLOCK_MS; ROUNDS
+    // interleaved rounds (the best block mean), so a clock that drifts while the tuner runs
+    // favours no candidate by its position in the list.  Under the 1 kW power cap the SM clock
+    // settles within tens of milliseconds of sustained load, at a level set by the kernel's
+    // own power draw, so the fastest variant of one call at full clock need not be the fastest
+    // of a step loop: at 16384^3, 14 moduli, the best single call (CTA per tile, dynamic units)
+    // ran 56.6-57.2 ms per call back to back, the CTA-pair variant (half the operand traffic)
+    // 51.4-52.1 ms at a 40-240 MHz higher clock.
+    constexpr int ROUNDS = 2, MAX_CALLS = 256;
+    constexpr float WARM_MS = 100.f, BLOCK_MS = 200.f;
+    auto time_block = [&](dgt_fp64_mode md, int S, float* mean) -> dgt_status {
+        float t = 0.f, spent = 0.f;
+        for (int c = 0; c < MAX_CALLS && spent < WARM_MS; ++c) {
+            dgt_status st = time_once(md, S, &t);
+            if (st != DGT_SUCCESS) return st;
+            spent += t;
+        }
+        float sum = 0.f;
+        int calls = 0;
+        while (calls < MAX_CALLS && (calls == 0 || sum < BLOCK_MS)) {
+            dgt_status st = time_once(md, S, &t);
+            if (st != DGT_SUCCESS) return st;
+            sum += t;
+            ++calls;
+        }
+        *mean = sum / (float)calls;
+        return DGT_SUCCESS;
+    };
     auto time_rounds = [&](const std::vector<int>& cands, int* knob, dgt_fp64_mode md, int S,
                            std::vector<float>& best) -> dgt_status {
         best.assign(cands.size(), 1e30f);
@@ -94,7 +119,7 @@ dgt_status dgt_autotune_dgemm(dgt_handle_t h, char ta, char tb, int64_t m, int64
             for (size_t c = 0; c < cands.size(); ++c) {
                 *knob = cands[c];
                 float t = 0.f;
-                dgt_status st = time_once(md, S, &t);
+                dgt_status st = time_block(md, S, &t);
                 if (st != DGT_SUCCESS) return st;
                 best[c] = std::min(best[c], t);
             }
