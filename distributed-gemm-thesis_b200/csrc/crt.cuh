@@ -114,8 +114,18 @@ struct CrtConst {
     // doubles, and fl(2^(41 l) / P)
     double Wf[MAX_MODULI][3];
     double Pf[3], Kf[3];
+    // the FP64 limb sums with an integer finish (F3_MAX < n <= F4_MAX): W and P in four 40-bit
+    // limbs as doubles, and fl(2^(40 l) / P)
+    double Wf4[MAX_MODULI][4];
+    double Pf4[4], Kf4[4];
 };
 constexpr int F3_MAX = 15;  // 15 terms r W_l < 2^49 sum below 2^53; P < 2^123 for 15 moduli
+// 20 terms r W_l < 2^48 sum below 2^53; P < 2^160 for 20 moduli.  A build with
+// DGT_RECON_F4 = 0 runs the integer limb path above 15 moduli instead (same doubles).
+#ifndef DGT_RECON_F4
+#define DGT_RECON_F4 1
+#endif
+constexpr int F4_MAX = DGT_RECON_F4 ? 20 : 0;
 
 // One product of a grouped reconstruction: its residue planes, exponents, scaling and output;
 // it owns threads [thread_begin, thread_begin + ceil(m/4) n) of the launch.  count > 1 makes

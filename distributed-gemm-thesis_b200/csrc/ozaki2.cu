@@ -148,15 +148,17 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
     double pd = 0;
     for (int l = MAX_NW; l >= 0; --l) pd = pd * 4294967296.0 + (double)cc.P[l];
     for (int l = 0; l <= MAX_NW; ++l) cc.kq[l] = std::ldexp(1.0, 32 * l) / pd;
-    // 41-bit limbs (bits [41 l, 41 l + 41)) for the FP64 reconstruction
-    auto limb41 = [](const Big& x, int l) {
+    // 41-bit limbs (bits [41 l, 41 l + 41)) for the FP64 reconstruction, 40-bit ones for the
+    // FP64 limb sums with the integer finish
+    auto limb = [](const Big& x, int l, int width) {
         uint64_t v = 0;
-        for (int b = 0; b < 41; ++b) {
-            const int bit = 41 * l + b, w = bit / 32;
+        for (int b = 0; b < width; ++b) {
+            const int bit = width * l + b, w = bit / 32;
             if (w < (int)x.size() && ((x[w] >> (bit % 32)) & 1u)) v |= 1ull << b;
         }
         return (double)v;
     };
+    auto limb41 = [&](const Big& x, int l) { return limb(x, l, 41); };
     for (int i = 0; i < n; ++i) {
         Big M = P;
         big_div_small(M, (uint32_t)kModuli[i]);
@@ -164,10 +166,15 @@ void crt_constants(int n, CrtConst& cc, ModTable& mt) {
         const uint32_t m_mod = big_div_small(Mm, (uint32_t)kModuli[i]);
         big_mul_small(M, inv_mod(m_mod, (uint32_t)kModuli[i]));  // W_i, as above
         for (int l = 0; l < 3; ++l) cc.Wf[i][l] = limb41(M, l);
+        for (int l = 0; l < 4; ++l) cc.Wf4[i][l] = limb(M, l, 40);
     }
     for (int l = 0; l < 3; ++l) {
         cc.Pf[l] = limb41(P, l);
         cc.Kf[l] = std::ldexp(1.0, 41 * l) / pd;
+    }
+    for (int l = 0; l < 4; ++l) {
+        cc.Pf4[l] = limb(P, l, 40);
+        cc.Kf4[l] = std::ldexp(1.0, 40 * l) / pd;
     }
 }
 
@@ -542,6 +549,77 @@ __device__ __forceinline__ double crt_value_f3(const uint32_t (&rr)[MAX_MODULI],
     return oz::scale2(zm, ez - 63 + shift);
 }
 
+// The same value as crt_value for F3_MAX < n <= F4_MAX moduli: the limb sums through the FP64
+// pipe, the rounding in integers.  X = S0 + S1 2^40 + S2 2^80 + S3 2^120 with
+// S_l = sum_j r_j w_jl (w_jl the 40-bit limbs of W_j: every term below 2^48, at most 20 of
+// them below 2^53, exact).  q = round(X / P) from S_l fl(2^(40 l) / P) (X / P < 20 * 255 <
+// 2^13, the estimate within 2^-37, inside the 2^-21 margin the norm rule leaves), and
+// d_l = S_l - q P_l is exact (q P_l < 2^53, the difference an integer below 2^53).  The d_l
+// become 64-bit integers, carries make the low three 40-bit digits non-negative (the top one
+// keeps the sign: |C'| < P / 2 < 2^159), and the digits pack into three 64-bit words of C' in
+// two's complement.  Its magnitude is rounded exactly as crt_value rounds it (top word, the
+// word below, a sticky bit for the rest, one conversion), so the result is the same double.
+template <int NM>
+__device__ __forceinline__ double crt_value_f4(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
+                                               int shift) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+    for (int j = 0; j < MAX_MODULI; ++j) {
+        if (NM ? j < NM : j < cc.n) {
+            const uint32_t r = __byte_perm(rr[j], 0u, 0x4440u + (uint32_t)sel);  // byte sel
+            const double rd = __hiloint2double(0x43300000, (int)r) - 4503599627370496.0;
+            s0 = fma(rd, cc.Wf4[j][0], s0);
+            s1 = fma(rd, cc.Wf4[j][1], s1);
+            s2 = fma(rd, cc.Wf4[j][2], s2);
+            s3 = fma(rd, cc.Wf4[j][3], s3);
+        }
+    }
+    const double q = rint(fma(s3, cc.Kf4[3], fma(s2, cc.Kf4[2], fma(s1, cc.Kf4[1], s0 * cc.Kf4[0]))));
+    long long d0 = __double2ll_rn(fma(-q, cc.Pf4[0], s0)), d1 = __double2ll_rn(fma(-q, cc.Pf4[1], s1));
+    long long d2 = __double2ll_rn(fma(-q, cc.Pf4[2], s2)), d3 = __double2ll_rn(fma(-q, cc.Pf4[3], s3));
+    constexpr long long M40 = (1ll << 40) - 1;
+    d1 += d0 >> 40;  // arithmetic shifts: floor division by 2^40
+    d0 &= M40;
+    d2 += d1 >> 40;
+    d1 &= M40;
+    d3 += d2 >> 40;
+    d2 &= M40;
+    // C' = d3 2^120 + d2 2^80 + d1 2^40 + d0, digits d0..d2 in [0, 2^40), as words
+    uint64_t w0 = (uint64_t)d0 | ((uint64_t)d1 << 40);
+    uint64_t w1 = ((uint64_t)d1 >> 24) | ((uint64_t)d2 << 16) | ((uint64_t)d3 << 56);
+    uint64_t w2 = (uint64_t)(d3 >> 8);
+    const bool neg = d3 < 0;
+    if (neg) {  // magnitude -C' (three-word two's complement negation)
+        const uint64_t n0 = ~w0 + 1ull;
+        const uint64_t c0 = w0 == 0ull ? 1ull : 0ull;
+        const uint64_t n1 = ~w1 + c0;
+        const uint64_t c1 = (c0 != 0ull && w1 == 0ull) ? 1ull : 0ull;
+        w2 = ~w2 + c1;
+        w1 = n1;
+        w0 = n0;
+    }
+    uint64_t hi = w0, lo = 0ull;
+    bool sticky = false;
+    int ti = 0;
+    if (w2 != 0ull) {
+        hi = w2;
+        lo = w1;
+        sticky = w0 != 0ull;
+        ti = 2;
+    } else if (w1 != 0ull) {
+        hi = w1;
+        lo = w0;
+        ti = 1;
+    }
+    if (hi == 0ull) return 0.0;
+    const int lz = __clzll((long long)hi);
+    const uint64_t top64 = lz ? (hi << lz) | (lo >> (64 - lz)) : hi;
+    sticky |= (lz ? (lo << lz) : lo) != 0ull;
+    const double d = __ull2double_rn(top64 | (uint64_t)sticky);
+    const double mag = oz::scale2(d, 64 * ti - lz + shift);
+    return neg ? -mag : mag;
+}
+
 // X = sum_j r_j W_j (NW-limb W, NX = NW + 1 limbs for X < 2^13 P) reduced mod P into the
 // symmetric range, rounded to FP64 once (round to nearest even), times 2^shift.  r_j is byte
 // `sel` of rr[j]; NM is the modulus count when known at compile time (0: cc.n).  Constant trip
@@ -551,6 +629,8 @@ __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], in
                                             int shift) {
     if constexpr (NM != 0 && NM <= F3_MAX) {
         return crt_value_f3<NM>(rr, sel, cc, shift);  // the FP64 form (same value)
+    } else if constexpr (NM != 0 && NM <= F4_MAX) {
+        return crt_value_f4<NM>(rr, sel, cc, shift);  // FP64 limb sums, integer rounding (same value)
     } else {
     if (NM == 0 && cc.n <= F3_MAX) return crt_value_f3<0>(rr, sel, cc, shift);
     constexpr int NX = NW + 1;

@@ -46,24 +46,26 @@ def test_bitwise_equal_to_exact_restatement(h, ta, tb, shape):
     assert np.array_equal(got, O.ozaki2_exact(A, B, 17, ta, tb))
 
 
-@pytest.mark.parametrize("nmod", [8, 12, 14, 15, 16, 20])
+@pytest.mark.parametrize("nmod", [8, 12, 14, 15, 16, 17, 18, 19, 20])
 def test_bitwise_for_every_kernel_specialisation(h, nmod):
-    """The reconstruction has limb-count / modulus-count specialisations (14 to 17 unpredicated,
-    the rest generic): each equals the exact restatement bit for bit."""
+    """The reconstruction has modulus-count specialisations (14 to 20; three 41-bit FP64 limbs
+    and a correctly rounded three-term sum up to 15 moduli, four 40-bit FP64 limbs with an
+    integer rounding above) and generic kernels for the other counts: each equals the exact
+    restatement bit for bit."""
     m, n, k = 97, 60, 300
     A, B, C = operands("N", "N", m, n, k, 50 + nmod, phi=1.0)
     got = run(h, "N", "N", m, n, k, 1.0, 0.0, nmod, A, B, C)
     assert np.array_equal(got, O.ozaki2_exact(A, B, nmod))
 
 
-@pytest.mark.parametrize("nmod", [9, 14, 15, 17])
+@pytest.mark.parametrize("nmod", [9, 14, 15, 16, 17, 20])
 @pytest.mark.parametrize("scale", [-540, 0, 500])
 def test_bitwise_across_the_exponent_range(h, nmod, scale):
     """Products that land in the subnormal range (~2^-1080), near 1 and near the overflow
     threshold (~2^1000), with a wide dynamic range inside each row: bit for bit the exact
-    restatement (the exact integer product rounded once, then scaled) for both reconstruction
-    forms -- three FP64 limbs and a correctly rounded three-term sum up to 15 moduli, 32-bit
-    integer limbs above."""
+    restatement (the exact integer product rounded once, then scaled) for every reconstruction
+    form -- three FP64 limbs and a correctly rounded three-term sum up to 15 moduli, four FP64
+    limbs with an integer rounding above, 32-bit integer limbs in the generic kernels."""
     m, n, k = 37, 29, 90
     A, B, _ = operands("N", "N", m, n, k, 70 + nmod, phi=2.0)
     A, B = np.ldexp(A, scale), np.ldexp(B, scale)
