@@ -126,6 +126,14 @@ constexpr int F3_MAX = 15;  // 15 terms r W_l < 2^49 sum below 2^53; P < 2^123 f
 #define DGT_RECON_F4 1
 #endif
 constexpr int F4_MAX = DGT_RECON_F4 ? 20 : 0;
+// Up to F3_MAX moduli: 0 rounds C' with the correctly rounded three-term FP64 sum
+// (crt_value_f3), 1 in integers as above 15 moduli (crt_value_fi); the same doubles either way.
+// Measured on one box, alternating builds: 16384^3 at 14 moduli 53.3-53.9 ms per call with the
+// FP64 sum against 54.9-55.9 with the integer rounding, the 256-product grouped pass at 15
+// moduli 15.4-15.5 against 15.7-15.9 ms.
+#ifndef DGT_RECON_F3_INT
+#define DGT_RECON_F3_INT 0
+#endif
 
 // One product of a grouped reconstruction: its residue planes, exponents, scaling and output;
 // it owns threads [thread_begin, thread_begin + ceil(m/4) n) of the launch.  count > 1 makes

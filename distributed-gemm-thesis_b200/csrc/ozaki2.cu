@@ -549,46 +549,59 @@ __device__ __forceinline__ double crt_value_f3(const uint32_t (&rr)[MAX_MODULI],
     return oz::scale2(zm, ez - 63 + shift);
 }
 
-// The same value as crt_value for F3_MAX < n <= F4_MAX moduli: the limb sums through the FP64
-// pipe, the rounding in integers.  X = S0 + S1 2^40 + S2 2^80 + S3 2^120 with
-// S_l = sum_j r_j w_jl (w_jl the 40-bit limbs of W_j: every term below 2^48, at most 20 of
-// them below 2^53, exact).  q = round(X / P) from S_l fl(2^(40 l) / P) (X / P < 20 * 255 <
-// 2^13, the estimate within 2^-37, inside the 2^-21 margin the norm rule leaves), and
-// d_l = S_l - q P_l is exact (q P_l < 2^53, the difference an integer below 2^53).  The d_l
-// become 64-bit integers, carries make the low three 40-bit digits non-negative (the top one
-// keeps the sign: |C'| < P / 2 < 2^159), and the digits pack into three 64-bit words of C' in
-// two's complement.  Its magnitude is rounded exactly as crt_value rounds it (top word, the
-// word below, a sticky bit for the rest, one conversion), so the result is the same double.
-template <int NM>
-__device__ __forceinline__ double crt_value_f4(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
+// The same value as crt_value with the limb sums through the FP64 pipe and the rounding in
+// integers: L = 3 limbs of 41 bits (the F3 constants, up to F3_MAX moduli) or L = 4 limbs of
+// 40 bits (F3_MAX < n <= F4_MAX).  X = sum_l S_l 2^(B l) with S_l = sum_j r_j w_jl (w_jl the
+// B-bit limbs of W_j: every term below 2^(B+8), the sum below 2^53, exact).  q = round(X / P)
+// from S_l fl(2^(B l) / P) (X / P < 20 * 255 < 2^13, the estimate within 2^-37, inside the
+// 2^-21 margin the norm rule leaves), and d_l = S_l - q P_l is exact (q P_l < 2^53, the
+// difference an integer below 2^53).  The d_l become 64-bit integers, carries make the low
+// L - 1 digits non-negative (the top one keeps the sign: |C'| < P / 2), and the digits pack
+// into three 64-bit words of C' in two's complement.  Its magnitude is rounded exactly as
+// crt_value rounds it (top word, the word below, a sticky bit for the rest, one conversion),
+// so the result is the same double.
+template <int L, int NM>
+__device__ __forceinline__ double crt_value_fi(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
                                                int shift) {
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    static_assert(L == 3 || L == 4, "FP64 limb sums: 3 or 4 limbs");
+    constexpr int B = L == 3 ? 41 : 40;
+    double sl[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) sl[l] = 0.0;
 #pragma unroll
     for (int j = 0; j < MAX_MODULI; ++j) {
         if (NM ? j < NM : j < cc.n) {
             const uint32_t r = __byte_perm(rr[j], 0u, 0x4440u + (uint32_t)sel);  // byte sel
             const double rd = __hiloint2double(0x43300000, (int)r) - 4503599627370496.0;
-            s0 = fma(rd, cc.Wf4[j][0], s0);
-            s1 = fma(rd, cc.Wf4[j][1], s1);
-            s2 = fma(rd, cc.Wf4[j][2], s2);
-            s3 = fma(rd, cc.Wf4[j][3], s3);
+#pragma unroll
+            for (int l = 0; l < L; ++l) sl[l] = fma(rd, L == 3 ? cc.Wf[j][l] : cc.Wf4[j][l], sl[l]);
         }
     }
-    const double q = rint(fma(s3, cc.Kf4[3], fma(s2, cc.Kf4[2], fma(s1, cc.Kf4[1], s0 * cc.Kf4[0]))));
-    long long d0 = __double2ll_rn(fma(-q, cc.Pf4[0], s0)), d1 = __double2ll_rn(fma(-q, cc.Pf4[1], s1));
-    long long d2 = __double2ll_rn(fma(-q, cc.Pf4[2], s2)), d3 = __double2ll_rn(fma(-q, cc.Pf4[3], s3));
-    constexpr long long M40 = (1ll << 40) - 1;
-    d1 += d0 >> 40;  // arithmetic shifts: floor division by 2^40
-    d0 &= M40;
-    d2 += d1 >> 40;
-    d1 &= M40;
-    d3 += d2 >> 40;
-    d2 &= M40;
-    // C' = d3 2^120 + d2 2^80 + d1 2^40 + d0, digits d0..d2 in [0, 2^40), as words
-    uint64_t w0 = (uint64_t)d0 | ((uint64_t)d1 << 40);
-    uint64_t w1 = ((uint64_t)d1 >> 24) | ((uint64_t)d2 << 16) | ((uint64_t)d3 << 56);
-    uint64_t w2 = (uint64_t)(d3 >> 8);
-    const bool neg = d3 < 0;
+    double xq = sl[0] * (L == 3 ? cc.Kf[0] : cc.Kf4[0]);
+#pragma unroll
+    for (int l = 1; l < L; ++l) xq = fma(sl[l], L == 3 ? cc.Kf[l] : cc.Kf4[l], xq);
+    const double q = rint(xq);
+    long long d[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) d[l] = __double2ll_rn(fma(-q, L == 3 ? cc.Pf[l] : cc.Pf4[l], sl[l]));
+    constexpr long long MB = (1ll << B) - 1;
+#pragma unroll
+    for (int l = 0; l + 1 < L; ++l) {
+        d[l + 1] += d[l] >> B;  // arithmetic shift: floor division by 2^B
+        d[l] &= MB;
+    }
+    // C' = sum_l d_l 2^(B l), digits d_0 .. d_(L-2) in [0, 2^B), as three words (the top
+    // digit's arithmetic shifts fill the words above it with its sign)
+    uint64_t w[3] = {0ull, 0ull, 0ull};
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        const int o = B * l, i = o / 64, sh = o % 64;
+        w[i] |= (uint64_t)d[l] << sh;
+        if (sh > 0 && i + 1 < 3) w[i + 1] |= (uint64_t)(d[l] >> (64 - sh));
+        if (l == L - 1 && i + 2 < 3) w[i + 2] = (uint64_t)(d[l] >> 63);
+    }
+    uint64_t w0 = w[0], w1 = w[1], w2 = w[2];
+    const bool neg = d[L - 1] < 0;
     if (neg) {  // magnitude -C' (three-word two's complement negation)
         const uint64_t n0 = ~w0 + 1ull;
         const uint64_t c0 = w0 == 0ull ? 1ull : 0ull;
@@ -615,8 +628,8 @@ __device__ __forceinline__ double crt_value_f4(const uint32_t (&rr)[MAX_MODULI],
     const int lz = __clzll((long long)hi);
     const uint64_t top64 = lz ? (hi << lz) | (lo >> (64 - lz)) : hi;
     sticky |= (lz ? (lo << lz) : lo) != 0ull;
-    const double d = __ull2double_rn(top64 | (uint64_t)sticky);
-    const double mag = oz::scale2(d, 64 * ti - lz + shift);
+    const double dv = __ull2double_rn(top64 | (uint64_t)sticky);
+    const double mag = oz::scale2(dv, 64 * ti - lz + shift);
     return neg ? -mag : mag;
 }
 
@@ -628,11 +641,15 @@ template <int NW, int NM>
 __device__ __forceinline__ double crt_value(const uint32_t (&rr)[MAX_MODULI], int sel, const CrtConst& cc,
                                             int shift) {
     if constexpr (NM != 0 && NM <= F3_MAX) {
-        return crt_value_f3<NM>(rr, sel, cc, shift);  // the FP64 form (same value)
+        if constexpr (DGT_RECON_F3_INT)
+            return crt_value_fi<3, NM>(rr, sel, cc, shift);  // FP64 limb sums, integer rounding
+        else
+            return crt_value_f3<NM>(rr, sel, cc, shift);  // the FP64 form (same value)
     } else if constexpr (NM != 0 && NM <= F4_MAX) {
-        return crt_value_f4<NM>(rr, sel, cc, shift);  // FP64 limb sums, integer rounding (same value)
+        return crt_value_fi<4, NM>(rr, sel, cc, shift);  // FP64 limb sums, integer rounding (same value)
     } else {
-    if (NM == 0 && cc.n <= F3_MAX) return crt_value_f3<0>(rr, sel, cc, shift);
+    if (NM == 0 && cc.n <= F3_MAX)
+        return DGT_RECON_F3_INT ? crt_value_fi<3, 0>(rr, sel, cc, shift) : crt_value_f3<0>(rr, sel, cc, shift);
     constexpr int NX = NW + 1;
     // The low NI limbs accumulate in 64-bit integers, the high ones in FP64, which is exact:
     // r W_l < 2^40 and at most 20 of them sum below 2^45 < 2^53.  Splitting the multiply-adds
