@@ -547,6 +547,57 @@ def sum3_rn(a: float, b: float, c: float) -> float:
     return th + add_round_odd(tl, ul)
 
 
+def crt_value_fi(residues, nmod: int, limbs: int) -> float:
+    """The reconstruction's FP64-limb form with the integer rounding (csrc/ozaki2.cu
+    crt_value_fi<L>, before the 2^shift scaling) restated step by step: S_l = sum_j r_j w_jl
+    over the B-bit limbs of the CRT weights W_j (B = 41 for 3 limbs, 40 for 4); q =
+    rint(S_0 K_0 + S_1 K_1 + ...) with K_l = fl(2^(B l) / fl(P)) and fl(P) accumulated from
+    P's 32-bit words as the host code does; d_l = fma(-q, P_l, S_l); carries that leave the
+    low digits in [0, 2^B); three 64-bit words of C' in two's complement; the magnitude's top
+    word, the word below and a sticky bit for the rest; one correctly rounded conversion.
+    Returns C' as the double the kernel hands the scaling.  Pure Python, small samples."""
+    import math
+
+    B = 41 if limbs == 3 else 40
+    mods = OZAKI2_MODULI[:nmod]
+    P = 1
+    for p in mods:
+        P *= p
+    mask = (1 << B) - 1
+    S = [0] * limbs
+    for r, p in zip(residues, mods):
+        M = P // p
+        W = M * pow(M % p, -1, p)
+        for l in range(limbs):
+            S[l] += int(r) * ((W >> (B * l)) & mask)
+    pd = 0.0
+    for i in reversed(range(6)):  # the host's fl(P): 32-bit words from the top
+        pd = pd * 4294967296.0 + float((P >> (32 * i)) & 0xFFFFFFFF)
+    K = [math.ldexp(1.0, B * l) / pd for l in range(limbs)]
+    xq = float(S[0]) * K[0]
+    for l in range(1, limbs):
+        xq = _fma(float(S[l]), K[l], xq)
+    q = float(round(xq))  # rint: ties to even
+    d = [int(_fma(-q, float((P >> (B * l)) & mask), float(S[l]))) for l in range(limbs)]
+    for l in range(limbs - 1):
+        d[l + 1] += d[l] >> B
+        d[l] &= mask
+    v = sum(d[l] << (B * l) for l in range(limbs))  # the three words' value, two's complement
+    neg = v < 0
+    mag = -v if neg else v
+    w = [(mag >> (64 * i)) & 0xFFFFFFFFFFFFFFFF for i in range(3)]
+    ti = 2 if w[2] else (1 if w[1] else 0)
+    hi, lo = w[ti], (w[ti - 1] if ti > 0 else 0)
+    sticky = ti == 2 and w[0] != 0
+    if hi == 0:
+        return 0.0
+    lz = 64 - hi.bit_length()
+    top64 = ((hi << lz) | (lo >> (64 - lz))) & 0xFFFFFFFFFFFFFFFF if lz else hi
+    sticky = sticky or (((lo << lz) & 0xFFFFFFFFFFFFFFFF) if lz else lo) != 0
+    val = math.ldexp(float(top64 | int(sticky)), 64 * ti - lz)
+    return -val if neg else val
+
+
 def ozaki2_sigmas(nmod: int, k: int):
     """(sigma_A, sigma_B) for nmod moduli and inner dimension k: s = sigma_A + sigma_B is the
     largest with (2^ceil(s/2) + sqrt(k)/2)(2^floor(s/2) + sqrt(k)/2) < (P/2)(1 - 2^-20), checked

@@ -116,6 +116,32 @@ def test_three_term_sum_is_correctly_rounded():
         assert O.sum3_rn(a, b, c) == float(Fraction(a) + Fraction(b) + Fraction(c)), (d0, d1, d2)
 
 
+@pytest.mark.parametrize("nmod,limbs", [(14, 3), (15, 3), (16, 4), (18, 4), (20, 4)])
+def test_limb_sums_with_integer_rounding(nmod, limbs):
+    """The reconstruction's FP64-limb form with the integer rounding (oracle.crt_value_fi
+    restates the kernel's steps) returns C' -- the symmetric residue of sum_j r_j W_j mod P --
+    rounded once to nearest-even: random residues, and residues of values one bit past the
+    53rd with ties and their neighbours, both signs, against Python's exact integers."""
+    import random
+
+    rnd = random.Random(100 + nmod)
+    mods = O.OZAKI2_MODULI[:nmod]
+    P = math.prod(mods)
+    targets = []
+    for _ in range(150):
+        r = [rnd.randrange(p) for p in mods]
+        x = sum(ri * (P // p) * pow((P // p) % p, -1, p) for ri, p in zip(r, mods)) % P
+        targets.append(x - P if x > P // 2 else x)
+    for _ in range(150):
+        s_ = rnd.randint(54, int(math.log2(P)) - 3)
+        C = (2 * rnd.randint(2 ** 52, 2 ** 53 - 1) + 1) * 2 ** (s_ - 54) + rnd.choice([-1, 0, 1])
+        targets.append(C * rnd.choice([-1, 1]))
+    targets += [0, 1, -1, 2 ** 53 + 1, -(2 ** 53 + 1)]
+    for C in targets:
+        res = [C % p for p in mods]
+        assert O.crt_value_fi(res, nmod, limbs) == float(C), (nmod, C)
+
+
 def _exact_max_scaled(A, B, nmod):
     """The same integer emulation with every row / column scaled by its max instead (the
     bound k 2^(2 beta) < P/2): the reference point the norm scaling improves on."""
